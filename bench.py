@@ -1,0 +1,406 @@
+"""Benchmark: fwd+bwd Mpix/s of the tetrahedral tile rasterizer (training step).
+
+Workload (default): 200,000 points drawn as a mixture of 64 anisotropic
+Gaussians plus 10% uniform background (seed 2), Delaunay-tetrahedralised
+(~1.3M tets), fp32 features with 30% of densities at 1e-4, one 1297x840
+camera on a radius-4 ring at height 0.5, 16x16 tiles, L1 loss against a
+random target.  A step is: projection, scan/emit/sort/ranges, blend forward,
+L1 loss, blend backward (the drop-in autograd path), and on N>1 ranks an
+NCCL all-reduce of the vertex and cell-value gradients (each rank renders its
+own ring view: data-parallel multi-view training, weak scaling).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Rank 0 prints one JSON line.  --impl reference times the CPU restatement of
+the reference path (the oracle, OpenMP on all host cores) on a bounded tile
+sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd Mpix/s @1.3M tets"
+UNIT = "Mpix/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--points", type=int, default=200_000)
+    ap.add_argument("--tile", type=int, default=16)
+    ap.add_argument("--height", type=int, default=840)
+    ap.add_argument("--width", type=int, default=1297)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=0, help="(profiling) run N steps after warmup, print nothing")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def workload(args, rank, world):
+    from radiance_meshes_b200 import scenes
+
+    mesh, view = scenes.workload_training_step(n_points=args.points, seed=2, tile_size=args.tile,
+                                               height=args.height, width=args.width)
+    if world > 1 and rank > 0:
+        th = 2.0 * math.pi * rank / world
+        view = scenes._view((4.0 * math.cos(th), 0.5, 4.0 * math.sin(th)), (0.0, 0.0, 0.0), args.height,
+                            args.width, 60.0, args.tile)
+    return mesh, view
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        if vis:
+            ids = [x.strip() for x in vis.split(",") if x.strip()]
+            index = ids[index] if index < len(ids) else index
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(k)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- b200 arm --
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    import radiance_meshes_b200 as RMB
+    from radiance_meshes_b200 import _capi
+    from radiance_meshes_b200 import rasterizer as R
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    RMB.install_dropin()
+    from delaunay_rasterization.internal.alphablend_tiled_slang_interp import AlphaBlendTiledRender
+    from delaunay_rasterization.internal.render_grid import RenderGrid
+    from delaunay_rasterization.internal.tile_shader_slang import vertex_and_tile_shader
+
+    mesh, view = workload(args, rank, world)
+    H, W = view.height, view.width
+    T, V = len(mesh.indices), len(mesh.vertices)
+    tcam = view.tcam(device=dev)
+    grid = RenderGrid(H, W, tile_width=args.tile, tile_height=args.tile)
+    rng = np.random.default_rng(1000 + rank)
+    target_h = torch.from_numpy(rng.uniform(size=(H, W, 3)).astype(np.float32))
+    verts_h = torch.from_numpy(mesh.vertices).pin_memory()
+    idx_h = torch.from_numpy(mesh.indices).pin_memory()
+    cv_h = torch.from_numpy(mesh.cell_values).pin_memory()
+    target_h = target_h.pin_memory()
+    verts = verts_h.to(dev).requires_grad_(True)
+    cv = cv_h.to(dev).requires_grad_(True)
+    idx = idx_h.to(dev)
+    target = target_h.to(dev)
+    jitter = torch.full((H, W, 2), 0.5, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    stats = {}
+
+    def step(v, c, i, tgt):
+        v.grad = None
+        c.grad = None
+        sorted_ids, ranges, vs, cc, mask, rect = vertex_and_tile_shader(i, v, tcam, grid)
+        img, distimg, _ = AlphaBlendTiledRender.apply(sorted_ids, ranges, i, v, c, grid, tcam, jitter, "cuda",
+                                                      mask.to(torch.int32))
+        loss = (img[..., :3] - tgt).abs().mean()
+        loss.backward()
+        if world > 1:
+            dist.all_reduce(v.grad)
+            dist.all_reduce(c.grad)
+        stats["P"] = int(sorted_ids.shape[0])
+        return loss, img
+
+    for _ in range(args.warmup):
+        step(verts, cv, idx, target)
+    torch.cuda.synchronize()
+    if args.profile_steps:
+        for _ in range(args.profile_steps):
+            step(verts, cv, idx, target)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    # ---- device-resident timing: K steps, per-step events, L2 flushed between steps
+    launches0 = _capi.launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    times = []
+    timer = R.StageTimer()
+    with ClockSampler(local) as clocks, timer:
+        for _ in range(args.steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            loss, img = step(verts, cv, idx, target)
+            b.record()
+            times.append((a, b))
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = _capi.launch_count() - launches0
+    total_ms = sum(a.elapsed_time(b) for a, b in times)
+    stages = timer.totals()
+    # Σ n_contrib of the last frame: the number of ray/tet tests per pass
+    # (the issue-rate unit), from a separate untimed forward
+    with torch.no_grad():
+        sorted_ids, ranges, vs, cc, mask, rect = vertex_and_tile_shader(idx, verts, tcam, grid)
+        _, _, ncs, _ = R.blend_fwd(sorted_ids, ranges, idx, verts.detach(), cv.detach(), jitter, R.camera(tcam),
+                                   tiles_touched=mask.to(torch.int32))
+        tests = int(ncs.sum().item())
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+    # ---- end to end: host buffers in, loss out, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        verts_d = torch.empty_like(verts)
+        cv_d = torch.empty_like(cv)
+        idx_d = torch.empty_like(idx)
+        tgt_d = torch.empty_like(target)
+        loss_h = torch.empty(1, dtype=torch.float32).pin_memory()
+        e2e_times = []
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            verts_d.detach().copy_(verts_h, non_blocking=True)
+            cv_d.detach().copy_(cv_h, non_blocking=True)
+            idx_d.copy_(idx_h, non_blocking=True)
+            tgt_d.copy_(target_h, non_blocking=True)
+            vd = verts_d.detach().requires_grad_(True)
+            cd = cv_d.detach().requires_grad_(True)
+            loss, _ = step(vd, cd, idx_d, tgt_d)
+            loss_h.copy_(loss.detach().reshape(1), non_blocking=True)
+            b.record()
+            b.synchronize()
+            e2e_times.append((a, b))
+        e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_times)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        h2d = (verts_h.numel() * 4 + cv_h.numel() * 4 + idx_h.numel() * 4 + target_h.numel() * 4)
+        e2e = {"value": world * H * W * args.steps / (e2e_ms * 1e-3) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4,
+               "ms_per_step": e2e_ms / args.steps}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    Npx = H * W
+    P = stats["P"]
+    G = grid.grid_width * grid.grid_height
+    value = world * Npx * args.steps / (total_ms * 1e-3) / 1e6
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        with open(pk) as f:
+            peaks = json.load(f)
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    # algorithmic bytes per launch of the dominant kernel (blend backward):
+    # 8G + 96P read (ranges, ids + 92 B tet record), 84 Npx read (saved state
+    # 40, grads 36, jitter 8), 2*(28T + 12V) gradient read-modify-write
+    per_stage = {k: {"ms_per_step": v[0] / args.steps, "calls": v[1]} for k, v in stages.items()}
+    dom = max(stages.items(), key=lambda kv: kv[1][0])[0]
+    bytes_alg = {
+        "rm_blend_bwd": 8 * G + 96 * P + 84 * Npx + 2 * (28 * T + 12 * V),
+        "rm_blend_fwd": 8 * G + 96 * P + 8 * Npx + 44 * Npx + T * (16 + 48 + 28 + 128),
+        "rm_sort_pairs": 24 * P,
+        "rm_project_fwd": 12 * V + 16 * T + 36 * T,
+    }
+    dom_ms = stages[dom][0] / stages[dom][1]
+    achieved = bytes_alg.get(dom, 0) / (dom_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get(dom)
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+            "frac": achieved / hbm_peak, "peak_source": peak_src, "traffic": traffic,
+            "algorithmic_bytes": int(bytes_alg.get(dom, 0)), "avg_launch_ms": dom_ms,
+            "issue": {"ray_tet_tests_per_pass": tests,
+                      "tests_per_s_fwd_plus_bwd": 2 * tests / (total_ms * 1e-3 / args.steps)}}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"training step: {args.points} mixture points, {T} tets, {W}x{H}, "
+                               f"tile {args.tile}, L1 loss", "tets": T, "points": args.points,
+                   "image": [H, W], "tile": args.tile, "pairs": P, "parallelism": f"dp{world} (views)" if world > 1
+                   else "single view", "l2": "flushed between steps (256 MiB write)",
+                   "seed": 2},
+        "e2e": e2e, "roofline": roof, "stages_ms": per_stage, "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(mesh, view, args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------- CPU (reference) --
+def cpu_sample(mesh, view, budget_s, target_frac=None):
+    """FP32 restatement of the reference path (oracle) on a bounded sample:
+    full projection / scan / sort / ranges, then blend fwd + L1 bwd on an even
+    subset of tiles.  Returns (Mpix/s, seconds, sample description, threads)."""
+    from oracle import oracle as O
+
+    tcam = view.tcam()
+    H, W = view.height, view.width
+    t0 = time.perf_counter()
+    L = O.rasterize_lists(mesh.indices, mesh.vertices, tcam)
+    t_lists = time.perf_counter() - t0
+    G = L["cam"].grid_width * L["cam"].grid_height
+    jitter = np.full((H, W, 2), 0.5, np.float32)
+    target = np.random.default_rng(1000).uniform(size=(H, W, 3)).astype(np.float32)
+    frac = target_frac or 1.0 / 64
+    while True:
+        stride = max(1, int(round(1.0 / frac)))
+        mask = np.zeros(G, np.uint8)
+        mask[::stride] = 1
+        t0 = time.perf_counter()
+        O.blend_fwd_bwd_f32_sample(L, mesh.indices, mesh.vertices, mesh.cell_values, jitter, mask, target)
+        t_blend = time.perf_counter() - t0
+        if target_frac is not None or t_blend > 0.2 * budget_s or stride == 1:
+            break
+        frac = min(1.0, frac * max(2.0, 0.5 * budget_s / max(t_blend, 1e-3)))
+    sample_tiles = int(mask.sum())
+    sample_frac = sample_tiles / G
+    px = sample_frac * H * W
+    t = t_lists * sample_frac + t_blend
+    return px / t / 1e6, t, (f"{sample_tiles}/{G} tiles ({px:.0f} px) fwd+bwd + stages a-c scaled by the tile "
+                             f"fraction (stages a-c {t_lists:.2f}s on all {len(mesh.indices)} tets)"), \
+        O.max_threads(), frac
+
+
+def cpu_baseline(mesh, view, budget_s):
+    mpix, t, desc, threads, _ = cpu_sample(mesh, view, budget_s)
+    return {"value": mpix, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc,
+            "what": "FP32 C++ restatement of the reference (oracle/), OpenMP"}
+
+
+def run_reference(args):
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    mesh, view = workload(args, 0, 1)
+    frac = None
+    for _ in range(args.warmup):
+        _, _, _, _, frac = cpu_sample(mesh, view, args.cpu_seconds, frac)
+    vals, secs = [], []
+    desc, threads = "", 0
+    for _ in range(args.steps):
+        mpix, t, desc, threads, frac = cpu_sample(mesh, view, args.cpu_seconds, frac)
+        vals.append(mpix)
+        secs.append(t)
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(secs)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"training step: {args.points} mixture points, {len(mesh.indices)} tets, "
+                               f"{view.width}x{view.height}, tile {args.tile}, L1 loss", "tets": len(mesh.indices),
+                   "image": [view.height, view.width], "tile": args.tile},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's path is Slang compiled by slangtorch, which is not installable offline; this arm "
+                "times the C++ restatement of that path (oracle/) on the host cores",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

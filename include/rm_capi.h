@@ -1,0 +1,214 @@
+/*
+ * rm_capi.h - C ABI of the B200 tetrahedral tile rasterizer (sm_100a).
+ *
+ * Each entry point replaces one kernel launch (or one library call) of the
+ * reference rasterizer in delaunay_rasterization/internal/.  Arguments are raw
+ * device pointers, element counts, a POD camera and a cudaStream_t passed as
+ * void*.  No torch types cross this boundary.  Every function returns an int
+ * status (RM_OK on success) and never throws; the message of the last failure
+ * on the calling thread is available from rm_last_error().
+ *
+ * Memory ownership: the caller allocates every buffer, including scratch
+ * ("workspace") memory whose size is returned by the *_workspace_size queries
+ * (two-phase, as with CUB).  The library itself never calls cudaMalloc on the
+ * render path.  All launches are stream-ordered; apart from rm_read_status no
+ * call synchronises the host with the device.
+ *
+ * Tensor layouts follow the reference: indices [T,4] int32, vertices [V,3]
+ * float32, cell_values [T,7] float32 (density, r, g, b, gx, gy, gz),
+ * ray_jitter [H,W,2], output image [H,W,4] (r, g, b, log-transmittance),
+ * distortion [H,W,5], n_contributors [H,W] int32, tile ranges [G,2] int32.
+ */
+#ifndef RM_CAPI_H
+#define RM_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define RM_API __attribute__((visibility("default")))
+#else
+#define RM_API
+#endif
+
+/* Status codes. */
+#define RM_OK 0
+#define RM_EINVAL 1      /* bad argument (null pointer, size, unsupported camera)   */
+#define RM_ECAPACITY 2   /* an output buffer is smaller than the pairs produced       */
+#define RM_ECUDA 3       /* a CUDA runtime call failed                                */
+#define RM_ETIMEOUT 4    /* a bounded device-side wait gave up (see rm_read_status)   */
+
+/* Bits of the device status word written by kernels that wait on other CTAs. */
+#define RM_STATUS_SCAN_TIMEOUT 0x1u
+#define RM_STATUS_SORT_TIMEOUT 0x2u
+#define RM_STATUS_CAPACITY 0x4u
+#define RM_STATUS_QUEUE_TIMEOUT 0x8u
+
+/*
+ * Pinhole camera.  Mirrors the reference's TensorCamera/Camera
+ * (delaunay_rasterization/internal/slang/camera.slang:13-76) as filled by
+ * utils/train_util.py:31-38 and data/camera.py:72-91.
+ * world_view is row-major world->camera (tcam['world_view_transform']),
+ * K is row-major 3x3 intrinsics.  Only camera_type 0 (perspective) with zero
+ * distortion is supported; anything else is rejected with RM_EINVAL.
+ */
+typedef struct rm_camera {
+    float world_view[16];
+    float K[9];
+    float cam_pos[3];
+    float min_t;
+    float distortion[4];
+    int32_t camera_type;
+    int32_t image_height;
+    int32_t image_width;
+    int32_t tile_height;
+    int32_t tile_width;
+    int32_t grid_height;
+    int32_t grid_width;
+    int32_t reserved;
+} rm_camera;
+
+/* Message of the last failing call on this thread ("" if none). */
+RM_API const char* rm_last_error(void);
+RM_API int rm_abi_version(void);
+
+/* Number of kernels this library has launched in the calling process. */
+RM_API uint64_t rm_launch_count(void);
+
+/*
+ * Copies the device status word (RM_STATUS_* bits) held in a workspace to the
+ * host and clears it.  This is the only call here that synchronises `stream`.
+ */
+RM_API int rm_read_status(const uint32_t* status_dev, uint32_t* status_host, void* stream);
+
+/* ---------------------------------------------------------------- stage (a) */
+/*
+ * Per-tet projection, cull, tile rectangle and depth key.
+ * Replaces vertex_shader (delaunay_rasterization/internal/slang/vertex_shader.slang:23-89)
+ * launched by VertexShader.forward (delaunay_rasterization/internal/tile_shader_slang.py:77-105).
+ * Every output row is written (culled tets get zeros), so the caller need not
+ * zero the outputs.  vs is [T,3] with only column 2 (the float depth key) set,
+ * as in the reference.
+ */
+RM_API int rm_project_fwd(const int32_t* indices, const float* vertices, int64_t n_tets,
+                   int64_t n_verts, const rm_camera* cam, int32_t* tiles_touched,
+                   int32_t* rect, float* vs, float* circumcenter, void* stream);
+
+/*
+ * Adjoint of the projection: dL/dvertices from dL/dvs[:,2] and dL/dcircumcenter
+ * through the FP64 circumsphere power.  Replaces vertex_shader.bwd
+ * (delaunay_rasterization/internal/tile_shader_slang.py:128-150).
+ * grad_vertices [V,3] is accumulated into (atomics); the caller zeroes it.
+ * grad_vs or grad_circumcenter may be NULL (treated as zeros).
+ */
+RM_API int rm_project_bwd(const int32_t* indices, const float* vertices, int64_t n_tets,
+                   int64_t n_verts, const rm_camera* cam, const int32_t* tiles_touched,
+                   const float* grad_vs, const float* grad_circumcenter,
+                   float* grad_vertices, void* stream);
+
+/* ---------------------------------------------------------------- stage (b) */
+RM_API size_t rm_scan_workspace_size(int64_t n_tets);
+
+/*
+ * Inclusive int32 prefix sum of tiles_touched; the total pair count P is
+ * written to *total_dev (int64, device memory).  Replaces
+ * torch.cumsum(tiles_touched) at delaunay_rasterization/internal/tile_shader_slang.py:36.
+ * Single pass with decoupled look-back; a look-back that waits too long sets
+ * RM_STATUS_SCAN_TIMEOUT in the workspace status word (first 4 bytes).
+ */
+RM_API int rm_scan_tiles(const int32_t* tiles_touched, int64_t n_tets, int32_t* offsets,
+                  int64_t* total_dev, void* workspace, size_t workspace_bytes,
+                  void* stream);
+
+/*
+ * Tile/tet pair emission: key = (tile_id << 32) | sortable(depth), value = tet
+ * id, rows in row-major rectangle order at the tet's exclusive offset.
+ * Replaces generate_keys (delaunay_rasterization/internal/slang/tile_shader.slang:138-186)
+ * launched at delaunay_rasterization/internal/tile_shader_slang.py:46-55.
+ * Pairs at positions >= capacity are dropped; if total_dev is non-NULL and
+ * *total_dev > capacity, RM_STATUS_CAPACITY is or-ed into *status_dev
+ * (status_dev may be NULL).
+ */
+RM_API int rm_emit_pairs(const float* vs, const int32_t* rect, const int32_t* offsets,
+                  int64_t n_tets, int32_t grid_width, int64_t capacity,
+                  const int64_t* total_dev, int64_t* keys, int32_t* values,
+                  uint32_t* status_dev, void* stream);
+
+/* ---------------------------------------------------------------- stage (c) */
+RM_API size_t rm_sort_workspace_size(int64_t n);
+
+/*
+ * Stable LSD radix sort (onesweep) of (key, value) pairs on key bits
+ * [0, end_bit).  Replaces sort_by_keys
+ * (delaunay_rasterization/internal/sort_by_keys/sort_by_keys.cu:10-53), which
+ * calls cub::DeviceRadixSort::SortPairs with end_bit = 32 + highest_tile_id_msb
+ * (delaunay_rasterization/internal/tile_shader_slang.py:57-59).
+ * n is the buffer capacity; if n_dev is non-NULL the pair count is read from
+ * device memory (<= n) so the call can be captured in a CUDA graph.
+ * Inputs are not modified.  Look-back waits are bounded (RM_STATUS_SORT_TIMEOUT).
+ */
+RM_API int rm_sort_pairs(const int64_t* keys_in, const int32_t* values_in, int64_t n,
+                  const int64_t* n_dev, int end_bit, int64_t* keys_out,
+                  int32_t* values_out, void* workspace, size_t workspace_bytes,
+                  void* stream);
+
+/*
+ * Per-tile [start, end) ranges of the sorted pair list; empty tiles get [0,0].
+ * Replaces compute_tile_ranges (delaunay_rasterization/internal/slang/tile_shader.slang:188-214)
+ * launched at delaunay_rasterization/internal/tile_shader_slang.py:61-69 (the
+ * ranges buffer is zero-filled here, as the reference's torch.zeros does).
+ */
+RM_API int rm_tile_ranges(const int64_t* sorted_keys, int64_t n, const int64_t* n_dev,
+                   int32_t* ranges, int64_t n_tiles, void* stream);
+
+/* ---------------------------------------------------------------- stage (d) */
+/* Bytes of packed per-tet records (128 B per tet) the blend passes need. */
+RM_API size_t rm_blend_workspace_size(int64_t n_tets);
+
+#define RM_BLEND_REUSE_RECORDS 0x1  /* workspace already holds this frame's records */
+
+/*
+ * Front-to-back tile blend.  Replaces splat_tiled
+ * (delaunay_rasterization/internal/slang/alphablend_shader_interp.slang:371-431,
+ * alpha_blend at :194-271) launched by AlphaBlendTiledRender.forward
+ * (delaunay_rasterization/internal/alphablend_tiled_slang_interp.py:165-202).
+ * tiles_touched may be NULL; when given, records are packed only for visible
+ * tets.  Writes every pixel of out_img [H,W,4], out_distortion [H,W,5] and
+ * n_contrib [H,W].
+ */
+RM_API int rm_blend_fwd(const int32_t* sorted_ids, const int32_t* ranges,
+                 const int32_t* indices, const float* vertices,
+                 const float* cell_values, int64_t n_tets, int64_t n_verts,
+                 const int32_t* tiles_touched, const float* ray_jitter,
+                 const rm_camera* cam, float* out_img, float* out_distortion,
+                 int32_t* n_contrib, void* workspace, size_t workspace_bytes,
+                 int flags, void* stream);
+
+/*
+ * Back-to-front adjoint of the blend.  Replaces splat_tiled.bwd
+ * (delaunay_rasterization/internal/alphablend_tiled_slang_interp.py:220-262),
+ * i.e. bwd_alpha_blend (delaunay_rasterization/internal/slang/alphablend_shader_interp.slang:273-369).
+ * grad_vertices [V,3] and grad_cell_values [T,7] are accumulated into; the
+ * caller zeroes them.  grad_distortion may be NULL (zeros).
+ */
+RM_API int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges,
+                 const int32_t* indices, const float* vertices,
+                 const float* cell_values, int64_t n_tets, int64_t n_verts,
+                 const int32_t* tiles_touched, const float* ray_jitter,
+                 const rm_camera* cam, const float* out_img,
+                 const float* out_distortion, const int32_t* n_contrib,
+                 const float* grad_img, const float* grad_distortion,
+                 float* grad_vertices, float* grad_cell_values, void* workspace,
+                 size_t workspace_bytes, int flags, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RM_CAPI_H */

@@ -1,0 +1,993 @@
+// rm_oracle.cpp - CPU oracle for the tetrahedral tile rasterizer.
+//
+// TEST INFRASTRUCTURE ONLY.  Nothing on the product path links, loads or calls
+// this file; only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+// leg use it, as the checker.
+//
+// It restates, in plain C++, the reference rasterizer of Radiance Meshes
+// (delaunay_rasterization/internal/slang/*.slang and sort_by_keys.cu):
+//
+//   * orc_project      vertex_shader.slang:23-89, camera.slang:104-170,382-508,
+//                      stable_power.slang:18-85, intersect.slang:76-89
+//   * orc_scan_emit    tile_shader_slang.py:36-55, tile_shader.slang:107-186
+//   * orc_sort         sort_by_keys.cu:36-48 (stable, bits [0, end_bit))
+//   * orc_ranges       tile_shader.slang:188-214
+//   * orc_blend_fwd_*  alphablend_shader_interp.slang:194-271,374-431,
+//                      interp_version.slang:21-126, intersect.slang:394-624,
+//                      camera.slang:298-346, safe-math.slang:137-172
+//   * orc_blend_bwd_*  alphablend_shader_interp.slang:128-192,273-369 with the
+//                      per-tet derivatives written out by hand (the reference
+//                      gets them from Slang autodiff of the functions above)
+//   * orc_project_bwd  adjoint of power_of_circumsphere (stable_power.slang:18-85)
+//   * orc_quadrature   midpoint quadrature of jaxutil/tetra_quad.py:58-99,143-224,
+//                      evaluated over exact ray/tet segments instead of brute force
+//
+// Rounding rules (shared with the CUDA kernels, which are written separately):
+// every dot product is an FMA chain  dot(a,b) = fma(a.z,b.z, fma(a.y,b.y, a.x*b.x)),
+// cross(a,b).x = fma(a.y,b.z, -(a.z*b.y)) (and cyclic), a*b+c in the reference
+// source is fma(a,b,c), lerp(x,y,s) = fma(y,s, x*(1-s)), normalize(v) = v/sqrt(dot(v,v)),
+// division and sqrt are IEEE correctly rounded, nothing else is contracted
+// (build with -ffp-contract=off).  Under these rules the integer outputs
+// (tile counts, rectangles, keys, sorted order, ranges, n_contributors) and the
+// log-transmittance channel are reproducible bit for bit on CPU and GPU.
+// The blend's colour path uses exp/expm1, whose last bits differ between libm
+// and CUDA; it is compared within a tolerance.
+//
+// The template parameter F selects FP32 (the bit-exact restatement) or FP64
+// (the judge integrator: same closed-form segment integral, double precision).
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include <omp.h>
+
+#include "../include/rm_capi.h"
+
+#define ORC_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+template <typename F>
+struct V3 {
+    F x, y, z;
+};
+
+template <typename F>
+inline V3<F> operator-(V3<F> a, V3<F> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <typename F>
+inline V3<F> operator+(V3<F> a, V3<F> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <typename F>
+inline V3<F> scale(V3<F> a, F s) { return {a.x * s, a.y * s, a.z * s}; }
+template <typename F>
+inline V3<F> neg(V3<F> a) { return {-a.x, -a.y, -a.z}; }
+template <typename F>
+inline F dot(V3<F> a, V3<F> b) { return std::fma(a.z, b.z, std::fma(a.y, b.y, a.x * b.x)); }
+template <typename F>
+inline V3<F> cross(V3<F> a, V3<F> b) {
+    return {std::fma(a.y, b.z, -(a.z * b.y)), std::fma(a.z, b.x, -(a.x * b.z)),
+            std::fma(a.x, b.y, -(a.y * b.x))};
+}
+// Plain (unrounded-order-free) helpers for adjoint arithmetic, where no
+// bit-exactness is claimed.
+template <typename F>
+inline V3<F> axpy(F a, V3<F> x, V3<F> y) { return {a * x.x + y.x, a * x.y + y.y, a * x.z + y.z}; }
+
+template <typename F>
+struct Cam {
+    F M[16], K[9], pos[3], min_t;
+    int H, W, th, tw, gh, gw;
+};
+
+template <typename F>
+Cam<F> load_cam(const rm_camera* c) {
+    Cam<F> r;
+    for (int i = 0; i < 16; ++i) r.M[i] = (F)c->world_view[i];
+    for (int i = 0; i < 9; ++i) r.K[i] = (F)c->K[i];
+    for (int i = 0; i < 3; ++i) r.pos[i] = (F)c->cam_pos[i];
+    r.min_t = (F)c->min_t;
+    r.H = c->image_height;
+    r.W = c->image_width;
+    r.th = c->tile_height;
+    r.tw = c->tile_width;
+    r.gh = c->grid_height;
+    r.gw = c->grid_width;
+    return r;
+}
+
+// ------------------------------------------------------------- projection ---
+const float kTiny = 1.0754944e-20f;  // safe-math.slang:2
+
+inline float safe_clipf(float v, float lo, float hi) { return std::fmax(std::fmin(v, hi), lo); }
+inline float safe_divf(float a, float b) {  // safe-math.slang:72-79
+    if (std::fabs(b) < kTiny) return safe_clipf(a / kTiny, -1e20f, 1e20f);
+    return safe_clipf(a / b, -1e20f, 1e20f);
+}
+
+// point2camspace (camera.slang:103-108): h = M * (p, 1), then h.xyz / h.w.
+inline V3<float> point2cam(const Cam<float>& c, V3<float> p) {
+    float h[4];
+    for (int k = 0; k < 4; ++k) {
+        const float* m = c.M + 4 * k;
+        h[k] = std::fma(m[3], 1.0f, std::fma(m[2], p.z, std::fma(m[1], p.y, m[0] * p.x)));
+    }
+    return {safe_divf(h[0], h[3]), safe_divf(h[1], h[3]), safe_divf(h[2], h[3])};
+}
+
+// camspace_to_image for a perspective camera without distortion (camera.slang:382-412).
+inline V3<float> cam2image(const Cam<float>& c, V3<float> p) {
+    float ux = p.x / p.z;
+    float uy = p.y / p.z;
+    return {std::fma(ux, c.K[0], c.K[2]), std::fma(uy, c.K[4], c.K[5]), p.z};
+}
+
+inline V3<float> lerp3(V3<float> a, V3<float> b, float s) {
+    float w = 1.0f - s;
+    return {std::fma(b.x, s, a.x * w), std::fma(b.y, s, a.y * w), std::fma(b.z, s, a.z * w)};
+}
+
+// find_extent (camera.slang:443-508): near-plane clip of each face at z = 1e-4,
+// then the image-space bounding box of the clipped polygons (2 samples per edge).
+void find_extent(const Cam<float>& c, const V3<float> v[4], V3<float>& mn, V3<float>& mx) {
+    mn = {1e20f, 1e20f, 1e20f};
+    mx = {-1e20f, -1e20f, -1e20f};
+    const float eps = 1e-4f;
+    static const int faces[4][3] = {{0, 1, 2}, {0, 2, 3}, {0, 3, 1}, {1, 3, 2}};
+    for (int f = 0; f < 4; ++f) {
+        V3<float> fv[3] = {v[faces[f][0]], v[faces[f][1]], v[faces[f][2]]};
+        V3<float> out[4];
+        int n = 0;
+        for (int j = 0; j < 3; ++j) {
+            V3<float> a = fv[j], b = fv[(j + 1) % 3];
+            bool ain = a.z > eps, bin = b.z > eps;
+            if (ain) {
+                bool found = false;
+                for (int k = 0; k < n; ++k)
+                    if (out[k].x == a.x && out[k].y == a.y && out[k].z == a.z) found = true;
+                if (!found) out[n++] = a;
+            }
+            if (ain != bin) {
+                float t = (eps - a.z) / (b.z - a.z);
+                out[n++] = lerp3(a, b, t);
+            }
+        }
+        if (n > 1) {
+            for (int j = 0; j < n; ++j) {
+                V3<float> s = out[j], e = out[(j + 1) % n];
+                for (int i = 0; i < 2; ++i) {
+                    float t = (float)i / 1.0f;
+                    V3<float> p = cam2image(c, lerp3(s, e, t));
+                    mn = {std::fmin(mn.x, p.x), std::fmin(mn.y, p.y), std::fmin(mn.z, p.z)};
+                    mx = {std::fmax(mx.x, p.x), std::fmax(mx.y, p.y), std::fmax(mx.z, p.z)};
+                }
+            }
+        }
+    }
+}
+
+// is_planar (intersect.slang:76-89).
+bool is_planar(const V3<float> v[4]) {
+    V3<float> n = cross(v[1] - v[0], v[2] - v[0]);
+    float l = std::sqrt(dot(n, n));
+    n = {n.x / l, n.y / l, n.z / l};
+    float d = dot(n, v[3] - v[0]);
+    return std::fabs(d) < 1e-3f;
+}
+
+inline double dlen(V3<double> a) { return std::sqrt(dot(a, a)); }
+
+// power_of_circumsphere (stable_power.slang:18-85), FP64.
+double power_of_circumsphere(V3<double> A, V3<double> B, V3<double> C, V3<double> D,
+                             V3<double> P, V3<double>& center) {
+    V3<double> a = B - A, b = C - A, c = D - A;
+    double aa = dot(a, a), bb = dot(b, b), cc = dot(c, c);
+    V3<double> cbc = cross(b, c), cca = cross(c, a), cab = cross(a, b);
+    double den = 2.0 * dot(a, cbc);
+    double radius;
+    if (std::fabs(den) < 1e-10) {
+        double m = std::fmax(dlen(B - A), std::fmax(dlen(C - A), std::fmax(dlen(D - A),
+                   std::fmax(dlen(C - B), std::fmax(dlen(D - B), dlen(D - C))))));
+        if (m < 1e-7) {
+            V3<double> s = ((A + B) + C) + D;
+            center = scale(s, 0.25);
+            radius = std::fmin(dlen(A - center), std::fmin(dlen(B - center),
+                     std::fmin(dlen(C - center), dlen(D - center))));
+            V3<double> df = center - P;
+            return dot(df, df) - radius * radius;
+        }
+        return -1e20;
+    }
+    V3<double> rel = {std::fma(cc, cab.x, std::fma(bb, cca.x, aa * cbc.x)) / den,
+                      std::fma(cc, cab.y, std::fma(bb, cca.y, aa * cbc.y)) / den,
+                      std::fma(cc, cab.z, std::fma(bb, cca.z, aa * cbc.z)) / den};
+    center = A + rel;
+    radius = dlen(rel);
+    V3<double> df = center - P;
+    return dot(df, df) - radius * radius;
+}
+
+inline V3<float> load_v(const float* verts, int i) {
+    return {verts[3 * (int64_t)i], verts[3 * (int64_t)i + 1], verts[3 * (int64_t)i + 2]};
+}
+
+inline uint32_t sortable(float v) {  // float2sortable_key (tile_shader.slang:107-136)
+    uint32_t b;
+    std::memcpy(&b, &v, 4);
+    return (b & 0x80000000u) ? ~b : (b ^ 0x80000000u);
+}
+
+// ------------------------------------------------------------------ blend ---
+template <typename F>
+struct Rec {
+    V3<F> n[4];
+    V3<F> v[4];
+    F density;
+    F base[3];
+    V3<F> grd;
+    F cv0;  // raw density (for the max(.,0) adjoint)
+};
+
+template <typename F>
+void make_rec(const V3<F> v[4], const F* cv, Rec<F>& r) {
+    V3<F> n0 = cross(v[1] - v[0], v[2] - v[0]);
+    if (dot(n0, v[3] - v[0]) > 0) n0 = neg(n0);
+    V3<F> n1 = cross(v[1] - v[0], v[3] - v[0]);
+    if (dot(n1, v[2] - v[0]) > 0) n1 = neg(n1);
+    V3<F> n2 = cross(v[2] - v[0], v[3] - v[0]);
+    if (dot(n2, v[1] - v[0]) > 0) n2 = neg(n2);
+    V3<F> n3 = cross(v[2] - v[1], v[3] - v[1]);
+    if (dot(n3, v[0] - v[1]) > 0) n3 = neg(n3);
+    r.n[0] = n0; r.n[1] = n1; r.n[2] = n2; r.n[3] = n3;
+    for (int i = 0; i < 4; ++i) r.v[i] = v[i];
+    r.cv0 = cv[0];
+    r.density = std::fmax(cv[0], F(0));
+    r.base[0] = cv[1]; r.base[1] = cv[2]; r.base[2] = cv[3];
+    r.grd = {cv[4], cv[5], cv[6]};
+}
+
+// get_ray (camera.slang:298-346), perspective without distortion.
+template <typename F>
+void make_ray(const Cam<F>& c, int px, int py, F jx, F jy, V3<F>& o, V3<F>& d) {
+    F ux = ((F)px + jx - c.K[2]) / c.K[0];
+    F uy = ((F)py + jy - c.K[5]) / c.K[4];
+    V3<F> dc = {ux, uy, F(1)};
+    F l = std::sqrt(dot(dc, dc));
+    dc = {dc.x / l, dc.y / l, dc.z / l};
+    V3<F> dw = {dot(V3<F>{c.M[0], c.M[4], c.M[8]}, dc), dot(V3<F>{c.M[1], c.M[5], c.M[9]}, dc),
+                dot(V3<F>{c.M[2], c.M[6], c.M[10]}, dc)};
+    l = std::sqrt(dot(dw, dw));
+    d = {dw.x / l, dw.y / l, dw.z / l};
+    o = {std::fma(d.x, c.min_t, c.pos[0]), std::fma(d.y, c.min_t, c.pos[1]),
+         std::fma(d.z, c.min_t, c.pos[2])};
+}
+
+// ray_tetrahedron_intersect_fused (intersect.slang:394-624) followed by the
+// clamps of evaluate_tetra_interp (interp_version.slang:88-89).
+template <typename F>
+struct Hit {
+    F t_enter_raw, t_exit_raw;  // before the clamps
+    F enter, exit;
+    int ie, ix;  // entering / exiting plane (-1: none)
+};
+
+template <typename F>
+bool intersect(const Rec<F>& r, V3<F> o, V3<F> d, Hit<F>& h) {
+    V3<F> a0 = r.v[0] - o, a1 = r.v[1] - o;
+    F te = F(-1e30), tx = F(1e30);
+    int ie = -1, ix = -1;
+    for (int i = 0; i < 4; ++i) {
+        F dist = -dot(r.n[i], i == 3 ? a1 : a0);
+        F den = dot(r.n[i], d);
+        if (std::fabs(den) < F(1e-10)) {
+            if (dist > F(0)) return false;
+        } else {
+            F tp = -dist / den;
+            if (den < F(0)) {
+                if (tp > te) { te = tp; ie = i; }
+            } else {
+                if (tp < tx) { tx = tp; ix = i; }
+            }
+        }
+    }
+    if (te > tx) return false;
+    if (tx <= F(0)) return false;
+    h.t_enter_raw = te;
+    h.t_exit_raw = tx;
+    h.enter = std::fmax(te, F(0));
+    h.exit = std::fmax(tx, h.enter);
+    h.ie = ie;
+    h.ix = ix;
+    return true;
+}
+
+template <typename F>
+inline F safe_exp(F v) {  // safe-math.slang:137-140
+    const F hi = (F)std::log(1e20);
+    return std::exp(std::fmax(std::fmin(v, hi), F(-1e20)));
+}
+
+template <typename F>
+inline F phi_fn(F x) {  // interp_version.slang:21-28
+    if (std::fabs(x) < F(1e-6)) return F(1) - x / F(2);
+    return -std::expm1(-x) / x;
+}
+
+// d phi / dx.  The autodiff expression exp(-x)/x + expm1(-x)/x^2 cancels badly
+// for small x in FP32; below the switch point a Taylor series of the same
+// function is used (-1/2 + x/3 - x^2/8 + x^3/30).
+template <typename F>
+inline F dphi_fn(F x) {
+    const F sw = sizeof(F) == 4 ? F(1e-2) : F(1e-4);
+    if (std::fabs(x) < sw) return F(-0.5) + x * (F(1) / F(3) + x * (F(-0.125) + x * (F(1) / F(30))));
+    return std::exp(-x) / x + std::expm1(-x) / (x * x);
+}
+
+template <typename F>
+struct Seg {
+    F rgb[3];
+    F a;          // density * dt
+    F dt;         // max(exit - enter, 0)
+    F c_enter, c_exit;  // scalar colour offsets dot(grd, v - v0)
+    F phi, alpha;
+    V3<F> ve, vx;  // enter/exit points relative to v0
+};
+
+// integrate_tetra_segment + compute_integral (interp_version.slang:30-69).
+template <typename F>
+void integrate(const Rec<F>& r, V3<F> o, V3<F> d, F enter, F exit, Seg<F>& s) {
+    s.dt = std::fmax(exit - enter, F(0));
+    s.ve = {std::fma(enter, d.x, o.x) - r.v[0].x, std::fma(enter, d.y, o.y) - r.v[0].y,
+            std::fma(enter, d.z, o.z) - r.v[0].z};
+    s.vx = {std::fma(exit, d.x, o.x) - r.v[0].x, std::fma(exit, d.y, o.y) - r.v[0].y,
+            std::fma(exit, d.z, o.z) - r.v[0].z};
+    s.c_enter = dot(r.grd, s.ve);
+    s.c_exit = dot(r.grd, s.vx);
+    F x = s.dt * r.density;
+    s.alpha = safe_exp(-x);
+    s.phi = phi_fn(x);
+    F w0 = s.phi - s.alpha, w1 = F(1) - s.phi;
+    for (int k = 0; k < 3; ++k) {
+        F ce = s.c_enter + r.base[k], cx = s.c_exit + r.base[k];
+        s.rgb[k] = std::fma(w1, ce, w0 * cx);
+    }
+    s.a = r.density * s.dt;
+}
+
+template <typename F>
+struct State {
+    F c[3];
+    F logT;
+    F D[5];
+};
+
+template <typename F>
+void update(State<F>& st, const Rec<F>& r, const Hit<F>& h, const Seg<F>& s) {
+    F T = safe_exp(st.logT);
+    for (int k = 0; k < 3; ++k) st.c[k] = std::fma(s.rgb[k], T, st.c[k]);
+    st.logT = st.logT - s.a;
+    F m0 = r.density;
+    F m1 = r.density * (h.exit + h.enter) / F(2);
+    F D2 = st.D[2], D3 = st.D[3];
+    st.D[0] = std::fma(F(2) * m1, D2, st.D[0]);
+    st.D[1] = std::fma(F(2) * m0, D3, st.D[1]);
+    st.D[2] = D2 + m0;
+    st.D[3] = D3 + m1;
+    st.D[4] = st.D[4] + r.density * r.density * s.dt / F(3);
+}
+
+struct Arrays {
+    const int32_t* ids;
+    const int32_t* ranges;
+    const int32_t* indices;
+    const float* jitter;
+};
+
+template <typename F>
+void build_recs(const int32_t* indices, const F* verts, const F* cv, int64_t T,
+                std::vector<Rec<F>>& recs, const std::vector<char>& need) {
+    recs.resize(T);
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < T; ++g) {
+        if (!need[g]) continue;
+        V3<F> v[4];
+        for (int i = 0; i < 4; ++i) {
+            int64_t vi = indices[4 * g + i];
+            v[i] = {verts[3 * vi], verts[3 * vi + 1], verts[3 * vi + 2]};
+        }
+        make_rec(v, cv + 7 * g, recs[g]);
+    }
+}
+
+std::vector<char> needed_tets(const int32_t* ids, const int32_t* ranges, int64_t G, int64_t T) {
+    std::vector<char> need(T, 0);
+    for (int64_t t = 0; t < G; ++t)
+        for (int32_t j = ranges[2 * t]; j < ranges[2 * t + 1]; ++j) need[ids[j]] = 1;
+    return need;
+}
+
+// Forward blend of one tile (alpha_blend, alphablend_shader_interp.slang:194-271).
+// cut == nullptr: per-pixel termination at log T < -5.5 (the reference rule).
+// cut != nullptr: exactly the first cut[pixel] entries are processed; own_nc
+// then receives where this precision's termination rule would have stopped.
+template <typename F>
+void blend_tile(int64_t tile, const Cam<F>& c, const Arrays& A, const std::vector<Rec<F>>& recs,
+                F* img, F* dist, int32_t* nc_out, const int32_t* cut, int32_t* own_nc,
+                const char* tile_mask, int64_t* inversions) {
+    int tx = (int)(tile % c.gw), ty = (int)(tile / c.gw);
+    if (tile_mask && !tile_mask[tile]) return;
+    int32_t s0 = A.ranges[2 * tile], s1 = A.ranges[2 * tile + 1];
+    for (int ly = 0; ly < c.th; ++ly)
+        for (int lx = 0; lx < c.tw; ++lx) {
+            int px = tx * c.tw + lx, py = ty * c.th + ly;
+            if (px >= c.W || py >= c.H) continue;
+            int64_t pix = (int64_t)py * c.W + px;
+            V3<F> o, d;
+            make_ray(c, px, py, (F)A.jitter[2 * pix], (F)A.jitter[2 * pix + 1], o, d);
+            State<F> st = {{0, 0, 0}, 0, {0, 0, 0, 0, 0}};
+            int32_t nc = 0, own = -1;
+            int32_t limit = cut ? cut[pix] : (s1 - s0);
+            F last_enter = F(-1);
+            for (int32_t j = s0; j < s1 && nc < limit; ++j) {
+                ++nc;
+                const Rec<F>& r = recs[A.ids[j]];
+                Hit<F> h;
+                if (!intersect(r, o, d, h)) continue;
+                Seg<F> s;
+                integrate(r, o, d, h.enter, h.exit, s);
+                if (!(s.a > F(0))) continue;
+                if (inversions && h.enter + F(1e-5) < last_enter) ++*inversions;
+                last_enter = h.enter;
+                update(st, r, h, s);
+                if (st.logT < F(-5.5)) {
+                    if (own < 0) own = nc;
+                    if (!cut) break;
+                }
+            }
+            if (own_nc) own_nc[pix] = own < 0 ? nc : own;
+            nc_out[pix] = nc;
+            for (int k = 0; k < 3; ++k) img[4 * pix + k] = st.c[k];
+            img[4 * pix + 3] = st.logT;
+            for (int k = 0; k < 5; ++k) dist[5 * pix + k] = st.D[k];
+        }
+}
+
+template <typename F>
+void blend_fwd(const int32_t* ids, const int32_t* ranges, const int32_t* indices, const F* verts,
+               const F* cv, int64_t T, const float* jitter, const rm_camera* cam, F* img, F* dist,
+               int32_t* nc, const int32_t* cut, int32_t* own_nc, const char* tile_mask,
+               int64_t* inversions) {
+    Cam<F> c = load_cam<F>(cam);
+    int64_t G = (int64_t)c.gw * c.gh;
+    std::vector<Rec<F>> recs;
+    build_recs(indices, verts, cv, T, recs, needed_tets(ids, ranges, G, T));
+    Arrays A = {ids, ranges, indices, jitter};
+    int64_t inv = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : inv)
+    for (int64_t t = 0; t < G; ++t) {
+        int64_t local = 0;
+        blend_tile(t, c, A, recs, img, dist, nc, cut, own_nc, tile_mask, inversions ? &local : nullptr);
+        inv += local;
+    }
+    if (inversions) *inversions = inv;
+}
+
+// Adjoint of one hit (the Slang autodiff of update_alpha_out,
+// evaluate_tetra_interp and load_tet_alphablend_interp, written out by hand).
+// Inputs: the state BEFORE the hit (old) and dL/d(state after the hit) in dS.
+// On return dS holds dL/d(old state); the per-tet gradients go to gv (4x3
+// vertex gradients) and gcv (7 cell-value gradients).
+template <typename F>
+void hit_adjoint(const Rec<F>& r, V3<F> o, V3<F> d, const Hit<F>& h, const Seg<F>& s,
+                 const State<F>& old, State<F>& dS, V3<F> gv[4], F gcv[7]) {
+    const F dens = r.density;
+    // ---- update_distortion_state
+    F m1 = dens * (h.exit + h.enter) / F(2);
+    F dm1 = dS.D[0] * F(2) * old.D[2] + dS.D[3];
+    F dm0 = dS.D[1] * F(2) * old.D[3] + dS.D[2];
+    F nD2 = dS.D[2] + dS.D[0] * F(2) * m1;
+    F nD3 = dS.D[3] + dS.D[1] * F(2) * dens;
+    F d_dens = dm0 + dm1 * (h.exit + h.enter) / F(2);
+    F d_enter = dm1 * dens / F(2);
+    F d_exit = dm1 * dens / F(2);
+    // self_dist = dens*dens*max(exit-enter,0)/3
+    F d_dt = dS.D[4] * dens * dens / F(3);
+    d_dens += dS.D[4] * F(2) * dens * s.dt / F(3);
+    // ---- update_pixel_state
+    F T = safe_exp(old.logT);
+    F d_rgb[3];
+    F dT = 0;
+    for (int k = 0; k < 3; ++k) {
+        d_rgb[k] = dS.c[k] * T;
+        dT += dS.c[k] * s.rgb[k];
+    }
+    F d_a = -dS.logT;
+    F d_logT_old = dS.logT + (old.logT < (F)std::log(1e20) ? dT * T : F(0));
+    // ---- compute_integral: rgb = w0*c_exit + w1*c_enter
+    F x = s.dt * dens;
+    F w0 = s.phi - s.alpha, w1 = F(1) - s.phi;
+    F d_w0 = 0, d_w1 = 0, d_sx = 0, d_se = 0;
+    for (int k = 0; k < 3; ++k) {
+        F ce = s.c_enter + r.base[k], cx = s.c_exit + r.base[k];
+        d_w0 += d_rgb[k] * cx;
+        d_w1 += d_rgb[k] * ce;
+        F dcx = d_rgb[k] * w0, dce = d_rgb[k] * w1;
+        gcv[1 + k] += dcx + dce;
+        d_sx += dcx;
+        d_se += dce;
+    }
+    F d_phi = d_w0 - d_w1;
+    F d_x = d_phi * dphi_fn(x) + d_w0 * s.alpha;  // d(-exp(-x))/dx = exp(-x)
+    // x = dt*dens, a = dens*dt
+    d_dt += d_x * dens + d_a * dens;
+    d_dens += d_x * s.dt + d_a * s.dt;
+    // c_enter = dot(grd, ve), ve = enter*d + o - v0 (likewise exit)
+    gcv[4] += d_se * s.ve.x + d_sx * s.vx.x;
+    gcv[5] += d_se * s.ve.y + d_sx * s.vx.y;
+    gcv[6] += d_se * s.ve.z + d_sx * s.vx.z;
+    V3<F> dve = scale(r.grd, d_se), dvx = scale(r.grd, d_sx);
+    d_enter += dot(dve, d);
+    d_exit += dot(dvx, d);
+    gv[0] = gv[0] - (dve + dvx);
+    // dt = max(exit - enter, 0)
+    if (h.exit - h.enter > F(0)) {
+        d_exit += d_dt;
+        d_enter -= d_dt;
+    }
+    // density = max(cv0, 0)
+    if (r.cv0 > F(0)) gcv[0] += d_dens;
+    // exit = max(t_exit, enter); enter = max(t_enter, 0)
+    F d_texit = 0, d_tenter = 0;
+    if (h.t_exit_raw > h.enter) d_texit = d_exit; else d_enter += d_exit;
+    if (h.t_enter_raw > F(0)) d_tenter = d_enter;
+    // t = dot(n, vref - o) / dot(n, d) for the selected planes
+    const int plane_p[4] = {1, 1, 2, 2}, plane_q[4] = {0, 0, 0, 1}, plane_r[4] = {2, 3, 3, 3};
+    const int sel[2] = {h.ie, h.ix};
+    const F dts[2] = {d_tenter, d_texit};
+    for (int w = 0; w < 2; ++w) {
+        int i = sel[w];
+        if (i < 0 || dts[w] == F(0)) continue;
+        V3<F> n = r.n[i];
+        V3<F> vr = r.v[i == 3 ? 1 : 0];
+        F den = dot(n, d);
+        F t = w == 0 ? h.t_enter_raw : h.t_exit_raw;
+        F g = dts[w] / den;
+        V3<F> gn = scale((vr - o) - scale(d, t), g);  // dt/dn
+        V3<F> gvr = scale(n, g);                        // dt/dvref
+        gv[i == 3 ? 1 : 0] = gv[i == 3 ? 1 : 0] + gvr;
+        // n = +-cross(P - Q, R - Q)
+        int P = plane_p[i], Q = plane_q[i], R = plane_r[i];
+        V3<F> ea = r.v[P] - r.v[Q], eb = r.v[R] - r.v[Q];
+        V3<F> nraw = cross(ea, eb);
+        F sg = (nraw.x == n.x && nraw.y == n.y && nraw.z == n.z) ? F(1) : F(-1);
+        V3<F> gc = scale(gn, sg);
+        V3<F> ga = cross(eb, gc), gb = cross(gc, ea);
+        gv[P] = gv[P] + ga;
+        gv[R] = gv[R] + gb;
+        gv[Q] = gv[Q] - (ga + gb);
+    }
+    // ---- propagate to the old state
+    dS.logT = d_logT_old;
+    dS.D[2] = nD2;
+    dS.D[3] = nD3;
+}
+
+// undo_alpha_out (alphablend_shader_interp.slang:128-192).
+template <typename F>
+void undo(State<F>& st, const Rec<F>& r, const Hit<F>& h, const Seg<F>& s) {
+    F logT_old = st.logT + s.a;
+    F T = safe_exp(logT_old);
+    for (int k = 0; k < 3; ++k) st.c[k] = st.c[k] - s.rgb[k] * T;
+    st.logT = logT_old;
+    F m0 = r.density;
+    F m1 = r.density * (h.exit + h.enter) / F(2);
+    st.D[2] = st.D[2] - m0;
+    st.D[3] = st.D[3] - m1;
+    st.D[0] = st.D[0] - F(2) * m1 * st.D[2];
+    st.D[1] = st.D[1] - F(2) * m0 * st.D[3];
+    st.D[4] = st.D[4] - r.density * r.density * s.dt / F(3);
+}
+
+inline void atomic_addd(double* p, double v) {
+#pragma omp atomic
+    *p += v;
+}
+
+// bwd_alpha_blend (alphablend_shader_interp.slang:273-369): walk each tile's
+// list back to front from the saved final state, skipping list offsets >=
+// n_contrib, undo each hit and back-propagate.
+template <typename F>
+void blend_bwd(const int32_t* ids, const int32_t* ranges, const int32_t* indices, const F* verts,
+               const F* cv, int64_t T, const float* jitter, const rm_camera* cam, const F* img,
+               const F* dist, const int32_t* nc, const F* gimg, const F* gdist, double* gverts,
+               double* gcv, const char* tile_mask = nullptr) {
+    Cam<F> c = load_cam<F>(cam);
+    int64_t G = (int64_t)c.gw * c.gh;
+    std::vector<Rec<F>> recs;
+    build_recs(indices, verts, cv, T, recs, needed_tets(ids, ranges, G, T));
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t tile = 0; tile < G; ++tile) {
+        if (tile_mask && !tile_mask[tile]) continue;
+        int tx = (int)(tile % c.gw), ty = (int)(tile / c.gw);
+        int32_t s0 = ranges[2 * tile], s1 = ranges[2 * tile + 1];
+        for (int ly = 0; ly < c.th; ++ly)
+            for (int lx = 0; lx < c.tw; ++lx) {
+                int px = tx * c.tw + lx, py = ty * c.th + ly;
+                if (px >= c.W || py >= c.H) continue;
+                int64_t pix = (int64_t)py * c.W + px;
+                V3<F> o, d;
+                make_ray(c, px, py, (F)jitter[2 * pix], (F)jitter[2 * pix + 1], o, d);
+                State<F> st, dS;
+                for (int k = 0; k < 3; ++k) st.c[k] = img[4 * pix + k];
+                st.logT = img[4 * pix + 3];
+                for (int k = 0; k < 5; ++k) st.D[k] = dist[5 * pix + k];
+                for (int k = 0; k < 3; ++k) dS.c[k] = gimg[4 * pix + k];
+                dS.logT = gimg[4 * pix + 3];
+                for (int k = 0; k < 5; ++k) dS.D[k] = gdist ? gdist[5 * pix + k] : F(0);
+                int32_t n = nc[pix];
+                for (int32_t j = s1 - 1; j >= s0; --j) {
+                    if (j - s0 >= n) continue;
+                    int32_t g = ids[j];
+                    const Rec<F>& r = recs[g];
+                    Hit<F> h;
+                    if (!intersect(r, o, d, h)) continue;
+                    Seg<F> s;
+                    integrate(r, o, d, h.enter, h.exit, s);
+                    if (!(s.a > F(0))) continue;
+                    undo(st, r, h, s);
+                    V3<F> gv[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+                    F gc[7] = {0, 0, 0, 0, 0, 0, 0};
+                    hit_adjoint(r, o, d, h, s, st, dS, gv, gc);
+                    for (int k = 0; k < 7; ++k)
+                        if (gc[k] != F(0)) atomic_addd(&gcv[7 * (int64_t)g + k], (double)gc[k]);
+                    for (int i = 0; i < 4; ++i) {
+                        int64_t vi = indices[4 * (int64_t)g + i];
+                        atomic_addd(&gverts[3 * vi], (double)gv[i].x);
+                        atomic_addd(&gverts[3 * vi + 1], (double)gv[i].y);
+                        atomic_addd(&gverts[3 * vi + 2], (double)gv[i].z);
+                    }
+                }
+            }
+    }
+}
+
+}  // namespace
+
+// =========================================================== exported API ===
+
+ORC_API int orc_abi_version() { return RM_ABI_VERSION; }
+
+// Stage (a): vertex_shader.slang:23-89.  Outputs fully written (zeros if culled).
+ORC_API void orc_project(const int32_t* indices, const float* verts, int64_t T, const rm_camera* cam,
+                         int32_t* tiles, int32_t* rect, float* vs, float* cc) {
+    Cam<float> c = load_cam<float>(cam);
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < T; ++g) {
+        tiles[g] = 0;
+        for (int k = 0; k < 4; ++k) rect[4 * g + k] = 0;
+        for (int k = 0; k < 3; ++k) vs[3 * g + k] = 0.f, cc[3 * g + k] = 0.f;
+        V3<float> v[4];
+        for (int i = 0; i < 4; ++i) v[i] = load_v(verts, indices[4 * g + i]);
+        if (is_planar(v)) continue;
+        V3<float> cs[4];
+        for (int i = 0; i < 4; ++i) cs[i] = point2cam(c, v[i]);
+        V3<float> mn, mx;
+        find_extent(c, cs, mn, mx);
+        if (mx.z <= 0.0f) continue;
+        V3<double> D[4];
+        for (int i = 0; i < 4; ++i) D[i] = {(double)v[i].x, (double)v[i].y, (double)v[i].z};
+        V3<double> P = {(double)c.pos[0], (double)c.pos[1], (double)c.pos[2]};
+        V3<double> center = {0, 0, 0};
+        float depth = (float)power_of_circumsphere(D[0], D[1], D[2], D[3], P, center);
+        if (depth < -1e19f) continue;
+        int r0 = (int)std::floor(std::fmax(0.f, std::fmin((float)c.gw, mn.x / (float)c.tw)));
+        int r1 = (int)std::floor(std::fmax(0.f, std::fmin((float)c.gh, mn.y / (float)c.th)));
+        int r2 = (int)std::ceil(std::fmax(0.f, std::fmin((float)c.gw, mx.x / (float)c.tw)));
+        int r3 = (int)std::ceil(std::fmax(0.f, std::fmin((float)c.gh, mx.y / (float)c.th)));
+        int n = (r2 - r0) * (r3 - r1);
+        if (n == 0) continue;
+        tiles[g] = n;
+        rect[4 * g] = r0; rect[4 * g + 1] = r1; rect[4 * g + 2] = r2; rect[4 * g + 3] = r3;
+        vs[3 * g + 2] = std::fmin(std::fmax(depth, -1e20f), 1e20f);
+        cc[3 * g] = (float)center.x;
+        cc[3 * g + 1] = (float)center.y;
+        cc[3 * g + 2] = (float)center.z;
+    }
+}
+
+// Stage (b): inclusive scan + generate_keys.  Returns P.  Writes at most cap pairs.
+ORC_API int64_t orc_scan_emit(const int32_t* tiles, const int32_t* rect, const float* vs, int64_t T,
+                              int32_t gw, int32_t* offsets, int64_t* keys, int32_t* vals, int64_t cap) {
+    int32_t run = 0;
+    for (int64_t g = 0; g < T; ++g) {
+        run += tiles[g];
+        offsets[g] = run;
+    }
+    int64_t P = run;
+    if (!keys) return P;
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < T; ++g) {
+        int64_t off = g == 0 ? 0 : offsets[g - 1];
+        uint32_t fk = sortable(vs[3 * g + 2]);
+        for (int32_t y = rect[4 * g + 1]; y < rect[4 * g + 3]; ++y)
+            for (int32_t x = rect[4 * g]; x < rect[4 * g + 2]; ++x) {
+                uint64_t key = ((uint64_t)(uint32_t)(y * gw + x) << 32) | fk;
+                if (off < cap) {
+                    keys[off] = (int64_t)key;
+                    vals[off] = (int32_t)g;
+                }
+                ++off;
+            }
+    }
+    return P;
+}
+
+// Stage (c): stable sort on key bits [0, end_bit) (CUB SortPairs semantics).
+ORC_API void orc_sort(int64_t* keys, int32_t* vals, int64_t n, int end_bit) {
+    uint64_t mask = end_bit >= 64 ? ~0ull : ((1ull << end_bit) - 1);
+    std::vector<int64_t> idx(n);
+    for (int64_t i = 0; i < n; ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
+        return ((uint64_t)keys[a] & mask) < ((uint64_t)keys[b] & mask);
+    });
+    std::vector<int64_t> k2(n);
+    std::vector<int32_t> v2(n);
+    for (int64_t i = 0; i < n; ++i) k2[i] = keys[idx[i]], v2[i] = vals[idx[i]];
+    std::memcpy(keys, k2.data(), n * sizeof(int64_t));
+    std::memcpy(vals, v2.data(), n * sizeof(int32_t));
+}
+
+// compute_tile_ranges (tile_shader.slang:188-214) over zero-filled ranges.
+ORC_API void orc_ranges(const int64_t* keys, int64_t n, int32_t* ranges, int64_t G) {
+    std::memset(ranges, 0, sizeof(int32_t) * 2 * G);
+    for (int64_t i = 0; i < n; ++i) {
+        uint32_t cur = (uint32_t)((uint64_t)keys[i] >> 32);
+        if (i == 0) {
+            ranges[2 * (int64_t)cur] = 0;
+        } else {
+            uint32_t prev = (uint32_t)((uint64_t)keys[i - 1] >> 32);
+            if (cur != prev) {
+                ranges[2 * (int64_t)prev + 1] = (int32_t)i;
+                ranges[2 * (int64_t)cur] = (int32_t)i;
+            }
+        }
+        if (i == n - 1) ranges[2 * (int64_t)cur + 1] = (int32_t)n;
+    }
+}
+
+// Stage (d) forward, FP32 restatement (reference termination rule).
+ORC_API void orc_blend_fwd_f32(const int32_t* ids, const int32_t* ranges, const int32_t* indices,
+                               const float* verts, const float* cv, int64_t T, const float* jitter,
+                               const rm_camera* cam, float* img, float* dist, int32_t* nc) {
+    blend_fwd<float>(ids, ranges, indices, verts, cv, T, jitter, cam, img, dist, nc, nullptr,
+                     nullptr, nullptr, nullptr);
+}
+
+// FP32 forward / backward restricted to the tiles with tile_mask[t] != 0
+// (bounded CPU samples of a large workload).
+ORC_API void orc_blend_fwd_f32_masked(const int32_t* ids, const int32_t* ranges, const int32_t* indices,
+                                      const float* verts, const float* cv, int64_t T, const float* jitter,
+                                      const rm_camera* cam, float* img, float* dist, int32_t* nc,
+                                      const char* tile_mask) {
+    blend_fwd<float>(ids, ranges, indices, verts, cv, T, jitter, cam, img, dist, nc, nullptr, nullptr,
+                     tile_mask, nullptr);
+}
+
+ORC_API void orc_blend_bwd_f32_masked(const int32_t* ids, const int32_t* ranges, const int32_t* indices,
+                                      const float* verts, const float* cv, int64_t T, const float* jitter,
+                                      const rm_camera* cam, const float* img, const float* dist,
+                                      const int32_t* nc, const float* gimg, const float* gdist,
+                                      double* gverts, double* gcv, const char* tile_mask) {
+    blend_bwd<float>(ids, ranges, indices, verts, cv, T, jitter, cam, img, dist, nc, gimg, gdist, gverts, gcv,
+                     tile_mask);
+}
+
+// Stage (d) forward, FP64 judge integrator.  cut (nullable) imposes the
+// per-pixel list cut of the FP32 path; own_nc (nullable) receives where the
+// FP64 termination rule would stop; inversions (nullable) counts hits whose
+// entry distance goes backwards along the sorted list (power order vs depth).
+ORC_API void orc_blend_fwd_f64(const int32_t* ids, const int32_t* ranges, const int32_t* indices,
+                               const double* verts, const double* cv, int64_t T,
+                               const float* jitter, const rm_camera* cam, double* img,
+                               double* dist, int32_t* nc, const int32_t* cut, int32_t* own_nc,
+                               const char* tile_mask, int64_t* inversions) {
+    blend_fwd<double>(ids, ranges, indices, verts, cv, T, jitter, cam, img, dist, nc, cut, own_nc,
+                      tile_mask, inversions);
+}
+
+ORC_API void orc_blend_bwd_f32(const int32_t* ids, const int32_t* ranges, const int32_t* indices,
+                               const float* verts, const float* cv, int64_t T, const float* jitter,
+                               const rm_camera* cam, const float* img, const float* dist,
+                               const int32_t* nc, const float* gimg, const float* gdist,
+                               double* gverts, double* gcv) {
+    blend_bwd<float>(ids, ranges, indices, verts, cv, T, jitter, cam, img, dist, nc, gimg, gdist,
+                     gverts, gcv);
+}
+
+ORC_API void orc_blend_bwd_f64(const int32_t* ids, const int32_t* ranges, const int32_t* indices,
+                               const double* verts, const double* cv, int64_t T,
+                               const float* jitter, const rm_camera* cam, const double* img,
+                               const double* dist, const int32_t* nc, const double* gimg,
+                               const double* gdist, double* gverts, double* gcv) {
+    blend_bwd<double>(ids, ranges, indices, verts, cv, T, jitter, cam, img, dist, nc, gimg, gdist,
+                      gverts, gcv);
+}
+
+// Linear functional L = sum(wimg*img) + sum(wdist*dist) of the FP64 forward
+// with the per-pixel cut imposed, restricted to the tiles in tile_mask
+// (nullable = all).  Used for central finite differences.
+ORC_API double orc_linear_loss_f64(const int32_t* ids, const int32_t* ranges, const int32_t* indices,
+                                   const double* verts, const double* cv, int64_t T,
+                                   const float* jitter, const rm_camera* cam, const int32_t* cut,
+                                   const double* wimg, const double* wdist, const char* tile_mask) {
+    int64_t npx = (int64_t)cam->image_height * cam->image_width;
+    std::vector<double> img(4 * npx, 0.0), dist(5 * npx, 0.0);
+    std::vector<int32_t> nc(npx, 0);
+    blend_fwd<double>(ids, ranges, indices, verts, cv, T, jitter, cam, img.data(), dist.data(),
+                      nc.data(), cut, nullptr, tile_mask, nullptr);
+    double L = 0;
+    for (int64_t i = 0; i < 4 * npx; ++i) L += wimg[i] * img[i];
+    if (wdist)
+        for (int64_t i = 0; i < 5 * npx; ++i) L += wdist[i] * dist[i];
+    return L;
+}
+
+// Adjoint of the projection (vertex_shader.bwd): FP64 gradients of
+// vs[:,2] = clamp(float(power)) and circumcenter = float(center) w.r.t. the
+// four vertices of every tet with tiles[g] > 0.
+ORC_API void orc_project_bwd(const int32_t* indices, const float* verts, int64_t T,
+                             const rm_camera* cam, const int32_t* tiles, const float* gvs,
+                             const float* gcc, double* gverts) {
+    V3<double> P = {(double)cam->cam_pos[0], (double)cam->cam_pos[1], (double)cam->cam_pos[2]};
+    for (int64_t g = 0; g < T; ++g) {
+        if (tiles[g] <= 0) continue;
+        V3<double> X[4];
+        for (int i = 0; i < 4; ++i) {
+            V3<float> v = load_v(verts, indices[4 * g + i]);
+            X[i] = {(double)v.x, (double)v.y, (double)v.z};
+        }
+        V3<double> center;
+        double pw = power_of_circumsphere(X[0], X[1], X[2], X[3], P, center);
+        float pf = (float)pw;
+        double gp = gvs ? (double)gvs[3 * g + 2] : 0.0;
+        if (!(pf > -1e20f && pf < 1e20f)) gp = 0.0;  // clamp to +-1e20 on store
+        V3<double> gC = {gcc ? (double)gcc[3 * g] : 0.0, gcc ? (double)gcc[3 * g + 1] : 0.0,
+                         gcc ? (double)gcc[3 * g + 2] : 0.0};
+        V3<double> G[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        V3<double> a = X[1] - X[0], b = X[2] - X[0], c = X[3] - X[0];
+        double den = 2.0 * dot(a, cross(b, c));
+        V3<double> df = center - P;
+        if (std::fabs(den) < 1e-10) {
+            // centroid branch: center = mean, radius = min corner distance
+            V3<double> gcen = axpy(2.0 * gp, df, gC);
+            int im = 0;
+            double best = 1e300;
+            for (int i = 0; i < 4; ++i) {
+                double l = dlen(X[i] - center);
+                if (l < best) best = l, im = i;
+            }
+            // radius^2 term: -(|X_im - center|^2)
+            V3<double> e = X[im] - center;
+            V3<double> ge = scale(e, -2.0 * gp);
+            for (int i = 0; i < 4; ++i) G[i] = axpy(0.25, gcen - ge, G[i]);
+            G[im] = G[im] + ge;
+        } else {
+            V3<double> cbc = cross(b, c), cca = cross(c, a), cab = cross(a, b);
+            double aa = dot(a, a), bb = dot(b, b), cc = dot(c, c);
+            V3<double> N = {aa * cbc.x + bb * cca.x + cc * cab.x, aa * cbc.y + bb * cca.y + cc * cab.y,
+                            aa * cbc.z + bb * cca.z + cc * cab.z};
+            V3<double> rel = center - X[0];
+            V3<double> gcen = axpy(2.0 * gp, df, gC);
+            V3<double> grel = axpy(-2.0 * gp, rel, gcen);
+            V3<double> gN = scale(grel, 1.0 / den);
+            double gden = -dot(grel, N) / (den * den);
+            double gaa = dot(gN, cbc), gbb = dot(gN, cca), gcc2 = dot(gN, cab);
+            V3<double> gcbc = axpy(2.0 * gden, a, scale(gN, aa));
+            V3<double> gcca = scale(gN, bb), gcab = scale(gN, cc);
+            V3<double> ga = axpy(2.0 * gden, cbc, scale(a, 2.0 * gaa));
+            V3<double> gb = scale(b, 2.0 * gbb), gc = scale(c, 2.0 * gcc2);
+            gb = gb + cross(c, gcbc);
+            gc = gc + cross(gcbc, b);
+            gc = gc + cross(a, gcca);
+            ga = ga + cross(gcca, c);
+            ga = ga + cross(b, gcab);
+            gb = gb + cross(gcab, a);
+            G[0] = gcen - ((ga + gb) + gc);
+            G[1] = ga;
+            G[2] = gb;
+            G[3] = gc;
+        }
+        for (int i = 0; i < 4; ++i) {
+            int64_t vi = indices[4 * g + i];
+            gverts[3 * vi] += G[i].x;
+            gverts[3 * vi + 1] += G[i].y;
+            gverts[3 * vi + 2] += G[i].z;
+        }
+    }
+}
+
+// FP64 power and circumcenter of the given tets (for finite-difference checks
+// of orc_project_bwd).  Vertices are double here.
+ORC_API void orc_power_f64(const int32_t* indices, const double* verts, int64_t T,
+                           const double* P3, double* power, double* center) {
+    V3<double> P = {P3[0], P3[1], P3[2]};
+    for (int64_t g = 0; g < T; ++g) {
+        V3<double> X[4];
+        for (int i = 0; i < 4; ++i) {
+            int64_t vi = indices[4 * g + i];
+            X[i] = {verts[3 * vi], verts[3 * vi + 1], verts[3 * vi + 2]};
+        }
+        V3<double> c = {0, 0, 0};
+        power[g] = power_of_circumsphere(X[0], X[1], X[2], X[3], P, c);
+        center[3 * g] = c.x;
+        center[3 * g + 1] = c.y;
+        center[3 * g + 2] = c.z;
+    }
+}
+
+// Midpoint quadrature restating jaxutil/tetra_quad.py:58-99,143-224 (density and
+// density-weighted colour summed over the tets containing each sample, alpha
+// weights (1-exp(-sigma*dt))*exp(-sum)), evaluated over the exact per-ray
+// segments of the tile list instead of a brute-force point-in-tet test.  Uses
+// the kernel's colour-gradient columns (cell_values[:,4:7]).  Samples are
+// n_samples points linspace(t0, t1) along the ray from o = cam_pos + min_t*d,
+// where t0/t1 are per call.  No early termination.  Output rgb + alpha.
+ORC_API void orc_quadrature_f64(const int32_t* ids, const int32_t* ranges, const int32_t* indices,
+                                const double* verts, const double* cv, int64_t T,
+                                const float* jitter, const rm_camera* cam, double t0, double t1,
+                                int n_samples, double* out) {
+    Cam<double> c = load_cam<double>(cam);
+    int64_t G = (int64_t)c.gw * c.gh;
+    std::vector<Rec<double>> recs;
+    build_recs(indices, verts, cv, T, recs, needed_tets(ids, ranges, G, T));
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t tile = 0; tile < G; ++tile) {
+        int tx = (int)(tile % c.gw), ty = (int)(tile / c.gw);
+        int32_t s0 = ranges[2 * tile], s1 = ranges[2 * tile + 1];
+        std::vector<int32_t> hit_ids;
+        std::vector<double> en, ex;
+        for (int ly = 0; ly < c.th; ++ly)
+            for (int lx = 0; lx < c.tw; ++lx) {
+                int px = tx * c.tw + lx, py = ty * c.th + ly;
+                if (px >= c.W || py >= c.H) continue;
+                int64_t pix = (int64_t)py * c.W + px;
+                V3<double> o, d;
+                make_ray(c, px, py, (double)jitter[2 * pix], (double)jitter[2 * pix + 1], o, d);
+                hit_ids.clear();
+                en.clear();
+                ex.clear();
+                for (int32_t j = s0; j < s1; ++j) {
+                    Hit<double> h;
+                    if (!intersect(recs[ids[j]], o, d, h)) continue;
+                    hit_ids.push_back(ids[j]);
+                    en.push_back(h.enter);
+                    ex.push_back(h.exit);
+                }
+                double col[3] = {0, 0, 0}, acc = 0, alpha = 0;
+                double dtq = (t1 - t0) / (n_samples - 1);
+                for (int k = 0; k + 1 < n_samples; ++k) {
+                    double tm = t0 + (k + 0.5) * dtq;
+                    double sig = 0, wc[3] = {0, 0, 0};
+                    for (size_t q = 0; q < hit_ids.size(); ++q) {
+                        if (tm < en[q] || tm > ex[q]) continue;
+                        const Rec<double>& r = recs[hit_ids[q]];
+                        V3<double> p = {o.x + tm * d.x, o.y + tm * d.y, o.z + tm * d.z};
+                        double s = dot(r.grd, p - r.v[0]);
+                        sig += r.density;
+                        for (int ch = 0; ch < 3; ++ch) wc[ch] += r.density * (r.base[ch] + s);
+                    }
+                    double w = (1.0 - std::exp(-sig * dtq)) * std::exp(-acc);
+                    acc += sig * dtq;
+                    alpha += w;
+                    if (sig > 1e-6)
+                        for (int ch = 0; ch < 3; ++ch) col[ch] += w * wc[ch] / sig;
+                }
+                for (int ch = 0; ch < 3; ++ch) out[4 * pix + ch] = col[ch];
+                out[4 * pix + 3] = alpha;
+            }
+    }
+}
+
+ORC_API int orc_max_threads() { return omp_get_max_threads(); }
+ORC_API void orc_set_threads(int n) { omp_set_num_threads(n); }

@@ -1,0 +1,106 @@
+"""ctypes binding of ``librm_b200.so`` (declared in ``include/rm_capi.h``).
+
+The library is loaded from ``radiance_meshes_b200/lib``.  There is no fallback:
+if the library is missing or a call fails, a ``RuntimeError`` carrying the
+library's own message is raised.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+from .camera import RMCamera
+
+RM_OK = 0
+RM_EINVAL = 1
+RM_ECAPACITY = 2
+RM_ECUDA = 3
+RM_ETIMEOUT = 4
+
+RM_STATUS_SCAN_TIMEOUT = 0x1
+RM_STATUS_SORT_TIMEOUT = 0x2
+RM_STATUS_CAPACITY = 0x4
+RM_STATUS_QUEUE_TIMEOUT = 0x8
+
+RM_BLEND_REUSE_RECORDS = 0x1
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "librm_b200.so")
+
+_lock = threading.Lock()
+_lib = None
+
+vp = ctypes.c_void_p
+i64 = ctypes.c_int64
+i32 = ctypes.c_int32
+sz = ctypes.c_size_t
+camp = ctypes.POINTER(RMCamera)
+
+# name -> (restype, argtypes); mirrors include/rm_capi.h
+SIGNATURES = {
+    "rm_last_error": (ctypes.c_char_p, []),
+    "rm_abi_version": (ctypes.c_int, []),
+    "rm_launch_count": (ctypes.c_uint64, []),
+    "rm_read_status": (ctypes.c_int, [vp, vp, vp]),
+    "rm_project_fwd": (ctypes.c_int, [vp, vp, i64, i64, camp, vp, vp, vp, vp, vp]),
+    "rm_project_bwd": (ctypes.c_int, [vp, vp, i64, i64, camp, vp, vp, vp, vp, vp]),
+    "rm_scan_workspace_size": (sz, [i64]),
+    "rm_scan_tiles": (ctypes.c_int, [vp, i64, vp, vp, vp, sz, vp]),
+    "rm_emit_pairs": (ctypes.c_int, [vp, vp, vp, i64, i32, i64, vp, vp, vp, vp, vp]),
+    "rm_sort_workspace_size": (sz, [i64]),
+    "rm_sort_pairs": (ctypes.c_int, [vp, vp, i64, vp, ctypes.c_int, vp, vp, vp, sz, vp]),
+    "rm_tile_ranges": (ctypes.c_int, [vp, i64, vp, vp, i64, vp]),
+    "rm_blend_workspace_size": (sz, [i64]),
+    "rm_blend_fwd": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, vp, vp, vp, vp, sz,
+                                    ctypes.c_int, vp]),
+    "rm_blend_bwd": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, vp, vp, vp, vp, vp,
+                                    vp, vp, vp, sz, ctypes.c_int, vp]),
+}
+
+
+def lib():
+    """Load the library (once) and bind its signatures."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not os.path.exists(LIB_PATH):
+                    raise RuntimeError(
+                        f"{LIB_PATH} is missing: build it with `python -m radiance_meshes_b200.build` "
+                        "(there is no CPU fallback)")
+                L = ctypes.CDLL(LIB_PATH)
+                for name, (res, args) in SIGNATURES.items():
+                    fn = getattr(L, name)
+                    fn.restype = res
+                    fn.argtypes = args
+                _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().rm_last_error().decode(errors="replace")
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != RM_OK:
+        raise RuntimeError(f"{what or 'radiance_meshes_b200'} failed (status {rc}): {last_error()}")
+
+
+def ptr(t) -> int | None:
+    """Raw device pointer of a tensor (None for None)."""
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def stream_handle(stream=None) -> int:
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def launch_count() -> int:
+    """Kernels launched by librm_b200.so in this process so far."""
+    return int(lib().rm_launch_count())

@@ -1,0 +1,148 @@
+"""Camera records for the rasterizer.
+
+The reference passes cameras to its kernels as a ``tcam`` dict
+(``utils/train_util.py:31-38`` plus ``data/camera.py:72-91``) which the Slang
+side loads into ``TensorCamera``/``Camera`` (``camera.slang:13-76``).  Here the
+same dict is converted into the POD ``rm_camera`` struct of ``include/rm_capi.h``.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+__all__ = [
+    "RMCamera",
+    "tcam_to_struct",
+    "make_tcam",
+    "look_at_world_view",
+    "intrinsics",
+    "pinhole_tcam",
+]
+
+
+class RMCamera(ctypes.Structure):
+    """ctypes mirror of ``rm_camera`` (include/rm_capi.h)."""
+
+    _fields_ = [
+        ("world_view", ctypes.c_float * 16),
+        ("K", ctypes.c_float * 9),
+        ("cam_pos", ctypes.c_float * 3),
+        ("min_t", ctypes.c_float),
+        ("distortion", ctypes.c_float * 4),
+        ("camera_type", ctypes.c_int32),
+        ("image_height", ctypes.c_int32),
+        ("image_width", ctypes.c_int32),
+        ("tile_height", ctypes.c_int32),
+        ("tile_width", ctypes.c_int32),
+        ("grid_height", ctypes.c_int32),
+        ("grid_width", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+def _as_np(x, n):
+    if hasattr(x, "detach"):
+        x = x.detach().to("cpu").numpy()
+    a = np.asarray(x, dtype=np.float32).reshape(-1)
+    if a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+def tcam_to_struct(tcam: dict) -> RMCamera:
+    """Convert a reference ``tcam`` dict into an ``rm_camera``.
+
+    Only perspective cameras without lens distortion are supported (the
+    reference's ``camera_type == 0`` with zero ``distortion_params``);
+    anything else raises ``ValueError``.
+    """
+    cam = RMCamera()
+    cam.world_view[:] = _as_np(tcam["world_view_transform"], 16).tolist()
+    cam.K[:] = _as_np(tcam["K"], 9).tolist()
+    cam.cam_pos[:] = _as_np(tcam["cam_pos"], 3).tolist()
+    cam.min_t = float(tcam.get("min_t", 0.1))
+    dist = tcam.get("distortion_params")
+    dist = np.zeros(4, np.float32) if dist is None else _as_np(dist, 4)
+    cam.distortion[:] = dist.tolist()
+    ctype = int(tcam.get("camera_type", 0))
+    if ctype != 0:
+        raise ValueError(f"camera_type {ctype} is not supported (perspective only)")
+    if float(np.dot(dist, dist)) >= 1e-9:
+        raise ValueError("lens distortion is not supported")
+    cam.camera_type = ctype
+    cam.image_height = int(tcam["image_height"])
+    cam.image_width = int(tcam["image_width"])
+    cam.tile_height = int(tcam["tile_height"])
+    cam.tile_width = int(tcam["tile_width"])
+    cam.grid_height = int(tcam["grid_height"])
+    cam.grid_width = int(tcam["grid_width"])
+    if cam.tile_height <= 0 or cam.tile_width <= 0:
+        raise ValueError("tile size must be positive")
+    if cam.grid_height * cam.tile_height < cam.image_height or cam.grid_width * cam.tile_width < cam.image_width:
+        raise ValueError("tile grid does not cover the image")
+    return cam
+
+
+def look_at_world_view(pos, target, up=(0.0, 1.0, 0.0)) -> np.ndarray:
+    """Row-major world->camera matrix (OpenCV axes: x right, y down, z forward)."""
+    pos = np.asarray(pos, np.float64)
+    target = np.asarray(target, np.float64)
+    up = np.asarray(up, np.float64)
+    z = target - pos
+    z /= np.linalg.norm(z)
+    x = np.cross(z, up)
+    if np.linalg.norm(x) < 1e-9:
+        x = np.cross(z, np.array([1.0, 0.0, 0.0]))
+    x /= np.linalg.norm(x)
+    y = np.cross(z, x)
+    R = np.stack([x, y, z], 0)
+    M = np.eye(4)
+    M[:3, :3] = R
+    M[:3, 3] = -R @ pos
+    return M.astype(np.float32)
+
+
+def intrinsics(height: int, width: int, fovy_deg: float):
+    """Square-pixel K with cx = W/2, cy = H/2 (data/camera.py:73-84)."""
+    fovy = math.radians(fovy_deg)
+    fy = height / (2.0 * math.tan(fovy / 2.0))
+    fx = fy
+    fovx = 2.0 * math.atan(width / (2.0 * fx))
+    K = np.array([[fx, 0.0, width / 2.0], [0.0, fy, height / 2.0], [0.0, 0.0, 1.0]], np.float32)
+    return K, fovx, fovy
+
+
+def make_tcam(world_view, K, cam_pos, height, width, tile_size=16, min_t=0.1, fovx=None, fovy=None,
+              device=None):
+    """Build a ``tcam`` dict with the reference's keys (utils/train_util.py:31-38)."""
+    import torch
+
+    grid_h = (height + tile_size - 1) // tile_size
+    grid_w = (width + tile_size - 1) // tile_size
+    dev = device if device is not None else "cpu"
+    return dict(
+        tile_height=tile_size,
+        tile_width=tile_size,
+        grid_height=grid_h,
+        grid_width=grid_w,
+        min_t=min_t,
+        world_view_transform=torch.as_tensor(np.asarray(world_view, np.float32)).to(dev),
+        cam_pos=torch.as_tensor(np.asarray(cam_pos, np.float32)).to(dev),
+        K=torch.as_tensor(np.asarray(K, np.float32)).to(dev),
+        image_height=height,
+        image_width=width,
+        fovy=fovy if fovy is not None else 0.0,
+        fovx=fovx if fovx is not None else 0.0,
+        distortion_params=torch.zeros(4).to(dev),
+        camera_type=0,
+    )
+
+
+def pinhole_tcam(pos, target, height, width, fovy_deg=60.0, tile_size=16, min_t=0.1, up=(0.0, 1.0, 0.0),
+                 device=None):
+    """Look-at pinhole camera as a reference ``tcam`` dict."""
+    M = look_at_world_view(pos, target, up)
+    K, fovx, fovy = intrinsics(height, width, fovy_deg)
+    return make_tcam(M, K, np.asarray(pos, np.float32), height, width, tile_size, min_t, fovx, fovy, device)

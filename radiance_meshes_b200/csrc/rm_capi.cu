@@ -1,0 +1,66 @@
+// rm_capi.cu - error reporting and shared host-side checks of the C ABI.
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "rm_internal.cuh"
+
+namespace {
+thread_local char g_last_error[512] = {0};
+std::atomic<uint64_t> g_launches{0};
+}
+
+namespace rm_host {
+
+int fail(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int check_launch(const char* what, int kernels) {
+    g_launches.fetch_add((uint64_t)kernels, std::memory_order_relaxed);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(RM_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    return RM_OK;
+}
+
+int check_cam(const rm_camera* cam) {
+    if (!cam) return fail(RM_EINVAL, "camera is NULL");
+    if (cam->camera_type != 0) return fail(RM_EINVAL, "camera_type %d unsupported (perspective only)", cam->camera_type);
+    float dd = 0.f;
+    for (int i = 0; i < 4; ++i) dd += cam->distortion[i] * cam->distortion[i];
+    if (dd >= 1e-9f) return fail(RM_EINVAL, "lens distortion is not supported");
+    if (cam->tile_width <= 0 || cam->tile_height <= 0) return fail(RM_EINVAL, "bad tile size");
+    if (cam->image_width <= 0 || cam->image_height <= 0) return fail(RM_EINVAL, "bad image size");
+    if ((int64_t)cam->grid_width * cam->tile_width < cam->image_width ||
+        (int64_t)cam->grid_height * cam->tile_height < cam->image_height)
+        return fail(RM_EINVAL, "tile grid does not cover the image");
+    if (cam->K[0] == 0.f || cam->K[4] == 0.f) return fail(RM_EINVAL, "zero focal length");
+    return RM_OK;
+}
+
+}  // namespace rm_host
+
+extern "C" {
+
+const char* rm_last_error(void) { return g_last_error; }
+
+int rm_abi_version(void) { return RM_ABI_VERSION; }
+
+uint64_t rm_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int rm_read_status(const uint32_t* status_dev, uint32_t* status_host, void* stream) {
+    if (!status_dev || !status_host) return rm_host::fail(RM_EINVAL, "rm_read_status: NULL pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpyAsync(status_host, status_dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync((void*)status_dev, 0, sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_read_status: %s", cudaGetErrorString(e));
+    return RM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,100 @@
+// rm_internal.cuh - device helpers shared by the rasterizer kernels (sm_100a).
+//
+// Rounding rules.  This translation unit family is compiled with --fmad=false,
+// so the compiler never contracts a*b+c on its own; every fused multiply-add
+// below is an explicit fmaf/fma.  Division and sqrt are IEEE correctly rounded
+// (-prec-div / -prec-sqrt default on; never -use_fast_math).  The rules are:
+//   dot(a,b)     = fma(a.z,b.z, fma(a.y,b.y, a.x*b.x))
+//   cross(a,b).x = fma(a.y,b.z, -(a.z*b.y))            (and cyclic)
+//   a*b + c      = fma(a,b,c)  where the reference source writes a*b + c
+//   lerp(x,y,s)  = fma(y,s, x*(1-s))
+//   normalize(v) = v / sqrt(dot(v,v))
+// With them the integer outputs of projection and blending (tile counts,
+// rectangles, depth keys, n_contributors) and the log-transmittance channel
+// are a pure function of the inputs, identical on every run and reproducible
+// on the CPU.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/rm_capi.h"
+
+namespace rm {
+
+struct f3 {
+    float x, y, z;
+};
+
+__device__ __forceinline__ f3 mk3(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ f3 operator-(f3 a, f3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ f3 operator+(f3 a, f3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ f3 neg3(f3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ f3 scale3(f3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ float dot3(f3 a, f3 b) { return fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x)); }
+__device__ __forceinline__ f3 cross3(f3 a, f3 b) {
+    return {fmaf(a.y, b.z, -(a.z * b.y)), fmaf(a.z, b.x, -(a.x * b.z)), fmaf(a.x, b.y, -(a.y * b.x))};
+}
+
+struct d3 {
+    double x, y, z;
+};
+__device__ __forceinline__ d3 operator-(d3 a, d3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ d3 operator+(d3 a, d3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ d3 scale3(d3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ double dot3(d3 a, d3 b) { return fma(a.z, b.z, fma(a.y, b.y, a.x * b.x)); }
+__device__ __forceinline__ d3 cross3(d3 a, d3 b) {
+    return {fma(a.y, b.z, -(a.z * b.y)), fma(a.z, b.x, -(a.x * b.z)), fma(a.x, b.y, -(a.y * b.x))};
+}
+__device__ __forceinline__ double len3(d3 a) { return sqrt(dot3(a, a)); }
+
+// log(1e20) rounded to float: the upper clip of safe_exp (safe-math.slang:137-140).
+constexpr float kLogMax = (float)46.051701859880914;
+
+__device__ __forceinline__ float safe_expf(float v) { return expf(fmaxf(fminf(v, kLogMax), -1e20f)); }
+
+// get_ray (camera.slang:298-346) for a perspective camera without distortion.
+__device__ __forceinline__ void make_ray(const rm_camera& c, int px, int py, float jx, float jy, f3& o,
+                                         f3& d) {
+    const float ux = ((float)px + jx - c.K[2]) / c.K[0];
+    const float uy = ((float)py + jy - c.K[5]) / c.K[4];
+    f3 dc = {ux, uy, 1.0f};
+    float l = sqrtf(dot3(dc, dc));
+    dc = {dc.x / l, dc.y / l, dc.z / l};
+    const float* M = c.world_view;
+    f3 dw = {dot3(mk3(M[0], M[4], M[8]), dc), dot3(mk3(M[1], M[5], M[9]), dc),
+             dot3(mk3(M[2], M[6], M[10]), dc)};
+    l = sqrtf(dot3(dw, dw));
+    d = {dw.x / l, dw.y / l, dw.z / l};
+    o = {fmaf(d.x, c.min_t, c.cam_pos[0]), fmaf(d.y, c.min_t, c.cam_pos[1]),
+         fmaf(d.z, c.min_t, c.cam_pos[2])};
+}
+
+// Packed per-tet record (128 B = 8 x float4) staged by the blend kernels.
+//   q0 = (n0, density)   q1 = (n1, r)   q2 = (n2, g)   q3 = (n3, b)
+//   q4 = (v0, gx)        q5 = (v1, gy)  q6 = (v2, gz)  q7 = (v3, flip bits)
+// n_i are the outward face normals of ray_tetrahedron_intersect_fused
+// (intersect.slang:449-475) after the orientation flip; bit i of the flip word
+// records whether n_i was negated.
+constexpr int kRecFloat4 = 8;
+
+__device__ __forceinline__ int tile_w_of(const rm_camera& c) { return c.tile_width; }
+
+// Bounded spin helper: returns false once the budget is exhausted.
+__device__ __forceinline__ bool spin_budget(uint32_t& left) {
+    if (left == 0) return false;
+    --left;
+    if ((left & 63u) == 0) __nanosleep(64);
+    return true;
+}
+
+}  // namespace rm
+
+// Host-side helpers (rm_capi.cu).
+namespace rm_host {
+int fail(int code, const char* fmt, ...);
+// Checks the launch status of the preceding kernel launches and adds
+// `kernels` to the process-wide launch counter.
+int check_launch(const char* what, int kernels = 1);
+int check_cam(const rm_camera* cam);
+}  // namespace rm_host

@@ -1,0 +1,317 @@
+// rm_project.cu - stage (a): per-tet projection, cull, tile rectangle and the
+// FP64 circumsphere-power depth key, plus its adjoint.
+//
+// Forward follows vertex_shader (vertex_shader.slang:23-89) with find_extent
+// (camera.slang:443-508), is_planar (intersect.slang:76-89) and
+// power_of_circumsphere (stable_power.slang:18-85).  One thread per tet; the
+// [T,4] index row is one 16-byte load and every output row is written once
+// (zeros for culled tets), so no separate zero-fill pass is needed.
+#include "rm_internal.cuh"
+
+namespace rm {
+namespace {
+
+__device__ __forceinline__ float safe_clipf(float v, float lo, float hi) { return fmaxf(fminf(v, hi), lo); }
+
+__device__ __forceinline__ float safe_divf(float a, float b) {  // safe-math.slang:72-79
+    const float tiny = 1.0754944e-20f;
+    if (fabsf(b) < tiny) return safe_clipf(a / tiny, -1e20f, 1e20f);
+    return safe_clipf(a / b, -1e20f, 1e20f);
+}
+
+__device__ __forceinline__ f3 point2cam(const rm_camera& c, f3 p) {  // camera.slang:103-108
+    const float* M = c.world_view;
+    float h0 = fmaf(M[3], 1.0f, fmaf(M[2], p.z, fmaf(M[1], p.y, M[0] * p.x)));
+    float h1 = fmaf(M[7], 1.0f, fmaf(M[6], p.z, fmaf(M[5], p.y, M[4] * p.x)));
+    float h2 = fmaf(M[11], 1.0f, fmaf(M[10], p.z, fmaf(M[9], p.y, M[8] * p.x)));
+    float h3 = fmaf(M[15], 1.0f, fmaf(M[14], p.z, fmaf(M[13], p.y, M[12] * p.x)));
+    return {safe_divf(h0, h3), safe_divf(h1, h3), safe_divf(h2, h3)};
+}
+
+__device__ __forceinline__ f3 lerp3(f3 a, f3 b, float s) {
+    const float w = 1.0f - s;
+    return {fmaf(b.x, s, a.x * w), fmaf(b.y, s, a.y * w), fmaf(b.z, s, a.z * w)};
+}
+
+struct BBox {
+    f3 mn, mx;
+};
+
+__device__ __forceinline__ void bbox_add(BBox& b, const rm_camera& c, f3 p) {
+    // camspace_to_image (camera.slang:382-412), perspective, no distortion
+    const float ux = p.x / p.z;
+    const float uy = p.y / p.z;
+    const float qx = fmaf(ux, c.K[0], c.K[2]);
+    const float qy = fmaf(uy, c.K[4], c.K[5]);
+    b.mn = {fminf(b.mn.x, qx), fminf(b.mn.y, qy), fminf(b.mn.z, p.z)};
+    b.mx = {fmaxf(b.mx.x, qx), fmaxf(b.mx.y, qy), fmaxf(b.mx.z, p.z)};
+}
+
+__device__ __forceinline__ bool eq3(f3 a, f3 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+
+// One face of find_extent: clip the triangle (a,b,c) against z = 1e-4 and add
+// the clipped polygon's vertices to the box when it has more than one vertex.
+// Sampling each edge at t = 0 and t = 1 (2 samples) yields exactly the polygon
+// vertices (lerp with s = 0 / 1 is exact), so the box is the box of the
+// polygon vertices; the de-duplication only matters for the vertex count.
+__device__ __forceinline__ void clip_face(const rm_camera& c, f3 a, f3 b, f3 cc, BBox& box) {
+    const float eps = 1e-4f;
+    f3 p[4];
+    int n = 0;
+    const f3 fv[3] = {a, b, cc};
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const f3 va = fv[j];
+        const f3 vb = fv[(j + 1) % 3];
+        const bool ain = va.z > eps;
+        const bool bin = vb.z > eps;
+        if (ain) {
+            bool found = false;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < n && eq3(p[k], va)) found = true;
+            if (!found) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (k == n) p[k] = va;
+                ++n;
+            }
+        }
+        if (ain != bin) {
+            const float t = (eps - va.z) / (vb.z - va.z);
+            const f3 q = lerp3(va, vb, t);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k == n) p[k] = q;
+            ++n;
+        }
+    }
+    if (n > 1) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < n) bbox_add(box, c, p[k]);
+    }
+}
+
+__device__ double power_of_circumsphere(d3 A, d3 B, d3 C, d3 D, d3 P, d3& center) {
+    const d3 a = B - A, b = C - A, c = D - A;
+    const double aa = dot3(a, a), bb = dot3(b, b), cc = dot3(c, c);
+    const d3 cbc = cross3(b, c), cca = cross3(c, a), cab = cross3(a, b);
+    const double den = 2.0 * dot3(a, cbc);
+    double radius;
+    if (fabs(den) < 1e-10) {
+        const double m = fmax(len3(B - A), fmax(len3(C - A), fmax(len3(D - A),
+                         fmax(len3(C - B), fmax(len3(D - B), len3(D - C))))));
+        if (m < 1e-7) {
+            center = scale3(((A + B) + C) + D, 0.25);
+            radius = fmin(len3(A - center), fmin(len3(B - center), fmin(len3(C - center), len3(D - center))));
+            const d3 df = center - P;
+            return dot3(df, df) - radius * radius;
+        }
+        center = {0.0, 0.0, 0.0};
+        return -1e20;
+    }
+    const d3 rel = {fma(cc, cab.x, fma(bb, cca.x, aa * cbc.x)) / den,
+                    fma(cc, cab.y, fma(bb, cca.y, aa * cbc.y)) / den,
+                    fma(cc, cab.z, fma(bb, cca.z, aa * cbc.z)) / den};
+    center = A + rel;
+    radius = len3(rel);
+    const d3 df = center - P;
+    return dot3(df, df) - radius * radius;
+}
+
+__device__ __forceinline__ f3 load_vertex(const float* __restrict__ v, int i) {
+    const float* p = v + 3 * (int64_t)i;
+    return {__ldg(p), __ldg(p + 1), __ldg(p + 2)};
+}
+
+__global__ void __launch_bounds__(256) project_fwd_kernel(const int4* __restrict__ indices,
+                                                          const float* __restrict__ verts, int64_t n_tets,
+                                                          const rm_camera cam, int32_t* __restrict__ tiles,
+                                                          int4* __restrict__ rect, float* __restrict__ vs,
+                                                          float* __restrict__ cc) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_tets) return;
+    const int4 id = __ldg(indices + g);
+    f3 v[4] = {load_vertex(verts, id.x), load_vertex(verts, id.y), load_vertex(verts, id.z),
+               load_vertex(verts, id.w)};
+    int n_tiles = 0;
+    int4 r = {0, 0, 0, 0};
+    float depth_out = 0.f;
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+    do {
+        // is_planar
+        f3 nrm = cross3(v[1] - v[0], v[2] - v[0]);
+        const float l = sqrtf(dot3(nrm, nrm));
+        nrm = {nrm.x / l, nrm.y / l, nrm.z / l};
+        if (fabsf(dot3(nrm, v[3] - v[0])) < 1e-3f) break;
+        // camera space + find_extent
+        const f3 cs0 = point2cam(cam, v[0]), cs1 = point2cam(cam, v[1]);
+        const f3 cs2 = point2cam(cam, v[2]), cs3 = point2cam(cam, v[3]);
+        BBox box = {{1e20f, 1e20f, 1e20f}, {-1e20f, -1e20f, -1e20f}};
+        clip_face(cam, cs0, cs1, cs2, box);
+        clip_face(cam, cs0, cs2, cs3, box);
+        clip_face(cam, cs0, cs3, cs1, box);
+        clip_face(cam, cs1, cs3, cs2, box);
+        if (box.mx.z <= 0.0f) break;
+        // depth key: FP64 power of the circumsphere w.r.t. the camera position
+        d3 center = {0.0, 0.0, 0.0};
+        const d3 P = {(double)cam.cam_pos[0], (double)cam.cam_pos[1], (double)cam.cam_pos[2]};
+        const double pw = power_of_circumsphere({(double)v[0].x, (double)v[0].y, (double)v[0].z},
+                                                {(double)v[1].x, (double)v[1].y, (double)v[1].z},
+                                                {(double)v[2].x, (double)v[2].y, (double)v[2].z},
+                                                {(double)v[3].x, (double)v[3].y, (double)v[3].z}, P, center);
+        const float depth = (float)pw;
+        if (depth < -1e19f) break;
+        const float gw = (float)cam.grid_width, gh = (float)cam.grid_height;
+        const float tw = (float)cam.tile_width, th = (float)cam.tile_height;
+        r.x = (int)floorf(fmaxf(0.f, fminf(gw, box.mn.x / tw)));
+        r.y = (int)floorf(fmaxf(0.f, fminf(gh, box.mn.y / th)));
+        r.z = (int)ceilf(fmaxf(0.f, fminf(gw, box.mx.x / tw)));
+        r.w = (int)ceilf(fmaxf(0.f, fminf(gh, box.mx.y / th)));
+        n_tiles = (r.z - r.x) * (r.w - r.y);
+        if (n_tiles == 0) {
+            r = {0, 0, 0, 0};
+            break;
+        }
+        depth_out = fminf(fmaxf(depth, -1e20f), 1e20f);
+        c0 = (float)center.x;
+        c1 = (float)center.y;
+        c2 = (float)center.z;
+    } while (0);
+    tiles[g] = n_tiles;
+    rect[g] = r;
+    vs[3 * g + 0] = 0.f;
+    vs[3 * g + 1] = 0.f;
+    vs[3 * g + 2] = depth_out;
+    cc[3 * g + 0] = c0;
+    cc[3 * g + 1] = c1;
+    cc[3 * g + 2] = c2;
+}
+
+__device__ __forceinline__ void atomic_add3(float* p, d3 g) {
+    atomicAdd(p, (float)g.x);
+    atomicAdd(p + 1, (float)g.y);
+    atomicAdd(p + 2, (float)g.z);
+}
+
+// Adjoint of vs[:,2] = clamp(float(power)) and circumcenter = float(center)
+// (vertex_shader.bwd, tile_shader_slang.py:128-150), evaluated in FP64.
+__global__ void __launch_bounds__(256) project_bwd_kernel(const int4* __restrict__ indices,
+                                                          const float* __restrict__ verts, int64_t n_tets,
+                                                          const rm_camera cam,
+                                                          const int32_t* __restrict__ tiles,
+                                                          const float* __restrict__ gvs,
+                                                          const float* __restrict__ gcc,
+                                                          float* __restrict__ gverts) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_tets) return;
+    if (tiles[g] <= 0) return;
+    const int4 id = __ldg(indices + g);
+    const int ids[4] = {id.x, id.y, id.z, id.w};
+    d3 X[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const f3 v = load_vertex(verts, ids[i]);
+        X[i] = {(double)v.x, (double)v.y, (double)v.z};
+    }
+    const d3 P = {(double)cam.cam_pos[0], (double)cam.cam_pos[1], (double)cam.cam_pos[2]};
+    d3 center;
+    const double pw = power_of_circumsphere(X[0], X[1], X[2], X[3], P, center);
+    const float pf = (float)pw;
+    double gp = gvs ? (double)gvs[3 * g + 2] : 0.0;
+    if (!(pf > -1e20f && pf < 1e20f)) gp = 0.0;
+    const d3 gC = {gcc ? (double)gcc[3 * g] : 0.0, gcc ? (double)gcc[3 * g + 1] : 0.0,
+                   gcc ? (double)gcc[3 * g + 2] : 0.0};
+    if (gp == 0.0 && gC.x == 0.0 && gC.y == 0.0 && gC.z == 0.0) return;
+    d3 G[4];
+    const d3 a = X[1] - X[0], b = X[2] - X[0], c = X[3] - X[0];
+    const d3 df = center - P;
+    const d3 gcen = {gC.x + 2.0 * gp * df.x, gC.y + 2.0 * gp * df.y, gC.z + 2.0 * gp * df.z};
+    const double den = 2.0 * dot3(a, cross3(b, c));
+    if (fabs(den) < 1e-10) {
+        int im = 0;
+        double best = 1e300;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const double l = len3(X[i] - center);
+            if (l < best) best = l, im = i;
+        }
+        const d3 ge = scale3(X[im] - center, -2.0 * gp);
+        const d3 share = scale3(gcen - ge, 0.25);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) G[i] = share;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (i == im) G[i] = G[i] + ge;
+    } else {
+        const d3 cbc = cross3(b, c), cca = cross3(c, a), cab = cross3(a, b);
+        const double aa = dot3(a, a), bb = dot3(b, b), cc2 = dot3(c, c);
+        const d3 N = {aa * cbc.x + bb * cca.x + cc2 * cab.x, aa * cbc.y + bb * cca.y + cc2 * cab.y,
+                      aa * cbc.z + bb * cca.z + cc2 * cab.z};
+        const d3 rel = center - X[0];
+        const d3 grel = {gcen.x - 2.0 * gp * rel.x, gcen.y - 2.0 * gp * rel.y, gcen.z - 2.0 * gp * rel.z};
+        const d3 gN = scale3(grel, 1.0 / den);
+        const double gden = -dot3(grel, N) / (den * den);
+        const double gaa = dot3(gN, cbc), gbb = dot3(gN, cca), gcc = dot3(gN, cab);
+        const d3 gcbc = scale3(gN, aa) + scale3(a, 2.0 * gden);
+        const d3 gcca = scale3(gN, bb), gcab = scale3(gN, cc2);
+        d3 ga = scale3(cbc, 2.0 * gden) + scale3(a, 2.0 * gaa);
+        d3 gb = scale3(b, 2.0 * gbb);
+        d3 gc = scale3(c, 2.0 * gcc);
+        gb = gb + cross3(c, gcbc);
+        gc = gc + cross3(gcbc, b);
+        gc = gc + cross3(a, gcca);
+        ga = ga + cross3(gcca, c);
+        ga = ga + cross3(b, gcab);
+        gb = gb + cross3(gcab, a);
+        G[0] = gcen - ((ga + gb) + gc);
+        G[1] = ga;
+        G[2] = gb;
+        G[3] = gc;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) atomic_add3(gverts + 3 * (int64_t)ids[i], G[i]);
+}
+
+}  // namespace
+}  // namespace rm
+
+extern "C" {
+
+int rm_project_fwd(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,
+                   const rm_camera* cam, int32_t* tiles_touched, int32_t* rect, float* vs,
+                   float* circumcenter, void* stream) {
+    int rc = rm_host::check_cam(cam);
+    if (rc) return rc;
+    if (n_tets < 0 || n_verts < 0) return rm_host::fail(RM_EINVAL, "rm_project_fwd: negative size");
+    if (n_tets == 0) return RM_OK;
+    if (!indices || !vertices || !tiles_touched || !rect || !vs || !circumcenter)
+        return rm_host::fail(RM_EINVAL, "rm_project_fwd: NULL pointer");
+    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15))
+        return rm_host::fail(RM_EINVAL, "rm_project_fwd: indices and rect must be 16-byte aligned");
+    const int threads = 256;
+    const int64_t blocks = (n_tets + threads - 1) / threads;
+    rm::project_fwd_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+        (const int4*)indices, vertices, n_tets, *cam, tiles_touched, (int4*)rect, vs, circumcenter);
+    return rm_host::check_launch("rm_project_fwd");
+}
+
+int rm_project_bwd(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,
+                   const rm_camera* cam, const int32_t* tiles_touched, const float* grad_vs,
+                   const float* grad_circumcenter, float* grad_vertices, void* stream) {
+    int rc = rm_host::check_cam(cam);
+    if (rc) return rc;
+    if (n_tets < 0 || n_verts < 0) return rm_host::fail(RM_EINVAL, "rm_project_bwd: negative size");
+    if (n_tets == 0 || (!grad_vs && !grad_circumcenter)) return RM_OK;
+    if (!indices || !vertices || !tiles_touched || !grad_vertices)
+        return rm_host::fail(RM_EINVAL, "rm_project_bwd: NULL pointer");
+    if ((uintptr_t)indices & 15) return rm_host::fail(RM_EINVAL, "rm_project_bwd: indices must be 16-byte aligned");
+    const int threads = 256;
+    const int64_t blocks = (n_tets + threads - 1) / threads;
+    rm::project_bwd_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+        (const int4*)indices, vertices, n_tets, *cam, tiles_touched, grad_vs, grad_circumcenter, grad_vertices);
+    return rm_host::check_launch("rm_project_bwd");
+}
+
+}  // extern "C"

@@ -1,0 +1,247 @@
+// rm_scan.cu - stage (b): prefix sum of per-tet tile counts, tile/tet pair
+// emission, and per-tile ranges of the sorted pair list.
+//
+//   rm_scan_tiles   torch.cumsum(tiles_touched) (tile_shader_slang.py:36), done
+//                   as a single-pass block scan with decoupled look-back
+//   rm_emit_pairs   generate_keys (tile_shader.slang:138-186)
+//   rm_tile_ranges  compute_tile_ranges (tile_shader.slang:188-214)
+#include "rm_internal.cuh"
+
+namespace rm {
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;  // 4096 tets per CTA
+constexpr uint64_t kFlagAgg = 1ull << 32;
+constexpr uint64_t kFlagInc = 2ull << 32;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+struct ScanWs {
+    uint32_t status;
+    uint32_t counter;
+    uint32_t pad[2];
+    // followed by uint64_t state[n_tiles]
+};
+
+__device__ __forceinline__ void st_release(uint64_t* p, uint64_t v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t ld_acquire(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_kernel(const int32_t* __restrict__ in, int64_t n,
+                                                            int32_t* __restrict__ out, int64_t* total_dev,
+                                                            ScanWs* ws) {
+    __shared__ uint32_t s_tile;
+    __shared__ int32_t s_warp[kScanThreads / 32];
+    __shared__ int32_t s_prefix;
+    uint64_t* state = reinterpret_cast<uint64_t*>(ws + 1);
+    if (threadIdx.x == 0) s_tile = atomicAdd(&ws->counter, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const int64_t base = (int64_t)tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int32_t v[kScanItems];
+    if (base + kScanItems <= n && ((((uintptr_t)(in + base)) & 15) == 0)) {
+        const int4* p = reinterpret_cast<const int4*>(in + base);
+#pragma unroll
+        for (int k = 0; k < kScanItems / 4; ++k) {
+            const int4 q = __ldg(p + k);
+            v[4 * k] = q.x;
+            v[4 * k + 1] = q.y;
+            v[4 * k + 2] = q.z;
+            v[4 * k + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) v[k] = (base + k < n) ? __ldg(in + base + k) : 0;
+    }
+    int32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) sum += v[k];
+    // block-wide exclusive scan of the per-thread sums
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int32_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0;
+        int32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        if (lane < kScanThreads / 32) s_warp[lane] = wi - w;  // exclusive warp offsets
+        const int32_t block_total = __shfl_sync(0xffffffffu, wi, kScanThreads / 32 - 1);
+        if (lane == 0) {
+            int32_t prefix = 0;
+            if (tile == 0) {
+                st_release(&state[0], kFlagInc | (uint32_t)block_total);
+            } else {
+                st_release(&state[tile], kFlagAgg | (uint32_t)block_total);
+                int64_t t = (int64_t)tile - 1;
+                uint32_t budget = kSpinLimit;
+                while (t >= 0) {
+                    const uint64_t s = ld_acquire(&state[t]);
+                    const uint64_t flag = s & (3ull << 32);
+                    if (flag == 0) {
+                        if (!spin_budget(budget)) {
+                            atomicOr(&ws->status, RM_STATUS_SCAN_TIMEOUT);
+                            break;
+                        }
+                        continue;
+                    }
+                    prefix += (int32_t)(uint32_t)s;
+                    if (flag == kFlagInc) break;
+                    --t;
+                }
+                st_release(&state[tile], kFlagInc | (uint32_t)(prefix + block_total));
+            }
+            s_prefix = prefix;
+            const int64_t last = (int64_t)tile * kScanTile + kScanTile;
+            if (last >= n) *total_dev = (int64_t)(prefix + block_total);
+        }
+    }
+    __syncthreads();
+    int32_t run = s_prefix + s_warp[warp] + incl - sum;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        run += v[k];
+        v[k] = run;
+    }
+    if (base + kScanItems <= n && ((((uintptr_t)(out + base)) & 15) == 0)) {
+        int4* p = reinterpret_cast<int4*>(out + base);
+#pragma unroll
+        for (int k = 0; k < kScanItems / 4; ++k) p[k] = make_int4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k)
+            if (base + k < n) out[base + k] = v[k];
+    }
+}
+
+__device__ __forceinline__ uint32_t sortable_key(float f) {  // tile_shader.slang:107-136
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b ^ 0x80000000u);
+}
+
+__global__ void __launch_bounds__(256) emit_kernel(const float* __restrict__ vs, const int4* __restrict__ rect,
+                                                   const int32_t* __restrict__ offsets, int64_t n_tets,
+                                                   int32_t grid_w, int64_t capacity,
+                                                   const int64_t* __restrict__ total_dev,
+                                                   int64_t* __restrict__ keys, int32_t* __restrict__ vals,
+                                                   uint32_t* status) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g == 0 && total_dev && status && *total_dev > capacity) atomicOr(status, RM_STATUS_CAPACITY);
+    if (g >= n_tets) return;
+    const int4 r = __ldg(rect + g);
+    const int32_t cnt = (r.z - r.x) * (r.w - r.y);
+    if (cnt <= 0) return;
+    int64_t off = g == 0 ? 0 : (int64_t)__ldg(offsets + g - 1);
+    const uint64_t fk = sortable_key(__ldg(vs + 3 * g + 2));
+    for (int32_t y = r.y; y < r.w; ++y) {
+        for (int32_t x = r.x; x < r.z; ++x) {
+            if (off < capacity) {
+                keys[off] = (int64_t)(((uint64_t)(uint32_t)(y * grid_w + x) << 32) | fk);
+                vals[off] = (int32_t)g;
+            }
+            ++off;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) ranges_kernel(const int64_t* __restrict__ keys, int64_t cap,
+                                                     const int64_t* __restrict__ n_dev,
+                                                     int32_t* __restrict__ ranges, int64_t n_tiles) {
+    const int64_t n = n_dev ? min(*n_dev, cap) : cap;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t cur = (uint32_t)((uint64_t)keys[i] >> 32);
+    if (cur >= n_tiles) return;
+    if (i == 0) {
+        ranges[2 * (int64_t)cur] = 0;
+    } else {
+        const uint32_t prev = (uint32_t)((uint64_t)keys[i - 1] >> 32);
+        if (cur != prev) {
+            if (prev < n_tiles) ranges[2 * (int64_t)prev + 1] = (int32_t)i;
+            ranges[2 * (int64_t)cur] = (int32_t)i;
+        }
+    }
+    if (i == n - 1) ranges[2 * (int64_t)cur + 1] = (int32_t)n;
+}
+
+}  // namespace
+}  // namespace rm
+
+extern "C" {
+
+size_t rm_scan_workspace_size(int64_t n_tets) {
+    const int64_t tiles = (n_tets + rm::kScanTile - 1) / rm::kScanTile;
+    return sizeof(rm::ScanWs) + sizeof(uint64_t) * (size_t)(tiles > 0 ? tiles : 1);
+}
+
+int rm_scan_tiles(const int32_t* tiles_touched, int64_t n_tets, int32_t* offsets, int64_t* total_dev,
+                  void* workspace, size_t workspace_bytes, void* stream) {
+    if (n_tets < 0) return rm_host::fail(RM_EINVAL, "rm_scan_tiles: negative size");
+    if (!total_dev) return rm_host::fail(RM_EINVAL, "rm_scan_tiles: total_dev is NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n_tets == 0) {
+        cudaError_t e = cudaMemsetAsync(total_dev, 0, sizeof(int64_t), s);
+        return e == cudaSuccess ? RM_OK : rm_host::fail(RM_ECUDA, "rm_scan_tiles: %s", cudaGetErrorString(e));
+    }
+    if (!tiles_touched || !offsets || !workspace) return rm_host::fail(RM_EINVAL, "rm_scan_tiles: NULL pointer");
+    if (n_tets >= (int64_t)INT32_MAX) return rm_host::fail(RM_EINVAL, "rm_scan_tiles: too many tets");
+    const size_t need = rm_scan_workspace_size(n_tets);
+    if (workspace_bytes < need)
+        return rm_host::fail(RM_EINVAL, "rm_scan_tiles: workspace %zu < %zu bytes", workspace_bytes, need);
+    if ((uintptr_t)workspace & 15) return rm_host::fail(RM_EINVAL, "rm_scan_tiles: workspace must be 16-byte aligned");
+    // status is preserved (it accumulates until rm_read_status); counter and tile states are reset
+    cudaError_t e = cudaMemsetAsync((char*)workspace + 4, 0, need - 4, s);
+    if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_scan_tiles: %s", cudaGetErrorString(e));
+    const int64_t blocks = (n_tets + rm::kScanTile - 1) / rm::kScanTile;
+    rm::scan_kernel<<<(unsigned)blocks, rm::kScanThreads, 0, s>>>(tiles_touched, n_tets, offsets, total_dev,
+                                                                 (rm::ScanWs*)workspace);
+    return rm_host::check_launch("rm_scan_tiles");
+}
+
+int rm_emit_pairs(const float* vs, const int32_t* rect, const int32_t* offsets, int64_t n_tets, int32_t grid_width,
+                  int64_t capacity, const int64_t* total_dev, int64_t* keys, int32_t* values, uint32_t* status_dev,
+                  void* stream) {
+    if (n_tets < 0 || capacity < 0) return rm_host::fail(RM_EINVAL, "rm_emit_pairs: negative size");
+    if (n_tets == 0) return RM_OK;
+    if (!vs || !rect || !offsets || (capacity > 0 && (!keys || !values)))
+        return rm_host::fail(RM_EINVAL, "rm_emit_pairs: NULL pointer");
+    if ((uintptr_t)rect & 15) return rm_host::fail(RM_EINVAL, "rm_emit_pairs: rect must be 16-byte aligned");
+    const int threads = 256;
+    const int64_t blocks = (n_tets + threads - 1) / threads;
+    rm::emit_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+        vs, (const int4*)rect, offsets, n_tets, grid_width, capacity, total_dev, keys, values, status_dev);
+    return rm_host::check_launch("rm_emit_pairs");
+}
+
+int rm_tile_ranges(const int64_t* sorted_keys, int64_t n, const int64_t* n_dev, int32_t* ranges, int64_t n_tiles,
+                   void* stream) {
+    if (n < 0 || n_tiles < 0) return rm_host::fail(RM_EINVAL, "rm_tile_ranges: negative size");
+    if (n_tiles == 0) return RM_OK;
+    if (!ranges) return rm_host::fail(RM_EINVAL, "rm_tile_ranges: NULL ranges");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(ranges, 0, sizeof(int32_t) * 2 * (size_t)n_tiles, s);
+    if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_tile_ranges: %s", cudaGetErrorString(e));
+    if (n == 0) return RM_OK;
+    if (!sorted_keys) return rm_host::fail(RM_EINVAL, "rm_tile_ranges: NULL keys");
+    const int threads = 256;
+    const int64_t blocks = (n + threads - 1) / threads;
+    rm::ranges_kernel<<<(unsigned)blocks, threads, 0, s>>>(sorted_keys, n, n_dev, ranges, n_tiles);
+    return rm_host::check_launch("rm_tile_ranges");
+}
+
+}  // extern "C"

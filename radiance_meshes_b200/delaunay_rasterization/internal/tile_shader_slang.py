@@ -1,0 +1,53 @@
+"""Projection and tile binning: drop-in for
+delaunay_rasterization/internal/tile_shader_slang.py (``vertex_and_tile_shader``,
+``VertexShader``), running the sm_100a kernels of librm_b200.so.
+
+Differences from the reference, none of them visible in the results:
+  * the NaN check on vertices (reference line 78) is not a host-side assert,
+    because that would synchronise the stream; non-finite vertices simply
+    produce non-finite depth keys as they would in the reference kernel;
+  * the pair count is read back once instead of three times;
+  * no cudaMalloc/cudaFree per call: scratch comes from a reusable pool.
+"""
+import torch
+
+from ... import rasterizer as R
+from ...camera import tcam_to_struct
+
+
+def ceil_div(x, y):
+    return (x + y - 1) // y
+
+
+def vertex_and_tile_shader(indices, vertices, cam, render_grid):
+    """Returns (sorted_tetra_idx [P] i32, tile_ranges [G,2] i32, vs_tetra [T,3],
+    circumcenter [T,3], mask [T] bool, rect_tile_space [T,4] i32) exactly as
+    the reference (tile_shader_slang.py:24-72)."""
+    tiles_touched, rect_tile_space, vs_tetra, circumcenter = VertexShader.apply(
+        indices, vertices, cam, render_grid)
+    with torch.no_grad():
+        camst = tcam_to_struct(cam)
+        lists = R.build_tile_lists(tiles_touched, rect_tile_space, vs_tetra, camst)
+    mask = tiles_touched > 0
+    return lists.sorted_ids, lists.ranges, vs_tetra, circumcenter, mask, rect_tile_space
+
+
+class VertexShader(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, indices, vertices, tcam, render_grid, device="cuda"):
+        camst = tcam_to_struct(tcam)
+        indices = indices.contiguous()
+        vertices = vertices.contiguous()
+        tiles_touched, rect_tile_space, vs_tetra, circumcenter = R.project_fwd(indices, vertices, camst)
+        ctx.save_for_backward(indices, vertices, tiles_touched)
+        ctx.camst = camst
+        ctx.render_grid = render_grid
+        ctx.mark_non_differentiable(tiles_touched, rect_tile_space)
+        return tiles_touched, rect_tile_space, vs_tetra, circumcenter
+
+    @staticmethod
+    def backward(ctx, grad_tiles_touched, grad_rect_tile_space, grad_vs_tetra, grad_circumcenter):
+        indices, vertices, tiles_touched = ctx.saved_tensors
+        grad_vertices = R.project_bwd(indices, vertices, ctx.camst, tiles_touched, grad_vs_tetra,
+                                      grad_circumcenter)
+        return None, grad_vertices, None, None

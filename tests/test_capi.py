@@ -1,0 +1,100 @@
+"""The C-ABI library: loads without a GPU, exports every symbol declared in
+include/rm_capi.h, answers size queries and rejects bad arguments before any
+device work."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from radiance_meshes_b200 import _capi as C
+from radiance_meshes_b200.camera import RMCamera, tcam_to_struct
+from radiance_meshes_b200 import scenes
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "rm_capi.h")).read()
+    return sorted(set(re.findall(r"RM_API\s+[\w\s\*]+?\b(rm_\w+)\s*\(", src)))
+
+
+def test_all_declared_symbols_exported():
+    names = declared_symbols()
+    assert len(names) >= 14
+    L = C.lib()
+    for n in names:
+        assert hasattr(L, n), n
+        assert n in C.SIGNATURES, f"{n} has no ctypes signature"
+
+
+def test_struct_layout():
+    # 33 floats then 8 int32 (include/rm_capi.h)
+    assert ctypes.sizeof(RMCamera) == 164
+    assert RMCamera.image_height.offset == 136
+
+
+def test_size_queries():
+    L = C.lib()
+    assert L.rm_abi_version() == 1
+    assert L.rm_blend_workspace_size(1000) == 1000 * 128
+    assert L.rm_scan_workspace_size(5000) >= 16 + 8 * 2
+    assert L.rm_sort_workspace_size(1_000_000) > 12 * 1_000_000
+
+
+def _cam():
+    mesh, view = scenes.workload_gradient_check()
+    return tcam_to_struct(view.tcam())
+
+
+def test_rejects_distortion_and_camera_type():
+    L = C.lib()
+    cam = _cam()
+    cam.distortion[0] = 0.1
+    rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None)
+    assert rc == C.RM_EINVAL and "distortion" in C.last_error()
+    cam = _cam()
+    cam.camera_type = 1
+    rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None)
+    assert rc == C.RM_EINVAL and "camera_type" in C.last_error()
+
+
+def test_rejects_null_and_misaligned():
+    L = C.lib()
+    cam = _cam()
+    assert L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None) == C.RM_EINVAL
+    assert "NULL" in C.last_error()
+    assert L.rm_sort_pairs(None, None, 10, None, 0, None, None, None, 0, None) == C.RM_EINVAL
+    assert L.rm_sort_pairs(None, None, 10, None, 65, None, None, None, 0, None) == C.RM_EINVAL
+    # unsupported tile size
+    cam.tile_width = 5
+    cam.tile_height = 5
+    cam.grid_width = 26
+    cam.grid_height = 26
+    rc = L.rm_blend_fwd(None, 16, 16, 16, 16, 10, 10, None, 16, ctypes.byref(cam), 16, 16, 16, 256, 10 * 128, 0,
+                        None)
+    assert rc == C.RM_EINVAL and "tile" in C.last_error()
+
+
+def test_zero_sizes_are_noops():
+    L = C.lib()
+    cam = _cam()
+    assert L.rm_project_fwd(None, None, 0, 0, ctypes.byref(cam), None, None, None, None, None) == C.RM_OK
+    assert L.rm_sort_pairs(None, None, 0, None, 40, None, None, None, 0, None) == C.RM_OK
+    assert L.rm_emit_pairs(None, None, None, 0, 1, 0, None, None, None, None, None) == C.RM_OK
+
+
+def test_python_camera_validation():
+    mesh, view = scenes.workload_gradient_check()
+    t = view.tcam()
+    t["distortion_params"] = [0.1, 0, 0, 0]
+    with pytest.raises(ValueError):
+        tcam_to_struct(t)
+    t = view.tcam()
+    t["grid_width"] = 1
+    with pytest.raises(ValueError):
+        tcam_to_struct(t)
+
+
+def test_launch_counter_starts_at_zero_without_gpu():
+    assert C.launch_count() >= 0

@@ -1,0 +1,106 @@
+"""Stage (d) backward and the projection adjoint on the GPU against the
+oracle's hand-derived adjoint evaluated in FP64 (which tests/test_oracle_grad.py
+checks against FP64 central differences).
+
+Metric: per parameter group (vertex positions, density, base RGB, colour
+gradient) the relative L2 error ||g_gpu - g_ref|| / ||g_ref||, which must be
+<= 1e-3 (the stated gradient tolerance); and per parameter
+|g_gpu - g_ref| <= 1e-3 |g_ref| + 1e-3 max|g_ref| for every entry.
+"""
+import numpy as np
+import pytest
+import torch
+
+import golden_util as G
+from gpu_util import run_gpu_forward, to_dev
+from oracle import oracle as O
+from radiance_meshes_b200 import rasterizer as R
+from radiance_meshes_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+GRAD_TOL = 1e-3
+
+
+def _groups(gv, gc):
+    return {"vertices": gv.ravel(), "density": gc[:, 0], "rgb": gc[:, 1:4].ravel(), "grd": gc[:, 4:7].ravel()}
+
+
+def _compare(gpu, ref):
+    out = {}
+    for k in ref:
+        a, b = gpu[k].astype(np.float64), ref[k]
+        nb = np.linalg.norm(b)
+        if nb == 0:
+            assert np.abs(a).max() == 0, k
+            continue
+        rel = np.linalg.norm(a - b) / nb
+        out[k] = rel
+        assert rel <= GRAD_TOL, f"{k}: relative L2 error {rel:.3e}"
+        bound = GRAD_TOL * np.abs(b) + GRAD_TOL * np.abs(b).max()
+        bad = np.abs(a - b) > bound
+        assert not bad.any(), f"{k}: {bad.sum()} entries out of tolerance, worst {np.abs(a - b)[bad].max():.3e}"
+    return out
+
+
+def _run(verts, idx, cv, tcam, jitter, loss, seed=0):
+    r = run_gpu_forward(verts, idx, cv, tcam, jitter)
+    img = r["img"].cpu().numpy()
+    H, W = img.shape[:2]
+    rng = np.random.default_rng(seed)
+    if loss == "l1":
+        target = rng.uniform(size=(H, W, 3)).astype(np.float32)
+        gimg = np.zeros((H, W, 4), np.float32)
+        gimg[..., :3] = np.sign(img[..., :3] - target) / (H * W * 3)
+        gdist = np.zeros((H, W, 5), np.float32)
+    else:
+        gimg = rng.normal(size=(H, W, 4)).astype(np.float32)
+        gdist = (rng.normal(size=(H, W, 5)) * 1e-3).astype(np.float32)
+    L = r["lists"]
+    gv, gc = R.blend_bwd(L.sorted_ids, L.ranges, r["i"], r["v"], r["c"], r["j"], r["cam"], r["img"], r["dist"],
+                         r["nc"], to_dev(gimg), to_dev(gdist), r["records"], reuse_records=True)
+    torch.cuda.synchronize()
+    lists = dict(cam=r["cam"], sorted_ids=L.sorted_ids.cpu().numpy(), ranges=L.ranges.cpu().numpy())
+    nc = r["nc"].cpu().numpy()[..., 0]
+    v64, c64 = verts.astype(np.float64), cv.astype(np.float64)
+    img64, dist64, _, _, _ = O.blend_fwd_f64(lists, idx, v64, c64, jitter, cut=nc)
+    rgv, rgc = O.blend_bwd(lists, idx, v64, c64, jitter, img64, dist64, nc, gimg.astype(np.float64),
+                           gdist.astype(np.float64), "f64")
+    return _compare(_groups(gv.cpu().numpy(), gc.cpu().numpy()), _groups(rgv, rgc))
+
+
+@pytest.mark.parametrize("loss", ["l1", "linear"])
+def test_backward_gradient_check_workload(cuda, loss):
+    mesh, view = scenes.workload_gradient_check()
+    jitter = np.random.default_rng(1).uniform(0, 1, (view.height, view.width, 2)).astype(np.float32)
+    rel = _run(mesh.vertices, mesh.indices, mesh.cell_values, view.tcam(), jitter, loss)
+    print("relative L2 errors", rel)
+
+
+@pytest.mark.parametrize("name", [n for n in G.names() if not n.startswith("ball")])
+def test_backward_golden_scenes(cuda, name):
+    z, tcam = G.load(name)
+    _run(z["vertices"], z["indices"], z["cell_values"], tcam, z["jitter"], "linear", seed=3)
+
+
+@pytest.mark.parametrize("tile", [4, 8, 32])
+def test_backward_tile_sizes(cuda, tile):
+    mesh, view = scenes.workload_gradient_check(tile)
+    jitter = np.full((view.height, view.width, 2), 0.5, np.float32)
+    _run(mesh.vertices, mesh.indices, mesh.cell_values, view.tcam(tile_size=tile), jitter, "linear", seed=tile)
+
+
+def test_project_backward(cuda):
+    mesh, view = scenes.workload_gradient_check()
+    tcam = view.tcam()
+    cam = R.camera(tcam)
+    v, i = to_dev(mesh.vertices), to_dev(mesh.indices)
+    tiles, rect, vs, cc = R.project_fwd(i, v, cam)
+    rng = np.random.default_rng(9)
+    T = len(mesh.indices)
+    gvs = rng.normal(size=(T, 3)).astype(np.float32)
+    gcc = rng.normal(size=(T, 3)).astype(np.float32)
+    gv = R.project_bwd(i, v, cam, tiles, to_dev(gvs), to_dev(gcc)).cpu().numpy()
+    ref = O.project_bwd(mesh.indices, mesh.vertices, cam, tiles.cpu().numpy(), gvs, gcc)
+    rel = np.linalg.norm(gv - ref) / np.linalg.norm(ref)
+    assert rel <= 1e-5, rel

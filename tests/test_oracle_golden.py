@@ -1,0 +1,35 @@
+"""The oracle reproduces the committed golden fixtures bit for bit (the
+FP32 restatement, including colour, uses the host libm, identical across
+machines running this image), and the FP64 integrator within float32
+storage precision."""
+import numpy as np
+import pytest
+
+import golden_util as G
+from oracle import oracle as O
+
+
+@pytest.mark.parametrize("name", G.names())
+def test_oracle_matches_golden(name):
+    z, tcam = G.load(name)
+    L = O.rasterize_lists(z["indices"], z["vertices"], tcam)
+    for k in ("tiles_touched", "rect", "offsets", "keys", "values", "sorted_keys", "sorted_ids", "ranges"):
+        assert np.array_equal(L[k], z[k]), k
+    for k in ("vs", "circumcenter"):
+        assert np.array_equal(L[k].view(np.uint32), z[k].view(np.uint32)), k
+    img, dist, nc = O.blend_fwd_f32(L, z["indices"], z["vertices"], z["cell_values"], z["jitter"])
+    assert np.array_equal(nc, z["n_contrib"])
+    assert np.array_equal(img.view(np.uint32), z["img"].view(np.uint32))
+    assert np.array_equal(dist.view(np.uint32), z["dist"].view(np.uint32))
+    img64 = O.blend_fwd_f64(L, z["indices"], z["vertices"].astype(np.float64), z["cell_values"].astype(np.float64),
+                            z["jitter"], cut=nc)[0]
+    assert np.abs(img64.astype(np.float32) - z["img64"]).max() <= 1e-6 * max(1.0, np.abs(z["img64"]).max())
+
+
+def test_golden_cover_reference_scenarios():
+    names = G.names()
+    for fam in ("single_tet_center", "single_tet_face", "single_tet_outside", "multi_tet_center",
+                "multi_tet_outside", "multi_tet_random_point", "ball2000"):
+        assert any(n.startswith(fam) for n in names), fam
+    z, _ = G.load("multi_tet_random_point")
+    assert len(z["sorted_ids"]) == 0  # empty pair list (camera on the hull looking out)
