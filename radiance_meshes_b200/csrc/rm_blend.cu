@@ -73,63 +73,106 @@ __global__ void __launch_bounds__(256) pack_kernel(const int4* __restrict__ indi
 __device__ __forceinline__ f3 xyz(float4 q) { return {q.x, q.y, q.z}; }
 
 // Ray / tet intersection (intersect.slang:394-624) on a staged record, with
-// the clamps of evaluate_tetra_interp (interp_version.slang:88-89).
+// the clamps of evaluate_tetra_interp (interp_version.slang:88-89), written
+// without branches: every plane is evaluated and the reference's sequential
+// "if (tplane > t_enter)" / "if (tplane < t_exit)" updates become selects.
+// The quotients are IEEE divisions, so t_enter / t_exit (and with them the
+// hit decision, log T and n_contributors) are bit-identical to the reference
+// rounding.  The backward also needs the selected planes and denominators.
 struct Isect {
     float te, tx;        // raw entering / exiting distances
     float enter, exit;   // clamped
-    bool hit;
+    float dene, denx;    // dot(n, d) of the selected planes
+    int ie, ix;          // selected planes (-1: none)
+    bool geo;            // geometric hit
 };
 
+template <bool PLANES>
 __device__ __forceinline__ Isect intersect(const float4* __restrict__ q, f3 o, f3 d) {
     const f3 a0 = xyz(q[4]) - o;
     const f3 a1 = xyz(q[5]) - o;
-    float te = -1e30f, tx = 1e30f;
+    float te = -1e30f, tx = 1e30f, dene = 1.f, denx = 1.f;
+    int ie = -1, ix = -1;
     bool miss = false;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const f3 n = xyz(q[i]);
         const float dist = -dot3(n, i == 3 ? a1 : a0);
         const float den = dot3(n, d);
-        if (fabsf(den) < 1e-10f) {
-            if (dist > 0.f) miss = true;
-        } else {
-            const float tp = -dist / den;
-            if (den < 0.f) {
-                if (tp > te) te = tp;
-            } else {
-                if (tp < tx) tx = tp;
-            }
+        const bool par = fabsf(den) < 1e-10f;
+        miss |= par && dist > 0.f;
+        const float tp = -dist / den;
+        const bool ue = !par && den < 0.f && tp > te;
+        const bool ux = !par && !(den < 0.f) && tp < tx;
+        te = ue ? tp : te;
+        tx = ux ? tp : tx;
+        if (PLANES) {
+            ie = ue ? i : ie;
+            dene = ue ? den : dene;
+            ix = ux ? i : ix;
+            denx = ux ? den : denx;
         }
     }
     Isect r;
     r.te = te;
     r.tx = tx;
-    r.hit = !miss && !(te > tx) && !(tx <= 0.f);
+    r.geo = !miss && !(te > tx) && !(tx <= 0.f);
     r.enter = fmaxf(te, 0.f);
     r.exit = fmaxf(tx, r.enter);
+    r.dene = dene;
+    r.denx = denx;
+    r.ie = ie;
+    r.ix = ix;
     return r;
 }
 
-__device__ __forceinline__ float phi_f(float x) {  // interp_version.slang:21-28
-    if (fabsf(x) < 1e-6f) return 1.0f - x / 2.0f;
-    return -expm1f(-x) / x;
+// Weights of the closed-form segment integral (interp_version.slang:21-40)
+// for optical depth x = density * dt >= 0:
+//   alpha = exp(-x), phi = (1 - exp(-x)) / x, w0 = phi - alpha, w1 = 1 - phi.
+// Below x = 0.25 w0 and w1 come from their Taylor series (8 terms, truncation
+// < 4e-10 relative), which avoids the cancellation in phi - alpha and 1 - phi;
+// above, phi = (1 - alpha) / x.  These feed only the colour channels, which
+// are compared within a tolerance (log T uses x itself, never these weights).
+struct Weights {
+    float alpha, w0, w1;
+};
+
+__device__ __forceinline__ Weights seg_weights(float x) {
+    Weights w;
+    w.alpha = __expf(-x);
+    if (x < 0.25f) {
+        // w1 = x/2 - x^2/6 + x^3/24 - x^4/120 + x^5/720 - x^6/5040 + x^7/40320
+        w.w1 = x * (0.5f + x * (-1.0f / 6.0f + x * (1.0f / 24.0f + x * (-1.0f / 120.0f + x * (1.0f / 720.0f +
+                 x * (-1.0f / 5040.0f + x * (1.0f / 40320.0f)))))));
+        // w0 = x/2 - x^2/3 + x^3/8 - x^4/30 + x^5/144 - x^6/840 + x^7/5760
+        w.w0 = x * (0.5f + x * (-1.0f / 3.0f + x * (0.125f + x * (-1.0f / 30.0f + x * (1.0f / 144.0f +
+                 x * (-1.0f / 840.0f + x * (1.0f / 5760.0f)))))));
+    } else {
+        const float phi = __fdividef(1.0f - w.alpha, x);
+        w.w0 = phi - w.alpha;
+        w.w1 = 1.0f - phi;
+    }
+    return w;
 }
 
-// d phi / dx; a Taylor series below 1e-2 avoids the cancellation of
-// exp(-x)/x + expm1(-x)/x^2 in single precision.
-__device__ __forceinline__ float dphi_f(float x) {
-    if (fabsf(x) < 1e-2f) return -0.5f + x * (1.0f / 3.0f + x * (-0.125f + x * (1.0f / 30.0f)));
-    return expf(-x) / x + expm1f(-x) / (x * x);
+// d phi / dx = -(d w1 / dx): series below 0.25, (alpha - phi) / x = -w0 / x above.
+__device__ __forceinline__ float dphi_f(float x, const Weights& w) {
+    if (x < 0.25f)
+        return -(0.5f + x * (-1.0f / 3.0f + x * (0.125f + x * (-1.0f / 30.0f + x * (1.0f / 144.0f +
+                 x * (-1.0f / 840.0f))))));
+    return -__fdividef(w.w0, x);
 }
 
 struct Segment {
     float dt, a, x;
     f3 ve, vx;
-    float ce, cx, alpha, phi, w0, w1;
+    float ce, cx;
+    Weights w;
     float rgb[3];
 };
 
-// integrate_tetra_segment + compute_integral (interp_version.slang:30-69).
+// integrate_tetra_segment + compute_integral (interp_version.slang:30-69):
+// rgb = w0 * c_exit + w1 * c_enter with c = base + dot(grd, p - v0).
 __device__ __forceinline__ void integrate(const float4* __restrict__ q, f3 o, f3 d, float enter, float exit,
                                           Segment& s) {
     const float density = q[0].w;
@@ -140,13 +183,10 @@ __device__ __forceinline__ void integrate(const float4* __restrict__ q, f3 o, f3
     s.ce = dot3(grd, s.ve);
     s.cx = dot3(grd, s.vx);
     s.x = s.dt * density;
-    s.alpha = safe_expf(-s.x);
-    s.phi = phi_f(s.x);
-    s.w0 = s.phi - s.alpha;
-    s.w1 = 1.0f - s.phi;
+    s.w = seg_weights(s.x);
     const float base[3] = {q[1].w, q[2].w, q[3].w};
 #pragma unroll
-    for (int k = 0; k < 3; ++k) s.rgb[k] = fmaf(s.w1, s.ce + base[k], s.w0 * (s.cx + base[k]));
+    for (int k = 0; k < 3; ++k) s.rgb[k] = fmaf(s.w.w1, s.ce + base[k], s.w.w0 * (s.cx + base[k]));
 }
 
 struct PixelState {
@@ -202,14 +242,14 @@ __global__ void __launch_bounds__(NT) blend_fwd_kernel(const int32_t* __restrict
                 if (!active) break;
                 ++nc;
                 const float4* q = srec[j];
-                const Isect is = intersect(q, o, d);
+                const Isect is = intersect<false>(q, o, d);
                 Segment s;
                 s.dt = fmaxf(is.exit - is.enter, 0.f);
                 const float density = q[0].w;
                 s.a = density * s.dt;
-                if (is.hit && s.a > 0.f) {
+                if (is.geo && s.a > 0.f) {
                     integrate(q, o, d, is.enter, is.exit, s);
-                    const float T = safe_expf(st.logT);
+                    const float T = __expf(st.logT);
 #pragma unroll
                     for (int k = 0; k < 3; ++k) st.c[k] = fmaf(s.rgb[k], T, st.c[k]);
                     st.logT = st.logT - s.a;
@@ -336,28 +376,11 @@ __global__ void __launch_bounds__(NT) blend_bwd_kernel(
             // ---- recompute the forward quantities of this entry
             const f3 a0 = xyz(q[4]) - o;
             const f3 a1 = xyz(q[5]) - o;
-            float te = -1e30f, tx = 1e30f, dene = 1.f, denx = 1.f;
-            int ie = -1, ix = -1;
-            bool miss = false;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const f3 nn = xyz(q[i]);
-                const float dst = -dot3(nn, i == 3 ? a1 : a0);
-                const float den = dot3(nn, d);
-                if (fabsf(den) < 1e-10f) {
-                    if (dst > 0.f) miss = true;
-                } else {
-                    const float tp = -dst / den;
-                    if (den < 0.f) {
-                        if (tp > te) { te = tp; ie = i; dene = den; }
-                    } else {
-                        if (tp < tx) { tx = tp; ix = i; denx = den; }
-                    }
-                }
-            }
-            const bool geo = !miss && !(te > tx) && !(tx <= 0.f);
-            const float enter = fmaxf(te, 0.f);
-            const float exit = fmaxf(tx, enter);
+            const Isect is = intersect<true>(q, o, d);
+            const float te = is.te, tx = is.tx, dene = is.dene, denx = is.denx;
+            const int ie = is.ie, ix = is.ix;
+            const bool geo = is.geo;
+            const float enter = is.enter, exit = is.exit;
             const float density = q[0].w;
             Segment s;
             s.dt = fmaxf(exit - enter, 0.f);
@@ -369,9 +392,9 @@ __global__ void __launch_bounds__(NT) blend_bwd_kernel(
                 const float m0 = density;
                 const float m1 = density * (exit + enter) / 2.0f;
                 const float logT_old = st.logT + s.a;
-                const float T = safe_expf(logT_old);
+                const float T = __expf(logT_old);
 #pragma unroll
-                for (int k = 0; k < 3; ++k) st.c[k] = st.c[k] - s.rgb[k] * T;
+                for (int k = 0; k < 3; ++k) st.c[k] = fmaf(-s.rgb[k], T, st.c[k]);
                 st.logT = logT_old;
                 st.D[2] = st.D[2] - m0;
                 st.D[3] = st.D[3] - m1;
@@ -397,7 +420,8 @@ __global__ void __launch_bounds__(NT) blend_bwd_kernel(
                     sum_drgb += d_rgb[k];
                 }
                 const float d_a = -dS.logT;
-                const float d_logT_old = dS.logT + (logT_old < kLogMax ? dT * T : 0.f);
+                // safe_exp's clip at log(1e20) never binds: log T <= 0
+                const float d_logT_old = dS.logT + dT * T;
                 // ---- adjoint of compute_integral / integrate_tetra_segment
                 const float base[3] = {q[1].w, q[2].w, q[3].w};
                 float d_w0 = 0.f, d_w1 = 0.f;
@@ -405,10 +429,10 @@ __global__ void __launch_bounds__(NT) blend_bwd_kernel(
                 for (int k = 0; k < 3; ++k) {
                     d_w0 = fmaf(d_rgb[k], s.cx + base[k], d_w0);
                     d_w1 = fmaf(d_rgb[k], s.ce + base[k], d_w1);
-                    gl[19 + k] = d_rgb[k] * (s.w0 + s.w1);
+                    gl[19 + k] = d_rgb[k] * (s.w.w0 + s.w.w1);
                 }
-                const float d_sx = sum_drgb * s.w0, d_se = sum_drgb * s.w1;
-                const float d_x = (d_w0 - d_w1) * dphi_f(s.x) + d_w0 * s.alpha;
+                const float d_sx = sum_drgb * s.w.w0, d_se = sum_drgb * s.w.w1;
+                const float d_x = (d_w0 - d_w1) * dphi_f(s.x, s.w) + d_w0 * s.w.alpha;
                 d_dt += (d_x + d_a) * density;
                 d_dens += (d_x + d_a) * s.dt;
                 const f3 grd = {q[4].w, q[5].w, q[6].w};
