@@ -168,13 +168,25 @@ RM_API int rm_tile_ranges(const int64_t* sorted_keys, int64_t n, const int64_t* 
                    int32_t* ranges, int64_t n_tiles, void* stream);
 
 /* ---------------------------------------------------------------- stage (d) */
-/* Bytes of packed per-tet records (128 B per tet) the blend passes need. */
-RM_API size_t rm_blend_workspace_size(int64_t n_tets);
+/*
+ * Scratch of the blend passes: packed per-tet records (128 B per tet), the
+ * heavy-first tile order of the work queue (4 B per tile) and queue tickets.
+ */
+RM_API size_t rm_blend_workspace_size(int64_t n_tets, int64_t n_tiles);
 
 #define RM_BLEND_REUSE_RECORDS 0x1  /* workspace already holds this frame's records */
+/* flags bits 8..15: log2 of the pixels per work item strip (16 or 64; 0 = 64) */
+#define RM_BLEND_STRIP_SHIFT 8
+#define RM_BLEND_STRIP(log2_pixels) ((log2_pixels) << RM_BLEND_STRIP_SHIFT)
+/* flags bits 16..19: heavy-tile threshold, in powers of two above the mean
+ * list length (0 = default, 1 = every tile is heavy); bits 20..23: resident
+ * CTAs per SM of the kernel that takes the heavy tiles (0 = default) */
+#define RM_BLEND_HEAVY_SHIFT 16
+#define RM_BLEND_PAIR_CTAS_SHIFT 20
 
 /*
- * Front-to-back tile blend.  Replaces splat_tiled
+ * Front-to-back tile blend.  A persistent kernel takes strips of pixels from
+ * a work queue ordered heaviest tile first.  Replaces splat_tiled
  * (delaunay_rasterization/internal/slang/alphablend_shader_interp.slang:371-431,
  * alpha_blend at :194-271) launched by AlphaBlendTiledRender.forward
  * (delaunay_rasterization/internal/alphablend_tiled_slang_interp.py:165-202).

@@ -4,22 +4,29 @@
 // Forward: splat_tiled / alpha_blend (alphablend_shader_interp.slang:194-271,
 // 371-431) with evaluate_tetra_interp and integrate_tetra_segment
 // (interp_version.slang:21-98) and ray_tetrahedron_intersect_fused
-// (intersect.slang:394-624).  One CTA per screen tile, one thread per pixel.
-// The tile's sorted list is walked in batches: each batch's per-tet records
-// (128 B, packed once per frame by pack_kernel) are gathered into shared
-// memory, then every pixel tests its ray against them in list order.  A pixel
-// stops at log T < -5.5; a warp whose pixels are all done skips the batch and
-// the CTA leaves the list once every pixel is done.
+// (intersect.slang:394-624).  Backward: bwd_alpha_blend
+// (alphablend_shader_interp.slang:273-369), with the per-tet derivatives that
+// the reference obtains from Slang autodiff written out by hand.
 //
-// Backward: bwd_alpha_blend (alphablend_shader_interp.slang:273-369).  Each
-// pixel walks its list back to front from the saved final state, skipping list
-// offsets >= n_contributors, undoes each hit and back-propagates through the
-// segment integral and the ray/plane intersection.  Per hit it produces 25
-// partial derivatives (four face-normal gradients, direct v0/v1 gradients and
-// the seven cell values); a warp reduce-scatter sums them across the 32 pixels
-// of a warp, one shared-memory atomic per value accumulates the CTA's sum per
-// list entry, and after each batch the sums are converted to vertex gradients
-// and added to global memory with one atomic per (tile, tet, component).
+// Work decomposition.  Per-tile list lengths are heavy-tailed (a few tiles
+// hold 10-30x the mean), and a pixel whose ray sees through a dense region
+// crosses thousands of tets.  Each pass therefore runs two persistent kernels
+// concurrently, fed by one heavy-first tile order computed on the device:
+//   * the dense kernel walks the ordinary tiles, one thread per pixel, in
+//     strips of 64 pixels (one CTA per strip);
+//   * the pair kernel takes the heavy tiles (list length >= ~4x the mean) and
+//     spreads each strip's (entry, pixel) pairs over 4 threads per pixel; the
+//     strictly ordered part of the walk (log T, termination, distortion
+//     moments in the forward; the undo chains in the backward) is a few adds
+//     per entry done by one owner thread per pixel, in the same arithmetic as
+//     the dense walk, so results do not depend on which kernel ran a tile.
+// In both, per-tet records (128 B, packed once per frame by pack_kernel) are
+// staged in shared memory per batch of list entries.  Backward gradients are
+// summed per list entry across the pixels of a CTA (warp reduce-scatter, then
+// shared-memory atomics) and converted to vertex gradients once per
+// (CTA, entry) before the global atomics.
+#include <mutex>
+
 #include "rm_internal.cuh"
 
 namespace rm {
@@ -27,6 +34,7 @@ namespace {
 
 constexpr float kTermLogT = -5.5f;  // alphablend_shader_interp.slang:257
 constexpr int kNGrad = 25;
+
 
 // ------------------------------------------------------------------ packing --
 __global__ void __launch_bounds__(256) pack_kernel(const int4* __restrict__ indices, const float* __restrict__ verts,
@@ -203,18 +211,100 @@ struct WarpShape {
     static constexpr int kWarps = NT >= 32 ? NT / 32 : 1;
 };
 
+// Work queue shared by the kernels of one pass.  order[] lists the tiles
+// heaviest first; info[0] is the number of heavy tiles (the first entries of
+// order[]), which go to the pair kernel, the rest to the dense kernel.
+struct Queue {
+    const int32_t* order;
+    const int32_t* info;
+    uint32_t* ticket;
+    int G;
+    int subs;  // strips per tile
+    bool heavy;
+};
+
+__device__ __forceinline__ int queue_items(const Queue& q) {
+    const int nh = __ldg(q.info);
+    return (q.heavy ? nh : q.G - nh) * q.subs;
+}
+
+__device__ __forceinline__ int queue_tile(const Queue& q, int item) {
+    const int first = q.heavy ? 0 : __ldg(q.info);
+    return __ldg(q.order + first + item / q.subs);
+}
+
+__device__ __forceinline__ int next_item(const Queue& q, int* s_item) {
+    if (threadIdx.x == 0) *s_item = (int)atomicAdd(q.ticket, 1u);
+    __syncthreads();
+    const int item = *s_item;
+    __syncthreads();
+    return item;
+}
+
+// One hit folded into the pixel state (update_alpha_out,
+// alphablend_shader_interp.slang:84-183): colour += rgb * T, log T -= a, and
+// the five distortion moments with m0 = density, m1 = density * (a + b) / 2.
+__device__ __forceinline__ void fold_hit(PixelState& st, float a, float m0, float m1, float d4, const float* rgb) {
+    const float T = __expf(st.logT);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) st.c[k] = fmaf(rgb[k], T, st.c[k]);
+    st.logT = st.logT - a;
+    const float D2 = st.D[2], D3 = st.D[3];
+    st.D[0] = fmaf(2.0f * m1, D2, st.D[0]);
+    st.D[1] = fmaf(2.0f * m0, D3, st.D[1]);
+    st.D[2] = D2 + m0;
+    st.D[3] = D3 + m1;
+    st.D[4] = st.D[4] + d4;
+}
+
+// Result of testing one ray against one list entry, in the exact arithmetic of
+// the dense path: a = density * dt (0 for a miss), m1, the D4 increment
+// density^2 * dt / 3 and the segment colour.
+struct EntryResult {
+    float a, m1, d4;
+    float rgb[3];
+};
+
+__device__ __forceinline__ EntryResult eval_entry(const float4* __restrict__ q, f3 o, f3 d) {
+    EntryResult r;
+    const Isect is = intersect<false>(q, o, d);
+    Segment s;
+    s.dt = fmaxf(is.exit - is.enter, 0.f);
+    const float density = q[0].w;
+    s.a = density * s.dt;
+    r.a = 0.f;
+    r.m1 = 0.f;
+    r.d4 = 0.f;
+    r.rgb[0] = r.rgb[1] = r.rgb[2] = 0.f;
+    if (is.geo && s.a > 0.f) {
+        integrate(q, o, d, is.enter, is.exit, s);
+        r.a = s.a;
+        r.m1 = density * (is.exit + is.enter) / 2.0f;
+        r.d4 = density * density * s.dt / 3.0f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) r.rgb[k] = s.rgb[k];
+    }
+    return r;
+}
+
+// Dense forward item: a strip of NT pixels (NT / tile_width rows), one thread
+// per pixel walking the tile's list in order.
+template <int B>
+struct FwdDenseSmem {
+    float4 srec[B][kRecFloat4];
+    int32_t sid[B];
+};
+
 template <int NT, int B>
-__global__ void __launch_bounds__(NT) blend_fwd_kernel(const int32_t* __restrict__ ids,
-                                                       const int2* __restrict__ ranges,
-                                                       const float4* __restrict__ recs,
-                                                       const float2* __restrict__ jitter, const rm_camera cam,
-                                                       float4* __restrict__ out_img, float* __restrict__ out_dist,
-                                                       int32_t* __restrict__ out_nc) {
-    __shared__ float4 srec[B][kRecFloat4];
-    __shared__ int32_t sid[B];
-    const int tile = blockIdx.x;
+__device__ __forceinline__ void fwd_dense_item(int tile, int sub, const int32_t* __restrict__ ids,
+                                               const int2* __restrict__ ranges, const float4* __restrict__ recs,
+                                               const float2* __restrict__ jitter, const rm_camera& cam,
+                                               float4* __restrict__ out_img, float* __restrict__ out_dist,
+                                               int32_t* __restrict__ out_nc, FwdDenseSmem<B>& S) {
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
-    const int lx = threadIdx.x % cam.tile_width, ly = threadIdx.x / cam.tile_width;
+    const int tp = sub * NT + (int)threadIdx.x;  // pixel index inside the tile (row-major)
+    const int lx = tp % cam.tile_width;
+    const int ly = tp / cam.tile_width;
     const int px = tx * cam.tile_width + lx, py = ty * cam.tile_height + ly;
     const bool inside = px < cam.image_width && py < cam.image_height;
     const int64_t pix = (int64_t)py * cam.image_width + px;
@@ -227,45 +317,29 @@ __global__ void __launch_bounds__(NT) blend_fwd_kernel(const int32_t* __restrict
     PixelState st = {{0.f, 0.f, 0.f}, 0.f, {0.f, 0.f, 0.f, 0.f, 0.f}};
     int32_t nc = 0;
     bool active = inside;
-    for (int base = rg.x; base < rg.y; base += B) {
-        const int n = min(B, rg.y - base);
-        __syncthreads();
-        for (int k = threadIdx.x; k < n; k += NT) sid[k] = __ldg(ids + base + k);
-        __syncthreads();
-        for (int k = threadIdx.x; k < n * kRecFloat4; k += NT) {
-            const int j = k >> 3, c = k & 7;
-            srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * sid[j] + c);
-        }
-        __syncthreads();
-        if (__any_sync(WarpShape<NT>::kMask, active)) {
-            for (int j = 0; j < n; ++j) {
-                if (!active) break;
-                ++nc;
-                const float4* q = srec[j];
-                const Isect is = intersect<false>(q, o, d);
-                Segment s;
-                s.dt = fmaxf(is.exit - is.enter, 0.f);
-                const float density = q[0].w;
-                s.a = density * s.dt;
-                if (is.geo && s.a > 0.f) {
-                    integrate(q, o, d, is.enter, is.exit, s);
-                    const float T = __expf(st.logT);
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) st.c[k] = fmaf(s.rgb[k], T, st.c[k]);
-                    st.logT = st.logT - s.a;
-                    const float m0 = density;
-                    const float m1 = density * (is.exit + is.enter) / 2.0f;
-                    const float D2 = st.D[2], D3 = st.D[3];
-                    st.D[0] = fmaf(2.0f * m1, D2, st.D[0]);
-                    st.D[1] = fmaf(2.0f * m0, D3, st.D[1]);
-                    st.D[2] = D2 + m0;
-                    st.D[3] = D3 + m1;
-                    st.D[4] = st.D[4] + density * density * s.dt / 3.0f;
-                    if (st.logT < kTermLogT) active = false;
+    if (__syncthreads_or(active)) {
+        for (int base = rg.x; base < rg.y; base += B) {
+            const int n = min(B, rg.y - base);
+            for (int k = threadIdx.x; k < n; k += NT) S.sid[k] = __ldg(ids + base + k);
+            __syncthreads();
+            for (int k = threadIdx.x; k < n * kRecFloat4; k += NT) {
+                const int j = k >> 3, c = k & 7;
+                S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
+            }
+            __syncthreads();
+            if (__any_sync(WarpShape<NT>::kMask, active)) {
+                for (int j = 0; j < n; ++j) {
+                    if (!active) break;
+                    ++nc;
+                    const EntryResult r = eval_entry(S.srec[j], o, d);
+                    if (r.a > 0.f) {
+                        fold_hit(st, r.a, S.srec[j][0].w, r.m1, r.d4, r.rgb);
+                        if (st.logT < kTermLogT) active = false;
+                    }
                 }
             }
+            if (!__syncthreads_or(active)) break;
         }
-        if (!__syncthreads_or(active)) break;
     }
     if (inside) {
         out_img[pix] = make_float4(st.c[0], st.c[1], st.c[2], st.logT);
@@ -273,6 +347,193 @@ __global__ void __launch_bounds__(NT) blend_fwd_kernel(const int32_t* __restrict
 #pragma unroll
         for (int k = 0; k < 5; ++k) dd[k] = st.D[k];
         out_nc[pix] = nc;
+    }
+}
+
+// Pair forward item: a strip of PX pixels (PX / tile_width rows of one tile)
+// handled by NT >= PX threads.  Threads 0..PX-1 own one pixel each.  Per batch
+// of B list entries the records are staged in shared memory, the still-active
+// pixels are compacted into slots, and all NT threads evaluate the
+// (entry, slot) pairs -- a warp takes one entry at a time (its record is read
+// as a broadcast) and its lanes take the slots -- writing each pair's a, m1,
+// D4 increment and colour to shared memory.  Each owner then folds its
+// pixel's results in list order: this sequential part is a handful of adds
+// per entry, so a pixel whose ray crosses thousands of tets no longer runs
+// the whole intersection/integration chain on one thread.  The fold uses
+// exactly the arithmetic of the one-thread-per-pixel walk, so n_contributors,
+// log T and the distortion moments are unchanged bit for bit.
+template <int PX, int B>
+struct FwdPairSmem {
+    float4 srec[B][kRecFloat4];
+    int32_t sid[B];
+    float ray[6][PX];      // o, d of each slot (structure of arrays)
+    float res[6][B][PX];   // a (0: miss), m1, d4, r, g, b per (entry, slot)
+    int32_t warp_base[(PX + 31) / 32];
+};
+
+template <int PX, int NT, int B>
+__device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* __restrict__ ids,
+                                         const int2* __restrict__ ranges, const float4* __restrict__ recs,
+                                         const float2* __restrict__ jitter, const rm_camera& cam,
+                                         float4* __restrict__ out_img, float* __restrict__ out_dist,
+                                         int32_t* __restrict__ out_nc, FwdPairSmem<PX, B>& S) {
+    constexpr unsigned kOwnMask = WarpShape<PX>::kMask;
+    constexpr int kWarps = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool owner = tid < PX;
+    const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
+    const int tp = sub * PX + tid;  // pixel index inside the tile (row-major)
+    const int lx = tp % cam.tile_width;
+    const int ly = tp / cam.tile_width;
+    const int px = tx * cam.tile_width + lx, py = ty * cam.tile_height + ly;
+    const bool inside = owner && px < cam.image_width && py < cam.image_height;
+    const int64_t pix = (int64_t)py * cam.image_width + px;
+    f3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
+    if (inside) {
+        const float2 j = __ldg(jitter + pix);
+        make_ray(cam, px, py, j.x, j.y, o, d);
+    }
+    const int2 rg = __ldg(ranges + tile);
+    PixelState st = {{0.f, 0.f, 0.f}, 0.f, {0.f, 0.f, 0.f, 0.f, 0.f}};
+    int32_t nc = 0;
+    bool active = inside;
+    int n_active = __syncthreads_count(active);
+    for (int base = rg.x; base < rg.y && n_active > 0; base += B) {
+        const int n = min(B, rg.y - base);
+        for (int k = tid; k < n; k += NT) S.sid[k] = __ldg(ids + base + k);
+        int slot = 0;
+        if (owner) {
+            const unsigned bal = __ballot_sync(kOwnMask, active);
+            if (lane == 0) S.warp_base[warp] = __popc(bal);
+            slot = __popc(bal & ((1u << lane) - 1u));
+        }
+        __syncthreads();
+        for (int k = tid; k < n * kRecFloat4; k += NT) {
+            const int j = k >> 3, c = k & 7;
+            S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
+        }
+        if (active) {
+            for (int w = 0; w < warp; ++w) slot += S.warp_base[w];
+            S.ray[0][slot] = o.x; S.ray[1][slot] = o.y; S.ray[2][slot] = o.z;
+            S.ray[3][slot] = d.x; S.ray[4][slot] = d.y; S.ray[5][slot] = d.z;
+        }
+        __syncthreads();
+        for (int j = warp; j < n; j += kWarps) {
+            const float4* q = S.srec[j];
+            for (int sl = lane; sl < n_active; sl += 32) {
+                const f3 ro = {S.ray[0][sl], S.ray[1][sl], S.ray[2][sl]};
+                const f3 rd = {S.ray[3][sl], S.ray[4][sl], S.ray[5][sl]};
+                const EntryResult r = eval_entry(q, ro, rd);
+                S.res[0][j][sl] = r.a;
+                S.res[1][j][sl] = r.m1;
+                S.res[2][j][sl] = r.d4;
+                S.res[3][j][sl] = r.rgb[0];
+                S.res[4][j][sl] = r.rgb[1];
+                S.res[5][j][sl] = r.rgb[2];
+            }
+        }
+        __syncthreads();
+        if (active) {
+            for (int j = 0; j < n; ++j) {
+                ++nc;
+                const float a = S.res[0][j][slot];
+                if (a > 0.f) {
+                    const float rgb[3] = {S.res[3][j][slot], S.res[4][j][slot], S.res[5][j][slot]};
+                    fold_hit(st, a, S.srec[j][0].w, S.res[1][j][slot], S.res[2][j][slot], rgb);
+                    if (st.logT < kTermLogT) {
+                        active = false;
+                        break;
+                    }
+                }
+            }
+        }
+        n_active = __syncthreads_count(active);
+    }
+    if (inside) {
+        out_img[pix] = make_float4(st.c[0], st.c[1], st.c[2], st.logT);
+        float* dd = out_dist + 5 * pix;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) dd[k] = st.D[k];
+        out_nc[pix] = nc;
+    }
+}
+
+template <int NT, int B>
+__global__ void __launch_bounds__(NT, (NT >= 64 ? 1024 / NT : 32)) blend_fwd_dense_kernel(
+    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
+    const float2* __restrict__ jitter, const rm_camera cam, float4* __restrict__ out_img,
+    float* __restrict__ out_dist, int32_t* __restrict__ out_nc, const Queue q) {
+    __shared__ FwdDenseSmem<B> S;
+    __shared__ int s_item;
+    const int n_items = queue_items(q);
+    for (;;) {
+        const int item = next_item(q, &s_item);
+        if (item >= n_items) return;
+        fwd_dense_item<NT, B>(queue_tile(q, item), item % q.subs, ids, ranges, recs, jitter, cam, out_img, out_dist,
+                              out_nc, S);
+    }
+}
+
+template <int PX, int NT, int B>
+__global__ void __launch_bounds__(NT, 768 / NT) blend_fwd_pair_kernel(
+    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
+    const float2* __restrict__ jitter, const rm_camera cam, float4* __restrict__ out_img,
+    float* __restrict__ out_dist, int32_t* __restrict__ out_nc, const Queue q) {
+    extern __shared__ __align__(16) unsigned char fwd_smem_raw[];
+    FwdPairSmem<PX, B>& S = *reinterpret_cast<FwdPairSmem<PX, B>*>(fwd_smem_raw);
+    __shared__ int s_item;
+    const int n_items = queue_items(q);
+    for (;;) {
+        const int item = next_item(q, &s_item);
+        if (item >= n_items) return;
+        fwd_pair_item<PX, NT, B>(queue_tile(q, item), item % q.subs, ids, ranges, recs, jitter, cam, out_img,
+                                 out_dist, out_nc, S);
+    }
+}
+
+// Orders the tiles heaviest first by floor(log2(list length)) (the order
+// inside a bucket does not matter), marks as heavy the tiles whose bucket is
+// at least heavy_shift above that of the mean non-empty list length and at
+// least 2^10 entries (info[0] = their count), and resets the queue tickets.
+__global__ void __launch_bounds__(1024) order_kernel(const int2* __restrict__ ranges, int G,
+                                                     int32_t* __restrict__ order, int32_t* info,
+                                                     uint32_t* tickets, int heavy_shift) {
+    __shared__ uint32_t cnt[33], base[33], cur[33];
+    __shared__ unsigned long long total;
+    __shared__ uint32_t nonempty;
+    if (threadIdx.x < 33) cnt[threadIdx.x] = 0, cur[threadIdx.x] = 0;
+    if (threadIdx.x == 0) total = 0ull, nonempty = 0u;
+    __syncthreads();
+    for (int t = threadIdx.x; t < G; t += blockDim.x) {
+        const int2 r = __ldg(ranges + t);
+        const uint32_t len = (uint32_t)max(r.y - r.x, 0);
+        atomicAdd(&cnt[32 - __clz(len)], 1u);
+        if (len) {
+            atomicAdd(&total, (unsigned long long)len);
+            atomicAdd(&nonempty, 1u);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int b = 32; b >= 0; --b) {
+            base[b] = run;
+            run += cnt[b];
+        }
+        const uint32_t mean = nonempty ? (uint32_t)(total / nonempty) : 0u;
+        // heavy_shift 1 sends every tile to the pair kernel
+        const int b_thr = heavy_shift == 1 ? 0 : max(11, 32 - __clz(mean) + heavy_shift);
+        int heavy = 0;
+        for (int b = 32; b >= b_thr; --b) heavy += (int)cnt[b];
+        info[0] = heavy;
+        for (int k = 0; k < 4; ++k) tickets[k] = 0u;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < G; t += blockDim.x) {
+        const int2 r = __ldg(ranges + t);
+        const uint32_t len = (uint32_t)max(r.y - r.x, 0);
+        const int b = 32 - __clz(len);
+        order[base[b] + atomicAdd(&cur[b], 1u)] = t;
     }
 }
 
@@ -306,179 +567,240 @@ struct ReduceScatter<M, 0> {
     static __device__ __forceinline__ void run(float*, int, int&) {}
 };
 
+// Adjoint of one hit (the Slang autodiff of update_alpha_out,
+// evaluate_tetra_interp and load_tet_alphablend_interp, written out by hand).
+// Inputs: the entry's intersection and segment, T = exp(log T) and D2, D3 of
+// the state before the hit, and dL/d(state after the hit) (dS_c, dS_logT,
+// dS_D).  Outputs the 25 per-entry partials gl[] (face normals 0..11, direct
+// v0 12..14, v1 15..17, density 18, rgb 19..21, grd 22..24) and returns
+// dL/d(log T before the hit); nD2 / nD3 receive dL/d(D2, D3 before the hit).
+__device__ __forceinline__ float hit_grads(const float4* __restrict__ q, f3 o, f3 d, const Isect& is,
+                                           const Segment& s, float T, float D2_old, float D3_old,
+                                           const float* dS_c, float dS_logT, const float* dS_D, float* gl,
+                                           float& nD2, float& nD3) {
+    const float density = q[0].w;
+    const float enter = is.enter, exit = is.exit;
+    const float m1 = density * (exit + enter) / 2.0f;
+    // update_distortion_state
+    const float dm1 = dS_D[0] * 2.0f * D2_old + dS_D[3];
+    const float dm0 = dS_D[1] * 2.0f * D3_old + dS_D[2];
+    nD2 = dS_D[2] + dS_D[0] * 2.0f * m1;
+    nD3 = dS_D[3] + dS_D[1] * 2.0f * density;
+    float d_dens = dm0 + dm1 * (exit + enter) * 0.5f;
+    float d_enter = dm1 * density * 0.5f;
+    float d_exit = d_enter;
+    float d_dt = dS_D[4] * density * density * (1.0f / 3.0f);
+    d_dens += dS_D[4] * 2.0f * density * s.dt * (1.0f / 3.0f);
+    // update_pixel_state
+    float d_rgb[3], dT = 0.f, sum_drgb = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        d_rgb[k] = dS_c[k] * T;
+        dT = fmaf(dS_c[k], s.rgb[k], dT);
+        sum_drgb += d_rgb[k];
+    }
+    const float d_a = -dS_logT;
+    // compute_integral / integrate_tetra_segment
+    const float base[3] = {q[1].w, q[2].w, q[3].w};
+    float d_w0 = 0.f, d_w1 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        d_w0 = fmaf(d_rgb[k], s.cx + base[k], d_w0);
+        d_w1 = fmaf(d_rgb[k], s.ce + base[k], d_w1);
+        gl[19 + k] = d_rgb[k] * (s.w.w0 + s.w.w1);
+    }
+    const float d_sx = sum_drgb * s.w.w0, d_se = sum_drgb * s.w.w1;
+    const float d_x = (d_w0 - d_w1) * dphi_f(s.x, s.w) + d_w0 * s.w.alpha;
+    d_dt += (d_x + d_a) * density;
+    d_dens += (d_x + d_a) * s.dt;
+    const f3 grd = {q[4].w, q[5].w, q[6].w};
+    gl[22] = d_se * s.ve.x + d_sx * s.vx.x;
+    gl[23] = d_se * s.ve.y + d_sx * s.vx.y;
+    gl[24] = d_se * s.ve.z + d_sx * s.vx.z;
+    const float d_sum = d_se + d_sx;
+    const float gd = dot3(grd, d);
+    d_enter += d_se * gd;
+    d_exit += d_sx * gd;
+    gl[12] = -grd.x * d_sum;
+    gl[13] = -grd.y * d_sum;
+    gl[14] = -grd.z * d_sum;
+    gl[15] = gl[16] = gl[17] = 0.f;
+    if (exit - enter > 0.f) {
+        d_exit += d_dt;
+        d_enter -= d_dt;
+    }
+    gl[18] = density > 0.f ? d_dens : 0.f;
+    float d_tx = 0.f;
+    if (is.tx > enter) d_tx = d_exit; else d_enter += d_exit;
+    const float d_te = is.te > 0.f ? d_enter : 0.f;
+    // plane intersections t = dot(n, vref - o) / dot(n, d)
+    const f3 a0 = xyz(q[4]) - o;
+    const f3 a1 = xyz(q[5]) - o;
+    const float ge = d_te / is.dene, gx = d_tx / is.denx;
+    const f3 ae = is.ie == 3 ? a1 : a0, ax = is.ix == 3 ? a1 : a0;
+    const f3 dne = {ge * (ae.x - is.te * d.x), ge * (ae.y - is.te * d.y), ge * (ae.z - is.te * d.z)};
+    const f3 dnx = {gx * (ax.x - is.tx * d.x), gx * (ax.y - is.tx * d.y), gx * (ax.z - is.tx * d.z)};
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const f3 np = xyz(q[p]);
+        const float se = (is.ie == p) ? ge : 0.f, sx = (is.ix == p) ? gx : 0.f;
+        gl[3 * p + 0] = (is.ie == p ? dne.x : 0.f) + (is.ix == p ? dnx.x : 0.f);
+        gl[3 * p + 1] = (is.ie == p ? dne.y : 0.f) + (is.ix == p ? dnx.y : 0.f);
+        gl[3 * p + 2] = (is.ie == p ? dne.z : 0.f) + (is.ix == p ? dnx.z : 0.f);
+        const float sref = se + sx;  // gradient of vref = +n * g
+        if (p == 3) {
+            gl[15] += np.x * sref;
+            gl[16] += np.y * sref;
+            gl[17] += np.z * sref;
+        } else {
+            gl[12] += np.x * sref;
+            gl[13] += np.y * sref;
+            gl[14] += np.z * sref;
+        }
+    }
+    // safe_exp's clip at log(1e20) never binds: log T <= 0
+    return dS_logT + dT * T;
+}
+
+// Converts the per-entry sums of the 25 partials into vertex and cell-value
+// gradients and adds them to global memory (one thread per entry).
 template <int NT, int B>
-__global__ void __launch_bounds__(NT) blend_bwd_kernel(
-    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
-    const int4* __restrict__ indices, const float2* __restrict__ jitter, const rm_camera cam,
-    const float4* __restrict__ img, const float* __restrict__ dist, const int32_t* __restrict__ ncs,
-    const float4* __restrict__ gimg, const float* __restrict__ gdist, float* __restrict__ gverts,
-    float* __restrict__ gcv) {
-    __shared__ float4 srec[B][kRecFloat4];
-    __shared__ int32_t sid[B];
-    __shared__ float sacc[B][kNGrad];
-    __shared__ int32_t smax[WarpShape<NT>::kWarps];
+__device__ __forceinline__ void flush_entries(int n, const float4 (*srec)[kRecFloat4], const int32_t* sid,
+                                              const float (*sacc)[kNGrad], const int4* __restrict__ indices,
+                                              float* __restrict__ gverts, float* __restrict__ gcv) {
+    for (int jj = threadIdx.x; jj < n; jj += NT) {
+        float v[kNGrad];
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < kNGrad; ++k) {
+            v[k] = sacc[jj][k];
+            any |= v[k] != 0.f;
+        }
+        if (!any) continue;
+        const float4* q = srec[jj];
+        const int g = sid[jj];
+        const f3 P[4] = {xyz(q[4]), xyz(q[5]), xyz(q[6]), xyz(q[7])};
+        const uint32_t flips = __float_as_uint(q[7].w);
+        f3 gv[4] = {{v[12], v[13], v[14]}, {v[15], v[16], v[17]}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        const int pp[4] = {1, 1, 2, 2}, pq[4] = {0, 0, 0, 1}, pr[4] = {2, 3, 3, 3};
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            f3 gc = {v[3 * p], v[3 * p + 1], v[3 * p + 2]};
+            if (flips & (1u << p)) gc = neg3(gc);
+            const f3 ea = P[pp[p]] - P[pq[p]], eb = P[pr[p]] - P[pq[p]];
+            const f3 ga = cross3(eb, gc), gb = cross3(gc, ea);
+            gv[pp[p]] = gv[pp[p]] + ga;
+            gv[pr[p]] = gv[pr[p]] + gb;
+            gv[pq[p]] = gv[pq[p]] - (ga + gb);
+        }
+        const int4 id = __ldg(indices + g);
+        const int vid[4] = {id.x, id.y, id.z, id.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float* dst = gverts + 3 * (int64_t)vid[i];
+            if (gv[i].x != 0.f) atomicAdd(dst, gv[i].x);
+            if (gv[i].y != 0.f) atomicAdd(dst + 1, gv[i].y);
+            if (gv[i].z != 0.f) atomicAdd(dst + 2, gv[i].z);
+        }
+        float* dc = gcv + 7 * (int64_t)g;
+#pragma unroll
+        for (int k = 0; k < 7; ++k)
+            if (v[18 + k] != 0.f) atomicAdd(dc + k, v[18 + k]);
+    }
+}
+
+// Dense backward item: a strip of NT pixels, one thread per pixel walking its
+// list back to front from the saved final state.
+template <int NT, int B>
+struct BwdDenseSmem {
+    float4 srec[B][kRecFloat4];
+    int32_t sid[B];
+    float sacc[B][kNGrad];
+    int32_t smax[WarpShape<NT>::kWarps];
+};
+
+template <int NT, int B>
+__device__ __forceinline__ void bwd_dense_item(
+    int tile, int sub, const int32_t* __restrict__ ids, const int2* __restrict__ ranges,
+    const float4* __restrict__ recs, const int4* __restrict__ indices, const float2* __restrict__ jitter,
+    const rm_camera& cam, const float4* __restrict__ img, const float* __restrict__ dist,
+    const int32_t* __restrict__ ncs, const float4* __restrict__ gimg, const float* __restrict__ gdist,
+    float* __restrict__ gverts, float* __restrict__ gcv, BwdDenseSmem<NT, B>& S) {
     constexpr unsigned kMask = WarpShape<NT>::kMask;
-    const int tile = blockIdx.x;
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
-    const int lx = threadIdx.x % cam.tile_width, ly = threadIdx.x / cam.tile_width;
+    const int tp = sub * NT + (int)threadIdx.x;  // pixel index inside the tile (row-major)
+    const int lx = tp % cam.tile_width;
+    const int ly = tp / cam.tile_width;
     const int px = tx * cam.tile_width + lx, py = ty * cam.tile_height + ly;
     const bool inside = px < cam.image_width && py < cam.image_height;
     const int64_t pix = (int64_t)py * cam.image_width + px;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     f3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
-    PixelState st = {{0.f, 0.f, 0.f}, 0.f, {0.f, 0.f, 0.f, 0.f, 0.f}};
-    PixelState dS = st;
+    float logT = 0.f, D2 = 0.f, D3 = 0.f;  // state along the reverse walk
+    float dS_c[3] = {0.f, 0.f, 0.f}, dS_logT = 0.f, dS_D[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     int32_t nc = 0;
     if (inside) {
         const float2 j = __ldg(jitter + pix);
         make_ray(cam, px, py, j.x, j.y, o, d);
-        const float4 a = __ldg(img + pix);
-        st.c[0] = a.x; st.c[1] = a.y; st.c[2] = a.z; st.logT = a.w;
+        logT = __ldg(img + pix).w;
+        D2 = __ldg(dist + 5 * pix + 2);
+        D3 = __ldg(dist + 5 * pix + 3);
         const float4 g = __ldg(gimg + pix);
-        dS.c[0] = g.x; dS.c[1] = g.y; dS.c[2] = g.z; dS.logT = g.w;
+        dS_c[0] = g.x; dS_c[1] = g.y; dS_c[2] = g.z; dS_logT = g.w;
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            st.D[k] = __ldg(dist + 5 * pix + k);
-            dS.D[k] = gdist ? __ldg(gdist + 5 * pix + k) : 0.f;
-        }
+        for (int k = 0; k < 5; ++k) dS_D[k] = gdist ? __ldg(gdist + 5 * pix + k) : 0.f;
         nc = __ldg(ncs + pix);
     }
     int32_t m = nc;
 #pragma unroll
     for (int off = WarpShape<NT>::kTopOffset; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(kMask, m, off));
-    if (lane == 0) smax[warp] = m;
+    if (lane == 0) S.smax[warp] = m;
     __syncthreads();
     int32_t tile_max = 0;
 #pragma unroll
-    for (int w = 0; w < WarpShape<NT>::kWarps; ++w) tile_max = max(tile_max, smax[w]);
+    for (int w = 0; w < WarpShape<NT>::kWarps; ++w) tile_max = max(tile_max, S.smax[w]);
     const int2 rg = __ldg(ranges + tile);
     const int end = min(rg.y, rg.x + tile_max);
     for (int top = end; top > rg.x; top -= B) {
         const int lo = max(rg.x, top - B);
         const int n = top - lo;
         __syncthreads();
-        for (int k = threadIdx.x; k < n; k += NT) sid[k] = __ldg(ids + lo + k);
-        for (int k = threadIdx.x; k < n * kNGrad; k += NT) (&sacc[0][0])[k] = 0.f;
+        for (int k = threadIdx.x; k < n; k += NT) S.sid[k] = __ldg(ids + lo + k);
+        for (int k = threadIdx.x; k < n * kNGrad; k += NT) (&S.sacc[0][0])[k] = 0.f;
         __syncthreads();
         for (int k = threadIdx.x; k < n * kRecFloat4; k += NT) {
             const int j = k >> 3, c = k & 7;
-            srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * sid[j] + c);
+            S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
         }
         __syncthreads();
         for (int jj = n - 1; jj >= 0; --jj) {
             const int off = lo + jj - rg.x;
             const bool act = inside && off < nc;
             if (!__any_sync(kMask, act)) continue;
-            const float4* q = srec[jj];
+            const float4* q = S.srec[jj];
             float gl[kNGrad];
 #pragma unroll
             for (int k = 0; k < kNGrad; ++k) gl[k] = 0.f;
-            // ---- recompute the forward quantities of this entry
-            const f3 a0 = xyz(q[4]) - o;
-            const f3 a1 = xyz(q[5]) - o;
             const Isect is = intersect<true>(q, o, d);
-            const float te = is.te, tx = is.tx, dene = is.dene, denx = is.denx;
-            const int ie = is.ie, ix = is.ix;
-            const bool geo = is.geo;
-            const float enter = is.enter, exit = is.exit;
             const float density = q[0].w;
             Segment s;
-            s.dt = fmaxf(exit - enter, 0.f);
+            s.dt = fmaxf(is.exit - is.enter, 0.f);
             s.a = density * s.dt;
-            const bool hit = act && geo && s.a > 0.f;
+            const bool hit = act && is.geo && s.a > 0.f;
             if (hit) {
-                integrate(q, o, d, enter, exit, s);
-                // ---- undo_alpha_out (alphablend_shader_interp.slang:128-192)
-                const float m0 = density;
-                const float m1 = density * (exit + enter) / 2.0f;
-                const float logT_old = st.logT + s.a;
+                integrate(q, o, d, is.enter, is.exit, s);
+                // undo_alpha_out (alphablend_shader_interp.slang:128-192): only log T, D2
+                // and D3 of the earlier state enter the adjoint
+                const float m1 = density * (is.exit + is.enter) / 2.0f;
+                const float logT_old = logT + s.a;
                 const float T = __expf(logT_old);
-#pragma unroll
-                for (int k = 0; k < 3; ++k) st.c[k] = fmaf(-s.rgb[k], T, st.c[k]);
-                st.logT = logT_old;
-                st.D[2] = st.D[2] - m0;
-                st.D[3] = st.D[3] - m1;
-                st.D[0] = st.D[0] - 2.0f * m1 * st.D[2];
-                st.D[1] = st.D[1] - 2.0f * m0 * st.D[3];
-                st.D[4] = st.D[4] - density * density * s.dt / 3.0f;
-                // ---- adjoint of update_distortion_state
-                const float dm1 = dS.D[0] * 2.0f * st.D[2] + dS.D[3];
-                const float dm0 = dS.D[1] * 2.0f * st.D[3] + dS.D[2];
-                const float nD2 = dS.D[2] + dS.D[0] * 2.0f * m1;
-                const float nD3 = dS.D[3] + dS.D[1] * 2.0f * m0;
-                float d_dens = dm0 + dm1 * (exit + enter) * 0.5f;
-                float d_enter = dm1 * density * 0.5f;
-                float d_exit = d_enter;
-                float d_dt = dS.D[4] * density * density * (1.0f / 3.0f);
-                d_dens += dS.D[4] * 2.0f * density * s.dt * (1.0f / 3.0f);
-                // ---- adjoint of update_pixel_state
-                float d_rgb[3], dT = 0.f, sum_drgb = 0.f;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    d_rgb[k] = dS.c[k] * T;
-                    dT = fmaf(dS.c[k], s.rgb[k], dT);
-                    sum_drgb += d_rgb[k];
-                }
-                const float d_a = -dS.logT;
-                // safe_exp's clip at log(1e20) never binds: log T <= 0
-                const float d_logT_old = dS.logT + dT * T;
-                // ---- adjoint of compute_integral / integrate_tetra_segment
-                const float base[3] = {q[1].w, q[2].w, q[3].w};
-                float d_w0 = 0.f, d_w1 = 0.f;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    d_w0 = fmaf(d_rgb[k], s.cx + base[k], d_w0);
-                    d_w1 = fmaf(d_rgb[k], s.ce + base[k], d_w1);
-                    gl[19 + k] = d_rgb[k] * (s.w.w0 + s.w.w1);
-                }
-                const float d_sx = sum_drgb * s.w.w0, d_se = sum_drgb * s.w.w1;
-                const float d_x = (d_w0 - d_w1) * dphi_f(s.x, s.w) + d_w0 * s.w.alpha;
-                d_dt += (d_x + d_a) * density;
-                d_dens += (d_x + d_a) * s.dt;
-                const f3 grd = {q[4].w, q[5].w, q[6].w};
-                gl[22] = d_se * s.ve.x + d_sx * s.vx.x;
-                gl[23] = d_se * s.ve.y + d_sx * s.vx.y;
-                gl[24] = d_se * s.ve.z + d_sx * s.vx.z;
-                const float d_sum = d_se + d_sx;
-                d_enter += d_se * dot3(grd, d);
-                d_exit += d_sx * dot3(grd, d);
-                gl[12] = -grd.x * d_sum;
-                gl[13] = -grd.y * d_sum;
-                gl[14] = -grd.z * d_sum;
-                if (exit - enter > 0.f) {
-                    d_exit += d_dt;
-                    d_enter -= d_dt;
-                }
-                gl[18] = density > 0.f ? d_dens : 0.f;
-                float d_tx = 0.f;
-                if (tx > enter) d_tx = d_exit; else d_enter += d_exit;
-                const float d_te = te > 0.f ? d_enter : 0.f;
-                // ---- adjoint of the plane intersections t = dot(n, vref - o) / dot(n, d)
-                const float ge = d_te / dene, gx = d_tx / denx;
-                const f3 ae = ie == 3 ? a1 : a0, ax = ix == 3 ? a1 : a0;
-                const f3 dne = {ge * (ae.x - te * d.x), ge * (ae.y - te * d.y), ge * (ae.z - te * d.z)};
-                const f3 dnx = {gx * (ax.x - tx * d.x), gx * (ax.y - tx * d.y), gx * (ax.z - tx * d.z)};
-#pragma unroll
-                for (int p = 0; p < 4; ++p) {
-                    const f3 np = xyz(q[p]);
-                    const float se = (ie == p) ? ge : 0.f, sx = (ix == p) ? gx : 0.f;
-                    gl[3 * p + 0] = (ie == p ? dne.x : 0.f) + (ix == p ? dnx.x : 0.f);
-                    gl[3 * p + 1] = (ie == p ? dne.y : 0.f) + (ix == p ? dnx.y : 0.f);
-                    gl[3 * p + 2] = (ie == p ? dne.z : 0.f) + (ix == p ? dnx.z : 0.f);
-                    const float sref = se + sx;  // gradient of vref = +n * g
-                    if (p == 3) {
-                        gl[15] += np.x * sref;
-                        gl[16] += np.y * sref;
-                        gl[17] += np.z * sref;
-                    } else {
-                        gl[12] += np.x * sref;
-                        gl[13] += np.y * sref;
-                        gl[14] += np.z * sref;
-                    }
-                }
-                dS.logT = d_logT_old;
-                dS.D[2] = nD2;
-                dS.D[3] = nD3;
+                D2 = D2 - density;
+                D3 = D3 - m1;
+                logT = logT_old;
+                float nD2, nD3;
+                dS_logT = hit_grads(q, o, d, is, s, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
+                dS_D[2] = nD2;
+                dS_D[3] = nD3;
             }
             if (__any_sync(kMask, hit)) {
                 using RS = ReduceScatter<kNGrad, WarpShape<NT>::kTopOffset>;
@@ -486,71 +808,435 @@ __global__ void __launch_bounds__(NT) blend_bwd_kernel(
                 RS::template run<kMask>(gl, lane, slot);
 #pragma unroll
                 for (int r = 0; r < RS::R; ++r)
-                    if (slot + r < kNGrad && gl[r] != 0.f) atomicAdd(&sacc[jj][slot + r], gl[r]);
+                    if (slot + r < kNGrad && gl[r] != 0.f) atomicAdd(&S.sacc[jj][slot + r], gl[r]);
             }
         }
         __syncthreads();
-        // ---- flush: per list entry, convert to vertex gradients and add to global memory
-        for (int jj = threadIdx.x; jj < n; jj += NT) {
-            float v[kNGrad];
-            bool any = false;
+        flush_entries<NT, B>(n, S.srec, S.sid, S.sacc, indices, gverts, gcv);
+    }
+}
+
+// Pair backward item: the same strip / thread split as the forward.  Per
+// batch of B entries (walked back to front) the pixels that still have list
+// offsets below their n_contributors are compacted into slots and
+//   A. all warps test the (entry, slot) pairs: a (0: no hit), m1 and
+//      dot(dL/dcolour, rgb);
+//   B. each owner walks its pixel's entries back to front and records, per
+//      hit, T and D2, D3 of the state before the hit and dL/d(log T, D2, D3)
+//      after it (the only state the adjoint reads; colour and D0, D1, D4 need
+//      no undo);
+//   C. all warps compute the 25 per-entry partials of every hit pair (warp =
+//      entry, lanes = slots), sum them over the warp with a reduce-scatter and
+//      add them to the entry's shared accumulator.
+template <int PX, int B>
+struct BwdPairSmem {
+    float4 srec[B][kRecFloat4];
+    int32_t sid[B];
+    float sacc[B][kNGrad];
+    float ray[6][PX];
+    float dc[6][PX];      // dL/dcolour (3), dL/dD0, dL/dD1, dL/dD4: constant along the walk
+    int32_t nc[PX];
+    float resA[3][B][PX];  // a (0: no hit), m1, dot(dL/dcolour, rgb)
+    float resB[6][B][PX];  // T, D2, D3 before the hit; dL/d(log T, D2, D3) after it
+    uint8_t hit_entry[PX][B];  // per slot: the batch entries it hits
+    int32_t hit_pre[PX + 1];   // exclusive prefix of the per-slot hit counts
+    int32_t warp_base[(PX + 31) / 32];
+    int32_t smax[(PX + 31) / 32];
+};
+
+template <int PX, int NT, int B>
+__device__ __forceinline__ void bwd_pair_item(
+    int tile, int sub, const int32_t* __restrict__ ids, const int2* __restrict__ ranges,
+    const float4* __restrict__ recs, const int4* __restrict__ indices, const float2* __restrict__ jitter,
+    const rm_camera& cam, const float4* __restrict__ img, const float* __restrict__ dist,
+    const int32_t* __restrict__ ncs, const float4* __restrict__ gimg, const float* __restrict__ gdist,
+    float* __restrict__ gverts, float* __restrict__ gcv, BwdPairSmem<PX, B>& S) {
+    constexpr unsigned kOwnMask = WarpShape<PX>::kMask;
+    constexpr int kWarps = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool owner = tid < PX;
+    const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
+    const int tp = sub * PX + tid;  // pixel index inside the tile (row-major)
+    const int lx = tp % cam.tile_width;
+    const int ly = tp / cam.tile_width;
+    const int px = tx * cam.tile_width + lx, py = ty * cam.tile_height + ly;
+    const bool inside = owner && px < cam.image_width && py < cam.image_height;
+    const int64_t pix = (int64_t)py * cam.image_width + px;
+    f3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
+    float logT = 0.f, D2 = 0.f, D3 = 0.f;  // state along the reverse walk
+    float dS_c[3] = {0.f, 0.f, 0.f}, dS_logT = 0.f, dS_D[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    int32_t nc = 0;
+    if (inside) {
+        const float2 j = __ldg(jitter + pix);
+        make_ray(cam, px, py, j.x, j.y, o, d);
+        logT = __ldg(img + pix).w;
+        D2 = __ldg(dist + 5 * pix + 2);
+        D3 = __ldg(dist + 5 * pix + 3);
+        const float4 g = __ldg(gimg + pix);
+        dS_c[0] = g.x; dS_c[1] = g.y; dS_c[2] = g.z; dS_logT = g.w;
 #pragma unroll
-            for (int k = 0; k < kNGrad; ++k) {
-                v[k] = sacc[jj][k];
-                any |= v[k] != 0.f;
-            }
-            if (!any) continue;
-            const float4* q = srec[jj];
-            const int g = sid[jj];
-            const f3 P[4] = {xyz(q[4]), xyz(q[5]), xyz(q[6]), xyz(q[7])};
-            const uint32_t flips = __float_as_uint(q[7].w);
-            f3 gv[4] = {{v[12], v[13], v[14]}, {v[15], v[16], v[17]}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-            const int pp[4] = {1, 1, 2, 2}, pq[4] = {0, 0, 0, 1}, pr[4] = {2, 3, 3, 3};
+        for (int k = 0; k < 5; ++k) dS_D[k] = gdist ? __ldg(gdist + 5 * pix + k) : 0.f;
+        nc = __ldg(ncs + pix);
+    }
+    if (owner) {
+        int32_t m = nc;
 #pragma unroll
-            for (int p = 0; p < 4; ++p) {
-                f3 gc = {v[3 * p], v[3 * p + 1], v[3 * p + 2]};
-                if (flips & (1u << p)) gc = neg3(gc);
-                const f3 ea = P[pp[p]] - P[pq[p]], eb = P[pr[p]] - P[pq[p]];
-                const f3 ga = cross3(eb, gc), gb = cross3(gc, ea);
-                gv[pp[p]] = gv[pp[p]] + ga;
-                gv[pr[p]] = gv[pr[p]] + gb;
-                gv[pq[p]] = gv[pq[p]] - (ga + gb);
-            }
-            const int4 id = __ldg(indices + g);
-            const int vid[4] = {id.x, id.y, id.z, id.w};
+        for (int off = WarpShape<PX>::kTopOffset; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(kOwnMask, m, off));
+        if (lane == 0) S.smax[warp] = m;
+    }
+    __syncthreads();
+    int32_t tile_max = 0;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                float* dst = gverts + 3 * (int64_t)vid[i];
-                if (gv[i].x != 0.f) atomicAdd(dst, gv[i].x);
-                if (gv[i].y != 0.f) atomicAdd(dst + 1, gv[i].y);
-                if (gv[i].z != 0.f) atomicAdd(dst + 2, gv[i].z);
-            }
-            float* dc = gcv + 7 * (int64_t)g;
-#pragma unroll
-            for (int k = 0; k < 7; ++k)
-                if (v[18 + k] != 0.f) atomicAdd(dc + k, v[18 + k]);
+    for (int w = 0; w < (PX + 31) / 32; ++w) tile_max = max(tile_max, S.smax[w]);
+    const int2 rg = __ldg(ranges + tile);
+    const int end = min(rg.y, rg.x + tile_max);
+    for (int top = end; top > rg.x; top -= B) {
+        const int lo = max(rg.x, top - B);
+        const int n = top - lo;
+        // pixels with list offsets below n_contributors in this batch
+        const bool walking = inside && (lo - rg.x) < nc;
+        __syncthreads();  // the previous batch's flush has read sid / srec / sacc
+        for (int k = tid; k < n; k += NT) S.sid[k] = __ldg(ids + lo + k);
+        for (int k = tid; k < n * kNGrad; k += NT) (&S.sacc[0][0])[k] = 0.f;
+        int slot = 0;
+        if (owner) {
+            const unsigned bal = __ballot_sync(kOwnMask, walking);
+            if (lane == 0) S.warp_base[warp] = __popc(bal);
+            slot = __popc(bal & ((1u << lane) - 1u));
         }
+        __syncthreads();
+        for (int k = tid; k < n * kRecFloat4; k += NT) {
+            const int j = k >> 3, c = k & 7;
+            S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
+        }
+        int k_act = 0;
+#pragma unroll
+        for (int w = 0; w < (PX + 31) / 32; ++w) k_act += S.warp_base[w];
+        if (walking) {
+            for (int w = 0; w < warp; ++w) slot += S.warp_base[w];
+            S.ray[0][slot] = o.x; S.ray[1][slot] = o.y; S.ray[2][slot] = o.z;
+            S.ray[3][slot] = d.x; S.ray[4][slot] = d.y; S.ray[5][slot] = d.z;
+            S.dc[0][slot] = dS_c[0]; S.dc[1][slot] = dS_c[1]; S.dc[2][slot] = dS_c[2];
+            S.dc[3][slot] = dS_D[0]; S.dc[4][slot] = dS_D[1]; S.dc[5][slot] = dS_D[4];
+            S.nc[slot] = nc;
+        }
+        __syncthreads();
+        // A: hit test of every (entry, slot) pair
+        for (int j = warp; j < n; j += kWarps) {
+            const float4* q = S.srec[j];
+            const float density = q[0].w;
+            for (int sl = lane; sl < k_act; sl += 32) {
+                float ra = 0.f, rm1 = 0.f, rdt = 0.f;
+                if (lo + j - rg.x < S.nc[sl]) {
+                    const f3 ro = {S.ray[0][sl], S.ray[1][sl], S.ray[2][sl]};
+                    const f3 rd = {S.ray[3][sl], S.ray[4][sl], S.ray[5][sl]};
+                    const Isect is = intersect<false>(q, ro, rd);
+                    Segment s;
+                    s.dt = fmaxf(is.exit - is.enter, 0.f);
+                    s.a = density * s.dt;
+                    if (is.geo && s.a > 0.f) {
+                        integrate(q, ro, rd, is.enter, is.exit, s);
+                        ra = s.a;
+                        rm1 = density * (is.exit + is.enter) / 2.0f;
+                        rdt = fmaf(S.dc[2][sl], s.rgb[2], fmaf(S.dc[1][sl], s.rgb[1], S.dc[0][sl] * s.rgb[0]));
+                    }
+                }
+                S.resA[0][j][sl] = ra;
+                S.resA[1][j][sl] = rm1;
+                S.resA[2][j][sl] = rdt;
+            }
+        }
+        __syncthreads();
+        // B: each owner walks its chains back to front and lists its hits
+        if (walking) {
+            int cnt = 0;
+            for (int j = n - 1; j >= 0; --j) {
+                const float a = S.resA[0][j][slot];
+                if (!(a > 0.f)) continue;
+                S.hit_entry[slot][cnt++] = (uint8_t)j;
+                const float density = S.srec[j][0].w;
+                const float m1 = S.resA[1][j][slot];
+                const float logT_old = logT + a;
+                const float T = __expf(logT_old);
+                D2 = D2 - density;
+                D3 = D3 - m1;
+                logT = logT_old;
+                S.resB[0][j][slot] = T;
+                S.resB[1][j][slot] = D2;
+                S.resB[2][j][slot] = D3;
+                S.resB[3][j][slot] = dS_logT;
+                S.resB[4][j][slot] = dS_D[2];
+                S.resB[5][j][slot] = dS_D[3];
+                dS_logT = dS_logT + S.resA[2][j][slot] * T;
+                dS_D[2] = dS_D[2] + dS_D[0] * 2.0f * m1;
+                dS_D[3] = dS_D[3] + dS_D[1] * 2.0f * density;
+            }
+            S.hit_pre[slot + 1] = cnt;
+        }
+        __syncthreads();
+        // exclusive prefix of the hit counts over the k_act slots
+        if (warp == 0) {
+            int carry = 0;
+            for (int s0 = 0; s0 < k_act; s0 += 32) {
+                const int v = (s0 + lane < k_act) ? S.hit_pre[s0 + lane + 1] : 0;
+                int inc = v;
+#pragma unroll
+                for (int o2 = 1; o2 < 32; o2 <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, inc, o2);
+                    if (lane >= o2) inc += y;
+                }
+                if (s0 + lane < k_act) S.hit_pre[s0 + lane + 1] = carry + inc;
+                carry += __shfl_sync(0xffffffffu, inc, 31);
+            }
+            if (lane == 0) S.hit_pre[0] = 0;
+        }
+        __syncthreads();
+        // C: adjoint of every hit, one hit per thread (the hits are packed, so
+        // all lanes do useful work); consecutive hits belong to one slot and
+        // hit different entries, so the per-entry shared accumulators see no
+        // address conflicts inside a warp
+        const int n_hits = S.hit_pre[k_act];
+        for (int h = tid; h < n_hits; h += NT) {
+            int lo_s = 0, hi_s = k_act - 1;
+            while (lo_s < hi_s) {  // last slot with hit_pre[slot] <= h
+                const int mid = (lo_s + hi_s + 1) >> 1;
+                if (S.hit_pre[mid] <= h) lo_s = mid; else hi_s = mid - 1;
+            }
+            const int sl = lo_s;
+            const int j = S.hit_entry[sl][h - S.hit_pre[sl]];
+            const float4* q = S.srec[j];
+            const f3 ro = {S.ray[0][sl], S.ray[1][sl], S.ray[2][sl]};
+            const f3 rd = {S.ray[3][sl], S.ray[4][sl], S.ray[5][sl]};
+            const Isect is = intersect<true>(q, ro, rd);
+            Segment sg;
+            sg.dt = fmaxf(is.exit - is.enter, 0.f);
+            sg.a = q[0].w * sg.dt;
+            integrate(q, ro, rd, is.enter, is.exit, sg);
+            const float dsc[3] = {S.dc[0][sl], S.dc[1][sl], S.dc[2][sl]};
+            const float dsd[5] = {S.dc[3][sl], S.dc[4][sl], S.resB[4][j][sl], S.resB[5][j][sl], S.dc[5][sl]};
+            float gl[kNGrad];
+            float nD2, nD3;
+            hit_grads(q, ro, rd, is, sg, S.resB[0][j][sl], S.resB[1][j][sl], S.resB[2][j][sl], dsc, S.resB[3][j][sl],
+                      dsd, gl, nD2, nD3);
+#pragma unroll
+            for (int k = 0; k < kNGrad; ++k)
+                if (gl[k] != 0.f) atomicAdd(&S.sacc[j][k], gl[k]);
+        }
+        __syncthreads();
+        flush_entries<NT, B>(n, S.srec, S.sid, S.sacc, indices, gverts, gcv);
     }
 }
 
 template <int NT, int B>
-int launch_fwd(const int32_t* ids, const int32_t* ranges, const float4* recs, const float* jitter,
-               const rm_camera& cam, float* img, float* dist, int32_t* nc, cudaStream_t s) {
-    const int G = cam.grid_width * cam.grid_height;
-    blend_fwd_kernel<NT, B><<<G, NT, 0, s>>>(ids, (const int2*)ranges, recs, (const float2*)jitter, cam,
-                                             (float4*)img, dist, nc);
-    return rm_host::check_launch("rm_blend_fwd");
+__global__ void __launch_bounds__(NT, (NT >= 64 ? 512 / NT : 16)) blend_bwd_dense_kernel(
+    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
+    const int4* __restrict__ indices, const float2* __restrict__ jitter, const rm_camera cam,
+    const float4* __restrict__ img, const float* __restrict__ dist, const int32_t* __restrict__ ncs,
+    const float4* __restrict__ gimg, const float* __restrict__ gdist, float* __restrict__ gverts,
+    float* __restrict__ gcv, const Queue q) {
+    __shared__ BwdDenseSmem<NT, B> S;
+    __shared__ int s_item;
+    const int n_items = queue_items(q);
+    for (;;) {
+        const int item = next_item(q, &s_item);
+        if (item >= n_items) return;
+        bwd_dense_item<NT, B>(queue_tile(q, item), item % q.subs, ids, ranges, recs, indices, jitter, cam, img,
+                              dist, ncs, gimg, gdist, gverts, gcv, S);
+    }
 }
 
-template <int NT, int B>
-int launch_bwd(const int32_t* ids, const int32_t* ranges, const float4* recs, const int32_t* indices,
-               const float* jitter, const rm_camera& cam, const float* img, const float* dist, const int32_t* nc,
-               const float* gimg, const float* gdist, float* gverts, float* gcv, cudaStream_t s) {
+template <int PX, int NT, int B>
+__global__ void __launch_bounds__(NT, 512 / NT) blend_bwd_pair_kernel(
+    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
+    const int4* __restrict__ indices, const float2* __restrict__ jitter, const rm_camera cam,
+    const float4* __restrict__ img, const float* __restrict__ dist, const int32_t* __restrict__ ncs,
+    const float4* __restrict__ gimg, const float* __restrict__ gdist, float* __restrict__ gverts,
+    float* __restrict__ gcv, const Queue q) {
+    extern __shared__ __align__(16) unsigned char bwd_smem_raw[];
+    BwdPairSmem<PX, B>& S = *reinterpret_cast<BwdPairSmem<PX, B>*>(bwd_smem_raw);
+    __shared__ int s_item;
+    const int n_items = queue_items(q);
+    for (;;) {
+        const int item = next_item(q, &s_item);
+        if (item >= n_items) return;
+        bwd_pair_item<PX, NT, B>(queue_tile(q, item), item % q.subs, ids, ranges, recs, indices, jitter, cam, img,
+                                 dist, ncs, gimg, gdist, gverts, gcv, S);
+    }
+}
+
+struct BlendWs {
+    float4* recs;
+    int32_t* order;
+    int32_t* info;
+    uint32_t* tickets;
+};
+
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+size_t blend_ws_bytes(int64_t n_tets, int64_t n_tiles) {
+    const size_t rec = align256((size_t)(n_tets > 0 ? n_tets : 1) * kRecFloat4 * sizeof(float4));
+    const size_t ord = align256((size_t)(n_tiles > 0 ? n_tiles : 1) * sizeof(int32_t));
+    return rec + ord + 256;
+}
+
+BlendWs blend_ws(void* base, int64_t n_tets, int64_t n_tiles) {
+    char* p = (char*)base;
+    const size_t rec = align256((size_t)(n_tets > 0 ? n_tets : 1) * kRecFloat4 * sizeof(float4));
+    const size_t ord = align256((size_t)(n_tiles > 0 ? n_tiles : 1) * sizeof(int32_t));
+    return {(float4*)p, (int32_t*)(p + rec), (int32_t*)(p + rec + ord), (uint32_t*)(p + rec + ord + 64)};
+}
+
+// Persistent grid: as many CTAs as fit on the device at once (cached per
+// kernel instantiation and device).
+template <typename K>
+int persistent_grid(K kernel, int threads, int smem, int n_items) {
+    static thread_local int cached_dev = -1, cached_blocks = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != cached_dev) {
+        int sms = 0, per_sm = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+        cached_blocks = sms * (per_sm > 0 ? per_sm : 1);
+        cached_dev = dev;
+    }
+    return n_items < cached_blocks ? n_items : cached_blocks;
+}
+
+int sm_count() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 1;
+}
+
+// The pair kernel of a pass runs on a per-device side stream, forked from and
+// joined back into the caller's stream with events (capturable in a CUDA graph).
+struct SideStream {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+std::mutex g_side_mu;
+SideStream g_side[64];
+
+int side_stream(SideStream** out) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return rm_host::fail(RM_ECUDA, "rm_blend: device ordinal %d", dev);
+    SideStream& s = g_side[dev];
+    if (!s.stream) {
+        if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming) != cudaSuccess)
+            return rm_host::fail(RM_ECUDA, "rm_blend: side stream: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    *out = &s;
+    return RM_OK;
+}
+
+int launch_order(const int32_t* ranges, int G, const BlendWs& w, int heavy_shift, cudaStream_t s) {
+    order_kernel<<<1, 1024, 0, s>>>((const int2*)ranges, G, w.order, w.info, w.tickets, heavy_shift);
+    return rm_host::check_launch("rm_blend order");
+}
+
+int fork_side(cudaStream_t s, SideStream* side) {
+    if (cudaEventRecord(side->fork, s) != cudaSuccess || cudaStreamWaitEvent(side->stream, side->fork, 0) != cudaSuccess)
+        return rm_host::fail(RM_ECUDA, "rm_blend: fork: %s", cudaGetErrorString(cudaGetLastError()));
+    return RM_OK;
+}
+
+int join_side(cudaStream_t s, SideStream* side) {
+    if (cudaEventRecord(side->join, side->stream) != cudaSuccess || cudaStreamWaitEvent(s, side->join, 0) != cudaSuccess)
+        return rm_host::fail(RM_ECUDA, "rm_blend: join: %s", cudaGetErrorString(cudaGetLastError()));
+    return RM_OK;
+}
+
+// Launch tunables carried in the flags word (include/rm_capi.h).
+struct Tuning {
+    int heavy_shift;       // heavy tiles: list-length bucket >= bucket(mean) + heavy_shift
+    int pair_ctas_per_sm;  // resident CTAs of the pair kernel per SM
+};
+
+Tuning tuning_from_flags(int flags, int def_shift, int def_ctas) {
+    Tuning t;
+    const int hs = (flags >> RM_BLEND_HEAVY_SHIFT) & 0xf;
+    const int pc = (flags >> RM_BLEND_PAIR_CTAS_SHIFT) & 0xf;
+    t.heavy_shift = hs ? hs : def_shift;
+    t.pair_ctas_per_sm = pc ? pc : def_ctas;
+    return t;
+}
+
+// Forward pass: order kernel, then the pair kernel (heavy tiles, side stream)
+// and the dense kernel (other tiles, caller's stream) concurrently; the side
+// stream is joined back after both launches.
+template <int PX, int B_DENSE, int PX_PAIR, int NT_PAIR, int B_PAIR>
+int launch_fwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, const float* jitter,
+               const rm_camera& cam, float* img, float* dist, int32_t* nc, const Tuning& tn, cudaStream_t s) {
     const int G = cam.grid_width * cam.grid_height;
-    blend_bwd_kernel<NT, B><<<G, NT, 0, s>>>(ids, (const int2*)ranges, recs, (const int4*)indices,
-                                             (const float2*)jitter, cam, (const float4*)img, dist, nc,
-                                             (const float4*)gimg, gdist, gverts, gcv);
-    return rm_host::check_launch("rm_blend_bwd");
+    int rc = launch_order(ranges, G, w, tn.heavy_shift, s);
+    if (rc) return rc;
+    const int subs = cam.tile_width * cam.tile_height / PX;
+    const int subs_pair = cam.tile_width * cam.tile_height / PX_PAIR;
+    const Queue qd = {w.order, w.info, w.tickets + 0, G, subs, false};
+    const Queue qp = {w.order, w.info, w.tickets + 1, G, subs_pair, true};
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    SideStream* side = nullptr;
+    if ((rc = side_stream(&side)) || (rc = fork_side(s, side))) return rc;
+    const int smem = (int)sizeof(FwdPairSmem<PX_PAIR, B_PAIR>);
+    cudaFuncSetAttribute(blend_fwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int pair_cap = tn.pair_ctas_per_sm * sm_count();
+    const int pair_grid = G * subs_pair < pair_cap ? G * subs_pair : pair_cap;
+    blend_fwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR><<<pair_grid, NT_PAIR, smem, side->stream>>>(
+        ids, (const int2*)ranges, w.recs, (const float2*)jitter, cam, (float4*)img, dist, nc, qp);
+    if ((rc = rm_host::check_launch("rm_blend_fwd (pair)"))) return rc;
+    const int grid = persistent_grid(blend_fwd_dense_kernel<PX, B_DENSE>, PX, 0, G * subs);
+    blend_fwd_dense_kernel<PX, B_DENSE><<<grid, PX, 0, s>>>(ids, (const int2*)ranges, w.recs,
+                                                            (const float2*)jitter, cam, (float4*)img, dist, nc, qd);
+    if ((rc = rm_host::check_launch("rm_blend_fwd (dense)"))) return rc;
+    return join_side(s, side);
+}
+
+template <int PX, int B_DENSE, int PX_PAIR, int NT_PAIR, int B_PAIR>
+int launch_bwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, const int32_t* indices,
+               const float* jitter, const rm_camera& cam, const float* img, const float* dist, const int32_t* nc,
+               const float* gimg, const float* gdist, float* gverts, float* gcv, const Tuning& tn, cudaStream_t s) {
+    const int G = cam.grid_width * cam.grid_height;
+    int rc = launch_order(ranges, G, w, tn.heavy_shift, s);
+    if (rc) return rc;
+    const int subs = cam.tile_width * cam.tile_height / PX;
+    const int subs_pair = cam.tile_width * cam.tile_height / PX_PAIR;
+    const Queue qd = {w.order, w.info, w.tickets + 2, G, subs, false};
+    const Queue qp = {w.order, w.info, w.tickets + 3, G, subs_pair, true};
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    SideStream* side = nullptr;
+    if ((rc = side_stream(&side)) || (rc = fork_side(s, side))) return rc;
+    const int smem = (int)sizeof(BwdPairSmem<PX_PAIR, B_PAIR>);
+    cudaFuncSetAttribute(blend_bwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int pair_cap = tn.pair_ctas_per_sm * sm_count();
+    const int pair_grid = G * subs_pair < pair_cap ? G * subs_pair : pair_cap;
+    blend_bwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR><<<pair_grid, NT_PAIR, smem, side->stream>>>(
+        ids, (const int2*)ranges, w.recs, (const int4*)indices, (const float2*)jitter, cam, (const float4*)img, dist,
+        nc, (const float4*)gimg, gdist, gverts, gcv, qp);
+    if ((rc = rm_host::check_launch("rm_blend_bwd (pair)"))) return rc;
+    const int grid = persistent_grid(blend_bwd_dense_kernel<PX, B_DENSE>, PX, 0, G * subs);
+    blend_bwd_dense_kernel<PX, B_DENSE><<<grid, PX, 0, s>>>(ids, (const int2*)ranges, w.recs, (const int4*)indices,
+                                                            (const float2*)jitter, cam, (const float4*)img, dist, nc,
+                                                            (const float4*)gimg, gdist, gverts, gcv, qd);
+    if ((rc = rm_host::check_launch("rm_blend_bwd (dense)"))) return rc;
+    return join_side(s, side);
+}
+
+// Strip of pixels handled by one CTA: flags may request 2^k pixels
+// (RM_BLEND_STRIP_SHIFT); default 64.  Must divide the tile and be a multiple
+// of the tile width.
+int strip_pixels(const rm_camera* cam, int flags) {
+    const int tile_px = cam->tile_width * cam->tile_height;
+    const int req = (flags >> RM_BLEND_STRIP_SHIFT) & 0xff;
+    int strip = req ? (1 << req) : 64;
+    if (tile_px < strip) strip = tile_px;
+    return strip;
 }
 
 int pack(const int32_t* indices, const float* vertices, const float* cv, int64_t n_tets, const int32_t* tiles,
@@ -562,7 +1248,7 @@ int pack(const int32_t* indices, const float* vertices, const float* cv, int64_t
 }
 
 int check_blend_args(const char* who, const int32_t* indices, const float* vertices, const float* cv, int64_t n_tets,
-                     const float* jitter, const rm_camera* cam, void* workspace, size_t workspace_bytes) {
+                     const float* jitter, const rm_camera* cam, void* workspace, size_t workspace_bytes, int flags) {
     int rc = rm_host::check_cam(cam);
     if (rc) return rc;
     if (n_tets < 0) return rm_host::fail(RM_EINVAL, "%s: negative size", who);
@@ -570,12 +1256,17 @@ int check_blend_args(const char* who, const int32_t* indices, const float* verti
         return rm_host::fail(RM_EINVAL, "%s: NULL pointer", who);
     if ((uintptr_t)indices & 15) return rm_host::fail(RM_EINVAL, "%s: indices must be 16-byte aligned", who);
     if ((uintptr_t)workspace & 15) return rm_host::fail(RM_EINVAL, "%s: workspace must be 16-byte aligned", who);
-    if (workspace_bytes < (size_t)n_tets * kRecFloat4 * sizeof(float4))
+    const int64_t G = (int64_t)cam->grid_width * cam->grid_height;
+    if (workspace_bytes < blend_ws_bytes(n_tets, G))
         return rm_host::fail(RM_EINVAL, "%s: workspace %zu < %zu bytes", who, workspace_bytes,
-                             (size_t)n_tets * kRecFloat4 * sizeof(float4));
+                             blend_ws_bytes(n_tets, G));
     const int nt = cam->tile_width * cam->tile_height;
     if (nt != 16 && nt != 64 && nt != 256 && nt != 1024)
         return rm_host::fail(RM_EINVAL, "%s: tile of %d pixels unsupported (16, 64, 256 or 1024)", who, nt);
+    const int strip = strip_pixels(cam, flags);
+    if ((strip != 16 && strip != 64) || nt % strip)
+        return rm_host::fail(RM_EINVAL, "%s: strip of %d pixels does not fit a %dx%d tile", who, strip,
+                             cam->tile_width, cam->tile_height);
     return RM_OK;
 }
 
@@ -584,9 +1275,7 @@ int check_blend_args(const char* who, const int32_t* indices, const float* verti
 
 extern "C" {
 
-size_t rm_blend_workspace_size(int64_t n_tets) {
-    return (size_t)(n_tets > 0 ? n_tets : 1) * rm::kRecFloat4 * sizeof(float4);
-}
+size_t rm_blend_workspace_size(int64_t n_tets, int64_t n_tiles) { return rm::blend_ws_bytes(n_tets, n_tiles); }
 
 int rm_blend_fwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices, const float* vertices,
                  const float* cell_values, int64_t n_tets, int64_t n_verts, const int32_t* tiles_touched,
@@ -594,24 +1283,23 @@ int rm_blend_fwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t
                  int32_t* n_contrib, void* workspace, size_t workspace_bytes, int flags, void* stream) {
     using namespace rm;
     int rc = check_blend_args("rm_blend_fwd", indices, vertices, cell_values, n_tets, ray_jitter, cam, workspace,
-                              workspace_bytes);
+                              workspace_bytes, flags);
     if (rc) return rc;
     if (!ranges || !out_img || !out_distortion || !n_contrib)
         return rm_host::fail(RM_EINVAL, "rm_blend_fwd: NULL pointer");
     if (((uintptr_t)out_img & 15) || ((uintptr_t)ranges & 7) || ((uintptr_t)ray_jitter & 7))
         return rm_host::fail(RM_EINVAL, "rm_blend_fwd: misaligned image / ranges / jitter");
     cudaStream_t s = (cudaStream_t)stream;
-    float4* recs = (float4*)workspace;
+    const BlendWs w = blend_ws(workspace, n_tets, (int64_t)cam->grid_width * cam->grid_height);
     if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
-        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, recs, s);
+        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
         if (rc) return rc;
     }
-    const int nt = cam->tile_width * cam->tile_height;
-    switch (nt) {
-        case 16: return launch_fwd<16, 64>(sorted_ids, ranges, recs, ray_jitter, *cam, out_img, out_distortion, n_contrib, s);
-        case 64: return launch_fwd<64, 64>(sorted_ids, ranges, recs, ray_jitter, *cam, out_img, out_distortion, n_contrib, s);
-        case 256: return launch_fwd<256, 64>(sorted_ids, ranges, recs, ray_jitter, *cam, out_img, out_distortion, n_contrib, s);
-        default: return launch_fwd<1024, 64>(sorted_ids, ranges, recs, ray_jitter, *cam, out_img, out_distortion, n_contrib, s);
+    // measured on the 1.3M-tet workload: every tile through the pair kernel, 3 CTAs/SM
+    const Tuning tn = tuning_from_flags(flags, 1, 3);
+    switch (strip_pixels(cam, flags)) {
+        case 16: return launch_fwd<16, 64, 16, 64, 32>(sorted_ids, ranges, w, ray_jitter, *cam, out_img, out_distortion, n_contrib, tn, s);
+        default: return launch_fwd<64, 64, 64, 256, 32>(sorted_ids, ranges, w, ray_jitter, *cam, out_img, out_distortion, n_contrib, tn, s);
     }
 }
 
@@ -622,7 +1310,7 @@ int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t
                  float* grad_cell_values, void* workspace, size_t workspace_bytes, int flags, void* stream) {
     using namespace rm;
     int rc = check_blend_args("rm_blend_bwd", indices, vertices, cell_values, n_tets, ray_jitter, cam, workspace,
-                              workspace_bytes);
+                              workspace_bytes, flags);
     if (rc) return rc;
     if (!ranges || !out_img || !out_distortion || !n_contrib || !grad_img || !grad_vertices || !grad_cell_values)
         return rm_host::fail(RM_EINVAL, "rm_blend_bwd: NULL pointer");
@@ -630,17 +1318,16 @@ int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t
         ((uintptr_t)ray_jitter & 7))
         return rm_host::fail(RM_EINVAL, "rm_blend_bwd: misaligned image / grad / ranges / jitter");
     cudaStream_t s = (cudaStream_t)stream;
-    float4* recs = (float4*)workspace;
+    const BlendWs w = blend_ws(workspace, n_tets, (int64_t)cam->grid_width * cam->grid_height);
     if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
-        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, recs, s);
+        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
         if (rc) return rc;
     }
-    const int nt = cam->tile_width * cam->tile_height;
-    switch (nt) {
-        case 16: return launch_bwd<16, 32>(sorted_ids, ranges, recs, indices, ray_jitter, *cam, out_img, out_distortion, n_contrib, grad_img, grad_distortion, grad_vertices, grad_cell_values, s);
-        case 64: return launch_bwd<64, 64>(sorted_ids, ranges, recs, indices, ray_jitter, *cam, out_img, out_distortion, n_contrib, grad_img, grad_distortion, grad_vertices, grad_cell_values, s);
-        case 256: return launch_bwd<256, 64>(sorted_ids, ranges, recs, indices, ray_jitter, *cam, out_img, out_distortion, n_contrib, grad_img, grad_distortion, grad_vertices, grad_cell_values, s);
-        default: return launch_bwd<1024, 64>(sorted_ids, ranges, recs, indices, ray_jitter, *cam, out_img, out_distortion, n_contrib, grad_img, grad_distortion, grad_vertices, grad_cell_values, s);
+    // measured: the one-thread-per-pixel backward alone is fastest
+    const Tuning tn = tuning_from_flags(flags, 15, 1);
+    switch (strip_pixels(cam, flags)) {
+        case 16: return launch_bwd<16, 32, 16, 64, 16>(sorted_ids, ranges, w, indices, ray_jitter, *cam, out_img, out_distortion, n_contrib, grad_img, grad_distortion, grad_vertices, grad_cell_values, tn, s);
+        default: return launch_bwd<64, 32, 64, 256, 16>(sorted_ids, ranges, w, indices, ray_jitter, *cam, out_img, out_distortion, n_contrib, grad_img, grad_distortion, grad_vertices, grad_cell_values, tn, s);
     }
 }
 

@@ -205,6 +205,20 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
     return TileLists(sv, ranges, P)
 
 
+_BLEND_FLAGS = {"fwd": 0, "bwd": 0}
+
+
+def set_blend_tuning(fwd_flags: int = 0, bwd_flags: int = 0) -> None:
+    """Launch tunables (RM_BLEND_STRIP / HEAVY / PAIR_CTAS bits of the flags
+    word) used by blend_fwd / blend_bwd; 0 selects the built-in defaults."""
+    _BLEND_FLAGS["fwd"] = int(fwd_flags)
+    _BLEND_FLAGS["bwd"] = int(bwd_flags)
+
+
+def blend_tuning() -> tuple[int, int]:
+    return _BLEND_FLAGS["fwd"], _BLEND_FLAGS["bwd"]
+
+
 def blend_fwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, cam: RMCamera,
               tiles_touched=None, records: torch.Tensor | None = None, reuse_records: bool = False):
     _require_cuda(sorted_ids=sorted_ids, ranges=ranges, indices=indices, vertices=vertices,
@@ -217,13 +231,13 @@ def blend_fwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, ca
     dev = vertices.device
     T = indices.shape[0]
     L = C.lib()
-    ws_n = L.rm_blend_workspace_size(T)
+    ws_n = L.rm_blend_workspace_size(T, cam.grid_width * cam.grid_height)
     if records is None:
         records = torch.empty(ws_n, dtype=torch.uint8, device=dev)
     img = torch.empty((H, W, 4), dtype=torch.float32, device=dev)
     dist = torch.empty((H, W, 5), dtype=torch.float32, device=dev)
     nc = torch.empty((H, W, 1), dtype=torch.int32, device=dev)
-    flags = C.RM_BLEND_REUSE_RECORDS if reuse_records else 0
+    flags = (C.RM_BLEND_REUSE_RECORDS if reuse_records else 0) | _BLEND_FLAGS["fwd"]
     _call("rm_blend_fwd", lambda: L.rm_blend_fwd(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(indices), C.ptr(vertices), C.ptr(cell_values),
                            T, vertices.shape[0], C.ptr(tiles_touched), C.ptr(ray_jitter), ctypes.byref(cam),
                            C.ptr(img), C.ptr(dist), C.ptr(nc), C.ptr(records), records.numel(), flags, _stream()))
@@ -246,7 +260,7 @@ def blend_bwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, ca
     if grad_cell_values is None:
         grad_cell_values = torch.zeros_like(cell_values)
     T = indices.shape[0]
-    flags = C.RM_BLEND_REUSE_RECORDS if reuse_records else 0
+    flags = (C.RM_BLEND_REUSE_RECORDS if reuse_records else 0) | _BLEND_FLAGS["bwd"]
     _call("rm_blend_bwd", lambda: C.lib().rm_blend_bwd(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(indices), C.ptr(vertices),
                                  C.ptr(cell_values), T, vertices.shape[0], C.ptr(tiles_touched), C.ptr(ray_jitter),
                                  ctypes.byref(cam), C.ptr(img), C.ptr(dist), C.ptr(nc), C.ptr(grad_img), C.ptr(gd),

@@ -37,7 +37,7 @@ def test_struct_layout():
 def test_size_queries():
     L = C.lib()
     assert L.rm_abi_version() == 1
-    assert L.rm_blend_workspace_size(1000) == 1000 * 128
+    assert L.rm_blend_workspace_size(1000, 300) >= 1000 * 128 + 300 * 4
     assert L.rm_scan_workspace_size(5000) >= 16 + 8 * 2
     assert L.rm_sort_workspace_size(1_000_000) > 12 * 1_000_000
 
@@ -71,7 +71,7 @@ def test_rejects_null_and_misaligned():
     cam.tile_height = 5
     cam.grid_width = 26
     cam.grid_height = 26
-    rc = L.rm_blend_fwd(None, 16, 16, 16, 16, 10, 10, None, 16, ctypes.byref(cam), 16, 16, 16, 256, 10 * 128, 0,
+    rc = L.rm_blend_fwd(None, 16, 16, 16, 16, 10, 10, None, 16, ctypes.byref(cam), 16, 16, 16, 256, 1 << 20, 0,
                         None)
     assert rc == C.RM_EINVAL and "tile" in C.last_error()
 

@@ -149,3 +149,25 @@ def test_project_backward(cuda):
     ref = O.project_bwd(mesh.indices, mesh.vertices, cam, tiles.cpu().numpy(), gvs, gcc)
     rel = np.linalg.norm(gv - ref) / np.linalg.norm(ref)
     assert rel <= 1e-5, rel
+
+
+@pytest.mark.parametrize("route", ["all_dense", "all_pair"])
+@pytest.mark.parametrize("tile", [4, 16])
+def test_backward_each_kernel_path(cuda, route, tile):
+    """Every tile through the one-thread-per-pixel backward, or every tile
+    through the pair-parallel backward (packed hits)."""
+    from radiance_meshes_b200 import _capi as C
+
+    shift = 15 if route == "all_dense" else 1
+    flags = (shift << C.RM_BLEND_HEAVY_SHIFT) | (2 << C.RM_BLEND_PAIR_CTAS_SHIFT)
+    old = R.blend_tuning()
+    R.set_blend_tuning(flags, flags)
+    try:
+        mesh, view = scenes.workload_gradient_check(tile)
+        jitter = np.random.default_rng(tile + 7).uniform(0, 1, (view.height, view.width, 2)).astype(np.float32)
+        _run(mesh.vertices, mesh.indices, mesh.cell_values, view.tcam(tile_size=tile), jitter, "linear",
+             seed=tile, check_f64=False)
+        _run(mesh.vertices, mesh.indices, mesh.cell_values, view.tcam(tile_size=tile), jitter, "linear_nodist",
+             seed=tile)
+    finally:
+        R.set_blend_tuning(*old)
