@@ -127,6 +127,23 @@ RM_API int rm_scan_tiles(const int32_t* tiles_touched, int64_t n_tets, int32_t* 
                   void* stream);
 
 /*
+ * rm_scan_tiles without a workspace argument: no counterpart in the reference.
+ * For callers that cannot allocate device memory (for example a host runtime
+ * that passes the library only its inputs and outputs and has no device
+ * allocator of its own).  The look-back scratch is a fixed array inside the
+ * library (about 128 KiB per GPU, held until the process exits), so at most
+ * 2^26 tets are accepted; larger inputs return RM_EINVAL.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) and caches
+ * it; make that first call before any stream capture.  All calls share the one
+ * array: calls whose kernels overlap on the GPU (different streams, or
+ * different host threads without ordering between them) race and must not be
+ * issued.  The call allocates nothing (no cudaMalloc, no allocating library
+ * routine); it clears the part of the array that must start at zero itself.
+ */
+RM_API int rm_scan_tiles_noalloc(const int32_t* tiles_touched, int64_t n_tets, int32_t* offsets,
+                                 int64_t* total_dev, void* stream);
+
+/*
  * Tile/tet pair emission: key = (tile_id << 32) | sortable(depth), value = tet
  * id, rows in row-major rectangle order at the tet's exclusive offset.
  * Replaces generate_keys (delaunay_rasterization/internal/slang/tile_shader.slang:138-186)

@@ -50,6 +50,7 @@ SIGNATURES = {
     "rm_project_bwd": (ctypes.c_int, [vp, vp, i64, i64, camp, vp, vp, vp, vp, vp]),
     "rm_scan_workspace_size": (sz, [i64]),
     "rm_scan_tiles": (ctypes.c_int, [vp, i64, vp, vp, vp, sz, vp]),
+    "rm_scan_tiles_noalloc": (ctypes.c_int, [vp, i64, vp, vp, vp]),
     "rm_emit_pairs": (ctypes.c_int, [vp, vp, vp, i64, i32, i64, vp, vp, vp, vp, vp]),
     "rm_sort_workspace_size": (sz, [i64]),
     "rm_sort_pairs": (ctypes.c_int, [vp, vp, i64, vp, ctypes.c_int, vp, vp, vp, sz, vp]),

@@ -5,6 +5,8 @@
 //                   as a single-pass block scan with decoupled look-back
 //   rm_emit_pairs   generate_keys (tile_shader.slang:138-186)
 //   rm_tile_ranges  compute_tile_ranges (tile_shader.slang:188-214)
+#include <mutex>
+
 #include "rm_internal.cuh"
 
 namespace rm {
@@ -242,6 +244,66 @@ int rm_tile_ranges(const int64_t* sorted_keys, int64_t n, const int64_t* n_dev, 
     const int64_t blocks = (n + threads - 1) / threads;
     rm::ranges_kernel<<<(unsigned)blocks, threads, 0, s>>>(sorted_keys, n, n_dev, ranges, n_tiles);
     return rm_host::check_launch("rm_tile_ranges");
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ no allocation --
+// A variant of rm_scan_tiles for callers that cannot allocate device memory
+// themselves, such as a host runtime that hands the library only its inputs
+// and outputs (an FFI caller with no device allocator of its own, or a plugin
+// inside an engine that owns every device allocation).  Its look-back scratch
+// lives in the fixed array below instead of a caller-provided workspace.
+namespace rm {
+namespace {
+
+// Largest tet count the fixed scratch covers: 2^26 tets (16,384 scan tiles).
+constexpr int64_t kNoAllocMaxTets = int64_t(1) << 26;
+constexpr size_t kNoAllocScratchBytes =
+    sizeof(ScanWs) + sizeof(uint64_t) * (size_t)((kNoAllocMaxTets + kScanTile - 1) / kScanTile);
+
+// 16 B header + 128 KiB of tile states.  Every GPU that loads this library
+// holds one copy until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scan_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+
+}  // namespace
+}  // namespace rm
+
+extern "C" {
+
+int rm_scan_tiles_noalloc(const int32_t* tiles_touched, int64_t n_tets, int32_t* offsets, int64_t* total_dev,
+                          void* stream) {
+    using namespace rm;
+    if (n_tets > kNoAllocMaxTets)
+        return rm_host::fail(RM_EINVAL,
+                             "rm_scan_tiles_noalloc: %lld tets exceed the fixed scratch limit of %lld tets; use "
+                             "rm_scan_tiles with a caller-provided workspace",
+                             (long long)n_tets, (long long)kNoAllocMaxTets);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_scan_tiles_noalloc: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= 64) return rm_host::fail(RM_EINVAL, "rm_scan_tiles_noalloc: device ordinal %d", dev);
+    void* scratch = nullptr;
+    {
+        // one-time set-up per device: the array's device address, looked up
+        // with that device current (the host-side symbol is not a device pointer)
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
+            if (e != cudaSuccess || !p)
+                return rm_host::fail(RM_ECUDA, "rm_scan_tiles_noalloc: cudaGetSymbolAddress: %s",
+                                     cudaGetErrorString(e));
+            g_noalloc_addr[dev] = p;
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    // rm_scan_tiles clears the queue counter and the tile states before the
+    // kernel runs, so the contents left by an earlier call do not matter
+    return rm_scan_tiles(tiles_touched, n_tets, offsets, total_dev, scratch, kNoAllocScratchBytes, stream);
 }
 
 }  // extern "C"
