@@ -236,6 +236,85 @@ RM_API int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges,
                  float* grad_vertices, float* grad_cell_values, void* workspace,
                  size_t workspace_bytes, int flags, void* stream);
 
+/* ------------------------------------------------------- batched views -- */
+/*
+ * Batched entry points render up to RM_MAX_VIEWS cameras of one mesh in one
+ * launch per stage.  They have no reference counterpart: the reference
+ * renders one camera per call (utils/train_util.py:15-77), and a batch of
+ * views through these calls yields, view by view, exactly what the
+ * single-camera calls yield.  Conventions:
+ *   - all cameras share one tile size;
+ *   - tiles get one global, view-major numbering: view v owns the tile ids
+ *     [tile_base(v), tile_base(v) + grid_w(v) * grid_h(v)), tile_base(v) being
+ *     the sum of the earlier views' grid sizes;
+ *   - per-view [T] arrays of the projection are stacked view-major ([n_views, T]);
+ *   - per-pixel buffers (ray_jitter, images, n_contrib and their gradients)
+ *     are the views' buffers concatenated in view order.
+ * Pair emission, sort and tile ranges then run once over all views with the
+ * single-camera calls (rm_scan_tiles over n_views * T counts, rm_sort_pairs
+ * with end_bit = 32 + bit length of the total tile count, rm_tile_ranges
+ * over the total tile count).
+ */
+#define RM_MAX_VIEWS 32
+
+/*
+ * Projection of every tet into every view; each tet's vertices are read once
+ * for all views.  Per view the outputs equal rm_project_fwd's: tiles_touched
+ * and rect [n_views, T] (rect rows of 4), depth [n_views, T] (rm_project_fwd's
+ * vs[:, 2]).  tiles_any [T] (optional) receives the tet's tile count summed
+ * over the views; circumcenter [T, 3] (optional) is view-independent.
+ */
+RM_API int rm_project_fwd_multi(const int32_t* indices, const float* vertices,
+                                int64_t n_tets, int64_t n_verts,
+                                const rm_camera* cams, int n_views,
+                                int32_t* tiles_touched, int32_t* rect,
+                                float* depth, int32_t* tiles_any,
+                                float* circumcenter, void* stream);
+
+/*
+ * Pair emission for the stacked projection: offsets is the inclusive scan of
+ * tiles_touched [n_views * T].  Pair (view v, tet g, tile (x, y)) gets the key
+ * ((tile_base(v) + y * grid_w(v) + x) << 32) | sortable(depth[v, g]) and the
+ * value g.  Capacity handling as rm_emit_pairs.
+ */
+RM_API int rm_emit_pairs_multi(const float* depth, const int32_t* rect,
+                               const int32_t* offsets, int64_t n_tets,
+                               const rm_camera* cams, int n_views,
+                               int64_t capacity, const int64_t* total_dev,
+                               int64_t* keys, int32_t* values,
+                               uint32_t* status_dev, void* stream);
+
+/* Total tile count of a batch (the ranges length and the blend workspace's
+ * n_tiles), or -1 on bad input. */
+RM_API int64_t rm_views_tile_count(const rm_camera* cams, int n_views);
+
+/*
+ * Blend of all views in one persistent launch fed by one work queue over the
+ * global tiles.  Arguments as rm_blend_fwd with the batched conventions above;
+ * tiles_touched, when given, is a [T] visibility count (tiles_any).
+ */
+RM_API int rm_blend_fwd_multi(const int32_t* sorted_ids, const int32_t* ranges,
+                              const int32_t* indices, const float* vertices,
+                              const float* cell_values, int64_t n_tets, int64_t n_verts,
+                              const int32_t* tiles_touched, const float* ray_jitter,
+                              const rm_camera* cams, int n_views, float* out_img,
+                              float* out_distortion, int32_t* n_contrib,
+                              void* workspace, size_t workspace_bytes, int flags,
+                              void* stream);
+
+/* Adjoint of rm_blend_fwd_multi; gradients of all views are summed into
+ * grad_vertices and grad_cell_values. */
+RM_API int rm_blend_bwd_multi(const int32_t* sorted_ids, const int32_t* ranges,
+                              const int32_t* indices, const float* vertices,
+                              const float* cell_values, int64_t n_tets, int64_t n_verts,
+                              const int32_t* tiles_touched, const float* ray_jitter,
+                              const rm_camera* cams, int n_views, const float* out_img,
+                              const float* out_distortion, const int32_t* n_contrib,
+                              const float* grad_img, const float* grad_distortion,
+                              float* grad_vertices, float* grad_cell_values,
+                              void* workspace, size_t workspace_bytes, int flags,
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif

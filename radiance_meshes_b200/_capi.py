@@ -28,6 +28,8 @@ RM_BLEND_STRIP_SHIFT = 8
 RM_BLEND_HEAVY_SHIFT = 16
 RM_BLEND_PAIR_CTAS_SHIFT = 20
 
+RM_MAX_VIEWS = 32
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "librm_b200.so")
 
@@ -60,6 +62,13 @@ SIGNATURES = {
                                     ctypes.c_int, vp]),
     "rm_blend_bwd": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, vp, vp, vp, vp, vp,
                                     vp, vp, vp, sz, ctypes.c_int, vp]),
+    "rm_project_fwd_multi": (ctypes.c_int, [vp, vp, i64, i64, camp, ctypes.c_int, vp, vp, vp, vp, vp, vp]),
+    "rm_emit_pairs_multi": (ctypes.c_int, [vp, vp, vp, i64, camp, ctypes.c_int, i64, vp, vp, vp, vp, vp]),
+    "rm_views_tile_count": (i64, [camp, ctypes.c_int]),
+    "rm_blend_fwd_multi": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, ctypes.c_int, vp, vp, vp,
+                                          vp, sz, ctypes.c_int, vp]),
+    "rm_blend_bwd_multi": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, ctypes.c_int, vp, vp, vp,
+                                          vp, vp, vp, vp, vp, sz, ctypes.c_int, vp]),
 }
 
 

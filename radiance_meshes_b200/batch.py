@@ -1,0 +1,278 @@
+"""Batched multi-view rendering: many cameras of one mesh, one launch per stage.
+
+The reference renders one camera per call (``utils/train_util.py:15-77``);
+a multi-view step there is N independent passes of
+``vertex_and_tile_shader`` + ``AlphaBlendTiledRender``, each with its own
+host synchronisations.  Here a batch of up to ``RM_MAX_VIEWS`` cameras runs as:
+
+  rm_project_fwd_multi   every tet projected into every view (vertices read once)
+  rm_scan_tiles          one scan over the stacked [n_views * T] tile counts
+  rm_emit_pairs_multi    pairs keyed by a global, view-major tile id
+  rm_sort_pairs          one radix sort over all views' pairs
+  rm_tile_ranges         ranges over the global tiles
+  rm_blend_fwd_multi     one persistent launch over all views' tiles
+  rm_blend_bwd_multi     its adjoint, gradients summed over the views
+
+Pair buffers have a fixed capacity, and the sort and ranges read the true
+pair count from the device, so a frame needs no host synchronisation and the
+whole sequence can be captured once in a CUDA graph and replayed.  A frame
+whose pairs exceed the capacity sets ``RM_STATUS_CAPACITY``; ``check()``
+reads that flag and ``ensure_capacity()`` grows the buffers.
+
+Per view, the results equal the single-camera path's bit for bit (the image,
+log T, distortion moments and n_contributors); gradients are the sum of the
+per-view gradients up to floating-point summation order.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Sequence
+
+import torch
+
+from . import _capi as C
+from .camera import RMCamera
+
+__all__ = ["ViewBatch", "BatchedRasterizer", "MAX_VIEWS"]
+
+MAX_VIEWS = 32
+
+
+class ViewBatch:
+    """Cameras of one batch (same tile size) and the derived offsets."""
+
+    def __init__(self, cams: Sequence[RMCamera]):
+        cams = list(cams)
+        if not 1 <= len(cams) <= MAX_VIEWS:
+            raise ValueError(f"a batch holds 1..{MAX_VIEWS} views, got {len(cams)}")
+        t0 = (cams[0].tile_height, cams[0].tile_width)
+        for c in cams:
+            if (c.tile_height, c.tile_width) != t0:
+                raise ValueError("all views of a batch must share one tile size")
+        self.cams = cams
+        self.n = len(cams)
+        self.array = (RMCamera * self.n)(*cams)
+        self.hw = [(c.image_height, c.image_width) for c in cams]
+        self.grid = [(c.grid_height, c.grid_width) for c in cams]
+        self.tile_base = [0]
+        self.pixel_base = [0]
+        for (gh, gw), (h, w) in zip(self.grid, self.hw):
+            self.tile_base.append(self.tile_base[-1] + gh * gw)
+            self.pixel_base.append(self.pixel_base[-1] + h * w)
+        self.n_tiles = self.tile_base[-1]
+        self.n_pixels = self.pixel_base[-1]
+        self.end_bit = 32 + int(self.n_tiles).bit_length()
+
+    def split(self, flat: torch.Tensor) -> list[torch.Tensor]:
+        """Per-view [H, W, ...] views of a concatenated [n_pixels, ...] buffer."""
+        out = []
+        for v, (h, w) in enumerate(self.hw):
+            a, b = self.pixel_base[v], self.pixel_base[v + 1]
+            out.append(flat[a:b].view(h, w, *flat.shape[1:]))
+        return out
+
+
+class BatchedRasterizer:
+    """Renders a ViewBatch of one mesh; forward, backward and a capturable
+    fwd+bwd step.
+
+    ``indices`` [T,4] int32, ``vertices`` [V,3] and ``cell_values`` [T,7]
+    float32 stay owned by the caller and are read in place on every frame
+    (update them with ``copy_`` to render new parameters).  ``jitter`` is the
+    concatenated per-pixel ray jitter [n_pixels, 2] (default 0.5).
+    """
+
+    def __init__(self, indices: torch.Tensor, vertices: torch.Tensor, cell_values: torch.Tensor,
+                 views: ViewBatch, jitter: torch.Tensor | None = None, capacity: int | None = None,
+                 fwd_flags: int = 0, bwd_flags: int = 0):
+        for name, t in (("indices", indices), ("vertices", vertices), ("cell_values", cell_values)):
+            if not t.is_cuda:
+                raise RuntimeError(f"{name} must be a CUDA tensor (the rasterizer has no CPU path)")
+        if indices.dtype != torch.int32 or not indices.is_contiguous():
+            raise ValueError("indices must be contiguous int32")
+        if vertices.dtype != torch.float32 or cell_values.dtype != torch.float32:
+            raise ValueError("vertices and cell_values must be float32")
+        self.indices, self.vertices, self.cell_values = indices, vertices, cell_values
+        self.views = views
+        self.fwd_flags, self.bwd_flags = int(fwd_flags), int(bwd_flags)
+        dev = vertices.device
+        self.device = dev
+        T, n = indices.shape[0], views.n
+        self.T, self.V = T, vertices.shape[0]
+        L = C.lib()
+        self.tiles = torch.empty(n * T, dtype=torch.int32, device=dev)
+        self.rect = torch.empty((n * T, 4), dtype=torch.int32, device=dev)
+        self.depth = torch.empty(n * T, dtype=torch.float32, device=dev)
+        self.tiles_any = torch.empty(T, dtype=torch.int32, device=dev)
+        self.offsets = torch.empty(n * T, dtype=torch.int32, device=dev)
+        self.total = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.total_host = torch.zeros(1, dtype=torch.int64).pin_memory()
+        self.scan_ws = torch.empty(L.rm_scan_workspace_size(n * T), dtype=torch.uint8, device=dev)
+        self.ranges = torch.empty((views.n_tiles, 2), dtype=torch.int32, device=dev)
+        self.blend_ws = torch.empty(L.rm_blend_workspace_size(T, views.n_tiles), dtype=torch.uint8, device=dev)
+        Npx = views.n_pixels
+        self.jitter = jitter if jitter is not None else torch.full((Npx, 2), 0.5, device=dev)
+        self.img = torch.empty((Npx, 4), dtype=torch.float32, device=dev)
+        self.dist = torch.empty((Npx, 5), dtype=torch.float32, device=dev)
+        self.nc = torch.empty(Npx, dtype=torch.int32, device=dev)
+        self.grad_img = torch.zeros((Npx, 4), dtype=torch.float32, device=dev)
+        self.grad_dist = None
+        self.grad_vertices = torch.zeros_like(vertices)
+        self.grad_cell_values = torch.zeros_like(cell_values)
+        self.capacity = 0
+        self.graph = None
+        if capacity is None:
+            capacity = self.measure_pairs()
+            capacity = int(capacity * 1.05) + 4096
+        self._alloc_pairs(capacity)
+
+    # ------------------------------------------------------------ buffers --
+    def _alloc_pairs(self, capacity: int):
+        capacity = max(int(capacity), 1)
+        dev = self.device
+        self.capacity = capacity
+        self.keys = torch.empty(capacity, dtype=torch.int64, device=dev)
+        self.vals = torch.empty(capacity, dtype=torch.int32, device=dev)
+        self.sorted_keys = torch.empty(capacity, dtype=torch.int64, device=dev)
+        self.sorted_ids = torch.empty(capacity, dtype=torch.int32, device=dev)
+        self.sort_ws = torch.empty(C.lib().rm_sort_workspace_size(capacity), dtype=torch.uint8, device=dev)
+        self.graph = None
+
+    def measure_pairs(self) -> int:
+        """Project and scan once, synchronously, and return the pair count."""
+        self._project_scan()
+        return int(self.total.item())
+
+    def ensure_capacity(self, headroom: float = 1.05) -> bool:
+        """Grow the pair buffers if the last frame overflowed them (reads the
+        pair count of the last frame); returns True if they were grown."""
+        P = int(self.total.item())
+        if P <= self.capacity:
+            return False
+        self._alloc_pairs(int(P * headroom) + 4096)
+        return True
+
+    # ------------------------------------------------------------- stages --
+    def _project_scan(self):
+        L, s, v = C.lib(), C.stream_handle(), self.views
+        nT = v.n * self.T
+        C.check(L.rm_project_fwd_multi(C.ptr(self.indices), C.ptr(self.vertices), self.T, self.V, v.array, v.n,
+                                       C.ptr(self.tiles), C.ptr(self.rect), C.ptr(self.depth),
+                                       C.ptr(self.tiles_any), None, s), "rm_project_fwd_multi")
+        C.check(L.rm_scan_tiles(C.ptr(self.tiles), nT, C.ptr(self.offsets), C.ptr(self.total),
+                                C.ptr(self.scan_ws), self.scan_ws.numel(), s), "rm_scan_tiles")
+
+    def _lists(self):
+        L, s, v = C.lib(), C.stream_handle(), self.views
+        C.check(L.rm_emit_pairs_multi(C.ptr(self.depth), C.ptr(self.rect), C.ptr(self.offsets), self.T, v.array,
+                                      v.n, self.capacity, C.ptr(self.total), C.ptr(self.keys), C.ptr(self.vals),
+                                      C.ptr(self.status), s), "rm_emit_pairs_multi")
+        C.check(L.rm_sort_pairs(C.ptr(self.keys), C.ptr(self.vals), self.capacity, C.ptr(self.total), v.end_bit,
+                                C.ptr(self.sorted_keys), C.ptr(self.sorted_ids), C.ptr(self.sort_ws),
+                                self.sort_ws.numel(), s), "rm_sort_pairs")
+        C.check(L.rm_tile_ranges(C.ptr(self.sorted_keys), self.capacity, C.ptr(self.total), C.ptr(self.ranges),
+                                 v.n_tiles, s), "rm_tile_ranges")
+
+    def _blend_fwd(self):
+        L, s, v = C.lib(), C.stream_handle(), self.views
+        C.check(L.rm_blend_fwd_multi(C.ptr(self.sorted_ids), C.ptr(self.ranges), C.ptr(self.indices),
+                                     C.ptr(self.vertices), C.ptr(self.cell_values), self.T, self.V,
+                                     C.ptr(self.tiles_any), C.ptr(self.jitter), v.array, v.n, C.ptr(self.img),
+                                     C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.blend_ws), self.blend_ws.numel(),
+                                     self.fwd_flags, s), "rm_blend_fwd_multi")
+
+    def _blend_bwd(self):
+        L, s, v = C.lib(), C.stream_handle(), self.views
+        self.grad_vertices.zero_()
+        self.grad_cell_values.zero_()
+        C.check(L.rm_blend_bwd_multi(C.ptr(self.sorted_ids), C.ptr(self.ranges), C.ptr(self.indices),
+                                     C.ptr(self.vertices), C.ptr(self.cell_values), self.T, self.V,
+                                     C.ptr(self.tiles_any), C.ptr(self.jitter), v.array, v.n, C.ptr(self.img),
+                                     C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.grad_img), C.ptr(self.grad_dist),
+                                     C.ptr(self.grad_vertices), C.ptr(self.grad_cell_values), C.ptr(self.blend_ws),
+                                     self.blend_ws.numel(), self.bwd_flags | C.RM_BLEND_REUSE_RECORDS, s),
+                "rm_blend_bwd_multi")
+
+    # ---------------------------------------------------------------- API --
+    def forward(self):
+        """Render every view (asynchronous, no host synchronisation).
+        Returns the concatenated (img [Npx,4], distortion [Npx,5], n_contrib [Npx])."""
+        self._project_scan()
+        self._lists()
+        self._blend_fwd()
+        return self.img, self.dist, self.nc
+
+    def backward(self, grad_img: torch.Tensor | None = None, grad_dist: torch.Tensor | None = None):
+        """Adjoint of the last forward; gradients of all views are summed.
+        Returns (grad_vertices, grad_cell_values)."""
+        if grad_img is not None:
+            self.grad_img.copy_(grad_img)
+        self.grad_dist = grad_dist
+        self._blend_bwd()
+        return self.grad_vertices, self.grad_cell_values
+
+    def check(self) -> None:
+        """Synchronise and raise if the last frame overflowed the pair buffers."""
+        P = int(self.total.item())
+        if P > self.capacity:
+            raise RuntimeError(f"pair capacity {self.capacity} exceeded ({P} pairs): call ensure_capacity()")
+
+    def images(self):
+        """Per-view (img [H,W,4], distortion [H,W,5], n_contrib [H,W,1])."""
+        v = self.views
+        return list(zip(v.split(self.img), v.split(self.dist), [x.unsqueeze(-1) for x in v.split(self.nc)]))
+
+
+def l1_grad_weights(views: ViewBatch, device) -> torch.Tensor:
+    """Per-pixel weight 1 / (3 * H_v * W_v): the gradient scale of a sum over
+    views of per-view mean L1 losses on the three colour channels."""
+    w = torch.empty(views.n_pixels, 1, device=device)
+    for v, (h, wd) in enumerate(views.hw):
+        w[views.pixel_base[v]:views.pixel_base[v + 1]] = 1.0 / (3.0 * h * wd)
+    return w
+
+
+class L1Step:
+    """One capturable multi-view training step: forward, the L1 loss against
+    ``target`` [Npx, 3] (sum over views of per-view means) and backward.
+    ``capture()`` records the step as a CUDA graph; ``run()`` replays it (or
+    launches eagerly before capture)."""
+
+    def __init__(self, rast: BatchedRasterizer, target: torch.Tensor):
+        self.r = rast
+        self.target = target
+        self.w = l1_grad_weights(rast.views, rast.device)
+        self.loss = torch.zeros((), device=rast.device)
+        self.graph = None
+
+    def _launch(self):
+        r = self.r
+        r.forward()
+        diff = r.img[:, :3] - self.target
+        self.loss.copy_((diff.abs() * self.w).sum())
+        r.grad_img[:, :3].copy_(torch.sign(diff) * self.w)
+        r.grad_img[:, 3].zero_()
+        r.grad_dist = None
+        r._blend_bwd()
+
+    def capture(self):
+        s = torch.cuda.Stream(device=self.r.device)
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            self._launch()  # warm-up outside capture (lazy init, attributes)
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._launch()
+        self.graph = g
+        return g
+
+    def run(self):
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._launch()
+        return self.loss

@@ -458,10 +458,10 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
     }
 }
 
-template <int NT, int B>
+template <int NT, int B, class V>
 __global__ void __launch_bounds__(NT, (NT >= 64 ? 1024 / NT : 32)) blend_fwd_dense_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
-    const float2* __restrict__ jitter, const rm_camera cam, float4* __restrict__ out_img,
+    const float2* __restrict__ jitter, const __grid_constant__ V views, float4* __restrict__ out_img,
     float* __restrict__ out_dist, int32_t* __restrict__ out_nc, const Queue q) {
     __shared__ FwdDenseSmem<B> S;
     __shared__ int s_item;
@@ -469,15 +469,18 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 1024 / NT : 32)) blend_fwd_den
     for (;;) {
         const int item = next_item(q, &s_item);
         if (item >= n_items) return;
-        fwd_dense_item<NT, B>(queue_tile(q, item), item % q.subs, ids, ranges, recs, jitter, cam, out_img, out_dist,
-                              out_nc, S);
+        const int t = queue_tile(q, item), v = views.find(t);
+        const int tb = views.tile_base(v);
+        const int64_t pb = views.pixel_base(v);
+        fwd_dense_item<NT, B>(t - tb, item % q.subs, ids, ranges + tb, recs, jitter + pb, views.camera(v),
+                              out_img + pb, out_dist + 5 * pb, out_nc + pb, S);
     }
 }
 
-template <int PX, int NT, int B>
+template <int PX, int NT, int B, class V>
 __global__ void __launch_bounds__(NT, 768 / NT) blend_fwd_pair_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
-    const float2* __restrict__ jitter, const rm_camera cam, float4* __restrict__ out_img,
+    const float2* __restrict__ jitter, const __grid_constant__ V views, float4* __restrict__ out_img,
     float* __restrict__ out_dist, int32_t* __restrict__ out_nc, const Queue q) {
     extern __shared__ __align__(16) unsigned char fwd_smem_raw[];
     FwdPairSmem<PX, B>& S = *reinterpret_cast<FwdPairSmem<PX, B>*>(fwd_smem_raw);
@@ -486,8 +489,11 @@ __global__ void __launch_bounds__(NT, 768 / NT) blend_fwd_pair_kernel(
     for (;;) {
         const int item = next_item(q, &s_item);
         if (item >= n_items) return;
-        fwd_pair_item<PX, NT, B>(queue_tile(q, item), item % q.subs, ids, ranges, recs, jitter, cam, out_img,
-                                 out_dist, out_nc, S);
+        const int t = queue_tile(q, item), v = views.find(t);
+        const int tb = views.tile_base(v);
+        const int64_t pb = views.pixel_base(v);
+        fwd_pair_item<PX, NT, B>(t - tb, item % q.subs, ids, ranges + tb, recs, jitter + pb, views.camera(v),
+                                 out_img + pb, out_dist + 5 * pb, out_nc + pb, S);
     }
 }
 
@@ -498,29 +504,44 @@ __global__ void __launch_bounds__(NT, 768 / NT) blend_fwd_pair_kernel(
 __global__ void __launch_bounds__(1024) order_kernel(const int2* __restrict__ ranges, int G,
                                                      int32_t* __restrict__ order, int32_t* info,
                                                      uint32_t* tickets, int heavy_shift) {
+    // Warp-aggregated counting: lanes that share a bucket elect one leader
+    // (match_any) for the shared atomic, and the list-length sum and the
+    // non-empty count are reduced per warp before one shared update each.
     __shared__ uint32_t cnt[33], base[33], cur[33];
-    __shared__ unsigned long long total;
-    __shared__ uint32_t nonempty;
+    __shared__ unsigned long long wtotal[32];
+    __shared__ uint32_t wnonempty[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x < 33) cnt[threadIdx.x] = 0, cur[threadIdx.x] = 0;
-    if (threadIdx.x == 0) total = 0ull, nonempty = 0u;
     __syncthreads();
-    for (int t = threadIdx.x; t < G; t += blockDim.x) {
-        const int2 r = __ldg(ranges + t);
-        const uint32_t len = (uint32_t)max(r.y - r.x, 0);
-        atomicAdd(&cnt[32 - __clz(len)], 1u);
-        if (len) {
-            atomicAdd(&total, (unsigned long long)len);
-            atomicAdd(&nonempty, 1u);
+    unsigned long long total = 0ull;
+    uint32_t nonempty = 0u;
+    const int G_pad = (G + 31) & ~31;  // whole warps iterate together
+    for (int t = threadIdx.x; t < G_pad; t += blockDim.x) {
+        uint32_t len = 0u;
+        if (t < G) {
+            const int2 r = __ldg(ranges + t);
+            len = (uint32_t)max(r.y - r.x, 0);
         }
+        total += len;
+        nonempty += __popc(__ballot_sync(0xffffffffu, len != 0u));
+        const int b = t < G ? 32 - __clz(len) : 33;
+        const unsigned peers = __match_any_sync(0xffffffffu, b);
+        if (b < 33 && lane == __ffs(peers) - 1) atomicAdd(&cnt[b], (uint32_t)__popc(peers));
     }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+    if (lane == 0) wtotal[warp] = total, wnonempty[warp] = nonempty;
     __syncthreads();
     if (threadIdx.x == 0) {
+        unsigned long long sum = 0ull;
+        uint32_t ne = 0u;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) sum += wtotal[k], ne += wnonempty[k];
         uint32_t run = 0;
         for (int b = 32; b >= 0; --b) {
             base[b] = run;
             run += cnt[b];
         }
-        const uint32_t mean = nonempty ? (uint32_t)(total / nonempty) : 0u;
+        const uint32_t mean = ne ? (uint32_t)(sum / ne) : 0u;
         // heavy_shift 1 sends every tile to the pair kernel
         const int b_thr = heavy_shift == 1 ? 0 : max(11, 32 - __clz(mean) + heavy_shift);
         int heavy = 0;
@@ -529,11 +550,19 @@ __global__ void __launch_bounds__(1024) order_kernel(const int2* __restrict__ ra
         for (int k = 0; k < 4; ++k) tickets[k] = 0u;
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < G; t += blockDim.x) {
-        const int2 r = __ldg(ranges + t);
-        const uint32_t len = (uint32_t)max(r.y - r.x, 0);
-        const int b = 32 - __clz(len);
-        order[base[b] + atomicAdd(&cur[b], 1u)] = t;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int t = threadIdx.x; t < G_pad; t += blockDim.x) {
+        int b = 33;
+        if (t < G) {
+            const int2 r = __ldg(ranges + t);
+            b = 32 - __clz((uint32_t)max(r.y - r.x, 0));
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, b);
+        const int leader = __ffs(peers) - 1;
+        uint32_t at = 0u;
+        if (b < 33 && lane == leader) at = atomicAdd(&cur[b], (uint32_t)__popc(peers));
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (b < 33) order[base[b] + at + __popc(peers & lt)] = t;
     }
 }
 
@@ -1027,10 +1056,10 @@ __device__ __forceinline__ void bwd_pair_item(
     }
 }
 
-template <int NT, int B>
+template <int NT, int B, class V>
 __global__ void __launch_bounds__(NT, (NT >= 64 ? 512 / NT : 16)) blend_bwd_dense_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
-    const int4* __restrict__ indices, const float2* __restrict__ jitter, const rm_camera cam,
+    const int4* __restrict__ indices, const float2* __restrict__ jitter, const __grid_constant__ V views,
     const float4* __restrict__ img, const float* __restrict__ dist, const int32_t* __restrict__ ncs,
     const float4* __restrict__ gimg, const float* __restrict__ gdist, float* __restrict__ gverts,
     float* __restrict__ gcv, const Queue q) {
@@ -1040,15 +1069,19 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 512 / NT : 16)) blend_bwd_dens
     for (;;) {
         const int item = next_item(q, &s_item);
         if (item >= n_items) return;
-        bwd_dense_item<NT, B>(queue_tile(q, item), item % q.subs, ids, ranges, recs, indices, jitter, cam, img,
-                              dist, ncs, gimg, gdist, gverts, gcv, S);
+        const int t = queue_tile(q, item), v = views.find(t);
+        const int tb = views.tile_base(v);
+        const int64_t pb = views.pixel_base(v);
+        bwd_dense_item<NT, B>(t - tb, item % q.subs, ids, ranges + tb, recs, indices, jitter + pb, views.camera(v),
+                              img + pb, dist + 5 * pb, ncs + pb, gimg + pb, gdist ? gdist + 5 * pb : nullptr,
+                              gverts, gcv, S);
     }
 }
 
-template <int PX, int NT, int B>
+template <int PX, int NT, int B, class V>
 __global__ void __launch_bounds__(NT, 512 / NT) blend_bwd_pair_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
-    const int4* __restrict__ indices, const float2* __restrict__ jitter, const rm_camera cam,
+    const int4* __restrict__ indices, const float2* __restrict__ jitter, const __grid_constant__ V views,
     const float4* __restrict__ img, const float* __restrict__ dist, const int32_t* __restrict__ ncs,
     const float4* __restrict__ gimg, const float* __restrict__ gdist, float* __restrict__ gverts,
     float* __restrict__ gcv, const Queue q) {
@@ -1059,8 +1092,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) blend_bwd_pair_kernel(
     for (;;) {
         const int item = next_item(q, &s_item);
         if (item >= n_items) return;
-        bwd_pair_item<PX, NT, B>(queue_tile(q, item), item % q.subs, ids, ranges, recs, indices, jitter, cam, img,
-                                 dist, ncs, gimg, gdist, gverts, gcv, S);
+        const int t = queue_tile(q, item), v = views.find(t);
+        const int tb = views.tile_base(v);
+        const int64_t pb = views.pixel_base(v);
+        bwd_pair_item<PX, NT, B>(t - tb, item % q.subs, ids, ranges + tb, recs, indices, jitter + pb,
+                                 views.camera(v), img + pb, dist + 5 * pb, ncs + pb, gimg + pb,
+                                 gdist ? gdist + 5 * pb : nullptr, gverts, gcv, S);
     }
 }
 
@@ -1110,27 +1147,48 @@ int sm_count() {
     return sms > 0 ? sms : 1;
 }
 
-// The pair kernel of a pass runs on a per-device side stream, forked from and
-// joined back into the caller's stream with events (capturable in a CUDA graph).
+// When a pass splits its tiles between the two kernels, the pair kernel runs
+// on a side stream forked from and joined back into the caller's stream with
+// events (capturable in a CUDA graph).  Each (device, caller stream) gets its
+// own side stream, so callers on different streams stay independent.
 struct SideStream {
+    int dev = -1;
+    cudaStream_t caller = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
 };
+constexpr int kSideStreams = 64;
 std::mutex g_side_mu;
-SideStream g_side[64];
+SideStream g_side[kSideStreams];
 
-int side_stream(SideStream** out) {
+// Caller holds g_side_mu.
+int side_stream(cudaStream_t caller, SideStream** out) {
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) return rm_host::fail(RM_ECUDA, "rm_blend: device ordinal %d", dev);
-    SideStream& s = g_side[dev];
-    if (!s.stream) {
-        if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming) != cudaSuccess)
-            return rm_host::fail(RM_ECUDA, "rm_blend: side stream: %s", cudaGetErrorString(cudaGetLastError()));
+    SideStream* free_slot = nullptr;
+    for (SideStream& e : g_side) {
+        if (e.stream && e.dev == dev && e.caller == caller) {
+            *out = &e;
+            return RM_OK;
+        }
+        if (!e.stream && !free_slot) free_slot = &e;
     }
-    *out = &s;
+    if (!free_slot) {  // table full: share the first side stream of this device
+        for (SideStream& e : g_side)
+            if (e.dev == dev) {
+                *out = &e;
+                return RM_OK;
+            }
+        return rm_host::fail(RM_ECUDA, "rm_blend: no side stream slot left");
+    }
+    SideStream& e = *free_slot;
+    if (cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e.fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e.join, cudaEventDisableTiming) != cudaSuccess)
+        return rm_host::fail(RM_ECUDA, "rm_blend: side stream: %s", cudaGetErrorString(cudaGetLastError()));
+    e.dev = dev;
+    e.caller = caller;
+    *out = &e;
     return RM_OK;
 }
 
@@ -1153,7 +1211,7 @@ int join_side(cudaStream_t s, SideStream* side) {
 
 // Launch tunables carried in the flags word (include/rm_capi.h).
 struct Tuning {
-    int heavy_shift;       // heavy tiles: list-length bucket >= bucket(mean) + heavy_shift
+    int heavy_shift;       // heavy tiles: list-length bucket >= bucket(mean) + heavy_shift; 1: all tiles
     int pair_ctas_per_sm;  // resident CTAs of the pair kernel per SM
 };
 
@@ -1166,64 +1224,84 @@ Tuning tuning_from_flags(int flags, int def_shift, int def_ctas) {
     return t;
 }
 
-// Forward pass: order kernel, then the pair kernel (heavy tiles, side stream)
-// and the dense kernel (other tiles, caller's stream) concurrently; the side
-// stream is joined back after both launches.
-template <int PX, int B_DENSE, int PX_PAIR, int NT_PAIR, int B_PAIR>
-int launch_fwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, const float* jitter,
-               const rm_camera& cam, float* img, float* dist, int32_t* nc, const Tuning& tn, cudaStream_t s) {
-    const int G = cam.grid_width * cam.grid_height;
+// Shape of one blend launch: G global tiles of tile_px pixels each.
+struct Shape {
+    int G;
+    int tile_px;
+};
+
+// Forward pass: order kernel, then the pair kernel (heavy tiles) and the
+// dense kernel (other tiles).  When every tile is heavy the pair kernel runs
+// alone on the caller's stream; otherwise it runs on the side stream
+// concurrently with the dense kernel and is joined back after both launches.
+template <int PX, int B_DENSE, int PX_PAIR, int NT_PAIR, int B_PAIR, class V>
+int launch_fwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, const float* jitter, const V& views,
+               const Shape& sh, float* img, float* dist, int32_t* nc, const Tuning& tn, cudaStream_t s) {
+    const int G = sh.G;
     int rc = launch_order(ranges, G, w, tn.heavy_shift, s);
     if (rc) return rc;
-    const int subs = cam.tile_width * cam.tile_height / PX;
-    const int subs_pair = cam.tile_width * cam.tile_height / PX_PAIR;
+    const int subs = sh.tile_px / PX;
+    const int subs_pair = sh.tile_px / PX_PAIR;
     const Queue qd = {w.order, w.info, w.tickets + 0, G, subs, false};
     const Queue qp = {w.order, w.info, w.tickets + 1, G, subs_pair, true};
-    std::lock_guard<std::mutex> lock(g_side_mu);
-    SideStream* side = nullptr;
-    if ((rc = side_stream(&side)) || (rc = fork_side(s, side))) return rc;
+    auto pair_kernel = blend_fwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, V>;
     const int smem = (int)sizeof(FwdPairSmem<PX_PAIR, B_PAIR>);
-    cudaFuncSetAttribute(blend_fwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const int pair_cap = tn.pair_ctas_per_sm * sm_count();
     const int pair_grid = G * subs_pair < pair_cap ? G * subs_pair : pair_cap;
-    blend_fwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR><<<pair_grid, NT_PAIR, smem, side->stream>>>(
-        ids, (const int2*)ranges, w.recs, (const float2*)jitter, cam, (float4*)img, dist, nc, qp);
+    if (tn.heavy_shift == 1) {
+        pair_kernel<<<pair_grid, NT_PAIR, smem, s>>>(ids, (const int2*)ranges, w.recs, (const float2*)jitter, views,
+                                                     (float4*)img, dist, nc, qp);
+        return rm_host::check_launch("rm_blend_fwd (pair)");
+    }
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    SideStream* side = nullptr;
+    if ((rc = side_stream(s, &side)) || (rc = fork_side(s, side))) return rc;
+    pair_kernel<<<pair_grid, NT_PAIR, smem, side->stream>>>(ids, (const int2*)ranges, w.recs, (const float2*)jitter,
+                                                            views, (float4*)img, dist, nc, qp);
     if ((rc = rm_host::check_launch("rm_blend_fwd (pair)"))) return rc;
-    const int grid = persistent_grid(blend_fwd_dense_kernel<PX, B_DENSE>, PX, 0, G * subs);
-    blend_fwd_dense_kernel<PX, B_DENSE><<<grid, PX, 0, s>>>(ids, (const int2*)ranges, w.recs,
-                                                            (const float2*)jitter, cam, (float4*)img, dist, nc, qd);
+    auto dense_kernel = blend_fwd_dense_kernel<PX, B_DENSE, V>;
+    const int grid = persistent_grid(dense_kernel, PX, 0, G * subs);
+    dense_kernel<<<grid, PX, 0, s>>>(ids, (const int2*)ranges, w.recs, (const float2*)jitter, views, (float4*)img,
+                                     dist, nc, qd);
     if ((rc = rm_host::check_launch("rm_blend_fwd (dense)"))) return rc;
     return join_side(s, side);
 }
 
-template <int PX, int B_DENSE, int PX_PAIR, int NT_PAIR, int B_PAIR>
+template <int PX, int B_DENSE, int PX_PAIR, int NT_PAIR, int B_PAIR, class V>
 int launch_bwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, const int32_t* indices,
-               const float* jitter, const rm_camera& cam, const float* img, const float* dist, const int32_t* nc,
-               const float* gimg, const float* gdist, float* gverts, float* gcv, const Tuning& tn, cudaStream_t s) {
-    const int G = cam.grid_width * cam.grid_height;
+               const float* jitter, const V& views, const Shape& sh, const float* img, const float* dist,
+               const int32_t* nc, const float* gimg, const float* gdist, float* gverts, float* gcv,
+               const Tuning& tn, cudaStream_t s) {
+    const int G = sh.G;
     int rc = launch_order(ranges, G, w, tn.heavy_shift, s);
     if (rc) return rc;
-    const int subs = cam.tile_width * cam.tile_height / PX;
-    const int subs_pair = cam.tile_width * cam.tile_height / PX_PAIR;
+    const int subs = sh.tile_px / PX;
+    const int subs_pair = sh.tile_px / PX_PAIR;
     const Queue qd = {w.order, w.info, w.tickets + 2, G, subs, false};
     const Queue qp = {w.order, w.info, w.tickets + 3, G, subs_pair, true};
-    std::lock_guard<std::mutex> lock(g_side_mu);
-    SideStream* side = nullptr;
-    if ((rc = side_stream(&side)) || (rc = fork_side(s, side))) return rc;
+    auto pair_kernel = blend_bwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, V>;
     const int smem = (int)sizeof(BwdPairSmem<PX_PAIR, B_PAIR>);
-    cudaFuncSetAttribute(blend_bwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const int pair_cap = tn.pair_ctas_per_sm * sm_count();
     const int pair_grid = G * subs_pair < pair_cap ? G * subs_pair : pair_cap;
-    blend_bwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR><<<pair_grid, NT_PAIR, smem, side->stream>>>(
-        ids, (const int2*)ranges, w.recs, (const int4*)indices, (const float2*)jitter, cam, (const float4*)img, dist,
-        nc, (const float4*)gimg, gdist, gverts, gcv, qp);
+    if (tn.heavy_shift == 1) {
+        pair_kernel<<<pair_grid, NT_PAIR, smem, s>>>(ids, (const int2*)ranges, w.recs, (const int4*)indices,
+                                                     (const float2*)jitter, views, (const float4*)img, dist, nc,
+                                                     (const float4*)gimg, gdist, gverts, gcv, qp);
+        return rm_host::check_launch("rm_blend_bwd (pair)");
+    }
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    SideStream* side = nullptr;
+    if ((rc = side_stream(s, &side)) || (rc = fork_side(s, side))) return rc;
+    pair_kernel<<<pair_grid, NT_PAIR, smem, side->stream>>>(ids, (const int2*)ranges, w.recs, (const int4*)indices,
+                                                            (const float2*)jitter, views, (const float4*)img, dist,
+                                                            nc, (const float4*)gimg, gdist, gverts, gcv, qp);
     if ((rc = rm_host::check_launch("rm_blend_bwd (pair)"))) return rc;
-    const int grid = persistent_grid(blend_bwd_dense_kernel<PX, B_DENSE>, PX, 0, G * subs);
-    blend_bwd_dense_kernel<PX, B_DENSE><<<grid, PX, 0, s>>>(ids, (const int2*)ranges, w.recs, (const int4*)indices,
-                                                            (const float2*)jitter, cam, (const float4*)img, dist, nc,
-                                                            (const float4*)gimg, gdist, gverts, gcv, qd);
+    auto dense_kernel = blend_bwd_dense_kernel<PX, B_DENSE, V>;
+    const int grid = persistent_grid(dense_kernel, PX, 0, G * subs);
+    dense_kernel<<<grid, PX, 0, s>>>(ids, (const int2*)ranges, w.recs, (const int4*)indices, (const float2*)jitter,
+                                     views, (const float4*)img, dist, nc, (const float4*)gimg, gdist, gverts, gcv, qd);
     if ((rc = rm_host::check_launch("rm_blend_bwd (dense)"))) return rc;
     return join_side(s, side);
 }
@@ -1247,27 +1325,94 @@ int pack(const int32_t* indices, const float* vertices, const float* cv, int64_t
     return rm_host::check_launch("rm_blend pack");
 }
 
+// Checks shared by all blend entry points; cam0 is the (first) camera, G the
+// total tile count of the launch.
 int check_blend_args(const char* who, const int32_t* indices, const float* vertices, const float* cv, int64_t n_tets,
-                     const float* jitter, const rm_camera* cam, void* workspace, size_t workspace_bytes, int flags) {
-    int rc = rm_host::check_cam(cam);
+                     const float* jitter, const rm_camera* cam0, int64_t G, void* workspace, size_t workspace_bytes,
+                     int flags) {
+    int rc = rm_host::check_cam(cam0);
     if (rc) return rc;
     if (n_tets < 0) return rm_host::fail(RM_EINVAL, "%s: negative size", who);
     if (!indices || !vertices || !cv || !jitter || !workspace)
         return rm_host::fail(RM_EINVAL, "%s: NULL pointer", who);
     if ((uintptr_t)indices & 15) return rm_host::fail(RM_EINVAL, "%s: indices must be 16-byte aligned", who);
     if ((uintptr_t)workspace & 15) return rm_host::fail(RM_EINVAL, "%s: workspace must be 16-byte aligned", who);
-    const int64_t G = (int64_t)cam->grid_width * cam->grid_height;
     if (workspace_bytes < blend_ws_bytes(n_tets, G))
         return rm_host::fail(RM_EINVAL, "%s: workspace %zu < %zu bytes", who, workspace_bytes,
                              blend_ws_bytes(n_tets, G));
-    const int nt = cam->tile_width * cam->tile_height;
+    const int nt = cam0->tile_width * cam0->tile_height;
     if (nt != 16 && nt != 64 && nt != 256 && nt != 1024)
         return rm_host::fail(RM_EINVAL, "%s: tile of %d pixels unsupported (16, 64, 256 or 1024)", who, nt);
-    const int strip = strip_pixels(cam, flags);
+    const int strip = strip_pixels(cam0, flags);
     if ((strip != 16 && strip != 64) || nt % strip)
         return rm_host::fail(RM_EINVAL, "%s: strip of %d pixels does not fit a %dx%d tile", who, strip,
-                             cam->tile_width, cam->tile_height);
+                             cam0->tile_width, cam0->tile_height);
     return RM_OK;
+}
+
+template <class V>
+int blend_fwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
+                  const float* vertices, const float* cell_values, int64_t n_tets, const int32_t* tiles_touched,
+                  const float* ray_jitter, const rm_camera* cam0, const V& views, const Shape& sh, float* out_img,
+                  float* out_distortion, int32_t* n_contrib, void* workspace, size_t workspace_bytes, int flags,
+                  void* stream) {
+    int rc = check_blend_args(who, indices, vertices, cell_values, n_tets, ray_jitter, cam0, sh.G, workspace,
+                              workspace_bytes, flags);
+    if (rc) return rc;
+    if (!ranges || !out_img || !out_distortion || !n_contrib) return rm_host::fail(RM_EINVAL, "%s: NULL pointer", who);
+    if (((uintptr_t)out_img & 15) || ((uintptr_t)ranges & 7) || ((uintptr_t)ray_jitter & 7))
+        return rm_host::fail(RM_EINVAL, "%s: misaligned image / ranges / jitter", who);
+    cudaStream_t s = (cudaStream_t)stream;
+    const BlendWs w = blend_ws(workspace, n_tets, sh.G);
+    if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
+        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
+        if (rc) return rc;
+    }
+    // measured on the 1.3M-tet workload: every tile through the pair kernel, 3 CTAs/SM
+    const Tuning tn = tuning_from_flags(flags, 1, 3);
+    switch (strip_pixels(cam0, flags)) {
+        case 16:
+            return launch_fwd<16, 64, 16, 64, 32>(sorted_ids, ranges, w, ray_jitter, views, sh, out_img,
+                                                  out_distortion, n_contrib, tn, s);
+        default:
+            return launch_fwd<64, 64, 64, 256, 32>(sorted_ids, ranges, w, ray_jitter, views, sh, out_img,
+                                                   out_distortion, n_contrib, tn, s);
+    }
+}
+
+template <class V>
+int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
+                  const float* vertices, const float* cell_values, int64_t n_tets, const int32_t* tiles_touched,
+                  const float* ray_jitter, const rm_camera* cam0, const V& views, const Shape& sh,
+                  const float* out_img, const float* out_distortion, const int32_t* n_contrib, const float* grad_img,
+                  const float* grad_distortion, float* grad_vertices, float* grad_cell_values, void* workspace,
+                  size_t workspace_bytes, int flags, void* stream) {
+    int rc = check_blend_args(who, indices, vertices, cell_values, n_tets, ray_jitter, cam0, sh.G, workspace,
+                              workspace_bytes, flags);
+    if (rc) return rc;
+    if (!ranges || !out_img || !out_distortion || !n_contrib || !grad_img || !grad_vertices || !grad_cell_values)
+        return rm_host::fail(RM_EINVAL, "%s: NULL pointer", who);
+    if (((uintptr_t)out_img & 15) || ((uintptr_t)grad_img & 15) || ((uintptr_t)ranges & 7) ||
+        ((uintptr_t)ray_jitter & 7))
+        return rm_host::fail(RM_EINVAL, "%s: misaligned image / grad / ranges / jitter", who);
+    cudaStream_t s = (cudaStream_t)stream;
+    const BlendWs w = blend_ws(workspace, n_tets, sh.G);
+    if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
+        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
+        if (rc) return rc;
+    }
+    // measured: the one-thread-per-pixel backward alone is fastest
+    const Tuning tn = tuning_from_flags(flags, 15, 1);
+    switch (strip_pixels(cam0, flags)) {
+        case 16:
+            return launch_bwd<16, 32, 16, 64, 16>(sorted_ids, ranges, w, indices, ray_jitter, views, sh, out_img,
+                                                  out_distortion, n_contrib, grad_img, grad_distortion, grad_vertices,
+                                                  grad_cell_values, tn, s);
+        default:
+            return launch_bwd<64, 32, 64, 256, 16>(sorted_ids, ranges, w, indices, ray_jitter, views, sh, out_img,
+                                                   out_distortion, n_contrib, grad_img, grad_distortion,
+                                                   grad_vertices, grad_cell_values, tn, s);
+    }
 }
 
 }  // namespace
@@ -1281,26 +1426,13 @@ int rm_blend_fwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t
                  const float* cell_values, int64_t n_tets, int64_t n_verts, const int32_t* tiles_touched,
                  const float* ray_jitter, const rm_camera* cam, float* out_img, float* out_distortion,
                  int32_t* n_contrib, void* workspace, size_t workspace_bytes, int flags, void* stream) {
-    using namespace rm;
-    int rc = check_blend_args("rm_blend_fwd", indices, vertices, cell_values, n_tets, ray_jitter, cam, workspace,
-                              workspace_bytes, flags);
+    int rc = rm_host::check_cam(cam);
     if (rc) return rc;
-    if (!ranges || !out_img || !out_distortion || !n_contrib)
-        return rm_host::fail(RM_EINVAL, "rm_blend_fwd: NULL pointer");
-    if (((uintptr_t)out_img & 15) || ((uintptr_t)ranges & 7) || ((uintptr_t)ray_jitter & 7))
-        return rm_host::fail(RM_EINVAL, "rm_blend_fwd: misaligned image / ranges / jitter");
-    cudaStream_t s = (cudaStream_t)stream;
-    const BlendWs w = blend_ws(workspace, n_tets, (int64_t)cam->grid_width * cam->grid_height);
-    if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
-        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
-        if (rc) return rc;
-    }
-    // measured on the 1.3M-tet workload: every tile through the pair kernel, 3 CTAs/SM
-    const Tuning tn = tuning_from_flags(flags, 1, 3);
-    switch (strip_pixels(cam, flags)) {
-        case 16: return launch_fwd<16, 64, 16, 64, 32>(sorted_ids, ranges, w, ray_jitter, *cam, out_img, out_distortion, n_contrib, tn, s);
-        default: return launch_fwd<64, 64, 64, 256, 32>(sorted_ids, ranges, w, ray_jitter, *cam, out_img, out_distortion, n_contrib, tn, s);
-    }
+    const rm::OneView one = {*cam};
+    const rm::Shape sh = {cam->grid_width * cam->grid_height, cam->tile_width * cam->tile_height};
+    return rm::blend_fwd_any("rm_blend_fwd", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
+                             tiles_touched, ray_jitter, cam, one, sh, out_img, out_distortion, n_contrib, workspace,
+                             workspace_bytes, flags, stream);
 }
 
 int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices, const float* vertices,
@@ -1308,27 +1440,44 @@ int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t
                  const float* ray_jitter, const rm_camera* cam, const float* out_img, const float* out_distortion,
                  const int32_t* n_contrib, const float* grad_img, const float* grad_distortion, float* grad_vertices,
                  float* grad_cell_values, void* workspace, size_t workspace_bytes, int flags, void* stream) {
-    using namespace rm;
-    int rc = check_blend_args("rm_blend_bwd", indices, vertices, cell_values, n_tets, ray_jitter, cam, workspace,
-                              workspace_bytes, flags);
+    int rc = rm_host::check_cam(cam);
     if (rc) return rc;
-    if (!ranges || !out_img || !out_distortion || !n_contrib || !grad_img || !grad_vertices || !grad_cell_values)
-        return rm_host::fail(RM_EINVAL, "rm_blend_bwd: NULL pointer");
-    if (((uintptr_t)out_img & 15) || ((uintptr_t)grad_img & 15) || ((uintptr_t)ranges & 7) ||
-        ((uintptr_t)ray_jitter & 7))
-        return rm_host::fail(RM_EINVAL, "rm_blend_bwd: misaligned image / grad / ranges / jitter");
-    cudaStream_t s = (cudaStream_t)stream;
-    const BlendWs w = blend_ws(workspace, n_tets, (int64_t)cam->grid_width * cam->grid_height);
-    if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
-        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
-        if (rc) return rc;
-    }
-    // measured: the one-thread-per-pixel backward alone is fastest
-    const Tuning tn = tuning_from_flags(flags, 15, 1);
-    switch (strip_pixels(cam, flags)) {
-        case 16: return launch_bwd<16, 32, 16, 64, 16>(sorted_ids, ranges, w, indices, ray_jitter, *cam, out_img, out_distortion, n_contrib, grad_img, grad_distortion, grad_vertices, grad_cell_values, tn, s);
-        default: return launch_bwd<64, 32, 64, 256, 16>(sorted_ids, ranges, w, indices, ray_jitter, *cam, out_img, out_distortion, n_contrib, grad_img, grad_distortion, grad_vertices, grad_cell_values, tn, s);
-    }
+    const rm::OneView one = {*cam};
+    const rm::Shape sh = {cam->grid_width * cam->grid_height, cam->tile_width * cam->tile_height};
+    return rm::blend_bwd_any("rm_blend_bwd", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
+                             tiles_touched, ray_jitter, cam, one, sh, out_img, out_distortion, n_contrib, grad_img,
+                             grad_distortion, grad_vertices, grad_cell_values, workspace, workspace_bytes, flags,
+                             stream);
+}
+
+int rm_blend_fwd_multi(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
+                       const float* vertices, const float* cell_values, int64_t n_tets, int64_t n_verts,
+                       const int32_t* tiles_touched, const float* ray_jitter, const rm_camera* cams, int n_views,
+                       float* out_img, float* out_distortion, int32_t* n_contrib, void* workspace,
+                       size_t workspace_bytes, int flags, void* stream) {
+    rm::ViewSet views;
+    int rc = rm_host::make_views("rm_blend_fwd_multi", cams, n_views, &views);
+    if (rc) return rc;
+    const rm::Shape sh = {views.tiles[n_views], cams[0].tile_width * cams[0].tile_height};
+    return rm::blend_fwd_any("rm_blend_fwd_multi", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
+                             tiles_touched, ray_jitter, cams, views, sh, out_img, out_distortion, n_contrib,
+                             workspace, workspace_bytes, flags, stream);
+}
+
+int rm_blend_bwd_multi(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
+                       const float* vertices, const float* cell_values, int64_t n_tets, int64_t n_verts,
+                       const int32_t* tiles_touched, const float* ray_jitter, const rm_camera* cams, int n_views,
+                       const float* out_img, const float* out_distortion, const int32_t* n_contrib,
+                       const float* grad_img, const float* grad_distortion, float* grad_vertices,
+                       float* grad_cell_values, void* workspace, size_t workspace_bytes, int flags, void* stream) {
+    rm::ViewSet views;
+    int rc = rm_host::make_views("rm_blend_bwd_multi", cams, n_views, &views);
+    if (rc) return rc;
+    const rm::Shape sh = {views.tiles[n_views], cams[0].tile_width * cams[0].tile_height};
+    return rm::blend_bwd_any("rm_blend_bwd_multi", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
+                             tiles_touched, ray_jitter, cams, views, sh, out_img, out_distortion, n_contrib,
+                             grad_img, grad_distortion, grad_vertices, grad_cell_values, workspace, workspace_bytes,
+                             flags, stream);
 }
 
 }  // extern "C"

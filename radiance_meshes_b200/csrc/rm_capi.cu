@@ -43,6 +43,31 @@ int check_cam(const rm_camera* cam) {
     return RM_OK;
 }
 
+int make_views(const char* who, const rm_camera* cams, int n, rm::ViewSet* out) {
+    if (!cams) return fail(RM_EINVAL, "%s: cameras are NULL", who);
+    if (n < 1 || n > RM_MAX_VIEWS) return fail(RM_EINVAL, "%s: %d views (1..%d)", who, n, RM_MAX_VIEWS);
+    out->n = n;
+    int64_t tiles = 0, pixels = 0;
+    for (int v = 0; v < n; ++v) {
+        int rc = check_cam(cams + v);
+        if (rc) return rc;
+        if (cams[v].tile_width != cams[0].tile_width || cams[v].tile_height != cams[0].tile_height)
+            return fail(RM_EINVAL, "%s: view %d has another tile size than view 0", who, v);
+        out->tiles[v] = (int)tiles;
+        out->pixels[v] = pixels;
+        out->cams[v] = cams[v];
+        tiles += (int64_t)cams[v].grid_width * cams[v].grid_height;
+        pixels += (int64_t)cams[v].image_width * cams[v].image_height;
+        if (tiles >= (1ll << 31)) return fail(RM_EINVAL, "%s: more than 2^31 tiles", who);
+    }
+    for (int v = n; v <= RM_MAX_VIEWS; ++v) {
+        out->tiles[v] = (int)tiles;
+        out->pixels[v] = pixels;
+    }
+    for (int v = n; v < RM_MAX_VIEWS; ++v) out->cams[v] = cams[0];
+    return RM_OK;
+}
+
 }  // namespace rm_host
 
 extern "C" {

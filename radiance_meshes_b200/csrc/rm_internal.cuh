@@ -80,6 +80,40 @@ constexpr int kRecFloat4 = 8;
 
 __device__ __forceinline__ int tile_w_of(const rm_camera& c) { return c.tile_width; }
 
+// Views of one launch, as the blend kernels see them.  Tiles of all views
+// share one global, view-major numbering (view v owns the tiles
+// [tile_base[v], tile_base[v + 1])) and the per-pixel buffers of all views are
+// concatenated (view v's pixel (x, y) is element pixel_base[v] + y * W + x).
+// OneView is the single-camera case; ViewSet carries up to RM_MAX_VIEWS
+// cameras by value in the kernel parameters, so a captured CUDA graph holds
+// its own copy.
+struct OneView {
+    rm_camera cam;
+    __device__ __forceinline__ int find(int) const { return 0; }
+    __device__ __forceinline__ const rm_camera& camera(int) const { return cam; }
+    __device__ __forceinline__ int tile_base(int) const { return 0; }
+    __device__ __forceinline__ int64_t pixel_base(int) const { return 0; }
+};
+
+struct ViewSet {
+    int n;
+    int tiles[RM_MAX_VIEWS + 1];        // tile_base, with tiles[n] = total tiles
+    int64_t pixels[RM_MAX_VIEWS + 1];   // pixel_base, with pixels[n] = total pixels
+    rm_camera cams[RM_MAX_VIEWS];
+    __device__ __forceinline__ int find(int tile) const {
+        int lo = 0, hi = n - 1;  // last view whose first tile is <= tile
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tiles[mid] <= tile) lo = mid;
+            else hi = mid - 1;
+        }
+        return lo;
+    }
+    __device__ __forceinline__ const rm_camera& camera(int v) const { return cams[v]; }
+    __device__ __forceinline__ int tile_base(int v) const { return tiles[v]; }
+    __device__ __forceinline__ int64_t pixel_base(int v) const { return pixels[v]; }
+};
+
 // Bounded spin helper: returns false once the budget is exhausted.
 __device__ __forceinline__ bool spin_budget(uint32_t& left) {
     if (left == 0) return false;
@@ -97,4 +131,7 @@ int fail(int code, const char* fmt, ...);
 // `kernels` to the process-wide launch counter.
 int check_launch(const char* what, int kernels = 1);
 int check_cam(const rm_camera* cam);
+// Validates n cameras (n in [1, RM_MAX_VIEWS], one tile size for all) and
+// fills the view table.
+int make_views(const char* who, const rm_camera* cams, int n, rm::ViewSet* out);
 }  // namespace rm_host

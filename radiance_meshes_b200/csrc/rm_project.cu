@@ -93,36 +93,117 @@ __device__ __forceinline__ void clip_face(const rm_camera& c, f3 a, f3 b, f3 cc,
     }
 }
 
-__device__ double power_of_circumsphere(d3 A, d3 B, d3 C, d3 D, d3 P, d3& center) {
+// Circumsphere of (A,B,C,D) (power_of_circumsphere, stable_power.slang:18-85,
+// without the final power): false when the tet is degenerate and not
+// collapsed to a point, in which case the reference returns power -1e20.
+__device__ bool circumsphere(d3 A, d3 B, d3 C, d3 D, d3& center, double& radius) {
     const d3 a = B - A, b = C - A, c = D - A;
     const double aa = dot3(a, a), bb = dot3(b, b), cc = dot3(c, c);
     const d3 cbc = cross3(b, c), cca = cross3(c, a), cab = cross3(a, b);
     const double den = 2.0 * dot3(a, cbc);
-    double radius;
     if (fabs(den) < 1e-10) {
         const double m = fmax(len3(B - A), fmax(len3(C - A), fmax(len3(D - A),
                          fmax(len3(C - B), fmax(len3(D - B), len3(D - C))))));
         if (m < 1e-7) {
             center = scale3(((A + B) + C) + D, 0.25);
             radius = fmin(len3(A - center), fmin(len3(B - center), fmin(len3(C - center), len3(D - center))));
-            const d3 df = center - P;
-            return dot3(df, df) - radius * radius;
+            return true;
         }
         center = {0.0, 0.0, 0.0};
-        return -1e20;
+        radius = 0.0;
+        return false;
     }
     const d3 rel = {fma(cc, cab.x, fma(bb, cca.x, aa * cbc.x)) / den,
                     fma(cc, cab.y, fma(bb, cca.y, aa * cbc.y)) / den,
                     fma(cc, cab.z, fma(bb, cca.z, aa * cbc.z)) / den};
     center = A + rel;
     radius = len3(rel);
+    return true;
+}
+
+// Power of P with respect to the sphere: |center - P|^2 - radius^2.
+__device__ __forceinline__ double sphere_power(d3 center, double radius, d3 P) {
     const d3 df = center - P;
     return dot3(df, df) - radius * radius;
+}
+
+__device__ double power_of_circumsphere(d3 A, d3 B, d3 C, d3 D, d3 P, d3& center) {
+    double radius;
+    if (!circumsphere(A, B, C, D, center, radius)) return -1e20;
+    return sphere_power(center, radius, P);
 }
 
 __device__ __forceinline__ f3 load_vertex(const float* __restrict__ v, int i) {
     const float* p = v + 3 * (int64_t)i;
     return {__ldg(p), __ldg(p + 1), __ldg(p + 2)};
+}
+
+// View-independent part of vertex_shader: the vertices, the planarity cull
+// (is_planar, intersect.slang:76-89) and the circumsphere.
+struct TetGeom {
+    f3 v[4];
+    bool planar;
+    bool sphere;  // false: power -1e20 (culled in every view)
+    d3 center;
+    double radius;
+};
+
+__device__ __forceinline__ TetGeom tet_geom(const int4* __restrict__ indices, const float* __restrict__ verts,
+                                            int64_t g) {
+    TetGeom t;
+    const int4 id = __ldg(indices + g);
+    t.v[0] = load_vertex(verts, id.x);
+    t.v[1] = load_vertex(verts, id.y);
+    t.v[2] = load_vertex(verts, id.z);
+    t.v[3] = load_vertex(verts, id.w);
+    f3 nrm = cross3(t.v[1] - t.v[0], t.v[2] - t.v[0]);
+    const float l = sqrtf(dot3(nrm, nrm));
+    nrm = {nrm.x / l, nrm.y / l, nrm.z / l};
+    t.planar = fabsf(dot3(nrm, t.v[3] - t.v[0])) < 1e-3f;
+    t.sphere = false;
+    t.center = {0.0, 0.0, 0.0};
+    t.radius = 0.0;
+    if (!t.planar)
+        t.sphere = circumsphere({(double)t.v[0].x, (double)t.v[0].y, (double)t.v[0].z},
+                                {(double)t.v[1].x, (double)t.v[1].y, (double)t.v[1].z},
+                                {(double)t.v[2].x, (double)t.v[2].y, (double)t.v[2].z},
+                                {(double)t.v[3].x, (double)t.v[3].y, (double)t.v[3].z}, t.center, t.radius);
+    return t;
+}
+
+// Per-view part of vertex_shader (vertex_shader.slang:36-89): camera space,
+// find_extent, the depth key and the tile rectangle.  Returns the tile count
+// (0: culled, r and depth zero).
+__device__ __forceinline__ int project_view(const rm_camera& cam, const TetGeom& t, int4& r, float& depth_out) {
+    r = {0, 0, 0, 0};
+    depth_out = 0.f;
+    if (t.planar) return 0;
+    const f3 cs0 = point2cam(cam, t.v[0]), cs1 = point2cam(cam, t.v[1]);
+    const f3 cs2 = point2cam(cam, t.v[2]), cs3 = point2cam(cam, t.v[3]);
+    BBox box = {{1e20f, 1e20f, 1e20f}, {-1e20f, -1e20f, -1e20f}};
+    clip_face(cam, cs0, cs1, cs2, box);
+    clip_face(cam, cs0, cs2, cs3, box);
+    clip_face(cam, cs0, cs3, cs1, box);
+    clip_face(cam, cs1, cs3, cs2, box);
+    if (box.mx.z <= 0.0f) return 0;
+    // depth key: FP64 power of the circumsphere w.r.t. the camera position
+    const d3 P = {(double)cam.cam_pos[0], (double)cam.cam_pos[1], (double)cam.cam_pos[2]};
+    const double pw = t.sphere ? sphere_power(t.center, t.radius, P) : -1e20;
+    const float depth = (float)pw;
+    if (depth < -1e19f) return 0;
+    const float gw = (float)cam.grid_width, gh = (float)cam.grid_height;
+    const float tw = (float)cam.tile_width, th = (float)cam.tile_height;
+    r.x = (int)floorf(fmaxf(0.f, fminf(gw, box.mn.x / tw)));
+    r.y = (int)floorf(fmaxf(0.f, fminf(gh, box.mn.y / th)));
+    r.z = (int)ceilf(fmaxf(0.f, fminf(gw, box.mx.x / tw)));
+    r.w = (int)ceilf(fmaxf(0.f, fminf(gh, box.mx.y / th)));
+    const int n_tiles = (r.z - r.x) * (r.w - r.y);
+    if (n_tiles == 0) {
+        r = {0, 0, 0, 0};
+        return 0;
+    }
+    depth_out = fminf(fmaxf(depth, -1e20f), 1e20f);
+    return n_tiles;
 }
 
 __global__ void __launch_bounds__(256) project_fwd_kernel(const int4* __restrict__ indices,
@@ -132,61 +213,48 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(const int4* __restrict
                                                           float* __restrict__ cc) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_tets) return;
-    const int4 id = __ldg(indices + g);
-    f3 v[4] = {load_vertex(verts, id.x), load_vertex(verts, id.y), load_vertex(verts, id.z),
-               load_vertex(verts, id.w)};
-    int n_tiles = 0;
-    int4 r = {0, 0, 0, 0};
-    float depth_out = 0.f;
-    float c0 = 0.f, c1 = 0.f, c2 = 0.f;
-    do {
-        // is_planar
-        f3 nrm = cross3(v[1] - v[0], v[2] - v[0]);
-        const float l = sqrtf(dot3(nrm, nrm));
-        nrm = {nrm.x / l, nrm.y / l, nrm.z / l};
-        if (fabsf(dot3(nrm, v[3] - v[0])) < 1e-3f) break;
-        // camera space + find_extent
-        const f3 cs0 = point2cam(cam, v[0]), cs1 = point2cam(cam, v[1]);
-        const f3 cs2 = point2cam(cam, v[2]), cs3 = point2cam(cam, v[3]);
-        BBox box = {{1e20f, 1e20f, 1e20f}, {-1e20f, -1e20f, -1e20f}};
-        clip_face(cam, cs0, cs1, cs2, box);
-        clip_face(cam, cs0, cs2, cs3, box);
-        clip_face(cam, cs0, cs3, cs1, box);
-        clip_face(cam, cs1, cs3, cs2, box);
-        if (box.mx.z <= 0.0f) break;
-        // depth key: FP64 power of the circumsphere w.r.t. the camera position
-        d3 center = {0.0, 0.0, 0.0};
-        const d3 P = {(double)cam.cam_pos[0], (double)cam.cam_pos[1], (double)cam.cam_pos[2]};
-        const double pw = power_of_circumsphere({(double)v[0].x, (double)v[0].y, (double)v[0].z},
-                                                {(double)v[1].x, (double)v[1].y, (double)v[1].z},
-                                                {(double)v[2].x, (double)v[2].y, (double)v[2].z},
-                                                {(double)v[3].x, (double)v[3].y, (double)v[3].z}, P, center);
-        const float depth = (float)pw;
-        if (depth < -1e19f) break;
-        const float gw = (float)cam.grid_width, gh = (float)cam.grid_height;
-        const float tw = (float)cam.tile_width, th = (float)cam.tile_height;
-        r.x = (int)floorf(fmaxf(0.f, fminf(gw, box.mn.x / tw)));
-        r.y = (int)floorf(fmaxf(0.f, fminf(gh, box.mn.y / th)));
-        r.z = (int)ceilf(fmaxf(0.f, fminf(gw, box.mx.x / tw)));
-        r.w = (int)ceilf(fmaxf(0.f, fminf(gh, box.mx.y / th)));
-        n_tiles = (r.z - r.x) * (r.w - r.y);
-        if (n_tiles == 0) {
-            r = {0, 0, 0, 0};
-            break;
-        }
-        depth_out = fminf(fmaxf(depth, -1e20f), 1e20f);
-        c0 = (float)center.x;
-        c1 = (float)center.y;
-        c2 = (float)center.z;
-    } while (0);
+    const TetGeom t = tet_geom(indices, verts, g);
+    int4 r;
+    float depth;
+    const int n_tiles = project_view(cam, t, r, depth);
     tiles[g] = n_tiles;
     rect[g] = r;
     vs[3 * g + 0] = 0.f;
     vs[3 * g + 1] = 0.f;
-    vs[3 * g + 2] = depth_out;
-    cc[3 * g + 0] = c0;
-    cc[3 * g + 1] = c1;
-    cc[3 * g + 2] = c2;
+    vs[3 * g + 2] = depth;
+    cc[3 * g + 0] = n_tiles ? (float)t.center.x : 0.f;
+    cc[3 * g + 1] = n_tiles ? (float)t.center.y : 0.f;
+    cc[3 * g + 2] = n_tiles ? (float)t.center.z : 0.f;
+}
+
+// All views of a batch: each thread loads its tet once and projects it into
+// every view; outputs are stacked view-major.
+__global__ void __launch_bounds__(256) project_fwd_multi_kernel(const int4* __restrict__ indices,
+                                                                const float* __restrict__ verts, int64_t n_tets,
+                                                                const __grid_constant__ ViewSet views,
+                                                                int32_t* __restrict__ tiles, int4* __restrict__ rect,
+                                                                float* __restrict__ depth, int32_t* __restrict__ any,
+                                                                float* __restrict__ cc) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_tets) return;
+    const TetGeom t = tet_geom(indices, verts, g);
+    int total = 0;
+    for (int v = 0; v < views.n; ++v) {
+        int4 r;
+        float dk;
+        const int n_tiles = project_view(views.cams[v], t, r, dk);
+        const int64_t o = (int64_t)v * n_tets + g;
+        tiles[o] = n_tiles;
+        rect[o] = r;
+        depth[o] = dk;
+        total += n_tiles;
+    }
+    if (any) any[g] = total;
+    if (cc) {
+        cc[3 * g + 0] = total ? (float)t.center.x : 0.f;
+        cc[3 * g + 1] = total ? (float)t.center.y : 0.f;
+        cc[3 * g + 2] = total ? (float)t.center.z : 0.f;
+    }
 }
 
 __device__ __forceinline__ void atomic_add3(float* p, d3 g) {
@@ -295,6 +363,25 @@ int rm_project_fwd(const int32_t* indices, const float* vertices, int64_t n_tets
     rm::project_fwd_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
         (const int4*)indices, vertices, n_tets, *cam, tiles_touched, (int4*)rect, vs, circumcenter);
     return rm_host::check_launch("rm_project_fwd");
+}
+
+int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,
+                         const rm_camera* cams, int n_views, int32_t* tiles_touched, int32_t* rect, float* depth,
+                         int32_t* tiles_any, float* circumcenter, void* stream) {
+    rm::ViewSet views;
+    int rc = rm_host::make_views("rm_project_fwd_multi", cams, n_views, &views);
+    if (rc) return rc;
+    if (n_tets < 0 || n_verts < 0) return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: negative size");
+    if (n_tets == 0) return RM_OK;
+    if (!indices || !vertices || !tiles_touched || !rect || !depth)
+        return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: NULL pointer");
+    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15))
+        return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: indices and rect must be 16-byte aligned");
+    const int threads = 256;
+    const int64_t blocks = (n_tets + threads - 1) / threads;
+    rm::project_fwd_multi_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+        (const int4*)indices, vertices, n_tets, views, tiles_touched, (int4*)rect, depth, tiles_any, circumcenter);
+    return rm_host::check_launch("rm_project_fwd_multi");
 }
 
 int rm_project_bwd(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,

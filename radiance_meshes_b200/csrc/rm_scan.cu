@@ -161,6 +161,38 @@ __global__ void __launch_bounds__(256) emit_kernel(const float* __restrict__ vs,
     }
 }
 
+// Emission for the stacked projection of a view batch: thread i handles
+// (view i / T, tet i % T) and numbers tiles globally (tile_base + local id).
+__global__ void __launch_bounds__(256) emit_multi_kernel(const float* __restrict__ depth,
+                                                         const int4* __restrict__ rect,
+                                                         const int32_t* __restrict__ offsets, int64_t n_tets,
+                                                         const __grid_constant__ ViewSet views, int64_t capacity,
+                                                         const int64_t* __restrict__ total_dev,
+                                                         int64_t* __restrict__ keys, int32_t* __restrict__ vals,
+                                                         uint32_t* status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && total_dev && status && *total_dev > capacity) atomicOr(status, RM_STATUS_CAPACITY);
+    if (i >= n_tets * views.n) return;
+    const int4 r = __ldg(rect + i);
+    const int32_t cnt = (r.z - r.x) * (r.w - r.y);
+    if (cnt <= 0) return;
+    const int v = (int)(i / n_tets);
+    const int64_t g = i - (int64_t)v * n_tets;
+    const int32_t grid_w = views.cams[v].grid_width;
+    const uint32_t tile0 = (uint32_t)views.tiles[v];
+    int64_t off = i == 0 ? 0 : (int64_t)__ldg(offsets + i - 1);
+    const uint64_t fk = sortable_key(__ldg(depth + i));
+    for (int32_t y = r.y; y < r.w; ++y) {
+        for (int32_t x = r.x; x < r.z; ++x) {
+            if (off < capacity) {
+                keys[off] = (int64_t)(((uint64_t)(tile0 + (uint32_t)(y * grid_w + x)) << 32) | fk);
+                vals[off] = (int32_t)g;
+            }
+            ++off;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) ranges_kernel(const int64_t* __restrict__ keys, int64_t cap,
                                                      const int64_t* __restrict__ n_dev,
                                                      int32_t* __restrict__ ranges, int64_t n_tiles) {
@@ -228,6 +260,31 @@ int rm_emit_pairs(const float* vs, const int32_t* rect, const int32_t* offsets, 
     rm::emit_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
         vs, (const int4*)rect, offsets, n_tets, grid_width, capacity, total_dev, keys, values, status_dev);
     return rm_host::check_launch("rm_emit_pairs");
+}
+
+int rm_emit_pairs_multi(const float* depth, const int32_t* rect, const int32_t* offsets, int64_t n_tets,
+                        const rm_camera* cams, int n_views, int64_t capacity, const int64_t* total_dev,
+                        int64_t* keys, int32_t* values, uint32_t* status_dev, void* stream) {
+    rm::ViewSet views;
+    int rc = rm_host::make_views("rm_emit_pairs_multi", cams, n_views, &views);
+    if (rc) return rc;
+    if (n_tets < 0 || capacity < 0) return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: negative size");
+    if (n_tets == 0) return RM_OK;
+    if (!depth || !rect || !offsets || (capacity > 0 && (!keys || !values)))
+        return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: NULL pointer");
+    if ((uintptr_t)rect & 15) return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: rect must be 16-byte aligned");
+    const int threads = 256;
+    const int64_t n = n_tets * n_views;
+    const int64_t blocks = (n + threads - 1) / threads;
+    rm::emit_multi_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+        depth, (const int4*)rect, offsets, n_tets, views, capacity, total_dev, keys, values, status_dev);
+    return rm_host::check_launch("rm_emit_pairs_multi");
+}
+
+int64_t rm_views_tile_count(const rm_camera* cams, int n_views) {
+    rm::ViewSet views;
+    if (rm_host::make_views("rm_views_tile_count", cams, n_views, &views)) return -1;
+    return views.tiles[n_views];
 }
 
 int rm_tile_ranges(const int64_t* sorted_keys, int64_t n, const int64_t* n_dev, int32_t* ranges, int64_t n_tiles,

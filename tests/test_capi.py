@@ -98,3 +98,46 @@ def test_python_camera_validation():
 
 def test_launch_counter_starts_at_zero_without_gpu():
     assert C.launch_count() >= 0
+
+
+def _ring_cams(res, tile=16):
+    views = scenes.ring_views(len(res), res, tile_size=tile)
+    return [tcam_to_struct(v.tcam()) for v in views]
+
+
+def test_view_batch_offsets_and_tile_count():
+    from radiance_meshes_b200 import batch as B
+
+    res = [(840, 1297), (1080, 1920), (480, 640)]
+    cams = _ring_cams(res)
+    vb = B.ViewBatch(cams)
+    grids = [((h + 15) // 16, (w + 15) // 16) for h, w in res]
+    assert vb.tile_base == [0, grids[0][0] * grids[0][1], grids[0][0] * grids[0][1] + grids[1][0] * grids[1][1],
+                            sum(a * b for a, b in grids)]
+    assert vb.pixel_base[-1] == sum(h * w for h, w in res)
+    assert vb.end_bit == 32 + vb.n_tiles.bit_length()
+    L = C.lib()
+    assert L.rm_views_tile_count(vb.array, vb.n) == vb.n_tiles
+    assert C.RM_MAX_VIEWS == B.MAX_VIEWS
+
+
+def test_view_batch_rejects_bad_batches():
+    from radiance_meshes_b200 import batch as B
+
+    L = C.lib()
+    cams = _ring_cams([(64, 64), (64, 64)], tile=16)
+    mixed = cams[:1] + _ring_cams([(64, 64)], tile=8)
+    with pytest.raises(ValueError):
+        B.ViewBatch(mixed)
+    arr = (RMCamera * 2)(*mixed)
+    assert L.rm_views_tile_count(arr, 2) == -1
+    assert "tile size" in C.last_error()
+    many = (RMCamera * (C.RM_MAX_VIEWS + 1))(*([cams[0]] * (C.RM_MAX_VIEWS + 1)))
+    assert L.rm_views_tile_count(many, C.RM_MAX_VIEWS + 1) == -1
+    assert L.rm_views_tile_count(arr, 0) == -1
+    rc = L.rm_project_fwd_multi(None, None, 10, 10, arr, 2, None, None, None, None, None, None)
+    assert rc == C.RM_EINVAL
+    ok = (RMCamera * 2)(*cams)
+    assert L.rm_project_fwd_multi(None, None, 10, 10, ok, 2, None, None, None, None, None, None) == C.RM_EINVAL
+    assert L.rm_project_fwd_multi(None, None, 0, 0, ok, 2, None, None, None, None, None, None) == C.RM_OK
+    assert L.rm_emit_pairs_multi(None, None, None, 0, ok, 2, 0, None, None, None, None, None) == C.RM_OK
