@@ -200,6 +200,10 @@ RM_API size_t rm_blend_workspace_size(int64_t n_tets, int64_t n_tiles);
  * CTAs per SM of the kernel that takes the heavy tiles (0 = default) */
 #define RM_BLEND_HEAVY_SHIFT 16
 #define RM_BLEND_PAIR_CTAS_SHIFT 20
+/* flags bits 24..27: log2 of the tets staged per shared-memory batch by the
+ * pass's main kernel (forward: the pair kernel, backward: the dense kernel);
+ * 4, 5 or 6 (0 = default 32) */
+#define RM_BLEND_BATCH_SHIFT 24
 
 /*
  * Front-to-back tile blend.  A persistent kernel takes strips of pixels from

@@ -27,6 +27,7 @@ RM_BLEND_REUSE_RECORDS = 0x1
 RM_BLEND_STRIP_SHIFT = 8
 RM_BLEND_HEAVY_SHIFT = 16
 RM_BLEND_PAIR_CTAS_SHIFT = 20
+RM_BLEND_BATCH_SHIFT = 24
 
 RM_MAX_VIEWS = 32
 

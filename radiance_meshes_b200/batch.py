@@ -32,6 +32,7 @@ from typing import Sequence
 import torch
 
 from . import _capi as C
+from . import rasterizer as R
 from .camera import RMCamera
 
 __all__ = ["ViewBatch", "BatchedRasterizer", "MAX_VIEWS"]
@@ -158,30 +159,30 @@ class BatchedRasterizer:
     def _project_scan(self):
         L, s, v = C.lib(), C.stream_handle(), self.views
         nT = v.n * self.T
-        C.check(L.rm_project_fwd_multi(C.ptr(self.indices), C.ptr(self.vertices), self.T, self.V, v.array, v.n,
+        R._call("rm_project_fwd_multi", lambda: L.rm_project_fwd_multi(C.ptr(self.indices), C.ptr(self.vertices), self.T, self.V, v.array, v.n,
                                        C.ptr(self.tiles), C.ptr(self.rect), C.ptr(self.depth),
-                                       C.ptr(self.tiles_any), None, s), "rm_project_fwd_multi")
-        C.check(L.rm_scan_tiles(C.ptr(self.tiles), nT, C.ptr(self.offsets), C.ptr(self.total),
-                                C.ptr(self.scan_ws), self.scan_ws.numel(), s), "rm_scan_tiles")
+                                       C.ptr(self.tiles_any), None, s))
+        R._call("rm_scan_tiles", lambda: L.rm_scan_tiles(C.ptr(self.tiles), nT, C.ptr(self.offsets), C.ptr(self.total),
+                                C.ptr(self.scan_ws), self.scan_ws.numel(), s))
 
     def _lists(self):
         L, s, v = C.lib(), C.stream_handle(), self.views
-        C.check(L.rm_emit_pairs_multi(C.ptr(self.depth), C.ptr(self.rect), C.ptr(self.offsets), self.T, v.array,
+        R._call("rm_emit_pairs_multi", lambda: L.rm_emit_pairs_multi(C.ptr(self.depth), C.ptr(self.rect), C.ptr(self.offsets), self.T, v.array,
                                       v.n, self.capacity, C.ptr(self.total), C.ptr(self.keys), C.ptr(self.vals),
-                                      C.ptr(self.status), s), "rm_emit_pairs_multi")
-        C.check(L.rm_sort_pairs(C.ptr(self.keys), C.ptr(self.vals), self.capacity, C.ptr(self.total), v.end_bit,
+                                      C.ptr(self.status), s))
+        R._call("rm_sort_pairs", lambda: L.rm_sort_pairs(C.ptr(self.keys), C.ptr(self.vals), self.capacity, C.ptr(self.total), v.end_bit,
                                 C.ptr(self.sorted_keys), C.ptr(self.sorted_ids), C.ptr(self.sort_ws),
-                                self.sort_ws.numel(), s), "rm_sort_pairs")
-        C.check(L.rm_tile_ranges(C.ptr(self.sorted_keys), self.capacity, C.ptr(self.total), C.ptr(self.ranges),
-                                 v.n_tiles, s), "rm_tile_ranges")
+                                self.sort_ws.numel(), s))
+        R._call("rm_tile_ranges", lambda: L.rm_tile_ranges(C.ptr(self.sorted_keys), self.capacity, C.ptr(self.total), C.ptr(self.ranges),
+                                 v.n_tiles, s))
 
     def _blend_fwd(self):
         L, s, v = C.lib(), C.stream_handle(), self.views
-        C.check(L.rm_blend_fwd_multi(C.ptr(self.sorted_ids), C.ptr(self.ranges), C.ptr(self.indices),
+        R._call("rm_blend_fwd_multi", lambda: L.rm_blend_fwd_multi(C.ptr(self.sorted_ids), C.ptr(self.ranges), C.ptr(self.indices),
                                      C.ptr(self.vertices), C.ptr(self.cell_values), self.T, self.V,
                                      C.ptr(self.tiles_any), C.ptr(self.jitter), v.array, v.n, C.ptr(self.img),
                                      C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.blend_ws), self.blend_ws.numel(),
-                                     self.fwd_flags, s), "rm_blend_fwd_multi")
+                                     self.fwd_flags, s))
 
     def _blend_bwd(self):
         L, s, v = C.lib(), C.stream_handle(), self.views

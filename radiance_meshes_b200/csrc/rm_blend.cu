@@ -1317,6 +1317,12 @@ int strip_pixels(const rm_camera* cam, int flags) {
     return strip;
 }
 
+// Tets per shared-memory batch: flags may request 2^k (RM_BLEND_BATCH_SHIFT).
+int batch_size(int flags, int def) {
+    const int req = (flags >> RM_BLEND_BATCH_SHIFT) & 0xf;
+    return req ? (1 << req) : def;
+}
+
 int pack(const int32_t* indices, const float* vertices, const float* cv, int64_t n_tets, const int32_t* tiles,
          float4* recs, cudaStream_t s) {
     const int threads = 256;
@@ -1370,14 +1376,23 @@ int blend_fwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
     }
     // measured on the 1.3M-tet workload: every tile through the pair kernel, 3 CTAs/SM
     const Tuning tn = tuning_from_flags(flags, 1, 3);
-    switch (strip_pixels(cam0, flags)) {
-        case 16:
-            return launch_fwd<16, 64, 16, 64, 32>(sorted_ids, ranges, w, ray_jitter, views, sh, out_img,
-                                                  out_distortion, n_contrib, tn, s);
+    // tets per shared-memory batch of the pair kernel: 16, 32 (default) or 64
+    const int key = strip_pixels(cam0, flags) * 1000 + batch_size(flags, 32);
+#define RM_FWD_CASE(PX, NT, BP)                                                                                  \
+    case PX * 1000 + BP:                                                                                         \
+        return launch_fwd<PX, 64, PX, NT, BP>(sorted_ids, ranges, w, ray_jitter, views, sh, out_img, out_distortion, \
+                                              n_contrib, tn, s);
+    switch (key) {
+        RM_FWD_CASE(16, 64, 16)
+        RM_FWD_CASE(16, 64, 32)
+        RM_FWD_CASE(16, 64, 64)
+        RM_FWD_CASE(64, 256, 16)
+        RM_FWD_CASE(64, 256, 32)
+        RM_FWD_CASE(64, 256, 64)
         default:
-            return launch_fwd<64, 64, 64, 256, 32>(sorted_ids, ranges, w, ray_jitter, views, sh, out_img,
-                                                   out_distortion, n_contrib, tn, s);
+            return rm_host::fail(RM_EINVAL, "%s: tets per batch %d unsupported (16, 32 or 64)", who, key % 1000);
     }
+#undef RM_FWD_CASE
 }
 
 template <class V>
@@ -1403,16 +1418,24 @@ int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
     }
     // measured: the one-thread-per-pixel backward alone is fastest
     const Tuning tn = tuning_from_flags(flags, 15, 1);
-    switch (strip_pixels(cam0, flags)) {
-        case 16:
-            return launch_bwd<16, 32, 16, 64, 16>(sorted_ids, ranges, w, indices, ray_jitter, views, sh, out_img,
-                                                  out_distortion, n_contrib, grad_img, grad_distortion, grad_vertices,
-                                                  grad_cell_values, tn, s);
+    // tets per shared-memory batch of the dense kernel: 16, 32 (default) or 64
+    const int key = strip_pixels(cam0, flags) * 1000 + batch_size(flags, 32);
+#define RM_BWD_CASE(PX, NT, BD)                                                                                  \
+    case PX * 1000 + BD:                                                                                         \
+        return launch_bwd<PX, BD, PX, NT, 16>(sorted_ids, ranges, w, indices, ray_jitter, views, sh, out_img,       \
+                                              out_distortion, n_contrib, grad_img, grad_distortion, grad_vertices,  \
+                                              grad_cell_values, tn, s);
+    switch (key) {
+        RM_BWD_CASE(16, 64, 16)
+        RM_BWD_CASE(16, 64, 32)
+        RM_BWD_CASE(16, 64, 64)
+        RM_BWD_CASE(64, 256, 16)
+        RM_BWD_CASE(64, 256, 32)
+        RM_BWD_CASE(64, 256, 64)
         default:
-            return launch_bwd<64, 32, 64, 256, 16>(sorted_ids, ranges, w, indices, ray_jitter, views, sh, out_img,
-                                                   out_distortion, n_contrib, grad_img, grad_distortion,
-                                                   grad_vertices, grad_cell_values, tn, s);
+            return rm_host::fail(RM_EINVAL, "%s: tets per batch %d unsupported (16, 32 or 64)", who, key % 1000);
     }
+#undef RM_BWD_CASE
 }
 
 }  // namespace

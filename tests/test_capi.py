@@ -141,3 +141,17 @@ def test_view_batch_rejects_bad_batches():
     assert L.rm_project_fwd_multi(None, None, 10, 10, ok, 2, None, None, None, None, None, None) == C.RM_EINVAL
     assert L.rm_project_fwd_multi(None, None, 0, 0, ok, 2, None, None, None, None, None, None) == C.RM_OK
     assert L.rm_emit_pairs_multi(None, None, None, 0, ok, 2, 0, None, None, None, None, None) == C.RM_OK
+
+
+def test_autotune_flag_packing():
+    from radiance_meshes_b200 import autotune as AT
+
+    f = AT.flags(strip=16, heavy_shift=3, pair_ctas=2, batch=64)
+    assert (f >> C.RM_BLEND_STRIP_SHIFT) & 0xff == 4
+    assert (f >> C.RM_BLEND_HEAVY_SHIFT) & 0xf == 3
+    assert (f >> C.RM_BLEND_PAIR_CTAS_SHIFT) & 0xf == 2
+    assert (f >> C.RM_BLEND_BATCH_SHIFT) & 0xf == 6
+    assert AT.flags() == 0
+    for tile in (8, 16, 32):
+        for cand in AT.candidates_fwd(tile) + AT.candidates_bwd(tile):
+            assert tile * tile % cand["strip"] == 0

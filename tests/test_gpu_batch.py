@@ -152,3 +152,47 @@ def test_capacity_overflow_is_reported_and_recovers(cuda):
     torch.cuda.synchronize()
     assert torch.equal(small.img.view(torch.int32), full.img.view(torch.int32))
     assert torch.equal(small.nc, full.nc)
+
+
+def test_every_tuning_gives_the_same_frame(cuda):
+    """The autotuner's candidates change only the work decomposition: the
+    forward is bit-identical and the gradients agree to summation order."""
+    from radiance_meshes_b200 import autotune as AT
+
+    mesh, views, cams = _scene(16)
+    i, v, c = _dev(mesh)
+    vb = B.ViewBatch(cams)
+    br = B.BatchedRasterizer(i, v, c, vb)
+    br.forward()
+    img0, nc0 = br.img.clone(), br.nc.clone()
+    br.grad_img.normal_(generator=torch.Generator("cuda").manual_seed(4))
+    gv0, gc0 = [t.clone() for t in br.backward()]
+    for cand in AT.candidates_fwd(16):
+        br.fwd_flags = AT.flags(**cand)
+        br._blend_fwd()
+        torch.cuda.synchronize()
+        assert torch.equal(br.img.view(torch.int32), img0.view(torch.int32)), cand
+        assert torch.equal(br.nc, nc0), cand
+    for cand in AT.candidates_bwd(16):
+        br.bwd_flags = AT.flags(**cand)
+        gv, gc = br.backward()
+        torch.cuda.synchronize()
+        assert float((gv - gv0).norm() / gv0.norm()) < 1e-5, cand
+        assert float((gc - gc0).norm() / gc0.norm()) < 1e-5, cand
+
+
+def test_autotuner_returns_a_valid_choice(cuda, tmp_path, monkeypatch):
+    from radiance_meshes_b200 import autotune as AT
+
+    monkeypatch.setenv("RM_AUTOTUNE_CACHE", str(tmp_path / "cache.json"))
+    mesh, views, cams = _scene(16)
+    i, v, c = _dev(mesh)
+    out = AT.tune_batch(i, v, c, views, tiles=(8, 16))
+    assert out["tile"] in (8, 16) and not out["cached"]
+    assert set(out["ms"]) == {"8", "16"}
+    again = AT.tune_batch(i, v, c, views, tiles=(8, 16))
+    assert again["cached"] and again["tile"] == out["tile"] and again["fwd_flags"] == out["fwd_flags"]
+    cams_t = [tcam_to_struct(x.tcam(tile_size=out["tile"])) for x in views]
+    br = B.BatchedRasterizer(i, v, c, B.ViewBatch(cams_t), fwd_flags=out["fwd_flags"], bwd_flags=out["bwd_flags"])
+    br.forward()
+    br.check()
