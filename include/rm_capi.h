@@ -293,9 +293,25 @@ RM_API int rm_emit_pairs_multi(const float* depth, const int32_t* rect,
 RM_API int64_t rm_views_tile_count(const rm_camera* cams, int n_views);
 
 /*
+ * Per-tet records of the blend kept outside the workspace, so that several
+ * batches on one mesh (possibly in flight on different streams) read one
+ * copy: rm_blend_records_size(T) bytes, filled by rm_blend_pack_records
+ * (tiles_touched may be NULL: every tet is packed).  No reference
+ * counterpart (the reference reloads each tet from its index and vertex
+ * arrays for every pixel batch, alphablend_shader_interp.slang:221-232).
+ */
+RM_API size_t rm_blend_records_size(int64_t n_tets);
+RM_API int rm_blend_pack_records(const int32_t* indices, const float* vertices,
+                                 const float* cell_values, int64_t n_tets, int64_t n_verts,
+                                 const int32_t* tiles_touched, void* records, void* stream);
+
+/*
  * Blend of all views in one persistent launch fed by one work queue over the
  * global tiles.  Arguments as rm_blend_fwd with the batched conventions above;
- * tiles_touched, when given, is a [T] visibility count (tiles_any).
+ * tiles_touched, when given, is a [T] visibility count (tiles_any).  records
+ * may be NULL (records are packed into the workspace, sized by
+ * rm_blend_workspace_size(T, n_tiles)) or hold rm_blend_pack_records' output
+ * (then the workspace needs only rm_blend_workspace_size(0, n_tiles) bytes).
  */
 RM_API int rm_blend_fwd_multi(const int32_t* sorted_ids, const int32_t* ranges,
                               const int32_t* indices, const float* vertices,
@@ -303,8 +319,8 @@ RM_API int rm_blend_fwd_multi(const int32_t* sorted_ids, const int32_t* ranges,
                               const int32_t* tiles_touched, const float* ray_jitter,
                               const rm_camera* cams, int n_views, float* out_img,
                               float* out_distortion, int32_t* n_contrib,
-                              void* workspace, size_t workspace_bytes, int flags,
-                              void* stream);
+                              const void* records, void* workspace,
+                              size_t workspace_bytes, int flags, void* stream);
 
 /* Adjoint of rm_blend_fwd_multi; gradients of all views are summed into
  * grad_vertices and grad_cell_values. */
@@ -316,8 +332,8 @@ RM_API int rm_blend_bwd_multi(const int32_t* sorted_ids, const int32_t* ranges,
                               const float* out_distortion, const int32_t* n_contrib,
                               const float* grad_img, const float* grad_distortion,
                               float* grad_vertices, float* grad_cell_values,
-                              void* workspace, size_t workspace_bytes, int flags,
-                              void* stream);
+                              const void* records, void* workspace,
+                              size_t workspace_bytes, int flags, void* stream);
 
 #ifdef __cplusplus
 }

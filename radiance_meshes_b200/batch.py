@@ -25,8 +25,6 @@ per-view gradients up to floating-point summation order.
 """
 from __future__ import annotations
 
-import ctypes
-import math
 from typing import Sequence
 
 import torch
@@ -86,7 +84,7 @@ class BatchedRasterizer:
 
     def __init__(self, indices: torch.Tensor, vertices: torch.Tensor, cell_values: torch.Tensor,
                  views: ViewBatch, jitter: torch.Tensor | None = None, capacity: int | None = None,
-                 fwd_flags: int = 0, bwd_flags: int = 0):
+                 fwd_flags: int = 0, bwd_flags: int = 0, records: torch.Tensor | None = None):
         for name, t in (("indices", indices), ("vertices", vertices), ("cell_values", cell_values)):
             if not t.is_cuda:
                 raise RuntimeError(f"{name} must be a CUDA tensor (the rasterizer has no CPU path)")
@@ -109,19 +107,20 @@ class BatchedRasterizer:
         self.offsets = torch.empty(n * T, dtype=torch.int32, device=dev)
         self.total = torch.zeros(1, dtype=torch.int64, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
-        self.total_host = torch.zeros(1, dtype=torch.int64).pin_memory()
         self.scan_ws = torch.empty(L.rm_scan_workspace_size(n * T), dtype=torch.uint8, device=dev)
         self.ranges = torch.empty((views.n_tiles, 2), dtype=torch.int32, device=dev)
-        self.blend_ws = torch.empty(L.rm_blend_workspace_size(T, views.n_tiles), dtype=torch.uint8, device=dev)
+        # records: per-tet blend records packed once per mesh (rm_blend_pack_records), shared by
+        # every batch on it; without them each forward packs its own into the workspace
+        self.records = records
+        ws_tets = 0 if records is not None else T
+        self.blend_ws = torch.empty(L.rm_blend_workspace_size(ws_tets, views.n_tiles), dtype=torch.uint8, device=dev)
         Npx = views.n_pixels
         self.jitter = jitter if jitter is not None else torch.full((Npx, 2), 0.5, device=dev)
         self.img = torch.empty((Npx, 4), dtype=torch.float32, device=dev)
         self.dist = torch.empty((Npx, 5), dtype=torch.float32, device=dev)
         self.nc = torch.empty(Npx, dtype=torch.int32, device=dev)
-        self.grad_img = torch.zeros((Npx, 4), dtype=torch.float32, device=dev)
+        self._grads = None  # (grad_img, grad_vertices, grad_cell_values), allocated on first use
         self.grad_dist = None
-        self.grad_vertices = torch.zeros_like(vertices)
-        self.grad_cell_values = torch.zeros_like(cell_values)
         self.capacity = 0
         self.graph = None
         if capacity is None:
@@ -130,6 +129,24 @@ class BatchedRasterizer:
         self._alloc_pairs(capacity)
 
     # ------------------------------------------------------------ buffers --
+    def _grad_bufs(self):
+        if self._grads is None:
+            self._grads = (torch.zeros((self.views.n_pixels, 4), dtype=torch.float32, device=self.device),
+                           torch.zeros_like(self.vertices), torch.zeros_like(self.cell_values))
+        return self._grads
+
+    @property
+    def grad_img(self):
+        return self._grad_bufs()[0]
+
+    @property
+    def grad_vertices(self):
+        return self._grad_bufs()[1]
+
+    @property
+    def grad_cell_values(self):
+        return self._grad_bufs()[2]
+
     def _alloc_pairs(self, capacity: int):
         capacity = max(int(capacity), 1)
         dev = self.device
@@ -181,7 +198,7 @@ class BatchedRasterizer:
         R._call("rm_blend_fwd_multi", lambda: L.rm_blend_fwd_multi(C.ptr(self.sorted_ids), C.ptr(self.ranges), C.ptr(self.indices),
                                      C.ptr(self.vertices), C.ptr(self.cell_values), self.T, self.V,
                                      C.ptr(self.tiles_any), C.ptr(self.jitter), v.array, v.n, C.ptr(self.img),
-                                     C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.blend_ws), self.blend_ws.numel(),
+                                     C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.records), C.ptr(self.blend_ws), self.blend_ws.numel(),
                                      self.fwd_flags, s))
 
     def _blend_bwd(self):
@@ -192,7 +209,7 @@ class BatchedRasterizer:
                                      C.ptr(self.vertices), C.ptr(self.cell_values), self.T, self.V,
                                      C.ptr(self.tiles_any), C.ptr(self.jitter), v.array, v.n, C.ptr(self.img),
                                      C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.grad_img), C.ptr(self.grad_dist),
-                                     C.ptr(self.grad_vertices), C.ptr(self.grad_cell_values), C.ptr(self.blend_ws),
+                                     C.ptr(self.grad_vertices), C.ptr(self.grad_cell_values), C.ptr(self.records), C.ptr(self.blend_ws),
                                      self.blend_ws.numel(), self.bwd_flags | C.RM_BLEND_REUSE_RECORDS, s),
                 "rm_blend_bwd_multi")
 

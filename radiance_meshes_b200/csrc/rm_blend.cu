@@ -1360,17 +1360,20 @@ template <class V>
 int blend_fwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
                   const float* vertices, const float* cell_values, int64_t n_tets, const int32_t* tiles_touched,
                   const float* ray_jitter, const rm_camera* cam0, const V& views, const Shape& sh, float* out_img,
-                  float* out_distortion, int32_t* n_contrib, void* workspace, size_t workspace_bytes, int flags,
-                  void* stream) {
-    int rc = check_blend_args(who, indices, vertices, cell_values, n_tets, ray_jitter, cam0, sh.G, workspace,
-                              workspace_bytes, flags);
+                  float* out_distortion, int32_t* n_contrib, const void* records, void* workspace,
+                  size_t workspace_bytes, int flags, void* stream) {
+    int rc = check_blend_args(who, indices, vertices, cell_values, records ? 0 : n_tets, ray_jitter, cam0, sh.G,
+                              workspace, workspace_bytes, flags);
     if (rc) return rc;
     if (!ranges || !out_img || !out_distortion || !n_contrib) return rm_host::fail(RM_EINVAL, "%s: NULL pointer", who);
     if (((uintptr_t)out_img & 15) || ((uintptr_t)ranges & 7) || ((uintptr_t)ray_jitter & 7))
         return rm_host::fail(RM_EINVAL, "%s: misaligned image / ranges / jitter", who);
     cudaStream_t s = (cudaStream_t)stream;
-    const BlendWs w = blend_ws(workspace, n_tets, sh.G);
-    if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
+    BlendWs w = blend_ws(workspace, records ? 0 : n_tets, sh.G);
+    if (records) {
+        if ((uintptr_t)records & 15) return rm_host::fail(RM_EINVAL, "%s: records must be 16-byte aligned", who);
+        w.recs = (float4*)records;  // packed by rm_blend_pack_records
+    } else if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
         rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
         if (rc) return rc;
     }
@@ -1400,10 +1403,10 @@ int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
                   const float* vertices, const float* cell_values, int64_t n_tets, const int32_t* tiles_touched,
                   const float* ray_jitter, const rm_camera* cam0, const V& views, const Shape& sh,
                   const float* out_img, const float* out_distortion, const int32_t* n_contrib, const float* grad_img,
-                  const float* grad_distortion, float* grad_vertices, float* grad_cell_values, void* workspace,
-                  size_t workspace_bytes, int flags, void* stream) {
-    int rc = check_blend_args(who, indices, vertices, cell_values, n_tets, ray_jitter, cam0, sh.G, workspace,
-                              workspace_bytes, flags);
+                  const float* grad_distortion, float* grad_vertices, float* grad_cell_values, const void* records,
+                  void* workspace, size_t workspace_bytes, int flags, void* stream) {
+    int rc = check_blend_args(who, indices, vertices, cell_values, records ? 0 : n_tets, ray_jitter, cam0, sh.G,
+                              workspace, workspace_bytes, flags);
     if (rc) return rc;
     if (!ranges || !out_img || !out_distortion || !n_contrib || !grad_img || !grad_vertices || !grad_cell_values)
         return rm_host::fail(RM_EINVAL, "%s: NULL pointer", who);
@@ -1411,8 +1414,11 @@ int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
         ((uintptr_t)ray_jitter & 7))
         return rm_host::fail(RM_EINVAL, "%s: misaligned image / grad / ranges / jitter", who);
     cudaStream_t s = (cudaStream_t)stream;
-    const BlendWs w = blend_ws(workspace, n_tets, sh.G);
-    if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
+    BlendWs w = blend_ws(workspace, records ? 0 : n_tets, sh.G);
+    if (records) {
+        if ((uintptr_t)records & 15) return rm_host::fail(RM_EINVAL, "%s: records must be 16-byte aligned", who);
+        w.recs = (float4*)records;  // packed by rm_blend_pack_records
+    } else if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
         rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
         if (rc) return rc;
     }
@@ -1445,6 +1451,21 @@ extern "C" {
 
 size_t rm_blend_workspace_size(int64_t n_tets, int64_t n_tiles) { return rm::blend_ws_bytes(n_tets, n_tiles); }
 
+size_t rm_blend_records_size(int64_t n_tets) {
+    return (size_t)(n_tets > 0 ? n_tets : 0) * rm::kRecFloat4 * sizeof(float4);
+}
+
+int rm_blend_pack_records(const int32_t* indices, const float* vertices, const float* cell_values, int64_t n_tets,
+                          int64_t n_verts, const int32_t* tiles_touched, void* records, void* stream) {
+    if (n_tets < 0 || n_verts < 0) return rm_host::fail(RM_EINVAL, "rm_blend_pack_records: negative size");
+    if (n_tets == 0) return RM_OK;
+    if (!indices || !vertices || !cell_values || !records)
+        return rm_host::fail(RM_EINVAL, "rm_blend_pack_records: NULL pointer");
+    if (((uintptr_t)indices & 15) || ((uintptr_t)records & 15))
+        return rm_host::fail(RM_EINVAL, "rm_blend_pack_records: indices and records must be 16-byte aligned");
+    return rm::pack(indices, vertices, cell_values, n_tets, tiles_touched, (float4*)records, (cudaStream_t)stream);
+}
+
 int rm_blend_fwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices, const float* vertices,
                  const float* cell_values, int64_t n_tets, int64_t n_verts, const int32_t* tiles_touched,
                  const float* ray_jitter, const rm_camera* cam, float* out_img, float* out_distortion,
@@ -1454,8 +1475,8 @@ int rm_blend_fwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t
     const rm::OneView one = {*cam};
     const rm::Shape sh = {cam->grid_width * cam->grid_height, cam->tile_width * cam->tile_height};
     return rm::blend_fwd_any("rm_blend_fwd", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
-                             tiles_touched, ray_jitter, cam, one, sh, out_img, out_distortion, n_contrib, workspace,
-                             workspace_bytes, flags, stream);
+                             tiles_touched, ray_jitter, cam, one, sh, out_img, out_distortion, n_contrib, nullptr,
+                             workspace, workspace_bytes, flags, stream);
 }
 
 int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices, const float* vertices,
@@ -1469,22 +1490,22 @@ int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t
     const rm::Shape sh = {cam->grid_width * cam->grid_height, cam->tile_width * cam->tile_height};
     return rm::blend_bwd_any("rm_blend_bwd", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
                              tiles_touched, ray_jitter, cam, one, sh, out_img, out_distortion, n_contrib, grad_img,
-                             grad_distortion, grad_vertices, grad_cell_values, workspace, workspace_bytes, flags,
-                             stream);
+                             grad_distortion, grad_vertices, grad_cell_values, nullptr, workspace, workspace_bytes,
+                             flags, stream);
 }
 
 int rm_blend_fwd_multi(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
                        const float* vertices, const float* cell_values, int64_t n_tets, int64_t n_verts,
                        const int32_t* tiles_touched, const float* ray_jitter, const rm_camera* cams, int n_views,
-                       float* out_img, float* out_distortion, int32_t* n_contrib, void* workspace,
-                       size_t workspace_bytes, int flags, void* stream) {
+                       float* out_img, float* out_distortion, int32_t* n_contrib, const void* records,
+                       void* workspace, size_t workspace_bytes, int flags, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_blend_fwd_multi", cams, n_views, &views);
     if (rc) return rc;
     const rm::Shape sh = {views.tiles[n_views], cams[0].tile_width * cams[0].tile_height};
     return rm::blend_fwd_any("rm_blend_fwd_multi", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
                              tiles_touched, ray_jitter, cams, views, sh, out_img, out_distortion, n_contrib,
-                             workspace, workspace_bytes, flags, stream);
+                             records, workspace, workspace_bytes, flags, stream);
 }
 
 int rm_blend_bwd_multi(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
@@ -1492,15 +1513,16 @@ int rm_blend_bwd_multi(const int32_t* sorted_ids, const int32_t* ranges, const i
                        const int32_t* tiles_touched, const float* ray_jitter, const rm_camera* cams, int n_views,
                        const float* out_img, const float* out_distortion, const int32_t* n_contrib,
                        const float* grad_img, const float* grad_distortion, float* grad_vertices,
-                       float* grad_cell_values, void* workspace, size_t workspace_bytes, int flags, void* stream) {
+                       float* grad_cell_values, const void* records, void* workspace, size_t workspace_bytes,
+                       int flags, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_blend_bwd_multi", cams, n_views, &views);
     if (rc) return rc;
     const rm::Shape sh = {views.tiles[n_views], cams[0].tile_width * cams[0].tile_height};
     return rm::blend_bwd_any("rm_blend_bwd_multi", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
                              tiles_touched, ray_jitter, cams, views, sh, out_img, out_distortion, n_contrib,
-                             grad_img, grad_distortion, grad_vertices, grad_cell_values, workspace, workspace_bytes,
-                             flags, stream);
+                             grad_img, grad_distortion, grad_vertices, grad_cell_values, records, workspace,
+                             workspace_bytes, flags, stream);
 }
 
 }  // extern "C"

@@ -29,6 +29,9 @@ __all__ = [
     "workload_training_step",
     "workload_multiview",
     "ring_views",
+    "sphere_view",
+    "serving_meshes",
+    "serving_trace",
 ]
 
 
@@ -184,3 +187,44 @@ def workload_multiview(n_points: int = 1_000_000, seed: int = 3, tile_size: int 
     order = [0, 8, 1, 12, 2, 9, 3, 13, 4, 10, 5, 14, 6, 11, 7, 15]
     views = ring_views(16, [res[i] for i in order], tile_size=tile_size)
     return Mesh(pts, idx, cv, f"mixture{n_points}"), views
+
+
+def sphere_view(rng, height: int, width: int, radius: float = 4.0, tile_size: int = 16) -> View:
+    """Camera at a uniformly random point of the radius-`radius` sphere,
+    looking at the origin (world up +y, or +x when looking along y)."""
+    d = rng.normal(size=3)
+    d /= np.linalg.norm(d)
+    up = (0.0, 1.0, 0.0) if abs(d[1]) < 0.99 else (1.0, 0.0, 0.0)
+    return _view(tuple(radius * d), (0.0, 0.0, 0.0), height, width, 60.0, tile_size, up=up)
+
+
+SERVING_RESOLUTIONS = [(480, 640), (720, 1280), (1080, 1920)]
+
+
+def serving_meshes(point_counts=(250_000, 1_000_000, 3_000_000), seeds=(4, 5, 6)):
+    """The resident meshes of the serving workload: mixture clouds of the
+    given sizes (30% of densities at 1e-4), one seed each."""
+    out = []
+    for n, s in zip(point_counts, seeds):
+        pts = mixture_points(n, s)
+        idx = delaunay(pts)
+        cv = make_features(len(idx), seed=s + 1000, low_density_frac=0.3)
+        out.append(Mesh(pts, idx, cv, f"mixture{n}"))
+    return out
+
+
+def serving_trace(n_requests: int, rate_hz: float, mesh_names, seed: int = 7, resolutions=None,
+                  tile_size: int = 16, radius: float = 4.0):
+    """Poisson request stream: exponential inter-arrival times at `rate_hz`,
+    each request picking a mesh uniformly, a camera uniformly on the sphere
+    and a resolution uniformly from `resolutions`.  Returns a list of
+    (arrival_s, mesh_name, View)."""
+    rng = np.random.default_rng(seed)
+    resolutions = resolutions or SERVING_RESOLUTIONS
+    t = np.cumsum(rng.exponential(1.0 / rate_hz, size=n_requests))
+    out = []
+    for k in range(n_requests):
+        name = mesh_names[int(rng.integers(0, len(mesh_names)))]
+        h, w = resolutions[int(rng.integers(0, len(resolutions)))]
+        out.append((float(t[k]), name, sphere_view(rng, h, w, radius, tile_size)))
+    return out

@@ -2,6 +2,8 @@
 include/rm_capi.h, answers size queries and rejects bad arguments before any
 device work."""
 import ctypes
+
+import numpy as np
 import os
 import re
 
@@ -155,3 +157,17 @@ def test_autotune_flag_packing():
     for tile in (8, 16, 32):
         for cand in AT.candidates_fwd(tile) + AT.candidates_bwd(tile):
             assert tile * tile % cand["strip"] == 0
+
+
+def test_serving_trace_is_seeded_poisson():
+    tr = scenes.serving_trace(4000, 200.0, ["a", "b", "c"], seed=7)
+    tr2 = scenes.serving_trace(4000, 200.0, ["a", "b", "c"], seed=7)
+    assert [x[0] for x in tr] == [x[0] for x in tr2]
+    gaps = np.diff([0.0] + [x[0] for x in tr])
+    assert abs(gaps.mean() - 1 / 200.0) < 0.1 / 200.0
+    names = [x[1] for x in tr]
+    assert all(abs(names.count(n) / len(names) - 1 / 3) < 0.05 for n in "abc")
+    res = [(v.height, v.width) for _, _, v in tr]
+    assert set(res) == set(scenes.SERVING_RESOLUTIONS)
+    for _, _, v in tr[:50]:
+        assert abs(np.linalg.norm(v.cam_pos) - 4.0) < 1e-5
