@@ -50,9 +50,17 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=0, help="(profiling) run N steps after warmup, print nothing")
-    ap.add_argument("--workload", choices=["training", "multiview"], default="training",
+    ap.add_argument("--workload", choices=["training", "multiview", "serving"], default="training",
                     help="training: the 1.3M-tet fwd+bwd step (default line); multiview: 16 views of a "
-                         "1M-point mesh, batched CUDA-graph step vs 16 plain per-view steps")
+                         "1M-point mesh, batched CUDA-graph step vs 16 plain per-view steps; serving: "
+                         "Poisson requests over three resident meshes, p50/p99 latency")
+    ap.add_argument("--sv-points", default="250000,1000000,3000000")
+    ap.add_argument("--sv-rate", type=float, default=200.0)
+    ap.add_argument("--sv-requests", type=int, default=2000)
+    ap.add_argument("--sv-warmup", type=int, default=200)
+    ap.add_argument("--sv-streams", type=int, default=4)
+    ap.add_argument("--sv-max-views", type=int, default=8)
+    ap.add_argument("--sv-tile", type=int, default=0, help="tile size (0: autotuned on the middle mesh)")
     ap.add_argument("--mv-points", type=int, default=1_000_000)
     ap.add_argument("--mv-views", type=int, default=16)
     ap.add_argument("--mv-tile", type=int, default=0, help="tile size of the batched step (0: autotuned)")
@@ -143,6 +151,7 @@ def run_b200(args):
 
     import radiance_meshes_b200 as RMB
     from radiance_meshes_b200 import _capi
+    from radiance_meshes_b200 import multigpu as MG
     from radiance_meshes_b200 import rasterizer as R
 
     world, rank, local = dist_env()
@@ -185,8 +194,7 @@ def run_b200(args):
         loss = (img[..., :3] - tgt).abs().mean()
         loss.backward()
         if world > 1:
-            dist.all_reduce(v.grad)
-            dist.all_reduce(c.grad)
+            MG.allreduce_grads([v.grad, c.grad])
         stats["P"] = int(sorted_ids.shape[0])
         return loss, img
 
@@ -546,8 +554,98 @@ def run_multiview(args):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------- serving --
+def _serving_mesh(job):
+    n, seed = job
+    from radiance_meshes_b200 import scenes
+
+    pts = scenes.mixture_points(n, seed)
+    idx = scenes.delaunay(pts)
+    cv = scenes.make_features(len(idx), seed=seed + 1000, low_density_frac=0.3)
+    return n, pts, idx, cv
+
+
+def run_serving(args):
+    """Three resident meshes (250k / 1M / 3M mixture points, seeds 4-6), a
+    Poisson stream of forward render requests (200 req/s, seed 7), each on a
+    uniformly chosen mesh with a camera uniform on the radius-4 sphere and a
+    resolution uniform over 640x480 / 1280x720 / 1920x1080; continuous
+    batching over streams under an HBM budget.  Reports p50/p99 latency
+    (result-ready event minus arrival) over the requests after the warm-up."""
+    import multiprocessing as mp
+
+    counts = [int(x) for x in args.sv_points.split(",")]
+    seeds = [4, 5, 6][:len(counts)]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(len(counts)) as pool:  # before any CUDA call
+        built = pool.map(_serving_mesh, list(zip(counts, seeds)))
+    gen_s = time.perf_counter() - t0
+
+    import torch
+
+    from radiance_meshes_b200 import _capi
+    from radiance_meshes_b200 import scenes
+    from radiance_meshes_b200 import serve as S
+    from radiance_meshes_b200.camera import tcam_to_struct
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    resident = [S.ResidentMesh(f"mixture{n}", idx, pts, cv, device=dev) for n, pts, idx, cv in built]
+    tets = {m.name: m.T for m in resident}
+    names = [m.name for m in resident]
+    tile, flags, tuned = args.sv_tile, 0, None
+    rng = np.random.default_rng(77)
+    sample_views = [scenes.sphere_view(rng, h, w) for (h, w) in scenes.SERVING_RESOLUTIONS for _ in range(2)]
+    if tile == 0:
+        from radiance_meshes_b200 import autotune
+
+        mid = resident[len(resident) // 2]
+        tuned = autotune.tune_batch(mid.indices, mid.vertices, mid.cell_values, sample_views[::2], device=dev,
+                                    tiles=(8, 16), backward=False)
+        tile, flags = tuned["tile"], tuned["fwd_flags"]
+    server = S.Server(resident, streams=args.sv_streams, max_views=args.sv_max_views, tile=tile, fwd_flags=flags,
+                      keep_outputs=False, device=dev)
+    server.calibrate({m.name: [tcam_to_struct(v.tcam(tile_size=tile)) for v in sample_views] for m in resident})
+    n_total = args.sv_warmup + args.sv_requests
+    trace = scenes.serving_trace(n_total, args.sv_rate, names, seed=7, tile_size=tile)
+    reqs = [S.RenderRequest(k, name, tcam_to_struct(v.tcam(tile_size=tile)), t)
+            for k, (t, name, v) in enumerate(trace)]
+    launches0 = _capi.launch_count()
+    with ClockSampler(local) as clocks:
+        results = server.run_trace(reqs, realtime=True)
+    launches = _capi.launch_count() - launches0
+    results.sort(key=lambda r: r.rid)
+    summ = S.latency_summary(results, skip=args.sv_warmup)
+    per_mesh = {}
+    for name in names:
+        sub = [r for r in results[args.sv_warmup:] if r.mesh == name]
+        if sub:
+            per_mesh[name] = {k: v for k, v in S.latency_summary(sub).items() if k in ("requests", "p50_ms", "p99_ms")}
+    views = np.array([r.batch_views for r in results[args.sv_warmup:]])
+    line = {
+        "metric": "serving p99 latency ms @200 req/s", "value": summ["p99_ms"], "unit": "ms", "n_gpus": 1,
+        "steps": args.sv_requests, "warmup": args.sv_warmup, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "p50_ms": summ["p50_ms"], "p90_ms": summ["p90_ms"], "p99_ms": summ["p99_ms"], "mean_ms": summ["mean_ms"],
+        "max_ms": summ["max_ms"], "frames_per_s": summ["frames_per_s"],
+        "config": {"workload": f"serving: meshes {counts} mixture points (seeds {seeds}), tets {tets}, Poisson "
+                               f"{args.sv_rate} req/s (seed 7), sphere poses r=4, resolutions 640x480/1280x720/"
+                               f"1920x1080, forward only",
+                   "streams": args.sv_streams, "max_views": args.sv_max_views, "tile": tile, "autotune": tuned,
+                   "hbm_budget_bytes": server.hbm_budget, "latency": "result-ready CUDA event minus arrival"},
+        "per_mesh": per_mesh, "batches": server.n_batches, "mean_views_per_batch": float(views.mean()),
+        "retries": server.n_retries, "peak_reserved_bytes": server.peak_reserved,
+        "resident_bytes": sum(m.nbytes for m in resident), "gpu_launches": int(launches),
+        "mesh_generation_s": gen_s, "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.impl == "b200" and args.workload == "serving":
+        return run_serving(args)
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "multiview":
