@@ -197,6 +197,25 @@ __device__ __forceinline__ void integrate(const float4* __restrict__ q, f3 o, f3
     for (int k = 0; k < 3; ++k) s.rgb[k] = fmaf(s.w.w1, s.ce + base[k], s.w.w0 * (s.cx + base[k]));
 }
 
+// Pixel (lx, ly) inside the tile of thread t of work item `sub`, for items of
+// NT pixels: square blocks of 8x8 (NT = 64) or 4x4 (NT = 16) pixels, row-major
+// over the tile, so that the pixels of one item see similar lists; tiles whose
+// sides are not multiples of the block fall back to runs of whole rows.
+template <int NT>
+__device__ __forceinline__ void strip_pixel(const rm_camera& cam, int sub, int t, int& lx, int& ly) {
+    constexpr int bw = NT >= 64 ? 8 : 4;
+    constexpr int bh = NT / bw;
+    if (cam.tile_width % bw == 0 && cam.tile_height % bh == 0) {
+        const int nbx = cam.tile_width / bw;
+        lx = (sub % nbx) * bw + t % bw;
+        ly = (sub / nbx) * bh + t / bw;
+    } else {
+        const int tp = sub * NT + t;
+        lx = tp % cam.tile_width;
+        ly = tp / cam.tile_width;
+    }
+}
+
 struct PixelState {
     float c[3];
     float logT;
@@ -302,9 +321,8 @@ __device__ __forceinline__ void fwd_dense_item(int tile, int sub, const int32_t*
                                                float4* __restrict__ out_img, float* __restrict__ out_dist,
                                                int32_t* __restrict__ out_nc, FwdDenseSmem<B>& S) {
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
-    const int tp = sub * NT + (int)threadIdx.x;  // pixel index inside the tile (row-major)
-    const int lx = tp % cam.tile_width;
-    const int ly = tp / cam.tile_width;
+    int lx, ly;
+    strip_pixel<NT>(cam, sub, (int)threadIdx.x, lx, ly);
     const int px = tx * cam.tile_width + lx, py = ty * cam.tile_height + ly;
     const bool inside = px < cam.image_width && py < cam.image_height;
     const int64_t pix = (int64_t)py * cam.image_width + px;
@@ -371,20 +389,30 @@ struct FwdPairSmem {
     int32_t warp_base[(PX + 31) / 32];
 };
 
+template <int PX, int B>
+__device__ __forceinline__ void store_result(FwdPairSmem<PX, B>& S, int j, int sl, const EntryResult& r) {
+    S.res[0][j][sl] = r.a;
+    S.res[1][j][sl] = r.m1;
+    S.res[2][j][sl] = r.d4;
+    S.res[3][j][sl] = r.rgb[0];
+    S.res[4][j][sl] = r.rgb[1];
+    S.res[5][j][sl] = r.rgb[2];
+}
+
 template <int PX, int NT, int B>
 __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* __restrict__ ids,
                                          const int2* __restrict__ ranges, const float4* __restrict__ recs,
                                          const float2* __restrict__ jitter, const rm_camera& cam,
                                          float4* __restrict__ out_img, float* __restrict__ out_dist,
                                          int32_t* __restrict__ out_nc, FwdPairSmem<PX, B>& S) {
+    static_assert(PX <= 64 && NT >= 64, "a lane evaluates at most two slots");
     constexpr unsigned kOwnMask = WarpShape<PX>::kMask;
     constexpr int kWarps = NT / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool owner = tid < PX;
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
-    const int tp = sub * PX + tid;  // pixel index inside the tile (row-major)
-    const int lx = tp % cam.tile_width;
-    const int ly = tp / cam.tile_width;
+    int lx, ly;
+    strip_pixel<PX>(cam, sub, tid, lx, ly);
     const int px = tx * cam.tile_width + lx, py = ty * cam.tile_height + ly;
     const bool inside = owner && px < cam.image_width && py < cam.image_height;
     const int64_t pix = (int64_t)py * cam.image_width + px;
@@ -418,32 +446,52 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
             S.ray[3][slot] = d.x; S.ray[4][slot] = d.y; S.ray[5][slot] = d.z;
         }
         __syncthreads();
-        for (int j = warp; j < n; j += kWarps) {
-            const float4* q = S.srec[j];
-            for (int sl = lane; sl < n_active; sl += 32) {
-                const f3 ro = {S.ray[0][sl], S.ray[1][sl], S.ray[2][sl]};
-                const f3 rd = {S.ray[3][sl], S.ray[4][sl], S.ray[5][sl]};
-                const EntryResult r = eval_entry(q, ro, rd);
-                S.res[0][j][sl] = r.a;
-                S.res[1][j][sl] = r.m1;
-                S.res[2][j][sl] = r.d4;
-                S.res[3][j][sl] = r.rgb[0];
-                S.res[4][j][sl] = r.rgb[1];
-                S.res[5][j][sl] = r.rgb[2];
+        // Evaluate.  Rays stay in registers for the whole batch.  With more than
+        // 32 active slots a lane takes slots lane and lane + 32 of each entry the
+        // warp takes; with fewer, the warp splits into groups of `span` lanes
+        // (the next power of two >= n_active, at least 4), each group taking
+        // its own entry, so lanes do not idle when most pixels have terminated.
+        if (n_active > 32) {
+            const bool has1 = lane + 32 < n_active;
+            const f3 o0 = {S.ray[0][lane], S.ray[1][lane], S.ray[2][lane]};
+            const f3 d0 = {S.ray[3][lane], S.ray[4][lane], S.ray[5][lane]};
+            f3 o1 = o0, d1 = d0;
+            if (has1) {
+                o1 = {S.ray[0][lane + 32], S.ray[1][lane + 32], S.ray[2][lane + 32]};
+                d1 = {S.ray[3][lane + 32], S.ray[4][lane + 32], S.ray[5][lane + 32]};
             }
+            for (int j = warp; j < n; j += kWarps) {
+                store_result(S, j, lane, eval_entry(S.srec[j], o0, d0));
+                if (has1) store_result(S, j, lane + 32, eval_entry(S.srec[j], o1, d1));
+            }
+        } else {
+            const int span = n_active <= 4 ? 4 : n_active <= 8 ? 8 : n_active <= 16 ? 16 : 32;
+            const int groups = 32 / span;
+            const int sl = lane & (span - 1);
+            const bool has = sl < n_active;
+            f3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
+            if (has) {
+                o = {S.ray[0][sl], S.ray[1][sl], S.ray[2][sl]};
+                d = {S.ray[3][sl], S.ray[4][sl], S.ray[5][sl]};
+            }
+            for (int j = warp * groups + lane / span; j < n; j += kWarps * groups)
+                if (has) store_result(S, j, sl, eval_entry(S.srec[j], o, d));
         }
         __syncthreads();
-        if (active) {
-            for (int j = 0; j < n; ++j) {
+        // Fold in list order; the hit tests of four entries are read ahead.
+        for (int j0 = 0; active && j0 < n; j0 += 4) {
+            float a4[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) a4[u] = j0 + u < n ? S.res[0][j0 + u][slot] : 0.f;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = j0 + u;
+                if (!active || j >= n) break;
                 ++nc;
-                const float a = S.res[0][j][slot];
-                if (a > 0.f) {
+                if (a4[u] > 0.f) {
                     const float rgb[3] = {S.res[3][j][slot], S.res[4][j][slot], S.res[5][j][slot]};
-                    fold_hit(st, a, S.srec[j][0].w, S.res[1][j][slot], S.res[2][j][slot], rgb);
-                    if (st.logT < kTermLogT) {
-                        active = false;
-                        break;
-                    }
+                    fold_hit(st, a4[u], S.srec[j][0].w, S.res[1][j][slot], S.res[2][j][slot], rgb);
+                    if (st.logT < kTermLogT) active = false;
                 }
             }
         }
@@ -757,9 +805,8 @@ __device__ __forceinline__ void bwd_dense_item(
     float* __restrict__ gverts, float* __restrict__ gcv, BwdDenseSmem<NT, B>& S) {
     constexpr unsigned kMask = WarpShape<NT>::kMask;
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
-    const int tp = sub * NT + (int)threadIdx.x;  // pixel index inside the tile (row-major)
-    const int lx = tp % cam.tile_width;
-    const int ly = tp / cam.tile_width;
+    int lx, ly;
+    strip_pixel<NT>(cam, sub, (int)threadIdx.x, lx, ly);
     const int px = tx * cam.tile_width + lx, py = ty * cam.tile_height + ly;
     const bool inside = px < cam.image_width && py < cam.image_height;
     const int64_t pix = (int64_t)py * cam.image_width + px;
@@ -885,9 +932,8 @@ __device__ __forceinline__ void bwd_pair_item(
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool owner = tid < PX;
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
-    const int tp = sub * PX + tid;  // pixel index inside the tile (row-major)
-    const int lx = tp % cam.tile_width;
-    const int ly = tp / cam.tile_width;
+    int lx, ly;
+    strip_pixel<PX>(cam, sub, tid, lx, ly);
     const int px = tx * cam.tile_width + lx, py = ty * cam.tile_height + ly;
     const bool inside = owner && px < cam.image_width && py < cam.image_height;
     const int64_t pix = (int64_t)py * cam.image_width + px;
