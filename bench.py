@@ -170,6 +170,7 @@ def run_b200(args):
     H, W = view.height, view.width
     T, V = len(mesh.indices), len(mesh.vertices)
     tcam = view.tcam(device=dev)
+    camst = R.camera(tcam)
     grid = RenderGrid(H, W, tile_width=args.tile, tile_height=args.tile)
     rng = np.random.default_rng(1000 + rank)
     target_h = torch.from_numpy(rng.uniform(size=(H, W, 3)).astype(np.float32))
@@ -196,6 +197,10 @@ def run_b200(args):
         if world > 1:
             MG.allreduce_grads([v.grad, c.grad])
         stats["P"] = int(sorted_ids.shape[0])
+        fine = R.fine_lists_of(sorted_ids, camst)
+        stats["P_blend"] = fine.n_pairs if fine is not None else stats["P"]
+        stats["G_blend"] = (fine.cam.grid_width * fine.cam.grid_height) if fine is not None else None
+        stats["fine"] = fine is not None
         return loss, img
 
     for _ in range(args.warmup):
@@ -235,7 +240,12 @@ def run_b200(args):
     # (the issue-rate unit), from a separate untimed forward
     with torch.no_grad():
         sorted_ids, ranges, vs, cc, mask, rect = vertex_and_tile_shader(idx, verts, tcam, grid)
-        _, _, ncs, _ = R.blend_fwd(sorted_ids, ranges, idx, verts.detach(), cv.detach(), jitter, R.camera(tcam),
+        fine = R.fine_lists_of(sorted_ids, camst)
+        if fine is not None:  # the lists the timed blend walked
+            sorted_ids, ranges, bcam = fine.sorted_ids, fine.ranges, fine.cam
+        else:
+            bcam = camst
+        _, _, ncs, _ = R.blend_fwd(sorted_ids, ranges, idx, verts.detach(), cv.detach(), jitter, bcam,
                                    tiles_touched=mask.to(torch.int32))
         tests = int(ncs.sum().item())
     if world > 1:
@@ -289,6 +299,9 @@ def run_b200(args):
     Npx = H * W
     P = stats["P"]
     G = grid.grid_width * grid.grid_height
+    # the blend walks the 8x8-pixel lists when the drop-in built them
+    Pb = stats["P_blend"]
+    Gb = stats["G_blend"] or G
     value = world * Npx * args.steps / (total_ms * 1e-3) / 1e6
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -303,8 +316,8 @@ def run_b200(args):
     per_stage = {k: {"ms_per_step": v[0] / args.steps, "calls": v[1]} for k, v in stages.items()}
     dom = max(stages.items(), key=lambda kv: kv[1][0])[0]
     bytes_alg = {
-        "rm_blend_bwd": 8 * G + 96 * P + 84 * Npx + 2 * (28 * T + 12 * V),
-        "rm_blend_fwd": 8 * G + 96 * P + 8 * Npx + 44 * Npx + T * (16 + 48 + 28 + 128),
+        "rm_blend_bwd": 8 * Gb + 96 * Pb + 84 * Npx + 2 * (28 * T + 12 * V),
+        "rm_blend_fwd": 8 * Gb + 96 * Pb + 8 * Npx + 44 * Npx + T * (16 + 48 + 28 + 128),
         "rm_sort_pairs": 24 * P,
         "rm_project_fwd": 12 * V + 16 * T + 36 * T,
     }
@@ -326,7 +339,9 @@ def run_b200(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"training step: {args.points} mixture points, {T} tets, {W}x{H}, "
                                f"tile {args.tile}, L1 loss", "tets": T, "points": args.points,
-                   "image": [H, W], "tile": args.tile, "pairs": P, "parallelism": f"dp{world} (views)" if world > 1
+                   "image": [H, W], "tile": args.tile, "pairs": P,
+                   "blend_lists": ("8x8-pixel lists built beside the 16x16 ones, %d pairs" % Pb) if stats["fine"]
+                   else "caller's tiles", "parallelism": f"dp{world} (views)" if world > 1
                    else "single view", "l2": "flushed between steps (256 MiB write)",
                    "seed": 2},
         "e2e": e2e, "roofline": roof, "stages_ms": per_stage, "gpu_launches": int(launches),

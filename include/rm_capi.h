@@ -240,6 +240,24 @@ RM_API int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges,
                  float* grad_vertices, float* grad_cell_values, void* workspace,
                  size_t workspace_bytes, int flags, void* stream);
 
+/*
+ * rm_project_fwd plus tile rectangles on a 2^fine_shift times finer grid
+ * (tiles of tile_width >> fine_shift by tile_height >> fine_shift pixels, grid
+ * grid_width << fine_shift by grid_height << fine_shift): rect_fine [T,4] and
+ * tiles_fine [T].  A fine rectangle covers the tet's screen box grown by 1/64
+ * pixel, clipped to its coarse rectangle, so the fine list of a fine tile
+ * holds, in the coarse list's order, every entry of the coarse list that can
+ * reach a pixel of that fine tile.  Blending over the fine lists therefore
+ * yields the image, log T and distortion of blending over the coarse lists
+ * with fewer ray/tet tests (n_contrib then counts fine-list entries).  No
+ * reference counterpart; fine_shift is 1, 2 or 3.
+ */
+RM_API int rm_project_fwd_fine(const int32_t* indices, const float* vertices, int64_t n_tets,
+                               int64_t n_verts, const rm_camera* cam, int fine_shift,
+                               int32_t* tiles_touched, int32_t* rect, float* vs,
+                               float* circumcenter, int32_t* tiles_fine, int32_t* rect_fine,
+                               void* stream);
+
 /* ------------------------------------------------------- batched views -- */
 /*
  * Batched entry points render up to RM_MAX_VIEWS cameras of one mesh in one

@@ -22,23 +22,41 @@ def ceil_div(x, y):
 def vertex_and_tile_shader(indices, vertices, cam, render_grid):
     """Returns (sorted_tetra_idx [P] i32, tile_ranges [G,2] i32, vs_tetra [T,3],
     circumcenter [T,3], mask [T] bool, rect_tile_space [T,4] i32) exactly as
-    the reference (tile_shader_slang.py:24-72)."""
+    the reference (tile_shader_slang.py:24-72).
+
+    For tiles of 16x16 pixels or more, the lists of the same frame on the grid
+    of 8x8-pixel tiles are built as well and attached to the returned
+    ``sorted_tetra_idx`` (attribute ``rm_fine``);
+    ``AlphaBlendTiledRender`` blends over them when it is handed that tensor,
+    which gives the same image with fewer ray/tet tests (see
+    ``rasterizer.FineLists``)."""
+    camst = tcam_to_struct(cam)
+    fs = R.fine_shift_for(camst) if R.fine_lists_enabled() else 0
+    pre = None
+    if fs:
+        with torch.no_grad():
+            tiles, rect, vs, cc, tiles_f, rect_f = R.project_fwd_fine(indices, vertices, camst, fs)
+        pre = (tiles, rect, vs, cc)
     tiles_touched, rect_tile_space, vs_tetra, circumcenter = VertexShader.apply(
-        indices, vertices, cam, render_grid)
+        indices, vertices, cam, render_grid, "cuda", pre)
     with torch.no_grad():
-        camst = tcam_to_struct(cam)
         lists = R.build_tile_lists(tiles_touched, rect_tile_space, vs_tetra, camst)
+        if fs:
+            R.attach_fine_lists(lists.sorted_ids, camst, fs, tiles_f, rect_f, vs_tetra)
     mask = tiles_touched > 0
     return lists.sorted_ids, lists.ranges, vs_tetra, circumcenter, mask, rect_tile_space
 
 
 class VertexShader(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, indices, vertices, tcam, render_grid, device="cuda"):
+    def forward(ctx, indices, vertices, tcam, render_grid, device="cuda", precomputed=None):
         camst = tcam_to_struct(tcam)
         indices = indices.contiguous()
         vertices = vertices.contiguous()
-        tiles_touched, rect_tile_space, vs_tetra, circumcenter = R.project_fwd(indices, vertices, camst)
+        if precomputed is not None:  # outputs of project_fwd_fine for these inputs
+            tiles_touched, rect_tile_space, vs_tetra, circumcenter = precomputed
+        else:
+            tiles_touched, rect_tile_space, vs_tetra, circumcenter = R.project_fwd(indices, vertices, camst)
         ctx.save_for_backward(indices, vertices, tiles_touched)
         ctx.camst = camst
         ctx.render_grid = render_grid
@@ -50,4 +68,4 @@ class VertexShader(torch.autograd.Function):
         indices, vertices, tiles_touched = ctx.saved_tensors
         grad_vertices = R.project_bwd(indices, vertices, ctx.camst, tiles_touched, grad_vs_tetra,
                                       grad_circumcenter)
-        return None, grad_vertices, None, None
+        return None, grad_vertices, None, None, None, None

@@ -23,6 +23,9 @@ __all__ = [
     "ScratchPool",
     "TileLists",
     "project_fwd",
+    "project_fwd_fine",
+    "fine_shift_for",
+    "fine_camera",
     "project_bwd",
     "build_tile_lists",
     "blend_fwd",
@@ -156,6 +159,45 @@ def project_fwd(indices: torch.Tensor, vertices: torch.Tensor, cam: RMCamera):
     return tiles, rect, vs, cc
 
 
+def fine_shift_for(cam: RMCamera) -> int:
+    """log2 of the split factor that brings the camera's tiles to 8x8 pixels
+    (0 when the tiles are already 8 pixels wide or smaller, or not square)."""
+    if cam.tile_width != cam.tile_height or cam.tile_width < 16 or cam.tile_width & (cam.tile_width - 1):
+        return 0
+    return int(cam.tile_width // 8).bit_length() - 1
+
+
+def fine_camera(cam: RMCamera, fine_shift: int) -> RMCamera:
+    """The same camera with tiles 2^fine_shift times smaller on a grid
+    2^fine_shift times larger (the grid covers the same pixels)."""
+    f = 1 << fine_shift
+    out = RMCamera()
+    ctypes.memmove(ctypes.byref(out), ctypes.byref(cam), ctypes.sizeof(RMCamera))
+    out.tile_width, out.tile_height = cam.tile_width // f, cam.tile_height // f
+    out.grid_width, out.grid_height = cam.grid_width * f, cam.grid_height * f
+    return out
+
+
+def project_fwd_fine(indices: torch.Tensor, vertices: torch.Tensor, cam: RMCamera, fine_shift: int):
+    """project_fwd plus the tets' rectangles on the 2^fine_shift times finer
+    tile grid (rm_project_fwd_fine)."""
+    _require_cuda(indices=indices, vertices=vertices)
+    indices = _i32(indices)
+    vertices = _f32(vertices)
+    T = indices.shape[0]
+    dev = vertices.device
+    tiles = torch.empty(T, dtype=torch.int32, device=dev)
+    rect = torch.empty((T, 4), dtype=torch.int32, device=dev)
+    vs = torch.empty((T, 3), dtype=torch.float32, device=dev)
+    cc = torch.empty((T, 3), dtype=torch.float32, device=dev)
+    tiles_f = torch.empty(T, dtype=torch.int32, device=dev)
+    rect_f = torch.empty((T, 4), dtype=torch.int32, device=dev)
+    _call("rm_project_fwd", lambda: C.lib().rm_project_fwd_fine(
+        C.ptr(indices), C.ptr(vertices), T, vertices.shape[0], ctypes.byref(cam), fine_shift, C.ptr(tiles),
+        C.ptr(rect), C.ptr(vs), C.ptr(cc), C.ptr(tiles_f), C.ptr(rect_f), _stream()))
+    return tiles, rect, vs, cc, tiles_f, rect_f
+
+
 def project_bwd(indices, vertices, cam: RMCamera, tiles, grad_vs, grad_cc, grad_vertices=None):
     indices = _i32(indices)
     vertices = _f32(vertices)
@@ -203,6 +245,58 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
     if keep_debug:
         return TileLists(sv, ranges, P, offsets, keys, vals, sk)
     return TileLists(sv, ranges, P)
+
+
+@dataclass
+class FineLists:
+    """Tile lists of one frame on the grid of 8x8-pixel tiles, kept beside the
+    lists of the caller's (larger) tiles.  Every entry of a coarse list that
+    can reach a pixel of a fine tile is in that fine tile's list, in the same
+    order (rm_project_fwd_fine), so blending over the fine lists gives the
+    coarse blend's image, log T and distortion bit for bit; n_contributors
+    then counts fine-list entries, which only the backward pass reads."""
+    shift: int
+    cam: RMCamera  # the fine camera
+    coarse_key: tuple
+    sorted_ids: torch.Tensor
+    ranges: torch.Tensor
+    n_pairs: int
+
+
+_FINE = {"enabled": True}
+
+
+def use_fine_lists(enabled: bool) -> None:
+    """Switch the drop-in's blending over 8x8-pixel lists on or off."""
+    _FINE["enabled"] = bool(enabled)
+
+
+def fine_lists_enabled() -> bool:
+    return _FINE["enabled"]
+
+
+def _cam_key(cam: RMCamera) -> tuple:
+    return (cam.image_height, cam.image_width, cam.tile_height, cam.tile_width, cam.grid_height, cam.grid_width,
+            tuple(cam.world_view), tuple(cam.K), tuple(cam.cam_pos), cam.min_t)
+
+
+def attach_fine_lists(sorted_ids: torch.Tensor, cam: RMCamera, fine_shift: int, tiles_fine, rect_fine, vs,
+                      pool: ScratchPool | None = None) -> FineLists:
+    """Build the fine lists from rm_project_fwd_fine's outputs and attach them
+    to the coarse ``sorted_ids`` tensor (attribute ``rm_fine``)."""
+    camf = fine_camera(cam, fine_shift)
+    fl = build_tile_lists(tiles_fine, rect_fine, vs, camf, pool=pool)
+    fine = FineLists(fine_shift, camf, _cam_key(cam), fl.sorted_ids, fl.ranges, fl.n_pairs)
+    sorted_ids.rm_fine = fine
+    return fine
+
+
+def fine_lists_of(sorted_ids: torch.Tensor, cam: RMCamera) -> FineLists | None:
+    """The fine lists attached to ``sorted_ids`` for this camera, if any."""
+    fine = getattr(sorted_ids, "rm_fine", None)
+    if fine is None or not _FINE["enabled"] or fine.coarse_key != _cam_key(cam):
+        return None
+    return fine
 
 
 _BLEND_FLAGS = {"fwd": 0, "bwd": 0}

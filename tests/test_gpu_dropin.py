@@ -90,3 +90,53 @@ def test_bad_camera_raises(cuda):
     with pytest.raises(ValueError):
         vertex_and_tile_shader(to_dev(mesh.indices), to_dev(mesh.vertices), tcam,
                                RenderGrid(view.height, view.width, 16, 16))
+
+
+def _dropin_step(mesh, view, jitter, fine, tile=16):
+    RMB.install_dropin()
+    from delaunay_rasterization.internal.alphablend_tiled_slang_interp import AlphaBlendTiledRender
+    from delaunay_rasterization.internal.render_grid import RenderGrid
+    from delaunay_rasterization.internal.tile_shader_slang import vertex_and_tile_shader
+    from radiance_meshes_b200 import rasterizer as R
+
+    R.use_fine_lists(fine)
+    try:
+        tcam = view.tcam(device="cuda", tile_size=tile)
+        grid = RenderGrid(view.height, view.width, tile_width=tile, tile_height=tile)
+        verts = to_dev(mesh.vertices).requires_grad_(True)
+        cv = to_dev(mesh.cell_values).requires_grad_(True)
+        idx = to_dev(mesh.indices)
+        sorted_ids, ranges, vs, cc, mask, rect = vertex_and_tile_shader(idx, verts, tcam, grid)
+        assert (getattr(sorted_ids, "rm_fine", None) is not None) == fine
+        img, dist, _ = AlphaBlendTiledRender.apply(sorted_ids, ranges, idx, verts, cv, grid, tcam, jitter, "cuda",
+                                                   mask.to(torch.int32))
+        g = torch.Generator(device="cuda").manual_seed(2)
+        w = torch.randn(img.shape, device="cuda", generator=g)
+        wd = torch.randn(dist.shape, device="cuda", generator=g) * 0.01
+        ((img * w).sum() + (dist * wd).sum()).backward()
+        torch.cuda.synchronize()
+        return sorted_ids, ranges, img.detach(), dist.detach(), verts.grad, cv.grad
+    finally:
+        R.use_fine_lists(True)
+
+
+@pytest.mark.parametrize("scene,tile", [("plain", 16), ("mixture", 16), ("mixture", 32)])
+def test_fine_lists_give_the_coarse_frame(cuda, scene, tile):
+    """Blending over the 8x8-pixel lists reproduces the blend over the
+    caller's 16x16 / 32x32 lists: image and distortion bit for bit, gradients
+    up to FP32 summation order; the lists returned to the caller are the
+    coarse ones."""
+    if scene == "plain":
+        mesh, view = scenes.workload_plain_forward()
+    else:
+        mesh, view = scenes.workload_training_step(n_points=20000, seed=2, height=420, width=649)
+    rng = np.random.default_rng(4)
+    jitter = torch.from_numpy(rng.uniform(0, 1, (view.height, view.width, 2)).astype(np.float32)).cuda()
+    ids_c, rg_c, img_c, dist_c, gv_c, gc_c = _dropin_step(mesh, view, jitter, False, tile)
+    ids_f, rg_f, img_f, dist_f, gv_f, gc_f = _dropin_step(mesh, view, jitter, True, tile)
+    assert torch.equal(ids_c, ids_f) and torch.equal(rg_c, rg_f)
+    assert torch.equal(img_c.view(torch.int32), img_f.view(torch.int32))
+    assert torch.equal(dist_c.view(torch.int32), dist_f.view(torch.int32))
+    assert ids_f.rm_fine.n_pairs > ids_c.shape[0]
+    for a, b in ((gv_f, gv_c), (gc_f, gc_c)):
+        assert float((a - b).norm() / b.norm()) < 1e-5
