@@ -197,10 +197,7 @@ def run_b200(args):
         if world > 1:
             MG.allreduce_grads([v.grad, c.grad])
         stats["P"] = int(sorted_ids.shape[0])
-        fine = R.fine_lists_of(sorted_ids, camst)
-        stats["P_blend"] = fine.n_pairs if fine is not None else stats["P"]
-        stats["G_blend"] = (fine.cam.grid_width * fine.cam.grid_height) if fine is not None else None
-        stats["fine"] = fine is not None
+        stats["fine"] = R.fine_lists_of(sorted_ids, camst)  # read after the timed steps
         return loss, img
 
     for _ in range(args.warmup):
@@ -300,8 +297,9 @@ def run_b200(args):
     P = stats["P"]
     G = grid.grid_width * grid.grid_height
     # the blend walks the 8x8-pixel lists when the drop-in built them
-    Pb = stats["P_blend"]
-    Gb = stats["G_blend"] or G
+    fine = stats["fine"]
+    Pb = fine.n_pairs if fine is not None else P
+    Gb = fine.cam.grid_width * fine.cam.grid_height if fine is not None else G
     value = world * Npx * args.steps / (total_ms * 1e-3) / 1e6
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -340,7 +338,7 @@ def run_b200(args):
         "config": {"workload": f"training step: {args.points} mixture points, {T} tets, {W}x{H}, "
                                f"tile {args.tile}, L1 loss", "tets": T, "points": args.points,
                    "image": [H, W], "tile": args.tile, "pairs": P,
-                   "blend_lists": ("8x8-pixel lists built beside the 16x16 ones, %d pairs" % Pb) if stats["fine"]
+                   "blend_lists": ("8x8-pixel lists built beside the 16x16 ones, %d pairs" % Pb) if fine is not None
                    else "caller's tiles", "parallelism": f"dp{world} (views)" if world > 1
                    else "single view", "l2": "flushed between steps (256 MiB write)",
                    "seed": 2},

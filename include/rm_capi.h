@@ -258,6 +258,23 @@ RM_API int rm_project_fwd_fine(const int32_t* indices, const float* vertices, in
                                float* circumcenter, int32_t* tiles_fine, int32_t* rect_fine,
                                void* stream);
 
+/*
+ * Fine lists from the sorted coarse lists: splits each coarse tile's list
+ * (sorted_ids, ranges [G,2]) in order into the lists of its 2^fine_shift x
+ * 2^fine_shift fine tiles, using rect_fine [T,4] of rm_project_fwd_fine.  The
+ * result equals emitting, sorting and ranging the fine pairs: fine_ids
+ * (capacity entries; 4^fine_shift * P always suffices) and fine_ranges
+ * [G * 4^fine_shift, 2] on the fine grid, *total_dev = fine pair count.
+ * Workspace: rm_fine_lists_workspace_size(fine tiles), 256-byte aligned.  No
+ * reference counterpart.
+ */
+RM_API size_t rm_fine_lists_workspace_size(int64_t n_fine_tiles);
+RM_API int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges,
+                         const int32_t* rect_fine, const rm_camera* cam, int fine_shift,
+                         int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
+                         int64_t* total_dev, void* workspace, size_t workspace_bytes,
+                         void* stream);
+
 /* ------------------------------------------------------- batched views -- */
 /*
  * Batched entry points render up to RM_MAX_VIEWS cameras of one mesh in one

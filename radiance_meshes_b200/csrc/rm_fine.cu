@@ -1,0 +1,145 @@
+// rm_fine.cu - tile lists on a finer grid, derived from the sorted lists.
+//
+// Given the sorted lists of the caller's tiles and each tet's rectangle on a
+// grid 2^fine_shift times finer (rm_project_fwd_fine), the list of a fine tile
+// is the subsequence of its coarse tile's list whose fine rectangle covers it.
+// Emitting fine pairs and sorting them again would reproduce exactly that
+// order (depth key, then tet id), so instead each coarse list is split once,
+// in order, into its 4 (or 16, 64) fine lists: a counting pass, a scan of the
+// counts in fine-tile order, and a writing pass.  One CTA walks one coarse
+// list in chunks of 256 entries; the ranks inside a chunk come from warp
+// ballots per fine tile.  No reference counterpart (the reference blends over
+// the coarse lists directly).
+#include "rm_internal.cuh"
+
+namespace rm {
+namespace {
+
+constexpr int kFineThreads = 256;
+constexpr int kFineWarps = kFineThreads / 32;
+constexpr int kMaxQuads = 64;  // fine tiles per coarse tile (fine_shift <= 3)
+
+__device__ __forceinline__ bool covers(int4 fr, int fx, int fy) {
+    return fr.x <= fx && fx < fr.z && fr.y <= fy && fy < fr.w;
+}
+
+// WRITE = false: counts[fine id] = entries of the coarse list covering the
+// fine tile.  WRITE = true: write the fine lists at their scanned offsets and
+// the fine ranges.
+template <bool WRITE>
+__global__ void __launch_bounds__(kFineThreads) fine_lists_kernel(
+    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const int4* __restrict__ rect_fine,
+    int grid_w, int f, int32_t* __restrict__ counts, const int32_t* __restrict__ incl,
+    int32_t* __restrict__ fine_ids, int64_t capacity, int2* __restrict__ fine_ranges, uint32_t* status) {
+    __shared__ uint32_t wtot[kFineWarps][kMaxQuads];
+    __shared__ uint32_t run[kMaxQuads];
+    __shared__ int32_t start[kMaxQuads];
+    const int t = blockIdx.x;
+    const int tx = t % grid_w, ty = t / grid_w;
+    const int Q = f * f;
+    const int fgw = grid_w * f;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    if (threadIdx.x < Q) {
+        run[threadIdx.x] = 0u;
+        if (WRITE) {
+            const int q = threadIdx.x;
+            const int fid = (ty * f + q / f) * fgw + tx * f + q % f;
+            start[q] = __ldg(incl + fid) - __ldg(counts + fid);
+        }
+    }
+    __syncthreads();
+    const int2 r = __ldg(ranges + t);
+    for (int base = r.x; base < r.y; base += kFineThreads) {
+        const int e = base + (int)threadIdx.x;
+        int4 fr = {0, 0, 0, 0};
+        int32_t g = 0;
+        if (e < r.y) {
+            g = __ldg(ids + e);
+            fr = __ldg(rect_fine + g);
+        }
+        for (int q = 0; q < Q; ++q) {
+            const bool in = covers(fr, tx * f + q % f, ty * f + q / f);
+            const unsigned bal = __ballot_sync(0xffffffffu, in);
+            if (lane == 0) wtot[warp][q] = __popc(bal);
+        }
+        __syncthreads();
+        if (WRITE) {
+            for (int q = 0; q < Q; ++q) {
+                const bool in = covers(fr, tx * f + q % f, ty * f + q / f);
+                const unsigned bal = __ballot_sync(0xffffffffu, in);
+                if (in) {
+                    uint32_t pos = run[q] + __popc(bal & lt);
+                    for (int w = 0; w < warp; ++w) pos += wtot[w][q];
+                    const int64_t o = (int64_t)start[q] + pos;
+                    if (o < capacity) fine_ids[o] = g;
+                    else if (status) atomicOr(status, RM_STATUS_CAPACITY);
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < Q) {
+            uint32_t s = 0;
+            for (int w = 0; w < kFineWarps; ++w) s += wtot[w][threadIdx.x];
+            run[threadIdx.x] += s;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < Q) {
+        const int q = threadIdx.x;
+        const int fid = (ty * f + q / f) * fgw + tx * f + q % f;
+        if (WRITE) fine_ranges[fid] = make_int2(start[q], start[q] + (int)run[q]);
+        else counts[fid] = (int32_t)run[q];
+    }
+}
+
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+}  // namespace
+}  // namespace rm
+
+extern "C" {
+
+size_t rm_fine_lists_workspace_size(int64_t n_fine_tiles) {
+    const int64_t n = n_fine_tiles > 0 ? n_fine_tiles : 1;
+    return 2 * rm::align256((size_t)n * 4) + 256 + rm_scan_workspace_size(n);
+}
+
+int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* rect_fine, const rm_camera* cam,
+                  int fine_shift, int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges, int64_t* total_dev,
+                  void* workspace, size_t workspace_bytes, void* stream) {
+    int rc = rm_host::check_cam(cam);
+    if (rc) return rc;
+    if (fine_shift < 1 || fine_shift > 3) return rm_host::fail(RM_EINVAL, "rm_fine_lists: fine_shift %d", fine_shift);
+    if (capacity < 0) return rm_host::fail(RM_EINVAL, "rm_fine_lists: negative capacity");
+    const int f = 1 << fine_shift;
+    const int64_t G = (int64_t)cam->grid_width * cam->grid_height;
+    const int64_t Gf = G * f * f;
+    if (Gf >= (int64_t)INT32_MAX) return rm_host::fail(RM_EINVAL, "rm_fine_lists: too many tiles");
+    if (!ranges || !rect_fine || !fine_ranges || !total_dev || !workspace || (capacity > 0 && (!sorted_ids || !fine_ids)))
+        return rm_host::fail(RM_EINVAL, "rm_fine_lists: NULL pointer");
+    if (((uintptr_t)rect_fine & 15) || ((uintptr_t)ranges & 7) || ((uintptr_t)fine_ranges & 7) ||
+        ((uintptr_t)workspace & 255))
+        return rm_host::fail(RM_EINVAL, "rm_fine_lists: misaligned rect_fine / ranges / workspace");
+    if (workspace_bytes < rm_fine_lists_workspace_size(Gf))
+        return rm_host::fail(RM_EINVAL, "rm_fine_lists: workspace %zu < %zu bytes", workspace_bytes,
+                             rm_fine_lists_workspace_size(Gf));
+    if (G == 0) return RM_OK;
+    char* p = (char*)workspace;
+    int32_t* counts = (int32_t*)p;
+    int32_t* incl = (int32_t*)(p + rm::align256((size_t)Gf * 4));
+    char* scan_ws = p + 2 * rm::align256((size_t)Gf * 4) + 256;
+    uint32_t* status = (uint32_t*)scan_ws;  // the scan workspace's status word
+    cudaStream_t s = (cudaStream_t)stream;
+    rm::fine_lists_kernel<false><<<(unsigned)G, rm::kFineThreads, 0, s>>>(
+        sorted_ids, (const int2*)ranges, (const int4*)rect_fine, cam->grid_width, f, counts, nullptr, nullptr, 0,
+        nullptr, nullptr);
+    if ((rc = rm_host::check_launch("rm_fine_lists (count)"))) return rc;
+    if ((rc = rm_scan_tiles(counts, Gf, incl, total_dev, scan_ws, rm_scan_workspace_size(Gf), stream))) return rc;
+    rm::fine_lists_kernel<true><<<(unsigned)G, rm::kFineThreads, 0, s>>>(
+        sorted_ids, (const int2*)ranges, (const int4*)rect_fine, cam->grid_width, f, counts, incl, fine_ids, capacity,
+        (int2*)fine_ranges, status);
+    return rm_host::check_launch("rm_fine_lists (write)");
+}
+
+}  // extern "C"

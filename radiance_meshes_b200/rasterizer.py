@@ -252,15 +252,20 @@ class FineLists:
     """Tile lists of one frame on the grid of 8x8-pixel tiles, kept beside the
     lists of the caller's (larger) tiles.  Every entry of a coarse list that
     can reach a pixel of a fine tile is in that fine tile's list, in the same
-    order (rm_project_fwd_fine), so blending over the fine lists gives the
-    coarse blend's image, log T and distortion bit for bit; n_contributors
-    then counts fine-list entries, which only the backward pass reads."""
+    order (rm_project_fwd_fine, rm_fine_lists), so blending over the fine
+    lists gives the coarse blend's image, log T and distortion bit for bit;
+    n_contributors then counts fine-list entries, which only the backward pass
+    reads."""
     shift: int
     cam: RMCamera  # the fine camera
     coarse_key: tuple
-    sorted_ids: torch.Tensor
+    sorted_ids: torch.Tensor  # capacity entries; the first n_pairs are used
     ranges: torch.Tensor
-    n_pairs: int
+    total: torch.Tensor  # [1] int64 on the device
+
+    @property
+    def n_pairs(self) -> int:
+        return int(self.total.item())
 
 
 _FINE = {"enabled": True}
@@ -280,13 +285,26 @@ def _cam_key(cam: RMCamera) -> tuple:
             tuple(cam.world_view), tuple(cam.K), tuple(cam.cam_pos), cam.min_t)
 
 
-def attach_fine_lists(sorted_ids: torch.Tensor, cam: RMCamera, fine_shift: int, tiles_fine, rect_fine, vs,
-                      pool: ScratchPool | None = None) -> FineLists:
-    """Build the fine lists from rm_project_fwd_fine's outputs and attach them
-    to the coarse ``sorted_ids`` tensor (attribute ``rm_fine``)."""
+def attach_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCamera, fine_shift: int,
+                      rect_fine: torch.Tensor, pool: ScratchPool | None = None) -> FineLists:
+    """Split the sorted coarse lists into the fine lists (rm_fine_lists, no
+    host synchronisation) and attach them to ``sorted_ids`` (attribute
+    ``rm_fine``)."""
+    pool = pool or _POOL
+    dev = sorted_ids.device
     camf = fine_camera(cam, fine_shift)
-    fl = build_tile_lists(tiles_fine, rect_fine, vs, camf, pool=pool)
-    fine = FineLists(fine_shift, camf, _cam_key(cam), fl.sorted_ids, fl.ranges, fl.n_pairs)
+    Gf = camf.grid_width * camf.grid_height
+    cap = max(int(sorted_ids.shape[0]) << (2 * fine_shift), 1)
+    fine_ids = torch.empty(cap, dtype=torch.int32, device=dev)
+    fine_ranges = torch.empty((Gf, 2), dtype=torch.int32, device=dev)
+    total = torch.empty(1, dtype=torch.int64, device=dev)
+    L = C.lib()
+    ws_n = L.rm_fine_lists_workspace_size(Gf)
+    ws = pool.get("fine", ws_n, dev)
+    _call("rm_fine_lists", lambda: L.rm_fine_lists(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(rect_fine),
+                                                   ctypes.byref(cam), fine_shift, cap, C.ptr(fine_ids),
+                                                   C.ptr(fine_ranges), C.ptr(total), C.ptr(ws), ws_n, _stream()))
+    fine = FineLists(fine_shift, camf, _cam_key(cam), fine_ids, fine_ranges, total)
     sorted_ids.rm_fine = fine
     return fine
 

@@ -138,5 +138,6 @@ def test_fine_lists_give_the_coarse_frame(cuda, scene, tile):
     assert torch.equal(img_c.view(torch.int32), img_f.view(torch.int32))
     assert torch.equal(dist_c.view(torch.int32), dist_f.view(torch.int32))
     assert ids_f.rm_fine.n_pairs > ids_c.shape[0]
+    assert ids_f.rm_fine.sorted_ids.shape[0] >= ids_f.rm_fine.n_pairs
     for a, b in ((gv_f, gv_c), (gc_f, gc_c)):
         assert float((a - b).norm() / b.norm()) < 1e-5
