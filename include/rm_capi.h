@@ -190,8 +190,20 @@ RM_API int rm_tile_ranges(const int64_t* sorted_keys, int64_t n, const int64_t* 
  * heavy-first tile order of the work queue (4 B per tile) and queue tickets.
  */
 RM_API size_t rm_blend_workspace_size(int64_t n_tets, int64_t n_tiles);
+/* Extra workspace bytes for RM_BLEND_HIT_MASKS over n_pairs list entries in
+ * n_tiles tiles of tile_pixels pixels (4 bytes per 32 entries per pixel). */
+RM_API size_t rm_blend_hit_mask_bytes(int64_t n_pairs, int64_t n_tiles, int tile_pixels);
 
 #define RM_BLEND_REUSE_RECORDS 0x1  /* workspace already holds this frame's records */
+/* Hit masks: with this flag on rm_blend_fwd and rm_blend_bwd (same lists, same
+ * workspace, 64-pixel work items) the forward stores, per list entry and work
+ * item, which pixels it counted as hits, and the backward revisits only those,
+ * skipping the ray/tet tests of the misses.  The workspace must extend
+ * rm_blend_hit_mask_bytes(P, G, tile pixels) beyond rm_blend_workspace_size;
+ * entries past that room are tested as without masks.  A forward without the
+ * flag (or with 16-pixel items) marks the masks invalid, and the backward then
+ * tests every entry. */
+#define RM_BLEND_HIT_MASKS 0x2
 /* flags bits 8..15: log2 of the pixels per work item strip (16 or 64; 0 = 64) */
 #define RM_BLEND_STRIP_SHIFT 8
 #define RM_BLEND_STRIP(log2_pixels) ((log2_pixels) << RM_BLEND_STRIP_SHIFT)

@@ -24,6 +24,7 @@ RM_STATUS_CAPACITY = 0x4
 RM_STATUS_QUEUE_TIMEOUT = 0x8
 
 RM_BLEND_REUSE_RECORDS = 0x1
+RM_BLEND_HIT_MASKS = 0x2
 RM_BLEND_STRIP_SHIFT = 8
 RM_BLEND_HEAVY_SHIFT = 16
 RM_BLEND_PAIR_CTAS_SHIFT = 20
@@ -59,6 +60,7 @@ SIGNATURES = {
     "rm_sort_pairs": (ctypes.c_int, [vp, vp, i64, vp, ctypes.c_int, vp, vp, vp, sz, vp]),
     "rm_tile_ranges": (ctypes.c_int, [vp, i64, vp, vp, i64, vp]),
     "rm_blend_workspace_size": (sz, [i64, i64]),
+    "rm_blend_hit_mask_bytes": (sz, [i64, i64, ctypes.c_int]),
     "rm_blend_fwd": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, vp, vp, vp, vp, sz,
                                     ctypes.c_int, vp]),
     "rm_blend_bwd": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, vp, vp, vp, vp, vp,

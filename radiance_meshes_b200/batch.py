@@ -84,7 +84,8 @@ class BatchedRasterizer:
 
     def __init__(self, indices: torch.Tensor, vertices: torch.Tensor, cell_values: torch.Tensor,
                  views: ViewBatch, jitter: torch.Tensor | None = None, capacity: int | None = None,
-                 fwd_flags: int = 0, bwd_flags: int = 0, records: torch.Tensor | None = None):
+                 fwd_flags: int = 0, bwd_flags: int = 0, records: torch.Tensor | None = None,
+                 hit_masks: bool = True):
         for name, t in (("indices", indices), ("vertices", vertices), ("cell_values", cell_values)):
             if not t.is_cuda:
                 raise RuntimeError(f"{name} must be a CUDA tensor (the rasterizer has no CPU path)")
@@ -95,6 +96,9 @@ class BatchedRasterizer:
         self.indices, self.vertices, self.cell_values = indices, vertices, cell_values
         self.views = views
         self.fwd_flags, self.bwd_flags = int(fwd_flags), int(bwd_flags)
+        # hit masks (RM_BLEND_HIT_MASKS): the forward records its hits so the
+        # backward skips the misses; forward-only users turn them off
+        self.hit_masks = bool(hit_masks)
         dev = vertices.device
         self.device = dev
         T, n = indices.shape[0], views.n
@@ -113,7 +117,8 @@ class BatchedRasterizer:
         # every batch on it; without them each forward packs its own into the workspace
         self.records = records
         ws_tets = 0 if records is not None else T
-        self.blend_ws = torch.empty(L.rm_blend_workspace_size(ws_tets, views.n_tiles), dtype=torch.uint8, device=dev)
+        self._ws_base = int(L.rm_blend_workspace_size(ws_tets, views.n_tiles))
+        self.blend_ws = None  # sized with the pair capacity (hit masks) in _alloc_pairs
         Npx = views.n_pixels
         self.jitter = jitter if jitter is not None else torch.full((Npx, 2), 0.5, device=dev)
         self.img = torch.empty((Npx, 4), dtype=torch.float32, device=dev)
@@ -156,6 +161,11 @@ class BatchedRasterizer:
         self.sorted_keys = torch.empty(capacity, dtype=torch.int64, device=dev)
         self.sorted_ids = torch.empty(capacity, dtype=torch.int32, device=dev)
         self.sort_ws = torch.empty(C.lib().rm_sort_workspace_size(capacity), dtype=torch.uint8, device=dev)
+        ws = self._ws_base
+        if self.hit_masks:
+            c0 = self.views.cams[0]
+            ws += int(C.lib().rm_blend_hit_mask_bytes(capacity, self.views.n_tiles, c0.tile_width * c0.tile_height))
+        self.blend_ws = torch.empty(ws, dtype=torch.uint8, device=dev)
         self.graph = None
 
     def measure_pairs(self) -> int:
@@ -199,7 +209,7 @@ class BatchedRasterizer:
                                      C.ptr(self.vertices), C.ptr(self.cell_values), self.T, self.V,
                                      C.ptr(self.tiles_any), C.ptr(self.jitter), v.array, v.n, C.ptr(self.img),
                                      C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.records), C.ptr(self.blend_ws), self.blend_ws.numel(),
-                                     self.fwd_flags, s))
+                                     self.fwd_flags | (C.RM_BLEND_HIT_MASKS if self.hit_masks else 0), s))
 
     def _blend_bwd(self):
         L, s, v = C.lib(), C.stream_handle(), self.views
@@ -210,7 +220,8 @@ class BatchedRasterizer:
                                      C.ptr(self.tiles_any), C.ptr(self.jitter), v.array, v.n, C.ptr(self.img),
                                      C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.grad_img), C.ptr(self.grad_dist),
                                      C.ptr(self.grad_vertices), C.ptr(self.grad_cell_values), C.ptr(self.records), C.ptr(self.blend_ws),
-                                     self.blend_ws.numel(), self.bwd_flags | C.RM_BLEND_REUSE_RECORDS, s),
+                                     self.blend_ws.numel(), self.bwd_flags | C.RM_BLEND_REUSE_RECORDS |
+                                     (C.RM_BLEND_HIT_MASKS if self.hit_masks else 0), s),
                 "rm_blend_bwd_multi")
 
     # ---------------------------------------------------------------- API --

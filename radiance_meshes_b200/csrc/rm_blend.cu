@@ -233,6 +233,35 @@ struct WarpShape {
 // Work queue shared by the kernels of one pass.  order[] lists the tiles
 // heaviest first; info[0] is the number of heavy tiles (the first entries of
 // order[]), which go to the pair kernel, the rest to the dense kernel.
+// Hit masks written by the forward and read by the backward
+// (RM_BLEND_HIT_MASKS; 64-pixel work items only).  A tile's list is cut into
+// blocks of 32 entries counted from its start; pixel p of work item `sub`
+// keeps, for block k of global tile t whose list starts at position x, one
+// word at mask_word(t, x, k, sub, subs, p) whose bit i says whether entry
+// x + 32k + i was a hit for that pixel before its termination.  Block ids
+// floor(x / 32) + k + t are distinct over all tiles, so the words never
+// overlap; a pixel's words of consecutive blocks are 64 words apart, and the
+// 64 pixels of an item are contiguous (coalesced stores and loads).  Words at
+// or beyond cap do not exist: the entries they would describe are tested.
+__device__ __forceinline__ int64_t mask_word(int gtile, int x, int k, int sub, int subs, int p) {
+    return (((int64_t)(x >> 5) + k + gtile) * subs + sub) * 64 + p;
+}
+
+struct HitMasks {
+    uint32_t* words;  // nullptr: no masks
+    int64_t cap;      // words
+    const uint32_t* header;  // kMaskValid: this pass's forward wrote masks with 64-pixel items
+    __device__ __forceinline__ bool has(int64_t m) const { return words != nullptr && m < cap; }
+};
+
+constexpr uint32_t kMaskValid = 0x6d61736bu;
+
+// The masks a kernel may use: none unless the header says the forward wrote them.
+__device__ __forceinline__ HitMasks live_masks(HitMasks hm) {
+    if (hm.words && (!hm.header || __ldcg(hm.header) != kMaskValid)) hm.words = nullptr;
+    return hm;
+}
+
 struct Queue {
     const int32_t* order;
     const int32_t* info;
@@ -240,6 +269,7 @@ struct Queue {
     int G;
     int subs;  // strips per tile
     bool heavy;
+    HitMasks hm;
 };
 
 __device__ __forceinline__ int queue_items(const Queue& q) {
@@ -258,6 +288,17 @@ __device__ __forceinline__ int next_item(const Queue& q, int* s_item) {
     const int item = *s_item;
     __syncthreads();
     return item;
+}
+
+// Stores the hit bits of one batch (B a multiple of 32, starting 32-aligned
+// relative to the list start) for pixel p: one word per 32 entries.
+__device__ __forceinline__ void write_masks(const HitMasks& hm, uint64_t hb, int gtile, int x, int base, int n,
+                                            int sub, int subs, int p) {
+    const int k0 = (base - x) >> 5;
+    for (int w = 0; w * 32 < n; ++w) {
+        const int64_t i = mask_word(gtile, x, k0 + w, sub, subs, p);
+        if (i < hm.cap) __stcg(hm.words + i, (uint32_t)(hb >> (32 * w)));
+    }
 }
 
 // One hit folded into the pixel state (update_alpha_out,
@@ -319,7 +360,9 @@ __device__ __forceinline__ void fwd_dense_item(int tile, int sub, const int32_t*
                                                const int2* __restrict__ ranges, const float4* __restrict__ recs,
                                                const float2* __restrict__ jitter, const rm_camera& cam,
                                                float4* __restrict__ out_img, float* __restrict__ out_dist,
-                                               int32_t* __restrict__ out_nc, FwdDenseSmem<B>& S) {
+                                               int32_t* __restrict__ out_nc, FwdDenseSmem<B>& S,
+                                               const HitMasks& hm, int subs, int gtile) {
+    constexpr bool kMasks = NT == 64 && B % 32 == 0;
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
     int lx, ly;
     strip_pixel<NT>(cam, sub, (int)threadIdx.x, lx, ly);
@@ -345,17 +388,20 @@ __device__ __forceinline__ void fwd_dense_item(int tile, int sub, const int32_t*
                 S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
             }
             __syncthreads();
+            uint64_t hb = 0;  // bit j: entry j of the batch was a hit
             if (__any_sync(WarpShape<NT>::kMask, active)) {
                 for (int j = 0; j < n; ++j) {
                     if (!active) break;
                     ++nc;
                     const EntryResult r = eval_entry(S.srec[j], o, d);
                     if (r.a > 0.f) {
+                        hb |= 1ull << j;
                         fold_hit(st, r.a, S.srec[j][0].w, r.m1, r.d4, r.rgb);
                         if (st.logT < kTermLogT) active = false;
                     }
                 }
             }
+            if (kMasks && hm.words) write_masks(hm, hb, gtile, rg.x, base, n, sub, subs, (int)threadIdx.x);
             if (!__syncthreads_or(active)) break;
         }
     }
@@ -404,8 +450,10 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
                                          const int2* __restrict__ ranges, const float4* __restrict__ recs,
                                          const float2* __restrict__ jitter, const rm_camera& cam,
                                          float4* __restrict__ out_img, float* __restrict__ out_dist,
-                                         int32_t* __restrict__ out_nc, FwdPairSmem<PX, B>& S) {
+                                         int32_t* __restrict__ out_nc, FwdPairSmem<PX, B>& S,
+                                         const HitMasks& hm, int subs, int gtile) {
     static_assert(PX <= 64 && NT >= 64, "a lane evaluates at most two slots");
+    constexpr bool kMasks = PX == 64 && B % 32 == 0;
     constexpr unsigned kOwnMask = WarpShape<PX>::kMask;
     constexpr int kWarps = NT / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -479,6 +527,7 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
         }
         __syncthreads();
         // Fold in list order; the hit tests of four entries are read ahead.
+        uint64_t hb = 0;  // bit j: entry j of the batch was a hit for this owner's pixel
         for (int j0 = 0; active && j0 < n; j0 += 4) {
             float a4[4];
 #pragma unroll
@@ -489,12 +538,14 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
                 if (!active || j >= n) break;
                 ++nc;
                 if (a4[u] > 0.f) {
+                    hb |= 1ull << j;
                     const float rgb[3] = {S.res[3][j][slot], S.res[4][j][slot], S.res[5][j][slot]};
                     fold_hit(st, a4[u], S.srec[j][0].w, S.res[1][j][slot], S.res[2][j][slot], rgb);
                     if (st.logT < kTermLogT) active = false;
                 }
             }
         }
+        if (kMasks && owner && hm.words) write_masks(hm, hb, gtile, rg.x, base, n, sub, subs, tid);
         n_active = __syncthreads_count(active);
     }
     if (inside) {
@@ -514,6 +565,7 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 1024 / NT : 32)) blend_fwd_den
     __shared__ FwdDenseSmem<B> S;
     __shared__ int s_item;
     const int n_items = queue_items(q);
+    const HitMasks hm = live_masks(q.hm);
     for (;;) {
         const int item = next_item(q, &s_item);
         if (item >= n_items) return;
@@ -521,7 +573,7 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 1024 / NT : 32)) blend_fwd_den
         const int tb = views.tile_base(v);
         const int64_t pb = views.pixel_base(v);
         fwd_dense_item<NT, B>(t - tb, item % q.subs, ids, ranges + tb, recs, jitter + pb, views.camera(v),
-                              out_img + pb, out_dist + 5 * pb, out_nc + pb, S);
+                              out_img + pb, out_dist + 5 * pb, out_nc + pb, S, hm, q.subs, t);
     }
 }
 
@@ -534,6 +586,7 @@ __global__ void __launch_bounds__(NT, 768 / NT) blend_fwd_pair_kernel(
     FwdPairSmem<PX, B>& S = *reinterpret_cast<FwdPairSmem<PX, B>*>(fwd_smem_raw);
     __shared__ int s_item;
     const int n_items = queue_items(q);
+    const HitMasks hm = live_masks(q.hm);
     for (;;) {
         const int item = next_item(q, &s_item);
         if (item >= n_items) return;
@@ -541,7 +594,7 @@ __global__ void __launch_bounds__(NT, 768 / NT) blend_fwd_pair_kernel(
         const int tb = views.tile_base(v);
         const int64_t pb = views.pixel_base(v);
         fwd_pair_item<PX, NT, B>(t - tb, item % q.subs, ids, ranges + tb, recs, jitter + pb, views.camera(v),
-                                 out_img + pb, out_dist + 5 * pb, out_nc + pb, S);
+                                 out_img + pb, out_dist + 5 * pb, out_nc + pb, S, hm, q.subs, t);
     }
 }
 
@@ -551,7 +604,8 @@ __global__ void __launch_bounds__(NT, 768 / NT) blend_fwd_pair_kernel(
 // least 2^10 entries (info[0] = their count), and resets the queue tickets.
 __global__ void __launch_bounds__(1024) order_kernel(const int2* __restrict__ ranges, int G,
                                                      int32_t* __restrict__ order, int32_t* info,
-                                                     uint32_t* tickets, int heavy_shift) {
+                                                     uint32_t* tickets, int heavy_shift, uint32_t* mask_header,
+                                                     uint32_t mask_state) {
     // Warp-aggregated counting: lanes that share a bucket elect one leader
     // (match_any) for the shared atomic, and the list-length sum and the
     // non-empty count are reduced per warp before one shared update each.
@@ -596,6 +650,7 @@ __global__ void __launch_bounds__(1024) order_kernel(const int2* __restrict__ ra
         for (int b = 32; b >= b_thr; --b) heavy += (int)cnt[b];
         info[0] = heavy;
         for (int k = 0; k < 4; ++k) tickets[k] = 0u;
+        if (mask_header) *mask_header = mask_state;
     }
     __syncthreads();
     const unsigned lt = (1u << lane) - 1u;
@@ -802,8 +857,9 @@ __device__ __forceinline__ void bwd_dense_item(
     const float4* __restrict__ recs, const int4* __restrict__ indices, const float2* __restrict__ jitter,
     const rm_camera& cam, const float4* __restrict__ img, const float* __restrict__ dist,
     const int32_t* __restrict__ ncs, const float4* __restrict__ gimg, const float* __restrict__ gdist,
-    float* __restrict__ gverts, float* __restrict__ gcv, BwdDenseSmem<NT, B>& S) {
+    float* __restrict__ gverts, float* __restrict__ gcv, BwdDenseSmem<NT, B>& S, const HitMasks& hm, int subs, int gtile) {
     constexpr unsigned kMask = WarpShape<NT>::kMask;
+    constexpr bool kMasks = NT == 64;
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
     int lx, ly;
     strip_pixel<NT>(cam, sub, (int)threadIdx.x, lx, ly);
@@ -837,12 +893,23 @@ __device__ __forceinline__ void bwd_dense_item(
     for (int w = 0; w < WarpShape<NT>::kWarps; ++w) tile_max = max(tile_max, S.smax[w]);
     const int2 rg = __ldg(ranges + tile);
     const int end = min(rg.y, rg.x + tile_max);
-    for (int top = end; top > rg.x; top -= B) {
-        const int lo = max(rg.x, top - B);
+    // batches aligned to multiples of B from the list start, so that one spans
+    // at most two 32-entry mask blocks (B <= 64)
+    for (int top = end, lo; top > rg.x; top = lo) {
+        lo = rg.x + ((top - 1 - rg.x) / B) * B;
         const int n = top - lo;
         __syncthreads();
         for (int k = threadIdx.x; k < n; k += NT) S.sid[k] = __ldg(ids + lo + k);
         for (int k = threadIdx.x; k < n * kNGrad; k += NT) (&S.sacc[0][0])[k] = 0.f;
+        // this pixel's hit bits of the (at most two) 32-entry blocks the batch spans
+        const int kb0 = (lo - rg.x) >> 5, kb1 = (top - 1 - rg.x) >> 5;
+        uint32_t hw0 = 0xffffffffu, hw1 = 0xffffffffu;
+        if (kMasks && hm.words) {
+            const int64_t i0 = mask_word(gtile, rg.x, kb0, sub, subs, (int)threadIdx.x);
+            const int64_t i1 = mask_word(gtile, rg.x, kb1, sub, subs, (int)threadIdx.x);
+            if (i0 < hm.cap) hw0 = __ldcg(hm.words + i0);
+            if (i1 < hm.cap) hw1 = __ldcg(hm.words + i1);
+        }
         __syncthreads();
         for (int k = threadIdx.x; k < n * kRecFloat4; k += NT) {
             const int j = k >> 3, c = k & 7;
@@ -851,7 +918,9 @@ __device__ __forceinline__ void bwd_dense_item(
         __syncthreads();
         for (int jj = n - 1; jj >= 0; --jj) {
             const int off = lo + jj - rg.x;
-            const bool act = inside && off < nc;
+            // with the forward's masks, only its hits are revisited
+            const uint32_t hw = (off >> 5) == kb0 ? hw0 : hw1;
+            const bool act = inside && off < nc && ((hw >> (off & 31)) & 1u);
             if (!__any_sync(kMask, act)) continue;
             const float4* q = S.srec[jj];
             float gl[kNGrad];
@@ -1112,6 +1181,7 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 512 / NT : 16)) blend_bwd_dens
     __shared__ BwdDenseSmem<NT, B> S;
     __shared__ int s_item;
     const int n_items = queue_items(q);
+    const HitMasks hm = live_masks(q.hm);
     for (;;) {
         const int item = next_item(q, &s_item);
         if (item >= n_items) return;
@@ -1120,7 +1190,7 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 512 / NT : 16)) blend_bwd_dens
         const int64_t pb = views.pixel_base(v);
         bwd_dense_item<NT, B>(t - tb, item % q.subs, ids, ranges + tb, recs, indices, jitter + pb, views.camera(v),
                               img + pb, dist + 5 * pb, ncs + pb, gimg + pb, gdist ? gdist + 5 * pb : nullptr,
-                              gverts, gcv, S);
+                              gverts, gcv, S, hm, q.subs, t);
     }
 }
 
@@ -1152,6 +1222,9 @@ struct BlendWs {
     int32_t* order;
     int32_t* info;
     uint32_t* tickets;
+    uint32_t* mask_header;  // nullptr: the workspace has no room for hit masks
+    uint32_t* mask_words;
+    int64_t mask_cap;
 };
 
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
@@ -1162,11 +1235,21 @@ size_t blend_ws_bytes(int64_t n_tets, int64_t n_tiles) {
     return rec + ord + 256;
 }
 
-BlendWs blend_ws(void* base, int64_t n_tets, int64_t n_tiles) {
+// Hit masks, when the caller's workspace is larger than blend_ws_bytes: a
+// 256-byte header, then the mask words (mask_word).
+BlendWs blend_ws(void* base, int64_t n_tets, int64_t n_tiles, size_t workspace_bytes) {
     char* p = (char*)base;
     const size_t rec = align256((size_t)(n_tets > 0 ? n_tets : 1) * kRecFloat4 * sizeof(float4));
     const size_t ord = align256((size_t)(n_tiles > 0 ? n_tiles : 1) * sizeof(int32_t));
-    return {(float4*)p, (int32_t*)(p + rec), (int32_t*)(p + rec + ord), (uint32_t*)(p + rec + ord + 64)};
+    BlendWs w = {(float4*)p, (int32_t*)(p + rec), (int32_t*)(p + rec + ord), (uint32_t*)(p + rec + ord + 64),
+                 nullptr, nullptr, 0};
+    const size_t end = rec + ord + 256;
+    if (workspace_bytes >= end + 256 + 64 * sizeof(uint32_t)) {
+        w.mask_header = (uint32_t*)(p + end);
+        w.mask_words = (uint32_t*)(p + end + 256);
+        w.mask_cap = (int64_t)((workspace_bytes - end - 256) / sizeof(uint32_t));
+    }
+    return w;
 }
 
 // Persistent grid: as many CTAs as fit on the device at once (cached per
@@ -1238,8 +1321,10 @@ int side_stream(cudaStream_t caller, SideStream** out) {
     return RM_OK;
 }
 
-int launch_order(const int32_t* ranges, int G, const BlendWs& w, int heavy_shift, cudaStream_t s) {
-    order_kernel<<<1, 1024, 0, s>>>((const int2*)ranges, G, w.order, w.info, w.tickets, heavy_shift);
+int launch_order(const int32_t* ranges, int G, const BlendWs& w, int heavy_shift, cudaStream_t s,
+                 uint32_t* mask_header = nullptr, uint32_t mask_state = 0u) {
+    order_kernel<<<1, 1024, 0, s>>>((const int2*)ranges, G, w.order, w.info, w.tickets, heavy_shift, mask_header,
+                                    mask_state);
     return rm_host::check_launch("rm_blend order");
 }
 
@@ -1259,6 +1344,7 @@ int join_side(cudaStream_t s, SideStream* side) {
 struct Tuning {
     int heavy_shift;       // heavy tiles: list-length bucket >= bucket(mean) + heavy_shift; 1: all tiles
     int pair_ctas_per_sm;  // resident CTAs of the pair kernel per SM
+    bool hit_masks;        // RM_BLEND_HIT_MASKS
 };
 
 Tuning tuning_from_flags(int flags, int def_shift, int def_ctas) {
@@ -1267,6 +1353,7 @@ Tuning tuning_from_flags(int flags, int def_shift, int def_ctas) {
     const int pc = (flags >> RM_BLEND_PAIR_CTAS_SHIFT) & 0xf;
     t.heavy_shift = hs ? hs : def_shift;
     t.pair_ctas_per_sm = pc ? pc : def_ctas;
+    t.hit_masks = (flags & RM_BLEND_HIT_MASKS) != 0;
     return t;
 }
 
@@ -1284,12 +1371,16 @@ template <int PX, int B_DENSE, int PX_PAIR, int NT_PAIR, int B_PAIR, class V>
 int launch_fwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, const float* jitter, const V& views,
                const Shape& sh, float* img, float* dist, int32_t* nc, const Tuning& tn, cudaStream_t s) {
     const int G = sh.G;
-    int rc = launch_order(ranges, G, w, tn.heavy_shift, s);
+    // hit masks need 64-pixel items in both kernels; the header records whether
+    // this forward wrote them, so a backward never reads stale masks
+    const bool masks = tn.hit_masks && PX == 64 && PX_PAIR == 64 && w.mask_header;
+    int rc = launch_order(ranges, G, w, tn.heavy_shift, s, w.mask_header, masks ? kMaskValid : 0u);
     if (rc) return rc;
     const int subs = sh.tile_px / PX;
     const int subs_pair = sh.tile_px / PX_PAIR;
-    const Queue qd = {w.order, w.info, w.tickets + 0, G, subs, false};
-    const Queue qp = {w.order, w.info, w.tickets + 1, G, subs_pair, true};
+    const HitMasks hm = {masks ? w.mask_words : nullptr, w.mask_cap, w.mask_header};
+    const Queue qd = {w.order, w.info, w.tickets + 0, G, subs, false, hm};
+    const Queue qp = {w.order, w.info, w.tickets + 1, G, subs_pair, true, hm};
     auto pair_kernel = blend_fwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, V>;
     const int smem = (int)sizeof(FwdPairSmem<PX_PAIR, B_PAIR>);
     cudaFuncSetAttribute(pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1324,8 +1415,10 @@ int launch_bwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, cons
     if (rc) return rc;
     const int subs = sh.tile_px / PX;
     const int subs_pair = sh.tile_px / PX_PAIR;
-    const Queue qd = {w.order, w.info, w.tickets + 2, G, subs, false};
-    const Queue qp = {w.order, w.info, w.tickets + 3, G, subs_pair, true};
+    const bool masks = tn.hit_masks && PX == 64 && w.mask_header;
+    const HitMasks hm = {masks ? w.mask_words : nullptr, w.mask_cap, w.mask_header};
+    const Queue qd = {w.order, w.info, w.tickets + 2, G, subs, false, hm};
+    const Queue qp = {w.order, w.info, w.tickets + 3, G, subs_pair, true, HitMasks{nullptr, 0, nullptr}};
     auto pair_kernel = blend_bwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, V>;
     const int smem = (int)sizeof(BwdPairSmem<PX_PAIR, B_PAIR>);
     cudaFuncSetAttribute(pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1415,7 +1508,7 @@ int blend_fwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
     if (((uintptr_t)out_img & 15) || ((uintptr_t)ranges & 7) || ((uintptr_t)ray_jitter & 7))
         return rm_host::fail(RM_EINVAL, "%s: misaligned image / ranges / jitter", who);
     cudaStream_t s = (cudaStream_t)stream;
-    BlendWs w = blend_ws(workspace, records ? 0 : n_tets, sh.G);
+    BlendWs w = blend_ws(workspace, records ? 0 : n_tets, sh.G, workspace_bytes);
     if (records) {
         if ((uintptr_t)records & 15) return rm_host::fail(RM_EINVAL, "%s: records must be 16-byte aligned", who);
         w.recs = (float4*)records;  // packed by rm_blend_pack_records
@@ -1460,7 +1553,7 @@ int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
         ((uintptr_t)ray_jitter & 7))
         return rm_host::fail(RM_EINVAL, "%s: misaligned image / grad / ranges / jitter", who);
     cudaStream_t s = (cudaStream_t)stream;
-    BlendWs w = blend_ws(workspace, records ? 0 : n_tets, sh.G);
+    BlendWs w = blend_ws(workspace, records ? 0 : n_tets, sh.G, workspace_bytes);
     if (records) {
         if ((uintptr_t)records & 15) return rm_host::fail(RM_EINVAL, "%s: records must be 16-byte aligned", who);
         w.recs = (float4*)records;  // packed by rm_blend_pack_records
@@ -1496,6 +1589,12 @@ int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
 extern "C" {
 
 size_t rm_blend_workspace_size(int64_t n_tets, int64_t n_tiles) { return rm::blend_ws_bytes(n_tets, n_tiles); }
+
+size_t rm_blend_hit_mask_bytes(int64_t n_pairs, int64_t n_tiles, int tile_pixels) {
+    const int64_t subs = tile_pixels > 64 ? tile_pixels / 64 : 1;
+    const int64_t blocks = (n_pairs > 0 ? n_pairs : 0) / 32 + (n_tiles > 0 ? n_tiles : 0) + 2;
+    return 256 + (size_t)blocks * (size_t)subs * 64 * sizeof(uint32_t);
+}
 
 size_t rm_blend_records_size(int64_t n_tets) {
     return (size_t)(n_tets > 0 ? n_tets : 0) * rm::kRecFloat4 * sizeof(float4);

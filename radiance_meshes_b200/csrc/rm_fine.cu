@@ -7,7 +7,7 @@
 // order (depth key, then tet id), so instead each coarse list is split once,
 // in order, into its 4 (or 16, 64) fine lists: a counting pass, a scan of the
 // counts in fine-tile order, and a writing pass.  One CTA walks one coarse
-// list in chunks of 256 entries; the ranks inside a chunk come from warp
+// list in chunks of 1024 entries; the ranks inside a chunk come from warp
 // ballots per fine tile.  No reference counterpart (the reference blends over
 // the coarse lists directly).
 #include "rm_internal.cuh"
@@ -15,7 +15,7 @@
 namespace rm {
 namespace {
 
-constexpr int kFineThreads = 256;
+constexpr int kFineThreads = 1024;
 constexpr int kFineWarps = kFineThreads / 32;
 constexpr int kMaxQuads = 64;  // fine tiles per coarse tile (fine_shift <= 3)
 

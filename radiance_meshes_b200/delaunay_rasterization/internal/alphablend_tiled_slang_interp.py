@@ -29,9 +29,10 @@ class AlphaBlendTiledRender(torch.autograd.Function):
         fine = R.fine_lists_of(sorted_tetra_idx, camst)
         if fine is not None:
             sorted_tetra_idx, tile_ranges, camst = fine.sorted_ids, fine.ranges, fine.cam
+        # hit masks let the backward skip the forward's misses
         output_img, distortion_img, n_contributors, records = R.blend_fwd(
             sorted_tetra_idx, tile_ranges, indices, vertices, tet_density, ray_jitter, camst,
-            tiles_touched=tiles_touched)
+            tiles_touched=tiles_touched, hit_masks=True)
         tet_alive = torch.zeros((indices.shape[0]), dtype=torch.bool, device=vertices.device)
         ctx.save_for_backward(sorted_tetra_idx, tile_ranges, indices, vertices, tet_density, output_img,
                               distortion_img, n_contributors, ray_jitter)
@@ -47,5 +48,6 @@ class AlphaBlendTiledRender(torch.autograd.Function):
          n_contributors, ray_jitter) = ctx.saved_tensors
         vertices_grad, tet_density_grad = R.blend_bwd(
             sorted_tetra_idx, tile_ranges, indices, vertices, tet_density, ray_jitter, ctx.camst, output_img,
-            distortion_img, n_contributors, grad_output_img, grad_distortion_img, ctx.records, reuse_records=True)
+            distortion_img, n_contributors, grad_output_img, grad_distortion_img, ctx.records, reuse_records=True,
+            hit_masks=True)
         return (None, None, None, vertices_grad, tet_density_grad, None, None, None, None, None)

@@ -332,7 +332,12 @@ def blend_tuning() -> tuple[int, int]:
 
 
 def blend_fwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, cam: RMCamera,
-              tiles_touched=None, records: torch.Tensor | None = None, reuse_records: bool = False):
+              tiles_touched=None, records: torch.Tensor | None = None, reuse_records: bool = False,
+              hit_masks: bool = False):
+    """Forward blend.  Returns (img, dist, n_contrib, workspace); pass the
+    workspace to blend_bwd.  hit_masks: also store which pixels hit each list
+    entry (RM_BLEND_HIT_MASKS) so that a blend_bwd with hit_masks=True skips
+    the misses."""
     _require_cuda(sorted_ids=sorted_ids, ranges=ranges, indices=indices, vertices=vertices,
                   cell_values=cell_values, ray_jitter=ray_jitter)
     indices = _i32(indices)
@@ -344,12 +349,16 @@ def blend_fwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, ca
     T = indices.shape[0]
     L = C.lib()
     ws_n = L.rm_blend_workspace_size(T, cam.grid_width * cam.grid_height)
+    if hit_masks:
+        ws_n += L.rm_blend_hit_mask_bytes(sorted_ids.shape[0], cam.grid_width * cam.grid_height,
+                                          cam.tile_width * cam.tile_height)
     if records is None:
         records = torch.empty(ws_n, dtype=torch.uint8, device=dev)
     img = torch.empty((H, W, 4), dtype=torch.float32, device=dev)
     dist = torch.empty((H, W, 5), dtype=torch.float32, device=dev)
     nc = torch.empty((H, W, 1), dtype=torch.int32, device=dev)
-    flags = (C.RM_BLEND_REUSE_RECORDS if reuse_records else 0) | _BLEND_FLAGS["fwd"]
+    flags = ((C.RM_BLEND_REUSE_RECORDS if reuse_records else 0) | (C.RM_BLEND_HIT_MASKS if hit_masks else 0) |
+             _BLEND_FLAGS["fwd"])
     _call("rm_blend_fwd", lambda: L.rm_blend_fwd(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(indices), C.ptr(vertices), C.ptr(cell_values),
                            T, vertices.shape[0], C.ptr(tiles_touched), C.ptr(ray_jitter), ctypes.byref(cam),
                            C.ptr(img), C.ptr(dist), C.ptr(nc), C.ptr(records), records.numel(), flags, _stream()))
@@ -358,7 +367,7 @@ def blend_fwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, ca
 
 def blend_bwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, cam: RMCamera, img, dist, nc,
               grad_img, grad_dist, records, tiles_touched=None, reuse_records=True,
-              grad_vertices=None, grad_cell_values=None):
+              grad_vertices=None, grad_cell_values=None, hit_masks: bool = False):
     indices = _i32(indices)
     vertices = _f32(vertices)
     cell_values = _f32(cell_values)
@@ -372,7 +381,8 @@ def blend_bwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, ca
     if grad_cell_values is None:
         grad_cell_values = torch.zeros_like(cell_values)
     T = indices.shape[0]
-    flags = (C.RM_BLEND_REUSE_RECORDS if reuse_records else 0) | _BLEND_FLAGS["bwd"]
+    flags = ((C.RM_BLEND_REUSE_RECORDS if reuse_records else 0) | (C.RM_BLEND_HIT_MASKS if hit_masks else 0) |
+             _BLEND_FLAGS["bwd"])
     _call("rm_blend_bwd", lambda: C.lib().rm_blend_bwd(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(indices), C.ptr(vertices),
                                  C.ptr(cell_values), T, vertices.shape[0], C.ptr(tiles_touched), C.ptr(ray_jitter),
                                  ctypes.byref(cam), C.ptr(img), C.ptr(dist), C.ptr(nc), C.ptr(grad_img), C.ptr(gd),

@@ -96,7 +96,7 @@ def batch_bytes(n_tets: int, views: B.ViewBatch, capacity: int) -> int:
     L = C.lib()
     proj = n * n_tets * (4 + 16 + 4 + 4) + n_tets * 4 + int(L.rm_scan_workspace_size(n * n_tets))
     pairs = capacity * (8 + 4 + 8 + 4) + int(L.rm_sort_workspace_size(max(capacity, 1)))
-    tiles = views.n_tiles * 8 + int(L.rm_blend_workspace_size(0, views.n_tiles))
+    tiles = views.n_tiles * 8 + int(L.rm_blend_workspace_size(0, views.n_tiles))  # no hit masks (forward only)
     pixels = views.n_pixels * (8 + 16 + 20 + 4)
     return proj + pairs + tiles + pixels + 4096
 
@@ -162,7 +162,8 @@ class Server:
             worst = 0.0
             for cam in cams:
                 vb = B.ViewBatch([cam])
-                r = B.BatchedRasterizer(m.indices, m.vertices, m.cell_values, vb, capacity=1, records=m.records)
+                r = B.BatchedRasterizer(m.indices, m.vertices, m.cell_values, vb, capacity=1, records=m.records,
+                                        hit_masks=False)
                 P = r.measure_pairs()
                 worst = max(worst, P / vb.n_pixels)
                 del r
@@ -223,7 +224,7 @@ class Server:
         cap = capacity if capacity is not None else self._capacity(mesh, vb)
         with torch.cuda.stream(stream):
             rast = B.BatchedRasterizer(mesh.indices, mesh.vertices, mesh.cell_values, vb, capacity=cap,
-                                       fwd_flags=self.fwd_flags, records=mesh.records)
+                                       fwd_flags=self.fwd_flags, records=mesh.records, hit_masks=False)
             rast.forward()
             total_host = torch.empty(1, dtype=torch.int64, pin_memory=True)
             total_host.copy_(rast.total, non_blocking=True)

@@ -65,8 +65,8 @@ def _compare(gpu, ref, rel_tol, entry_rtol=None, entry_atol=None, what="", trim=
     return out
 
 
-def _run(verts, idx, cv, tcam, jitter, loss, seed=0, check_f64=True):
-    r = run_gpu_forward(verts, idx, cv, tcam, jitter)
+def _run(verts, idx, cv, tcam, jitter, loss, seed=0, check_f64=True, hit_masks=False):
+    r = run_gpu_forward(verts, idx, cv, tcam, jitter, hit_masks=hit_masks)
     img = r["img"].cpu().numpy()
     H, W = img.shape[:2]
     rng = np.random.default_rng(seed)
@@ -82,7 +82,8 @@ def _run(verts, idx, cv, tcam, jitter, loss, seed=0, check_f64=True):
             gdist[:] = 0.0
     L = r["lists"]
     gv, gc = R.blend_bwd(L.sorted_ids, L.ranges, r["i"], r["v"], r["c"], r["j"], r["cam"], r["img"], r["dist"],
-                         r["nc"], to_dev(gimg), to_dev(gdist), r["records"], reuse_records=True)
+                         r["nc"], to_dev(gimg), to_dev(gdist), r["records"], reuse_records=True,
+                         hit_masks=hit_masks)
     torch.cuda.synchronize()
     lists = dict(cam=r["cam"], sorted_ids=L.sorted_ids.cpu().numpy(), ranges=L.ranges.cpu().numpy())
     nc = r["nc"].cpu().numpy()[..., 0]
@@ -171,3 +172,50 @@ def test_backward_each_kernel_path(cuda, route, tile):
              seed=tile)
     finally:
         R.set_blend_tuning(*old)
+
+
+@pytest.mark.parametrize("fwd_route", ["all_pair", "split"])
+@pytest.mark.parametrize("tile", [8, 16, 32])
+def test_backward_with_hit_masks(cuda, fwd_route, tile):
+    """The backward that revisits only the forward's hits (RM_BLEND_HIT_MASKS)
+    matches the FP32 restatement like the full backward, whichever forward
+    kernel recorded the masks; the forward's outputs do not change."""
+    from radiance_meshes_b200 import _capi as C
+
+    fwd_flags = 0 if fwd_route == "all_pair" else (2 << C.RM_BLEND_HEAVY_SHIFT) | (2 << C.RM_BLEND_PAIR_CTAS_SHIFT)
+    old = R.blend_tuning()
+    R.set_blend_tuning(fwd_flags, 0)
+    try:
+        mesh, view = scenes.workload_gradient_check(tile)
+        jitter = np.random.default_rng(tile + 3).uniform(0, 1, (view.height, view.width, 2)).astype(np.float32)
+        a = run_gpu_forward(mesh.vertices, mesh.indices, mesh.cell_values, view.tcam(tile_size=tile), jitter)
+        b = run_gpu_forward(mesh.vertices, mesh.indices, mesh.cell_values, view.tcam(tile_size=tile), jitter,
+                            hit_masks=True)
+        assert torch.equal(a["img"], b["img"]) and torch.equal(a["nc"], b["nc"])
+        for loss in ("linear", "l1"):
+            _run(mesh.vertices, mesh.indices, mesh.cell_values, view.tcam(tile_size=tile), jitter, loss,
+                 seed=tile, check_f64=False, hit_masks=True)
+    finally:
+        R.set_blend_tuning(*old)
+
+
+def test_hit_masks_invalidated_by_a_forward_without_them(cuda):
+    """A forward without RM_BLEND_HIT_MASKS on a workspace that holds masks
+    from an earlier frame marks them invalid: a masked backward then tests
+    every entry and still matches."""
+    mesh, view = scenes.workload_gradient_check(8)
+    tcam = view.tcam(tile_size=8)
+    jitter = np.full((view.height, view.width, 2), 0.5, np.float32)
+    r = run_gpu_forward(mesh.vertices, mesh.indices, mesh.cell_values, tcam, jitter, hit_masks=True)
+    L = r["lists"]
+    cv2 = r["c"] * 0.5  # another frame: different densities, same lists
+    img2, dist2, nc2, _ = R.blend_fwd(L.sorted_ids, L.ranges, r["i"], r["v"], cv2, r["j"], r["cam"],
+                                      tiles_touched=r["tiles"], records=r["records"], hit_masks=False)
+    g = torch.randn_like(img2)
+    gv_m, gc_m = R.blend_bwd(L.sorted_ids, L.ranges, r["i"], r["v"], cv2, r["j"], r["cam"], img2, dist2, nc2, g,
+                             None, r["records"], reuse_records=True, hit_masks=True)
+    gv, gc = R.blend_bwd(L.sorted_ids, L.ranges, r["i"], r["v"], cv2, r["j"], r["cam"], img2, dist2, nc2, g, None,
+                         r["records"], reuse_records=True, hit_masks=False)
+    torch.cuda.synchronize()
+    assert float((gv_m - gv).norm() / gv.norm()) < 1e-5
+    assert float((gc_m - gc).norm() / gc.norm()) < 1e-5
