@@ -461,15 +461,15 @@ def run_multiview(args):
         from radiance_meshes_b200 import autotune
 
         tuned = autotune.tune_batch(idx, verts, cv, [v for v in views], device=dev)
-        tile = tuned["tile"]
+        tile, fine_shift = tuned["tile"], tuned["fine_shift"]
         fwd_flags, bwd_flags = tuned["fwd_flags"], tuned["bwd_flags"]
     else:
-        fwd_flags = bwd_flags = 0
+        fwd_flags = bwd_flags = fine_shift = 0
     cams = [tcam_to_struct(v.tcam(tile_size=tile)) for v in views]
     vb = B.ViewBatch(cams)
     gen = torch.Generator(device=dev).manual_seed(7)
     target = torch.rand(vb.n_pixels, 3, device=dev, generator=gen)
-    br = B.BatchedRasterizer(idx, verts, cv, vb, fwd_flags=fwd_flags, bwd_flags=bwd_flags)
+    br = B.BatchedRasterizer(idx, verts, cv, vb, fwd_flags=fwd_flags, bwd_flags=bwd_flags, fine_shift=fine_shift)
     step = B.L1Step(br, target)
     step.run()
     br.check()
@@ -556,6 +556,8 @@ def run_multiview(args):
         "config": {"workload": f"multi-view: {args.mv_points} mixture points (seed 3), {T} tets, {nv} ring views "
                                f"{[(v.width, v.height) for v in views]}, fwd + L1 + bwd",
                    "tets": T, "views": nv, "pixels": vb.n_pixels, "pairs": P, "tile": tile,
+                   "blend_tile": tile >> fine_shift,
+                   "blend_pairs": int(br.fine_total.item()) if fine_shift else P,
                    "autotune": tuned, "l2": "flushed between steps (256 MiB write)",
                    "batched": "one launch per stage over all views, CUDA graph replay",
                    "per_view": "drop-in autograd path per camera, host sync per view: 16x16 tiles with "
@@ -607,7 +609,7 @@ def run_serving(args):
     resident = [S.ResidentMesh(f"mixture{n}", idx, pts, cv, device=dev) for n, pts, idx, cv in built]
     tets = {m.name: m.T for m in resident}
     names = [m.name for m in resident]
-    tile, flags, tuned = args.sv_tile, 0, None
+    tile, flags, tuned, fine_shift = args.sv_tile, 0, None, 0
     rng = np.random.default_rng(77)
     sample_views = [scenes.sphere_view(rng, h, w) for (h, w) in scenes.SERVING_RESOLUTIONS for _ in range(2)]
     if tile == 0:
@@ -615,10 +617,12 @@ def run_serving(args):
 
         mid = resident[len(resident) // 2]
         tuned = autotune.tune_batch(mid.indices, mid.vertices, mid.cell_values, sample_views[::2], device=dev,
-                                    tiles=(8, 16), backward=False)
-        tile, flags = tuned["tile"], tuned["fwd_flags"]
+                                    tiles=(8, 16, 32), backward=False)
+        tile, flags, fine_shift = tuned["tile"], tuned["fwd_flags"], tuned["fine_shift"]
+    else:
+        fine_shift = 0
     server = S.Server(resident, streams=args.sv_streams, max_views=args.sv_max_views, tile=tile, fwd_flags=flags,
-                      keep_outputs=False, device=dev)
+                      fine_shift=fine_shift, keep_outputs=False, device=dev)
     server.calibrate({m.name: [tcam_to_struct(v.tcam(tile_size=tile)) for v in sample_views] for m in resident})
     n_total = args.sv_warmup + args.sv_requests
     trace = scenes.serving_trace(n_total, args.sv_rate, names, seed=7, tile_size=tile)

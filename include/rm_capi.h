@@ -314,13 +314,32 @@ RM_API int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges,
  * and rect [n_views, T] (rect rows of 4), depth [n_views, T] (rm_project_fwd's
  * vs[:, 2]).  tiles_any [T] (optional) receives the tet's tile count summed
  * over the views; circumcenter [T, 3] (optional) is view-independent.
+ * rect_fine [n_views, T, 4] (optional) receives rm_project_fwd_fine's
+ * rectangles on the 2^fine_shift times finer grid.
  */
 RM_API int rm_project_fwd_multi(const int32_t* indices, const float* vertices,
                                 int64_t n_tets, int64_t n_verts,
                                 const rm_camera* cams, int n_views,
                                 int32_t* tiles_touched, int32_t* rect,
                                 float* depth, int32_t* tiles_any,
-                                float* circumcenter, void* stream);
+                                float* circumcenter, int fine_shift,
+                                int32_t* rect_fine, void* stream);
+
+/*
+ * rm_fine_lists for a view batch: the coarse lists of all views (global
+ * view-major tiles) split into the lists of the finer tiles, numbered
+ * view-major on the finer grids (view v's fine tiles start at
+ * tile_base(v) * 4^fine_shift), using rect_fine [n_views, T, 4] of
+ * rm_project_fwd_multi.  Blending a batch of the fine cameras (tiles
+ * 2^fine_shift times smaller, grids that much larger) over these lists gives
+ * the coarse batch's images bit for bit.
+ */
+RM_API int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges,
+                               const int32_t* rect_fine, int64_t n_tets,
+                               const rm_camera* cams, int n_views, int fine_shift,
+                               int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
+                               int64_t* total_dev, void* workspace, size_t workspace_bytes,
+                               void* stream);
 
 /*
  * Pair emission for the stacked projection: offsets is the inclusive scan of

@@ -2,9 +2,10 @@
 
 Knobs, all measured on the caller's own mesh and cameras:
 
-* tile size: 8, 16 or 32 pixels square.  Smaller tiles mean more tile/tet
-  pairs (longer sort, more list traffic) but fewer wasted ray/tet tests per
-  pixel; larger tiles the reverse.
+* tile size of the sorted lists (8, 16 or 32 pixels square) and of the
+  blend (the same, or 2^k times smaller, down to 8: the sorted lists are then
+  split in order, rm_fine_lists_multi).  Smaller blend tiles waste fewer
+  ray/tet tests per pixel; smaller list tiles cost more pairs to sort.
 * work split between the two blend kernels, i.e. pixels per thread: the
   one-thread-per-pixel dense kernel versus the pair kernel that spreads a
   strip's (entry, pixel) tests over four threads per pixel (heavy-tile
@@ -32,7 +33,7 @@ from . import _capi as C
 from . import batch as B
 from .camera import tcam_to_struct
 
-__all__ = ["flags", "tune_batch", "candidates_fwd", "candidates_bwd", "cache_path"]
+__all__ = ["flags", "tune_batch", "candidates_fwd", "candidates_bwd", "cache_path", "list_configs"]
 
 _lock = threading.Lock()
 
@@ -54,7 +55,7 @@ def flags(strip: int = 0, heavy_shift: int = 0, pair_ctas: int = 0, batch: int =
 def candidates_fwd(tile: int):
     out = []
     for b in (16, 32, 64):
-        for ctas in (2, 3):
+        for ctas in (2, 3, 4):
             out.append(dict(strip=64 if tile >= 8 else 16, heavy_shift=1, pair_ctas=ctas, batch=b))
     out.append(dict(strip=16, heavy_shift=1, pair_ctas=3, batch=32))
     out.append(dict(strip=64 if tile >= 8 else 16, heavy_shift=3, pair_ctas=2, batch=32))
@@ -120,13 +121,27 @@ def _time(fn, reps=2):
     return best
 
 
+def list_configs(tiles):
+    """(list tile, fine shift) pairs: lists sorted on `tile`-pixel tiles and
+    blended on tiles 2^shift times smaller, down to 8 pixels."""
+    out = []
+    for t in tiles:
+        shift = 0
+        while (t >> shift) >= 8:
+            out.append((t, shift))
+            shift += 1
+    return out
+
+
 def tune_batch(indices: torch.Tensor, vertices: torch.Tensor, cell_values: torch.Tensor, views: Sequence,
                device=None, tiles=(8, 16, 32), backward: bool = True, use_cache: bool = True) -> dict:
-    """Pick the tile size and blend flags for rendering ``views`` (objects
-    with ``tcam(tile_size=...)``, e.g. ``scenes.View``) of this mesh.
+    """Pick the list tile size, the blend tile size (fine split) and the blend
+    flags for rendering ``views`` (objects with ``tcam(tile_size=...)``, e.g.
+    ``scenes.View``) of this mesh.
 
-    Returns {"tile", "fwd_flags", "bwd_flags", "fwd", "bwd", "ms"} where
-    "ms" holds the measured times per tile size (lists, blend fwd, blend bwd).
+    Returns {"tile", "fine_shift", "fwd_flags", "bwd_flags", "fwd", "bwd",
+    "ms"} where "ms" holds the measured times per configuration
+    ("<tile>/<blend tile>": lists, blend fwd, blend bwd).
     """
     device = device or vertices.device
     key = _key(device, indices.shape[0], views, tiles, backward)
@@ -135,13 +150,14 @@ def tune_batch(indices: torch.Tensor, vertices: torch.Tensor, cell_values: torch
         if hit is not None:
             return dict(hit, cached=True)
     results = {}
-    for tile in tiles:
+    for tile, shift in list_configs(tiles):
         cams = [tcam_to_struct(v.tcam(tile_size=tile)) for v in views]
         vb = B.ViewBatch(cams)
-        br = B.BatchedRasterizer(indices, vertices, cell_values, vb)
+        br = B.BatchedRasterizer(indices, vertices, cell_values, vb, fine_shift=shift)
+        btile = tile >> shift
         t_lists = _time(lambda: (br._project_scan(), br._lists()))
         best_f = None
-        for cand in candidates_fwd(tile):
+        for cand in candidates_fwd(btile):
             br.fwd_flags = flags(**cand)
             t = _time(br._blend_fwd)
             if best_f is None or t < best_f[0]:
@@ -152,23 +168,25 @@ def tune_batch(indices: torch.Tensor, vertices: torch.Tensor, cell_values: torch
         if backward:
             br.grad_img.normal_()
             best_b = None
-            for cand in candidates_bwd(tile):
+            for cand in candidates_bwd(btile):
                 br.bwd_flags = flags(**cand)
                 t = _time(br._blend_bwd)
                 if best_b is None or t < best_b[0]:
                     best_b = (t, cand)
-        results[tile] = dict(lists=t_lists, fwd=best_f[0], bwd=best_b[0], fwd_cand=best_f[1], bwd_cand=best_b[1],
-                             pairs=int(br.total.item()))
+        pairs = int(br.fine_total.item()) if shift else int(br.total.item())
+        results[(tile, shift)] = dict(lists=t_lists, fwd=best_f[0], bwd=best_b[0], fwd_cand=best_f[1],
+                                      bwd_cand=best_b[1], pairs=pairs)
         del br
         torch.cuda.empty_cache()
-    tile = min(results, key=lambda t: results[t]["lists"] + results[t]["fwd"] + results[t]["bwd"])
-    r = results[tile]
-    out = {"tile": tile, "fwd_flags": flags(**r["fwd_cand"]),
+    best = min(results, key=lambda t: results[t]["lists"] + results[t]["fwd"] + results[t]["bwd"])
+    r = results[best]
+    name = lambda ts: f"{ts[0]}/{ts[0] >> ts[1]}"
+    out = {"tile": best[0], "fine_shift": best[1], "fwd_flags": flags(**r["fwd_cand"]),
            "bwd_flags": flags(**r["bwd_cand"]) if r["bwd_cand"] else 0,
            "fwd": r["fwd_cand"], "bwd": r["bwd_cand"],
-           "ms": {str(t): {k: round(v, 4) for k, v in results[t].items() if k in ("lists", "fwd", "bwd")}
+           "ms": {name(t): {k: round(v, 4) for k, v in results[t].items() if k in ("lists", "fwd", "bwd")}
                   for t in results},
-           "pairs": {str(t): results[t]["pairs"] for t in results}}
+           "pairs": {name(t): results[t]["pairs"] for t in results}}
     if use_cache:
         _store_cache(key, out)
     return dict(out, cached=False)

@@ -85,7 +85,7 @@ class BatchedRasterizer:
     def __init__(self, indices: torch.Tensor, vertices: torch.Tensor, cell_values: torch.Tensor,
                  views: ViewBatch, jitter: torch.Tensor | None = None, capacity: int | None = None,
                  fwd_flags: int = 0, bwd_flags: int = 0, records: torch.Tensor | None = None,
-                 hit_masks: bool = True):
+                 hit_masks: bool = True, fine_shift: int = 0):
         for name, t in (("indices", indices), ("vertices", vertices), ("cell_values", cell_values)):
             if not t.is_cuda:
                 raise RuntimeError(f"{name} must be a CUDA tensor (the rasterizer has no CPU path)")
@@ -95,6 +95,12 @@ class BatchedRasterizer:
             raise ValueError("vertices and cell_values must be float32")
         self.indices, self.vertices, self.cell_values = indices, vertices, cell_values
         self.views = views
+        # fine_shift > 0: lists are sorted on the cameras' tiles, then split in
+        # order into the lists of tiles 2^fine_shift times smaller, which the
+        # blend walks (same images; cheaper than sorting at the small tiles)
+        self.fine_shift = int(fine_shift)
+        self.blend_views = ViewBatch([R.fine_camera(c, self.fine_shift) for c in views.cams]) \
+            if self.fine_shift else views
         self.fwd_flags, self.bwd_flags = int(fwd_flags), int(bwd_flags)
         # hit masks (RM_BLEND_HIT_MASKS): the forward records its hits so the
         # backward skips the misses; forward-only users turn them off
@@ -117,7 +123,13 @@ class BatchedRasterizer:
         # every batch on it; without them each forward packs its own into the workspace
         self.records = records
         ws_tets = 0 if records is not None else T
-        self._ws_base = int(L.rm_blend_workspace_size(ws_tets, views.n_tiles))
+        bv = self.blend_views
+        self._ws_base = int(L.rm_blend_workspace_size(ws_tets, bv.n_tiles))
+        if self.fine_shift:
+            self.rect_fine = torch.empty((n * T, 4), dtype=torch.int32, device=dev)
+            self.fine_ranges = torch.empty((bv.n_tiles, 2), dtype=torch.int32, device=dev)
+            self.fine_total = torch.zeros(1, dtype=torch.int64, device=dev)
+            self.fine_ws = torch.empty(L.rm_fine_lists_workspace_size(bv.n_tiles), dtype=torch.uint8, device=dev)
         self.blend_ws = None  # sized with the pair capacity (hit masks) in _alloc_pairs
         Npx = views.n_pixels
         self.jitter = jitter if jitter is not None else torch.full((Npx, 2), 0.5, device=dev)
@@ -161,10 +173,15 @@ class BatchedRasterizer:
         self.sorted_keys = torch.empty(capacity, dtype=torch.int64, device=dev)
         self.sorted_ids = torch.empty(capacity, dtype=torch.int32, device=dev)
         self.sort_ws = torch.empty(C.lib().rm_sort_workspace_size(capacity), dtype=torch.uint8, device=dev)
+        blend_pairs = capacity
+        if self.fine_shift:
+            blend_pairs = capacity << (2 * self.fine_shift)  # a coarse entry splits into at most 4^s
+            self.fine_ids = torch.empty(blend_pairs, dtype=torch.int32, device=dev)
         ws = self._ws_base
         if self.hit_masks:
-            c0 = self.views.cams[0]
-            ws += int(C.lib().rm_blend_hit_mask_bytes(capacity, self.views.n_tiles, c0.tile_width * c0.tile_height))
+            bv = self.blend_views
+            c0 = bv.cams[0]
+            ws += int(C.lib().rm_blend_hit_mask_bytes(blend_pairs, bv.n_tiles, c0.tile_width * c0.tile_height))
         self.blend_ws = torch.empty(ws, dtype=torch.uint8, device=dev)
         self.graph = None
 
@@ -186,9 +203,10 @@ class BatchedRasterizer:
     def _project_scan(self):
         L, s, v = C.lib(), C.stream_handle(), self.views
         nT = v.n * self.T
-        R._call("rm_project_fwd_multi", lambda: L.rm_project_fwd_multi(C.ptr(self.indices), C.ptr(self.vertices), self.T, self.V, v.array, v.n,
-                                       C.ptr(self.tiles), C.ptr(self.rect), C.ptr(self.depth),
-                                       C.ptr(self.tiles_any), None, s))
+        rf = self.rect_fine if self.fine_shift else None
+        R._call("rm_project_fwd_multi", lambda: L.rm_project_fwd_multi(
+            C.ptr(self.indices), C.ptr(self.vertices), self.T, self.V, v.array, v.n, C.ptr(self.tiles),
+            C.ptr(self.rect), C.ptr(self.depth), C.ptr(self.tiles_any), None, self.fine_shift, C.ptr(rf), s))
         R._call("rm_scan_tiles", lambda: L.rm_scan_tiles(C.ptr(self.tiles), nT, C.ptr(self.offsets), C.ptr(self.total),
                                 C.ptr(self.scan_ws), self.scan_ws.numel(), s))
 
@@ -202,20 +220,33 @@ class BatchedRasterizer:
                                 self.sort_ws.numel(), s))
         R._call("rm_tile_ranges", lambda: L.rm_tile_ranges(C.ptr(self.sorted_keys), self.capacity, C.ptr(self.total), C.ptr(self.ranges),
                                  v.n_tiles, s))
+        if self.fine_shift:
+            R._call("rm_fine_lists", lambda: L.rm_fine_lists_multi(
+                C.ptr(self.sorted_ids), C.ptr(self.ranges), C.ptr(self.rect_fine), self.T, v.array, v.n,
+                self.fine_shift, self.fine_ids.shape[0], C.ptr(self.fine_ids), C.ptr(self.fine_ranges),
+                C.ptr(self.fine_total), C.ptr(self.fine_ws), self.fine_ws.numel(), s))
+
+    def _blend_lists(self):
+        """(sorted ids, ranges, views) that the blend walks."""
+        if self.fine_shift:
+            return self.fine_ids, self.fine_ranges, self.blend_views
+        return self.sorted_ids, self.ranges, self.views
 
     def _blend_fwd(self):
-        L, s, v = C.lib(), C.stream_handle(), self.views
-        R._call("rm_blend_fwd_multi", lambda: L.rm_blend_fwd_multi(C.ptr(self.sorted_ids), C.ptr(self.ranges), C.ptr(self.indices),
+        L, s = C.lib(), C.stream_handle()
+        ids, rg, v = self._blend_lists()
+        R._call("rm_blend_fwd_multi", lambda: L.rm_blend_fwd_multi(C.ptr(ids), C.ptr(rg), C.ptr(self.indices),
                                      C.ptr(self.vertices), C.ptr(self.cell_values), self.T, self.V,
                                      C.ptr(self.tiles_any), C.ptr(self.jitter), v.array, v.n, C.ptr(self.img),
                                      C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.records), C.ptr(self.blend_ws), self.blend_ws.numel(),
                                      self.fwd_flags | (C.RM_BLEND_HIT_MASKS if self.hit_masks else 0), s))
 
     def _blend_bwd(self):
-        L, s, v = C.lib(), C.stream_handle(), self.views
+        L, s = C.lib(), C.stream_handle()
+        ids, rg, v = self._blend_lists()
         self.grad_vertices.zero_()
         self.grad_cell_values.zero_()
-        C.check(L.rm_blend_bwd_multi(C.ptr(self.sorted_ids), C.ptr(self.ranges), C.ptr(self.indices),
+        C.check(L.rm_blend_bwd_multi(C.ptr(ids), C.ptr(rg), C.ptr(self.indices),
                                      C.ptr(self.vertices), C.ptr(self.cell_values), self.T, self.V,
                                      C.ptr(self.tiles_any), C.ptr(self.jitter), v.array, v.n, C.ptr(self.img),
                                      C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.grad_img), C.ptr(self.grad_dist),

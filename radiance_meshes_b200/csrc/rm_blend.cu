@@ -578,7 +578,7 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 1024 / NT : 32)) blend_fwd_den
 }
 
 template <int PX, int NT, int B, class V>
-__global__ void __launch_bounds__(NT, 768 / NT) blend_fwd_pair_kernel(
+__global__ void __launch_bounds__(NT, 1024 / NT) blend_fwd_pair_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
     const float2* __restrict__ jitter, const __grid_constant__ V views, float4* __restrict__ out_img,
     float* __restrict__ out_dist, int32_t* __restrict__ out_nc, const Queue q) {
@@ -1516,8 +1516,8 @@ int blend_fwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
         rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
         if (rc) return rc;
     }
-    // measured on the 1.3M-tet workload: every tile through the pair kernel, 3 CTAs/SM
-    const Tuning tn = tuning_from_flags(flags, 1, 3);
+    // measured on the 1.3M-tet workload: every tile through the pair kernel, 4 CTAs/SM
+    const Tuning tn = tuning_from_flags(flags, 1, 4);
     // tets per shared-memory batch of the pair kernel: 16, 32 (default) or 64
     const int key = strip_pixels(cam0, flags) * 1000 + batch_size(flags, 32);
 #define RM_FWD_CASE(PX, NT, BP)                                                                                  \
@@ -1563,8 +1563,8 @@ int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
     }
     // measured: the one-thread-per-pixel backward alone is fastest
     const Tuning tn = tuning_from_flags(flags, 15, 1);
-    // tets per shared-memory batch of the dense kernel: 16, 32 (default) or 64
-    const int key = strip_pixels(cam0, flags) * 1000 + batch_size(flags, 32);
+    // tets per shared-memory batch of the dense kernel: 16, 32 or 64 (default)
+    const int key = strip_pixels(cam0, flags) * 1000 + batch_size(flags, 64);
 #define RM_BWD_CASE(PX, NT, BD)                                                                                  \
     case PX * 1000 + BD:                                                                                         \
         return launch_bwd<PX, BD, PX, NT, 16>(sorted_ids, ranges, w, indices, ray_jitter, views, sh, out_img,       \

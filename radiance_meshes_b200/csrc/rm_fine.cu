@@ -26,25 +26,34 @@ __device__ __forceinline__ bool covers(int4 fr, int fx, int fy) {
 // WRITE = false: counts[fine id] = entries of the coarse list covering the
 // fine tile.  WRITE = true: write the fine lists at their scanned offsets and
 // the fine ranges.
+// Views: tile t of the coarse (global, view-major) numbering belongs to view
+// v = views.find(t); its fine tiles are numbered view-major too, view v's
+// starting at tiles[v] * f^2; rect_fine rows are stacked view-major ([v, T]).
 template <bool WRITE>
 __global__ void __launch_bounds__(kFineThreads) fine_lists_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const int4* __restrict__ rect_fine,
-    int grid_w, int f, int32_t* __restrict__ counts, const int32_t* __restrict__ incl,
-    int32_t* __restrict__ fine_ids, int64_t capacity, int2* __restrict__ fine_ranges, uint32_t* status) {
+    int64_t n_tets, const __grid_constant__ ViewSet views, int f, int32_t* __restrict__ counts,
+    const int32_t* __restrict__ incl, int32_t* __restrict__ fine_ids, int64_t capacity,
+    int2* __restrict__ fine_ranges, uint32_t* status) {
     __shared__ uint32_t wtot[kFineWarps][kMaxQuads];
     __shared__ uint32_t run[kMaxQuads];
     __shared__ int32_t start[kMaxQuads];
     const int t = blockIdx.x;
-    const int tx = t % grid_w, ty = t / grid_w;
+    const int v = views.find(t);
+    const int local = t - views.tiles[v];
+    const int grid_w = views.cams[v].grid_width;
+    const int tx = local % grid_w, ty = local / grid_w;
     const int Q = f * f;
     const int fgw = grid_w * f;
+    const int64_t fbase = (int64_t)views.tiles[v] * Q;
+    const int4* __restrict__ rf_v = rect_fine + (int64_t)v * n_tets;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     if (threadIdx.x < Q) {
         run[threadIdx.x] = 0u;
         if (WRITE) {
             const int q = threadIdx.x;
-            const int fid = (ty * f + q / f) * fgw + tx * f + q % f;
+            const int64_t fid = fbase + (ty * f + q / f) * fgw + tx * f + q % f;
             start[q] = __ldg(incl + fid) - __ldg(counts + fid);
         }
     }
@@ -56,7 +65,7 @@ __global__ void __launch_bounds__(kFineThreads) fine_lists_kernel(
         int32_t g = 0;
         if (e < r.y) {
             g = __ldg(ids + e);
-            fr = __ldg(rect_fine + g);
+            fr = __ldg(rf_v + g);
         }
         for (int q = 0; q < Q; ++q) {
             const bool in = covers(fr, tx * f + q % f, ty * f + q / f);
@@ -87,7 +96,7 @@ __global__ void __launch_bounds__(kFineThreads) fine_lists_kernel(
     }
     if (threadIdx.x < Q) {
         const int q = threadIdx.x;
-        const int fid = (ty * f + q / f) * fgw + tx * f + q % f;
+        const int64_t fid = fbase + (ty * f + q / f) * fgw + tx * f + q % f;
         if (WRITE) fine_ranges[fid] = make_int2(start[q], start[q] + (int)run[q]);
         else counts[fid] = (int32_t)run[q];
     }
@@ -105,24 +114,30 @@ size_t rm_fine_lists_workspace_size(int64_t n_fine_tiles) {
     return 2 * rm::align256((size_t)n * 4) + 256 + rm_scan_workspace_size(n);
 }
 
-int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* rect_fine, const rm_camera* cam,
-                  int fine_shift, int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges, int64_t* total_dev,
-                  void* workspace, size_t workspace_bytes, void* stream) {
-    int rc = rm_host::check_cam(cam);
-    if (rc) return rc;
-    if (fine_shift < 1 || fine_shift > 3) return rm_host::fail(RM_EINVAL, "rm_fine_lists: fine_shift %d", fine_shift);
-    if (capacity < 0) return rm_host::fail(RM_EINVAL, "rm_fine_lists: negative capacity");
+}  // extern "C"
+
+namespace {
+
+int fine_lists_impl(const char* who, const int32_t* sorted_ids, const int32_t* ranges, const int32_t* rect_fine,
+                    int64_t n_tets, const rm::ViewSet& views, int fine_shift, int64_t capacity, int32_t* fine_ids,
+                    int32_t* fine_ranges, int64_t* total_dev, void* workspace, size_t workspace_bytes, void* stream) {
+    if (fine_shift < 1 || fine_shift > 3) return rm_host::fail(RM_EINVAL, "%s: fine_shift %d", who, fine_shift);
+    if (capacity < 0 || n_tets < 0) return rm_host::fail(RM_EINVAL, "%s: negative size", who);
     const int f = 1 << fine_shift;
-    const int64_t G = (int64_t)cam->grid_width * cam->grid_height;
+    for (int v = 0; v < views.n; ++v)
+        if (views.cams[v].tile_width % f || views.cams[v].tile_height % f)
+            return rm_host::fail(RM_EINVAL, "%s: tile %dx%d not divisible by %d", who, views.cams[v].tile_width,
+                                 views.cams[v].tile_height, f);
+    const int64_t G = views.tiles[views.n];
     const int64_t Gf = G * f * f;
-    if (Gf >= (int64_t)INT32_MAX) return rm_host::fail(RM_EINVAL, "rm_fine_lists: too many tiles");
+    if (Gf >= (int64_t)INT32_MAX) return rm_host::fail(RM_EINVAL, "%s: too many tiles", who);
     if (!ranges || !rect_fine || !fine_ranges || !total_dev || !workspace || (capacity > 0 && (!sorted_ids || !fine_ids)))
-        return rm_host::fail(RM_EINVAL, "rm_fine_lists: NULL pointer");
+        return rm_host::fail(RM_EINVAL, "%s: NULL pointer", who);
     if (((uintptr_t)rect_fine & 15) || ((uintptr_t)ranges & 7) || ((uintptr_t)fine_ranges & 7) ||
         ((uintptr_t)workspace & 255))
-        return rm_host::fail(RM_EINVAL, "rm_fine_lists: misaligned rect_fine / ranges / workspace");
+        return rm_host::fail(RM_EINVAL, "%s: misaligned rect_fine / ranges / workspace", who);
     if (workspace_bytes < rm_fine_lists_workspace_size(Gf))
-        return rm_host::fail(RM_EINVAL, "rm_fine_lists: workspace %zu < %zu bytes", workspace_bytes,
+        return rm_host::fail(RM_EINVAL, "%s: workspace %zu < %zu bytes", who, workspace_bytes,
                              rm_fine_lists_workspace_size(Gf));
     if (G == 0) return RM_OK;
     char* p = (char*)workspace;
@@ -132,14 +147,40 @@ int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges, const int32_
     uint32_t* status = (uint32_t*)scan_ws;  // the scan workspace's status word
     cudaStream_t s = (cudaStream_t)stream;
     rm::fine_lists_kernel<false><<<(unsigned)G, rm::kFineThreads, 0, s>>>(
-        sorted_ids, (const int2*)ranges, (const int4*)rect_fine, cam->grid_width, f, counts, nullptr, nullptr, 0,
+        sorted_ids, (const int2*)ranges, (const int4*)rect_fine, n_tets, views, f, counts, nullptr, nullptr, 0,
         nullptr, nullptr);
-    if ((rc = rm_host::check_launch("rm_fine_lists (count)"))) return rc;
+    int rc = rm_host::check_launch("rm_fine_lists (count)");
+    if (rc) return rc;
     if ((rc = rm_scan_tiles(counts, Gf, incl, total_dev, scan_ws, rm_scan_workspace_size(Gf), stream))) return rc;
     rm::fine_lists_kernel<true><<<(unsigned)G, rm::kFineThreads, 0, s>>>(
-        sorted_ids, (const int2*)ranges, (const int4*)rect_fine, cam->grid_width, f, counts, incl, fine_ids, capacity,
+        sorted_ids, (const int2*)ranges, (const int4*)rect_fine, n_tets, views, f, counts, incl, fine_ids, capacity,
         (int2*)fine_ranges, status);
     return rm_host::check_launch("rm_fine_lists (write)");
+}
+
+}  // namespace
+
+extern "C" {
+
+int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* rect_fine, const rm_camera* cam,
+                  int fine_shift, int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges, int64_t* total_dev,
+                  void* workspace, size_t workspace_bytes, void* stream) {
+    rm::ViewSet views;
+    int rc = rm_host::make_views("rm_fine_lists", cam, 1, &views);
+    if (rc) return rc;
+    return fine_lists_impl("rm_fine_lists", sorted_ids, ranges, rect_fine, 0, views, fine_shift, capacity, fine_ids,
+                           fine_ranges, total_dev, workspace, workspace_bytes, stream);
+}
+
+int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* rect_fine, int64_t n_tets,
+                        const rm_camera* cams, int n_views, int fine_shift, int64_t capacity, int32_t* fine_ids,
+                        int32_t* fine_ranges, int64_t* total_dev, void* workspace, size_t workspace_bytes,
+                        void* stream) {
+    rm::ViewSet views;
+    int rc = rm_host::make_views("rm_fine_lists_multi", cams, n_views, &views);
+    if (rc) return rc;
+    return fine_lists_impl("rm_fine_lists_multi", sorted_ids, ranges, rect_fine, n_tets, views, fine_shift, capacity,
+                           fine_ids, fine_ranges, total_dev, workspace, workspace_bytes, stream);
 }
 
 }  // extern "C"

@@ -285,16 +285,24 @@ __global__ void __launch_bounds__(256) project_fwd_multi_kernel(const int4* __re
                                                                 const __grid_constant__ ViewSet views,
                                                                 int32_t* __restrict__ tiles, int4* __restrict__ rect,
                                                                 float* __restrict__ depth, int32_t* __restrict__ any,
-                                                                float* __restrict__ cc) {
+                                                                float* __restrict__ cc, int fine_shift,
+                                                                int4* __restrict__ rect_fine) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_tets) return;
     const TetGeom t = tet_geom(indices, verts, g);
     int total = 0;
     for (int v = 0; v < views.n; ++v) {
-        int4 r;
+        int4 r, rf;
         float dk;
-        const int n_tiles = project_view(views.cams[v], t, r, dk);
+        int nf;
         const int64_t o = (int64_t)v * n_tets + g;
+        int n_tiles;
+        if (rect_fine) {
+            n_tiles = project_view<true>(views.cams[v], t, r, dk, fine_shift, &rf, &nf);
+            rect_fine[o] = rf;
+        } else {
+            n_tiles = project_view(views.cams[v], t, r, dk);
+        }
         tiles[o] = n_tiles;
         rect[o] = r;
         depth[o] = dk;
@@ -441,7 +449,7 @@ int rm_project_fwd_fine(const int32_t* indices, const float* vertices, int64_t n
 
 int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,
                          const rm_camera* cams, int n_views, int32_t* tiles_touched, int32_t* rect, float* depth,
-                         int32_t* tiles_any, float* circumcenter, void* stream) {
+                         int32_t* tiles_any, float* circumcenter, int fine_shift, int32_t* rect_fine, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_project_fwd_multi", cams, n_views, &views);
     if (rc) return rc;
@@ -449,12 +457,16 @@ int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t 
     if (n_tets == 0) return RM_OK;
     if (!indices || !vertices || !tiles_touched || !rect || !depth)
         return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: NULL pointer");
-    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15))
-        return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: indices and rect must be 16-byte aligned");
+    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15) || ((uintptr_t)rect_fine & 15))
+        return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: indices and rects must be 16-byte aligned");
+    if (rect_fine && (fine_shift < 1 || fine_shift > 3 || (cams[0].tile_width >> fine_shift) << fine_shift !=
+                      cams[0].tile_width || (cams[0].tile_height >> fine_shift) << fine_shift != cams[0].tile_height))
+        return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: tile not divisible by 2^%d", fine_shift);
     const int threads = 256;
     const int64_t blocks = (n_tets + threads - 1) / threads;
     rm::project_fwd_multi_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
-        (const int4*)indices, vertices, n_tets, views, tiles_touched, (int4*)rect, depth, tiles_any, circumcenter);
+        (const int4*)indices, vertices, n_tets, views, tiles_touched, (int4*)rect, depth, tiles_any, circumcenter,
+        fine_shift, (int4*)rect_fine);
     return rm_host::check_launch("rm_project_fwd_multi");
 }
 

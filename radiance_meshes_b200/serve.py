@@ -89,14 +89,18 @@ class ResidentMesh:
                 self.records.numel())
 
 
-def batch_bytes(n_tets: int, views: B.ViewBatch, capacity: int) -> int:
+def batch_bytes(n_tets: int, views: B.ViewBatch, capacity: int, fine_shift: int = 0) -> int:
     """Device bytes a forward batch allocates (projection, lists, sort,
-    ranges, queue and per-pixel buffers)."""
+    ranges, fine lists, queue and per-pixel buffers)."""
     n = views.n
     L = C.lib()
     proj = n * n_tets * (4 + 16 + 4 + 4) + n_tets * 4 + int(L.rm_scan_workspace_size(n * n_tets))
     pairs = capacity * (8 + 4 + 8 + 4) + int(L.rm_sort_workspace_size(max(capacity, 1)))
-    tiles = views.n_tiles * 8 + int(L.rm_blend_workspace_size(0, views.n_tiles))  # no hit masks (forward only)
+    q = 1 << (2 * fine_shift)
+    blend_tiles = views.n_tiles * q
+    tiles = views.n_tiles * 8 + int(L.rm_blend_workspace_size(0, blend_tiles))  # no hit masks (forward only)
+    if fine_shift:
+        tiles += n * n_tets * 16 + capacity * q * 4 + blend_tiles * 8 + int(L.rm_fine_lists_workspace_size(blend_tiles))
     pixels = views.n_pixels * (8 + 16 + 20 + 4)
     return proj + pairs + tiles + pixels + 4096
 
@@ -125,7 +129,7 @@ class Server:
 
     def __init__(self, meshes: Sequence[ResidentMesh], streams: int = 4, max_views: int = 8,
                  hbm_budget: int | None = None, tile: int = 16, fwd_flags: int = 0, pair_headroom: float = 1.25,
-                 keep_outputs: bool = True, device=None):
+                 keep_outputs: bool = True, device=None, fine_shift: int = 0):
         self.device = torch.device(device or "cuda")
         self.meshes = {m.name: m for m in meshes}
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(streams)]
@@ -138,6 +142,7 @@ class Server:
         self.reserved = 0
         self.tile = int(tile)
         self.fwd_flags = int(fwd_flags)
+        self.fine_shift = int(fine_shift)  # blend on tiles 2^fine_shift times smaller (split lists)
         self.headroom = float(pair_headroom)
         self.pair_slack = 4096  # extra pair slots per batch
         self.keep_outputs = keep_outputs
@@ -201,10 +206,10 @@ class Server:
             mesh, q = self.meshes[name], self.pending[name]
             reqs = [q[0]]
             vb = B.ViewBatch([q[0].cam])
-            need = batch_bytes(mesh.T, vb, self._capacity(mesh, vb))
+            need = batch_bytes(mesh.T, vb, self._capacity(mesh, vb), self.fine_shift)
             for r in list(q)[1:self.max_views]:
                 vb2 = B.ViewBatch([x.cam for x in reqs] + [r.cam])
-                need2 = batch_bytes(mesh.T, vb2, self._capacity(mesh, vb2))
+                need2 = batch_bytes(mesh.T, vb2, self._capacity(mesh, vb2), self.fine_shift)
                 if self.reserved + need2 > self.hbm_budget:
                     break
                 reqs.append(r)
@@ -224,7 +229,8 @@ class Server:
         cap = capacity if capacity is not None else self._capacity(mesh, vb)
         with torch.cuda.stream(stream):
             rast = B.BatchedRasterizer(mesh.indices, mesh.vertices, mesh.cell_values, vb, capacity=cap,
-                                       fwd_flags=self.fwd_flags, records=mesh.records, hit_masks=False)
+                                       fwd_flags=self.fwd_flags, records=mesh.records, hit_masks=False,
+                                       fine_shift=self.fine_shift)
             rast.forward()
             total_host = torch.empty(1, dtype=torch.int64, pin_memory=True)
             total_host.copy_(rast.total, non_blocking=True)
@@ -250,7 +256,7 @@ class Server:
                 # overflow: re-run this batch with the exact pair count on the same stream
                 self.n_retries += 1
                 self.reserved -= b.nbytes
-                need = batch_bytes(b.mesh.T, b.rast.views, P)
+                need = batch_bytes(b.mesh.T, b.rast.views, P, self.fine_shift)
                 nb = self._launch(b.mesh, b.reqs, b.rast.views, need, capacity=P, stream_idx=b.stream_idx)
                 nb.retried = True
                 self.inflight.remove(nb)

@@ -189,10 +189,45 @@ def test_autotuner_returns_a_valid_choice(cuda, tmp_path, monkeypatch):
     i, v, c = _dev(mesh)
     out = AT.tune_batch(i, v, c, views, tiles=(8, 16))
     assert out["tile"] in (8, 16) and not out["cached"]
-    assert set(out["ms"]) == {"8", "16"}
+    assert set(out["ms"]) == {"8/8", "16/16", "16/8"}
     again = AT.tune_batch(i, v, c, views, tiles=(8, 16))
     assert again["cached"] and again["tile"] == out["tile"] and again["fwd_flags"] == out["fwd_flags"]
+    assert again["fine_shift"] == out["fine_shift"]
     cams_t = [tcam_to_struct(x.tcam(tile_size=out["tile"])) for x in views]
-    br = B.BatchedRasterizer(i, v, c, B.ViewBatch(cams_t), fwd_flags=out["fwd_flags"], bwd_flags=out["bwd_flags"])
+    br = B.BatchedRasterizer(i, v, c, B.ViewBatch(cams_t), fwd_flags=out["fwd_flags"], bwd_flags=out["bwd_flags"],
+                             fine_shift=out["fine_shift"])
     br.forward()
     br.check()
+
+
+@pytest.mark.parametrize("tile,shift", [(16, 1), (32, 1), (32, 2)])
+def test_batch_fine_split_gives_the_coarse_frames(cuda, tile, shift):
+    """Lists sorted on the cameras' tiles and split into tiles 2^shift times
+    smaller (rm_fine_lists_multi) render every view exactly as the
+    single-camera blend over the coarse lists; the gradients are the sum of
+    the single-camera gradients."""
+    mesh, views, cams = _scene(tile)
+    i, v, c = _dev(mesh)
+    vb = B.ViewBatch(cams)
+    jit = _jitter(vb, seed=6)
+    br = B.BatchedRasterizer(i, v, c, vb, jitter=jit, fine_shift=shift)
+    br.forward()
+    br.check()
+    g = torch.Generator("cuda").manual_seed(8)
+    gimg = torch.randn(vb.n_pixels, 4, device="cuda", generator=g)
+    gv_b, gc_b = br.backward(gimg, None)
+    torch.cuda.synchronize()
+    assert int(br.fine_total.item()) > int(br.total.item())
+    gv_s, gc_s = torch.zeros_like(v), torch.zeros_like(c)
+    pj, pg = vb.split(jit), vb.split(gimg)
+    for k, cam in enumerate(cams):
+        ref = _single(i, v, c, cam, pj[k].contiguous())
+        img_b, dist_b, _ = br.images()[k]
+        assert torch.equal(img_b.view(torch.int32), ref["img"].view(torch.int32))
+        assert torch.equal(dist_b.view(torch.int32), ref["dist"].view(torch.int32))
+        R.blend_bwd(ref["lists"].sorted_ids, ref["lists"].ranges, i, v, c, pj[k].contiguous(), cam, ref["img"],
+                    ref["dist"], ref["nc"], pg[k].contiguous(), None, ref["recs"], tiles_touched=ref["tiles"],
+                    grad_vertices=gv_s, grad_cell_values=gc_s)
+    torch.cuda.synchronize()
+    for a, b in ((gv_b, gv_s), (gc_b, gc_s)):
+        assert float((a - b).norm() / b.norm()) < 1e-5

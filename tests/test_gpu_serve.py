@@ -31,9 +31,14 @@ def _same(a, b):
             torch.equal(a.dist.view(torch.int32), b.dist.view(torch.int32)) and torch.equal(a.nc, b.nc))
 
 
-def _calibrate(server, meshes):
-    cams = [tcam_to_struct(v.tcam()) for v in scenes.ring_views(4, RES, radius=2.8)]
+def _calibrate(server, meshes, tile=None):
+    cams = [tcam_to_struct(v.tcam(tile_size=tile)) for v in scenes.ring_views(4, RES, radius=2.8)]
     server.calibrate({m.name: cams for m in meshes})
+
+
+def _views(n, seed=11, radius=2.8):
+    return [v for _, _, v in scenes.serving_trace(n, 500.0, ["ball", "cube"], seed=seed, resolutions=RES,
+                                                  radius=radius)]
 
 
 def test_results_same_alone_and_mixed(meshes):
@@ -51,6 +56,18 @@ def test_results_same_alone_and_mixed(meshes):
         a = alone.render_alone(q)
         assert a.batch_views == 1
         assert _same(a, by_id[q.rid]), q.rid
+
+
+def test_fine_split_serving_same_alone_and_mixed(meshes):
+    reqs = [S.RenderRequest(q.rid, q.mesh, tcam_to_struct(v.tcam(tile_size=16)), q.arrival)
+            for q, v in zip(_trace(24, seed=21), _views(24, seed=21))]
+    mixed = S.Server(meshes, streams=3, max_views=4, tile=16, fine_shift=1)
+    _calibrate(mixed, meshes, tile=16)
+    res = {r.rid: r for r in mixed.run_trace(reqs, realtime=False)}
+    alone = S.Server(meshes, streams=1, max_views=1, tile=16, fine_shift=1)
+    _calibrate(alone, meshes, tile=16)
+    for q in reqs:
+        assert _same(alone.render_alone(q), res[q.rid]), q.rid
 
 
 def test_overflow_is_retried(meshes):
