@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--sv-streams", type=int, default=4)
     ap.add_argument("--sv-max-views", type=int, default=8)
     ap.add_argument("--sv-tile", type=int, default=0, help="tile size (0: autotuned on the middle mesh)")
+    ap.add_argument("--sv-low-rate", type=float, default=120.0,
+                    help="a second Poisson run at this rate (0: none): latency below saturation")
     ap.add_argument("--mv-points", type=int, default=1_000_000)
     ap.add_argument("--mv-views", type=int, default=16)
     ap.add_argument("--mv-tile", type=int, default=0, help="tile size of the batched step (0: autotuned)")
@@ -632,6 +634,22 @@ def run_serving(args):
     with ClockSampler(local) as clocks:
         results = server.run_trace(reqs, realtime=True)
     launches = _capi.launch_count() - launches0
+    low = None
+    if args.sv_low_rate > 0:
+        n_low = args.sv_warmup + args.sv_requests // 2
+        trace_low = scenes.serving_trace(n_low, args.sv_low_rate, names, seed=9, tile_size=tile)
+        reqs_low = [S.RenderRequest(10 ** 6 + k, name, tcam_to_struct(v.tcam(tile_size=tile)), t)
+                    for k, (t, name, v) in enumerate(trace_low)]
+        res_low = sorted(server.run_trace(reqs_low, realtime=True), key=lambda r: r.rid)
+        low = dict(S.latency_summary(res_low, skip=args.sv_warmup), rate_req_per_s=args.sv_low_rate)
+    # capacity: the same server fed a backlog (all requests at once), frames/s
+    backlog = [S.RenderRequest(n_total + k, name, tcam_to_struct(v.tcam(tile_size=tile)), 0.0)
+               for k, (t, name, v) in enumerate(scenes.serving_trace(600, args.sv_rate, names, seed=8,
+                                                                       tile_size=tile))]
+    t_cap = time.perf_counter()
+    cap_res = server.run_trace(backlog, realtime=False)
+    torch.cuda.synchronize()
+    capacity_fps = len(cap_res) / (time.perf_counter() - t_cap)
     results.sort(key=lambda r: r.rid)
     summ = S.latency_summary(results, skip=args.sv_warmup)
     per_mesh = {}
@@ -646,6 +664,7 @@ def run_serving(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "p50_ms": summ["p50_ms"], "p90_ms": summ["p90_ms"], "p99_ms": summ["p99_ms"], "mean_ms": summ["mean_ms"],
         "max_ms": summ["max_ms"], "frames_per_s": summ["frames_per_s"],
+        "capacity_frames_per_s": capacity_fps, "at_lower_rate": low,
         "config": {"workload": f"serving: meshes {counts} mixture points (seeds {seeds}), tets {tets}, Poisson "
                                f"{args.sv_rate} req/s (seed 7), sphere poses r=4, resolutions 640x480/1280x720/"
                                f"1920x1080, forward only",

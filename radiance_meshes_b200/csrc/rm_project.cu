@@ -171,6 +171,38 @@ __device__ __forceinline__ TetGeom tet_geom(const int4* __restrict__ indices, co
     return t;
 }
 
+// Early cull of tets wholly outside the view: when all four vertices lie in
+// the open half-space beyond one side of the image (one pixel of margin) or
+// behind the camera, so does their hull, hence every vertex and clipped point
+// that find_extent keeps, and the rectangle below would come out empty.  The
+// test is linear in the vertices (no divisions) and only ever reports tets
+// that the full computation culls, with a tolerance far above its rounding.
+// It needs an affine world-to-camera matrix (last row 0 0 0 1).
+__device__ __forceinline__ bool outside_view(const rm_camera& c, const TetGeom& t) {
+    const float* M = c.world_view;
+    if (!(M[12] == 0.f && M[13] == 0.f && M[14] == 0.f && M[15] == 1.f)) return false;
+    const float fx = c.K[0], cx = c.K[2], fy = c.K[4], cy = c.K[5];
+    const float gw = (float)c.grid_width * (float)c.tile_width, gh = (float)c.grid_height * (float)c.tile_height;
+    const float m = 1.0f, tol = 1e-4f;
+    bool behind = true, left = true, right = true, top = true, bottom = true;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const f3 p = t.v[i];
+        const float x = fmaf(M[3], 1.0f, fmaf(M[2], p.z, fmaf(M[1], p.y, M[0] * p.x)));
+        const float y = fmaf(M[7], 1.0f, fmaf(M[6], p.z, fmaf(M[5], p.y, M[4] * p.x)));
+        const float z = fmaf(M[11], 1.0f, fmaf(M[10], p.z, fmaf(M[9], p.y, M[8] * p.x)));
+        const float az = fabsf(z);
+        const float ex = tol * (fabsf(fx * x) + (fabsf(cx) + gw + m) * az) + 1e-6f;
+        const float ey = tol * (fabsf(fy * y) + (fabsf(cy) + gh + m) * az) + 1e-6f;
+        behind &= z < 0.f;
+        left &= fmaf(fx, x, (cx + m) * z) < -ex;
+        right &= fmaf(gw + m - cx, z, -(fx * x)) < -ex;
+        top &= fmaf(fy, y, (cy + m) * z) < -ey;
+        bottom &= fmaf(gh + m - cy, z, -(fy * y)) < -ey;
+    }
+    return behind || left || right || top || bottom;
+}
+
 // Per-view part of vertex_shader (vertex_shader.slang:36-89): camera space,
 // find_extent, the depth key and the tile rectangle.  Returns the tile count
 // (0: culled, r and depth zero).
@@ -183,7 +215,7 @@ __device__ __forceinline__ int project_view(const rm_camera& cam, const TetGeom&
         *rf = {0, 0, 0, 0};
         *n_fine = 0;
     }
-    if (t.planar) return 0;
+    if (t.planar || outside_view(cam, t)) return 0;
     const f3 cs0 = point2cam(cam, t.v[0]), cs1 = point2cam(cam, t.v[1]);
     const f3 cs2 = point2cam(cam, t.v[2]), cs3 = point2cam(cam, t.v[3]);
     BBox box = {{1e20f, 1e20f, 1e20f}, {-1e20f, -1e20f, -1e20f}};
