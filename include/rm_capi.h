@@ -332,7 +332,9 @@ RM_API int rm_project_fwd_multi(const int32_t* indices, const float* vertices,
  * tile_base(v) * 4^fine_shift), using rect_fine [n_views, T, 4] of
  * rm_project_fwd_multi.  Blending a batch of the fine cameras (tiles
  * 2^fine_shift times smaller, grids that much larger) over these lists gives
- * the coarse batch's images bit for bit.
+ * the coarse batch's images bit for bit.  rect_fine may be NULL when
+ * fine_shift is 1 and the sorted values carry the packed 2x2 coverage bits of
+ * rm_emit_pairs_multi; fine_ids then hold the plain tet ids.
  */
 RM_API int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges,
                                const int32_t* rect_fine, int64_t n_tets,
@@ -345,14 +347,20 @@ RM_API int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges,
  * Pair emission for the stacked projection: offsets is the inclusive scan of
  * tiles_touched [n_views * T].  Pair (view v, tet g, tile (x, y)) gets the key
  * ((tile_base(v) + y * grid_w(v) + x) << 32) | sortable(depth[v, g]) and the
- * value g.  Capacity handling as rm_emit_pairs.
+ * value g.  Capacity handling as rm_emit_pairs.  rect_fine_2x (optional,
+ * [n_views, T, 4], rm_project_fwd_multi's rectangles for fine_shift 1): the
+ * value then also carries, in bits 28..31, which of the tile's 2x2 fine tiles
+ * the fine rectangle covers (bit qy * 2 + qx; T < 2^28), for
+ * rm_fine_lists_multi to split the sorted lists without reading the
+ * rectangles again.  Such values are not plain tet ids.
  */
 RM_API int rm_emit_pairs_multi(const float* depth, const int32_t* rect,
                                const int32_t* offsets, int64_t n_tets,
                                const rm_camera* cams, int n_views,
                                int64_t capacity, const int64_t* total_dev,
                                int64_t* keys, int32_t* values,
-                               uint32_t* status_dev, void* stream);
+                               uint32_t* status_dev, const int32_t* rect_fine_2x,
+                               void* stream);
 
 /* Total tile count of a batch (the ranges length and the blend workspace's
  * n_tiles), or -1 on bad input. */

@@ -72,7 +72,7 @@ SIGNATURES = {
                                             ctypes.c_int, vp, vp]),
     "rm_fine_lists_multi": (ctypes.c_int, [vp, vp, vp, i64, camp, ctypes.c_int, ctypes.c_int, i64, vp, vp, vp, vp,
                                            sz, vp]),
-    "rm_emit_pairs_multi": (ctypes.c_int, [vp, vp, vp, i64, camp, ctypes.c_int, i64, vp, vp, vp, vp, vp]),
+    "rm_emit_pairs_multi": (ctypes.c_int, [vp, vp, vp, i64, camp, ctypes.c_int, i64, vp, vp, vp, vp, vp, vp]),
     "rm_views_tile_count": (i64, [camp, ctypes.c_int]),
     "rm_blend_records_size": (sz, [i64]),
     "rm_blend_pack_records": (ctypes.c_int, [vp, vp, vp, i64, i64, vp, vp, vp]),

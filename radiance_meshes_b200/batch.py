@@ -212,9 +212,13 @@ class BatchedRasterizer:
 
     def _lists(self):
         L, s, v = C.lib(), C.stream_handle(), self.views
-        R._call("rm_emit_pairs_multi", lambda: L.rm_emit_pairs_multi(C.ptr(self.depth), C.ptr(self.rect), C.ptr(self.offsets), self.T, v.array,
-                                      v.n, self.capacity, C.ptr(self.total), C.ptr(self.keys), C.ptr(self.vals),
-                                      C.ptr(self.status), s))
+        # fine_shift 1: the 2x2 coverage bits ride in the sorted values, so the
+        # split reads no rectangles
+        packed = self.fine_shift == 1 and self.T < (1 << 28)
+        rfp = self.rect_fine if packed else None
+        R._call("rm_emit_pairs_multi", lambda: L.rm_emit_pairs_multi(
+            C.ptr(self.depth), C.ptr(self.rect), C.ptr(self.offsets), self.T, v.array, v.n, self.capacity,
+            C.ptr(self.total), C.ptr(self.keys), C.ptr(self.vals), C.ptr(self.status), C.ptr(rfp), s))
         R._call("rm_sort_pairs", lambda: L.rm_sort_pairs(C.ptr(self.keys), C.ptr(self.vals), self.capacity, C.ptr(self.total), v.end_bit,
                                 C.ptr(self.sorted_keys), C.ptr(self.sorted_ids), C.ptr(self.sort_ws),
                                 self.sort_ws.numel(), s))
@@ -222,7 +226,8 @@ class BatchedRasterizer:
                                  v.n_tiles, s))
         if self.fine_shift:
             R._call("rm_fine_lists", lambda: L.rm_fine_lists_multi(
-                C.ptr(self.sorted_ids), C.ptr(self.ranges), C.ptr(self.rect_fine), self.T, v.array, v.n,
+                C.ptr(self.sorted_ids), C.ptr(self.ranges), None if packed else C.ptr(self.rect_fine), self.T,
+                v.array, v.n,
                 self.fine_shift, self.fine_ids.shape[0], C.ptr(self.fine_ids), C.ptr(self.fine_ranges),
                 C.ptr(self.fine_total), C.ptr(self.fine_ws), self.fine_ws.numel(), s))
 

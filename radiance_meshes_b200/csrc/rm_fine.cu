@@ -29,7 +29,7 @@ __device__ __forceinline__ bool covers(int4 fr, int fx, int fy) {
 // Views: tile t of the coarse (global, view-major) numbering belongs to view
 // v = views.find(t); its fine tiles are numbered view-major too, view v's
 // starting at tiles[v] * f^2; rect_fine rows are stacked view-major ([v, T]).
-template <bool WRITE>
+template <bool WRITE, bool PACKED>
 __global__ void __launch_bounds__(kFineThreads) fine_lists_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const int4* __restrict__ rect_fine,
     int64_t n_tets, const __grid_constant__ ViewSet views, int f, int32_t* __restrict__ counts,
@@ -63,19 +63,25 @@ __global__ void __launch_bounds__(kFineThreads) fine_lists_kernel(
         const int e = base + (int)threadIdx.x;
         int4 fr = {0, 0, 0, 0};
         int32_t g = 0;
+        uint32_t packed = 0;  // PACKED: the 2x2 coverage bits carried in the value's top bits
         if (e < r.y) {
             g = __ldg(ids + e);
-            fr = __ldg(rf_v + g);
+            if (PACKED) {
+                packed = (uint32_t)g >> 28;
+                g &= 0x0fffffff;
+            } else {
+                fr = __ldg(rf_v + g);
+            }
         }
         for (int q = 0; q < Q; ++q) {
-            const bool in = covers(fr, tx * f + q % f, ty * f + q / f);
+            const bool in = PACKED ? ((packed >> q) & 1u) != 0 : covers(fr, tx * f + q % f, ty * f + q / f);
             const unsigned bal = __ballot_sync(0xffffffffu, in);
             if (lane == 0) wtot[warp][q] = __popc(bal);
         }
         __syncthreads();
         if (WRITE) {
             for (int q = 0; q < Q; ++q) {
-                const bool in = covers(fr, tx * f + q % f, ty * f + q / f);
+                const bool in = PACKED ? ((packed >> q) & 1u) != 0 : covers(fr, tx * f + q % f, ty * f + q / f);
                 const unsigned bal = __ballot_sync(0xffffffffu, in);
                 if (in) {
                     uint32_t pos = run[q] + __popc(bal & lt);
@@ -131,7 +137,10 @@ int fine_lists_impl(const char* who, const int32_t* sorted_ids, const int32_t* r
     const int64_t G = views.tiles[views.n];
     const int64_t Gf = G * f * f;
     if (Gf >= (int64_t)INT32_MAX) return rm_host::fail(RM_EINVAL, "%s: too many tiles", who);
-    if (!ranges || !rect_fine || !fine_ranges || !total_dev || !workspace || (capacity > 0 && (!sorted_ids || !fine_ids)))
+    // no rect_fine: the 2x2 coverage bits come packed in bits 28..31 of the ids
+    const bool packed = rect_fine == nullptr;
+    if (packed && fine_shift != 1) return rm_host::fail(RM_EINVAL, "%s: packed masks need fine_shift 1", who);
+    if (!ranges || !fine_ranges || !total_dev || !workspace || (capacity > 0 && (!sorted_ids || !fine_ids)))
         return rm_host::fail(RM_EINVAL, "%s: NULL pointer", who);
     if (((uintptr_t)rect_fine & 15) || ((uintptr_t)ranges & 7) || ((uintptr_t)fine_ranges & 7) ||
         ((uintptr_t)workspace & 255))
@@ -146,15 +155,16 @@ int fine_lists_impl(const char* who, const int32_t* sorted_ids, const int32_t* r
     char* scan_ws = p + 2 * rm::align256((size_t)Gf * 4) + 256;
     uint32_t* status = (uint32_t*)scan_ws;  // the scan workspace's status word
     cudaStream_t s = (cudaStream_t)stream;
-    rm::fine_lists_kernel<false><<<(unsigned)G, rm::kFineThreads, 0, s>>>(
-        sorted_ids, (const int2*)ranges, (const int4*)rect_fine, n_tets, views, f, counts, nullptr, nullptr, 0,
-        nullptr, nullptr);
+    auto count = packed ? rm::fine_lists_kernel<false, true> : rm::fine_lists_kernel<false, false>;
+    auto write = packed ? rm::fine_lists_kernel<true, true> : rm::fine_lists_kernel<true, false>;
+    count<<<(unsigned)G, rm::kFineThreads, 0, s>>>(sorted_ids, (const int2*)ranges, (const int4*)rect_fine, n_tets,
+                                                   views, f, counts, nullptr, nullptr, 0, nullptr, nullptr);
     int rc = rm_host::check_launch("rm_fine_lists (count)");
     if (rc) return rc;
     if ((rc = rm_scan_tiles(counts, Gf, incl, total_dev, scan_ws, rm_scan_workspace_size(Gf), stream))) return rc;
-    rm::fine_lists_kernel<true><<<(unsigned)G, rm::kFineThreads, 0, s>>>(
-        sorted_ids, (const int2*)ranges, (const int4*)rect_fine, n_tets, views, f, counts, incl, fine_ids, capacity,
-        (int2*)fine_ranges, status);
+    write<<<(unsigned)G, rm::kFineThreads, 0, s>>>(sorted_ids, (const int2*)ranges, (const int4*)rect_fine, n_tets,
+                                                   views, f, counts, incl, fine_ids, capacity, (int2*)fine_ranges,
+                                                   status);
     return rm_host::check_launch("rm_fine_lists (write)");
 }
 

@@ -142,7 +142,7 @@ def test_view_batch_rejects_bad_batches():
     ok = (RMCamera * 2)(*cams)
     assert L.rm_project_fwd_multi(None, None, 10, 10, ok, 2, None, None, None, None, None, 0, None, None) == C.RM_EINVAL
     assert L.rm_project_fwd_multi(None, None, 0, 0, ok, 2, None, None, None, None, None, 0, None, None) == C.RM_OK
-    assert L.rm_emit_pairs_multi(None, None, None, 0, ok, 2, 0, None, None, None, None, None) == C.RM_OK
+    assert L.rm_emit_pairs_multi(None, None, None, 0, ok, 2, 0, None, None, None, None, None, None) == C.RM_OK
 
 
 def test_autotune_flag_packing():
