@@ -409,6 +409,29 @@ RM_API int rm_blend_bwd_multi(const int32_t* sorted_ids, const int32_t* ranges,
                               const void* records, void* workspace,
                               size_t workspace_bytes, int flags, void* stream);
 
+/* ------------------------------------------- densification statistics -- */
+/*
+ * Per-tet statistics of one view for densification.  Replaces calc_tet_err
+ * (delaunay_rasterization/internal/slang/alphablend_shader_interp.slang:433-599)
+ * launched by render_err (delaunay_rasterization/internal/render_err.py:138-150).
+ * Walks the tile lists front to back from each pixel centre; for every hit
+ * adds to tet_err [T,16] (float, accumulated) in columns 0, 1, 2, 5: T, T*e,
+ * T*e^2, T*s (T = exp(log T) * density * dt, e = pixel_err [H,W], s = ssim_err
+ * [H,W]), 6-8 / 9-11 / 13-15: T times the entry point / exit point / segment
+ * midpoint, 12: T; and to tet_count [T,2] (int32, accumulated) the hit count
+ * and the maximum of int(65535 * T).  Columns 3 and 4 are left untouched, as
+ * in the reference, whose walk also starts from log T = 1 and stops once
+ * log T < -5.5.  Workspace and flags as rm_blend_fwd (records are packed
+ * unless RM_BLEND_REUSE_RECORDS).
+ */
+RM_API int rm_calc_tet_err(const int32_t* sorted_ids, const int32_t* ranges,
+                           const int32_t* indices, const float* vertices,
+                           const float* cell_values, int64_t n_tets, int64_t n_verts,
+                           const int32_t* tiles_touched, const rm_camera* cam,
+                           const float* pixel_err, const float* ssim_err,
+                           float* tet_err, int32_t* tet_count, void* workspace,
+                           size_t workspace_bytes, int flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

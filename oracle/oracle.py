@@ -54,6 +54,8 @@ def lib():
                                         f32p, f32p, i32p, f32p, ctypes.c_void_p, f64p, f64p]
         L.orc_blend_bwd_f64.argtypes = [i32p, i32p, i32p, f64p, f64p, ctypes.c_int64, f32p, cam,
                                         f64p, f64p, i32p, f64p, ctypes.c_void_p, f64p, f64p]
+        L.orc_calc_tet_err.argtypes = [i32p, i32p, i32p, f32p, f32p, ctypes.c_int64, cam, f32p, f32p, f64p,
+                                       i64p, i32p]
         L.orc_linear_loss_f64.restype = ctypes.c_double
         L.orc_linear_loss_f64.argtypes = [i32p, i32p, i32p, f64p, f64p, ctypes.c_int64, f32p, cam,
                                           ctypes.c_void_p, f64p, ctypes.c_void_p, ctypes.c_void_p]
@@ -140,6 +142,19 @@ def rasterize_lists(indices, vertices, tcam):
     ranges = tile_ranges(sk, cs.grid_width * cs.grid_height)
     return dict(cam=cs, tiles_touched=tiles, rect=rect, vs=vs, circumcenter=cc, offsets=offsets,
                 keys=keys, values=vals, sorted_keys=sk, sorted_ids=sv, ranges=ranges)
+
+
+def calc_tet_err(lists, indices, vertices, cell_values, pixel_err, ssim_err):
+    """calc_tet_err (alphablend_shader_interp.slang:433-599) on the CPU:
+    returns (tet_err [T,16] float64, count [T] int64, tmax [T] int32)."""
+    T = len(indices)
+    err = np.zeros((T, 16), np.float64)
+    cnt = np.zeros(T, np.int64)
+    tmax = np.zeros(T, np.int32)
+    lib().orc_calc_tet_err(_c(lists["sorted_ids"], np.int32), _c(lists["ranges"], np.int32), _c(indices, np.int32),
+                           _c(vertices, np.float32), _c(cell_values, np.float32), T, cam_ref(lists["cam"]),
+                           _c(pixel_err, np.float32), _c(ssim_err, np.float32), err, cnt, tmax)
+    return err, cnt, tmax
 
 
 def blend_fwd_f32(lists, indices, vertices, cell_values, jitter):

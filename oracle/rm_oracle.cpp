@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <climits>
 #include <cstring>
 #include <vector>
 
@@ -753,6 +754,74 @@ ORC_API void orc_ranges(const int64_t* keys, int64_t n, int32_t* ranges, int64_t
             }
         }
         if (i == n - 1) ranges[2 * (int64_t)cur + 1] = (int32_t)n;
+    }
+}
+
+// float -> int32 conversion with truncation, saturating like the GPU's
+// cvt.rzi.s32.f32 (NaN -> 0).
+inline int32_t f2i_rz_sat(float x) {
+    if (std::isnan(x)) return 0;
+    if (x >= 2147483648.0f) return INT32_MAX;
+    if (x <= -2147483648.0f) return INT32_MIN;
+    return (int32_t)x;
+}
+
+// calc_tet_err / kern_calc_tet_err (alphablend_shader_interp.slang:433-599),
+// FP32 walk from each pixel centre; per hit T = exp(log T) * density * dt with
+// log T starting at 1 (the reference initialises the state alpha with 1) and
+// the walk stopping once log T < -5.5.  Columns 0,1,2,5,6..15 of tet_err
+// receive T, T e, T e^2, T s, T p_enter, T p_exit, T, T p_mid (sums in double);
+// count[g] the hits, tmax[g] the maximum of int(65535 T).
+ORC_API void orc_calc_tet_err(const int32_t* ids, const int32_t* ranges, const int32_t* indices,
+                              const float* verts, const float* cv, int64_t T, const rm_camera* cam,
+                              const float* pixel_err, const float* ssim_err, double* tet_err, int64_t* count,
+                              int32_t* tmax) {
+    Cam<float> c = load_cam<float>(cam);
+    int64_t G = (int64_t)c.gw * c.gh;
+    std::vector<Rec<float>> recs;
+    build_recs(indices, verts, cv, T, recs, needed_tets(ids, ranges, G, T));
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t t = 0; t < G; ++t) {
+        int tx = (int)(t % c.gw), ty = (int)(t / c.gw);
+        int32_t s0 = ranges[2 * t], s1 = ranges[2 * t + 1];
+        for (int ly = 0; ly < c.th; ++ly)
+            for (int lx = 0; lx < c.tw; ++lx) {
+                int px = tx * c.tw + lx, py = ty * c.th + ly;
+                if (px >= c.W || py >= c.H) continue;
+                int64_t pix = (int64_t)py * c.W + px;
+                V3<float> o, d;
+                make_ray(c, px, py, 0.5f, 0.5f, o, d);
+                const float e = pixel_err[pix], sv = ssim_err[pix];
+                float logT = 1.0f;
+                for (int32_t j = s0; j < s1; ++j) {
+                    const int32_t g = ids[j];
+                    const Rec<float>& r = recs[g];
+                    Hit<float> h;
+                    if (!intersect(r, o, d, h)) continue;
+                    const float dt = std::fmax(h.exit - h.enter, 0.f);
+                    const float a = r.density * dt;
+                    if (!(a > 0.f)) continue;
+                    const float Tw = std::exp(logT) * a;
+                    const float mid = 0.5f * (h.enter + h.exit);
+                    const float v[16] = {Tw, Tw * e, Tw * e * e, 0.f, 0.f, Tw * sv,
+                                         Tw * std::fma(h.enter, d.x, o.x), Tw * std::fma(h.enter, d.y, o.y),
+                                         Tw * std::fma(h.enter, d.z, o.z), Tw * std::fma(h.exit, d.x, o.x),
+                                         Tw * std::fma(h.exit, d.y, o.y), Tw * std::fma(h.exit, d.z, o.z), Tw,
+                                         Tw * std::fma(mid, d.x, o.x), Tw * std::fma(mid, d.y, o.y),
+                                         Tw * std::fma(mid, d.z, o.z)};
+                    for (int k = 0; k < 16; ++k)
+                        if (k != 3 && k != 4) atomic_addd(tet_err + 16 * (int64_t)g + k, (double)v[k]);
+                    const int32_t ti = f2i_rz_sat(65535.0f * Tw);
+#pragma omp atomic
+                    count[g] += 1;
+                    int32_t cur = __atomic_load_n(tmax + g, __ATOMIC_RELAXED);
+                    while (ti > cur && !__atomic_compare_exchange_n(tmax + g, &cur, ti, true, __ATOMIC_RELAXED,
+                                                                    __ATOMIC_RELAXED)) {
+                    }
+                    logT = logT - a;
+                    if (logT < -5.5f) break;
+                }
+            }
     }
 }
 

@@ -15,7 +15,7 @@ def install_dropin() -> None:
     drop-in modules (same names and signatures as the reference)."""
     from . import delaunay_rasterization as pkg
     from .delaunay_rasterization import internal
-    from .delaunay_rasterization.internal import (alphablend_tiled_slang_interp, render_grid,
+    from .delaunay_rasterization.internal import (alphablend_tiled_slang_interp, render_err, render_grid,
                                                   tile_shader_slang, util)
 
     sys.modules["delaunay_rasterization"] = pkg
@@ -24,3 +24,4 @@ def install_dropin() -> None:
     sys.modules["delaunay_rasterization.internal.alphablend_tiled_slang_interp"] = alphablend_tiled_slang_interp
     sys.modules["delaunay_rasterization.internal.render_grid"] = render_grid
     sys.modules["delaunay_rasterization.internal.util"] = util
+    sys.modules["delaunay_rasterization.internal.render_err"] = render_err

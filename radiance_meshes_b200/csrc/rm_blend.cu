@@ -1217,6 +1217,147 @@ __global__ void __launch_bounds__(NT, 512 / NT) blend_bwd_pair_kernel(
     }
 }
 
+// ------------------------------------------------------ per-tet statistics --
+// calc_tet_err / kern_calc_tet_err (alphablend_shader_interp.slang:433-599):
+// the forward walk from each pixel centre, accumulating per hit into
+// tet_err[g, c] (float) the weight T = exp(log T) * a and its products with
+// the pixel's error, squared error and SSIM error, the entry / exit points
+// and the midpoint of the segment, and into tet_count[g] the hit count and
+// the maximum of int(65535 * T).  As in the reference the walk starts from
+// log T = 1 (its kern_calc_tet_err initialises the state alpha with 1) and
+// stops once log T < -5.5.  Sums are formed per list entry across a work
+// item (warp reduce-scatter, shared atomics) before one global atomic per
+// (item, entry, column), instead of 16 atomics per (pixel, hit).
+constexpr int kErrVals = 14;
+__constant__ int kErrCol[kErrVals] = {0, 1, 2, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15};
+
+template <int B>
+struct ErrSmem {
+    float4 srec[B][kRecFloat4];
+    int32_t sid[B];
+    float sacc[B][kErrVals];
+    int32_t scount[B];
+    int32_t smax[B];
+};
+
+template <int NT, int B>
+__device__ __forceinline__ void err_item(int tile, int sub, const int32_t* __restrict__ ids,
+                                         const int2* __restrict__ ranges, const float4* __restrict__ recs,
+                                         const rm_camera& cam, const float* __restrict__ pixel_err,
+                                         const float* __restrict__ ssim_err, float* __restrict__ tet_err,
+                                         int32_t* __restrict__ tet_count, ErrSmem<B>& S) {
+    constexpr unsigned kMask = WarpShape<NT>::kMask;
+    const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
+    int lx, ly;
+    strip_pixel<NT>(cam, sub, (int)threadIdx.x, lx, ly);
+    const int px = tx * cam.tile_width + lx, py = ty * cam.tile_height + ly;
+    const bool inside = px < cam.image_width && py < cam.image_height;
+    const int64_t pix = (int64_t)py * cam.image_width + px;
+    const int lane = threadIdx.x & 31;
+    f3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
+    float err = 0.f, serr = 0.f;
+    if (inside) {
+        make_ray(cam, px, py, 0.5f, 0.5f, o, d);  // pixel centre
+        err = __ldg(pixel_err + pix);
+        serr = __ldg(ssim_err + pix);
+    }
+    float logT = 1.0f;
+    bool active = inside;
+    const int2 rg = __ldg(ranges + tile);
+    for (int base = rg.x; base < rg.y && __syncthreads_or(active); base += B) {
+        const int n = min(B, rg.y - base);
+        for (int k = threadIdx.x; k < n; k += NT) {
+            S.sid[k] = __ldg(ids + base + k);
+            S.scount[k] = 0;
+            S.smax[k] = 0;
+        }
+        for (int k = threadIdx.x; k < n * kErrVals; k += NT) (&S.sacc[0][0])[k] = 0.f;
+        __syncthreads();
+        for (int k = threadIdx.x; k < n * kRecFloat4; k += NT) {
+            const int j = k >> 3, c = k & 7;
+            S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
+        }
+        __syncthreads();
+        for (int j = 0; j < n; ++j) {
+            if (!__any_sync(kMask, active)) break;
+            const float4* q = S.srec[j];
+            const Isect is = intersect<false>(q, o, d);
+            const float dt = fmaxf(is.exit - is.enter, 0.f);
+            const float a = q[0].w * dt;
+            const bool hit = active && is.geo && a > 0.f;
+            float v[kErrVals];
+#pragma unroll
+            for (int k = 0; k < kErrVals; ++k) v[k] = 0.f;
+            int tint = 0;
+            if (hit) {
+                const float T = expf(logT) * a;
+                const float mid = 0.5f * (is.enter + is.exit);
+                v[0] = T;
+                v[1] = T * err;
+                v[2] = T * err * err;
+                v[3] = T * serr;
+                v[4] = T * fmaf(is.enter, d.x, o.x);
+                v[5] = T * fmaf(is.enter, d.y, o.y);
+                v[6] = T * fmaf(is.enter, d.z, o.z);
+                v[7] = T * fmaf(is.exit, d.x, o.x);
+                v[8] = T * fmaf(is.exit, d.y, o.y);
+                v[9] = T * fmaf(is.exit, d.z, o.z);
+                v[10] = T;
+                v[11] = T * fmaf(mid, d.x, o.x);
+                v[12] = T * fmaf(mid, d.y, o.y);
+                v[13] = T * fmaf(mid, d.z, o.z);
+                tint = __float2int_rz(65535.0f * T);
+                logT = logT - a;
+                if (logT < kTermLogT) active = false;
+            }
+            if (__any_sync(kMask, hit)) {
+                using RS = ReduceScatter<kErrVals, WarpShape<NT>::kTopOffset>;
+                int slot = 0;
+                RS::template run<kMask>(v, lane, slot);
+#pragma unroll
+                for (int r = 0; r < RS::R; ++r)
+                    if (slot + r < kErrVals && v[r] != 0.f) atomicAdd(&S.sacc[j][slot + r], v[r]);
+                const unsigned bal = __ballot_sync(kMask, hit);
+#pragma unroll
+                for (int off = WarpShape<NT>::kTopOffset; off > 0; off >>= 1)
+                    tint = max(tint, __shfl_xor_sync(kMask, tint, off));
+                if (lane == 0) {
+                    atomicAdd(&S.scount[j], __popc(bal));
+                    atomicMax(&S.smax[j], tint);
+                }
+            }
+        }
+        __syncthreads();
+        for (int jj = threadIdx.x; jj < n; jj += NT) {
+            const int cnt = S.scount[jj];
+            if (cnt == 0) continue;
+            const int64_t g = S.sid[jj];
+            float* te = tet_err + 16 * g;
+#pragma unroll
+            for (int k = 0; k < kErrVals; ++k)
+                if (S.sacc[jj][k] != 0.f) atomicAdd(te + kErrCol[k], S.sacc[jj][k]);
+            atomicAdd(tet_count + 2 * g, cnt);
+            atomicMax(tet_count + 2 * g + 1, S.smax[jj]);
+        }
+    }
+}
+
+template <int NT, int B>
+__global__ void __launch_bounds__(NT, (NT >= 64 ? 1024 / NT : 32)) err_kernel(
+    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
+    const rm_camera cam, const float* __restrict__ pixel_err, const float* __restrict__ ssim_err,
+    float* __restrict__ tet_err, int32_t* __restrict__ tet_count, const Queue q) {
+    __shared__ ErrSmem<B> S;
+    __shared__ int s_item;
+    const int n_items = queue_items(q);
+    for (;;) {
+        const int item = next_item(q, &s_item);
+        if (item >= n_items) return;
+        err_item<NT, B>(queue_tile(q, item), item % q.subs, ids, ranges, recs, cam, pixel_err, ssim_err, tet_err,
+                        tet_count, S);
+    }
+}
+
 struct BlendWs {
     float4* recs;
     int32_t* order;
@@ -1594,6 +1735,42 @@ size_t rm_blend_hit_mask_bytes(int64_t n_pairs, int64_t n_tiles, int tile_pixels
     const int64_t subs = tile_pixels > 64 ? tile_pixels / 64 : 1;
     const int64_t blocks = (n_pairs > 0 ? n_pairs : 0) / 32 + (n_tiles > 0 ? n_tiles : 0) + 2;
     return 256 + (size_t)blocks * (size_t)subs * 64 * sizeof(uint32_t);
+}
+
+int rm_calc_tet_err(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices, const float* vertices,
+                    const float* cell_values, int64_t n_tets, int64_t n_verts, const int32_t* tiles_touched,
+                    const rm_camera* cam, const float* pixel_err, const float* ssim_err, float* tet_err,
+                    int32_t* tet_count, void* workspace, size_t workspace_bytes, int flags, void* stream) {
+    using namespace rm;
+    int rc = rm_host::check_cam(cam);
+    if (rc) return rc;
+    const int64_t G = (int64_t)cam->grid_width * cam->grid_height;
+    // the camera check of the blend calls; jitter is unused (pixel centres)
+    rc = check_blend_args("rm_calc_tet_err", indices, vertices, cell_values, n_tets, pixel_err, cam, G, workspace,
+                          workspace_bytes, flags);
+    if (rc) return rc;
+    if (!ranges || !ssim_err || !tet_err || !tet_count) return rm_host::fail(RM_EINVAL, "rm_calc_tet_err: NULL pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    const BlendWs w = blend_ws(workspace, n_tets, G, workspace_bytes);
+    if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
+        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
+        if (rc) return rc;
+    }
+    // every tile in one heavy-first queue (heavy_shift 1 marks all tiles heavy)
+    if ((rc = launch_order(ranges, (int)G, w, 1, s))) return rc;
+    const int strip = strip_pixels(cam, flags);
+    const int subs = cam->tile_width * cam->tile_height / strip;
+    const Queue qd = {w.order, w.info, w.tickets + 0, (int)G, subs, true, HitMasks{nullptr, 0, nullptr}};
+    if (strip == 16) {
+        const int grid = persistent_grid(err_kernel<16, 32>, 16, 0, (int)G * subs);
+        err_kernel<16, 32><<<grid, 16, 0, s>>>(sorted_ids, (const int2*)ranges, w.recs, *cam, pixel_err, ssim_err,
+                                                tet_err, tet_count, qd);
+    } else {
+        const int grid = persistent_grid(err_kernel<64, 32>, 64, 0, (int)G * subs);
+        err_kernel<64, 32><<<grid, 64, 0, s>>>(sorted_ids, (const int2*)ranges, w.recs, *cam, pixel_err, ssim_err,
+                                                tet_err, tet_count, qd);
+    }
+    return rm_host::check_launch("rm_calc_tet_err");
 }
 
 size_t rm_blend_records_size(int64_t n_tets) {

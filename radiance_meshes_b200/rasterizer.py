@@ -30,6 +30,7 @@ __all__ = [
     "build_tile_lists",
     "blend_fwd",
     "blend_bwd",
+    "calc_tet_err",
     "end_bit_for",
     "read_status",
 ]
@@ -389,6 +390,34 @@ def blend_bwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, ca
                                  C.ptr(grad_vertices), C.ptr(grad_cell_values), C.ptr(records), records.numel(),
                                  flags, _stream()))
     return grad_vertices, grad_cell_values
+
+
+def calc_tet_err(sorted_ids, ranges, indices, vertices, cell_values, cam: RMCamera, pixel_err, ssim_err,
+                 tiles_touched=None, tet_err=None, tet_count=None):
+    """Per-tet densification statistics of one view (rm_calc_tet_err):
+    accumulates into tet_err [T,16] float32 and tet_count [T,2] int32
+    (allocated zeroed when not given) and returns them."""
+    _require_cuda(sorted_ids=sorted_ids, ranges=ranges, indices=indices, vertices=vertices,
+                  cell_values=cell_values, pixel_err=pixel_err, ssim_err=ssim_err)
+    indices = _i32(indices)
+    vertices = _f32(vertices)
+    cell_values = _f32(cell_values)
+    pixel_err = _f32(pixel_err)
+    ssim_err = _f32(ssim_err)
+    T = indices.shape[0]
+    dev = vertices.device
+    if tet_err is None:
+        tet_err = torch.zeros((T, 16), dtype=torch.float32, device=dev)
+    if tet_count is None:
+        tet_count = torch.zeros((T, 2), dtype=torch.int32, device=dev)
+    L = C.lib()
+    ws_n = L.rm_blend_workspace_size(T, cam.grid_width * cam.grid_height)
+    ws = _POOL.get("err", ws_n, dev)
+    _call("rm_calc_tet_err", lambda: L.rm_calc_tet_err(
+        C.ptr(sorted_ids), C.ptr(ranges), C.ptr(indices), C.ptr(vertices), C.ptr(cell_values), T, vertices.shape[0],
+        C.ptr(tiles_touched), ctypes.byref(cam), C.ptr(pixel_err), C.ptr(ssim_err), C.ptr(tet_err),
+        C.ptr(tet_count), C.ptr(ws), ws_n, 0, _stream()))
+    return tet_err, tet_count
 
 
 def read_status(workspace: torch.Tensor) -> int:

@@ -130,3 +130,45 @@ def test_ranges_empty_tiles():
     keys = (np.array([1, 1, 3, 3, 3, 6], np.int64) << 32)
     r = O.tile_ranges(keys, 8)
     assert r.tolist() == [[0, 0], [0, 2], [0, 0], [2, 5], [0, 0], [0, 0], [5, 6], [0, 0]]
+
+
+def test_ssim_map_properties():
+    import torch
+
+    from radiance_meshes_b200.ssim import ssim_map
+
+    g = torch.Generator().manual_seed(0)
+    a = torch.rand(3, 40, 50, generator=g)
+    assert torch.allclose(ssim_map(a, a), torch.ones_like(a), atol=1e-6)
+    b = (a + 0.1 * torch.randn(3, 40, 50, generator=g)).clamp(0, 1)
+    m = ssim_map(a, b)
+    assert m.shape == a.shape and float(m.mean()) < 0.99
+    assert torch.allclose(m, ssim_map(b, a), atol=1e-6)  # symmetric
+    # a constant image against itself shifted by a constant: mean term only
+    c1 = torch.full((1, 30, 30), 0.3)
+    c2 = torch.full((1, 30, 30), 0.5)
+    inner = ssim_map(c1, c2)[0, 10:20, 10:20]
+    expect = (2 * 0.3 * 0.5 + 1e-4) / (0.09 + 0.25 + 1e-4)
+    assert torch.allclose(inner, torch.full_like(inner, expect), atol=1e-4)  # float32 variance residue
+
+
+def test_oracle_calc_tet_err_basic():
+    """Hit counts of calc_tet_err equal the hits the FP32 forward walk makes
+    with its log T starting at 1 (termination at -5.5): on an optically thin
+    scene every processed entry with a > 0 counts."""
+    import numpy as np
+
+    from oracle import oracle as O
+    from radiance_meshes_b200 import scenes
+
+    mesh, view = scenes.workload_gradient_check()
+    cv = mesh.cell_values.copy()
+    cv[:, 0] = 1e-3  # thin: no pixel terminates
+    L = O.rasterize_lists(mesh.indices, mesh.vertices, view.tcam())
+    pe = np.ones((view.height, view.width), np.float32)
+    se = np.zeros((view.height, view.width), np.float32)
+    err, cnt, tmax = O.calc_tet_err(L, mesh.indices, mesh.vertices, cv, pe, se)
+    assert cnt.sum() > 0
+    assert np.allclose(err[:, 0], err[:, 12]) and np.allclose(err[:, 0], err[:, 1])  # e = 1
+    assert np.all(err[:, 5] == 0) and np.all(err[:, 2] == err[:, 1])
+    assert np.all(tmax[cnt == 0] == 0)
