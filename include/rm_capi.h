@@ -432,6 +432,37 @@ RM_API int rm_calc_tet_err(const int32_t* sorted_ids, const int32_t* ranges,
                            float* tet_err, int32_t* tet_count, void* workspace,
                            size_t workspace_bytes, int flags, void* stream);
 
+/* ------------------------------------------------- per-tet feature producer -- */
+/*
+ * The cell values the blend consumes, from the model's raw per-tet outputs:
+ * activate_output (utils/model_util.py:93-105) with offset_normalize (:82-91)
+ * and eval_sh (utils/eval_sh_py.py:138-200), fused, one thread per tet.
+ * In: indices [T,4], vertices [V,3], circumcenters [T,3], density [T,1],
+ * rgb [T,3], grd [T,3], sh_rest [T, n_rest, 3] (SH rows 1.. of degree
+ * sh_degree <= 4; n_rest >= (sh_degree + 1)^2 - 1), camera_center (3 floats,
+ * host memory).  Out: features [T,7] = (density, softplus_10(colour at v0
+ * evaluated through the SH), grd * min(rgb) / |v0 - circumcenter|).
+ */
+RM_API int rm_activate_features(const int32_t* indices, const float* vertices,
+                                const float* circumcenters, const float* density,
+                                const float* rgb, const float* grd, const float* sh_rest,
+                                int n_rest, int sh_degree, const float* camera_center,
+                                int64_t n_tets, float* features, void* stream);
+
+/* Adjoint of rm_activate_features: writes grad_density [T], grad_rgb [T,3],
+ * grad_grd [T,3], grad_sh_rest [T,n_rest,3] and grad_circumcenters [T,3];
+ * accumulates grad_vertices [V,3] (the mean and |v0 - circumcenter| carry
+ * gradient; the vertex offsets inside the colour are detached, as in the
+ * reference). */
+RM_API int rm_activate_features_bwd(const int32_t* indices, const float* vertices,
+                                    const float* circumcenters, const float* density,
+                                    const float* rgb, const float* grd, const float* sh_rest,
+                                    int n_rest, int sh_degree, const float* camera_center,
+                                    int64_t n_tets, const float* grad_features,
+                                    float* grad_density, float* grad_rgb, float* grad_grd,
+                                    float* grad_sh_rest, float* grad_vertices,
+                                    float* grad_circumcenters, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,10 @@ SIGNATURES = {
     "rm_views_tile_count": (i64, [camp, ctypes.c_int]),
     "rm_calc_tet_err": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, camp, vp, vp, vp, vp, vp, sz,
                                        ctypes.c_int, vp]),
+    "rm_activate_features": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp, i64, vp,
+                                            vp]),
+    "rm_activate_features_bwd": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp, i64,
+                                                vp, vp, vp, vp, vp, vp, vp, vp]),
     "rm_blend_records_size": (sz, [i64]),
     "rm_blend_pack_records": (ctypes.c_int, [vp, vp, vp, i64, i64, vp, vp, vp]),
     "rm_blend_fwd_multi": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, ctypes.c_int, vp, vp, vp,
