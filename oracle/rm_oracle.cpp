@@ -80,6 +80,9 @@ template <typename F>
 struct Cam {
     F M[16], K[9], pos[3], min_t;
     int H, W, th, tw, gh, gw;
+    int type;     // 0 perspective, 1 fisheye
+    float k[4];   // distortion k1, k2, p1, p2 (applied in float, as the reference's shader does)
+    bool distorted;
 };
 
 template <typename F>
@@ -89,6 +92,10 @@ Cam<F> load_cam(const rm_camera* c) {
     for (int i = 0; i < 9; ++i) r.K[i] = (F)c->K[i];
     for (int i = 0; i < 3; ++i) r.pos[i] = (F)c->cam_pos[i];
     r.min_t = (F)c->min_t;
+    r.type = c->camera_type;
+    for (int i = 0; i < 4; ++i) r.k[i] = c->distortion[i];
+    // dot(distortion_params, distortion_params) >= 1e-9 (camera.slang:244-246)
+    r.distorted = r.k[0] * r.k[0] + r.k[1] * r.k[1] + r.k[2] * r.k[2] + r.k[3] * r.k[3] >= 1e-9f;
     r.H = c->image_height;
     r.W = c->image_width;
     r.th = c->tile_height;
@@ -117,10 +124,35 @@ inline V3<float> point2cam(const Cam<float>& c, V3<float> p) {
     return {safe_divf(h[0], h[3]), safe_divf(h[1], h[3]), safe_divf(h[2], h[3])};
 }
 
-// camspace_to_image for a perspective camera without distortion (camera.slang:382-412).
+// distort (camera.slang:357-378), plain float arithmetic in source order.
+inline void distort(const float k[4], float& x, float& y) {
+    const float r2 = x * x + y * y;
+    const float radial = r2 * (k[0] + r2 * k[1]);
+    const float tx = 2.0f * k[2] * x * y + k[3] * (r2 + 2.0f * x * x);
+    const float ty = 2.0f * k[3] * x * y + k[2] * (r2 + 2.0f * y * y);
+    const float dx = x + x * radial + tx;
+    const float dy = y + y * radial + ty;
+    x = dx;
+    y = dy;
+}
+
+// camspace_to_image (camera.slang:382-412): perspective division or the
+// fisheye angle map, distortion, then K.
 inline V3<float> cam2image(const Cam<float>& c, V3<float> p) {
-    float ux = p.x / p.z;
-    float uy = p.y / p.z;
+    float ux, uy;
+    if (c.type == 1) {
+        const float l = std::sqrt(std::fma(p.z, p.z, std::fma(p.y, p.y, p.x * p.x)));
+        const V3<float> dir = {p.x / l, p.y / l, p.z / l};
+        const float theta = std::acos(std::fmin(std::fmax(dir.z, 0.f), 1.f));
+        const float st = std::sin(theta);
+        const float f = st < 1e-6f ? 1.0f : theta / st;
+        ux = dir.x * f;
+        uy = dir.y * f;
+    } else {
+        ux = p.x / p.z;
+        uy = p.y / p.z;
+    }
+    if (c.distorted) distort(c.k, ux, uy);
     return {std::fma(ux, c.K[0], c.K[2]), std::fma(uy, c.K[4], c.K[5]), p.z};
 }
 
@@ -155,10 +187,12 @@ void find_extent(const Cam<float>& c, const V3<float> v[4], V3<float>& mn, V3<fl
             }
         }
         if (n > 1) {
+            // update_bounds_from_edge (camera.slang:416-439): n_samples per edge
+            const int ns = c.type == 1 ? 4 : (c.distorted ? 3 : 2);
             for (int j = 0; j < n; ++j) {
                 V3<float> s = out[j], e = out[(j + 1) % n];
-                for (int i = 0; i < 2; ++i) {
-                    float t = (float)i / 1.0f;
+                for (int i = 0; i < ns; ++i) {
+                    float t = (float)i / (float)(ns - 1);
                     V3<float> p = cam2image(c, lerp3(s, e, t));
                     mn = {std::fmin(mn.x, p.x), std::fmin(mn.y, p.y), std::fmin(mn.z, p.z)};
                     mx = {std::fmax(mx.x, p.x), std::fmax(mx.y, p.y), std::fmax(mx.z, p.z)};
@@ -249,16 +283,57 @@ void make_rec(const V3<F> v[4], const F* cv, Rec<F>& r) {
 }
 
 // get_ray (camera.slang:298-346), perspective without distortion.
+// undistort (camera.slang:241-296): 10 Newton steps, plain float arithmetic
+// in source order; the shader works in float whatever F is.
+inline void undistort(const float k[4], float& ux, float& uy) {
+    const float k1 = k[0], k2 = k[1], p1 = k[2], p2 = k[3];
+    const float pdx = ux, pdy = uy;
+    float x = ux, y = uy;
+    for (int i = 0; i < 10; ++i) {
+        const float r2 = x * x + y * y;
+        const float d = 1.0f + r2 * (k1 + r2 * k2);
+        const float fx = d * x + 2.0f * p1 * x * y + p2 * (r2 + 2.0f * x * x) - pdx;
+        const float fy = d * y + 2.0f * p2 * x * y + p1 * (r2 + 2.0f * y * y) - pdy;
+        const float d_r = k1 + r2 * (2.0f * k2);
+        const float d_x = 2.0f * x * d_r;
+        const float d_y = 2.0f * y * d_r;
+        const float fx_x = d + d_x * x + 2.0f * p1 * y + 6.0f * p2 * x;
+        const float fx_y = d_y * x + 2.0f * p1 * x + 2.0f * p2 * y;
+        const float fy_x = d_x * y + 2.0f * p2 * y + 2.0f * p1 * x;
+        const float fy_y = d + d_y * y + 2.0f * p2 * x + 6.0f * p1 * y;
+        const float den = fy_x * fx_y - fx_x * fy_y;
+        if (std::fabs(den) < 1e-9f) break;
+        x = x + (fx * fy_y - fy * fx_y) / den;
+        y = y + (fy * fx_x - fx * fy_x) / den;
+    }
+    ux = x;
+    uy = y;
+}
+
 template <typename F>
 void make_ray(const Cam<F>& c, int px, int py, F jx, F jy, V3<F>& o, V3<F>& d) {
     F ux = ((F)px + jx - c.K[2]) / c.K[0];
     F uy = ((F)py + jy - c.K[5]) / c.K[4];
-    V3<F> dc = {ux, uy, F(1)};
-    F l = std::sqrt(dot(dc, dc));
-    dc = {dc.x / l, dc.y / l, dc.z / l};
+    V3<F> dc;
+    if ((c.type == 0 || c.type == 1) && c.distorted) {
+        float x = (float)ux, y = (float)uy;
+        undistort(c.k, x, y);
+        ux = (F)x;
+        uy = (F)y;
+    }
+    if (c.type == 1) {  // fisheye: angle |p| from the axis, clamped to pi
+        F theta = std::sqrt(ux * ux + uy * uy);
+        theta = std::fmin(F(3.14159265f), theta);
+        const F s = theta < F(1e-6f) ? F(1) : std::sin(theta) / theta;
+        dc = {ux * s, uy * s, std::cos(theta)};
+    } else {
+        dc = {ux, uy, F(1)};
+        F l = std::sqrt(dot(dc, dc));
+        dc = {dc.x / l, dc.y / l, dc.z / l};
+    }
     V3<F> dw = {dot(V3<F>{c.M[0], c.M[4], c.M[8]}, dc), dot(V3<F>{c.M[1], c.M[5], c.M[9]}, dc),
                 dot(V3<F>{c.M[2], c.M[6], c.M[10]}, dc)};
-    l = std::sqrt(dot(dw, dw));
+    F l = std::sqrt(dot(dw, dw));
     d = {dw.x / l, dw.y / l, dw.z / l};
     o = {std::fma(d.x, c.min_t, c.pos[0]), std::fma(d.y, c.min_t, c.pos[1]),
          std::fma(d.z, c.min_t, c.pos[2])};

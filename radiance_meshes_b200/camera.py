@@ -54,9 +54,10 @@ def _as_np(x, n):
 def tcam_to_struct(tcam: dict) -> RMCamera:
     """Convert a reference ``tcam`` dict into an ``rm_camera``.
 
-    Only perspective cameras without lens distortion are supported (the
-    reference's ``camera_type == 0`` with zero ``distortion_params``);
-    anything else raises ``ValueError``.
+    Perspective (``camera_type == 0``) and fisheye (``camera_type == 1``)
+    cameras with the reference's radial/tangential ``distortion_params``
+    (k1, k2, p1, p2) are supported; any other camera type raises
+    ``ValueError``.
     """
     cam = RMCamera()
     cam.world_view[:] = _as_np(tcam["world_view_transform"], 16).tolist()
@@ -67,10 +68,10 @@ def tcam_to_struct(tcam: dict) -> RMCamera:
     dist = np.zeros(4, np.float32) if dist is None else _as_np(dist, 4)
     cam.distortion[:] = dist.tolist()
     ctype = int(tcam.get("camera_type", 0))
-    if ctype != 0:
-        raise ValueError(f"camera_type {ctype} is not supported (perspective only)")
-    if float(np.dot(dist, dist)) >= 1e-9:
-        raise ValueError("lens distortion is not supported")
+    if ctype not in (0, 1):
+        raise ValueError(f"camera_type {ctype} is not supported (0 perspective, 1 fisheye)")
+    if not np.all(np.isfinite(dist)):
+        raise ValueError("distortion_params must be finite")
     cam.camera_type = ctype
     cam.image_height = int(tcam["image_height"])
     cam.image_width = int(tcam["image_width"])

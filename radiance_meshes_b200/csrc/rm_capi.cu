@@ -30,10 +30,10 @@ int check_launch(const char* what, int kernels) {
 
 int check_cam(const rm_camera* cam) {
     if (!cam) return fail(RM_EINVAL, "camera is NULL");
-    if (cam->camera_type != 0) return fail(RM_EINVAL, "camera_type %d unsupported (perspective only)", cam->camera_type);
-    float dd = 0.f;
-    for (int i = 0; i < 4; ++i) dd += cam->distortion[i] * cam->distortion[i];
-    if (dd >= 1e-9f) return fail(RM_EINVAL, "lens distortion is not supported");
+    if (cam->camera_type != 0 && cam->camera_type != 1)
+        return fail(RM_EINVAL, "camera_type %d unsupported (0 perspective, 1 fisheye)", cam->camera_type);
+    for (int i = 0; i < 4; ++i)
+        if (!(cam->distortion[i] == cam->distortion[i])) return fail(RM_EINVAL, "distortion parameter is NaN");
     if (cam->tile_width <= 0 || cam->tile_height <= 0) return fail(RM_EINVAL, "bad tile size");
     if (cam->image_width <= 0 || cam->image_height <= 0) return fail(RM_EINVAL, "bad image size");
     if ((int64_t)cam->grid_width * cam->tile_width < cam->image_width ||

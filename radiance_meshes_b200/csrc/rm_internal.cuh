@@ -53,18 +53,68 @@ constexpr float kLogMax = (float)46.051701859880914;
 
 __device__ __forceinline__ float safe_expf(float v) { return expf(fmaxf(fminf(v, kLogMax), -1e20f)); }
 
-// get_ray (camera.slang:298-346) for a perspective camera without distortion.
+// Lens distortion is on when dot(distortion, distortion) >= 1e-9
+// (camera.slang:244-246, 359-361).
+__device__ __forceinline__ bool cam_distorted(const rm_camera& c) {
+    const float* k = c.distortion;
+    return k[0] * k[0] + k[1] * k[1] + k[2] * k[2] + k[3] * k[3] >= 1e-9f;
+}
+
+// undistort (camera.slang:241-296): 10 Newton steps on the radial (k1, k2)
+// and tangential (p1, p2) model, stopping early on a singular Jacobian.  The
+// distortion arithmetic is written with plain operations in the reference's
+// textual order (no fused multiply-add).
+__device__ __forceinline__ void undistort(const rm_camera& c, float& ux, float& uy) {
+    const float k1 = c.distortion[0], k2 = c.distortion[1], p1 = c.distortion[2], p2 = c.distortion[3];
+    const float pdx = ux, pdy = uy;
+    float x = ux, y = uy;
+    for (int i = 0; i < 10; ++i) {
+        const float r2 = x * x + y * y;
+        const float d = 1.0f + r2 * (k1 + r2 * k2);
+        const float fx = d * x + 2.0f * p1 * x * y + p2 * (r2 + 2.0f * x * x) - pdx;
+        const float fy = d * y + 2.0f * p2 * x * y + p1 * (r2 + 2.0f * y * y) - pdy;
+        const float d_r = k1 + r2 * (2.0f * k2);
+        const float d_x = 2.0f * x * d_r;
+        const float d_y = 2.0f * y * d_r;
+        const float fx_x = d + d_x * x + 2.0f * p1 * y + 6.0f * p2 * x;
+        const float fx_y = d_y * x + 2.0f * p1 * x + 2.0f * p2 * y;
+        const float fy_x = d_x * y + 2.0f * p2 * y + 2.0f * p1 * x;
+        const float fy_y = d + d_y * y + 2.0f * p2 * x + 6.0f * p1 * y;
+        const float den = fy_x * fx_y - fx_x * fy_y;
+        if (fabsf(den) < 1e-9f) break;
+        x = x + (fx * fy_y - fy * fx_y) / den;
+        y = y + (fy * fx_x - fx * fy_x) / den;
+    }
+    ux = x;
+    uy = y;
+}
+
+// get_ray (camera.slang:298-346): pixel -> normalised image point,
+// undistorted for perspective (0) and fisheye (1) cameras, then the camera
+// ray (fisheye: angle theta = |p| from the axis, clamped to pi), rotated to
+// the world and started min_t along the ray.  The pinhole path without
+// distortion is exactly the declared-rounding path of the tests.
 __device__ __forceinline__ void make_ray(const rm_camera& c, int px, int py, float jx, float jy, f3& o,
                                          f3& d) {
-    const float ux = ((float)px + jx - c.K[2]) / c.K[0];
-    const float uy = ((float)py + jy - c.K[5]) / c.K[4];
-    f3 dc = {ux, uy, 1.0f};
-    float l = sqrtf(dot3(dc, dc));
-    dc = {dc.x / l, dc.y / l, dc.z / l};
+    float ux = ((float)px + jx - c.K[2]) / c.K[0];
+    float uy = ((float)py + jy - c.K[5]) / c.K[4];
+    const bool fisheye = c.camera_type == 1;
+    if ((c.camera_type == 0 || fisheye) && cam_distorted(c)) undistort(c, ux, uy);
+    f3 dc;
+    if (fisheye) {
+        float theta = sqrtf(ux * ux + uy * uy);
+        theta = fminf(3.14159265f, theta);
+        const float s = theta < 1e-6f ? 1.0f : sinf(theta) / theta;
+        dc = {ux * s, uy * s, cosf(theta)};
+    } else {
+        dc = {ux, uy, 1.0f};
+        const float l = sqrtf(dot3(dc, dc));
+        dc = {dc.x / l, dc.y / l, dc.z / l};
+    }
     const float* M = c.world_view;
     f3 dw = {dot3(mk3(M[0], M[4], M[8]), dc), dot3(mk3(M[1], M[5], M[9]), dc),
              dot3(mk3(M[2], M[6], M[10]), dc)};
-    l = sqrtf(dot3(dw, dw));
+    const float l = sqrtf(dot3(dw, dw));
     d = {dw.x / l, dw.y / l, dw.z / l};
     o = {fmaf(d.x, c.min_t, c.cam_pos[0]), fmaf(d.y, c.min_t, c.cam_pos[1]),
          fmaf(d.z, c.min_t, c.cam_pos[2])};

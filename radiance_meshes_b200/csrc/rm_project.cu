@@ -38,9 +38,32 @@ struct BBox {
 };
 
 __device__ __forceinline__ void bbox_add(BBox& b, const rm_camera& c, f3 p) {
-    // camspace_to_image (camera.slang:382-412), perspective, no distortion
-    const float ux = p.x / p.z;
-    const float uy = p.y / p.z;
+    // camspace_to_image (camera.slang:382-412): perspective division or the
+    // fisheye angle map, then distort (camera.slang:357-378), then K
+    float ux, uy;
+    if (c.camera_type == 1) {
+        const float l = sqrtf(dot3(p, p));
+        const f3 dir = {p.x / l, p.y / l, p.z / l};
+        const float theta = acosf(fminf(fmaxf(dir.z, 0.f), 1.f));
+        const float st = sinf(theta);
+        const float f = st < 1e-6f ? 1.0f : theta / st;
+        ux = dir.x * f;
+        uy = dir.y * f;
+    } else {
+        ux = p.x / p.z;
+        uy = p.y / p.z;
+    }
+    if (cam_distorted(c)) {
+        const float k1 = c.distortion[0], k2 = c.distortion[1], p1 = c.distortion[2], p2 = c.distortion[3];
+        const float r2 = ux * ux + uy * uy;
+        const float radial = r2 * (k1 + r2 * k2);
+        const float tx = 2.0f * p1 * ux * uy + p2 * (r2 + 2.0f * ux * ux);
+        const float ty = 2.0f * p2 * ux * uy + p1 * (r2 + 2.0f * uy * uy);
+        const float dx = ux + ux * radial + tx;
+        const float dy = uy + uy * radial + ty;
+        ux = dx;
+        uy = dy;
+    }
     const float qx = fmaf(ux, c.K[0], c.K[2]);
     const float qy = fmaf(uy, c.K[4], c.K[5]);
     b.mn = {fminf(b.mn.x, qx), fminf(b.mn.y, qy), fminf(b.mn.z, p.z)};
@@ -90,6 +113,22 @@ __device__ __forceinline__ void clip_face(const rm_camera& c, f3 a, f3 b, f3 cc,
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (k < n) bbox_add(box, c, p[k]);
+        // update_bounds_from_edge (camera.slang:416-439): 2 samples per edge
+        // (its endpoints) for a plain perspective camera, 3 with distortion,
+        // 4 for a fisheye; samples at t = i / (n_samples - 1) from each edge's
+        // start, so the interior ones are added here
+        const int ns = c.camera_type == 1 ? 4 : (cam_distorted(c) ? 3 : 2);
+        if (ns > 2) {
+            for (int k = 0; k < n; ++k) {
+                f3 a = p[0], b = p[0];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (q == k) a = p[q];
+                    if (q == (k + 1) % n) b = p[q];
+                }
+                for (int i = 1; i < ns - 1; ++i) bbox_add(box, c, lerp3(a, b, (float)i / (float)(ns - 1)));
+            }
+        }
     }
 }
 
@@ -180,6 +219,7 @@ __device__ __forceinline__ TetGeom tet_geom(const int4* __restrict__ indices, co
 // It needs an affine world-to-camera matrix (last row 0 0 0 1).
 __device__ __forceinline__ bool outside_view(const rm_camera& c, const TetGeom& t) {
     const float* M = c.world_view;
+    if (c.camera_type != 0 || cam_distorted(c)) return false;  // the test assumes the pinhole projection
     if (!(M[12] == 0.f && M[13] == 0.f && M[14] == 0.f && M[15] == 1.f)) return false;
     const float fx = c.K[0], cx = c.K[2], fy = c.K[4], cy = c.K[5];
     const float gw = (float)c.grid_width * (float)c.tile_width, gh = (float)c.grid_height * (float)c.tile_height;

@@ -49,16 +49,25 @@ def _cam():
     return tcam_to_struct(view.tcam())
 
 
-def test_rejects_distortion_and_camera_type():
+def test_camera_types_and_distortion():
+    """Perspective and fisheye cameras with distortion pass the camera check
+    (the call then stops at its NULL buffers); other camera types and NaN
+    distortion are rejected."""
     L = C.lib()
+    for ctype in (0, 1):
+        cam = _cam()
+        cam.camera_type = ctype
+        cam.distortion[0] = 0.1
+        rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None)
+        assert rc == C.RM_EINVAL and "NULL" in C.last_error()
     cam = _cam()
-    cam.distortion[0] = 0.1
-    rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None)
-    assert rc == C.RM_EINVAL and "distortion" in C.last_error()
-    cam = _cam()
-    cam.camera_type = 1
+    cam.camera_type = 2
     rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None)
     assert rc == C.RM_EINVAL and "camera_type" in C.last_error()
+    cam = _cam()
+    cam.distortion[1] = float("nan")
+    rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None)
+    assert rc == C.RM_EINVAL and "NaN" in C.last_error()
 
 
 def test_rejects_null_and_misaligned():
@@ -90,6 +99,13 @@ def test_python_camera_validation():
     mesh, view = scenes.workload_gradient_check()
     t = view.tcam()
     t["distortion_params"] = [0.1, 0, 0, 0]
+    t["camera_type"] = 1
+    assert tcam_to_struct(t).camera_type == 1
+    t["camera_type"] = 3
+    with pytest.raises(ValueError):
+        tcam_to_struct(t)
+    t = view.tcam()
+    t["distortion_params"] = [float("inf"), 0, 0, 0]
     with pytest.raises(ValueError):
         tcam_to_struct(t)
     t = view.tcam()

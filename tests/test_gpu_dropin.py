@@ -86,7 +86,7 @@ def test_bad_camera_raises(cuda):
 
     mesh, view = scenes.workload_gradient_check()
     tcam = view.tcam(device="cuda")
-    tcam["camera_type"] = 1
+    tcam["camera_type"] = 2  # neither perspective nor fisheye
     with pytest.raises(ValueError):
         vertex_and_tile_shader(to_dev(mesh.indices), to_dev(mesh.vertices), tcam,
                                RenderGrid(view.height, view.width, 16, 16))
