@@ -849,6 +849,9 @@ struct BwdDenseSmem {
     int32_t sid[B];
     float sacc[B][kNGrad];
     int32_t smax[WarpShape<NT>::kWarps];
+    uint32_t sor[WarpShape<NT>::kWarps][2];  // per warp: OR of its pixels' hit bits (two 32-entry blocks)
+    uint8_t cidx[B];                          // batch positions of the entries some pixel hit
+    int32_t n_keep;
 };
 
 template <int NT, int B>
@@ -899,8 +902,6 @@ __device__ __forceinline__ void bwd_dense_item(
         lo = rg.x + ((top - 1 - rg.x) / B) * B;
         const int n = top - lo;
         __syncthreads();
-        for (int k = threadIdx.x; k < n; k += NT) S.sid[k] = __ldg(ids + lo + k);
-        for (int k = threadIdx.x; k < n * kNGrad; k += NT) (&S.sacc[0][0])[k] = 0.f;
         // this pixel's hit bits of the (at most two) 32-entry blocks the batch spans
         const int kb0 = (lo - rg.x) >> 5, kb1 = (top - 1 - rg.x) >> 5;
         uint32_t hw0 = 0xffffffffu, hw1 = 0xffffffffu;
@@ -910,14 +911,53 @@ __device__ __forceinline__ void bwd_dense_item(
             if (i0 < hm.cap) hw0 = __ldcg(hm.words + i0);
             if (i1 < hm.cap) hw1 = __ldcg(hm.words + i1);
         }
+        // entries no pixel of the item hit are dropped from the batch before
+        // staging (the masks of pixels past their n_contributors are zero)
+        uint32_t o0 = hw0, o1 = hw1;
+#pragma unroll
+        for (int off = WarpShape<NT>::kTopOffset; off > 0; off >>= 1) {
+            o0 |= __shfl_xor_sync(kMask, o0, off);
+            o1 |= __shfl_xor_sync(kMask, o1, off);
+        }
+        if (lane == 0) {
+            S.sor[warp][0] = o0;
+            S.sor[warp][1] = o1;
+        }
         __syncthreads();
-        for (int k = threadIdx.x; k < n * kRecFloat4; k += NT) {
+        if (warp == 0) {
+            uint32_t c0 = 0, c1 = 0;
+#pragma unroll
+            for (int w = 0; w < WarpShape<NT>::kWarps; ++w) {
+                c0 |= S.sor[w][0];
+                c1 |= S.sor[w][1];
+            }
+            int base_c = 0;
+            constexpr int kLanes = NT >= 32 ? 32 : NT;
+            for (int k0 = 0; k0 < n; k0 += kLanes) {
+                const int k = k0 + lane;
+                bool keep = false;
+                if (k < n) {
+                    const int off = lo + k - rg.x;
+                    keep = ((((off >> 5) == kb0 ? c0 : c1) >> (off & 31)) & 1u) != 0u;
+                }
+                const unsigned bal = __ballot_sync(kMask, keep);
+                if (keep) S.cidx[base_c + __popc(bal & ((1u << lane) - 1u))] = (uint8_t)k;
+                base_c += __popc(bal);
+            }
+            if (lane == 0) S.n_keep = base_c;
+        }
+        __syncthreads();
+        const int nk = S.n_keep;
+        for (int k = threadIdx.x; k < nk; k += NT) S.sid[k] = __ldg(ids + lo + S.cidx[k]);
+        for (int k = threadIdx.x; k < nk * kNGrad; k += NT) (&S.sacc[0][0])[k] = 0.f;
+        __syncthreads();
+        for (int k = threadIdx.x; k < nk * kRecFloat4; k += NT) {
             const int j = k >> 3, c = k & 7;
             S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
         }
         __syncthreads();
-        for (int jj = n - 1; jj >= 0; --jj) {
-            const int off = lo + jj - rg.x;
+        for (int jj = nk - 1; jj >= 0; --jj) {
+            const int off = lo + S.cidx[jj] - rg.x;
             // with the forward's masks, only its hits are revisited
             const uint32_t hw = (off >> 5) == kb0 ? hw0 : hw1;
             const bool act = inside && off < nc && ((hw >> (off & 31)) & 1u);
@@ -957,7 +997,7 @@ __device__ __forceinline__ void bwd_dense_item(
             }
         }
         __syncthreads();
-        flush_entries<NT, B>(n, S.srec, S.sid, S.sacc, indices, gverts, gcv);
+        flush_entries<NT, B>(nk, S.srec, S.sid, S.sacc, indices, gverts, gcv);
     }
 }
 

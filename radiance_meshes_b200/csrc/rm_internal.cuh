@@ -89,28 +89,9 @@ __device__ __forceinline__ void undistort(const rm_camera& c, float& ux, float& 
     uy = y;
 }
 
-// get_ray (camera.slang:298-346): pixel -> normalised image point,
-// undistorted for perspective (0) and fisheye (1) cameras, then the camera
-// ray (fisheye: angle theta = |p| from the axis, clamped to pi), rotated to
-// the world and started min_t along the ray.  The pinhole path without
-// distortion is exactly the declared-rounding path of the tests.
-__device__ __forceinline__ void make_ray(const rm_camera& c, int px, int py, float jx, float jy, f3& o,
-                                         f3& d) {
-    float ux = ((float)px + jx - c.K[2]) / c.K[0];
-    float uy = ((float)py + jy - c.K[5]) / c.K[4];
-    const bool fisheye = c.camera_type == 1;
-    if ((c.camera_type == 0 || fisheye) && cam_distorted(c)) undistort(c, ux, uy);
-    f3 dc;
-    if (fisheye) {
-        float theta = sqrtf(ux * ux + uy * uy);
-        theta = fminf(3.14159265f, theta);
-        const float s = theta < 1e-6f ? 1.0f : sinf(theta) / theta;
-        dc = {ux * s, uy * s, cosf(theta)};
-    } else {
-        dc = {ux, uy, 1.0f};
-        const float l = sqrtf(dot3(dc, dc));
-        dc = {dc.x / l, dc.y / l, dc.z / l};
-    }
+// Ray direction in world space from a camera-space direction, normalised,
+// and the origin min_t along it (get_ray, camera.slang:331-346).
+__device__ __forceinline__ void ray_to_world(const rm_camera& c, f3 dc, f3& o, f3& d) {
     const float* M = c.world_view;
     f3 dw = {dot3(mk3(M[0], M[4], M[8]), dc), dot3(mk3(M[1], M[5], M[9]), dc),
              dot3(mk3(M[2], M[6], M[10]), dc)};
@@ -118,6 +99,43 @@ __device__ __forceinline__ void make_ray(const rm_camera& c, int px, int py, flo
     d = {dw.x / l, dw.y / l, dw.z / l};
     o = {fmaf(d.x, c.min_t, c.cam_pos[0]), fmaf(d.y, c.min_t, c.cam_pos[1]),
          fmaf(d.z, c.min_t, c.cam_pos[2])};
+}
+
+// Camera-space direction of a normalised image point for a fisheye or a
+// distorted camera: undistorted, then (fisheye) the angle theta = |p| from
+// the axis, clamped to pi.  Kept out of line: it runs once per pixel and its
+// registers would otherwise count against the blend loops.
+static __device__ __noinline__ f3 general_dir(const rm_camera& c, float ux, float uy) {
+    const bool fisheye = c.camera_type == 1;
+    if (cam_distorted(c)) undistort(c, ux, uy);
+    if (fisheye) {
+        float theta = sqrtf(ux * ux + uy * uy);
+        theta = fminf(3.14159265f, theta);
+        const float s = theta < 1e-6f ? 1.0f : sinf(theta) / theta;
+        return {ux * s, uy * s, cosf(theta)};
+    }
+    f3 dc = {ux, uy, 1.0f};
+    const float l = sqrtf(dot3(dc, dc));
+    return {dc.x / l, dc.y / l, dc.z / l};
+}
+
+// get_ray (camera.slang:298-346): pixel -> normalised image point,
+// undistorted for perspective (0) and fisheye (1) cameras, then the camera
+// ray, rotated to the world and started min_t along the ray.  The pinhole
+// path without distortion is exactly the declared-rounding path of the tests.
+__device__ __forceinline__ void make_ray(const rm_camera& c, int px, int py, float jx, float jy, f3& o,
+                                         f3& d) {
+    const float ux = ((float)px + jx - c.K[2]) / c.K[0];
+    const float uy = ((float)py + jy - c.K[5]) / c.K[4];
+    f3 dc;
+    if (c.camera_type == 0 && !cam_distorted(c)) {
+        dc = {ux, uy, 1.0f};
+        const float l = sqrtf(dot3(dc, dc));
+        dc = {dc.x / l, dc.y / l, dc.z / l};
+    } else {
+        dc = general_dir(c, ux, uy);
+    }
+    ray_to_world(c, dc, o, d);
 }
 
 // Packed per-tet record (128 B = 8 x float4) staged by the blend kernels.
@@ -184,4 +202,12 @@ int check_cam(const rm_camera* cam);
 // Validates n cameras (n in [1, RM_MAX_VIEWS], one tile size for all) and
 // fills the view table.
 int make_views(const char* who, const rm_camera* cams, int n, rm::ViewSet* out);
+// True unless the camera is a plain perspective one with all distortion
+// coefficients zero; kernels instantiated for the plain camera leave out the
+// fisheye and distortion code (a conservative test: a camera with tiny
+// nonzero coefficients takes the general code, which tests them itself).
+inline bool cam_general(const rm_camera& c) {
+    return c.camera_type != 0 || c.distortion[0] != 0.f || c.distortion[1] != 0.f || c.distortion[2] != 0.f ||
+           c.distortion[3] != 0.f;
+}
 }  // namespace rm_host

@@ -37,11 +37,14 @@ struct BBox {
     f3 mn, mx;
 };
 
+// GENERAL = false: a perspective camera without distortion (the host picks
+// the instantiation with rm_host::cam_general).
+template <bool GENERAL>
 __device__ __forceinline__ void bbox_add(BBox& b, const rm_camera& c, f3 p) {
     // camspace_to_image (camera.slang:382-412): perspective division or the
     // fisheye angle map, then distort (camera.slang:357-378), then K
     float ux, uy;
-    if (c.camera_type == 1) {
+    if (GENERAL && c.camera_type == 1) {
         const float l = sqrtf(dot3(p, p));
         const f3 dir = {p.x / l, p.y / l, p.z / l};
         const float theta = acosf(fminf(fmaxf(dir.z, 0.f), 1.f));
@@ -53,7 +56,7 @@ __device__ __forceinline__ void bbox_add(BBox& b, const rm_camera& c, f3 p) {
         ux = p.x / p.z;
         uy = p.y / p.z;
     }
-    if (cam_distorted(c)) {
+    if (GENERAL && cam_distorted(c)) {
         const float k1 = c.distortion[0], k2 = c.distortion[1], p1 = c.distortion[2], p2 = c.distortion[3];
         const float r2 = ux * ux + uy * uy;
         const float radial = r2 * (k1 + r2 * k2);
@@ -77,6 +80,7 @@ __device__ __forceinline__ bool eq3(f3 a, f3 b) { return a.x == b.x && a.y == b.
 // Sampling each edge at t = 0 and t = 1 (2 samples) yields exactly the polygon
 // vertices (lerp with s = 0 / 1 is exact), so the box is the box of the
 // polygon vertices; the de-duplication only matters for the vertex count.
+template <bool GENERAL>
 __device__ __forceinline__ void clip_face(const rm_camera& c, f3 a, f3 b, f3 cc, BBox& box) {
     const float eps = 1e-4f;
     f3 p[4];
@@ -112,13 +116,13 @@ __device__ __forceinline__ void clip_face(const rm_camera& c, f3 a, f3 b, f3 cc,
     if (n > 1) {
 #pragma unroll
         for (int k = 0; k < 4; ++k)
-            if (k < n) bbox_add(box, c, p[k]);
+            if (k < n) bbox_add<GENERAL>(box, c, p[k]);
         // update_bounds_from_edge (camera.slang:416-439): 2 samples per edge
         // (its endpoints) for a plain perspective camera, 3 with distortion,
         // 4 for a fisheye; samples at t = i / (n_samples - 1) from each edge's
         // start, so the interior ones are added here
-        const int ns = c.camera_type == 1 ? 4 : (cam_distorted(c) ? 3 : 2);
-        if (ns > 2) {
+        const int ns = !GENERAL ? 2 : (c.camera_type == 1 ? 4 : (cam_distorted(c) ? 3 : 2));
+        if (GENERAL && ns > 2) {
             for (int k = 0; k < n; ++k) {
                 f3 a = p[0], b = p[0];
 #pragma unroll
@@ -126,7 +130,8 @@ __device__ __forceinline__ void clip_face(const rm_camera& c, f3 a, f3 b, f3 cc,
                     if (q == k) a = p[q];
                     if (q == (k + 1) % n) b = p[q];
                 }
-                for (int i = 1; i < ns - 1; ++i) bbox_add(box, c, lerp3(a, b, (float)i / (float)(ns - 1)));
+                for (int i = 1; i < ns - 1; ++i)
+                    bbox_add<GENERAL>(box, c, lerp3(a, b, (float)i / (float)(ns - 1)));
             }
         }
     }
@@ -246,7 +251,7 @@ __device__ __forceinline__ bool outside_view(const rm_camera& c, const TetGeom& 
 // Per-view part of vertex_shader (vertex_shader.slang:36-89): camera space,
 // find_extent, the depth key and the tile rectangle.  Returns the tile count
 // (0: culled, r and depth zero).
-template <bool FINE = false>
+template <bool GENERAL, bool FINE = false>
 __device__ __forceinline__ int project_view(const rm_camera& cam, const TetGeom& t, int4& r, float& depth_out,
                                             int fine_shift = 0, int4* rf = nullptr, int* n_fine = nullptr) {
     r = {0, 0, 0, 0};
@@ -259,10 +264,10 @@ __device__ __forceinline__ int project_view(const rm_camera& cam, const TetGeom&
     const f3 cs0 = point2cam(cam, t.v[0]), cs1 = point2cam(cam, t.v[1]);
     const f3 cs2 = point2cam(cam, t.v[2]), cs3 = point2cam(cam, t.v[3]);
     BBox box = {{1e20f, 1e20f, 1e20f}, {-1e20f, -1e20f, -1e20f}};
-    clip_face(cam, cs0, cs1, cs2, box);
-    clip_face(cam, cs0, cs2, cs3, box);
-    clip_face(cam, cs0, cs3, cs1, box);
-    clip_face(cam, cs1, cs3, cs2, box);
+    clip_face<GENERAL>(cam, cs0, cs1, cs2, box);
+    clip_face<GENERAL>(cam, cs0, cs2, cs3, box);
+    clip_face<GENERAL>(cam, cs0, cs3, cs1, box);
+    clip_face<GENERAL>(cam, cs1, cs3, cs2, box);
     if (box.mx.z <= 0.0f) return 0;
     // depth key: FP64 power of the circumsphere w.r.t. the camera position
     const d3 P = {(double)cam.cam_pos[0], (double)cam.cam_pos[1], (double)cam.cam_pos[2]};
@@ -302,6 +307,7 @@ __device__ __forceinline__ int project_view(const rm_camera& cam, const TetGeom&
     return n_tiles;
 }
 
+template <bool GENERAL>
 __global__ void __launch_bounds__(256) project_fwd_kernel(const int4* __restrict__ indices,
                                                           const float* __restrict__ verts, int64_t n_tets,
                                                           const rm_camera cam, int32_t* __restrict__ tiles,
@@ -312,7 +318,7 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(const int4* __restrict
     const TetGeom t = tet_geom(indices, verts, g);
     int4 r;
     float depth;
-    const int n_tiles = project_view(cam, t, r, depth);
+    const int n_tiles = project_view<GENERAL>(cam, t, r, depth);
     tiles[g] = n_tiles;
     rect[g] = r;
     vs[3 * g + 0] = 0.f;
@@ -324,6 +330,7 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(const int4* __restrict
 }
 
 // Projection plus the rectangles on a grid of 2^fine_shift times smaller tiles.
+template <bool GENERAL>
 __global__ void __launch_bounds__(256) project_fwd_fine_kernel(const int4* __restrict__ indices,
                                                                const float* __restrict__ verts, int64_t n_tets,
                                                                const rm_camera cam, int fine_shift,
@@ -337,7 +344,7 @@ __global__ void __launch_bounds__(256) project_fwd_fine_kernel(const int4* __res
     int4 r, rf;
     float depth;
     int nf;
-    const int n_tiles = project_view<true>(cam, t, r, depth, fine_shift, &rf, &nf);
+    const int n_tiles = project_view<GENERAL, true>(cam, t, r, depth, fine_shift, &rf, &nf);
     tiles[g] = n_tiles;
     rect[g] = r;
     vs[3 * g + 0] = 0.f;
@@ -352,6 +359,7 @@ __global__ void __launch_bounds__(256) project_fwd_fine_kernel(const int4* __res
 
 // All views of a batch: each thread loads its tet once and projects it into
 // every view; outputs are stacked view-major.
+template <bool GENERAL>
 __global__ void __launch_bounds__(256) project_fwd_multi_kernel(const int4* __restrict__ indices,
                                                                 const float* __restrict__ verts, int64_t n_tets,
                                                                 const __grid_constant__ ViewSet views,
@@ -370,10 +378,10 @@ __global__ void __launch_bounds__(256) project_fwd_multi_kernel(const int4* __re
         const int64_t o = (int64_t)v * n_tets + g;
         int n_tiles;
         if (rect_fine) {
-            n_tiles = project_view<true>(views.cams[v], t, r, dk, fine_shift, &rf, &nf);
+            n_tiles = project_view<GENERAL, true>(views.cams[v], t, r, dk, fine_shift, &rf, &nf);
             rect_fine[o] = rf;
         } else {
-            n_tiles = project_view(views.cams[v], t, r, dk);
+            n_tiles = project_view<GENERAL>(views.cams[v], t, r, dk);
         }
         tiles[o] = n_tiles;
         rect[o] = r;
@@ -491,7 +499,8 @@ int rm_project_fwd(const int32_t* indices, const float* vertices, int64_t n_tets
         return rm_host::fail(RM_EINVAL, "rm_project_fwd: indices and rect must be 16-byte aligned");
     const int threads = 256;
     const int64_t blocks = (n_tets + threads - 1) / threads;
-    rm::project_fwd_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+    auto kernel = rm_host::cam_general(*cam) ? rm::project_fwd_kernel<true> : rm::project_fwd_kernel<false>;
+    kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
         (const int4*)indices, vertices, n_tets, *cam, tiles_touched, (int4*)rect, vs, circumcenter);
     return rm_host::check_launch("rm_project_fwd");
 }
@@ -513,7 +522,9 @@ int rm_project_fwd_fine(const int32_t* indices, const float* vertices, int64_t n
         return rm_host::fail(RM_EINVAL, "rm_project_fwd_fine: indices and rects must be 16-byte aligned");
     const int threads = 256;
     const int64_t blocks = (n_tets + threads - 1) / threads;
-    rm::project_fwd_fine_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+    auto kernel =
+        rm_host::cam_general(*cam) ? rm::project_fwd_fine_kernel<true> : rm::project_fwd_fine_kernel<false>;
+    kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
         (const int4*)indices, vertices, n_tets, *cam, fine_shift, tiles_touched, (int4*)rect, vs, circumcenter,
         tiles_fine, (int4*)rect_fine);
     return rm_host::check_launch("rm_project_fwd_fine");
@@ -536,7 +547,10 @@ int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t 
         return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: tile not divisible by 2^%d", fine_shift);
     const int threads = 256;
     const int64_t blocks = (n_tets + threads - 1) / threads;
-    rm::project_fwd_multi_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+    bool general = false;
+    for (int v = 0; v < n_views; ++v) general |= rm_host::cam_general(cams[v]);
+    auto kernel = general ? rm::project_fwd_multi_kernel<true> : rm::project_fwd_multi_kernel<false>;
+    kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
         (const int4*)indices, vertices, n_tets, views, tiles_touched, (int4*)rect, depth, tiles_any, circumcenter,
         fine_shift, (int4*)rect_fine);
     return rm_host::check_launch("rm_project_fwd_multi");
