@@ -39,7 +39,7 @@ UNIT = "Mpix/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=150)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--points", type=int, default=200_000)
@@ -112,6 +112,11 @@ class ClockSampler:
             self.thread.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+        # nvidia-smi's start-up (NVML initialisation) stalls CUDA calls of this
+        # process for a while: wait for its first sample before the timed region
+        t0 = time.time()
+        while self.proc is not None and not self.lines and self.proc.poll() is None and time.time() - t0 < 15:
+            time.sleep(0.02)
         return self
 
     def _read(self):
@@ -188,10 +193,12 @@ def run_b200(args):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
     stats = {}
 
-    def step(v, c, i, tgt):
+    def step(v, c, i, tgt, features_ready=None):
         v.grad = None
         c.grad = None
         sorted_ids, ranges, vs, cc, mask, rect = vertex_and_tile_shader(i, v, tcam, grid)
+        if features_ready is not None:  # cell values and target still in flight during the tiling
+            torch.cuda.current_stream().wait_event(features_ready)
         img, distimg, _ = AlphaBlendTiledRender.apply(sorted_ids, ranges, i, v, c, grid, tcam, jitter, "cuda",
                                                       mask.to(torch.int32))
         loss = (img[..., :3] - tgt).abs().mean()
@@ -199,7 +206,7 @@ def run_b200(args):
         if world > 1:
             MG.allreduce_grads([v.grad, c.grad])
         stats["P"] = int(sorted_ids.shape[0])
-        stats["fine"] = R.fine_lists_of(sorted_ids, camst)  # read after the timed steps
+        stats["fine"] = R.fine_lists_of(sorted_ids, camst, jitter)  # read after the timed steps
         return loss, img
 
     for _ in range(args.warmup):
@@ -239,7 +246,7 @@ def run_b200(args):
     # (the issue-rate unit), from a separate untimed forward
     with torch.no_grad():
         sorted_ids, ranges, vs, cc, mask, rect = vertex_and_tile_shader(idx, verts, tcam, grid)
-        fine = R.fine_lists_of(sorted_ids, camst)
+        fine = R.fine_lists_of(sorted_ids, camst, jitter)
         if fine is not None:  # the lists the timed blend walked
             sorted_ids, ranges, bcam = fine.sorted_ids, fine.ranges, fine.cam
         else:
@@ -260,6 +267,10 @@ def run_b200(args):
         idx_d = torch.empty_like(idx)
         tgt_d = torch.empty_like(target)
         loss_h = torch.empty(1, dtype=torch.float32).pin_memory()
+        # Host->device copies on a copy stream: the tiling starts once the
+        # vertices and indices are in, while the cell values and the target
+        # image (needed from the blend on) are still being copied.
+        copy_stream = torch.cuda.Stream(device=dev)
         e2e_times = []
         if world > 1:
             dist.barrier()
@@ -269,13 +280,20 @@ def run_b200(args):
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record()
-            verts_d.detach().copy_(verts_h, non_blocking=True)
-            cv_d.detach().copy_(cv_h, non_blocking=True)
-            idx_d.copy_(idx_h, non_blocking=True)
-            tgt_d.copy_(target_h, non_blocking=True)
+            geometry_ready = torch.cuda.Event()
+            features_ready = torch.cuda.Event()
+            copy_stream.wait_event(a)
+            with torch.cuda.stream(copy_stream):
+                idx_d.copy_(idx_h, non_blocking=True)
+                verts_d.detach().copy_(verts_h, non_blocking=True)
+                geometry_ready.record()
+                cv_d.detach().copy_(cv_h, non_blocking=True)
+                tgt_d.copy_(target_h, non_blocking=True)
+                features_ready.record()
+            torch.cuda.current_stream().wait_event(geometry_ready)
             vd = verts_d.detach().requires_grad_(True)
             cd = cv_d.detach().requires_grad_(True)
-            loss, _ = step(vd, cd, idx_d, tgt_d)
+            loss, _ = step(vd, cd, idx_d, tgt_d, features_ready)
             loss_h.copy_(loss.detach().reshape(1), non_blocking=True)
             b.record()
             b.synchronize()

@@ -253,36 +253,49 @@ RM_API int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges,
                  size_t workspace_bytes, int flags, void* stream);
 
 /*
- * rm_project_fwd plus tile rectangles on a 2^fine_shift times finer grid
- * (tiles of tile_width >> fine_shift by tile_height >> fine_shift pixels, grid
- * grid_width << fine_shift by grid_height << fine_shift): rect_fine [T,4] and
- * tiles_fine [T].  A fine rectangle covers the tet's screen box grown by 1/64
- * pixel, clipped to its coarse rectangle, so the fine list of a fine tile
- * holds, in the coarse list's order, every entry of the coarse list that can
- * reach a pixel of that fine tile.  Blending over the fine lists therefore
- * yields the image, log T and distortion of blending over the coarse lists
- * with fewer ray/tet tests (n_contrib then counts fine-list entries).  No
- * reference counterpart; fine_shift is 1, 2 or 3.
+ * rm_project_fwd plus each tet's image-space bounding box: box [T,4] float
+ * (min x, min y, max x, max y in pixels, from the same clipped and projected
+ * points as rect; zeros for culled tets).  The lists of smaller tiles are cut
+ * from the coarse lists with it (rm_fine_lists).  No reference counterpart.
  */
 RM_API int rm_project_fwd_fine(const int32_t* indices, const float* vertices, int64_t n_tets,
-                               int64_t n_verts, const rm_camera* cam, int fine_shift,
+                               int64_t n_verts, const rm_camera* cam,
                                int32_t* tiles_touched, int32_t* rect, float* vs,
-                               float* circumcenter, int32_t* tiles_fine, int32_t* rect_fine,
-                               void* stream);
+                               float* circumcenter, float* box, void* stream);
+
+/*
+ * Bounds of the per-pixel ray jitter [n_pixels, 2]: bounds [4] on the device
+ * = (min jx, min jy, max jx, max jy), NaNs ignored.  Two small launches, no
+ * host synchronisation.  Workspace: rm_jitter_bounds_workspace_size() bytes,
+ * 16-byte aligned.  No reference counterpart.
+ */
+RM_API size_t rm_jitter_bounds_workspace_size(void);
+RM_API int rm_jitter_bounds(const float* ray_jitter, int64_t n_pixels, float* bounds,
+                            void* workspace, size_t workspace_bytes, void* stream);
 
 /*
  * Fine lists from the sorted coarse lists: splits each coarse tile's list
  * (sorted_ids, ranges [G,2]) in order into the lists of its 2^fine_shift x
- * 2^fine_shift fine tiles, using rect_fine [T,4] of rm_project_fwd_fine.  The
- * result equals emitting, sorting and ranging the fine pairs: fine_ids
- * (capacity entries; 4^fine_shift * P always suffices) and fine_ranges
- * [G * 4^fine_shift, 2] on the fine grid, *total_dev = fine pair count.
+ * 2^fine_shift fine tiles (tile_width >> fine_shift by tile_height >>
+ * fine_shift pixels, on a grid 2^fine_shift times larger).  An entry goes to
+ * a fine tile when its tet's box (rm_project_fwd_fine), grown by 1/64 pixel,
+ * meets the image points that the fine tile's pixel rays pass through with
+ * any jitter inside jitter_bounds (rm_jitter_bounds of the ray_jitter that
+ * the blend will use).  So the fine list of a fine tile holds, in the coarse
+ * list's order, every entry of the coarse list that can reach one of its
+ * rays, and blending over the fine lists yields the image, log T and
+ * distortion of blending over the coarse lists with fewer ray/tet tests
+ * (n_contrib then counts fine-list entries).  The result equals emitting,
+ * sorting and ranging the fine pairs: fine_ids (capacity entries;
+ * 4^fine_shift * P always suffices) and fine_ranges [G * 4^fine_shift, 2] on
+ * the fine grid, *total_dev = fine pair count.  fine_shift is 1, 2 or 3.
  * Workspace: rm_fine_lists_workspace_size(fine tiles), 256-byte aligned.  No
  * reference counterpart.
  */
 RM_API size_t rm_fine_lists_workspace_size(int64_t n_fine_tiles);
 RM_API int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges,
-                         const int32_t* rect_fine, const rm_camera* cam, int fine_shift,
+                         const float* box, const float* jitter_bounds,
+                         const rm_camera* cam, int fine_shift,
                          int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
                          int64_t* total_dev, void* workspace, size_t workspace_bytes,
                          void* stream);
@@ -314,30 +327,30 @@ RM_API int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges,
  * and rect [n_views, T] (rect rows of 4), depth [n_views, T] (rm_project_fwd's
  * vs[:, 2]).  tiles_any [T] (optional) receives the tet's tile count summed
  * over the views; circumcenter [T, 3] (optional) is view-independent.
- * rect_fine [n_views, T, 4] (optional) receives rm_project_fwd_fine's
- * rectangles on the 2^fine_shift times finer grid.
+ * box [n_views, T, 4] (optional) receives rm_project_fwd_fine's image-space
+ * boxes.
  */
 RM_API int rm_project_fwd_multi(const int32_t* indices, const float* vertices,
                                 int64_t n_tets, int64_t n_verts,
                                 const rm_camera* cams, int n_views,
                                 int32_t* tiles_touched, int32_t* rect,
                                 float* depth, int32_t* tiles_any,
-                                float* circumcenter, int fine_shift,
-                                int32_t* rect_fine, void* stream);
+                                float* circumcenter, float* box, void* stream);
 
 /*
  * rm_fine_lists for a view batch: the coarse lists of all views (global
  * view-major tiles) split into the lists of the finer tiles, numbered
  * view-major on the finer grids (view v's fine tiles start at
- * tile_base(v) * 4^fine_shift), using rect_fine [n_views, T, 4] of
- * rm_project_fwd_multi.  Blending a batch of the fine cameras (tiles
- * 2^fine_shift times smaller, grids that much larger) over these lists gives
- * the coarse batch's images bit for bit.  rect_fine may be NULL when
- * fine_shift is 1 and the sorted values carry the packed 2x2 coverage bits of
+ * tile_base(v) * 4^fine_shift), using box [n_views, T, 4] of
+ * rm_project_fwd_multi and the bounds of the batch's concatenated ray jitter.
+ * Blending a batch of the fine cameras (tiles 2^fine_shift times smaller,
+ * grids that much larger) over these lists gives the coarse batch's images
+ * bit for bit.  box (and jitter_bounds) may be NULL when fine_shift is 1 and
+ * the sorted values carry the packed 2x2 coverage bits of
  * rm_emit_pairs_multi; fine_ids then hold the plain tet ids.
  */
 RM_API int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges,
-                               const int32_t* rect_fine, int64_t n_tets,
+                               const float* box, const float* jitter_bounds, int64_t n_tets,
                                const rm_camera* cams, int n_views, int fine_shift,
                                int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
                                int64_t* total_dev, void* workspace, size_t workspace_bytes,
@@ -347,20 +360,21 @@ RM_API int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges,
  * Pair emission for the stacked projection: offsets is the inclusive scan of
  * tiles_touched [n_views * T].  Pair (view v, tet g, tile (x, y)) gets the key
  * ((tile_base(v) + y * grid_w(v) + x) << 32) | sortable(depth[v, g]) and the
- * value g.  Capacity handling as rm_emit_pairs.  rect_fine_2x (optional,
- * [n_views, T, 4], rm_project_fwd_multi's rectangles for fine_shift 1): the
- * value then also carries, in bits 28..31, which of the tile's 2x2 fine tiles
- * the fine rectangle covers (bit qy * 2 + qx; T < 2^28), for
- * rm_fine_lists_multi to split the sorted lists without reading the
- * rectangles again.  Such values are not plain tet ids.
+ * value g.  Capacity handling as rm_emit_pairs.  box_2x (optional,
+ * [n_views, T, 4], rm_project_fwd_multi's boxes) with jitter_bounds
+ * (rm_jitter_bounds of the batch's ray jitter): the value then also carries,
+ * in bits 28..31, which of the tile's 2x2 half-size tiles the tet can reach
+ * (the test of rm_fine_lists; bit qy * 2 + qx; T < 2^28; even tile sizes),
+ * for rm_fine_lists_multi to split the sorted lists without reading the boxes
+ * again.  Such values are not plain tet ids.
  */
 RM_API int rm_emit_pairs_multi(const float* depth, const int32_t* rect,
                                const int32_t* offsets, int64_t n_tets,
                                const rm_camera* cams, int n_views,
                                int64_t capacity, const int64_t* total_dev,
                                int64_t* keys, int32_t* values,
-                               uint32_t* status_dev, const int32_t* rect_fine_2x,
-                               void* stream);
+                               uint32_t* status_dev, const float* box_2x,
+                               const float* jitter_bounds, void* stream);
 
 /* Total tile count of a batch (the ranges length and the blend workspace's
  * n_tiles), or -1 on bad input. */

@@ -126,7 +126,9 @@ class BatchedRasterizer:
         bv = self.blend_views
         self._ws_base = int(L.rm_blend_workspace_size(ws_tets, bv.n_tiles))
         if self.fine_shift:
-            self.rect_fine = torch.empty((n * T, 4), dtype=torch.int32, device=dev)
+            self.box = torch.empty((n * T, 4), dtype=torch.float32, device=dev)
+            self.jitter_bounds = torch.empty(4, dtype=torch.float32, device=dev)
+            self.jitter_ws = torch.empty(L.rm_jitter_bounds_workspace_size(), dtype=torch.uint8, device=dev)
             self.fine_ranges = torch.empty((bv.n_tiles, 2), dtype=torch.int32, device=dev)
             self.fine_total = torch.zeros(1, dtype=torch.int64, device=dev)
             self.fine_ws = torch.empty(L.rm_fine_lists_workspace_size(bv.n_tiles), dtype=torch.uint8, device=dev)
@@ -203,10 +205,10 @@ class BatchedRasterizer:
     def _project_scan(self):
         L, s, v = C.lib(), C.stream_handle(), self.views
         nT = v.n * self.T
-        rf = self.rect_fine if self.fine_shift else None
+        box = self.box if self.fine_shift else None
         R._call("rm_project_fwd_multi", lambda: L.rm_project_fwd_multi(
             C.ptr(self.indices), C.ptr(self.vertices), self.T, self.V, v.array, v.n, C.ptr(self.tiles),
-            C.ptr(self.rect), C.ptr(self.depth), C.ptr(self.tiles_any), None, self.fine_shift, C.ptr(rf), s))
+            C.ptr(self.rect), C.ptr(self.depth), C.ptr(self.tiles_any), None, C.ptr(box), s))
         R._call("rm_scan_tiles", lambda: L.rm_scan_tiles(C.ptr(self.tiles), nT, C.ptr(self.offsets), C.ptr(self.total),
                                 C.ptr(self.scan_ws), self.scan_ws.numel(), s))
 
@@ -215,10 +217,16 @@ class BatchedRasterizer:
         # fine_shift 1: the 2x2 coverage bits ride in the sorted values, so the
         # split reads no rectangles
         packed = self.fine_shift == 1 and self.T < (1 << 28)
-        rfp = self.rect_fine if packed else None
+        if self.fine_shift:
+            # the lists of the smaller tiles depend on the ray jitter's range
+            R._call("rm_jitter_bounds", lambda: L.rm_jitter_bounds(
+                C.ptr(self.jitter), self.jitter.numel() // 2, C.ptr(self.jitter_bounds), C.ptr(self.jitter_ws),
+                self.jitter_ws.numel(), s))
+        bp = self.box if packed else None
+        jb = self.jitter_bounds if packed else None
         R._call("rm_emit_pairs_multi", lambda: L.rm_emit_pairs_multi(
             C.ptr(self.depth), C.ptr(self.rect), C.ptr(self.offsets), self.T, v.array, v.n, self.capacity,
-            C.ptr(self.total), C.ptr(self.keys), C.ptr(self.vals), C.ptr(self.status), C.ptr(rfp), s))
+            C.ptr(self.total), C.ptr(self.keys), C.ptr(self.vals), C.ptr(self.status), C.ptr(bp), C.ptr(jb), s))
         R._call("rm_sort_pairs", lambda: L.rm_sort_pairs(C.ptr(self.keys), C.ptr(self.vals), self.capacity, C.ptr(self.total), v.end_bit,
                                 C.ptr(self.sorted_keys), C.ptr(self.sorted_ids), C.ptr(self.sort_ws),
                                 self.sort_ws.numel(), s))
@@ -226,8 +234,8 @@ class BatchedRasterizer:
                                  v.n_tiles, s))
         if self.fine_shift:
             R._call("rm_fine_lists", lambda: L.rm_fine_lists_multi(
-                C.ptr(self.sorted_ids), C.ptr(self.ranges), None if packed else C.ptr(self.rect_fine), self.T,
-                v.array, v.n,
+                C.ptr(self.sorted_ids), C.ptr(self.ranges), None if packed else C.ptr(self.box),
+                None if packed else C.ptr(self.jitter_bounds), self.T, v.array, v.n,
                 self.fine_shift, self.fine_ids.shape[0], C.ptr(self.fine_ids), C.ptr(self.fine_ranges),
                 C.ptr(self.fine_total), C.ptr(self.fine_ws), self.fine_ws.numel(), s))
 

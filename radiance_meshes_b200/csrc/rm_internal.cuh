@@ -182,6 +182,22 @@ struct ViewSet {
     __device__ __forceinline__ int64_t pixel_base(int v) const { return pixels[v]; }
 };
 
+// Whether a tet can reach a pixel of the tile with pixel columns [x0, x0 + w)
+// and rows [y0, y0 + h).  The ray of pixel (px, py) passes through the image
+// point (px + jx, py + jy); with the jitter inside jb = (min jx, min jy,
+// max jx, max jy) every such point of the tile lies in
+// [x0 + jb.x, x0 + w - 1 + jb.z] x [y0 + jb.y, y0 + h - 1 + jb.w] (rounding
+// is monotone, so the float sums bound the float sums of the kernels).  A ray
+// through a point farther than kBoxMargin from the tet's image-space box
+// (rm_project_fwd_fine) misses the tet; the margin covers the rounding of the
+// projection against the ray setup many times over.
+constexpr float kBoxMargin = 1.0f / 64.0f;
+
+__device__ __forceinline__ bool box_meets_tile(float4 b, float4 jb, int x0, int y0, int w, int h) {
+    return b.x - kBoxMargin <= (float)(x0 + w - 1) + jb.z && b.z + kBoxMargin >= (float)x0 + jb.x &&
+           b.y - kBoxMargin <= (float)(y0 + h - 1) + jb.w && b.w + kBoxMargin >= (float)y0 + jb.y;
+}
+
 // Bounded spin helper: returns false once the budget is exhausted.
 __device__ __forceinline__ bool spin_budget(uint32_t& left) {
     if (left == 0) return false;

@@ -251,15 +251,14 @@ __device__ __forceinline__ bool outside_view(const rm_camera& c, const TetGeom& 
 // Per-view part of vertex_shader (vertex_shader.slang:36-89): camera space,
 // find_extent, the depth key and the tile rectangle.  Returns the tile count
 // (0: culled, r and depth zero).
-template <bool GENERAL, bool FINE = false>
+// BOX: also return the image-space bounding box (pixels: min x, min y, max x,
+// max y; zeros when culled) from which the lists of smaller tiles are cut.
+template <bool GENERAL, bool BOX = false>
 __device__ __forceinline__ int project_view(const rm_camera& cam, const TetGeom& t, int4& r, float& depth_out,
-                                            int fine_shift = 0, int4* rf = nullptr, int* n_fine = nullptr) {
+                                            float4* box_out = nullptr) {
     r = {0, 0, 0, 0};
     depth_out = 0.f;
-    if (FINE) {
-        *rf = {0, 0, 0, 0};
-        *n_fine = 0;
-    }
+    if (BOX) *box_out = {0.f, 0.f, 0.f, 0.f};
     if (t.planar || outside_view(cam, t)) return 0;
     const f3 cs0 = point2cam(cam, t.v[0]), cs1 = point2cam(cam, t.v[1]);
     const f3 cs2 = point2cam(cam, t.v[2]), cs3 = point2cam(cam, t.v[3]);
@@ -286,24 +285,7 @@ __device__ __forceinline__ int project_view(const rm_camera& cam, const TetGeom&
         return 0;
     }
     depth_out = fminf(fmaxf(depth, -1e20f), 1e20f);
-    if (FINE) {
-        // Rectangle on the grid of tiles 2^fine_shift times smaller, from the
-        // box grown by 1/64 pixel and clipped to the coarse rectangle: it holds
-        // every tet whose box comes within 1/64 pixel of the fine tile.
-        const int f = 1 << fine_shift;
-        const float ftw = tw / (float)f, fth = th / (float)f;
-        const float fgw = gw * (float)f, fgh = gh * (float)f;
-        const float m = 1.0f / 64.0f;
-        int4 q;
-        q.x = max((int)floorf(fmaxf(0.f, fminf(fgw, (box.mn.x - m) / ftw))), r.x * f);
-        q.y = max((int)floorf(fmaxf(0.f, fminf(fgh, (box.mn.y - m) / fth))), r.y * f);
-        q.z = min((int)ceilf(fmaxf(0.f, fminf(fgw, (box.mx.x + m) / ftw))), r.z * f);
-        q.w = min((int)ceilf(fmaxf(0.f, fminf(fgh, (box.mx.y + m) / fth))), r.w * f);
-        if (q.z > q.x && q.w > q.y) {
-            *rf = q;
-            *n_fine = (q.z - q.x) * (q.w - q.y);
-        }
-    }
+    if (BOX) *box_out = {box.mn.x, box.mn.y, box.mx.x, box.mx.y};
     return n_tiles;
 }
 
@@ -329,22 +311,20 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(const int4* __restrict
     cc[3 * g + 2] = n_tiles ? (float)t.center.z : 0.f;
 }
 
-// Projection plus the rectangles on a grid of 2^fine_shift times smaller tiles.
+// Projection plus each tet's image-space bounding box.
 template <bool GENERAL>
 __global__ void __launch_bounds__(256) project_fwd_fine_kernel(const int4* __restrict__ indices,
                                                                const float* __restrict__ verts, int64_t n_tets,
-                                                               const rm_camera cam, int fine_shift,
-                                                               int32_t* __restrict__ tiles, int4* __restrict__ rect,
-                                                               float* __restrict__ vs, float* __restrict__ cc,
-                                                               int32_t* __restrict__ tiles_fine,
-                                                               int4* __restrict__ rect_fine) {
+                                                               const rm_camera cam, int32_t* __restrict__ tiles,
+                                                               int4* __restrict__ rect, float* __restrict__ vs,
+                                                               float* __restrict__ cc, float4* __restrict__ box) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_tets) return;
     const TetGeom t = tet_geom(indices, verts, g);
-    int4 r, rf;
+    int4 r;
+    float4 b;
     float depth;
-    int nf;
-    const int n_tiles = project_view<GENERAL, true>(cam, t, r, depth, fine_shift, &rf, &nf);
+    const int n_tiles = project_view<GENERAL, true>(cam, t, r, depth, &b);
     tiles[g] = n_tiles;
     rect[g] = r;
     vs[3 * g + 0] = 0.f;
@@ -353,8 +333,7 @@ __global__ void __launch_bounds__(256) project_fwd_fine_kernel(const int4* __res
     cc[3 * g + 0] = n_tiles ? (float)t.center.x : 0.f;
     cc[3 * g + 1] = n_tiles ? (float)t.center.y : 0.f;
     cc[3 * g + 2] = n_tiles ? (float)t.center.z : 0.f;
-    tiles_fine[g] = nf;
-    rect_fine[g] = rf;
+    box[g] = b;
 }
 
 // All views of a batch: each thread loads its tet once and projects it into
@@ -365,21 +344,20 @@ __global__ void __launch_bounds__(256) project_fwd_multi_kernel(const int4* __re
                                                                 const __grid_constant__ ViewSet views,
                                                                 int32_t* __restrict__ tiles, int4* __restrict__ rect,
                                                                 float* __restrict__ depth, int32_t* __restrict__ any,
-                                                                float* __restrict__ cc, int fine_shift,
-                                                                int4* __restrict__ rect_fine) {
+                                                                float* __restrict__ cc, float4* __restrict__ box) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_tets) return;
     const TetGeom t = tet_geom(indices, verts, g);
     int total = 0;
     for (int v = 0; v < views.n; ++v) {
-        int4 r, rf;
+        int4 r;
+        float4 b;
         float dk;
-        int nf;
         const int64_t o = (int64_t)v * n_tets + g;
         int n_tiles;
-        if (rect_fine) {
-            n_tiles = project_view<GENERAL, true>(views.cams[v], t, r, dk, fine_shift, &rf, &nf);
-            rect_fine[o] = rf;
+        if (box) {
+            n_tiles = project_view<GENERAL, true>(views.cams[v], t, r, dk, &b);
+            box[o] = b;
         } else {
             n_tiles = project_view<GENERAL>(views.cams[v], t, r, dk);
         }
@@ -506,33 +484,28 @@ int rm_project_fwd(const int32_t* indices, const float* vertices, int64_t n_tets
 }
 
 int rm_project_fwd_fine(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,
-                        const rm_camera* cam, int fine_shift, int32_t* tiles_touched, int32_t* rect, float* vs,
-                        float* circumcenter, int32_t* tiles_fine, int32_t* rect_fine, void* stream) {
+                        const rm_camera* cam, int32_t* tiles_touched, int32_t* rect, float* vs, float* circumcenter,
+                        float* box, void* stream) {
     int rc = rm_host::check_cam(cam);
     if (rc) return rc;
     if (n_tets < 0 || n_verts < 0) return rm_host::fail(RM_EINVAL, "rm_project_fwd_fine: negative size");
-    if (fine_shift < 1 || fine_shift > 3 || (cam->tile_width >> fine_shift) << fine_shift != cam->tile_width ||
-        (cam->tile_height >> fine_shift) << fine_shift != cam->tile_height)
-        return rm_host::fail(RM_EINVAL, "rm_project_fwd_fine: tile %dx%d not divisible by 2^%d", cam->tile_width,
-                             cam->tile_height, fine_shift);
     if (n_tets == 0) return RM_OK;
-    if (!indices || !vertices || !tiles_touched || !rect || !vs || !circumcenter || !tiles_fine || !rect_fine)
+    if (!indices || !vertices || !tiles_touched || !rect || !vs || !circumcenter || !box)
         return rm_host::fail(RM_EINVAL, "rm_project_fwd_fine: NULL pointer");
-    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15) || ((uintptr_t)rect_fine & 15))
-        return rm_host::fail(RM_EINVAL, "rm_project_fwd_fine: indices and rects must be 16-byte aligned");
+    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15) || ((uintptr_t)box & 15))
+        return rm_host::fail(RM_EINVAL, "rm_project_fwd_fine: indices, rect and box must be 16-byte aligned");
     const int threads = 256;
     const int64_t blocks = (n_tets + threads - 1) / threads;
     auto kernel =
         rm_host::cam_general(*cam) ? rm::project_fwd_fine_kernel<true> : rm::project_fwd_fine_kernel<false>;
     kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
-        (const int4*)indices, vertices, n_tets, *cam, fine_shift, tiles_touched, (int4*)rect, vs, circumcenter,
-        tiles_fine, (int4*)rect_fine);
+        (const int4*)indices, vertices, n_tets, *cam, tiles_touched, (int4*)rect, vs, circumcenter, (float4*)box);
     return rm_host::check_launch("rm_project_fwd_fine");
 }
 
 int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,
                          const rm_camera* cams, int n_views, int32_t* tiles_touched, int32_t* rect, float* depth,
-                         int32_t* tiles_any, float* circumcenter, int fine_shift, int32_t* rect_fine, void* stream) {
+                         int32_t* tiles_any, float* circumcenter, float* box, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_project_fwd_multi", cams, n_views, &views);
     if (rc) return rc;
@@ -540,11 +513,8 @@ int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t 
     if (n_tets == 0) return RM_OK;
     if (!indices || !vertices || !tiles_touched || !rect || !depth)
         return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: NULL pointer");
-    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15) || ((uintptr_t)rect_fine & 15))
-        return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: indices and rects must be 16-byte aligned");
-    if (rect_fine && (fine_shift < 1 || fine_shift > 3 || (cams[0].tile_width >> fine_shift) << fine_shift !=
-                      cams[0].tile_width || (cams[0].tile_height >> fine_shift) << fine_shift != cams[0].tile_height))
-        return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: tile not divisible by 2^%d", fine_shift);
+    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15) || ((uintptr_t)box & 15))
+        return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: indices, rect and box must be 16-byte aligned");
     const int threads = 256;
     const int64_t blocks = (n_tets + threads - 1) / threads;
     bool general = false;
@@ -552,7 +522,7 @@ int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t 
     auto kernel = general ? rm::project_fwd_multi_kernel<true> : rm::project_fwd_multi_kernel<false>;
     kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
         (const int4*)indices, vertices, n_tets, views, tiles_touched, (int4*)rect, depth, tiles_any, circumcenter,
-        fine_shift, (int4*)rect_fine);
+        (float4*)box);
     return rm_host::check_launch("rm_project_fwd_multi");
 }
 

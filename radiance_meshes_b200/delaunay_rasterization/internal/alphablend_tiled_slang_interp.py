@@ -25,8 +25,8 @@ class AlphaBlendTiledRender(torch.autograd.Function):
         vertices = vertices.contiguous()
         tet_density = tet_density.contiguous()
         ray_jitter = ray_jitter.contiguous()
-        # lists of the 8x8-pixel tiles built with these ones (same image, fewer tests)
-        fine = R.fine_lists_of(sorted_tetra_idx, camst)
+        # lists of the 8x8-pixel tiles cut from these ones for this jitter (same image, fewer tests)
+        fine = R.fine_lists_of(sorted_tetra_idx, camst, ray_jitter)
         if fine is not None:
             sorted_tetra_idx, tile_ranges, camst = fine.sorted_ids, fine.ranges, fine.cam
         # hit masks let the backward skip the forward's misses

@@ -33,10 +33,10 @@ def render_err(gt_image, camera, model, tile_size=16, min_t=0.1, **kwargs):
         _, cell_values[mask] = model.get_cell_values(camera, mask)
         camst = tcam_to_struct(tcam)
         ids, rg, bcam = sorted_ids, ranges, camst
-        fine = R.fine_lists_of(sorted_ids, camst)
+        jitter = torch.full((camera.image_height, camera.image_width, 2), 0.5, device=device)
+        fine = R.fine_lists_of(sorted_ids, camst, jitter)
         if fine is not None:
             ids, rg, bcam = fine.sorted_ids, fine.ranges, fine.cam
-        jitter = torch.full((camera.image_height, camera.image_width, 2), 0.5, device=device)
         img, _, _, _ = R.blend_fwd(ids, rg, indices, vertices, cell_values, jitter, bcam,
                                    tiles_touched=mask.to(torch.int32))
         render_img = img.permute(2, 0, 1)[:3].clip(min=0, max=1)

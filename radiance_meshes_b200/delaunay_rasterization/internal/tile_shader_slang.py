@@ -24,25 +24,25 @@ def vertex_and_tile_shader(indices, vertices, cam, render_grid):
     circumcenter [T,3], mask [T] bool, rect_tile_space [T,4] i32) exactly as
     the reference (tile_shader_slang.py:24-72).
 
-    For tiles of 16x16 pixels or more, the lists of the same frame on the grid
-    of 8x8-pixel tiles are built as well and attached to the returned
-    ``sorted_tetra_idx`` (attribute ``rm_fine``);
-    ``AlphaBlendTiledRender`` blends over them when it is handed that tensor,
-    which gives the same image with fewer ray/tet tests (see
-    ``rasterizer.FineLists``)."""
+    For tiles of 16x16 pixels or more, what it takes to cut the lists of the
+    same frame on the grid of 8x8-pixel tiles (the tets' image boxes) is
+    attached to the returned ``sorted_tetra_idx`` (attribute ``rm_fine``);
+    ``AlphaBlendTiledRender`` cuts them for its ray jitter and blends over
+    them when it is handed that tensor, which gives the same image with fewer
+    ray/tet tests (see ``rasterizer.FineLists``)."""
     camst = tcam_to_struct(cam)
     fs = R.fine_shift_for(camst) if R.fine_lists_enabled() else 0
     pre = None
     if fs:
         with torch.no_grad():
-            tiles, rect, vs, cc, tiles_f, rect_f = R.project_fwd_fine(indices, vertices, camst, fs)
+            tiles, rect, vs, cc, box = R.project_fwd_fine(indices, vertices, camst)
         pre = (tiles, rect, vs, cc)
     tiles_touched, rect_tile_space, vs_tetra, circumcenter = VertexShader.apply(
         indices, vertices, cam, render_grid, "cuda", pre)
     with torch.no_grad():
         lists = R.build_tile_lists(tiles_touched, rect_tile_space, vs_tetra, camst)
         if fs:
-            R.attach_fine_lists(lists.sorted_ids, lists.ranges, camst, fs, rect_f)
+            R.attach_fine_lists(lists.sorted_ids, lists.ranges, camst, fs, box)
     mask = tiles_touched > 0
     return lists.sorted_ids, lists.ranges, vs_tetra, circumcenter, mask, rect_tile_space
 

@@ -24,6 +24,8 @@ __all__ = [
     "TileLists",
     "project_fwd",
     "project_fwd_fine",
+    "jitter_bounds",
+    "split_fine_lists",
     "fine_shift_for",
     "fine_camera",
     "project_bwd",
@@ -179,9 +181,10 @@ def fine_camera(cam: RMCamera, fine_shift: int) -> RMCamera:
     return out
 
 
-def project_fwd_fine(indices: torch.Tensor, vertices: torch.Tensor, cam: RMCamera, fine_shift: int):
-    """project_fwd plus the tets' rectangles on the 2^fine_shift times finer
-    tile grid (rm_project_fwd_fine)."""
+def project_fwd_fine(indices: torch.Tensor, vertices: torch.Tensor, cam: RMCamera):
+    """project_fwd plus each tet's image-space bounding box [T,4] (min x, min y,
+    max x, max y in pixels; rm_project_fwd_fine), from which the lists of
+    smaller tiles are cut."""
     _require_cuda(indices=indices, vertices=vertices)
     indices = _i32(indices)
     vertices = _f32(vertices)
@@ -191,12 +194,28 @@ def project_fwd_fine(indices: torch.Tensor, vertices: torch.Tensor, cam: RMCamer
     rect = torch.empty((T, 4), dtype=torch.int32, device=dev)
     vs = torch.empty((T, 3), dtype=torch.float32, device=dev)
     cc = torch.empty((T, 3), dtype=torch.float32, device=dev)
-    tiles_f = torch.empty(T, dtype=torch.int32, device=dev)
-    rect_f = torch.empty((T, 4), dtype=torch.int32, device=dev)
+    box = torch.empty((T, 4), dtype=torch.float32, device=dev)
     _call("rm_project_fwd", lambda: C.lib().rm_project_fwd_fine(
-        C.ptr(indices), C.ptr(vertices), T, vertices.shape[0], ctypes.byref(cam), fine_shift, C.ptr(tiles),
-        C.ptr(rect), C.ptr(vs), C.ptr(cc), C.ptr(tiles_f), C.ptr(rect_f), _stream()))
-    return tiles, rect, vs, cc, tiles_f, rect_f
+        C.ptr(indices), C.ptr(vertices), T, vertices.shape[0], ctypes.byref(cam), C.ptr(tiles), C.ptr(rect),
+        C.ptr(vs), C.ptr(cc), C.ptr(box), _stream()))
+    return tiles, rect, vs, cc, box
+
+
+def jitter_bounds(ray_jitter: torch.Tensor, pool: ScratchPool | None = None) -> torch.Tensor:
+    """(min jx, min jy, max jx, max jy) of a per-pixel ray jitter [..., 2], as a
+    [4] tensor on the device (rm_jitter_bounds; no host synchronisation)."""
+    pool = pool or _POOL
+    _require_cuda(ray_jitter=ray_jitter)
+    ray_jitter = _f32(ray_jitter)
+    if ray_jitter.shape[-1] != 2:
+        raise ValueError("ray_jitter must have 2 values per pixel")
+    out = torch.empty(4, dtype=torch.float32, device=ray_jitter.device)
+    L = C.lib()
+    ws_n = L.rm_jitter_bounds_workspace_size()
+    ws = pool.get("jitter", ws_n, ray_jitter.device)
+    _call("rm_jitter_bounds", lambda: L.rm_jitter_bounds(C.ptr(ray_jitter), ray_jitter.numel() // 2, C.ptr(out),
+                                                         C.ptr(ws), ws_n, _stream()))
+    return out
 
 
 def project_bwd(indices, vertices, cam: RMCamera, tiles, grad_vs, grad_cc, grad_vertices=None):
@@ -250,13 +269,13 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
 
 @dataclass
 class FineLists:
-    """Tile lists of one frame on the grid of 8x8-pixel tiles, kept beside the
-    lists of the caller's (larger) tiles.  Every entry of a coarse list that
-    can reach a pixel of a fine tile is in that fine tile's list, in the same
-    order (rm_project_fwd_fine, rm_fine_lists), so blending over the fine
-    lists gives the coarse blend's image, log T and distortion bit for bit;
-    n_contributors then counts fine-list entries, which only the backward pass
-    reads."""
+    """Tile lists of one frame on the grid of 8x8-pixel tiles, cut from the
+    lists of the caller's (larger) tiles for one ray jitter.  Every entry of a
+    coarse list that can reach a ray of a fine tile's pixels is in that fine
+    tile's list, in the same order (rm_project_fwd_fine, rm_jitter_bounds,
+    rm_fine_lists), so blending over the fine lists with that jitter gives the
+    coarse blend's image, log T and distortion bit for bit; n_contributors then
+    counts fine-list entries, which only the backward pass reads."""
     shift: int
     cam: RMCamera  # the fine camera
     coarse_key: tuple
@@ -267,6 +286,21 @@ class FineLists:
     @property
     def n_pairs(self) -> int:
         return int(self.total.item())
+
+
+@dataclass
+class PendingFineLists:
+    """What the projection leaves on the sorted coarse ids: the coarse ranges,
+    the tets' image boxes and the split factor.  The split itself needs the
+    ray jitter of the blend, so it runs in fine_lists_of (once per jitter)."""
+    shift: int
+    coarse_cam: RMCamera
+    coarse_key: tuple
+    ranges: torch.Tensor
+    box: torch.Tensor
+    jitter: torch.Tensor | None = None  # the jitter of `lists` (kept alive so identity stays meaningful)
+    jitter_version: int = -1
+    lists: FineLists | None = None
 
 
 _FINE = {"enabled": True}
@@ -287,10 +321,18 @@ def _cam_key(cam: RMCamera) -> tuple:
 
 
 def attach_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCamera, fine_shift: int,
-                      rect_fine: torch.Tensor, pool: ScratchPool | None = None) -> FineLists:
-    """Split the sorted coarse lists into the fine lists (rm_fine_lists, no
-    host synchronisation) and attach them to ``sorted_ids`` (attribute
-    ``rm_fine``)."""
+                      box: torch.Tensor) -> PendingFineLists:
+    """Record on ``sorted_ids`` (attribute ``rm_fine``) what fine_lists_of needs
+    to cut the 2^fine_shift times smaller tiles' lists from these lists."""
+    pend = PendingFineLists(fine_shift, cam, _cam_key(cam), ranges, box)
+    sorted_ids.rm_fine = pend
+    return pend
+
+
+def split_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCamera, fine_shift: int,
+                     box: torch.Tensor, bounds: torch.Tensor, pool: ScratchPool | None = None) -> FineLists:
+    """Split the sorted coarse lists into the fine lists for the jitter bounds
+    ``bounds`` (rm_fine_lists, no host synchronisation)."""
     pool = pool or _POOL
     dev = sorted_ids.device
     camf = fine_camera(cam, fine_shift)
@@ -302,20 +344,25 @@ def attach_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCam
     L = C.lib()
     ws_n = L.rm_fine_lists_workspace_size(Gf)
     ws = pool.get("fine", ws_n, dev)
-    _call("rm_fine_lists", lambda: L.rm_fine_lists(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(rect_fine),
+    _call("rm_fine_lists", lambda: L.rm_fine_lists(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(box), C.ptr(bounds),
                                                    ctypes.byref(cam), fine_shift, cap, C.ptr(fine_ids),
                                                    C.ptr(fine_ranges), C.ptr(total), C.ptr(ws), ws_n, _stream()))
-    fine = FineLists(fine_shift, camf, _cam_key(cam), fine_ids, fine_ranges, total)
-    sorted_ids.rm_fine = fine
-    return fine
+    return FineLists(fine_shift, camf, _cam_key(cam), fine_ids, fine_ranges, total)
 
 
-def fine_lists_of(sorted_ids: torch.Tensor, cam: RMCamera) -> FineLists | None:
-    """The fine lists attached to ``sorted_ids`` for this camera, if any."""
-    fine = getattr(sorted_ids, "rm_fine", None)
-    if fine is None or not _FINE["enabled"] or fine.coarse_key != _cam_key(cam):
+def fine_lists_of(sorted_ids: torch.Tensor, cam: RMCamera, ray_jitter: torch.Tensor) -> FineLists | None:
+    """The fine lists of ``sorted_ids`` for this camera and ray jitter, if the
+    projection prepared them (cut on the first call for a jitter tensor and
+    kept while that tensor is unchanged)."""
+    pend = getattr(sorted_ids, "rm_fine", None)
+    if pend is None or not _FINE["enabled"] or pend.coarse_key != _cam_key(cam):
         return None
-    return fine
+    if pend.lists is not None and pend.jitter is ray_jitter and pend.jitter_version == ray_jitter._version:
+        return pend.lists
+    bounds = jitter_bounds(ray_jitter)
+    pend.lists = split_fine_lists(sorted_ids, pend.ranges, pend.coarse_cam, pend.shift, pend.box, bounds)
+    pend.jitter, pend.jitter_version = ray_jitter, ray_jitter._version
+    return pend.lists
 
 
 _BLEND_FLAGS = {"fwd": 0, "bwd": 0}

@@ -153,12 +153,12 @@ def test_view_batch_rejects_bad_batches():
     many = (RMCamera * (C.RM_MAX_VIEWS + 1))(*([cams[0]] * (C.RM_MAX_VIEWS + 1)))
     assert L.rm_views_tile_count(many, C.RM_MAX_VIEWS + 1) == -1
     assert L.rm_views_tile_count(arr, 0) == -1
-    rc = L.rm_project_fwd_multi(None, None, 10, 10, arr, 2, None, None, None, None, None, 0, None, None)
+    rc = L.rm_project_fwd_multi(None, None, 10, 10, arr, 2, None, None, None, None, None, None, None)
     assert rc == C.RM_EINVAL
     ok = (RMCamera * 2)(*cams)
-    assert L.rm_project_fwd_multi(None, None, 10, 10, ok, 2, None, None, None, None, None, 0, None, None) == C.RM_EINVAL
-    assert L.rm_project_fwd_multi(None, None, 0, 0, ok, 2, None, None, None, None, None, 0, None, None) == C.RM_OK
-    assert L.rm_emit_pairs_multi(None, None, None, 0, ok, 2, 0, None, None, None, None, None, None) == C.RM_OK
+    assert L.rm_project_fwd_multi(None, None, 10, 10, ok, 2, None, None, None, None, None, None, None) == C.RM_EINVAL
+    assert L.rm_project_fwd_multi(None, None, 0, 0, ok, 2, None, None, None, None, None, None, None) == C.RM_OK
+    assert L.rm_emit_pairs_multi(None, None, None, 0, ok, 2, 0, None, None, None, None, None, None, None) == C.RM_OK
 
 
 def test_autotune_flag_packing():

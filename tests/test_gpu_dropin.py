@@ -120,24 +120,36 @@ def _dropin_step(mesh, view, jitter, fine, tile=16):
         R.use_fine_lists(True)
 
 
-@pytest.mark.parametrize("scene,tile", [("plain", 16), ("mixture", 16), ("mixture", 32)])
-def test_fine_lists_give_the_coarse_frame(cuda, scene, tile):
+@pytest.mark.parametrize("scene,tile,jit", [("plain", 16, "unit"), ("mixture", 16, "unit"), ("mixture", 32, "unit"),
+                                            ("mixture", 16, "half"), ("mixture", 16, "wide"),
+                                            ("plain", 32, "wide")])
+def test_fine_lists_give_the_coarse_frame(cuda, scene, tile, jit):
     """Blending over the 8x8-pixel lists reproduces the blend over the
-    caller's 16x16 / 32x32 lists: image and distortion bit for bit, gradients
-    up to FP32 summation order; the lists returned to the caller are the
-    coarse ones."""
+    caller's 16x16 / 32x32 lists for any ray jitter (uniform in [0, 1) as in
+    training, the constant 0.5 of render(), and a jitter that reaches up to
+    1.5 pixels past the pixel): image and distortion bit for bit, gradients up
+    to FP32 summation order; the lists returned to the caller are the coarse
+    ones."""
     if scene == "plain":
         mesh, view = scenes.workload_plain_forward()
     else:
         mesh, view = scenes.workload_training_step(n_points=20000, seed=2, height=420, width=649)
     rng = np.random.default_rng(4)
-    jitter = torch.from_numpy(rng.uniform(0, 1, (view.height, view.width, 2)).astype(np.float32)).cuda()
+    shape = (view.height, view.width, 2)
+    if jit == "unit":
+        j = rng.uniform(0, 1, shape)
+    elif jit == "half":
+        j = np.full(shape, 0.5)
+    else:
+        j = rng.uniform(-1.5, 2.5, shape)
+    jitter = torch.from_numpy(j.astype(np.float32)).cuda()
     ids_c, rg_c, img_c, dist_c, gv_c, gc_c = _dropin_step(mesh, view, jitter, False, tile)
     ids_f, rg_f, img_f, dist_f, gv_f, gc_f = _dropin_step(mesh, view, jitter, True, tile)
     assert torch.equal(ids_c, ids_f) and torch.equal(rg_c, rg_f)
     assert torch.equal(img_c.view(torch.int32), img_f.view(torch.int32))
     assert torch.equal(dist_c.view(torch.int32), dist_f.view(torch.int32))
-    assert ids_f.rm_fine.n_pairs > ids_c.shape[0]
-    assert ids_f.rm_fine.sorted_ids.shape[0] >= ids_f.rm_fine.n_pairs
+    fine = ids_f.rm_fine.lists
+    assert fine.n_pairs > ids_c.shape[0]
+    assert fine.sorted_ids.shape[0] >= fine.n_pairs
     for a, b in ((gv_f, gv_c), (gc_f, gc_c)):
         assert float((a - b).norm() / b.norm()) < 1e-5
