@@ -253,15 +253,20 @@ RM_API int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges,
                  size_t workspace_bytes, int flags, void* stream);
 
 /*
- * rm_project_fwd plus each tet's image-space bounding box: box [T,4] float
- * (min x, min y, max x, max y in pixels, from the same clipped and projected
- * points as rect; zeros for culled tets).  The lists of smaller tiles are cut
- * from the coarse lists with it (rm_fine_lists).  No reference counterpart.
+ * rm_project_fwd plus each tet's image footprint, footprint [T,12] float:
+ *   [0:4]  the image-space bounding box (min x, min y, max x, max y in pixels,
+ *          from the same clipped and projected points as rect);
+ *   [4:12] the four projected vertices (x0 y0 x1 y1 x2 y2 x3 y3) when all four
+ *          lie in front of a pinhole camera without distortion (z > 1e-4, so
+ *          nothing is clipped) and within 8192 pixels of the image origin,
+ *          NaN otherwise;
+ * zeros for culled tets.  The lists of smaller tiles are cut from the coarse
+ * lists with it (rm_fine_lists).  No reference counterpart.
  */
 RM_API int rm_project_fwd_fine(const int32_t* indices, const float* vertices, int64_t n_tets,
                                int64_t n_verts, const rm_camera* cam,
                                int32_t* tiles_touched, int32_t* rect, float* vs,
-                               float* circumcenter, float* box, void* stream);
+                               float* circumcenter, float* footprint, void* stream);
 
 /*
  * Bounds of the per-pixel ray jitter [n_pixels, 2]: bounds [4] on the device
@@ -278,10 +283,12 @@ RM_API int rm_jitter_bounds(const float* ray_jitter, int64_t n_pixels, float* bo
  * (sorted_ids, ranges [G,2]) in order into the lists of its 2^fine_shift x
  * 2^fine_shift fine tiles (tile_width >> fine_shift by tile_height >>
  * fine_shift pixels, on a grid 2^fine_shift times larger).  An entry goes to
- * a fine tile when its tet's box (rm_project_fwd_fine), grown by 1/64 pixel,
- * meets the image points that the fine tile's pixel rays pass through with
- * any jitter inside jitter_bounds (rm_jitter_bounds of the ray_jitter that
- * the blend will use).  So the fine list of a fine tile holds, in the coarse
+ * a fine tile when its tet's footprint (rm_project_fwd_fine) can meet the
+ * image points that the fine tile's pixel rays pass through with any jitter
+ * inside jitter_bounds (rm_jitter_bounds of the ray_jitter that the blend
+ * will use): the box grown by 1/64 pixel meets them, and, when the projected
+ * vertices are given, no edge of their convex hull has all of them more than
+ * 1/16 pixel outside.  So the fine list of a fine tile holds, in the coarse
  * list's order, every entry of the coarse list that can reach one of its
  * rays, and blending over the fine lists yields the image, log T and
  * distortion of blending over the coarse lists with fewer ray/tet tests
@@ -294,7 +301,7 @@ RM_API int rm_jitter_bounds(const float* ray_jitter, int64_t n_pixels, float* bo
  */
 RM_API size_t rm_fine_lists_workspace_size(int64_t n_fine_tiles);
 RM_API int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges,
-                         const float* box, const float* jitter_bounds,
+                         const float* footprint, const float* jitter_bounds,
                          const rm_camera* cam, int fine_shift,
                          int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
                          int64_t* total_dev, void* workspace, size_t workspace_bytes,
@@ -327,30 +334,30 @@ RM_API int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges,
  * and rect [n_views, T] (rect rows of 4), depth [n_views, T] (rm_project_fwd's
  * vs[:, 2]).  tiles_any [T] (optional) receives the tet's tile count summed
  * over the views; circumcenter [T, 3] (optional) is view-independent.
- * box [n_views, T, 4] (optional) receives rm_project_fwd_fine's image-space
- * boxes.
+ * footprint [n_views, T, 12] (optional) receives rm_project_fwd_fine's
+ * footprints.
  */
 RM_API int rm_project_fwd_multi(const int32_t* indices, const float* vertices,
                                 int64_t n_tets, int64_t n_verts,
                                 const rm_camera* cams, int n_views,
                                 int32_t* tiles_touched, int32_t* rect,
                                 float* depth, int32_t* tiles_any,
-                                float* circumcenter, float* box, void* stream);
+                                float* circumcenter, float* footprint, void* stream);
 
 /*
  * rm_fine_lists for a view batch: the coarse lists of all views (global
  * view-major tiles) split into the lists of the finer tiles, numbered
  * view-major on the finer grids (view v's fine tiles start at
- * tile_base(v) * 4^fine_shift), using box [n_views, T, 4] of
+ * tile_base(v) * 4^fine_shift), using footprint [n_views, T, 12] of
  * rm_project_fwd_multi and the bounds of the batch's concatenated ray jitter.
  * Blending a batch of the fine cameras (tiles 2^fine_shift times smaller,
  * grids that much larger) over these lists gives the coarse batch's images
- * bit for bit.  box (and jitter_bounds) may be NULL when fine_shift is 1 and
+ * bit for bit.  footprint (and jitter_bounds) may be NULL when fine_shift is 1 and
  * the sorted values carry the packed 2x2 coverage bits of
  * rm_emit_pairs_multi; fine_ids then hold the plain tet ids.
  */
 RM_API int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges,
-                               const float* box, const float* jitter_bounds, int64_t n_tets,
+                               const float* footprint, const float* jitter_bounds, int64_t n_tets,
                                const rm_camera* cams, int n_views, int fine_shift,
                                int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
                                int64_t* total_dev, void* workspace, size_t workspace_bytes,
@@ -360,20 +367,20 @@ RM_API int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges,
  * Pair emission for the stacked projection: offsets is the inclusive scan of
  * tiles_touched [n_views * T].  Pair (view v, tet g, tile (x, y)) gets the key
  * ((tile_base(v) + y * grid_w(v) + x) << 32) | sortable(depth[v, g]) and the
- * value g.  Capacity handling as rm_emit_pairs.  box_2x (optional,
- * [n_views, T, 4], rm_project_fwd_multi's boxes) with jitter_bounds
+ * value g.  Capacity handling as rm_emit_pairs.  footprint_2x (optional,
+ * [n_views, T, 12], rm_project_fwd_multi's footprints) with jitter_bounds
  * (rm_jitter_bounds of the batch's ray jitter): the value then also carries,
  * in bits 28..31, which of the tile's 2x2 half-size tiles the tet can reach
  * (the test of rm_fine_lists; bit qy * 2 + qx; T < 2^28; even tile sizes),
- * for rm_fine_lists_multi to split the sorted lists without reading the boxes
- * again.  Such values are not plain tet ids.
+ * for rm_fine_lists_multi to split the sorted lists without reading the
+ * footprints again.  Such values are not plain tet ids.
  */
 RM_API int rm_emit_pairs_multi(const float* depth, const int32_t* rect,
                                const int32_t* offsets, int64_t n_tets,
                                const rm_camera* cams, int n_views,
                                int64_t capacity, const int64_t* total_dev,
                                int64_t* keys, int32_t* values,
-                               uint32_t* status_dev, const float* box_2x,
+                               uint32_t* status_dev, const float* footprint_2x,
                                const float* jitter_bounds, void* stream);
 
 /* Total tile count of a batch (the ranges length and the blend workspace's

@@ -126,7 +126,7 @@ class BatchedRasterizer:
         bv = self.blend_views
         self._ws_base = int(L.rm_blend_workspace_size(ws_tets, bv.n_tiles))
         if self.fine_shift:
-            self.box = torch.empty((n * T, 4), dtype=torch.float32, device=dev)
+            self.footprint = torch.empty((n * T, 12), dtype=torch.float32, device=dev)
             self.jitter_bounds = torch.empty(4, dtype=torch.float32, device=dev)
             self.jitter_ws = torch.empty(L.rm_jitter_bounds_workspace_size(), dtype=torch.uint8, device=dev)
             self.fine_ranges = torch.empty((bv.n_tiles, 2), dtype=torch.int32, device=dev)
@@ -205,10 +205,10 @@ class BatchedRasterizer:
     def _project_scan(self):
         L, s, v = C.lib(), C.stream_handle(), self.views
         nT = v.n * self.T
-        box = self.box if self.fine_shift else None
+        fp = self.footprint if self.fine_shift else None
         R._call("rm_project_fwd_multi", lambda: L.rm_project_fwd_multi(
             C.ptr(self.indices), C.ptr(self.vertices), self.T, self.V, v.array, v.n, C.ptr(self.tiles),
-            C.ptr(self.rect), C.ptr(self.depth), C.ptr(self.tiles_any), None, C.ptr(box), s))
+            C.ptr(self.rect), C.ptr(self.depth), C.ptr(self.tiles_any), None, C.ptr(fp), s))
         R._call("rm_scan_tiles", lambda: L.rm_scan_tiles(C.ptr(self.tiles), nT, C.ptr(self.offsets), C.ptr(self.total),
                                 C.ptr(self.scan_ws), self.scan_ws.numel(), s))
 
@@ -222,11 +222,11 @@ class BatchedRasterizer:
             R._call("rm_jitter_bounds", lambda: L.rm_jitter_bounds(
                 C.ptr(self.jitter), self.jitter.numel() // 2, C.ptr(self.jitter_bounds), C.ptr(self.jitter_ws),
                 self.jitter_ws.numel(), s))
-        bp = self.box if packed else None
+        fp = self.footprint if packed else None
         jb = self.jitter_bounds if packed else None
         R._call("rm_emit_pairs_multi", lambda: L.rm_emit_pairs_multi(
             C.ptr(self.depth), C.ptr(self.rect), C.ptr(self.offsets), self.T, v.array, v.n, self.capacity,
-            C.ptr(self.total), C.ptr(self.keys), C.ptr(self.vals), C.ptr(self.status), C.ptr(bp), C.ptr(jb), s))
+            C.ptr(self.total), C.ptr(self.keys), C.ptr(self.vals), C.ptr(self.status), C.ptr(fp), C.ptr(jb), s))
         R._call("rm_sort_pairs", lambda: L.rm_sort_pairs(C.ptr(self.keys), C.ptr(self.vals), self.capacity, C.ptr(self.total), v.end_bit,
                                 C.ptr(self.sorted_keys), C.ptr(self.sorted_ids), C.ptr(self.sort_ws),
                                 self.sort_ws.numel(), s))
@@ -234,7 +234,7 @@ class BatchedRasterizer:
                                  v.n_tiles, s))
         if self.fine_shift:
             R._call("rm_fine_lists", lambda: L.rm_fine_lists_multi(
-                C.ptr(self.sorted_ids), C.ptr(self.ranges), None if packed else C.ptr(self.box),
+                C.ptr(self.sorted_ids), C.ptr(self.ranges), None if packed else C.ptr(self.footprint),
                 None if packed else C.ptr(self.jitter_bounds), self.T, v.array, v.n,
                 self.fine_shift, self.fine_ids.shape[0], C.ptr(self.fine_ids), C.ptr(self.fine_ranges),
                 C.ptr(self.fine_total), C.ptr(self.fine_ws), self.fine_ws.numel(), s))

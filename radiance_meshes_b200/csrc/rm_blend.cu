@@ -251,7 +251,6 @@ struct HitMasks {
     uint32_t* words;  // nullptr: no masks
     int64_t cap;      // words
     const uint32_t* header;  // kMaskValid: this pass's forward wrote masks with 64-pixel items
-    __device__ __forceinline__ bool has(int64_t m) const { return words != nullptr && m < cap; }
 };
 
 constexpr uint32_t kMaskValid = 0x6d61736bu;

@@ -1,10 +1,10 @@
 // rm_fine.cu - tile lists on a finer grid, derived from the sorted lists.
 //
-// Given the sorted lists of the caller's tiles, each tet's image-space box
-// (rm_project_fwd_fine) and the bounds of the per-pixel ray jitter
-// (rm_jitter_bounds), the list of a fine tile (2^fine_shift times smaller) is
-// the subsequence of its coarse tile's list of the tets that can reach one of
-// its pixels' rays (box_meets_tile).  Emitting fine pairs and sorting them
+// Given the sorted lists of the caller's tiles, each tet's image footprint
+// (rm_project_fwd_fine: box and projected vertices) and the bounds of the
+// per-pixel ray jitter (rm_jitter_bounds), the list of a fine tile
+// (2^fine_shift times smaller) is the subsequence of its coarse tile's list of
+// the tets that can reach one of its pixels' rays (tet_meets_tile).  Emitting fine pairs and sorting them
 // again would reproduce exactly that order (depth key, then tet id), so
 // instead each coarse list is split once, in order, into its 4 (or 16, 64)
 // fine lists: a counting pass, a scan of the counts in fine-tile order, and a
@@ -74,10 +74,10 @@ __global__ void __launch_bounds__(32) jitter_final_kernel(const float4* __restri
 // the fine ranges.  FS = fine shift (2^FS x 2^FS fine tiles per tile).
 // Views: tile t of the coarse (global, view-major) numbering belongs to view
 // v = views.find(t); its fine tiles are numbered view-major too, view v's
-// starting at tiles[v] * f^2; box rows are stacked view-major ([v, T]).
+// starting at tiles[v] * f^2; footprint rows are stacked view-major ([v, T]).
 template <bool WRITE, bool PACKED, int FS>
 __global__ void __launch_bounds__(kFineThreads) fine_lists_kernel(
-    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ box,
+    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ footprint,
     const float4* __restrict__ jitter_bounds, int64_t n_tets, const __grid_constant__ ViewSet views,
     int32_t* __restrict__ counts, const int32_t* __restrict__ incl, int32_t* __restrict__ fine_ids,
     int64_t capacity, int2* __restrict__ fine_ranges, uint32_t* status) {
@@ -93,17 +93,11 @@ __global__ void __launch_bounds__(kFineThreads) fine_lists_kernel(
     const int tx = local % grid_w, ty = local / grid_w;
     const int fgw = grid_w * f;
     const int64_t fbase = (int64_t)views.tiles[v] * Q;
-    const float4* __restrict__ box_v = box + (int64_t)v * n_tets;
+    const float4* __restrict__ fp_v = footprint + (int64_t)v * n_tets * 3;
     const int ftw = views.cams[v].tile_width / f, fth = views.cams[v].tile_height / f;
     const int px0 = tx * views.cams[v].tile_width, py0 = ty * views.cams[v].tile_height;
     const float4 jb = PACKED ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(jitter_bounds);
     const int2 r = __ldg(ranges + t);
-    // entry e (tet box b, packed bits) reaches fine tile q
-    auto reaches = [&](int e, float4 b, uint32_t packed, int q) {
-        if (e >= r.y) return false;
-        if (PACKED) return ((packed >> q) & 1u) != 0;
-        return box_meets_tile(b, jb, px0 + q % f * ftw, py0 + q / f * fth, ftw, fth);
-    };
     auto fine_id = [&](int q) { return fbase + (int64_t)(ty * f + q / f) * fgw + tx * f + q % f; };
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -112,70 +106,68 @@ __global__ void __launch_bounds__(kFineThreads) fine_lists_kernel(
         if (WRITE) start[threadIdx.x] = __ldg(incl + fine_id(threadIdx.x)) - __ldg(counts + fine_id(threadIdx.x));
     }
     __syncthreads();
-    uint32_t c[WRITE ? 1 : Q];  // counting pass: this warp's counts (lane-uniform)
-    if (!WRITE) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) c[q] = 0u;
-    }
     for (int base = r.x; base < r.y; base += kFineThreads) {
         const int e = base + (int)threadIdx.x;
-        float4 b = {0.f, 0.f, 0.f, 0.f};
         int32_t g = 0;
-        uint32_t packed = 0;  // PACKED: the 2x2 coverage bits carried in the value's top bits
+        uint64_t bits = 0;  // bit q: the entry reaches fine tile q
         if (e < r.y) {
             g = __ldg(ids + e);
-            if (PACKED) {
-                packed = (uint32_t)g >> 28;
+            if (PACKED) {  // the 2x2 bits carried in the value's top bits
+                bits = (uint32_t)g >> 28;
                 g &= 0x0fffffff;
             } else {
-                b = __ldg(box_v + g);
+                const Footprint fp = {__ldg(fp_v + 3 * (int64_t)g), __ldg(fp_v + 3 * (int64_t)g + 1),
+                                      __ldg(fp_v + 3 * (int64_t)g + 2)};
+                const HullEdges he = hull_edges(fp, (float)px0, (float)py0);
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                    if (tet_meets_tile(fp, he, px0, py0, jb, px0 + q % f * ftw, py0 + q / f * fth, ftw, fth))
+                        bits |= 1ull << q;
             }
         }
-        if (!WRITE) {
+        if constexpr (!WRITE) {
 #pragma unroll
-            for (int q = 0; q < Q; ++q) c[q] += __popc(__ballot_sync(0xffffffffu, reaches(e, b, packed, q)));
-            continue;
-        }
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const unsigned bal = __ballot_sync(0xffffffffu, reaches(e, b, packed, q));
-            if (lane == 0) wcnt[warp][q] = __popc(bal);
-        }
-        __syncthreads();
-        if (warp == 0) {
-            // per fine tile: exclusive prefix over the warps, offset by the
-            // entries of the earlier chunks
             for (int q = 0; q < Q; ++q) {
-                const uint32_t x = wcnt[lane][q];
-                uint32_t inc = x;
+                const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
+                if (lane == 0 && bal) atomicAdd(&run[q], (uint32_t)__popc(bal));
+            }
+        } else {
 #pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, off);
-                    if (lane >= off) inc += y;
+            for (int q = 0; q < Q; ++q) {
+                const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
+                if (lane == 0) wcnt[warp][q] = __popc(bal);
+            }
+            __syncthreads();
+            if (warp == 0) {
+                // per fine tile: exclusive prefix over the warps, offset by the
+                // entries of the earlier chunks
+                for (int q = 0; q < Q; ++q) {
+                    const uint32_t x = wcnt[lane][q];
+                    uint32_t inc = x;
+#pragma unroll
+                    for (int off = 1; off < 32; off <<= 1) {
+                        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, off);
+                        if (lane >= off) inc += y;
+                    }
+                    const uint32_t r0 = run[q];
+                    wpre[lane][q] = r0 + inc - x;
+                    __syncwarp();
+                    if (lane == 31) run[q] = r0 + inc;
+                    __syncwarp();
                 }
-                const uint32_t r0 = run[q];
-                wpre[lane][q] = r0 + inc - x;
-                __syncwarp();
-                if (lane == 31) run[q] = r0 + inc;
-                __syncwarp();
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const bool in = (bits >> q) & 1u;
+                const unsigned bal = __ballot_sync(0xffffffffu, in);
+                if (in) {
+                    const int64_t o = (int64_t)start[q] + wpre[warp][q] + __popc(bal & lt);
+                    if (o < capacity) fine_ids[o] = g;
+                    else if (status) atomicOr(status, RM_STATUS_CAPACITY);
+                }
             }
         }
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const bool in = reaches(e, b, packed, q);
-            const unsigned bal = __ballot_sync(0xffffffffu, in);
-            if (in) {
-                const int64_t o = (int64_t)start[q] + wpre[warp][q] + __popc(bal & lt);
-                if (o < capacity) fine_ids[o] = g;
-                else if (status) atomicOr(status, RM_STATUS_CAPACITY);
-            }
-        }
-    }
-    if (!WRITE && lane == 0) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-            if (c[q]) atomicAdd(&run[q], c[q]);
     }
     __syncthreads();
     if (threadIdx.x < Q) {
@@ -222,7 +214,7 @@ int rm_jitter_bounds(const float* jitter, int64_t n_pixels, float* bounds, void*
 
 namespace {
 
-int fine_lists_impl(const char* who, const int32_t* sorted_ids, const int32_t* ranges, const float* box,
+int fine_lists_impl(const char* who, const int32_t* sorted_ids, const int32_t* ranges, const float* footprint,
                     const float* jitter_bounds, int64_t n_tets, const rm::ViewSet& views, int fine_shift,
                     int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges, int64_t* total_dev, void* workspace,
                     size_t workspace_bytes, void* stream) {
@@ -236,15 +228,15 @@ int fine_lists_impl(const char* who, const int32_t* sorted_ids, const int32_t* r
     const int64_t G = views.tiles[views.n];
     const int64_t Gf = G * f * f;
     if (Gf >= (int64_t)INT32_MAX) return rm_host::fail(RM_EINVAL, "%s: too many tiles", who);
-    // no box: the 2x2 coverage bits come packed in bits 28..31 of the ids
-    const bool packed = box == nullptr;
+    // no footprint: the 2x2 coverage bits come packed in bits 28..31 of the ids
+    const bool packed = footprint == nullptr;
     if (packed && fine_shift != 1) return rm_host::fail(RM_EINVAL, "%s: packed masks need fine_shift 1", who);
-    if (!packed && !jitter_bounds) return rm_host::fail(RM_EINVAL, "%s: box without jitter_bounds", who);
+    if (!packed && !jitter_bounds) return rm_host::fail(RM_EINVAL, "%s: footprint without jitter_bounds", who);
     if (!ranges || !fine_ranges || !total_dev || !workspace || (capacity > 0 && (!sorted_ids || !fine_ids)))
         return rm_host::fail(RM_EINVAL, "%s: NULL pointer", who);
-    if (((uintptr_t)box & 15) || ((uintptr_t)jitter_bounds & 15) || ((uintptr_t)ranges & 7) ||
+    if (((uintptr_t)footprint & 15) || ((uintptr_t)jitter_bounds & 15) || ((uintptr_t)ranges & 7) ||
         ((uintptr_t)fine_ranges & 7) || ((uintptr_t)workspace & 255))
-        return rm_host::fail(RM_EINVAL, "%s: misaligned box / jitter_bounds / ranges / workspace", who);
+        return rm_host::fail(RM_EINVAL, "%s: misaligned footprint / jitter_bounds / ranges / workspace", who);
     if (workspace_bytes < rm_fine_lists_workspace_size(Gf))
         return rm_host::fail(RM_EINVAL, "%s: workspace %zu < %zu bytes", who, workspace_bytes,
                              rm_fine_lists_workspace_size(Gf));
@@ -271,13 +263,13 @@ int fine_lists_impl(const char* who, const int32_t* sorted_ids, const int32_t* r
         count = rm::fine_lists_kernel<false, false, 3>;
         write = rm::fine_lists_kernel<true, false, 3>;
     }
-    count<<<(unsigned)G, rm::kFineThreads, 0, s>>>(sorted_ids, (const int2*)ranges, (const float4*)box,
+    count<<<(unsigned)G, rm::kFineThreads, 0, s>>>(sorted_ids, (const int2*)ranges, (const float4*)footprint,
                                                    (const float4*)jitter_bounds, n_tets, views, counts, nullptr,
                                                    nullptr, 0, nullptr, nullptr);
     int rc = rm_host::check_launch("rm_fine_lists (count)");
     if (rc) return rc;
     if ((rc = rm_scan_tiles(counts, Gf, incl, total_dev, scan_ws, rm_scan_workspace_size(Gf), stream))) return rc;
-    write<<<(unsigned)G, rm::kFineThreads, 0, s>>>(sorted_ids, (const int2*)ranges, (const float4*)box,
+    write<<<(unsigned)G, rm::kFineThreads, 0, s>>>(sorted_ids, (const int2*)ranges, (const float4*)footprint,
                                                    (const float4*)jitter_bounds, n_tets, views, counts, incl,
                                                    fine_ids, capacity, (int2*)fine_ranges, status);
     return rm_host::check_launch("rm_fine_lists (write)");
@@ -287,25 +279,26 @@ int fine_lists_impl(const char* who, const int32_t* sorted_ids, const int32_t* r
 
 extern "C" {
 
-int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges, const float* box, const float* jitter_bounds,
-                  const rm_camera* cam, int fine_shift, int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
-                  int64_t* total_dev, void* workspace, size_t workspace_bytes, void* stream) {
+int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges, const float* footprint,
+                  const float* jitter_bounds, const rm_camera* cam, int fine_shift, int64_t capacity,
+                  int32_t* fine_ids, int32_t* fine_ranges, int64_t* total_dev, void* workspace,
+                  size_t workspace_bytes, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_fine_lists", cam, 1, &views);
     if (rc) return rc;
-    if (!box) return rm_host::fail(RM_EINVAL, "rm_fine_lists: NULL box");
-    return fine_lists_impl("rm_fine_lists", sorted_ids, ranges, box, jitter_bounds, 0, views, fine_shift, capacity,
-                           fine_ids, fine_ranges, total_dev, workspace, workspace_bytes, stream);
+    if (!footprint) return rm_host::fail(RM_EINVAL, "rm_fine_lists: NULL footprint");
+    return fine_lists_impl("rm_fine_lists", sorted_ids, ranges, footprint, jitter_bounds, 0, views, fine_shift,
+                           capacity, fine_ids, fine_ranges, total_dev, workspace, workspace_bytes, stream);
 }
 
-int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges, const float* box,
+int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges, const float* footprint,
                         const float* jitter_bounds, int64_t n_tets, const rm_camera* cams, int n_views,
                         int fine_shift, int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
                         int64_t* total_dev, void* workspace, size_t workspace_bytes, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_fine_lists_multi", cams, n_views, &views);
     if (rc) return rc;
-    return fine_lists_impl("rm_fine_lists_multi", sorted_ids, ranges, box, jitter_bounds, n_tets, views, fine_shift,
+    return fine_lists_impl("rm_fine_lists_multi", sorted_ids, ranges, footprint, jitter_bounds, n_tets, views, fine_shift,
                            capacity, fine_ids, fine_ranges, total_dev, workspace, workspace_bytes, stream);
 }
 

@@ -251,14 +251,14 @@ __device__ __forceinline__ bool outside_view(const rm_camera& c, const TetGeom& 
 // Per-view part of vertex_shader (vertex_shader.slang:36-89): camera space,
 // find_extent, the depth key and the tile rectangle.  Returns the tile count
 // (0: culled, r and depth zero).
-// BOX: also return the image-space bounding box (pixels: min x, min y, max x,
-// max y; zeros when culled) from which the lists of smaller tiles are cut.
+// BOX: also return the tet's image footprint (box and projected vertices,
+// Footprint; zeros when culled) from which the lists of smaller tiles are cut.
 template <bool GENERAL, bool BOX = false>
 __device__ __forceinline__ int project_view(const rm_camera& cam, const TetGeom& t, int4& r, float& depth_out,
-                                            float4* box_out = nullptr) {
+                                            Footprint* fp = nullptr) {
     r = {0, 0, 0, 0};
     depth_out = 0.f;
-    if (BOX) *box_out = {0.f, 0.f, 0.f, 0.f};
+    if (BOX) *fp = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
     if (t.planar || outside_view(cam, t)) return 0;
     const f3 cs0 = point2cam(cam, t.v[0]), cs1 = point2cam(cam, t.v[1]);
     const f3 cs2 = point2cam(cam, t.v[2]), cs3 = point2cam(cam, t.v[3]);
@@ -285,7 +285,23 @@ __device__ __forceinline__ int project_view(const rm_camera& cam, const TetGeom&
         return 0;
     }
     depth_out = fminf(fmaxf(depth, -1e20f), 1e20f);
-    if (BOX) *box_out = {box.mn.x, box.mn.y, box.mx.x, box.mx.y};
+    if (BOX) {
+        fp->box = {box.mn.x, box.mn.y, box.mx.x, box.mx.y};
+        // the projected vertices (camspace_to_image as in bbox_add) when no
+        // vertex is clipped and the camera is a plain pinhole
+        const f3 cs[4] = {cs0, cs1, cs2, cs3};
+        float q[8];
+        bool ok = !GENERAL;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            q[2 * i] = fmaf(cs[i].x / cs[i].z, cam.K[0], cam.K[2]);
+            q[2 * i + 1] = fmaf(cs[i].y / cs[i].z, cam.K[4], cam.K[5]);
+            ok &= cs[i].z > 1e-4f && fabsf(q[2 * i]) <= kHullRange && fabsf(q[2 * i + 1]) <= kHullRange;
+        }
+        const float nan = __int_as_float(0x7fc00000);
+        fp->p01 = ok ? make_float4(q[0], q[1], q[2], q[3]) : make_float4(nan, nan, nan, nan);
+        fp->p23 = ok ? make_float4(q[4], q[5], q[6], q[7]) : make_float4(nan, nan, nan, nan);
+    }
     return n_tiles;
 }
 
@@ -317,14 +333,14 @@ __global__ void __launch_bounds__(256) project_fwd_fine_kernel(const int4* __res
                                                                const float* __restrict__ verts, int64_t n_tets,
                                                                const rm_camera cam, int32_t* __restrict__ tiles,
                                                                int4* __restrict__ rect, float* __restrict__ vs,
-                                                               float* __restrict__ cc, float4* __restrict__ box) {
+                                                               float* __restrict__ cc, float4* __restrict__ fp) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_tets) return;
     const TetGeom t = tet_geom(indices, verts, g);
     int4 r;
-    float4 b;
+    Footprint f;
     float depth;
-    const int n_tiles = project_view<GENERAL, true>(cam, t, r, depth, &b);
+    const int n_tiles = project_view<GENERAL, true>(cam, t, r, depth, &f);
     tiles[g] = n_tiles;
     rect[g] = r;
     vs[3 * g + 0] = 0.f;
@@ -333,7 +349,9 @@ __global__ void __launch_bounds__(256) project_fwd_fine_kernel(const int4* __res
     cc[3 * g + 0] = n_tiles ? (float)t.center.x : 0.f;
     cc[3 * g + 1] = n_tiles ? (float)t.center.y : 0.f;
     cc[3 * g + 2] = n_tiles ? (float)t.center.z : 0.f;
-    box[g] = b;
+    fp[3 * g] = f.box;
+    fp[3 * g + 1] = f.p01;
+    fp[3 * g + 2] = f.p23;
 }
 
 // All views of a batch: each thread loads its tet once and projects it into
@@ -344,20 +362,22 @@ __global__ void __launch_bounds__(256) project_fwd_multi_kernel(const int4* __re
                                                                 const __grid_constant__ ViewSet views,
                                                                 int32_t* __restrict__ tiles, int4* __restrict__ rect,
                                                                 float* __restrict__ depth, int32_t* __restrict__ any,
-                                                                float* __restrict__ cc, float4* __restrict__ box) {
+                                                                float* __restrict__ cc, float4* __restrict__ fp) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_tets) return;
     const TetGeom t = tet_geom(indices, verts, g);
     int total = 0;
     for (int v = 0; v < views.n; ++v) {
         int4 r;
-        float4 b;
+        Footprint f;
         float dk;
         const int64_t o = (int64_t)v * n_tets + g;
         int n_tiles;
-        if (box) {
-            n_tiles = project_view<GENERAL, true>(views.cams[v], t, r, dk, &b);
-            box[o] = b;
+        if (fp) {
+            n_tiles = project_view<GENERAL, true>(views.cams[v], t, r, dk, &f);
+            fp[3 * o] = f.box;
+            fp[3 * o + 1] = f.p01;
+            fp[3 * o + 2] = f.p23;
         } else {
             n_tiles = project_view<GENERAL>(views.cams[v], t, r, dk);
         }
@@ -485,27 +505,28 @@ int rm_project_fwd(const int32_t* indices, const float* vertices, int64_t n_tets
 
 int rm_project_fwd_fine(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,
                         const rm_camera* cam, int32_t* tiles_touched, int32_t* rect, float* vs, float* circumcenter,
-                        float* box, void* stream) {
+                        float* footprint, void* stream) {
     int rc = rm_host::check_cam(cam);
     if (rc) return rc;
     if (n_tets < 0 || n_verts < 0) return rm_host::fail(RM_EINVAL, "rm_project_fwd_fine: negative size");
     if (n_tets == 0) return RM_OK;
-    if (!indices || !vertices || !tiles_touched || !rect || !vs || !circumcenter || !box)
+    if (!indices || !vertices || !tiles_touched || !rect || !vs || !circumcenter || !footprint)
         return rm_host::fail(RM_EINVAL, "rm_project_fwd_fine: NULL pointer");
-    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15) || ((uintptr_t)box & 15))
-        return rm_host::fail(RM_EINVAL, "rm_project_fwd_fine: indices, rect and box must be 16-byte aligned");
+    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15) || ((uintptr_t)footprint & 15))
+        return rm_host::fail(RM_EINVAL, "rm_project_fwd_fine: indices, rect and footprint must be 16-byte aligned");
     const int threads = 256;
     const int64_t blocks = (n_tets + threads - 1) / threads;
     auto kernel =
         rm_host::cam_general(*cam) ? rm::project_fwd_fine_kernel<true> : rm::project_fwd_fine_kernel<false>;
     kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
-        (const int4*)indices, vertices, n_tets, *cam, tiles_touched, (int4*)rect, vs, circumcenter, (float4*)box);
+        (const int4*)indices, vertices, n_tets, *cam, tiles_touched, (int4*)rect, vs, circumcenter,
+        (float4*)footprint);
     return rm_host::check_launch("rm_project_fwd_fine");
 }
 
 int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,
                          const rm_camera* cams, int n_views, int32_t* tiles_touched, int32_t* rect, float* depth,
-                         int32_t* tiles_any, float* circumcenter, float* box, void* stream) {
+                         int32_t* tiles_any, float* circumcenter, float* footprint, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_project_fwd_multi", cams, n_views, &views);
     if (rc) return rc;
@@ -513,8 +534,8 @@ int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t 
     if (n_tets == 0) return RM_OK;
     if (!indices || !vertices || !tiles_touched || !rect || !depth)
         return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: NULL pointer");
-    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15) || ((uintptr_t)box & 15))
-        return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: indices, rect and box must be 16-byte aligned");
+    if (((uintptr_t)indices & 15) || ((uintptr_t)rect & 15) || ((uintptr_t)footprint & 15))
+        return rm_host::fail(RM_EINVAL, "rm_project_fwd_multi: indices, rect and footprint must be 16-byte aligned");
     const int threads = 256;
     const int64_t blocks = (n_tets + threads - 1) / threads;
     bool general = false;
@@ -522,7 +543,7 @@ int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t 
     auto kernel = general ? rm::project_fwd_multi_kernel<true> : rm::project_fwd_multi_kernel<false>;
     kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
         (const int4*)indices, vertices, n_tets, views, tiles_touched, (int4*)rect, depth, tiles_any, circumcenter,
-        (float4*)box);
+        (float4*)footprint);
     return rm_host::check_launch("rm_project_fwd_multi");
 }
 

@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(256) emit_multi_kernel(const float* __restrict
                                                          const __grid_constant__ ViewSet views, int64_t capacity,
                                                          const int64_t* __restrict__ total_dev,
                                                          int64_t* __restrict__ keys, int32_t* __restrict__ vals,
-                                                         uint32_t* status, const float4* __restrict__ box,
+                                                         uint32_t* status, const float4* __restrict__ footprint,
                                                          const float4* __restrict__ jitter_bounds) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0 && total_dev && status && *total_dev > capacity) atomicOr(status, RM_STATUS_CAPACITY);
@@ -183,20 +183,27 @@ __global__ void __launch_bounds__(256) emit_multi_kernel(const float* __restrict
     const uint32_t tile0 = (uint32_t)views.tiles[v];
     int64_t off = i == 0 ? 0 : (int64_t)__ldg(offsets + i - 1);
     const uint64_t fk = sortable_key(__ldg(depth + i));
-    // with box: bits 28..31 of the value say which of the tile's 2x2 half-size
-    // tiles the tet can reach (bit qy * 2 + qx, box_meets_tile)
-    const float4 bx = box ? __ldg(box + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 jb = box ? __ldg(jitter_bounds) : make_float4(0.f, 0.f, 0.f, 0.f);
+    // with footprint: bits 28..31 of the value say which of the tile's 2x2
+    // half-size tiles the tet can reach (bit qy * 2 + qx, tet_meets_tile)
     const int tw = views.cams[v].tile_width, th = views.cams[v].tile_height;
     const int hw = tw >> 1, hh = th >> 1;
+    Footprint fp = {};
+    HullEdges he = {};
+    float4 jb = {0.f, 0.f, 0.f, 0.f};
+    if (footprint) {
+        fp = {__ldg(footprint + 3 * i), __ldg(footprint + 3 * i + 1), __ldg(footprint + 3 * i + 2)};
+        he = hull_edges(fp, (float)(r.x * tw), (float)(r.y * th));
+        jb = __ldg(jitter_bounds);
+    }
     for (int32_t y = r.y; y < r.w; ++y) {
         for (int32_t x = r.x; x < r.z; ++x) {
             if (off < capacity) {
                 uint32_t q = 0;
-                if (box) {
+                if (footprint) {
 #pragma unroll
                     for (int b = 0; b < 4; ++b)
-                        if (box_meets_tile(bx, jb, x * tw + (b & 1) * hw, y * th + (b >> 1) * hh, hw, hh))
+                        if (tet_meets_tile(fp, he, r.x * tw, r.y * th, jb, x * tw + (b & 1) * hw,
+                                           y * th + (b >> 1) * hh, hw, hh))
                             q |= 1u << b;
                 }
                 keys[off] = (int64_t)(((uint64_t)(tile0 + (uint32_t)(y * grid_w + x)) << 32) | fk);
@@ -278,7 +285,7 @@ int rm_emit_pairs(const float* vs, const int32_t* rect, const int32_t* offsets, 
 
 int rm_emit_pairs_multi(const float* depth, const int32_t* rect, const int32_t* offsets, int64_t n_tets,
                         const rm_camera* cams, int n_views, int64_t capacity, const int64_t* total_dev,
-                        int64_t* keys, int32_t* values, uint32_t* status_dev, const float* box_2x,
+                        int64_t* keys, int32_t* values, uint32_t* status_dev, const float* footprint_2x,
                         const float* jitter_bounds, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_emit_pairs_multi", cams, n_views, &views);
@@ -287,12 +294,13 @@ int rm_emit_pairs_multi(const float* depth, const int32_t* rect, const int32_t* 
     if (n_tets == 0) return RM_OK;
     if (!depth || !rect || !offsets || (capacity > 0 && (!keys || !values)))
         return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: NULL pointer");
-    if (((uintptr_t)rect & 15) || ((uintptr_t)box_2x & 15) || ((uintptr_t)jitter_bounds & 15))
-        return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: rect, box and jitter_bounds must be 16-byte aligned");
-    if (box_2x && !jitter_bounds) return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: box without jitter_bounds");
-    if (box_2x && n_tets >= (1ll << 28))
+    if (((uintptr_t)rect & 15) || ((uintptr_t)footprint_2x & 15) || ((uintptr_t)jitter_bounds & 15))
+        return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: rect, footprint, jitter_bounds not 16-byte aligned");
+    if (footprint_2x && !jitter_bounds)
+        return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: footprint without jitter_bounds");
+    if (footprint_2x && n_tets >= (1ll << 28))
         return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: packed fine masks need fewer than 2^28 tets");
-    if (box_2x)
+    if (footprint_2x)
         for (int v = 0; v < n_views; ++v)
             if ((cams[v].tile_width & 1) || (cams[v].tile_height & 1))
                 return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: packed fine masks need even tile sizes");
@@ -301,7 +309,7 @@ int rm_emit_pairs_multi(const float* depth, const int32_t* rect, const int32_t* 
     const int64_t blocks = (n + threads - 1) / threads;
     rm::emit_multi_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
         depth, (const int4*)rect, offsets, n_tets, views, capacity, total_dev, keys, values, status_dev,
-        (const float4*)box_2x, (const float4*)jitter_bounds);
+        (const float4*)footprint_2x, (const float4*)jitter_bounds);
     return rm_host::check_launch("rm_emit_pairs_multi");
 }
 

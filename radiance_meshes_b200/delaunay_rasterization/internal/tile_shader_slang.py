@@ -25,7 +25,7 @@ def vertex_and_tile_shader(indices, vertices, cam, render_grid):
     the reference (tile_shader_slang.py:24-72).
 
     For tiles of 16x16 pixels or more, what it takes to cut the lists of the
-    same frame on the grid of 8x8-pixel tiles (the tets' image boxes) is
+    same frame on the grid of 8x8-pixel tiles (the tets' image footprints) is
     attached to the returned ``sorted_tetra_idx`` (attribute ``rm_fine``);
     ``AlphaBlendTiledRender`` cuts them for its ray jitter and blends over
     them when it is handed that tensor, which gives the same image with fewer
@@ -35,14 +35,14 @@ def vertex_and_tile_shader(indices, vertices, cam, render_grid):
     pre = None
     if fs:
         with torch.no_grad():
-            tiles, rect, vs, cc, box = R.project_fwd_fine(indices, vertices, camst)
+            tiles, rect, vs, cc, footprint = R.project_fwd_fine(indices, vertices, camst)
         pre = (tiles, rect, vs, cc)
     tiles_touched, rect_tile_space, vs_tetra, circumcenter = VertexShader.apply(
         indices, vertices, cam, render_grid, "cuda", pre)
     with torch.no_grad():
         lists = R.build_tile_lists(tiles_touched, rect_tile_space, vs_tetra, camst)
         if fs:
-            R.attach_fine_lists(lists.sorted_ids, lists.ranges, camst, fs, box)
+            R.attach_fine_lists(lists.sorted_ids, lists.ranges, camst, fs, footprint)
     mask = tiles_touched > 0
     return lists.sorted_ids, lists.ranges, vs_tetra, circumcenter, mask, rect_tile_space
 

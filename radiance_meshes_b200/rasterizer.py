@@ -182,8 +182,8 @@ def fine_camera(cam: RMCamera, fine_shift: int) -> RMCamera:
 
 
 def project_fwd_fine(indices: torch.Tensor, vertices: torch.Tensor, cam: RMCamera):
-    """project_fwd plus each tet's image-space bounding box [T,4] (min x, min y,
-    max x, max y in pixels; rm_project_fwd_fine), from which the lists of
+    """project_fwd plus each tet's image footprint [T,12] (box, then the four
+    projected vertices or NaN; rm_project_fwd_fine), from which the lists of
     smaller tiles are cut."""
     _require_cuda(indices=indices, vertices=vertices)
     indices = _i32(indices)
@@ -194,11 +194,11 @@ def project_fwd_fine(indices: torch.Tensor, vertices: torch.Tensor, cam: RMCamer
     rect = torch.empty((T, 4), dtype=torch.int32, device=dev)
     vs = torch.empty((T, 3), dtype=torch.float32, device=dev)
     cc = torch.empty((T, 3), dtype=torch.float32, device=dev)
-    box = torch.empty((T, 4), dtype=torch.float32, device=dev)
+    footprint = torch.empty((T, 12), dtype=torch.float32, device=dev)
     _call("rm_project_fwd", lambda: C.lib().rm_project_fwd_fine(
         C.ptr(indices), C.ptr(vertices), T, vertices.shape[0], ctypes.byref(cam), C.ptr(tiles), C.ptr(rect),
-        C.ptr(vs), C.ptr(cc), C.ptr(box), _stream()))
-    return tiles, rect, vs, cc, box
+        C.ptr(vs), C.ptr(cc), C.ptr(footprint), _stream()))
+    return tiles, rect, vs, cc, footprint
 
 
 def jitter_bounds(ray_jitter: torch.Tensor, pool: ScratchPool | None = None) -> torch.Tensor:
@@ -291,13 +291,13 @@ class FineLists:
 @dataclass
 class PendingFineLists:
     """What the projection leaves on the sorted coarse ids: the coarse ranges,
-    the tets' image boxes and the split factor.  The split itself needs the
+    the tets' image footprints and the split factor.  The split itself needs the
     ray jitter of the blend, so it runs in fine_lists_of (once per jitter)."""
     shift: int
     coarse_cam: RMCamera
     coarse_key: tuple
     ranges: torch.Tensor
-    box: torch.Tensor
+    footprint: torch.Tensor
     jitter: torch.Tensor | None = None  # the jitter of `lists` (kept alive so identity stays meaningful)
     jitter_version: int = -1
     lists: FineLists | None = None
@@ -321,16 +321,16 @@ def _cam_key(cam: RMCamera) -> tuple:
 
 
 def attach_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCamera, fine_shift: int,
-                      box: torch.Tensor) -> PendingFineLists:
+                      footprint: torch.Tensor) -> PendingFineLists:
     """Record on ``sorted_ids`` (attribute ``rm_fine``) what fine_lists_of needs
     to cut the 2^fine_shift times smaller tiles' lists from these lists."""
-    pend = PendingFineLists(fine_shift, cam, _cam_key(cam), ranges, box)
+    pend = PendingFineLists(fine_shift, cam, _cam_key(cam), ranges, footprint)
     sorted_ids.rm_fine = pend
     return pend
 
 
 def split_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCamera, fine_shift: int,
-                     box: torch.Tensor, bounds: torch.Tensor, pool: ScratchPool | None = None) -> FineLists:
+                     footprint: torch.Tensor, bounds: torch.Tensor, pool: ScratchPool | None = None) -> FineLists:
     """Split the sorted coarse lists into the fine lists for the jitter bounds
     ``bounds`` (rm_fine_lists, no host synchronisation)."""
     pool = pool or _POOL
@@ -344,7 +344,7 @@ def split_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCame
     L = C.lib()
     ws_n = L.rm_fine_lists_workspace_size(Gf)
     ws = pool.get("fine", ws_n, dev)
-    _call("rm_fine_lists", lambda: L.rm_fine_lists(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(box), C.ptr(bounds),
+    _call("rm_fine_lists", lambda: L.rm_fine_lists(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(footprint), C.ptr(bounds),
                                                    ctypes.byref(cam), fine_shift, cap, C.ptr(fine_ids),
                                                    C.ptr(fine_ranges), C.ptr(total), C.ptr(ws), ws_n, _stream()))
     return FineLists(fine_shift, camf, _cam_key(cam), fine_ids, fine_ranges, total)
@@ -360,7 +360,7 @@ def fine_lists_of(sorted_ids: torch.Tensor, cam: RMCamera, ray_jitter: torch.Ten
     if pend.lists is not None and pend.jitter is ray_jitter and pend.jitter_version == ray_jitter._version:
         return pend.lists
     bounds = jitter_bounds(ray_jitter)
-    pend.lists = split_fine_lists(sorted_ids, pend.ranges, pend.coarse_cam, pend.shift, pend.box, bounds)
+    pend.lists = split_fine_lists(sorted_ids, pend.ranges, pend.coarse_cam, pend.shift, pend.footprint, bounds)
     pend.jitter, pend.jitter_version = ray_jitter, ray_jitter._version
     return pend.lists
 

@@ -46,40 +46,60 @@ def test_integer_stages_plain_forward_workload(cuda, plain_forward_oracle, tile)
     assert np.array_equal(L.ranges.cpu().numpy(), lists["ranges"])
 
 
-def _fine_rects(box, rect, jb, tile, f, gw, gh):
-    """Rectangles on the fine grid of the fine tiles whose pixel rays a tet can
-    reach: the fine tiles of the tet's coarse rectangle passing the test of
-    rm_fine_lists (box grown by 1/64 pixel against the jittered footprint),
-    restated in float32 (the set is an interval in each axis)."""
-    w = tile // f
-    m = np.float32(1.0 / 64.0)
-    b = box.astype(np.float32)
+def _fine_bits(fp, jb, ox, oy, tw, th, f):
+    """Bit q of entry i: the tet with footprint fp[i] can reach fine tile q of
+    the coarse tile with pixel origin (ox[i], oy[i]) under the jitter bounds
+    jb -- the test of rm_fine_lists (box grown by 1/64 pixel, then the edges of
+    the projected vertices' hull with 1/16 pixel), restated in float32 with
+    the kernel's operation order."""
+    f32 = np.float32
+    m, hm = f32(1.0 / 64.0), f32(1.0 / 16.0)
+    fp = fp.astype(np.float32)
     jb = jb.astype(np.float32)
-    out = np.zeros_like(rect)
-
-    def axis(lo_b, hi_b, r0, r1, jmin, jmax, n):
-        lo = np.full(len(b), n, np.int64)
-        hi = np.full(len(b), -1, np.int64)
-        for t in range(n):
-            ok = (lo_b - m <= np.float32(t * w + w - 1) + jmax) & (hi_b + m >= np.float32(t * w) + jmin)
-            ok &= (r0 * f <= t) & (t < r1 * f)
-            lo = np.where(ok & (t < lo), t, lo)
-            hi = np.where(ok, t, hi)
-        return lo, hi + 1
-
-    x0, x1 = axis(b[:, 0], b[:, 2], rect[:, 0], rect[:, 2], jb[0], jb[2], gw * f)
-    y0, y1 = axis(b[:, 1], b[:, 3], rect[:, 1], rect[:, 3], jb[1], jb[3], gh * f)
-    ok = (x1 > x0) & (y1 > y0)
-    out[:, 0], out[:, 1], out[:, 2], out[:, 3] = x0, y0, x1, y1
-    out[~ok] = 0
-    return out
+    box = fp[:, 0:4]
+    oxf, oyf = ox.astype(np.float32), oy.astype(np.float32)
+    px = np.stack([fp[:, 4], fp[:, 6], fp[:, 8], fp[:, 10]], 1) - oxf[:, None]
+    py = np.stack([fp[:, 5], fp[:, 7], fp[:, 9], fp[:, 11]], 1) - oyf[:, None]
+    valid = ~np.isnan(fp[:, 4])
+    edges = []
+    z = f32(0)
+    with np.errstate(invalid="ignore", over="ignore"):
+        for a, b, o1, o2 in ((0, 1, 2, 3), (0, 2, 1, 3), (0, 3, 1, 2), (1, 2, 0, 3), (1, 3, 0, 2), (2, 3, 0, 1)):
+            nx = py[:, b] - py[:, a]
+            ny = px[:, a] - px[:, b]
+            ca = nx * px[:, a] + ny * py[:, a]
+            s1 = nx * px[:, o1] + ny * py[:, o1] - ca
+            s2 = nx * px[:, o2] + ny * py[:, o2] - ca
+            pos = (s1 <= 0) & (s2 <= 0)
+            neg = ~pos & (s1 >= 0) & (s2 >= 0)
+            sg = np.where(pos, f32(1), np.where(neg, f32(-1), f32(0))).astype(np.float32)
+            edges.append((np.where(valid, sg * nx, z), np.where(valid, sg * ny, z), np.where(valid, sg * ca, z)))
+        w, h = tw // f, th // f
+        bits = np.zeros(len(fp), np.int64)
+        for q in range(f * f):
+            dx, dy = q % f * w, q // f * h
+            x0, y0 = ox + dx, oy + dy
+            ok = (box[:, 0] - m <= (x0 + w - 1).astype(np.float32) + jb[2]) & \
+                 (box[:, 2] + m >= x0.astype(np.float32) + jb[0])
+            ok &= (box[:, 1] - m <= (y0 + h - 1).astype(np.float32) + jb[3]) & \
+                  (box[:, 3] + m >= y0.astype(np.float32) + jb[1])
+            xlo, xhi = f32(dx) + jb[0], f32(dx + w - 1) + jb[2]
+            ylo, yhi = f32(dy) + jb[1], f32(dy + h - 1) + jb[3]
+            sep = np.zeros(len(fp), bool)
+            for nx, ny, c in edges:
+                d = (nx * np.where(nx > 0, xlo, xhi).astype(np.float32)
+                     + ny * np.where(ny > 0, ylo, yhi).astype(np.float32)) - c
+                sep |= d > hm * (np.abs(nx) + np.abs(ny))
+            bits |= (ok & ~sep).astype(np.int64) << q
+    return bits
 
 
 @pytest.mark.parametrize("tile,jit", [(16, "unit"), (32, "unit"), (16, "half"), (16, "wide")])
-def test_fine_lists_split_equals_fine_sort(cuda, tile, jit):
-    """Splitting the sorted coarse lists (rm_fine_lists) gives exactly the
-    lists that emitting and sorting the pairs of the fine tiles each tet can
-    reach gives."""
+def test_fine_lists_split_matches_restatement(cuda, tile, jit):
+    """Splitting the sorted coarse lists (rm_fine_lists) keeps, for every fine
+    tile, exactly the coarse entries that reach it (float32 restatement of the
+    footprint test), in the coarse order, with the fine ranges of that
+    order; the projection with footprints equals the plain projection."""
     import torch
 
     from radiance_meshes_b200 import rasterizer as R
@@ -90,11 +110,15 @@ def test_fine_lists_split_equals_fine_sort(cuda, tile, jit):
     cam = tcam_to_struct(view.tcam())
     fs = R.fine_shift_for(cam)
     assert fs == (1 if tile == 16 else 2)
+    f = 1 << fs
     i = torch.from_numpy(mesh.indices).cuda()
     v = torch.from_numpy(mesh.vertices).cuda()
-    tiles, rect, vs, cc, box = R.project_fwd_fine(i, v, cam)
+    tiles, rect, vs, cc, fp = R.project_fwd_fine(i, v, cam)
     t0, r0, vs0, cc0 = R.project_fwd(i, v, cam)
     assert torch.equal(tiles, t0) and torch.equal(rect, r0) and torch.equal(vs, vs0) and torch.equal(cc, cc0)
+    fpn = fp.cpu().numpy()
+    vis = tiles.cpu().numpy() > 0
+    assert (~np.isnan(fpn[vis, 4])).mean() > 0.9  # most visible tets carry their projected vertices
     rng = np.random.default_rng(7)
     shape = (view.height, view.width, 2)
     j = {"unit": rng.uniform(0, 1, shape), "half": np.full(shape, 0.5), "wide": rng.uniform(-1.5, 2.5, shape)}[jit]
@@ -104,18 +128,34 @@ def test_fine_lists_split_equals_fine_sort(cuda, tile, jit):
     assert np.array_equal(jb.cpu().numpy(), np.array([jj[:, 0].min(), jj[:, 1].min(), jj[:, 0].max(),
                                                       jj[:, 1].max()], np.float32))
     coarse = R.build_tile_lists(tiles, rect, vs, cam)
-    fine = R.split_fine_lists(coarse.sorted_ids, coarse.ranges, cam, fs, box, jb)
-    rf_np = _fine_rects(box.cpu().numpy(), rect.cpu().numpy(), jb.cpu().numpy(), tile, 1 << fs, cam.grid_width,
-                        cam.grid_height)
-    rf = torch.from_numpy(rf_np).cuda()
-    tf = ((rf[:, 2] - rf[:, 0]) * (rf[:, 3] - rf[:, 1])).to(torch.int32).contiguous()
-    assert bool(((tf > 0) <= (tiles > 0)).all())
-    ref = R.build_tile_lists(tf, rf, vs, R.fine_camera(cam, fs))
+    fine = R.split_fine_lists(coarse.sorted_ids, coarse.ranges, cam, fs, fp, jb)
+    # restatement: entry e of coarse tile t goes to fine tile q when bit q is set
+    ids = coarse.sorted_ids.cpu().numpy()
+    rg = coarse.ranges.cpu().numpy()
+    G = cam.grid_width * cam.grid_height
+    t_of = np.repeat(np.arange(G), rg[:, 1] - rg[:, 0])
+    assert len(t_of) == len(ids)
+    tx, ty = t_of % cam.grid_width, t_of // cam.grid_width
+    jbn = jb.cpu().numpy()
+    bits = _fine_bits(fpn[ids], jbn, tx * tile, ty * tile, tile, tile, f)
+    fgw = cam.grid_width * f
+    e_all, q_all = np.nonzero((bits[:, None] >> np.arange(f * f)[None, :]) & 1)
+    fid = (ty[e_all] * f + q_all // f) * fgw + tx[e_all] * f + q_all % f
+    order = np.argsort(fid, kind="stable")
+    ref_ids = ids[e_all[order]]
+    ref_len = np.bincount(fid, minlength=G * f * f)
     n = fine.n_pairs
-    assert n == ref.n_pairs == int(tf.sum())
-    assert torch.equal(fine.sorted_ids[:n], ref.sorted_ids)
-    lf = fine.ranges[:, 1] - fine.ranges[:, 0]
-    lr = ref.ranges[:, 1] - ref.ranges[:, 0]
-    assert torch.equal(lf, lr)
-    ne = lr > 0
-    assert torch.equal(fine.ranges[ne], ref.ranges[ne])
+    assert n == len(ref_ids)
+    assert np.array_equal(fine.sorted_ids[:n].cpu().numpy(), ref_ids)
+    fr = fine.ranges.cpu().numpy()
+    assert np.array_equal(fr[:, 1] - fr[:, 0], ref_len)
+    start = np.concatenate([[0], np.cumsum(ref_len)[:-1]])
+    ne = ref_len > 0
+    assert np.array_equal(fr[ne, 0], start[ne])
+    # the hull edges remove entries that the box alone keeps
+    fp_box = fpn[ids].copy()
+    fp_box[:, 4:] = np.nan
+    box_bits = _fine_bits(fp_box, jbn, tx * tile, ty * tile, tile, tile, f)
+    assert not np.any(bits & ~box_bits)
+    n_box = int(((box_bits[:, None] >> np.arange(f * f)[None, :]) & 1).sum())
+    assert n < 0.9 * n_box
