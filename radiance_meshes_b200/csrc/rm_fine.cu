@@ -4,13 +4,14 @@
 // (rm_project_fwd_fine: box and projected vertices) and the bounds of the
 // per-pixel ray jitter (rm_jitter_bounds), the list of a fine tile
 // (2^fine_shift times smaller) is the subsequence of its coarse tile's list of
-// the tets that can reach one of its pixels' rays (tet_meets_tile).  Emitting fine pairs and sorting them
-// again would reproduce exactly that order (depth key, then tet id), so
-// instead each coarse list is split once, in order, into its 4 (or 16, 64)
-// fine lists: a counting pass, a scan of the counts in fine-tile order, and a
-// writing pass.  One CTA walks one coarse list in chunks of 1024 entries; the
-// ranks inside a chunk come from warp ballots per fine tile.  No reference
-// counterpart (the reference blends over the coarse lists directly).
+// the tets that can reach one of its pixels' rays (footprint_bits).  Emitting
+// fine pairs and sorting them again would reproduce exactly that order (depth
+// key, then tet id), so instead each coarse list is split once, in order, into
+// its 4 (or 16, 64) fine lists: a counting pass, a scan of the counts in
+// fine-tile order, and a writing pass.  One CTA walks one coarse list in
+// chunks of 1024 entries; the ranks inside a chunk come from warp ballots per
+// fine tile.  No reference counterpart (the reference blends over the coarse
+// lists directly).
 #include <algorithm>
 
 #include "rm_internal.cuh"
@@ -76,7 +77,7 @@ __global__ void __launch_bounds__(32) jitter_final_kernel(const float4* __restri
 // v = views.find(t); its fine tiles are numbered view-major too, view v's
 // starting at tiles[v] * f^2; footprint rows are stacked view-major ([v, T]).
 template <bool WRITE, bool PACKED, int FS>
-__global__ void __launch_bounds__(kFineThreads) fine_lists_kernel(
+__global__ void __launch_bounds__(kFineThreads, 2) fine_lists_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ footprint,
     const float4* __restrict__ jitter_bounds, int64_t n_tets, const __grid_constant__ ViewSet views,
     int32_t* __restrict__ counts, const int32_t* __restrict__ incl, int32_t* __restrict__ fine_ids,
@@ -118,11 +119,7 @@ __global__ void __launch_bounds__(kFineThreads) fine_lists_kernel(
             } else {
                 const Footprint fp = {__ldg(fp_v + 3 * (int64_t)g), __ldg(fp_v + 3 * (int64_t)g + 1),
                                       __ldg(fp_v + 3 * (int64_t)g + 2)};
-                const HullEdges he = hull_edges(fp, (float)px0, (float)py0);
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                    if (tet_meets_tile(fp, he, px0, py0, jb, px0 + q % f * ftw, py0 + q / f * fth, ftw, fth))
-                        bits |= 1ull << q;
+                bits = footprint_bits<f>(fp, jb, px0, py0, ftw, fth);
             }
         }
         if constexpr (!WRITE) {

@@ -210,22 +210,26 @@ struct Footprint {
 constexpr float kHullMargin = 1.0f / 16.0f;
 constexpr float kHullRange = 8192.0f;
 
-// Outward edge lines of the hull, relative to the origin (ox, oy): a point p
-// is outside edge k when nx[k] * px + ny[k] * py - c[k] > 0.  Candidate edges
-// are the 6 vertex pairs; a pair is a hull edge when the other two points lie
-// on one side of its line (rounding can only misjudge points within rounding
-// distance of the line, far inside the margin).  Other pairs, and all pairs
-// without valid points, get a zero line that separates nothing.  Plain float
-// operations in this order (no fused multiply-add).
-struct HullEdges {
-    float nx[6], ny[6], c[6];
-};
-
-__device__ __forceinline__ HullEdges hull_edges(const Footprint& f, float ox, float oy) {
-    HullEdges e;
-    const bool valid = !isnan(f.p01.x);
-    const float px[4] = {f.p01.x - ox, f.p01.z - ox, f.p23.x - ox, f.p23.z - ox};
-    const float py[4] = {f.p01.y - oy, f.p01.w - oy, f.p23.y - oy, f.p23.w - oy};
+// Bit q (q < F * F) set: the tet with footprint f can reach a pixel ray of
+// sub-tile q (column q % F, row q / F; w x h pixels) of the tile whose pixel
+// origin is (ox, oy), under the jitter bounds jb.  First the box test
+// (box_meets_tile); then, when the projected vertices are given, every edge
+// of their convex hull: the 6 vertex pairs, a pair being a hull edge when the
+// other two points lie on one side of its line (rounding can only misjudge
+// points within rounding distance of the line, far inside the margin).  A
+// sub-tile whose jittered footprint lies more than kHullMargin outside one
+// hull edge is dropped.  Coordinates are taken relative to (ox, oy); plain
+// float operations in this order (no fused multiply-add).
+template <int F>
+__device__ __forceinline__ uint64_t footprint_bits(const Footprint& f, float4 jb, int ox, int oy, int w, int h) {
+    uint64_t bits = 0;
+#pragma unroll
+    for (int q = 0; q < F * F; ++q)
+        if (box_meets_tile(f.box, jb, ox + q % F * w, oy + q / F * h, w, h)) bits |= 1ull << q;
+    if (bits == 0 || isnan(f.p01.x)) return bits;
+    const float fx = (float)ox, fy = (float)oy;
+    const float px[4] = {f.p01.x - fx, f.p01.z - fx, f.p23.x - fx, f.p23.z - fx};
+    const float py[4] = {f.p01.y - fy, f.p01.w - fy, f.p23.y - fy, f.p23.w - fy};
     const int ea[6] = {0, 0, 0, 1, 1, 2}, eb[6] = {1, 2, 3, 2, 3, 3};
     const int o1[6] = {2, 1, 1, 0, 0, 0}, o2[6] = {3, 3, 2, 3, 2, 1};
 #pragma unroll
@@ -237,37 +241,20 @@ __device__ __forceinline__ HullEdges hull_edges(const Footprint& f, float ox, fl
         const float s2 = nx * px[o2[k]] + ny * py[o2[k]] - ca;
         const bool out_pos = s1 <= 0.f && s2 <= 0.f;  // the others on the negative side: n points out
         const bool out_neg = !out_pos && s1 >= 0.f && s2 >= 0.f;
-        const float sg = out_pos ? 1.0f : (out_neg ? -1.0f : 0.0f);
-        e.nx[k] = valid ? sg * nx : 0.f;
-        e.ny[k] = valid ? sg * ny : 0.f;
-        e.c[k] = valid ? sg * ca : 0.f;
-    }
-    return e;
-}
-
-// Whether the rectangle [xlo, xhi] x [ylo, yhi] (relative to the edges'
-// origin) lies farther than kHullMargin outside one edge of the hull.
-__device__ __forceinline__ bool hull_separates(const HullEdges& e, float xlo, float ylo, float xhi, float yhi) {
-    bool sep = false;
+        if (!out_pos && !out_neg) continue;
+        const float sg = out_pos ? 1.0f : -1.0f;
+        const float ex = sg * nx, ey = sg * ny, ec = sg * ca;
+        const float margin = kHullMargin * (fabsf(ex) + fabsf(ey));
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        const float nx = e.nx[k], ny = e.ny[k];
-        const float d = nx * (nx > 0.f ? xlo : xhi) + ny * (ny > 0.f ? ylo : yhi) - e.c[k];
-        sep |= d > kHullMargin * (fabsf(nx) + fabsf(ny));
+        for (int q = 0; q < F * F; ++q) {
+            const int dx = q % F * w, dy = q / F * h;
+            const float xlo = (float)dx + jb.x, xhi = (float)(dx + w - 1) + jb.z;
+            const float ylo = (float)dy + jb.y, yhi = (float)(dy + h - 1) + jb.w;
+            const float d = ex * (ex > 0.f ? xlo : xhi) + ey * (ey > 0.f ? ylo : yhi) - ec;
+            if (d > margin) bits &= ~(1ull << q);
+        }
     }
-    return sep;
-}
-
-// Whether a tet can reach a pixel ray of the tile with pixel columns
-// [x0, x0 + w) and rows [y0, y0 + h) under the jitter bounds jb (see
-// box_meets_tile); e are the tet's hull edges relative to the integer point
-// (ox, oy).
-__device__ __forceinline__ bool tet_meets_tile(const Footprint& f, const HullEdges& e, int ox, int oy, float4 jb,
-                                               int x0, int y0, int w, int h) {
-    if (!box_meets_tile(f.box, jb, x0, y0, w, h)) return false;
-    const float xlo = (float)(x0 - ox) + jb.x, xhi = (float)(x0 - ox + w - 1) + jb.z;
-    const float ylo = (float)(y0 - oy) + jb.y, yhi = (float)(y0 - oy + h - 1) + jb.w;
-    return !hull_separates(e, xlo, ylo, xhi, yhi);
+    return bits;
 }
 
 // Bounded spin helper: returns false once the budget is exhausted.

@@ -184,28 +184,20 @@ __global__ void __launch_bounds__(256) emit_multi_kernel(const float* __restrict
     int64_t off = i == 0 ? 0 : (int64_t)__ldg(offsets + i - 1);
     const uint64_t fk = sortable_key(__ldg(depth + i));
     // with footprint: bits 28..31 of the value say which of the tile's 2x2
-    // half-size tiles the tet can reach (bit qy * 2 + qx, tet_meets_tile)
+    // half-size tiles the tet can reach (bit qy * 2 + qx, footprint_bits)
     const int tw = views.cams[v].tile_width, th = views.cams[v].tile_height;
     const int hw = tw >> 1, hh = th >> 1;
     Footprint fp = {};
-    HullEdges he = {};
     float4 jb = {0.f, 0.f, 0.f, 0.f};
     if (footprint) {
         fp = {__ldg(footprint + 3 * i), __ldg(footprint + 3 * i + 1), __ldg(footprint + 3 * i + 2)};
-        he = hull_edges(fp, (float)(r.x * tw), (float)(r.y * th));
         jb = __ldg(jitter_bounds);
     }
     for (int32_t y = r.y; y < r.w; ++y) {
         for (int32_t x = r.x; x < r.z; ++x) {
             if (off < capacity) {
                 uint32_t q = 0;
-                if (footprint) {
-#pragma unroll
-                    for (int b = 0; b < 4; ++b)
-                        if (tet_meets_tile(fp, he, r.x * tw, r.y * th, jb, x * tw + (b & 1) * hw,
-                                           y * th + (b >> 1) * hh, hw, hh))
-                            q |= 1u << b;
-                }
+                if (footprint) q = (uint32_t)footprint_bits<2>(fp, jb, x * tw, y * th, hw, hh);
                 keys[off] = (int64_t)(((uint64_t)(tile0 + (uint32_t)(y * grid_w + x)) << 32) | fk);
                 vals[off] = (int32_t)((uint32_t)g | (q << 28));
             }
