@@ -7,10 +7,12 @@ same dict is converted into the POD ``rm_camera`` struct of ``include/rm_capi.h`
 """
 from __future__ import annotations
 
+import collections
 import ctypes
 import math
 
 import numpy as np
+import torch
 
 __all__ = [
     "RMCamera",
@@ -51,6 +53,22 @@ def _as_np(x, n):
     return a
 
 
+_CACHE: "collections.OrderedDict" = collections.OrderedDict()
+_CACHE_MAX = 64
+_FIELDS = ("world_view_transform", "K", "cam_pos", "distortion_params", "min_t", "camera_type", "image_height",
+           "image_width", "tile_height", "tile_width", "grid_height", "grid_width")
+
+
+def _key_of(x):
+    if isinstance(x, torch.Tensor):
+        # identity, storage and version: an in-place change bumps the version,
+        # and the cache holds the tensor, so neither id nor storage is reused
+        return ("t", id(x), x.data_ptr(), x._version, str(x.device), tuple(x.shape), str(x.dtype))
+    if x is None or isinstance(x, (int, float, str)):
+        return ("v", x)
+    return ("a", tuple(np.asarray(x, dtype=np.float64).reshape(-1).tolist()))
+
+
 def tcam_to_struct(tcam: dict) -> RMCamera:
     """Convert a reference ``tcam`` dict into an ``rm_camera``.
 
@@ -58,7 +76,26 @@ def tcam_to_struct(tcam: dict) -> RMCamera:
     cameras with the reference's radial/tangential ``distortion_params``
     (k1, k2, p1, p2) are supported; any other camera type raises
     ``ValueError``.
+
+    The camera's matrices usually live on the GPU (``Camera.to_dict(device)``
+    in the reference), and reading them to the host waits for the stream, so
+    the conversion is cached: a dict whose tensors are the same objects,
+    unchanged in place, with the same other fields returns (a copy of) the
+    earlier result without touching the device.
     """
+    key = tuple(_key_of(tcam.get(k)) for k in _FIELDS)
+    hit = _CACHE.get(key)
+    if hit is not None:
+        _CACHE.move_to_end(key)
+        return RMCamera.from_buffer_copy(hit[1])
+    cam = _convert(tcam)
+    _CACHE[key] = (tuple(tcam.get(k) for k in _FIELDS), RMCamera.from_buffer_copy(cam))
+    while len(_CACHE) > _CACHE_MAX:
+        _CACHE.popitem(last=False)
+    return cam
+
+
+def _convert(tcam: dict) -> RMCamera:
     cam = RMCamera()
     cam.world_view[:] = _as_np(tcam["world_view_transform"], 16).tolist()
     cam.K[:] = _as_np(tcam["K"], 9).tolist()
@@ -118,8 +155,6 @@ def intrinsics(height: int, width: int, fovy_deg: float):
 def make_tcam(world_view, K, cam_pos, height, width, tile_size=16, min_t=0.1, fovx=None, fovy=None,
               device=None):
     """Build a ``tcam`` dict with the reference's keys (utils/train_util.py:31-38)."""
-    import torch
-
     grid_h = (height + tile_size - 1) // tile_size
     grid_w = (width + tile_size - 1) // tile_size
     dev = device if device is not None else "cpu"

@@ -103,10 +103,12 @@ def _stream():
 
 class StageTimer:
     """Records a CUDA event pair around every C-ABI call on the launching
-    (current) stream while active; ``totals()`` returns milliseconds per stage."""
+    (current) stream while active (or only around the stages named in
+    ``only``); ``totals()`` returns milliseconds per stage."""
 
-    def __init__(self):
+    def __init__(self, only=None):
         self.events = []
+        self.only = None if only is None else set(only)
 
     def __enter__(self):
         global _TIMER
@@ -140,7 +142,7 @@ _TIMER: StageTimer | None = None
 
 
 def _call(name, fn):
-    if _TIMER is None:
+    if _TIMER is None or (_TIMER.only is not None and name not in _TIMER.only):
         rc = fn()
     else:
         rc = _TIMER.record(name, fn)
@@ -231,40 +233,68 @@ def project_bwd(indices, vertices, cam: RMCamera, tiles, grad_vs, grad_cc, grad_
     return grad_vertices
 
 
+_PAIR_GUESS: dict = {}  # device -> pair count of the last frame built there
+
+
 def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, cam: RMCamera,
                      pool: ScratchPool | None = None, keep_debug: bool = False) -> TileLists:
     """Scan, emit, sort and range the tile/tet pairs.
 
     The pair count P is read back to the host once (the reference reads it
-    three times: tile_shader_slang.py:38-44,68)."""
+    three times: tile_shader_slang.py:38-44,68).  After the first frame on a
+    device, the pair buffers are sized from the previous frame's count (plus
+    a quarter) and emission, sort and ranges are queued before P is read, so
+    the GPU keeps working while the host waits for it; the kernels take the
+    pair count from the device.  Should P exceed that capacity, the frame is
+    built again with buffers of exactly P.  The returned tensors are the
+    first P entries of those buffers."""
     pool = pool or _POOL
     dev = tiles.device
     T = tiles.shape[0]
     G = cam.grid_width * cam.grid_height
     L = C.lib()
     s = _stream()
+    end_bit = end_bit_for(cam.grid_width, cam.grid_height)
     offsets = torch.empty(T, dtype=torch.int32, device=dev)
     total = torch.zeros(1, dtype=torch.int64, device=dev)
     ws_n = L.rm_scan_workspace_size(T)
     ws = pool.get("scan", ws_n, dev)
     _call("rm_scan_tiles", lambda: L.rm_scan_tiles(C.ptr(tiles), T, C.ptr(offsets), C.ptr(total), C.ptr(ws), ws_n, s))
-    P = int(total.item())
-    keys = torch.empty(P, dtype=torch.int64, device=dev)
-    vals = torch.empty(P, dtype=torch.int32, device=dev)
-    _call("rm_emit_pairs", lambda: L.rm_emit_pairs(C.ptr(vs), C.ptr(rect), C.ptr(offsets), T, cam.grid_width, P, None, C.ptr(keys),
-                            C.ptr(vals), None, s))
-    sk = torch.empty(P, dtype=torch.int64, device=dev)
-    sv = torch.empty(P, dtype=torch.int32, device=dev)
-    if P > 0:
-        ws_n = L.rm_sort_workspace_size(P)
-        ws = pool.get("sort", ws_n, dev)
-        _call("rm_sort_pairs", lambda: L.rm_sort_pairs(C.ptr(keys), C.ptr(vals), P, None, end_bit_for(cam.grid_width, cam.grid_height),
-                                C.ptr(sk), C.ptr(sv), C.ptr(ws), ws_n, s))
-    ranges = torch.empty((G, 2), dtype=torch.int32, device=dev)
-    _call("rm_tile_ranges", lambda: L.rm_tile_ranges(C.ptr(sk), P, None, C.ptr(ranges), G, s))
+
+    def pairs(cap, n_dev):
+        keys = torch.empty(cap, dtype=torch.int64, device=dev)
+        vals = torch.empty(cap, dtype=torch.int32, device=dev)
+        _call("rm_emit_pairs", lambda: L.rm_emit_pairs(C.ptr(vs), C.ptr(rect), C.ptr(offsets), T, cam.grid_width,
+                                                       cap, C.ptr(n_dev), C.ptr(keys), C.ptr(vals), None, s))
+        sk = torch.empty(cap, dtype=torch.int64, device=dev)
+        sv = torch.empty(cap, dtype=torch.int32, device=dev)
+        if cap > 0:
+            sws_n = L.rm_sort_workspace_size(cap)
+            sws = pool.get("sort", sws_n, dev)
+            _call("rm_sort_pairs", lambda: L.rm_sort_pairs(C.ptr(keys), C.ptr(vals), cap, C.ptr(n_dev), end_bit,
+                                                           C.ptr(sk), C.ptr(sv), C.ptr(sws), sws_n, s))
+        ranges = torch.empty((G, 2), dtype=torch.int32, device=dev)
+        _call("rm_tile_ranges", lambda: L.rm_tile_ranges(C.ptr(sk), cap, C.ptr(n_dev), C.ptr(ranges), G, s))
+        return keys, vals, sk, sv, ranges
+
+    key = str(dev)
+    guess = _PAIR_GUESS.get(key)
+    out = None
+    if guess is not None:
+        cap = guess + guess // 4 + 4096
+        out = pairs(cap, total)
+        P = int(total.item())
+        if P > cap:
+            out = None
+    else:
+        P = int(total.item())
+    if out is None:
+        out = pairs(P, None)
+    _PAIR_GUESS[key] = P
+    keys, vals, sk, sv, ranges = out
     if keep_debug:
-        return TileLists(sv, ranges, P, offsets, keys, vals, sk)
-    return TileLists(sv, ranges, P)
+        return TileLists(sv[:P], ranges, P, offsets, keys[:P], vals[:P], sk[:P])
+    return TileLists(sv[:P], ranges, P)
 
 
 @dataclass

@@ -187,3 +187,24 @@ def test_serving_trace_is_seeded_poisson():
     assert set(res) == set(scenes.SERVING_RESOLUTIONS)
     for _, _, v in tr[:50]:
         assert abs(np.linalg.norm(v.cam_pos) - 4.0) < 1e-5
+
+
+def test_tcam_conversion_cache():
+    """tcam_to_struct returns the same camera from its cache for the same
+    tensors, a fresh one after an in-place change, and independent copies."""
+    import torch
+
+    from radiance_meshes_b200.camera import pinhole_tcam, tcam_to_struct
+
+    tcam = pinhole_tcam((0.0, 0.0, -3.0), (0.0, 0.0, 0.0), 64, 96)
+    a = tcam_to_struct(tcam)
+    b = tcam_to_struct(tcam)
+    assert bytes(a) == bytes(b)
+    b.min_t = 7.0  # a copy: the cached camera is untouched
+    assert tcam_to_struct(tcam).min_t == a.min_t
+    with torch.no_grad():
+        tcam["cam_pos"][0] += 1.0
+    c = tcam_to_struct(tcam)
+    assert c.cam_pos[0] == a.cam_pos[0] + 1.0
+    tcam2 = dict(tcam, tile_width=8, tile_height=8, grid_width=12, grid_height=8)
+    assert tcam_to_struct(tcam2).tile_width == 8
