@@ -280,7 +280,10 @@ RM_API int rm_jitter_bounds(const float* ray_jitter, int64_t n_pixels, float* bo
 
 /*
  * Fine lists from the sorted coarse lists: splits each coarse tile's list
- * (sorted_ids, ranges [G,2]) in order into the lists of its 2^fine_shift x
+ * (sorted_ids, ranges [G,2]; sorted_keys are rm_sort_pairs' sorted keys,
+ * whose high word is each entry's tile; n_pairs entries, or
+ * min(*n_pairs_dev, n_pairs) when n_pairs_dev is given) in order into the
+ * lists of its 2^fine_shift x
  * 2^fine_shift fine tiles (tile_width >> fine_shift by tile_height >>
  * fine_shift pixels, on a grid 2^fine_shift times larger).  An entry goes to
  * a fine tile when its tet's footprint (rm_project_fwd_fine) can meet the
@@ -296,11 +299,12 @@ RM_API int rm_jitter_bounds(const float* ray_jitter, int64_t n_pixels, float* bo
  * sorting and ranging the fine pairs: fine_ids (capacity entries;
  * 4^fine_shift * P always suffices) and fine_ranges [G * 4^fine_shift, 2] on
  * the fine grid, *total_dev = fine pair count.  fine_shift is 1, 2 or 3.
- * Workspace: rm_fine_lists_workspace_size(fine tiles), 256-byte aligned.  No
- * reference counterpart.
+ * Workspace: rm_fine_lists_workspace_size(fine tiles, n_pairs, fine_shift),
+ * 256-byte aligned.  No reference counterpart.
  */
-RM_API size_t rm_fine_lists_workspace_size(int64_t n_fine_tiles);
-RM_API int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges,
+RM_API size_t rm_fine_lists_workspace_size(int64_t n_fine_tiles, int64_t n_pairs, int fine_shift);
+RM_API int rm_fine_lists(const int64_t* sorted_keys, const int32_t* sorted_ids, int64_t n_pairs,
+                         const int64_t* n_pairs_dev, const int32_t* ranges,
                          const float* footprint, const float* jitter_bounds,
                          const rm_camera* cam, int fine_shift,
                          int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
@@ -356,7 +360,8 @@ RM_API int rm_project_fwd_multi(const int32_t* indices, const float* vertices,
  * the sorted values carry the packed 2x2 coverage bits of
  * rm_emit_pairs_multi; fine_ids then hold the plain tet ids.
  */
-RM_API int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges,
+RM_API int rm_fine_lists_multi(const int64_t* sorted_keys, const int32_t* sorted_ids, int64_t n_pairs,
+                               const int64_t* n_pairs_dev, const int32_t* ranges,
                                const float* footprint, const float* jitter_bounds, int64_t n_tets,
                                const rm_camera* cams, int n_views, int fine_shift,
                                int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,

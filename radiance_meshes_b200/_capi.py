@@ -68,11 +68,12 @@ SIGNATURES = {
     "rm_project_fwd_fine": (ctypes.c_int, [vp, vp, i64, i64, camp, vp, vp, vp, vp, vp, vp]),
     "rm_jitter_bounds_workspace_size": (sz, []),
     "rm_jitter_bounds": (ctypes.c_int, [vp, i64, vp, vp, sz, vp]),
-    "rm_fine_lists_workspace_size": (sz, [i64]),
-    "rm_fine_lists": (ctypes.c_int, [vp, vp, vp, vp, camp, ctypes.c_int, i64, vp, vp, vp, vp, sz, vp]),
+    "rm_fine_lists_workspace_size": (sz, [i64, i64, ctypes.c_int]),
+    "rm_fine_lists": (ctypes.c_int, [vp, vp, i64, vp, vp, vp, vp, camp, ctypes.c_int, i64, vp, vp, vp, vp, sz,
+                                     vp]),
     "rm_project_fwd_multi": (ctypes.c_int, [vp, vp, i64, i64, camp, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp]),
-    "rm_fine_lists_multi": (ctypes.c_int, [vp, vp, vp, vp, i64, camp, ctypes.c_int, ctypes.c_int, i64, vp, vp, vp,
-                                           vp, sz, vp]),
+    "rm_fine_lists_multi": (ctypes.c_int, [vp, vp, i64, vp, vp, vp, vp, i64, camp, ctypes.c_int, ctypes.c_int, i64,
+                                           vp, vp, vp, vp, sz, vp]),
     "rm_emit_pairs_multi": (ctypes.c_int, [vp, vp, vp, i64, camp, ctypes.c_int, i64, vp, vp, vp, vp, vp, vp, vp]),
     "rm_views_tile_count": (i64, [camp, ctypes.c_int]),
     "rm_calc_tet_err": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, camp, vp, vp, vp, vp, vp, sz,

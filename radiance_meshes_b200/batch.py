@@ -131,7 +131,6 @@ class BatchedRasterizer:
             self.jitter_ws = torch.empty(L.rm_jitter_bounds_workspace_size(), dtype=torch.uint8, device=dev)
             self.fine_ranges = torch.empty((bv.n_tiles, 2), dtype=torch.int32, device=dev)
             self.fine_total = torch.zeros(1, dtype=torch.int64, device=dev)
-            self.fine_ws = torch.empty(L.rm_fine_lists_workspace_size(bv.n_tiles), dtype=torch.uint8, device=dev)
         self.blend_ws = None  # sized with the pair capacity (hit masks) in _alloc_pairs
         Npx = views.n_pixels
         self.jitter = jitter if jitter is not None else torch.full((Npx, 2), 0.5, device=dev)
@@ -179,6 +178,8 @@ class BatchedRasterizer:
         if self.fine_shift:
             blend_pairs = capacity << (2 * self.fine_shift)  # a coarse entry splits into at most 4^s
             self.fine_ids = torch.empty(blend_pairs, dtype=torch.int32, device=dev)
+            fws = C.lib().rm_fine_lists_workspace_size(self.blend_views.n_tiles, capacity, self.fine_shift)
+            self.fine_ws = torch.empty(fws, dtype=torch.uint8, device=dev)
         ws = self._ws_base
         if self.hit_masks:
             bv = self.blend_views
@@ -234,7 +235,8 @@ class BatchedRasterizer:
                                  v.n_tiles, s))
         if self.fine_shift:
             R._call("rm_fine_lists", lambda: L.rm_fine_lists_multi(
-                C.ptr(self.sorted_ids), C.ptr(self.ranges), None if packed else C.ptr(self.footprint),
+                C.ptr(self.sorted_keys), C.ptr(self.sorted_ids), self.capacity, C.ptr(self.total),
+                C.ptr(self.ranges), None if packed else C.ptr(self.footprint),
                 None if packed else C.ptr(self.jitter_bounds), self.T, v.array, v.n,
                 self.fine_shift, self.fine_ids.shape[0], C.ptr(self.fine_ids), C.ptr(self.fine_ranges),
                 C.ptr(self.fine_total), C.ptr(self.fine_ws), self.fine_ws.numel(), s))

@@ -7,11 +7,13 @@
 // the tets that can reach one of its pixels' rays (footprint_bits).  Emitting
 // fine pairs and sorting them again would reproduce exactly that order (depth
 // key, then tet id), so instead each coarse list is split once, in order, into
-// its 4 (or 16, 64) fine lists: a counting pass, a scan of the counts in
-// fine-tile order, and a writing pass.  One CTA walks one coarse list in
-// chunks of 1024 entries; the ranks inside a chunk come from warp ballots per
-// fine tile.  No reference counterpart (the reference blends over the coarse
-// lists directly).
+// its 4 (or 16, 64) fine lists: a flat pass over all entries that computes
+// each entry's reach bits (the entry's tile is the high word of its sorted
+// key) and counts them per fine tile, a scan of the counts in fine-tile
+// order, and a writing pass in which one CTA walks one coarse list in chunks
+// of 1024 entries, the ranks inside a chunk coming from warp ballots per fine
+// tile.  No reference counterpart (the reference blends over the coarse lists
+// directly).
 #include <algorithm>
 
 #include "rm_internal.cuh"
@@ -70,41 +72,104 @@ __global__ void __launch_bounds__(32) jitter_final_kernel(const float4* __restri
     if (threadIdx.x == 0) *out = m;
 }
 
-// WRITE = false: counts[fine id] = entries of the coarse list reaching the
-// fine tile.  WRITE = true: write the fine lists at their scanned offsets and
-// the fine ranges.  FS = fine shift (2^FS x 2^FS fine tiles per tile).
-// Views: tile t of the coarse (global, view-major) numbering belongs to view
-// v = views.find(t); its fine tiles are numbered view-major too, view v's
-// starting at tiles[v] * f^2; footprint rows are stacked view-major ([v, T]).
-template <bool WRITE, bool PACKED, int FS>
-__global__ void __launch_bounds__(kFineThreads, 2) fine_lists_kernel(
-    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ footprint,
-    const float4* __restrict__ jitter_bounds, int64_t n_tets, const __grid_constant__ ViewSet views,
-    int32_t* __restrict__ counts, const int32_t* __restrict__ incl, int32_t* __restrict__ fine_ids,
-    int64_t capacity, int2* __restrict__ fine_ranges, uint32_t* status) {
+// Storage of an entry's reach bits (one bit per fine tile of its tile).
+template <int FS>
+struct FineBits;
+template <>
+struct FineBits<1> {
+    using type = uint8_t;
+};
+template <>
+struct FineBits<2> {
+    using type = uint16_t;
+};
+template <>
+struct FineBits<3> {
+    using type = uint64_t;
+};
+
+// Fine tile id of sub-tile q of coarse tile t: view v's fine tiles are
+// numbered view-major from tiles[v] * f^2, row-major on its fine grid.
+template <int FS>
+__device__ __forceinline__ int64_t fine_tile_id(const ViewSet& views, int t, int q) {
+    constexpr int f = 1 << FS;
+    const int v = views.find(t);
+    const int local = t - views.tiles[v];
+    const int gw = views.cams[v].grid_width;
+    const int tx = local % gw, ty = local / gw;
+    return (int64_t)views.tiles[v] * (f * f) + (int64_t)(ty * f + q / f) * (gw * f) + tx * f + q % f;
+}
+
+// Pass 1, flat over the sorted coarse entries (their tile is the key's high
+// word): each entry's reach bits -- footprint_bits against its tile's fine
+// tiles, or the packed bits of the value -- stored for pass 3 (not when
+// packed), and the entry counts per fine tile (warp-aggregated atomics over
+// the lanes of one tile).  Footprint rows are stacked view-major ([v, T]).
+template <bool PACKED, int FS>
+__global__ void __launch_bounds__(256) fine_bits_kernel(
+    const int64_t* __restrict__ keys, const int32_t* __restrict__ ids, int64_t cap, const int64_t* __restrict__ n_dev,
+    const float4* __restrict__ footprint, const float4* __restrict__ jitter_bounds, int64_t n_tets,
+    const __grid_constant__ ViewSet views, typename FineBits<FS>::type* __restrict__ bits_out,
+    int32_t* __restrict__ counts) {
     constexpr int f = 1 << FS, Q = f * f;
-    __shared__ uint32_t wcnt[kFineWarps][Q];  // WRITE: this chunk's count per (warp, fine tile)
-    __shared__ uint32_t wpre[kFineWarps][Q];  // WRITE: the warp's first position per fine tile
+    const int64_t n = n_dev ? min(*n_dev, cap) : cap;
+    const float4 jb = PACKED ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(jitter_bounds);
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = (int64_t)blockIdx.x * 256; base < n; base += (int64_t)gridDim.x * 256) {
+        const int64_t e = base + threadIdx.x;
+        const bool in = e < n;
+        int t = -1;
+        uint64_t bits = 0;
+        if (in) {
+            t = (int)((uint64_t)__ldg((const unsigned long long*)keys + e) >> 32);
+            int32_t g = __ldg(ids + e);
+            if (PACKED) {
+                bits = (uint32_t)g >> 28;
+            } else {
+                const int v = views.find(t);
+                const int local = t - views.tiles[v];
+                const rm_camera& c = views.cams[v];
+                const int tx = local % c.grid_width, ty = local / c.grid_width;
+                const float4* fp_g = footprint + 3 * ((int64_t)v * n_tets + g);
+                const Footprint fp = {__ldg(fp_g), __ldg(fp_g + 1), __ldg(fp_g + 2)};
+                bits = footprint_bits<f>(fp, jb, tx * c.tile_width, ty * c.tile_height, c.tile_width / f,
+                                         c.tile_height / f);
+                bits_out[e] = (typename FineBits<FS>::type)bits;
+            }
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, t);
+        const bool leader = in && lane == __ffs(peers) - 1;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u) & peers;
+            if (leader && bal) atomicAdd(counts + fine_tile_id<FS>(views, t, q), __popc(bal));
+        }
+    }
+}
+
+// Pass 3, one CTA per coarse tile: write the entries of its list into the
+// lists of its fine tiles at their scanned offsets, in list order (ranks from
+// warp ballots and a warp-0 scan of the per-warp counts per chunk of 1024
+// entries), and the fine ranges.
+template <bool PACKED, int FS>
+__global__ void __launch_bounds__(kFineThreads, 2) fine_write_kernel(
+    const int32_t* __restrict__ ids, const int2* __restrict__ ranges,
+    const typename FineBits<FS>::type* __restrict__ bits_in, const __grid_constant__ ViewSet views,
+    const int32_t* __restrict__ counts, const int32_t* __restrict__ incl, int32_t* __restrict__ fine_ids,
+    int64_t capacity, int2* __restrict__ fine_ranges, uint32_t* status) {
+    constexpr int Q = (1 << FS) * (1 << FS);
+    __shared__ uint32_t wcnt[kFineWarps][Q];  // this chunk's count per (warp, fine tile)
+    __shared__ uint32_t wpre[kFineWarps][Q];  // the warp's first position per fine tile
     __shared__ uint32_t run[Q];               // entries per fine tile so far
     __shared__ int32_t start[Q];
     const int t = blockIdx.x;
-    const int v = views.find(t);
-    const int local = t - views.tiles[v];
-    const int grid_w = views.cams[v].grid_width;
-    const int tx = local % grid_w, ty = local / grid_w;
-    const int fgw = grid_w * f;
-    const int64_t fbase = (int64_t)views.tiles[v] * Q;
-    const float4* __restrict__ fp_v = footprint + (int64_t)v * n_tets * 3;
-    const int ftw = views.cams[v].tile_width / f, fth = views.cams[v].tile_height / f;
-    const int px0 = tx * views.cams[v].tile_width, py0 = ty * views.cams[v].tile_height;
-    const float4 jb = PACKED ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(jitter_bounds);
     const int2 r = __ldg(ranges + t);
-    auto fine_id = [&](int q) { return fbase + (int64_t)(ty * f + q / f) * fgw + tx * f + q % f; };
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     if (threadIdx.x < Q) {
+        const int64_t fid = fine_tile_id<FS>(views, t, threadIdx.x);
         run[threadIdx.x] = 0u;
-        if (WRITE) start[threadIdx.x] = __ldg(incl + fine_id(threadIdx.x)) - __ldg(counts + fine_id(threadIdx.x));
+        start[threadIdx.x] = __ldg(incl + fid) - __ldg(counts + fid);
     }
     __syncthreads();
     for (int base = r.x; base < r.y; base += kFineThreads) {
@@ -117,60 +182,49 @@ __global__ void __launch_bounds__(kFineThreads, 2) fine_lists_kernel(
                 bits = (uint32_t)g >> 28;
                 g &= 0x0fffffff;
             } else {
-                const Footprint fp = {__ldg(fp_v + 3 * (int64_t)g), __ldg(fp_v + 3 * (int64_t)g + 1),
-                                      __ldg(fp_v + 3 * (int64_t)g + 2)};
-                bits = footprint_bits<f>(fp, jb, px0, py0, ftw, fth);
+                bits = bits_in[e];
             }
         }
-        if constexpr (!WRITE) {
 #pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
+            if (lane == 0) wcnt[warp][q] = __popc(bal);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            // per fine tile: exclusive prefix over the warps, offset by the
+            // entries of the earlier chunks
             for (int q = 0; q < Q; ++q) {
-                const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
-                if (lane == 0 && bal) atomicAdd(&run[q], (uint32_t)__popc(bal));
-            }
-        } else {
+                const uint32_t x = wcnt[lane][q];
+                uint32_t inc = x;
 #pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const unsigned bal = __ballot_sync(0xffffffffu, (bits >> q) & 1u);
-                if (lane == 0) wcnt[warp][q] = __popc(bal);
-            }
-            __syncthreads();
-            if (warp == 0) {
-                // per fine tile: exclusive prefix over the warps, offset by the
-                // entries of the earlier chunks
-                for (int q = 0; q < Q; ++q) {
-                    const uint32_t x = wcnt[lane][q];
-                    uint32_t inc = x;
-#pragma unroll
-                    for (int off = 1; off < 32; off <<= 1) {
-                        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, off);
-                        if (lane >= off) inc += y;
-                    }
-                    const uint32_t r0 = run[q];
-                    wpre[lane][q] = r0 + inc - x;
-                    __syncwarp();
-                    if (lane == 31) run[q] = r0 + inc;
-                    __syncwarp();
+                for (int off = 1; off < 32; off <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, off);
+                    if (lane >= off) inc += y;
                 }
+                const uint32_t r0 = run[q];
+                wpre[lane][q] = r0 + inc - x;
+                __syncwarp();
+                if (lane == 31) run[q] = r0 + inc;
+                __syncwarp();
             }
-            __syncthreads();
+        }
+        __syncthreads();
 #pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const bool in = (bits >> q) & 1u;
-                const unsigned bal = __ballot_sync(0xffffffffu, in);
-                if (in) {
-                    const int64_t o = (int64_t)start[q] + wpre[warp][q] + __popc(bal & lt);
-                    if (o < capacity) fine_ids[o] = g;
-                    else if (status) atomicOr(status, RM_STATUS_CAPACITY);
-                }
+        for (int q = 0; q < Q; ++q) {
+            const bool hit = (bits >> q) & 1u;
+            const unsigned bal = __ballot_sync(0xffffffffu, hit);
+            if (hit) {
+                const int64_t o = (int64_t)start[q] + wpre[warp][q] + __popc(bal & lt);
+                if (o < capacity) fine_ids[o] = g;
+                else if (status) atomicOr(status, RM_STATUS_CAPACITY);
             }
         }
     }
     __syncthreads();
     if (threadIdx.x < Q) {
         const int q = threadIdx.x;
-        if (WRITE) fine_ranges[fine_id(q)] = make_int2(start[q], start[q] + (int)run[q]);
-        else counts[fine_id(q)] = (int32_t)run[q];
+        fine_ranges[fine_tile_id<FS>(views, t, q)] = make_int2(start[q], start[q] + (int)run[q]);
     }
 }
 
@@ -181,9 +235,12 @@ size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 extern "C" {
 
-size_t rm_fine_lists_workspace_size(int64_t n_fine_tiles) {
+size_t rm_fine_lists_workspace_size(int64_t n_fine_tiles, int64_t n_pairs, int fine_shift) {
     const int64_t n = n_fine_tiles > 0 ? n_fine_tiles : 1;
-    return 2 * rm::align256((size_t)n * 4) + 256 + rm_scan_workspace_size(n);
+    const int64_t p = n_pairs > 0 ? n_pairs : 1;
+    const size_t bits = fine_shift <= 1 ? 1 : (fine_shift == 2 ? 2 : 8);
+    return 2 * rm::align256((size_t)n * 4) + 256 + rm::align256(rm_scan_workspace_size(n)) +
+           rm::align256((size_t)p * bits);
 }
 
 size_t rm_jitter_bounds_workspace_size(void) { return sizeof(float4) * rm::kBoundsBlocks; }
@@ -211,12 +268,41 @@ int rm_jitter_bounds(const float* jitter, int64_t n_pixels, float* bounds, void*
 
 namespace {
 
-int fine_lists_impl(const char* who, const int32_t* sorted_ids, const int32_t* ranges, const float* footprint,
+template <bool PACKED, int FS>
+int launch_split(const int64_t* keys, const int32_t* ids, int64_t n_pairs, const int64_t* n_pairs_dev,
+                 const int32_t* ranges, const float* footprint, const float* jitter_bounds, int64_t n_tets,
+                 const rm::ViewSet& views, int64_t G, int64_t Gf, int64_t capacity, int32_t* fine_ids,
+                 int32_t* fine_ranges, int64_t* total_dev, char* ws, cudaStream_t s) {
+    using Bits = typename rm::FineBits<FS>::type;
+    int32_t* counts = (int32_t*)ws;
+    int32_t* incl = (int32_t*)(ws + rm::align256((size_t)Gf * 4));
+    char* scan_ws = ws + 2 * rm::align256((size_t)Gf * 4) + 256;
+    uint32_t* status = (uint32_t*)scan_ws;  // the scan workspace's status word
+    Bits* bits = (Bits*)(scan_ws + rm::align256(rm_scan_workspace_size(Gf)));
+    if (cudaMemsetAsync(counts, 0, (size_t)Gf * 4, s) != cudaSuccess) return rm_host::check_launch("rm_fine_lists");
+    if (n_pairs > 0) {
+        const int64_t want = (n_pairs + 255) / 256;
+        const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, 148 * 16));
+        rm::fine_bits_kernel<PACKED, FS><<<blocks, 256, 0, s>>>(
+            keys, ids, n_pairs, n_pairs_dev, (const float4*)footprint, (const float4*)jitter_bounds, n_tets, views,
+            bits, counts);
+        int rc = rm_host::check_launch("rm_fine_lists (bits)");
+        if (rc) return rc;
+    }
+    int rc = rm_scan_tiles(counts, Gf, incl, total_dev, scan_ws, rm_scan_workspace_size(Gf), s);
+    if (rc) return rc;
+    rm::fine_write_kernel<PACKED, FS><<<(unsigned)G, rm::kFineThreads, 0, s>>>(
+        ids, (const int2*)ranges, bits, views, counts, incl, fine_ids, capacity, (int2*)fine_ranges, status);
+    return rm_host::check_launch("rm_fine_lists (write)");
+}
+
+int fine_lists_impl(const char* who, const int64_t* sorted_keys, const int32_t* sorted_ids, int64_t n_pairs,
+                    const int64_t* n_pairs_dev, const int32_t* ranges, const float* footprint,
                     const float* jitter_bounds, int64_t n_tets, const rm::ViewSet& views, int fine_shift,
                     int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges, int64_t* total_dev, void* workspace,
                     size_t workspace_bytes, void* stream) {
     if (fine_shift < 1 || fine_shift > 3) return rm_host::fail(RM_EINVAL, "%s: fine_shift %d", who, fine_shift);
-    if (capacity < 0 || n_tets < 0) return rm_host::fail(RM_EINVAL, "%s: negative size", who);
+    if (capacity < 0 || n_tets < 0 || n_pairs < 0) return rm_host::fail(RM_EINVAL, "%s: negative size", who);
     const int f = 1 << fine_shift;
     for (int v = 0; v < views.n; ++v)
         if (views.cams[v].tile_width % f || views.cams[v].tile_height % f)
@@ -229,54 +315,39 @@ int fine_lists_impl(const char* who, const int32_t* sorted_ids, const int32_t* r
     const bool packed = footprint == nullptr;
     if (packed && fine_shift != 1) return rm_host::fail(RM_EINVAL, "%s: packed masks need fine_shift 1", who);
     if (!packed && !jitter_bounds) return rm_host::fail(RM_EINVAL, "%s: footprint without jitter_bounds", who);
-    if (!ranges || !fine_ranges || !total_dev || !workspace || (capacity > 0 && (!sorted_ids || !fine_ids)))
+    if (!ranges || !fine_ranges || !total_dev || !workspace ||
+        (n_pairs > 0 && (!sorted_keys || !sorted_ids)) || (capacity > 0 && !fine_ids))
         return rm_host::fail(RM_EINVAL, "%s: NULL pointer", who);
     if (((uintptr_t)footprint & 15) || ((uintptr_t)jitter_bounds & 15) || ((uintptr_t)ranges & 7) ||
-        ((uintptr_t)fine_ranges & 7) || ((uintptr_t)workspace & 255))
-        return rm_host::fail(RM_EINVAL, "%s: misaligned footprint / jitter_bounds / ranges / workspace", who);
-    if (workspace_bytes < rm_fine_lists_workspace_size(Gf))
-        return rm_host::fail(RM_EINVAL, "%s: workspace %zu < %zu bytes", who, workspace_bytes,
-                             rm_fine_lists_workspace_size(Gf));
+        ((uintptr_t)sorted_keys & 7) || ((uintptr_t)fine_ranges & 7) || ((uintptr_t)workspace & 255))
+        return rm_host::fail(RM_EINVAL, "%s: misaligned footprint / jitter_bounds / keys / ranges / workspace", who);
+    const size_t need = rm_fine_lists_workspace_size(Gf, n_pairs, fine_shift);
+    if (workspace_bytes < need)
+        return rm_host::fail(RM_EINVAL, "%s: workspace %zu < %zu bytes", who, workspace_bytes, need);
     if (G == 0) return RM_OK;
-    char* p = (char*)workspace;
-    int32_t* counts = (int32_t*)p;
-    int32_t* incl = (int32_t*)(p + rm::align256((size_t)Gf * 4));
-    char* scan_ws = p + 2 * rm::align256((size_t)Gf * 4) + 256;
-    uint32_t* status = (uint32_t*)scan_ws;  // the scan workspace's status word
+    char* ws = (char*)workspace;
     cudaStream_t s = (cudaStream_t)stream;
-    using Kernel = void (*)(const int32_t*, const int2*, const float4*, const float4*, int64_t, const rm::ViewSet,
-                            int32_t*, const int32_t*, int32_t*, int64_t, int2*, uint32_t*);
-    Kernel count, write;
-    if (packed) {
-        count = rm::fine_lists_kernel<false, true, 1>;
-        write = rm::fine_lists_kernel<true, true, 1>;
-    } else if (fine_shift == 1) {
-        count = rm::fine_lists_kernel<false, false, 1>;
-        write = rm::fine_lists_kernel<true, false, 1>;
-    } else if (fine_shift == 2) {
-        count = rm::fine_lists_kernel<false, false, 2>;
-        write = rm::fine_lists_kernel<true, false, 2>;
-    } else {
-        count = rm::fine_lists_kernel<false, false, 3>;
-        write = rm::fine_lists_kernel<true, false, 3>;
-    }
-    count<<<(unsigned)G, rm::kFineThreads, 0, s>>>(sorted_ids, (const int2*)ranges, (const float4*)footprint,
-                                                   (const float4*)jitter_bounds, n_tets, views, counts, nullptr,
-                                                   nullptr, 0, nullptr, nullptr);
-    int rc = rm_host::check_launch("rm_fine_lists (count)");
-    if (rc) return rc;
-    if ((rc = rm_scan_tiles(counts, Gf, incl, total_dev, scan_ws, rm_scan_workspace_size(Gf), stream))) return rc;
-    write<<<(unsigned)G, rm::kFineThreads, 0, s>>>(sorted_ids, (const int2*)ranges, (const float4*)footprint,
-                                                   (const float4*)jitter_bounds, n_tets, views, counts, incl,
-                                                   fine_ids, capacity, (int2*)fine_ranges, status);
-    return rm_host::check_launch("rm_fine_lists (write)");
+    if (packed)
+        return launch_split<true, 1>(sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint, jitter_bounds,
+                                     n_tets, views, G, Gf, capacity, fine_ids, fine_ranges, total_dev, ws, s);
+    if (fine_shift == 1)
+        return launch_split<false, 1>(sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint,
+                                      jitter_bounds, n_tets, views, G, Gf, capacity, fine_ids, fine_ranges, total_dev,
+                                      ws, s);
+    if (fine_shift == 2)
+        return launch_split<false, 2>(sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint,
+                                      jitter_bounds, n_tets, views, G, Gf, capacity, fine_ids, fine_ranges, total_dev,
+                                      ws, s);
+    return launch_split<false, 3>(sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint, jitter_bounds,
+                                  n_tets, views, G, Gf, capacity, fine_ids, fine_ranges, total_dev, ws, s);
 }
 
 }  // namespace
 
 extern "C" {
 
-int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges, const float* footprint,
+int rm_fine_lists(const int64_t* sorted_keys, const int32_t* sorted_ids, int64_t n_pairs,
+                  const int64_t* n_pairs_dev, const int32_t* ranges, const float* footprint,
                   const float* jitter_bounds, const rm_camera* cam, int fine_shift, int64_t capacity,
                   int32_t* fine_ids, int32_t* fine_ranges, int64_t* total_dev, void* workspace,
                   size_t workspace_bytes, void* stream) {
@@ -284,19 +355,22 @@ int rm_fine_lists(const int32_t* sorted_ids, const int32_t* ranges, const float*
     int rc = rm_host::make_views("rm_fine_lists", cam, 1, &views);
     if (rc) return rc;
     if (!footprint) return rm_host::fail(RM_EINVAL, "rm_fine_lists: NULL footprint");
-    return fine_lists_impl("rm_fine_lists", sorted_ids, ranges, footprint, jitter_bounds, 0, views, fine_shift,
-                           capacity, fine_ids, fine_ranges, total_dev, workspace, workspace_bytes, stream);
+    return fine_lists_impl("rm_fine_lists", sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint,
+                           jitter_bounds, 0, views, fine_shift, capacity, fine_ids, fine_ranges, total_dev, workspace,
+                           workspace_bytes, stream);
 }
 
-int rm_fine_lists_multi(const int32_t* sorted_ids, const int32_t* ranges, const float* footprint,
+int rm_fine_lists_multi(const int64_t* sorted_keys, const int32_t* sorted_ids, int64_t n_pairs,
+                        const int64_t* n_pairs_dev, const int32_t* ranges, const float* footprint,
                         const float* jitter_bounds, int64_t n_tets, const rm_camera* cams, int n_views,
                         int fine_shift, int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
                         int64_t* total_dev, void* workspace, size_t workspace_bytes, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_fine_lists_multi", cams, n_views, &views);
     if (rc) return rc;
-    return fine_lists_impl("rm_fine_lists_multi", sorted_ids, ranges, footprint, jitter_bounds, n_tets, views, fine_shift,
-                           capacity, fine_ids, fine_ranges, total_dev, workspace, workspace_bytes, stream);
+    return fine_lists_impl("rm_fine_lists_multi", sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint,
+                           jitter_bounds, n_tets, views, fine_shift, capacity, fine_ids, fine_ranges, total_dev,
+                           workspace, workspace_bytes, stream);
 }
 
 }  // extern "C"

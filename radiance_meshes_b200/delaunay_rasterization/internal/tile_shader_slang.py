@@ -42,7 +42,7 @@ def vertex_and_tile_shader(indices, vertices, cam, render_grid):
     with torch.no_grad():
         lists = R.build_tile_lists(tiles_touched, rect_tile_space, vs_tetra, camst)
         if fs:
-            R.attach_fine_lists(lists.sorted_ids, lists.ranges, camst, fs, footprint)
+            R.attach_fine_lists(lists.sorted_ids, lists.ranges, camst, fs, footprint, lists.sorted_keys)
     mask = tiles_touched > 0
     return lists.sorted_ids, lists.ranges, vs_tetra, circumcenter, mask, rect_tile_space
 

@@ -294,7 +294,7 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
     keys, vals, sk, sv, ranges = out
     if keep_debug:
         return TileLists(sv[:P], ranges, P, offsets, keys[:P], vals[:P], sk[:P])
-    return TileLists(sv[:P], ranges, P)
+    return TileLists(sv[:P], ranges, P, sorted_keys=sk[:P])
 
 
 @dataclass
@@ -328,6 +328,7 @@ class PendingFineLists:
     coarse_key: tuple
     ranges: torch.Tensor
     footprint: torch.Tensor
+    sorted_keys: torch.Tensor
     jitter: torch.Tensor | None = None  # the jitter of `lists` (kept alive so identity stays meaningful)
     jitter_version: int = -1
     lists: FineLists | None = None
@@ -351,18 +352,19 @@ def _cam_key(cam: RMCamera) -> tuple:
 
 
 def attach_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCamera, fine_shift: int,
-                      footprint: torch.Tensor) -> PendingFineLists:
+                      footprint: torch.Tensor, sorted_keys: torch.Tensor) -> PendingFineLists:
     """Record on ``sorted_ids`` (attribute ``rm_fine``) what fine_lists_of needs
     to cut the 2^fine_shift times smaller tiles' lists from these lists."""
-    pend = PendingFineLists(fine_shift, cam, _cam_key(cam), ranges, footprint)
+    pend = PendingFineLists(fine_shift, cam, _cam_key(cam), ranges, footprint, sorted_keys)
     sorted_ids.rm_fine = pend
     return pend
 
 
 def split_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCamera, fine_shift: int,
-                     footprint: torch.Tensor, bounds: torch.Tensor, pool: ScratchPool | None = None) -> FineLists:
-    """Split the sorted coarse lists into the fine lists for the jitter bounds
-    ``bounds`` (rm_fine_lists, no host synchronisation)."""
+                     footprint: torch.Tensor, bounds: torch.Tensor, sorted_keys: torch.Tensor,
+                     pool: ScratchPool | None = None) -> FineLists:
+    """Split the sorted coarse lists (ids and keys) into the fine lists for
+    the jitter bounds ``bounds`` (rm_fine_lists, no host synchronisation)."""
     pool = pool or _POOL
     dev = sorted_ids.device
     camf = fine_camera(cam, fine_shift)
@@ -372,11 +374,13 @@ def split_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCame
     fine_ranges = torch.empty((Gf, 2), dtype=torch.int32, device=dev)
     total = torch.empty(1, dtype=torch.int64, device=dev)
     L = C.lib()
-    ws_n = L.rm_fine_lists_workspace_size(Gf)
+    P = int(sorted_ids.shape[0])
+    ws_n = L.rm_fine_lists_workspace_size(Gf, P, fine_shift)
     ws = pool.get("fine", ws_n, dev)
-    _call("rm_fine_lists", lambda: L.rm_fine_lists(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(footprint), C.ptr(bounds),
-                                                   ctypes.byref(cam), fine_shift, cap, C.ptr(fine_ids),
-                                                   C.ptr(fine_ranges), C.ptr(total), C.ptr(ws), ws_n, _stream()))
+    _call("rm_fine_lists", lambda: L.rm_fine_lists(C.ptr(sorted_keys), C.ptr(sorted_ids), P, None, C.ptr(ranges),
+                                                   C.ptr(footprint), C.ptr(bounds), ctypes.byref(cam), fine_shift,
+                                                   cap, C.ptr(fine_ids), C.ptr(fine_ranges), C.ptr(total), C.ptr(ws),
+                                                   ws_n, _stream()))
     return FineLists(fine_shift, camf, _cam_key(cam), fine_ids, fine_ranges, total)
 
 
@@ -390,7 +394,8 @@ def fine_lists_of(sorted_ids: torch.Tensor, cam: RMCamera, ray_jitter: torch.Ten
     if pend.lists is not None and pend.jitter is ray_jitter and pend.jitter_version == ray_jitter._version:
         return pend.lists
     bounds = jitter_bounds(ray_jitter)
-    pend.lists = split_fine_lists(sorted_ids, pend.ranges, pend.coarse_cam, pend.shift, pend.footprint, bounds)
+    pend.lists = split_fine_lists(sorted_ids, pend.ranges, pend.coarse_cam, pend.shift, pend.footprint, bounds,
+                                  pend.sorted_keys)
     pend.jitter, pend.jitter_version = ray_jitter, ray_jitter._version
     return pend.lists
 

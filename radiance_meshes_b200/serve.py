@@ -100,7 +100,7 @@ def batch_bytes(n_tets: int, views: B.ViewBatch, capacity: int, fine_shift: int 
     blend_tiles = views.n_tiles * q
     tiles = views.n_tiles * 8 + int(L.rm_blend_workspace_size(0, blend_tiles))  # no hit masks (forward only)
     if fine_shift:
-        tiles += (n * n_tets * 48 + capacity * q * 4 + blend_tiles * 8 + int(L.rm_fine_lists_workspace_size(blend_tiles))
+        tiles += (n * n_tets * 48 + capacity * q * 4 + blend_tiles * 8 + int(L.rm_fine_lists_workspace_size(blend_tiles, capacity, fine_shift))
                   + int(L.rm_jitter_bounds_workspace_size()) + 16)
     pixels = views.n_pixels * (8 + 16 + 20 + 4)
     return proj + pairs + tiles + pixels + 4096

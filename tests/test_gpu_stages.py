@@ -128,7 +128,7 @@ def test_fine_lists_split_matches_restatement(cuda, tile, jit):
     assert np.array_equal(jb.cpu().numpy(), np.array([jj[:, 0].min(), jj[:, 1].min(), jj[:, 0].max(),
                                                       jj[:, 1].max()], np.float32))
     coarse = R.build_tile_lists(tiles, rect, vs, cam)
-    fine = R.split_fine_lists(coarse.sorted_ids, coarse.ranges, cam, fs, fp, jb)
+    fine = R.split_fine_lists(coarse.sorted_ids, coarse.ranges, cam, fs, fp, jb, coarse.sorted_keys)
     # restatement: entry e of coarse tile t goes to fine tile q when bit q is set
     ids = coarse.sorted_ids.cpu().numpy()
     rg = coarse.ranges.cpu().numpy()

@@ -55,7 +55,7 @@ def test_calc_tet_err_matches_oracle(cuda, scene):
     t2, r2, vs2, cc2, fp = R.project_fwd_fine(i, v, cam)
     L2 = R.build_tile_lists(t2, r2, vs2, cam)
     half = torch.full((view.height, view.width, 2), 0.5, device="cuda")
-    F = R.split_fine_lists(L2.sorted_ids, L2.ranges, cam, fs, fp, R.jitter_bounds(half))
+    F = R.split_fine_lists(L2.sorted_ids, L2.ranges, cam, fs, fp, R.jitter_bounds(half), L2.sorted_keys)
     err2, cnt2 = R.calc_tet_err(F.sorted_ids, F.ranges, i, v, c, F.cam, to_dev(pe), to_dev(se), tiles_touched=t2)
     _check(err2, cnt2, ref_err, ref_cnt, ref_max)
 
