@@ -136,28 +136,65 @@ __device__ __forceinline__ uint32_t sortable_key(float f) {  // tile_shader.slan
     return (b & 0x80000000u) ? ~b : (b ^ 0x80000000u);
 }
 
-__global__ void __launch_bounds__(256) emit_kernel(const float* __restrict__ vs, const int4* __restrict__ rect,
-                                                   const int32_t* __restrict__ offsets, int64_t n_tets,
-                                                   int32_t grid_w, int64_t capacity,
-                                                   const int64_t* __restrict__ total_dev,
-                                                   int64_t* __restrict__ keys, int32_t* __restrict__ vals,
-                                                   uint32_t* status) {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g == 0 && total_dev && status && *total_dev > capacity) atomicOr(status, RM_STATUS_CAPACITY);
-    if (g >= n_tets) return;
-    const int4 r = __ldg(rect + g);
-    const int32_t cnt = (r.z - r.x) * (r.w - r.y);
-    if (cnt <= 0) return;
-    int64_t off = g == 0 ? 0 : (int64_t)__ldg(offsets + g - 1);
-    const uint64_t fk = sortable_key(__ldg(vs + 3 * g + 2));
-    for (int32_t y = r.y; y < r.w; ++y) {
-        for (int32_t x = r.x; x < r.z; ++x) {
-            if (off < capacity) {
-                keys[off] = (int64_t)(((uint64_t)(uint32_t)(y * grid_w + x) << 32) | fk);
-                vals[off] = (int32_t)g;
-            }
-            ++off;
-        }
+// Flat emission: each CTA writes kEmitPerCta consecutive pairs, each thread
+// kEmitItems of them.  Pair p belongs to the first tet g whose inclusive
+// offset exceeds p; its rank k = p - (exclusive offset of g) walks g's rect
+// row-major, exactly the order of generate_keys' nested loops
+// (tile_shader.slang:51-97), so keys and values are those of the per-tet
+// loop.  The offsets of the tets the CTA's pairs span are staged in shared
+// memory when they fit (the search then runs there), else searched in
+// global memory.  Work per thread is even however large a tet's rect is.
+constexpr int kEmitThreads = 256;
+constexpr int kEmitItems = 4;
+constexpr int kEmitPerCta = kEmitThreads * kEmitItems;
+constexpr int kEmitStage = 2048;
+
+// First index in [lo, hi) with a[index] > p (hi when none).
+__device__ __forceinline__ int64_t upper_bound_i32(const int32_t* a, int64_t lo, int64_t hi, int64_t p) {
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if ((int64_t)a[mid] > p) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kEmitThreads) emit_kernel(const float* __restrict__ vs, const int4* __restrict__ rect,
+                                                            const int32_t* __restrict__ offsets, int64_t n_tets,
+                                                            int32_t grid_w, int64_t capacity,
+                                                            const int64_t* __restrict__ total_dev,
+                                                            int64_t* __restrict__ keys, int32_t* __restrict__ vals,
+                                                            uint32_t* status) {
+    __shared__ int32_t soff[kEmitStage];
+    __shared__ int64_t sg[2];
+    const int64_t n_pairs = min((int64_t)__ldg(offsets + n_tets - 1), capacity);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && total_dev && status && *total_dev > capacity)
+        atomicOr(status, RM_STATUS_CAPACITY);
+    const int64_t p0 = (int64_t)blockIdx.x * kEmitPerCta;
+    if (p0 >= n_pairs) return;
+    const int64_t p1 = min(p0 + kEmitPerCta, n_pairs);  // exclusive
+    if (threadIdx.x < 2) sg[threadIdx.x] = upper_bound_i32(offsets, 0, n_tets, threadIdx.x ? p1 - 1 : p0);
+    __syncthreads();
+    const int64_t g0 = sg[0], g1 = sg[1];
+    const bool staged = g1 - g0 + 1 <= kEmitStage;
+    if (staged)
+        for (int64_t i = threadIdx.x; i <= g1 - g0; i += kEmitThreads) soff[i] = __ldg(offsets + g0 + i);
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kEmitItems; ++it) {
+        const int64_t p = p0 + it * kEmitThreads + threadIdx.x;  // consecutive threads, consecutive pairs
+        if (p >= p1) break;
+        int64_t g;
+        if (staged) g = g0 + upper_bound_i32(soff, 0, g1 - g0 + 1, p);
+        else g = upper_bound_i32(offsets, g0, g1 + 1, p);
+        const int64_t excl = g == 0 ? 0 : (int64_t)__ldg(offsets + g - 1);
+        const int32_t k = (int32_t)(p - excl);
+        const int4 r = __ldg(rect + g);
+        const int32_t w = r.z - r.x;
+        const int32_t y = r.y + k / w, x = r.x + k % w;
+        const uint64_t fk = sortable_key(__ldg(vs + 3 * g + 2));
+        keys[p] = (int64_t)(((uint64_t)(uint32_t)(y * grid_w + x) << 32) | fk);
+        vals[p] = (int32_t)g;
     }
 }
 
@@ -268,9 +305,16 @@ int rm_emit_pairs(const float* vs, const int32_t* rect, const int32_t* offsets, 
     if (!vs || !rect || !offsets || (capacity > 0 && (!keys || !values)))
         return rm_host::fail(RM_EINVAL, "rm_emit_pairs: NULL pointer");
     if ((uintptr_t)rect & 15) return rm_host::fail(RM_EINVAL, "rm_emit_pairs: rect must be 16-byte aligned");
-    const int threads = 256;
-    const int64_t blocks = (n_tets + threads - 1) / threads;
-    rm::emit_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+    if (capacity == 0) {
+        // nothing to write; still flag an overflow of a zero capacity
+        if (status_dev && total_dev)
+            rm::emit_kernel<<<1, rm::kEmitThreads, 0, (cudaStream_t)stream>>>(
+                vs, (const int4*)rect, offsets, n_tets, grid_width, capacity, total_dev, keys, values, status_dev);
+        return rm_host::check_launch("rm_emit_pairs");
+    }
+    const int64_t blocks = (capacity + rm::kEmitPerCta - 1) / rm::kEmitPerCta;
+    if (blocks > 0x7fffffff) return rm_host::fail(RM_EINVAL, "rm_emit_pairs: capacity too large");
+    rm::emit_kernel<<<(unsigned)blocks, rm::kEmitThreads, 0, (cudaStream_t)stream>>>(
         vs, (const int4*)rect, offsets, n_tets, grid_width, capacity, total_dev, keys, values, status_dev);
     return rm_host::check_launch("rm_emit_pairs");
 }
