@@ -5,6 +5,7 @@
 //                   as a single-pass block scan with decoupled look-back
 //   rm_emit_pairs   generate_keys (tile_shader.slang:138-186)
 //   rm_tile_ranges  compute_tile_ranges (tile_shader.slang:188-214)
+#include <algorithm>
 #include <mutex>
 
 #include "rm_internal.cuh"
@@ -198,48 +199,58 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(const float* __restr
     }
 }
 
-// Emission for the stacked projection of a view batch: thread i handles
-// (view i / T, tet i % T) and numbers tiles globally (tile_base + local id).
-__global__ void __launch_bounds__(256) emit_multi_kernel(const float* __restrict__ depth,
-                                                         const int4* __restrict__ rect,
-                                                         const int32_t* __restrict__ offsets, int64_t n_tets,
-                                                         const __grid_constant__ ViewSet views, int64_t capacity,
-                                                         const int64_t* __restrict__ total_dev,
-                                                         int64_t* __restrict__ keys, int32_t* __restrict__ vals,
-                                                         uint32_t* status, const float4* __restrict__ footprint,
-                                                         const float4* __restrict__ jitter_bounds) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0 && total_dev && status && *total_dev > capacity) atomicOr(status, RM_STATUS_CAPACITY);
-    if (i >= n_tets * views.n) return;
-    const int4 r = __ldg(rect + i);
-    const int32_t cnt = (r.z - r.x) * (r.w - r.y);
-    if (cnt <= 0) return;
-    const int v = (int)(i / n_tets);
-    const int64_t g = i - (int64_t)v * n_tets;
-    const int32_t grid_w = views.cams[v].grid_width;
-    const uint32_t tile0 = (uint32_t)views.tiles[v];
-    int64_t off = i == 0 ? 0 : (int64_t)__ldg(offsets + i - 1);
-    const uint64_t fk = sortable_key(__ldg(depth + i));
-    // with footprint: bits 28..31 of the value say which of the tile's 2x2
-    // half-size tiles the tet can reach (bit qy * 2 + qx, footprint_bits)
-    const int tw = views.cams[v].tile_width, th = views.cams[v].tile_height;
-    const int hw = tw >> 1, hh = th >> 1;
-    Footprint fp = {};
-    float4 jb = {0.f, 0.f, 0.f, 0.f};
-    if (footprint) {
-        fp = {__ldg(footprint + 3 * i), __ldg(footprint + 3 * i + 1), __ldg(footprint + 3 * i + 2)};
-        jb = __ldg(jitter_bounds);
-    }
-    for (int32_t y = r.y; y < r.w; ++y) {
-        for (int32_t x = r.x; x < r.z; ++x) {
-            if (off < capacity) {
-                uint32_t q = 0;
-                if (footprint) q = (uint32_t)footprint_bits<2>(fp, jb, x * tw, y * th, hw, hh);
-                keys[off] = (int64_t)(((uint64_t)(tile0 + (uint32_t)(y * grid_w + x)) << 32) | fk);
-                vals[off] = (int32_t)((uint32_t)g | (q << 28));
-            }
-            ++off;
+// Emission for the stacked projection of a view batch, flat like emit_kernel:
+// the items are the (view, tet) pairs in view-major order (item i = view
+// i / T, tet i % T), and tiles are numbered globally (tile_base + local id).
+__global__ void __launch_bounds__(kEmitThreads) emit_multi_kernel(
+    const float* __restrict__ depth, const int4* __restrict__ rect, const int32_t* __restrict__ offsets,
+    int64_t n_tets, const __grid_constant__ ViewSet views, int64_t capacity, const int64_t* __restrict__ total_dev,
+    int64_t* __restrict__ keys, int32_t* __restrict__ vals, uint32_t* status, const float4* __restrict__ footprint,
+    const float4* __restrict__ jitter_bounds) {
+    __shared__ int32_t soff[kEmitStage];
+    __shared__ int64_t sg[2];
+    const int64_t n_items = n_tets * views.n;
+    const int64_t n_pairs = min((int64_t)__ldg(offsets + n_items - 1), capacity);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && total_dev && status && *total_dev > capacity)
+        atomicOr(status, RM_STATUS_CAPACITY);
+    const int64_t p0 = (int64_t)blockIdx.x * kEmitPerCta;
+    if (p0 >= n_pairs) return;
+    const int64_t p1 = min(p0 + kEmitPerCta, n_pairs);  // exclusive
+    if (threadIdx.x < 2) sg[threadIdx.x] = upper_bound_i32(offsets, 0, n_items, threadIdx.x ? p1 - 1 : p0);
+    __syncthreads();
+    const int64_t i0 = sg[0], i1 = sg[1];
+    const bool staged = i1 - i0 + 1 <= kEmitStage;
+    if (staged)
+        for (int64_t k = threadIdx.x; k <= i1 - i0; k += kEmitThreads) soff[k] = __ldg(offsets + i0 + k);
+    __syncthreads();
+    const float4 jb = footprint ? __ldg(jitter_bounds) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 1
+    for (int it = 0; it < kEmitItems; ++it) {
+        const int64_t p = p0 + it * kEmitThreads + threadIdx.x;
+        if (p >= p1) break;
+        int64_t i;
+        if (staged) i = i0 + upper_bound_i32(soff, 0, i1 - i0 + 1, p);
+        else i = upper_bound_i32(offsets, i0, i1 + 1, p);
+        const int64_t excl = i == 0 ? 0 : (int64_t)__ldg(offsets + i - 1);
+        const int32_t k = (int32_t)(p - excl);
+        const int v = (int)(i / n_tets);
+        const int64_t g = i - (int64_t)v * n_tets;
+        const rm_camera& c = views.cams[v];
+        const int4 r = __ldg(rect + i);
+        const int32_t w = r.z - r.x;
+        const int32_t y = r.y + k / w, x = r.x + k % w;
+        const uint64_t fk = sortable_key(__ldg(depth + i));
+        // with footprint: bits 28..31 of the value say which of the tile's 2x2
+        // half-size tiles the tet can reach (bit qy * 2 + qx, footprint_bits)
+        uint32_t q = 0;
+        if (footprint) {
+            const Footprint fp = {__ldg(footprint + 3 * i), __ldg(footprint + 3 * i + 1),
+                                  __ldg(footprint + 3 * i + 2)};
+            q = (uint32_t)footprint_bits<2>(fp, jb, x * c.tile_width, y * c.tile_height, c.tile_width >> 1,
+                                            c.tile_height >> 1);
         }
+        keys[p] = (int64_t)(((uint64_t)((uint32_t)views.tiles[v] + (uint32_t)(y * c.grid_width + x)) << 32) | fk);
+        vals[p] = (int32_t)((uint32_t)g | (q << 28));
     }
 }
 
@@ -340,10 +351,9 @@ int rm_emit_pairs_multi(const float* depth, const int32_t* rect, const int32_t* 
         for (int v = 0; v < n_views; ++v)
             if ((cams[v].tile_width & 1) || (cams[v].tile_height & 1))
                 return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: packed fine masks need even tile sizes");
-    const int threads = 256;
-    const int64_t n = n_tets * n_views;
-    const int64_t blocks = (n + threads - 1) / threads;
-    rm::emit_multi_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+    const int64_t blocks = std::max<int64_t>(1, (capacity + rm::kEmitPerCta - 1) / rm::kEmitPerCta);
+    if (blocks > 0x7fffffff) return rm_host::fail(RM_EINVAL, "rm_emit_pairs_multi: capacity too large");
+    rm::emit_multi_kernel<<<(unsigned)blocks, rm::kEmitThreads, 0, (cudaStream_t)stream>>>(
         depth, (const int4*)rect, offsets, n_tets, views, capacity, total_dev, keys, values, status_dev,
         (const float4*)footprint_2x, (const float4*)jitter_bounds);
     return rm_host::check_launch("rm_emit_pairs_multi");
