@@ -291,7 +291,12 @@ RM_API int rm_jitter_bounds(const float* ray_jitter, int64_t n_pixels, float* bo
  * inside jitter_bounds (rm_jitter_bounds of the ray_jitter that the blend
  * will use): the box grown by 1/64 pixel meets them, and, when the projected
  * vertices are given, no edge of their convex hull has all of them more than
- * 1/16 pixel outside.  So the fine list of a fine tile holds, in the coarse
+ * 1/16 pixel outside.  For a camera whose cam_pos is not the centre of its
+ * world_view (rays and projection then see the scene from different points)
+ * the image points are widened by 2 x focal length x offset / min_t pixels,
+ * and without bound when the two cannot be reconciled (a projective last
+ * row, a matrix that is not a rotation, an offset with min_t <= 0).  So the
+ * fine list of a fine tile holds, in the coarse
  * list's order, every entry of the coarse list that can reach one of its
  * rays, and blending over the fine lists yields the image, log T and
  * distortion of blending over the coarse lists with fewer ray/tet tests

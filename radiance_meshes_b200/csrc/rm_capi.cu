@@ -1,5 +1,6 @@
 // rm_capi.cu - error reporting and shared host-side checks of the C ABI.
 #include <atomic>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -56,6 +57,7 @@ int make_views(const char* who, const rm_camera* cams, int n, rm::ViewSet* out) 
         out->tiles[v] = (int)tiles;
         out->pixels[v] = pixels;
         out->cams[v] = cams[v];
+        out->parallax[v] = parallax_px(cams[v]);
         tiles += (int64_t)cams[v].grid_width * cams[v].grid_height;
         pixels += (int64_t)cams[v].image_width * cams[v].image_height;
         if (tiles >= (1ll << 31)) return fail(RM_EINVAL, "%s: more than 2^31 tiles", who);
@@ -64,8 +66,36 @@ int make_views(const char* who, const rm_camera* cams, int n, rm::ViewSet* out) 
         out->tiles[v] = (int)tiles;
         out->pixels[v] = pixels;
     }
-    for (int v = n; v < RM_MAX_VIEWS; ++v) out->cams[v] = cams[0];
+    for (int v = n; v < RM_MAX_VIEWS; ++v) {
+        out->cams[v] = cams[0];
+        out->parallax[v] = out->parallax[0];
+    }
     return RM_OK;
+}
+
+float parallax_px(const rm_camera& c) {
+    const float* M = c.world_view;
+    if (!(M[12] == 0.f && M[13] == 0.f && M[14] == 0.f && M[15] == 1.f)) return INFINITY;
+    double R[3][3], t[3];
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) R[i][j] = M[4 * i + j];
+        t[i] = M[4 * i + 3];
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            const double d = R[i][0] * R[j][0] + R[i][1] * R[j][1] + R[i][2] * R[j][2] - (i == j ? 1.0 : 0.0);
+            if (!(std::fabs(d) <= 1e-5)) return INFINITY;  // not a rotation: rays and projection disagree
+        }
+    double off2 = 0.0;
+    for (int j = 0; j < 3; ++j) {
+        const double center = -(R[0][j] * t[0] + R[1][j] * t[1] + R[2][j] * t[2]);
+        const double d = (double)c.cam_pos[j] - center;
+        off2 += d * d;
+    }
+    if (off2 == 0.0) return 0.f;
+    if (!(c.min_t > 0.f)) return INFINITY;
+    const double f = std::fmax(std::fabs((double)c.K[0]), std::fabs((double)c.K[4]));
+    return (float)(2.0 * f * std::sqrt(off2) / (double)c.min_t);
 }
 
 }  // namespace rm_host

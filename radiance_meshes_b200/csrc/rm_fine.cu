@@ -132,7 +132,10 @@ __global__ void __launch_bounds__(256) fine_bits_kernel(
                 const int tx = local % c.grid_width, ty = local / c.grid_width;
                 const float4* fp_g = footprint + 3 * ((int64_t)v * n_tets + g);
                 const Footprint fp = {__ldg(fp_g), __ldg(fp_g + 1), __ldg(fp_g + 2)};
-                bits = footprint_bits<f>(fp, jb, tx * c.tile_width, ty * c.tile_height, c.tile_width / f,
+                // the jitter range widened by the view's parallax allowance
+                const float a = views.parallax[v];
+                const float4 jbv = {jb.x - a, jb.y - a, jb.z + a, jb.w + a};
+                bits = footprint_bits<f>(fp, jbv, tx * c.tile_width, ty * c.tile_height, c.tile_width / f,
                                          c.tile_height / f);
                 bits_out[e] = (typename FineBits<FS>::type)bits;
             }

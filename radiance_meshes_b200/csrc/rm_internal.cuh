@@ -168,6 +168,7 @@ struct ViewSet {
     int tiles[RM_MAX_VIEWS + 1];        // tile_base, with tiles[n] = total tiles
     int64_t pixels[RM_MAX_VIEWS + 1];   // pixel_base, with pixels[n] = total pixels
     rm_camera cams[RM_MAX_VIEWS];
+    float parallax[RM_MAX_VIEWS];       // rm_host::parallax_px of each camera
     __device__ __forceinline__ int find(int tile) const {
         int lo = 0, hi = n - 1;  // last view whose first tile is <= tile
         while (lo < hi) {
@@ -277,6 +278,13 @@ int check_cam(const rm_camera* cam);
 // Validates n cameras (n in [1, RM_MAX_VIEWS], one tile size for all) and
 // fills the view table.
 int make_views(const char* who, const rm_camera* cams, int n, rm::ViewSet* out);
+// Pixels by which a ray of the camera can miss the image point its pixel
+// names, at the depths rays reach, because rays start from cam_pos while the
+// projection uses the centre of world_view: 2 x focal length x offset / min_t
+// (rays start min_t along their direction); 0 for a centred camera, infinity
+// when the two cannot be reconciled (projective last row, a matrix that is
+// not a rotation, or an offset with min_t <= 0).
+float parallax_px(const rm_camera& c);
 // True unless the camera is a plain perspective one with all distortion
 // coefficients zero; kernels instantiated for the plain camera leave out the
 // fisheye and distortion code (a conservative test: a camera with tiny

@@ -246,7 +246,9 @@ __global__ void __launch_bounds__(kEmitThreads) emit_multi_kernel(
         if (footprint) {
             const Footprint fp = {__ldg(footprint + 3 * i), __ldg(footprint + 3 * i + 1),
                                   __ldg(footprint + 3 * i + 2)};
-            q = (uint32_t)footprint_bits<2>(fp, jb, x * c.tile_width, y * c.tile_height, c.tile_width >> 1,
+            const float a = views.parallax[v];  // the view's parallax allowance
+            const float4 jbv = {jb.x - a, jb.y - a, jb.z + a, jb.w + a};
+            q = (uint32_t)footprint_bits<2>(fp, jbv, x * c.tile_width, y * c.tile_height, c.tile_width >> 1,
                                             c.tile_height >> 1);
         }
         keys[p] = (int64_t)(((uint64_t)((uint32_t)views.tiles[v] + (uint32_t)(y * c.grid_width + x)) << 32) | fk);

@@ -92,7 +92,7 @@ def test_bad_camera_raises(cuda):
                                RenderGrid(view.height, view.width, 16, 16))
 
 
-def _dropin_step(mesh, view, jitter, fine, tile=16):
+def _dropin_step(mesh, view, jitter, fine, tile=16, cam_shift=None):
     RMB.install_dropin()
     from delaunay_rasterization.internal.alphablend_tiled_slang_interp import AlphaBlendTiledRender
     from delaunay_rasterization.internal.render_grid import RenderGrid
@@ -102,6 +102,8 @@ def _dropin_step(mesh, view, jitter, fine, tile=16):
     R.use_fine_lists(fine)
     try:
         tcam = view.tcam(device="cuda", tile_size=tile)
+        if cam_shift is not None:  # rays from a point off the projection centre
+            tcam["cam_pos"] = tcam["cam_pos"] + torch.tensor(cam_shift, device="cuda")
         grid = RenderGrid(view.height, view.width, tile_width=tile, tile_height=tile)
         verts = to_dev(mesh.vertices).requires_grad_(True)
         cv = to_dev(mesh.cell_values).requires_grad_(True)
@@ -122,7 +124,7 @@ def _dropin_step(mesh, view, jitter, fine, tile=16):
 
 @pytest.mark.parametrize("scene,tile,jit", [("plain", 16, "unit"), ("mixture", 16, "unit"), ("mixture", 32, "unit"),
                                             ("mixture", 16, "half"), ("mixture", 16, "wide"),
-                                            ("plain", 32, "wide")])
+                                            ("plain", 32, "wide"), ("mixture", 16, "offcentre")])
 def test_fine_lists_give_the_coarse_frame(cuda, scene, tile, jit):
     """Blending over the 8x8-pixel lists reproduces the blend over the
     caller's 16x16 / 32x32 lists for any ray jitter (uniform in [0, 1) as in
@@ -136,15 +138,19 @@ def test_fine_lists_give_the_coarse_frame(cuda, scene, tile, jit):
         mesh, view = scenes.workload_training_step(n_points=20000, seed=2, height=420, width=649)
     rng = np.random.default_rng(4)
     shape = (view.height, view.width, 2)
-    if jit == "unit":
+    cam_shift = None
+    if jit == "offcentre":  # rays start 2.3e-5 away from the projection centre
+        j = rng.uniform(0, 1, shape)
+        cam_shift = [2e-5, -1e-5, 5e-6]
+    elif jit == "unit":
         j = rng.uniform(0, 1, shape)
     elif jit == "half":
         j = np.full(shape, 0.5)
     else:
         j = rng.uniform(-1.5, 2.5, shape)
     jitter = torch.from_numpy(j.astype(np.float32)).cuda()
-    ids_c, rg_c, img_c, dist_c, gv_c, gc_c = _dropin_step(mesh, view, jitter, False, tile)
-    ids_f, rg_f, img_f, dist_f, gv_f, gc_f = _dropin_step(mesh, view, jitter, True, tile)
+    ids_c, rg_c, img_c, dist_c, gv_c, gc_c = _dropin_step(mesh, view, jitter, False, tile, cam_shift)
+    ids_f, rg_f, img_f, dist_f, gv_f, gc_f = _dropin_step(mesh, view, jitter, True, tile, cam_shift)
     assert torch.equal(ids_c, ids_f) and torch.equal(rg_c, rg_f)
     assert torch.equal(img_c.view(torch.int32), img_f.view(torch.int32))
     assert torch.equal(dist_c.view(torch.int32), dist_f.view(torch.int32))

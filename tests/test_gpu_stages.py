@@ -94,6 +94,23 @@ def _fine_bits(fp, jb, ox, oy, tw, th, f):
     return bits
 
 
+def _parallax_px(cam):
+    """The library's parallax allowance of a camera (2 x focal x offset of
+    cam_pos from the world_view centre / min_t), restated in float64."""
+    M = [float(x) for x in cam.world_view]
+    R = [[M[4 * i + j] for j in range(3)] for i in range(3)]
+    t = [M[4 * i + 3] for i in range(3)]
+    off2 = 0.0
+    for j in range(3):
+        center = -(R[0][j] * t[0] + R[1][j] * t[1] + R[2][j] * t[2])
+        d = float(cam.cam_pos[j]) - center
+        off2 += d * d
+    if off2 == 0.0:
+        return np.float32(0.0)
+    f = max(abs(float(cam.K[0])), abs(float(cam.K[4])))
+    return np.float32(2.0 * f * np.sqrt(off2) / float(np.float32(cam.min_t)))
+
+
 @pytest.mark.parametrize("tile,jit", [(16, "unit"), (32, "unit"), (16, "half"), (16, "wide")])
 def test_fine_lists_split_matches_restatement(cuda, tile, jit):
     """Splitting the sorted coarse lists (rm_fine_lists) keeps, for every fine
@@ -136,7 +153,10 @@ def test_fine_lists_split_matches_restatement(cuda, tile, jit):
     t_of = np.repeat(np.arange(G), rg[:, 1] - rg[:, 0])
     assert len(t_of) == len(ids)
     tx, ty = t_of % cam.grid_width, t_of // cam.grid_width
+    # the kernels widen the jitter range by the camera's parallax allowance
+    a = _parallax_px(cam)
     jbn = jb.cpu().numpy()
+    jbn = np.array([jbn[0] - a, jbn[1] - a, jbn[2] + a, jbn[3] + a], np.float32)
     bits = _fine_bits(fpn[ids], jbn, tx * tile, ty * tile, tile, tile, f)
     fgw = cam.grid_width * f
     e_all, q_all = np.nonzero((bits[:, None] >> np.arange(f * f)[None, :]) & 1)
