@@ -179,3 +179,36 @@ def test_fine_lists_split_matches_restatement(cuda, tile, jit):
     assert not np.any(bits & ~box_bits)
     n_box = int(((box_bits[:, None] >> np.arange(f * f)[None, :]) & 1).sum())
     assert n < 0.9 * n_box
+
+
+def test_pair_buffers_sized_from_the_previous_frame(cuda):
+    """build_tile_lists sizes the pair buffers from the previous frame's count
+    and queues emission, sort and ranges before reading P; a frame with many
+    more pairs than the last is rebuilt at its exact size.  The lists equal
+    those built with exactly sized buffers, whichever path a frame takes."""
+    from radiance_meshes_b200 import rasterizer as R
+    from radiance_meshes_b200 import scenes
+    from radiance_meshes_b200.camera import tcam_to_struct
+
+    small_mesh, small_view = scenes.workload_plain_forward()
+    big_mesh, big_view = scenes.workload_training_step(n_points=20000, seed=2, height=420, width=649)
+
+    def lists(mesh, view):
+        cam = tcam_to_struct(view.tcam())
+        i = torch.from_numpy(mesh.indices).cuda()
+        v = torch.from_numpy(mesh.vertices).cuda()
+        tiles, rect, vs, cc = R.project_fwd(i, v, cam)
+        L = R.build_tile_lists(tiles, rect, vs, cam, keep_debug=True)
+        return L.sorted_ids.clone(), L.ranges.clone(), L.sorted_keys.clone()
+
+    def exact(mesh, view):
+        R._PAIR_GUESS.clear()  # no previous frame: buffers of exactly P
+        return lists(mesh, view)
+
+    ref_small, ref_big = exact(small_mesh, small_view), exact(big_mesh, big_view)
+    for mesh, view, ref in ((small_mesh, small_view, ref_small), (big_mesh, big_view, ref_big),
+                            (big_mesh, big_view, ref_big), (small_mesh, small_view, ref_small)):
+        got = lists(mesh, view)  # big after small outgrows the small frame's buffers; the others fit
+        for a, b in zip(got, ref):
+            assert torch.equal(a, b)
+    assert ref_big[0].shape[0] > 2 * ref_small[0].shape[0]
