@@ -151,6 +151,32 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def issue_roofline(kernel, launch_ms, tests, clocks, **extra):
+    """The blend kernels are bound by instruction issue, not HBM: the
+    kernel's warp instructions per launch (ray/tet tests of this pass x the
+    instructions per test of the profiled capture, profiles/issue_model.json)
+    over its measured launch time, against the SM's issue peak (148 SMs x 4
+    schedulers x the sampled SM clock)."""
+    out = {"ray_tet_tests_per_pass": tests, **extra}
+    path = os.path.join(ROOT, "profiles", "issue_model.json")
+    if not os.path.exists(path):
+        return out
+    with open(path) as f:
+        model = json.load(f).get(kernel)
+    if not model or not launch_ms:
+        return out
+    import torch
+
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    warp_inst = tests * model["thread_instructions_per_test"] / model["active_lanes_per_instruction"]
+    achieved = warp_inst / (launch_ms * 1e-3) / 1e9
+    peak = sms * 4 * mhz * 1e6 / 1e9
+    out.update({"bound": "issue", "unit": "G warp instructions/s", "achieved": achieved, "peak": peak,
+                "frac": achieved / peak, "instructions_per_test_source": "profiles/issue_model.json"})
+    return out
+
+
 # ------------------------------------------------------------- b200 arm --
 def run_b200(args):
     import torch
@@ -365,8 +391,8 @@ def run_b200(args):
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": achieved / hbm_peak, "peak_source": peak_src, "traffic": traffic,
             "algorithmic_bytes": int(bytes_alg.get(dom, 0)), "avg_launch_ms": dom_ms,
-            "issue": {"ray_tet_tests_per_pass": tests,
-                      "tests_per_s_fwd_plus_bwd": 2 * tests / (total_ms * 1e-3 / args.steps)}}
+            "issue": issue_roofline(dom, dom_ms, tests, clocks.summary(),
+                                    tests_per_s_fwd_plus_bwd=2 * tests / (total_ms * 1e-3 / args.steps))}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
