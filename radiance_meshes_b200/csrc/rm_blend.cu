@@ -767,7 +767,9 @@ __device__ __forceinline__ float hit_grads(const float4* __restrict__ q, f3 o, f
     // plane intersections t = dot(n, vref - o) / dot(n, d)
     const f3 a0 = xyz(q[4]) - o;
     const f3 a1 = xyz(q[5]) - o;
-    const float ge = d_te / is.dene, gx = d_tx / is.denx;
+    // gradient factors only (the hit and its t values are exact above): the
+    // approximate quotient (2 ulp) is far inside the gradients' tolerance
+    const float ge = __fdividef(d_te, is.dene), gx = __fdividef(d_tx, is.denx);
     const f3 ae = is.ie == 3 ? a1 : a0, ax = is.ix == 3 ? a1 : a0;
     const f3 dne = {ge * (ae.x - is.te * d.x), ge * (ae.y - is.te * d.y), ge * (ae.z - is.te * d.z)};
     const f3 dnx = {gx * (ax.x - is.tx * d.x), gx * (ax.y - is.tx * d.y), gx * (ax.z - is.tx * d.z)};
