@@ -260,8 +260,8 @@ RM_API int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges,
  *          lie in front of a pinhole camera without distortion (z > 1e-4, so
  *          nothing is clipped) and within 8192 pixels of the image origin,
  *          NaN otherwise;
- * zeros for culled tets.  The lists of smaller tiles are cut from the coarse
- * lists with it (rm_fine_lists).  No reference counterpart.
+ * rows of culled tets are not written.  The lists of smaller tiles are cut
+ * from the coarse lists with it (rm_fine_lists).  No reference counterpart.
  */
 RM_API int rm_project_fwd_fine(const int32_t* indices, const float* vertices, int64_t n_tets,
                                int64_t n_verts, const rm_camera* cam,
@@ -339,12 +339,14 @@ RM_API int rm_fine_lists(const int64_t* sorted_keys, const int32_t* sorted_ids, 
 
 /*
  * Projection of every tet into every view; each tet's vertices are read once
- * for all views.  Per view the outputs equal rm_project_fwd's: tiles_touched
- * and rect [n_views, T] (rect rows of 4), depth [n_views, T] (rm_project_fwd's
- * vs[:, 2]).  tiles_any [T] (optional) receives the tet's tile count summed
+ * for all views.  Per view the outputs equal rm_project_fwd's where
+ * tiles_touched > 0: tiles_touched and rect [n_views, T] (rect rows of 4),
+ * depth [n_views, T] (rm_project_fwd's vs[:, 2]).  tiles_any [T] (optional) receives the tet's tile count summed
  * over the views; circumcenter [T, 3] (optional) is view-independent.
  * footprint [n_views, T, 12] (optional) receives rm_project_fwd_fine's
- * footprints.
+ * footprints.  Only tiles_touched is written for a (view, tet) without
+ * tiles: its rect, depth and footprint rows are left as they were (the
+ * batched stages never read them).
  */
 RM_API int rm_project_fwd_multi(const int32_t* indices, const float* vertices,
                                 int64_t n_tets, int64_t n_verts,

@@ -349,9 +349,11 @@ __global__ void __launch_bounds__(256) project_fwd_fine_kernel(const int4* __res
     cc[3 * g + 0] = n_tiles ? (float)t.center.x : 0.f;
     cc[3 * g + 1] = n_tiles ? (float)t.center.y : 0.f;
     cc[3 * g + 2] = n_tiles ? (float)t.center.z : 0.f;
-    fp[3 * g] = f.box;
-    fp[3 * g + 1] = f.p01;
-    fp[3 * g + 2] = f.p23;
+    if (n_tiles) {  // only listed tets' footprints are ever read
+        fp[3 * g] = f.box;
+        fp[3 * g + 1] = f.p01;
+        fp[3 * g + 2] = f.p23;
+    }
 }
 
 // All views of a batch: each thread loads its tet once and projects it into
@@ -375,15 +377,20 @@ __global__ void __launch_bounds__(256) project_fwd_multi_kernel(const int4* __re
         int n_tiles;
         if (fp) {
             n_tiles = project_view<GENERAL, true>(views.cams[v], t, r, dk, &f);
-            fp[3 * o] = f.box;
-            fp[3 * o + 1] = f.p01;
-            fp[3 * o + 2] = f.p23;
         } else {
             n_tiles = project_view<GENERAL>(views.cams[v], t, r, dk);
         }
         tiles[o] = n_tiles;
-        rect[o] = r;
-        depth[o] = dk;
+        // the rows of (view, tet) pairs without tiles are never read: not written
+        if (n_tiles) {
+            rect[o] = r;
+            depth[o] = dk;
+            if (fp) {
+                fp[3 * o] = f.box;
+                fp[3 * o + 1] = f.p01;
+                fp[3 * o + 2] = f.p23;
+            }
+        }
         total += n_tiles;
     }
     if (any) any[g] = total;
