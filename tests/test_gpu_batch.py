@@ -201,13 +201,18 @@ def test_autotuner_returns_a_valid_choice(cuda, tmp_path, monkeypatch):
     br.check()
 
 
-@pytest.mark.parametrize("tile,shift", [(16, 1), (32, 1), (32, 2)])
-def test_batch_fine_split_gives_the_coarse_frames(cuda, tile, shift):
+@pytest.mark.parametrize("tile,shift,offcentre", [(16, 1, False), (32, 1, False), (32, 2, False), (16, 1, True),
+                                                  (32, 2, True)])
+def test_batch_fine_split_gives_the_coarse_frames(cuda, tile, shift, offcentre):
     """Lists sorted on the cameras' tiles and split into tiles 2^shift times
     smaller (rm_fine_lists_multi) render every view exactly as the
     single-camera blend over the coarse lists; the gradients are the sum of
-    the single-camera gradients."""
+    the single-camera gradients.  Also with cameras whose rays start a little
+    off their projection centre (the split widens its test per view)."""
     mesh, views, cams = _scene(tile)
+    if offcentre:
+        for k, cam in enumerate(cams):
+            cam.cam_pos[k % 3] += 3e-5 * (k + 1)
     i, v, c = _dev(mesh)
     vb = B.ViewBatch(cams)
     jit = _jitter(vb, seed=6)
