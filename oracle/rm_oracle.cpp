@@ -34,7 +34,7 @@
 // and CUDA; it is compared within a tolerance.
 //
 // The template parameter F selects FP32 (the bit-exact restatement) or FP64
-// (the judge integrator: same closed-form segment integral, double precision).
+// (the reference integrator: same closed-form segment integral, double precision).
 
 #include <algorithm>
 #include <cmath>
@@ -927,7 +927,7 @@ ORC_API void orc_blend_bwd_f32_masked(const int32_t* ids, const int32_t* ranges,
                      tile_mask);
 }
 
-// Stage (d) forward, FP64 judge integrator.  cut (nullable) imposes the
+// Stage (d) forward, FP64 reference integrator.  cut (nullable) imposes the
 // per-pixel list cut of the FP32 path; own_nc (nullable) receives where the
 // FP64 termination rule would stop; inversions (nullable) counts hits whose
 // entry distance goes backwards along the sorted list (power order vs depth).

@@ -7,7 +7,7 @@ colour gradient), with the relative L2 error ||g_gpu - g_ref|| / ||g_ref||:
   * the adjoint evaluated in FP32 with the reference's rounding (the
     reference's own backward, restated): <= 1e-4, and every entry within
     1e-3 |g_ref| + 1e-4 max|g_ref|;
-  * the adjoint evaluated in FP64 (the judge): <= 1e-3, the stated gradient
+  * the adjoint evaluated in FP64 (the exact reference): <= 1e-3, the stated gradient
     tolerance, after removing the 0.1% of entries with the largest deviation
     (<= 5e-3 without trimming).  Rays are jittered randomly; near-tangent
     hits still occur, where d(segment length)/d(vertex) is unbounded.  At pixel
