@@ -208,3 +208,34 @@ def test_tcam_conversion_cache():
     assert c.cam_pos[0] == a.cam_pos[0] + 1.0
     tcam2 = dict(tcam, tile_width=8, tile_height=8, grid_width=12, grid_height=8)
     assert tcam_to_struct(tcam2).tile_width == 8
+
+
+def test_fine_list_entry_points_validate():
+    """The footprint, jitter-bounds and split entry points reject missing or
+    misaligned buffers and bad split factors before touching the device, and
+    size their workspaces from the fine tiles and pairs."""
+    L = C.lib()
+    cam = _cam()
+    cams = (RMCamera * 1)(cam)
+    rc = L.rm_project_fwd_fine(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None, None)
+    assert rc == C.RM_EINVAL and "NULL" in C.last_error()
+    assert L.rm_project_fwd_fine(None, None, 0, 0, ctypes.byref(cam), None, None, None, None, None, None) == C.RM_OK
+    assert L.rm_jitter_bounds_workspace_size() >= 16
+    assert L.rm_jitter_bounds(None, 10, None, None, 0, None) == C.RM_EINVAL
+    assert L.rm_jitter_bounds(8, 10, 16, 16, 0, None) == C.RM_EINVAL and "workspace" in C.last_error()
+    assert L.rm_jitter_bounds(4, 10, 16, 16, 1 << 20, None) == C.RM_EINVAL and "misaligned" in C.last_error()
+    small = L.rm_fine_lists_workspace_size(1000, 10, 1)
+    assert L.rm_fine_lists_workspace_size(1000, 1_000_000, 1) >= small + 1_000_000 - 256
+    assert L.rm_fine_lists_workspace_size(1000, 1_000_000, 3) >= 8 * 1_000_000
+    ws = 1 << 30
+    rc = L.rm_fine_lists(16, 16, 10, None, 16, None, 16, ctypes.byref(cam), 1, 10, 16, 16, 16, 256, ws, None)
+    assert rc == C.RM_EINVAL and "footprint" in C.last_error()
+    rc = L.rm_fine_lists(16, 16, 10, None, 16, 16, None, ctypes.byref(cam), 1, 10, 16, 16, 16, 256, ws, None)
+    assert rc == C.RM_EINVAL and "jitter_bounds" in C.last_error()
+    rc = L.rm_fine_lists(16, 16, 10, None, 16, 16, 16, ctypes.byref(cam), 4, 10, 16, 16, 16, 256, ws, None)
+    assert rc == C.RM_EINVAL and "fine_shift" in C.last_error()
+    rc = L.rm_fine_lists(16, 16, 10, None, 16, 24, 16, ctypes.byref(cam), 1, 10, 16, 16, 16, 256, ws, None)
+    assert rc == C.RM_EINVAL and "misaligned" in C.last_error()
+    # packed bits (no footprint) only for a 2x split
+    rc = L.rm_fine_lists_multi(16, 16, 10, None, 16, None, None, 10, cams, 1, 2, 10, 16, 16, 16, 256, ws, None)
+    assert rc == C.RM_EINVAL and "packed" in C.last_error()
