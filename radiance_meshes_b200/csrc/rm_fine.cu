@@ -194,23 +194,21 @@ __global__ void __launch_bounds__(kFineThreads, 2) fine_write_kernel(
             if (lane == 0) wcnt[warp][q] = __popc(bal);
         }
         __syncthreads();
-        if (warp == 0) {
-            // per fine tile: exclusive prefix over the warps, offset by the
-            // entries of the earlier chunks
-            for (int q = 0; q < Q; ++q) {
-                const uint32_t x = wcnt[lane][q];
-                uint32_t inc = x;
+        // per fine tile (one warp each): exclusive prefix over the warps,
+        // offset by the entries of the earlier chunks
+        for (int q = warp; q < Q; q += kFineWarps) {
+            const uint32_t x = wcnt[lane][q];
+            uint32_t inc = x;
 #pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, off);
-                    if (lane >= off) inc += y;
-                }
-                const uint32_t r0 = run[q];
-                wpre[lane][q] = r0 + inc - x;
-                __syncwarp();
-                if (lane == 31) run[q] = r0 + inc;
-                __syncwarp();
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, inc, off);
+                if (lane >= off) inc += y;
             }
+            const uint32_t r0 = run[q];
+            wpre[lane][q] = r0 + inc - x;
+            __syncwarp();
+            if (lane == 31) run[q] = r0 + inc;
+            __syncwarp();
         }
         __syncthreads();
 #pragma unroll
