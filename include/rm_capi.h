@@ -11,8 +11,16 @@
  * Memory ownership: the caller allocates every buffer, including scratch
  * ("workspace") memory whose size is returned by the *_workspace_size queries
  * (two-phase, as with CUB).  The library itself never calls cudaMalloc on the
- * render path.  All launches are stream-ordered; apart from rm_read_status no
- * call synchronises the host with the device.
+ * render path.  All launches are stream-ordered; apart from rm_read_status and
+ * rm_scan_noalloc_read_status no call synchronises the host with the device.
+ *
+ * Errors found on the device (an index outside [0, n_verts), a non-finite
+ * vertex, a pair count beyond int32, a full buffer, a bounded wait that gave
+ * up) set RM_STATUS_* bits in a caller-visible status word instead of
+ * faulting or stopping the stream; the work item concerned is skipped and
+ * every store stays in bounds.  The reference asserts on the host instead
+ * (delaunay_rasterization/internal/tile_shader_slang.py:78), which would
+ * synchronise the stream.
  *
  * Tensor layouts follow the reference: indices [T,4] int32, vertices [V,3]
  * float32, cell_values [T,7] float32 (density, r, g, b, gx, gy, gz),
@@ -29,7 +37,7 @@
 extern "C" {
 #endif
 
-#define RM_ABI_VERSION 1
+#define RM_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define RM_API __attribute__((visibility("default")))
@@ -44,11 +52,15 @@ extern "C" {
 #define RM_ECUDA 3       /* a CUDA runtime call failed                                */
 #define RM_ETIMEOUT 4    /* a bounded device-side wait gave up (see rm_read_status)   */
 
-/* Bits of the device status word written by kernels that wait on other CTAs. */
-#define RM_STATUS_SCAN_TIMEOUT 0x1u
-#define RM_STATUS_SORT_TIMEOUT 0x2u
-#define RM_STATUS_CAPACITY 0x4u
+/* Bits of a device status word (uint32, or-ed by the kernels, read and
+ * cleared with rm_read_status). */
+#define RM_STATUS_SCAN_TIMEOUT 0x1u   /* a scan look-back gave up (offsets invalid)          */
+#define RM_STATUS_SORT_TIMEOUT 0x2u   /* a sort look-back gave up (order invalid)            */
+#define RM_STATUS_CAPACITY 0x4u       /* more pairs than the buffers hold (retry larger)     */
 #define RM_STATUS_QUEUE_TIMEOUT 0x8u
+#define RM_STATUS_BAD_INDEX 0x10u     /* a tet index outside [0, n_verts): tet culled, unread */
+#define RM_STATUS_NONFINITE 0x20u     /* a tet vertex is NaN or infinite: tet culled          */
+#define RM_STATUS_OVERFLOW 0x40u      /* the pair count exceeds INT32_MAX (int32 offsets)     */
 
 /*
  * Pinhole camera.  Mirrors the reference's TensorCamera/Camera
@@ -87,6 +99,17 @@ RM_API uint64_t rm_launch_count(void);
  */
 RM_API int rm_read_status(const uint32_t* status_dev, uint32_t* status_host, void* stream);
 
+/*
+ * Iteration limit of every bounded device-side wait launched after this call
+ * by any thread of the process (scan and sort look-backs); 0 restores the
+ * default of 2^22 polls (about a second).  A wait that reaches the limit sets
+ * its RM_STATUS_*_TIMEOUT bit and the kernel goes on with every store in
+ * bounds.  Small values make waits give up on purpose (tests of the error
+ * path); there is no other reason to change it.
+ */
+RM_API void rm_set_wait_limit(uint32_t polls);
+RM_API uint32_t rm_wait_limit(void);
+
 /* ---------------------------------------------------------------- stage (a) */
 /*
  * Per-tet projection, cull, tile rectangle and depth key.
@@ -94,11 +117,16 @@ RM_API int rm_read_status(const uint32_t* status_dev, uint32_t* status_host, voi
  * launched by VertexShader.forward (delaunay_rasterization/internal/tile_shader_slang.py:77-105).
  * Every output row is written (culled tets get zeros), so the caller need not
  * zero the outputs.  vs is [T,3] with only column 2 (the float depth key) set,
- * as in the reference.
+ * as in the reference.  A tet with an index outside [0, n_verts) is culled
+ * before any vertex load and sets RM_STATUS_BAD_INDEX; a tet with a NaN or
+ * infinite vertex is culled and sets RM_STATUS_NONFINITE (the reference
+ * asserts on NaN vertices on the host, tile_shader_slang.py:78).  The bits are
+ * or-ed into *status_dev (may be NULL).
  */
 RM_API int rm_project_fwd(const int32_t* indices, const float* vertices, int64_t n_tets,
                    int64_t n_verts, const rm_camera* cam, int32_t* tiles_touched,
-                   int32_t* rect, float* vs, float* circumcenter, void* stream);
+                   int32_t* rect, float* vs, float* circumcenter, uint32_t* status_dev,
+                   void* stream);
 
 /*
  * Adjoint of the projection: dL/dvertices from dL/dvs[:,2] and dL/dcircumcenter
@@ -120,7 +148,10 @@ RM_API size_t rm_scan_workspace_size(int64_t n_tets);
  * written to *total_dev (int64, device memory).  Replaces
  * torch.cumsum(tiles_touched) at delaunay_rasterization/internal/tile_shader_slang.py:36.
  * Single pass with decoupled look-back; a look-back that waits too long sets
- * RM_STATUS_SCAN_TIMEOUT in the workspace status word (first 4 bytes).
+ * RM_STATUS_SCAN_TIMEOUT in the workspace status word (first 4 bytes), and a
+ * total above INT32_MAX (the offsets are int32, as the reference's cumsum)
+ * sets RM_STATUS_OVERFLOW there.  The word keeps its bits across calls until
+ * rm_read_status clears it; the rest of the workspace is reset by every call.
  */
 RM_API int rm_scan_tiles(const int32_t* tiles_touched, int64_t n_tets, int32_t* offsets,
                   int64_t* total_dev, void* workspace, size_t workspace_bytes,
@@ -139,9 +170,21 @@ RM_API int rm_scan_tiles(const int32_t* tiles_touched, int64_t n_tets, int32_t* 
  * different host threads without ordering between them) race and must not be
  * issued.  The call allocates nothing (no cudaMalloc, no allocating library
  * routine); it clears the part of the array that must start at zero itself.
+ * The array's address is looked up once per CUDA context (a context created
+ * after cudaDeviceReset, or another context made current by the driver API,
+ * gets its own lookup).  Timeouts and overflow set their bits in the array's
+ * status word, which rm_scan_noalloc_read_status reads.
  */
 RM_API int rm_scan_tiles_noalloc(const int32_t* tiles_touched, int64_t n_tets, int32_t* offsets,
                                  int64_t* total_dev, void* stream);
+
+/*
+ * Reads and clears the status word (RM_STATUS_* bits) of the fixed scratch of
+ * rm_scan_tiles_noalloc in the current context, after the work queued on
+ * `stream`; synchronises `stream`.  Allocates nothing.  No counterpart in the
+ * reference.
+ */
+RM_API int rm_scan_noalloc_read_status(uint32_t* status_host, void* stream);
 
 /*
  * Tile/tet pair emission: key = (tile_id << 32) | sortable(depth), value = tet
@@ -168,12 +211,14 @@ RM_API size_t rm_sort_workspace_size(int64_t n);
  * (delaunay_rasterization/internal/tile_shader_slang.py:57-59).
  * n is the buffer capacity; if n_dev is non-NULL the pair count is read from
  * device memory (<= n) so the call can be captured in a CUDA graph.
- * Inputs are not modified.  Look-back waits are bounded (RM_STATUS_SORT_TIMEOUT).
+ * Inputs are not modified.  Look-back waits are bounded: one that gives up
+ * sets RM_STATUS_SORT_TIMEOUT in *status_dev, or, when status_dev is NULL, in
+ * the workspace's status word (its first 4 bytes).
  */
 RM_API int rm_sort_pairs(const int64_t* keys_in, const int32_t* values_in, int64_t n,
                   const int64_t* n_dev, int end_bit, int64_t* keys_out,
                   int32_t* values_out, void* workspace, size_t workspace_bytes,
-                  void* stream);
+                  uint32_t* status_dev, void* stream);
 
 /*
  * Per-tile [start, end) ranges of the sorted pair list; empty tiles get [0,0].
@@ -261,12 +306,14 @@ RM_API int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges,
  *          nothing is clipped) and within 8192 pixels of the image origin,
  *          NaN otherwise;
  * rows of culled tets are not written.  The lists of smaller tiles are cut
- * from the coarse lists with it (rm_fine_lists).  No reference counterpart.
+ * from the coarse lists with it (rm_fine_lists).  Index and vertex checks and
+ * status_dev as rm_project_fwd.  No reference counterpart.
  */
 RM_API int rm_project_fwd_fine(const int32_t* indices, const float* vertices, int64_t n_tets,
                                int64_t n_verts, const rm_camera* cam,
                                int32_t* tiles_touched, int32_t* rect, float* vs,
-                               float* circumcenter, float* footprint, void* stream);
+                               float* circumcenter, float* footprint, uint32_t* status_dev,
+                               void* stream);
 
 /*
  * Bounds of the per-pixel ray jitter [n_pixels, 2]: bounds [4] on the device
@@ -305,7 +352,10 @@ RM_API int rm_jitter_bounds(const float* ray_jitter, int64_t n_pixels, float* bo
  * 4^fine_shift * P always suffices) and fine_ranges [G * 4^fine_shift, 2] on
  * the fine grid, *total_dev = fine pair count.  fine_shift is 1, 2 or 3.
  * Workspace: rm_fine_lists_workspace_size(fine tiles, n_pairs, fine_shift),
- * 256-byte aligned.  No reference counterpart.
+ * 256-byte aligned.  The split's own scan look-back and a fine list longer
+ * than capacity set RM_STATUS_SCAN_TIMEOUT / RM_STATUS_CAPACITY in
+ * *status_dev (status_dev may be NULL: the bits then stay in the workspace).
+ * No reference counterpart.
  */
 RM_API size_t rm_fine_lists_workspace_size(int64_t n_fine_tiles, int64_t n_pairs, int fine_shift);
 RM_API int rm_fine_lists(const int64_t* sorted_keys, const int32_t* sorted_ids, int64_t n_pairs,
@@ -314,7 +364,7 @@ RM_API int rm_fine_lists(const int64_t* sorted_keys, const int32_t* sorted_ids, 
                          const rm_camera* cam, int fine_shift,
                          int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
                          int64_t* total_dev, void* workspace, size_t workspace_bytes,
-                         void* stream);
+                         uint32_t* status_dev, void* stream);
 
 /* ------------------------------------------------------- batched views -- */
 /*
@@ -346,14 +396,16 @@ RM_API int rm_fine_lists(const int64_t* sorted_keys, const int32_t* sorted_ids, 
  * footprint [n_views, T, 12] (optional) receives rm_project_fwd_fine's
  * footprints.  Only tiles_touched is written for a (view, tet) without
  * tiles: its rect, depth and footprint rows are left as they were (the
- * batched stages never read them).
+ * batched stages never read them).  Index and vertex checks and status_dev
+ * as rm_project_fwd.
  */
 RM_API int rm_project_fwd_multi(const int32_t* indices, const float* vertices,
                                 int64_t n_tets, int64_t n_verts,
                                 const rm_camera* cams, int n_views,
                                 int32_t* tiles_touched, int32_t* rect,
                                 float* depth, int32_t* tiles_any,
-                                float* circumcenter, float* footprint, void* stream);
+                                float* circumcenter, float* footprint,
+                                uint32_t* status_dev, void* stream);
 
 /*
  * rm_fine_lists for a view batch: the coarse lists of all views (global
@@ -365,7 +417,8 @@ RM_API int rm_project_fwd_multi(const int32_t* indices, const float* vertices,
  * grids that much larger) over these lists gives the coarse batch's images
  * bit for bit.  footprint (and jitter_bounds) may be NULL when fine_shift is 1 and
  * the sorted values carry the packed 2x2 coverage bits of
- * rm_emit_pairs_multi; fine_ids then hold the plain tet ids.
+ * rm_emit_pairs_multi; fine_ids then hold the plain tet ids.  status_dev as
+ * rm_fine_lists.
  */
 RM_API int rm_fine_lists_multi(const int64_t* sorted_keys, const int32_t* sorted_ids, int64_t n_pairs,
                                const int64_t* n_pairs_dev, const int32_t* ranges,
@@ -373,7 +426,7 @@ RM_API int rm_fine_lists_multi(const int64_t* sorted_keys, const int32_t* sorted
                                const rm_camera* cams, int n_views, int fine_shift,
                                int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
                                int64_t* total_dev, void* workspace, size_t workspace_bytes,
-                               void* stream);
+                               uint32_t* status_dev, void* stream);
 
 /*
  * Pair emission for the stacked projection: offsets is the inclusive scan of
@@ -403,7 +456,8 @@ RM_API int64_t rm_views_tile_count(const rm_camera* cams, int n_views);
  * Per-tet records of the blend kept outside the workspace, so that several
  * batches on one mesh (possibly in flight on different streams) read one
  * copy: rm_blend_records_size(T) bytes, filled by rm_blend_pack_records
- * (tiles_touched may be NULL: every tet is packed).  No reference
+ * (tiles_touched may be NULL: every tet is packed; a tet with an index outside
+ * [0, n_verts) gets an all-zero record, which no ray hits).  No reference
  * counterpart (the reference reloads each tet from its index and vertex
  * arrays for every pixel batch, alphablend_shader_interp.slang:221-232).
  */
@@ -474,9 +528,10 @@ RM_API int rm_calc_tet_err(const int32_t* sorted_ids, const int32_t* ranges,
  * rgb [T,3], grd [T,3], sh_rest [T, n_rest, 3] (SH rows 1.. of degree
  * sh_degree <= 4; n_rest >= (sh_degree + 1)^2 - 1), camera_center (3 floats,
  * host memory).  Out: features [T,7] = (density, softplus_10(colour at v0
- * evaluated through the SH), grd * min(rgb) / |v0 - circumcenter|).
+ * evaluated through the SH), grd * min(rgb) / |v0 - circumcenter|).  A tet
+ * with an index outside [0, n_verts) gets zero features and no gradients.
  */
-RM_API int rm_activate_features(const int32_t* indices, const float* vertices,
+RM_API int rm_activate_features(const int32_t* indices, const float* vertices, int64_t n_verts,
                                 const float* circumcenters, const float* density,
                                 const float* rgb, const float* grd, const float* sh_rest,
                                 int n_rest, int sh_degree, const float* camera_center,
@@ -487,7 +542,7 @@ RM_API int rm_activate_features(const int32_t* indices, const float* vertices,
  * accumulates grad_vertices [V,3] (the mean and |v0 - circumcenter| carry
  * gradient; the vertex offsets inside the colour are detached, as in the
  * reference). */
-RM_API int rm_activate_features_bwd(const int32_t* indices, const float* vertices,
+RM_API int rm_activate_features_bwd(const int32_t* indices, const float* vertices, int64_t n_verts,
                                     const float* circumcenters, const float* density,
                                     const float* rgb, const float* grd, const float* sh_rest,
                                     int n_rest, int sh_degree, const float* camera_center,

@@ -209,9 +209,11 @@ class BatchedRasterizer:
         fp = self.footprint if self.fine_shift else None
         R._call("rm_project_fwd_multi", lambda: L.rm_project_fwd_multi(
             C.ptr(self.indices), C.ptr(self.vertices), self.T, self.V, v.array, v.n, C.ptr(self.tiles),
-            C.ptr(self.rect), C.ptr(self.depth), C.ptr(self.tiles_any), None, C.ptr(fp), s))
+            C.ptr(self.rect), C.ptr(self.depth), C.ptr(self.tiles_any), None, C.ptr(fp), C.ptr(self.status), s))
         R._call("rm_scan_tiles", lambda: L.rm_scan_tiles(C.ptr(self.tiles), nT, C.ptr(self.offsets), C.ptr(self.total),
                                 C.ptr(self.scan_ws), self.scan_ws.numel(), s))
+        # the scan's timeout / overflow bits (its workspace's status word) join the batch's status word
+        self.status.bitwise_or_(self.scan_ws[:4].view(torch.int32))
 
     def _lists(self):
         L, s, v = C.lib(), C.stream_handle(), self.views
@@ -230,7 +232,7 @@ class BatchedRasterizer:
             C.ptr(self.total), C.ptr(self.keys), C.ptr(self.vals), C.ptr(self.status), C.ptr(fp), C.ptr(jb), s))
         R._call("rm_sort_pairs", lambda: L.rm_sort_pairs(C.ptr(self.keys), C.ptr(self.vals), self.capacity, C.ptr(self.total), v.end_bit,
                                 C.ptr(self.sorted_keys), C.ptr(self.sorted_ids), C.ptr(self.sort_ws),
-                                self.sort_ws.numel(), s))
+                                self.sort_ws.numel(), C.ptr(self.status), s))
         R._call("rm_tile_ranges", lambda: L.rm_tile_ranges(C.ptr(self.sorted_keys), self.capacity, C.ptr(self.total), C.ptr(self.ranges),
                                  v.n_tiles, s))
         if self.fine_shift:
@@ -239,7 +241,7 @@ class BatchedRasterizer:
                 C.ptr(self.ranges), None if packed else C.ptr(self.footprint),
                 None if packed else C.ptr(self.jitter_bounds), self.T, v.array, v.n,
                 self.fine_shift, self.fine_ids.shape[0], C.ptr(self.fine_ids), C.ptr(self.fine_ranges),
-                C.ptr(self.fine_total), C.ptr(self.fine_ws), self.fine_ws.numel(), s))
+                C.ptr(self.fine_total), C.ptr(self.fine_ws), self.fine_ws.numel(), C.ptr(self.status), s))
 
     def _blend_lists(self):
         """(sorted ids, ranges, views) that the blend walks."""
@@ -289,8 +291,16 @@ class BatchedRasterizer:
         return self.grad_vertices, self.grad_cell_values
 
     def check(self) -> None:
-        """Synchronise and raise if the last frame overflowed the pair buffers."""
+        """Synchronise and raise if the last frame overflowed the pair buffers
+        or a kernel reported an error in the batch's status word (bad index,
+        non-finite vertex, int32 overflow, a wait that gave up: raised as
+        ``_capi.DeviceStatusError``).  The status word is cleared."""
         P = int(self.total.item())
+        bits = int(self.status.item()) & 0xffffffff
+        self.status.zero_()
+        self.scan_ws[:4].zero_()
+        if bits & ~C.RM_STATUS_CAPACITY:
+            raise C.DeviceStatusError(bits & ~C.RM_STATUS_CAPACITY, "BatchedRasterizer")
         if P > self.capacity:
             raise RuntimeError(f"pair capacity {self.capacity} exceeded ({P} pairs): call ensure_capacity()")
 

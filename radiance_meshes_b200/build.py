@@ -52,13 +52,21 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
     out = lib_path()
     if not force and not _stale(out, deps):
         return out
-    objs = []
-    for src in srcs:
+    def compile_one(src):
         obj = os.path.join(LIBDIR, os.path.basename(src).replace(".cu", ".o"))
         cmd = [nvcc(), *NVCC_FLAGS, *(extra_flags or []), "-c", src, "-o", obj]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, obj, cmd, r
+
+    # the translation units are independent: compile them concurrently
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, srcs))
+    objs = []
+    for src, obj, cmd, r in results:
         if verbose:
             print(" ".join(cmd), flush=True)
-        r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
         if verbose and (r.stdout or r.stderr):

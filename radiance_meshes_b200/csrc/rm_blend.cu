@@ -37,13 +37,21 @@ constexpr int kNGrad = 25;
 
 
 // ------------------------------------------------------------------ packing --
+// A tet with an index outside [0, n_verts) gets an all-zero record: zero
+// normals and zero density, so no ray hits it, and its vertices are never read.
 __global__ void __launch_bounds__(256) pack_kernel(const int4* __restrict__ indices, const float* __restrict__ verts,
-                                                   const float* __restrict__ cv, int64_t n_tets,
+                                                   int64_t n_verts, const float* __restrict__ cv, int64_t n_tets,
                                                    const int32_t* __restrict__ tiles, float4* __restrict__ recs) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_tets) return;
     if (tiles && __ldg(tiles + g) <= 0) return;
     const int4 id = __ldg(indices + g);
+    if (!tet_indices_ok(id, n_verts)) {
+        float4* r = recs + (int64_t)kRecFloat4 * g;
+#pragma unroll
+        for (int k = 0; k < kRecFloat4; ++k) r[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
     const int ids[4] = {id.x, id.y, id.z, id.w};
     f3 v[4];
 #pragma unroll
@@ -1644,11 +1652,11 @@ int batch_size(int flags, int def) {
     return req ? (1 << req) : def;
 }
 
-int pack(const int32_t* indices, const float* vertices, const float* cv, int64_t n_tets, const int32_t* tiles,
-         float4* recs, cudaStream_t s) {
+int pack(const int32_t* indices, const float* vertices, int64_t n_verts, const float* cv, int64_t n_tets,
+         const int32_t* tiles, float4* recs, cudaStream_t s) {
     const int threads = 256;
     const int64_t blocks = (n_tets + threads - 1) / threads;
-    pack_kernel<<<(unsigned)blocks, threads, 0, s>>>((const int4*)indices, vertices, cv, n_tets, tiles, recs);
+    pack_kernel<<<(unsigned)blocks, threads, 0, s>>>((const int4*)indices, vertices, n_verts, cv, n_tets, tiles, recs);
     return rm_host::check_launch("rm_blend pack");
 }
 
@@ -1679,7 +1687,8 @@ int check_blend_args(const char* who, const int32_t* indices, const float* verti
 
 template <class V>
 int blend_fwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
-                  const float* vertices, const float* cell_values, int64_t n_tets, const int32_t* tiles_touched,
+                  const float* vertices, const float* cell_values, int64_t n_tets, int64_t n_verts,
+                  const int32_t* tiles_touched,
                   const float* ray_jitter, const rm_camera* cam0, const V& views, const Shape& sh, float* out_img,
                   float* out_distortion, int32_t* n_contrib, const void* records, void* workspace,
                   size_t workspace_bytes, int flags, void* stream) {
@@ -1695,7 +1704,7 @@ int blend_fwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
         if ((uintptr_t)records & 15) return rm_host::fail(RM_EINVAL, "%s: records must be 16-byte aligned", who);
         w.recs = (float4*)records;  // packed by rm_blend_pack_records
     } else if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
-        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
+        rc = pack(indices, vertices, n_verts, cell_values, n_tets, tiles_touched, w.recs, s);
         if (rc) return rc;
     }
     // measured on the 1.3M-tet workload: every tile through the pair kernel, 4 CTAs/SM
@@ -1721,7 +1730,8 @@ int blend_fwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
 
 template <class V>
 int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
-                  const float* vertices, const float* cell_values, int64_t n_tets, const int32_t* tiles_touched,
+                  const float* vertices, const float* cell_values, int64_t n_tets, int64_t n_verts,
+                  const int32_t* tiles_touched,
                   const float* ray_jitter, const rm_camera* cam0, const V& views, const Shape& sh,
                   const float* out_img, const float* out_distortion, const int32_t* n_contrib, const float* grad_img,
                   const float* grad_distortion, float* grad_vertices, float* grad_cell_values, const void* records,
@@ -1740,7 +1750,7 @@ int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
         if ((uintptr_t)records & 15) return rm_host::fail(RM_EINVAL, "%s: records must be 16-byte aligned", who);
         w.recs = (float4*)records;  // packed by rm_blend_pack_records
     } else if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
-        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
+        rc = pack(indices, vertices, n_verts, cell_values, n_tets, tiles_touched, w.recs, s);
         if (rc) return rc;
     }
     // measured: the one-thread-per-pixel backward alone is fastest
@@ -1794,7 +1804,7 @@ int rm_calc_tet_err(const int32_t* sorted_ids, const int32_t* ranges, const int3
     cudaStream_t s = (cudaStream_t)stream;
     const BlendWs w = blend_ws(workspace, n_tets, G, workspace_bytes);
     if (!(flags & RM_BLEND_REUSE_RECORDS) && n_tets > 0) {
-        rc = pack(indices, vertices, cell_values, n_tets, tiles_touched, w.recs, s);
+        rc = pack(indices, vertices, n_verts, cell_values, n_tets, tiles_touched, w.recs, s);
         if (rc) return rc;
     }
     // every tile in one heavy-first queue (heavy_shift 1 marks all tiles heavy)
@@ -1826,7 +1836,8 @@ int rm_blend_pack_records(const int32_t* indices, const float* vertices, const f
         return rm_host::fail(RM_EINVAL, "rm_blend_pack_records: NULL pointer");
     if (((uintptr_t)indices & 15) || ((uintptr_t)records & 15))
         return rm_host::fail(RM_EINVAL, "rm_blend_pack_records: indices and records must be 16-byte aligned");
-    return rm::pack(indices, vertices, cell_values, n_tets, tiles_touched, (float4*)records, (cudaStream_t)stream);
+    return rm::pack(indices, vertices, n_verts, cell_values, n_tets, tiles_touched, (float4*)records,
+                    (cudaStream_t)stream);
 }
 
 int rm_blend_fwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices, const float* vertices,
@@ -1837,7 +1848,7 @@ int rm_blend_fwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t
     if (rc) return rc;
     const rm::OneView one = {*cam};
     const rm::Shape sh = {cam->grid_width * cam->grid_height, cam->tile_width * cam->tile_height};
-    return rm::blend_fwd_any("rm_blend_fwd", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
+    return rm::blend_fwd_any("rm_blend_fwd", sorted_ids, ranges, indices, vertices, cell_values, n_tets, n_verts,
                              tiles_touched, ray_jitter, cam, one, sh, out_img, out_distortion, n_contrib, nullptr,
                              workspace, workspace_bytes, flags, stream);
 }
@@ -1851,7 +1862,7 @@ int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t
     if (rc) return rc;
     const rm::OneView one = {*cam};
     const rm::Shape sh = {cam->grid_width * cam->grid_height, cam->tile_width * cam->tile_height};
-    return rm::blend_bwd_any("rm_blend_bwd", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
+    return rm::blend_bwd_any("rm_blend_bwd", sorted_ids, ranges, indices, vertices, cell_values, n_tets, n_verts,
                              tiles_touched, ray_jitter, cam, one, sh, out_img, out_distortion, n_contrib, grad_img,
                              grad_distortion, grad_vertices, grad_cell_values, nullptr, workspace, workspace_bytes,
                              flags, stream);
@@ -1866,7 +1877,7 @@ int rm_blend_fwd_multi(const int32_t* sorted_ids, const int32_t* ranges, const i
     int rc = rm_host::make_views("rm_blend_fwd_multi", cams, n_views, &views);
     if (rc) return rc;
     const rm::Shape sh = {views.tiles[n_views], cams[0].tile_width * cams[0].tile_height};
-    return rm::blend_fwd_any("rm_blend_fwd_multi", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
+    return rm::blend_fwd_any("rm_blend_fwd_multi", sorted_ids, ranges, indices, vertices, cell_values, n_tets, n_verts,
                              tiles_touched, ray_jitter, cams, views, sh, out_img, out_distortion, n_contrib,
                              records, workspace, workspace_bytes, flags, stream);
 }
@@ -1882,7 +1893,7 @@ int rm_blend_bwd_multi(const int32_t* sorted_ids, const int32_t* ranges, const i
     int rc = rm_host::make_views("rm_blend_bwd_multi", cams, n_views, &views);
     if (rc) return rc;
     const rm::Shape sh = {views.tiles[n_views], cams[0].tile_width * cams[0].tile_height};
-    return rm::blend_bwd_any("rm_blend_bwd_multi", sorted_ids, ranges, indices, vertices, cell_values, n_tets,
+    return rm::blend_bwd_any("rm_blend_bwd_multi", sorted_ids, ranges, indices, vertices, cell_values, n_tets, n_verts,
                              tiles_touched, ray_jitter, cams, views, sh, out_img, out_distortion, n_contrib,
                              grad_img, grad_distortion, grad_vertices, grad_cell_values, records, workspace,
                              workspace_bytes, flags, stream);

@@ -10,6 +10,8 @@
 namespace {
 thread_local char g_last_error[512] = {0};
 std::atomic<uint64_t> g_launches{0};
+constexpr uint32_t kDefaultWaitLimit = 1u << 22;
+std::atomic<uint32_t> g_wait_limit{kDefaultWaitLimit};
 }
 
 namespace rm_host {
@@ -21,6 +23,8 @@ int fail(int code, const char* fmt, ...) {
     va_end(ap);
     return code;
 }
+
+uint32_t wait_limit() { return g_wait_limit.load(std::memory_order_relaxed); }
 
 int check_launch(const char* what, int kernels) {
     g_launches.fetch_add((uint64_t)kernels, std::memory_order_relaxed);
@@ -107,6 +111,12 @@ const char* rm_last_error(void) { return g_last_error; }
 int rm_abi_version(void) { return RM_ABI_VERSION; }
 
 uint64_t rm_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+void rm_set_wait_limit(uint32_t polls) {
+    g_wait_limit.store(polls ? polls : kDefaultWaitLimit, std::memory_order_relaxed);
+}
+
+uint32_t rm_wait_limit(void) { return g_wait_limit.load(std::memory_order_relaxed); }
 
 int rm_read_status(const uint32_t* status_dev, uint32_t* status_host, void* stream) {
     if (!status_dev || !status_host) return rm_host::fail(RM_EINVAL, "rm_read_status: NULL pointer");

@@ -83,7 +83,7 @@ __device__ __forceinline__ f3 vload(const float* p, int i) {
 
 template <int DEG, bool BWD>
 __global__ void __launch_bounds__(128) features_kernel(
-    const int4* __restrict__ indices, const float* __restrict__ verts, const float* __restrict__ ccs,
+    const int4* __restrict__ indices, const float* __restrict__ verts, int64_t n_verts, const float* __restrict__ ccs,
     const float* __restrict__ density, const float* __restrict__ rgb, const float* __restrict__ grd,
     const float* __restrict__ sh, int n_rest, f3 cam, int64_t n_tets, float* __restrict__ feat,
     const float* __restrict__ gfeat, float* __restrict__ g_density, float* __restrict__ g_rgb,
@@ -92,6 +92,18 @@ __global__ void __launch_bounds__(128) features_kernel(
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_tets) return;
     const int4 id = __ldg(indices + t);
+    if (!tet_indices_ok(id, n_verts)) {  // zero features, no gradients; the vertices are never read
+        if (!BWD) {
+#pragma unroll
+            for (int k = 0; k < 7; ++k) feat[7 * t + k] = 0.f;
+        } else {
+            g_density[t] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) g_rgb[3 * t + k] = g_grd[3 * t + k] = g_cc[3 * t + k] = 0.f;
+            for (int k = 0; k < 3 * n_rest; ++k) g_sh[(int64_t)3 * n_rest * t + k] = 0.f;
+        }
+        return;
+    }
     const int vid[4] = {id.x, id.y, id.z, id.w};
     f3 v[4];
 #pragma unroll
@@ -232,7 +244,8 @@ __global__ void __launch_bounds__(128) features_kernel(
 }
 
 template <bool BWD>
-int launch_features(int deg, const int32_t* indices, const float* vertices, const float* ccs, const float* density,
+int launch_features(int deg, const int32_t* indices, const float* vertices, int64_t n_verts, const float* ccs,
+                    const float* density,
                     const float* rgb, const float* grd, const float* sh, int n_rest, const float* cam, int64_t T,
                     float* feat, const float* gfeat, float* gd, float* grgb, float* ggrd, float* gsh, float* gv,
                     float* gcc, cudaStream_t s) {
@@ -240,7 +253,8 @@ int launch_features(int deg, const int32_t* indices, const float* vertices, cons
     const int64_t blocks = (T + threads - 1) / threads;
     const f3 c = {cam[0], cam[1], cam[2]};
 #define RM_FEAT(D)                                                                                              \
-    features_kernel<D, BWD><<<(unsigned)blocks, threads, 0, s>>>((const int4*)indices, vertices, ccs, density,    \
+    features_kernel<D, BWD><<<(unsigned)blocks, threads, 0, s>>>((const int4*)indices, vertices, n_verts, ccs,    \
+                                                                 density,                                         \
                                                                  rgb, grd, sh, n_rest, c, T, feat, gfeat, gd,      \
                                                                  grgb, ggrd, gsh, gv, gcc)
     switch (deg) {
@@ -273,19 +287,21 @@ int check_features(const char* who, const int32_t* indices, const float* vertice
 
 extern "C" {
 
-int rm_activate_features(const int32_t* indices, const float* vertices, const float* circumcenters,
+int rm_activate_features(const int32_t* indices, const float* vertices, int64_t n_verts, const float* circumcenters,
                          const float* density, const float* rgb, const float* grd, const float* sh_rest, int n_rest,
                          int sh_degree, const float* camera_center, int64_t n_tets, float* features, void* stream) {
     int rc = rm::check_features("rm_activate_features", indices, vertices, circumcenters, density, rgb, grd, sh_rest,
                                 n_rest, sh_degree, camera_center, n_tets);
     if (rc || n_tets == 0) return rc;
     if (!features) return rm_host::fail(RM_EINVAL, "rm_activate_features: NULL output");
-    return rm::launch_features<false>(sh_degree, indices, vertices, circumcenters, density, rgb, grd, sh_rest, n_rest,
+    if (n_verts < 0) return rm_host::fail(RM_EINVAL, "rm_activate_features: negative vertex count");
+    return rm::launch_features<false>(sh_degree, indices, vertices, n_verts, circumcenters, density, rgb, grd, sh_rest, n_rest,
                                       camera_center, n_tets, features, nullptr, nullptr, nullptr, nullptr, nullptr,
                                       nullptr, nullptr, (cudaStream_t)stream);
 }
 
-int rm_activate_features_bwd(const int32_t* indices, const float* vertices, const float* circumcenters,
+int rm_activate_features_bwd(const int32_t* indices, const float* vertices, int64_t n_verts,
+                             const float* circumcenters,
                              const float* density, const float* rgb, const float* grd, const float* sh_rest,
                              int n_rest, int sh_degree, const float* camera_center, int64_t n_tets,
                              const float* grad_features, float* grad_density, float* grad_rgb, float* grad_grd,
@@ -296,7 +312,8 @@ int rm_activate_features_bwd(const int32_t* indices, const float* vertices, cons
     if (!grad_features || !grad_density || !grad_rgb || !grad_grd || !grad_vertices || !grad_circumcenters ||
         (n_rest > 0 && !grad_sh_rest))
         return rm_host::fail(RM_EINVAL, "rm_activate_features_bwd: NULL pointer");
-    return rm::launch_features<true>(sh_degree, indices, vertices, circumcenters, density, rgb, grd, sh_rest, n_rest,
+    if (n_verts < 0) return rm_host::fail(RM_EINVAL, "rm_activate_features_bwd: negative vertex count");
+    return rm::launch_features<true>(sh_degree, indices, vertices, n_verts, circumcenters, density, rgb, grd, sh_rest, n_rest,
                                      camera_center, n_tets, nullptr, grad_features, grad_density, grad_rgb, grad_grd,
                                      grad_sh_rest, grad_vertices, grad_circumcenters, (cudaStream_t)stream);
 }

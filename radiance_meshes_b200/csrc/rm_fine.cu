@@ -273,12 +273,13 @@ template <bool PACKED, int FS>
 int launch_split(const int64_t* keys, const int32_t* ids, int64_t n_pairs, const int64_t* n_pairs_dev,
                  const int32_t* ranges, const float* footprint, const float* jitter_bounds, int64_t n_tets,
                  const rm::ViewSet& views, int64_t G, int64_t Gf, int64_t capacity, int32_t* fine_ids,
-                 int32_t* fine_ranges, int64_t* total_dev, char* ws, cudaStream_t s) {
+                 int32_t* fine_ranges, int64_t* total_dev, char* ws, uint32_t* status_dev, cudaStream_t s) {
     using Bits = typename rm::FineBits<FS>::type;
     int32_t* counts = (int32_t*)ws;
     int32_t* incl = (int32_t*)(ws + rm::align256((size_t)Gf * 4));
     char* scan_ws = ws + 2 * rm::align256((size_t)Gf * 4) + 256;
-    uint32_t* status = (uint32_t*)scan_ws;  // the scan workspace's status word
+    // the caller's status word, else the scan workspace's own
+    uint32_t* status = status_dev ? status_dev : (uint32_t*)scan_ws;
     Bits* bits = (Bits*)(scan_ws + rm::align256(rm_scan_workspace_size(Gf)));
     if (cudaMemsetAsync(counts, 0, (size_t)Gf * 4, s) != cudaSuccess) return rm_host::check_launch("rm_fine_lists");
     if (n_pairs > 0) {
@@ -290,7 +291,7 @@ int launch_split(const int64_t* keys, const int32_t* ids, int64_t n_pairs, const
         int rc = rm_host::check_launch("rm_fine_lists (bits)");
         if (rc) return rc;
     }
-    int rc = rm_scan_tiles(counts, Gf, incl, total_dev, scan_ws, rm_scan_workspace_size(Gf), s);
+    int rc = rm_host::scan_tiles_status(counts, Gf, incl, total_dev, scan_ws, rm_scan_workspace_size(Gf), status, s);
     if (rc) return rc;
     rm::fine_write_kernel<PACKED, FS><<<(unsigned)G, rm::kFineThreads, 0, s>>>(
         ids, (const int2*)ranges, bits, views, counts, incl, fine_ids, capacity, (int2*)fine_ranges, status);
@@ -301,7 +302,7 @@ int fine_lists_impl(const char* who, const int64_t* sorted_keys, const int32_t* 
                     const int64_t* n_pairs_dev, const int32_t* ranges, const float* footprint,
                     const float* jitter_bounds, int64_t n_tets, const rm::ViewSet& views, int fine_shift,
                     int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges, int64_t* total_dev, void* workspace,
-                    size_t workspace_bytes, void* stream) {
+                    size_t workspace_bytes, uint32_t* status_dev, void* stream) {
     if (fine_shift < 1 || fine_shift > 3) return rm_host::fail(RM_EINVAL, "%s: fine_shift %d", who, fine_shift);
     if (capacity < 0 || n_tets < 0 || n_pairs < 0) return rm_host::fail(RM_EINVAL, "%s: negative size", who);
     const int f = 1 << fine_shift;
@@ -330,17 +331,17 @@ int fine_lists_impl(const char* who, const int64_t* sorted_keys, const int32_t* 
     cudaStream_t s = (cudaStream_t)stream;
     if (packed)
         return launch_split<true, 1>(sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint, jitter_bounds,
-                                     n_tets, views, G, Gf, capacity, fine_ids, fine_ranges, total_dev, ws, s);
+                                     n_tets, views, G, Gf, capacity, fine_ids, fine_ranges, total_dev, ws, status_dev, s);
     if (fine_shift == 1)
         return launch_split<false, 1>(sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint,
                                       jitter_bounds, n_tets, views, G, Gf, capacity, fine_ids, fine_ranges, total_dev,
-                                      ws, s);
+                                      ws, status_dev, s);
     if (fine_shift == 2)
         return launch_split<false, 2>(sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint,
                                       jitter_bounds, n_tets, views, G, Gf, capacity, fine_ids, fine_ranges, total_dev,
-                                      ws, s);
+                                      ws, status_dev, s);
     return launch_split<false, 3>(sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint, jitter_bounds,
-                                  n_tets, views, G, Gf, capacity, fine_ids, fine_ranges, total_dev, ws, s);
+                                  n_tets, views, G, Gf, capacity, fine_ids, fine_ranges, total_dev, ws, status_dev, s);
 }
 
 }  // namespace
@@ -351,27 +352,28 @@ int rm_fine_lists(const int64_t* sorted_keys, const int32_t* sorted_ids, int64_t
                   const int64_t* n_pairs_dev, const int32_t* ranges, const float* footprint,
                   const float* jitter_bounds, const rm_camera* cam, int fine_shift, int64_t capacity,
                   int32_t* fine_ids, int32_t* fine_ranges, int64_t* total_dev, void* workspace,
-                  size_t workspace_bytes, void* stream) {
+                  size_t workspace_bytes, uint32_t* status_dev, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_fine_lists", cam, 1, &views);
     if (rc) return rc;
     if (!footprint) return rm_host::fail(RM_EINVAL, "rm_fine_lists: NULL footprint");
     return fine_lists_impl("rm_fine_lists", sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint,
                            jitter_bounds, 0, views, fine_shift, capacity, fine_ids, fine_ranges, total_dev, workspace,
-                           workspace_bytes, stream);
+                           workspace_bytes, status_dev, stream);
 }
 
 int rm_fine_lists_multi(const int64_t* sorted_keys, const int32_t* sorted_ids, int64_t n_pairs,
                         const int64_t* n_pairs_dev, const int32_t* ranges, const float* footprint,
                         const float* jitter_bounds, int64_t n_tets, const rm_camera* cams, int n_views,
                         int fine_shift, int64_t capacity, int32_t* fine_ids, int32_t* fine_ranges,
-                        int64_t* total_dev, void* workspace, size_t workspace_bytes, void* stream) {
+                        int64_t* total_dev, void* workspace, size_t workspace_bytes, uint32_t* status_dev,
+                        void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_fine_lists_multi", cams, n_views, &views);
     if (rc) return rc;
     return fine_lists_impl("rm_fine_lists_multi", sorted_keys, sorted_ids, n_pairs, n_pairs_dev, ranges, footprint,
                            jitter_bounds, n_tets, views, fine_shift, capacity, fine_ids, fine_ranges, total_dev,
-                           workspace, workspace_bytes, stream);
+                           workspace, workspace_bytes, status_dev, stream);
 }
 
 }  // extern "C"

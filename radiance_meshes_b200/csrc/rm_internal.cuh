@@ -258,6 +258,13 @@ __device__ __forceinline__ uint64_t footprint_bits(const Footprint& f, float4 jb
     return bits;
 }
 
+// Whether a tet's four vertex indices lie in [0, n_verts): a tet that fails
+// is culled before any vertex load (RM_STATUS_BAD_INDEX).
+__device__ __forceinline__ bool tet_indices_ok(int4 id, int64_t n_verts) {
+    return id.x >= 0 && id.y >= 0 && id.z >= 0 && id.w >= 0 && (int64_t)id.x < n_verts &&
+           (int64_t)id.y < n_verts && (int64_t)id.z < n_verts && (int64_t)id.w < n_verts;
+}
+
 // Bounded spin helper: returns false once the budget is exhausted.
 __device__ __forceinline__ bool spin_budget(uint32_t& left) {
     if (left == 0) return false;
@@ -271,6 +278,13 @@ __device__ __forceinline__ bool spin_budget(uint32_t& left) {
 // Host-side helpers (rm_capi.cu).
 namespace rm_host {
 int fail(int code, const char* fmt, ...);
+// Iteration limit of the bounded device-side waits (rm_set_wait_limit); the
+// host passes it to every kernel that waits.
+uint32_t wait_limit();
+// rm_scan_tiles with the timeout / overflow bits or-ed into `status` instead
+// of the workspace's own status word (status NULL: the workspace's word).
+int scan_tiles_status(const int32_t* tiles_touched, int64_t n_tets, int32_t* offsets, int64_t* total_dev,
+                      void* workspace, size_t workspace_bytes, uint32_t* status, void* stream);
 // Checks the launch status of the preceding kernel launches and adds
 // `kernels` to the process-wide launch counter.
 int check_launch(const char* what, int kernels = 1);

@@ -183,30 +183,52 @@ __device__ __forceinline__ f3 load_vertex(const float* __restrict__ v, int i) {
 }
 
 // View-independent part of vertex_shader: the vertices, the planarity cull
-// (is_planar, intersect.slang:76-89) and the circumsphere.
+// (is_planar, intersect.slang:76-89) and the circumsphere.  Input checks come
+// first: a tet with an index outside [0, n_verts) is culled before any vertex
+// load (err = RM_STATUS_BAD_INDEX), one with a NaN or infinite vertex is
+// culled too (err = RM_STATUS_NONFINITE; the reference asserts on NaN
+// vertices on the host, tile_shader_slang.py:78).  Culling goes through
+// `planar`, which every view tests first.
 struct TetGeom {
     f3 v[4];
     bool planar;
     bool sphere;  // false: power -1e20 (culled in every view)
     d3 center;
     double radius;
+    uint32_t err;
 };
 
 __device__ __forceinline__ TetGeom tet_geom(const int4* __restrict__ indices, const float* __restrict__ verts,
-                                            int64_t g) {
+                                            int64_t g, int64_t n_verts) {
     TetGeom t;
+    t.err = 0u;
+    t.sphere = false;
+    t.center = {0.0, 0.0, 0.0};
+    t.radius = 0.0;
     const int4 id = __ldg(indices + g);
+    if (!tet_indices_ok(id, n_verts)) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) t.v[i] = {0.f, 0.f, 0.f};
+        t.planar = true;
+        t.err = RM_STATUS_BAD_INDEX;
+        return t;
+    }
     t.v[0] = load_vertex(verts, id.x);
     t.v[1] = load_vertex(verts, id.y);
     t.v[2] = load_vertex(verts, id.z);
     t.v[3] = load_vertex(verts, id.w);
+    bool finite = true;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) finite &= isfinite(t.v[i].x) && isfinite(t.v[i].y) && isfinite(t.v[i].z);
+    if (!finite) {
+        t.planar = true;
+        t.err = RM_STATUS_NONFINITE;
+        return t;
+    }
     f3 nrm = cross3(t.v[1] - t.v[0], t.v[2] - t.v[0]);
     const float l = sqrtf(dot3(nrm, nrm));
     nrm = {nrm.x / l, nrm.y / l, nrm.z / l};
     t.planar = fabsf(dot3(nrm, t.v[3] - t.v[0])) < 1e-3f;
-    t.sphere = false;
-    t.center = {0.0, 0.0, 0.0};
-    t.radius = 0.0;
     if (!t.planar)
         t.sphere = circumsphere({(double)t.v[0].x, (double)t.v[0].y, (double)t.v[0].z},
                                 {(double)t.v[1].x, (double)t.v[1].y, (double)t.v[1].z},
@@ -308,12 +330,14 @@ __device__ __forceinline__ int project_view(const rm_camera& cam, const TetGeom&
 template <bool GENERAL>
 __global__ void __launch_bounds__(256) project_fwd_kernel(const int4* __restrict__ indices,
                                                           const float* __restrict__ verts, int64_t n_tets,
-                                                          const rm_camera cam, int32_t* __restrict__ tiles,
-                                                          int4* __restrict__ rect, float* __restrict__ vs,
-                                                          float* __restrict__ cc) {
+                                                          int64_t n_verts, const rm_camera cam,
+                                                          int32_t* __restrict__ tiles, int4* __restrict__ rect,
+                                                          float* __restrict__ vs, float* __restrict__ cc,
+                                                          uint32_t* status) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_tets) return;
-    const TetGeom t = tet_geom(indices, verts, g);
+    const TetGeom t = tet_geom(indices, verts, g, n_verts);
+    if (t.err && status) atomicOr(status, t.err);
     int4 r;
     float depth;
     const int n_tiles = project_view<GENERAL>(cam, t, r, depth);
@@ -331,12 +355,14 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(const int4* __restrict
 template <bool GENERAL>
 __global__ void __launch_bounds__(256) project_fwd_fine_kernel(const int4* __restrict__ indices,
                                                                const float* __restrict__ verts, int64_t n_tets,
-                                                               const rm_camera cam, int32_t* __restrict__ tiles,
-                                                               int4* __restrict__ rect, float* __restrict__ vs,
-                                                               float* __restrict__ cc, float4* __restrict__ fp) {
+                                                               int64_t n_verts, const rm_camera cam,
+                                                               int32_t* __restrict__ tiles, int4* __restrict__ rect,
+                                                               float* __restrict__ vs, float* __restrict__ cc,
+                                                               float4* __restrict__ fp, uint32_t* status) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_tets) return;
-    const TetGeom t = tet_geom(indices, verts, g);
+    const TetGeom t = tet_geom(indices, verts, g, n_verts);
+    if (t.err && status) atomicOr(status, t.err);
     int4 r;
     Footprint f;
     float depth;
@@ -361,13 +387,16 @@ __global__ void __launch_bounds__(256) project_fwd_fine_kernel(const int4* __res
 template <bool GENERAL>
 __global__ void __launch_bounds__(256) project_fwd_multi_kernel(const int4* __restrict__ indices,
                                                                 const float* __restrict__ verts, int64_t n_tets,
+                                                                int64_t n_verts,
                                                                 const __grid_constant__ ViewSet views,
                                                                 int32_t* __restrict__ tiles, int4* __restrict__ rect,
                                                                 float* __restrict__ depth, int32_t* __restrict__ any,
-                                                                float* __restrict__ cc, float4* __restrict__ fp) {
+                                                                float* __restrict__ cc, float4* __restrict__ fp,
+                                                                uint32_t* status) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_tets) return;
-    const TetGeom t = tet_geom(indices, verts, g);
+    const TetGeom t = tet_geom(indices, verts, g, n_verts);
+    if (t.err && status) atomicOr(status, t.err);
     int total = 0;
     for (int v = 0; v < views.n; ++v) {
         int4 r;
@@ -411,7 +440,7 @@ __device__ __forceinline__ void atomic_add3(float* p, d3 g) {
 // (vertex_shader.bwd, tile_shader_slang.py:128-150), evaluated in FP64.
 __global__ void __launch_bounds__(256) project_bwd_kernel(const int4* __restrict__ indices,
                                                           const float* __restrict__ verts, int64_t n_tets,
-                                                          const rm_camera cam,
+                                                          int64_t n_verts, const rm_camera cam,
                                                           const int32_t* __restrict__ tiles,
                                                           const float* __restrict__ gvs,
                                                           const float* __restrict__ gcc,
@@ -420,6 +449,7 @@ __global__ void __launch_bounds__(256) project_bwd_kernel(const int4* __restrict
     if (g >= n_tets) return;
     if (tiles[g] <= 0) return;
     const int4 id = __ldg(indices + g);
+    if (!tet_indices_ok(id, n_verts)) return;  // culled by the forward
     const int ids[4] = {id.x, id.y, id.z, id.w};
     d3 X[4];
 #pragma unroll
@@ -493,7 +523,7 @@ extern "C" {
 
 int rm_project_fwd(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,
                    const rm_camera* cam, int32_t* tiles_touched, int32_t* rect, float* vs,
-                   float* circumcenter, void* stream) {
+                   float* circumcenter, uint32_t* status_dev, void* stream) {
     int rc = rm_host::check_cam(cam);
     if (rc) return rc;
     if (n_tets < 0 || n_verts < 0) return rm_host::fail(RM_EINVAL, "rm_project_fwd: negative size");
@@ -506,13 +536,14 @@ int rm_project_fwd(const int32_t* indices, const float* vertices, int64_t n_tets
     const int64_t blocks = (n_tets + threads - 1) / threads;
     auto kernel = rm_host::cam_general(*cam) ? rm::project_fwd_kernel<true> : rm::project_fwd_kernel<false>;
     kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
-        (const int4*)indices, vertices, n_tets, *cam, tiles_touched, (int4*)rect, vs, circumcenter);
+        (const int4*)indices, vertices, n_tets, n_verts, *cam, tiles_touched, (int4*)rect, vs, circumcenter,
+        status_dev);
     return rm_host::check_launch("rm_project_fwd");
 }
 
 int rm_project_fwd_fine(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,
                         const rm_camera* cam, int32_t* tiles_touched, int32_t* rect, float* vs, float* circumcenter,
-                        float* footprint, void* stream) {
+                        float* footprint, uint32_t* status_dev, void* stream) {
     int rc = rm_host::check_cam(cam);
     if (rc) return rc;
     if (n_tets < 0 || n_verts < 0) return rm_host::fail(RM_EINVAL, "rm_project_fwd_fine: negative size");
@@ -526,14 +557,15 @@ int rm_project_fwd_fine(const int32_t* indices, const float* vertices, int64_t n
     auto kernel =
         rm_host::cam_general(*cam) ? rm::project_fwd_fine_kernel<true> : rm::project_fwd_fine_kernel<false>;
     kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
-        (const int4*)indices, vertices, n_tets, *cam, tiles_touched, (int4*)rect, vs, circumcenter,
-        (float4*)footprint);
+        (const int4*)indices, vertices, n_tets, n_verts, *cam, tiles_touched, (int4*)rect, vs, circumcenter,
+        (float4*)footprint, status_dev);
     return rm_host::check_launch("rm_project_fwd_fine");
 }
 
 int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t n_tets, int64_t n_verts,
                          const rm_camera* cams, int n_views, int32_t* tiles_touched, int32_t* rect, float* depth,
-                         int32_t* tiles_any, float* circumcenter, float* footprint, void* stream) {
+                         int32_t* tiles_any, float* circumcenter, float* footprint, uint32_t* status_dev,
+                         void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_project_fwd_multi", cams, n_views, &views);
     if (rc) return rc;
@@ -549,8 +581,8 @@ int rm_project_fwd_multi(const int32_t* indices, const float* vertices, int64_t 
     for (int v = 0; v < n_views; ++v) general |= rm_host::cam_general(cams[v]);
     auto kernel = general ? rm::project_fwd_multi_kernel<true> : rm::project_fwd_multi_kernel<false>;
     kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
-        (const int4*)indices, vertices, n_tets, views, tiles_touched, (int4*)rect, depth, tiles_any, circumcenter,
-        (float4*)footprint);
+        (const int4*)indices, vertices, n_tets, n_verts, views, tiles_touched, (int4*)rect, depth, tiles_any,
+        circumcenter, (float4*)footprint, status_dev);
     return rm_host::check_launch("rm_project_fwd_multi");
 }
 
@@ -567,7 +599,8 @@ int rm_project_bwd(const int32_t* indices, const float* vertices, int64_t n_tets
     const int threads = 256;
     const int64_t blocks = (n_tets + threads - 1) / threads;
     rm::project_bwd_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
-        (const int4*)indices, vertices, n_tets, *cam, tiles_touched, grad_vs, grad_circumcenter, grad_vertices);
+        (const int4*)indices, vertices, n_tets, n_verts, *cam, tiles_touched, grad_vs, grad_circumcenter,
+        grad_vertices);
     return rm_host::check_launch("rm_project_bwd");
 }
 

@@ -18,7 +18,7 @@ constexpr int kScanItems = 16;
 constexpr int kScanTile = kScanThreads * kScanItems;  // 4096 tets per CTA
 constexpr uint64_t kFlagAgg = 1ull << 32;
 constexpr uint64_t kFlagInc = 2ull << 32;
-constexpr uint32_t kSpinLimit = 1u << 22;
+constexpr uint64_t kFlagOvf = 4ull << 32;  // an inclusive prefix up to this tile exceeds INT32_MAX
 
 struct ScanWs {
     uint32_t status;
@@ -36,12 +36,18 @@ __device__ __forceinline__ uint64_t ld_acquire(const uint64_t* p) {
     return v;
 }
 
+// Tile states: bits 0..31 the tile's aggregate or inclusive prefix (uint32),
+// bit 32 aggregate ready, bit 33 inclusive prefix ready, bit 34 overflow.
+// Sums are formed in int64; a prefix above INT32_MAX (the offsets are int32,
+// as the reference's cumsum) sets RM_STATUS_OVERFLOW.  The look-back polls a
+// predecessor at most spin_limit times, then sets RM_STATUS_SCAN_TIMEOUT and
+// goes on (the offsets are then invalid; every store stays in bounds).
 __global__ void __launch_bounds__(kScanThreads) scan_kernel(const int32_t* __restrict__ in, int64_t n,
                                                             int32_t* __restrict__ out, int64_t* total_dev,
-                                                            ScanWs* ws) {
+                                                            ScanWs* ws, uint32_t* status, uint32_t spin_limit) {
     __shared__ uint32_t s_tile;
-    __shared__ int32_t s_warp[kScanThreads / 32];
-    __shared__ int32_t s_prefix;
+    __shared__ int64_t s_warp[kScanThreads / 32];
+    __shared__ int64_t s_prefix;
     uint64_t* state = reinterpret_cast<uint64_t*>(ws + 1);
     if (threadIdx.x == 0) s_tile = atomicAdd(&ws->counter, 1u);
     __syncthreads();
@@ -62,60 +68,64 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const int32_t* __res
 #pragma unroll
         for (int k = 0; k < kScanItems; ++k) v[k] = (base + k < n) ? __ldg(in + base + k) : 0;
     }
-    int32_t sum = 0;
+    int64_t sum = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) sum += v[k];
     // block-wide exclusive scan of the per-thread sums
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int32_t incl = sum;
+    int64_t incl = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        const int64_t y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += y;
     }
     if (lane == 31) s_warp[warp] = incl;
     __syncthreads();
     if (warp == 0) {
-        int32_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0;
-        int32_t wi = w;
+        int64_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0;
+        int64_t wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+            const int64_t y = __shfl_up_sync(0xffffffffu, wi, o);
             if (lane >= o) wi += y;
         }
         if (lane < kScanThreads / 32) s_warp[lane] = wi - w;  // exclusive warp offsets
-        const int32_t block_total = __shfl_sync(0xffffffffu, wi, kScanThreads / 32 - 1);
+        const int64_t block_total = __shfl_sync(0xffffffffu, wi, kScanThreads / 32 - 1);
         if (lane == 0) {
-            int32_t prefix = 0;
-            if (tile == 0) {
-                st_release(&state[0], kFlagInc | (uint32_t)block_total);
-            } else {
-                st_release(&state[tile], kFlagAgg | (uint32_t)block_total);
+            int64_t prefix = 0;
+            bool ovf = block_total > (int64_t)INT32_MAX || block_total < 0;
+            if (tile != 0) {
+                st_release(&state[tile], kFlagAgg | (ovf ? kFlagOvf : 0ull) | (uint32_t)block_total);
                 int64_t t = (int64_t)tile - 1;
-                uint32_t budget = kSpinLimit;
+                uint32_t budget = spin_limit;
                 while (t >= 0) {
                     const uint64_t s = ld_acquire(&state[t]);
                     const uint64_t flag = s & (3ull << 32);
                     if (flag == 0) {
                         if (!spin_budget(budget)) {
-                            atomicOr(&ws->status, RM_STATUS_SCAN_TIMEOUT);
+                            atomicOr(status, RM_STATUS_SCAN_TIMEOUT);
                             break;
                         }
                         continue;
                     }
-                    prefix += (int32_t)(uint32_t)s;
+                    prefix += (int64_t)(uint32_t)s;
+                    ovf |= (s & kFlagOvf) != 0;
                     if (flag == kFlagInc) break;
                     --t;
                 }
-                st_release(&state[tile], kFlagInc | (uint32_t)(prefix + block_total));
             }
+            const int64_t tile_incl = prefix + block_total;
+            ovf |= tile_incl > (int64_t)INT32_MAX;
+            if (ovf) atomicOr(status, RM_STATUS_OVERFLOW);
+            st_release(&state[tile], kFlagInc | (ovf ? kFlagOvf : 0ull) | (uint32_t)tile_incl);
             s_prefix = prefix;
             const int64_t last = (int64_t)tile * kScanTile + kScanTile;
-            if (last >= n) *total_dev = (int64_t)(prefix + block_total);
+            if (last >= n) *total_dev = tile_incl;
         }
     }
     __syncthreads();
-    int32_t run = s_prefix + s_warp[warp] + incl - sum;
+    // int32 offsets (wrapped when RM_STATUS_OVERFLOW is set)
+    int32_t run = (int32_t)(s_prefix + s_warp[warp] + incl - sum);
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         run += v[k];
@@ -288,6 +298,14 @@ size_t rm_scan_workspace_size(int64_t n_tets) {
 
 int rm_scan_tiles(const int32_t* tiles_touched, int64_t n_tets, int32_t* offsets, int64_t* total_dev,
                   void* workspace, size_t workspace_bytes, void* stream) {
+    return rm_host::scan_tiles_status(tiles_touched, n_tets, offsets, total_dev, workspace, workspace_bytes, nullptr,
+                                      stream);
+}
+
+}  // extern "C"
+
+int rm_host::scan_tiles_status(const int32_t* tiles_touched, int64_t n_tets, int32_t* offsets, int64_t* total_dev,
+                               void* workspace, size_t workspace_bytes, uint32_t* status, void* stream) {
     if (n_tets < 0) return rm_host::fail(RM_EINVAL, "rm_scan_tiles: negative size");
     if (!total_dev) return rm_host::fail(RM_EINVAL, "rm_scan_tiles: total_dev is NULL");
     cudaStream_t s = (cudaStream_t)stream;
@@ -305,10 +323,14 @@ int rm_scan_tiles(const int32_t* tiles_touched, int64_t n_tets, int32_t* offsets
     cudaError_t e = cudaMemsetAsync((char*)workspace + 4, 0, need - 4, s);
     if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_scan_tiles: %s", cudaGetErrorString(e));
     const int64_t blocks = (n_tets + rm::kScanTile - 1) / rm::kScanTile;
-    rm::scan_kernel<<<(unsigned)blocks, rm::kScanThreads, 0, s>>>(tiles_touched, n_tets, offsets, total_dev,
-                                                                 (rm::ScanWs*)workspace);
+    rm::ScanWs* ws = (rm::ScanWs*)workspace;
+    rm::scan_kernel<<<(unsigned)blocks, rm::kScanThreads, 0, s>>>(tiles_touched, n_tets, offsets, total_dev, ws,
+                                                                 status ? status : &ws->status,
+                                                                 rm_host::wait_limit());
     return rm_host::check_launch("rm_scan_tiles");
 }
+
+extern "C" {
 
 int rm_emit_pairs(const float* vs, const int32_t* rect, const int32_t* offsets, int64_t n_tets, int32_t grid_width,
                   int64_t capacity, const int64_t* total_dev, int64_t* keys, int32_t* values, uint32_t* status_dev,
@@ -403,8 +425,77 @@ constexpr size_t kNoAllocScratchBytes =
 // holds one copy until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scan_scratch[kNoAllocScratchBytes];
 
+// The array's device address, looked up once per CUDA context.  Each context
+// loads the module on its own (a context created after cudaDeviceReset, or
+// one made current through the driver API, sees the array at another
+// address), so the cache is keyed by the context's unique id, never reused
+// within a process, rather than by the device ordinal.
+typedef int (*CtxGetCurrentFn)(void** ctx);
+typedef int (*CtxGetIdFn)(void* ctx, unsigned long long* id);
+struct NoAllocSlot {
+    unsigned long long ctx_id;
+    void* addr;
+};
+constexpr int kNoAllocSlots = 64;
 std::mutex g_noalloc_mu;
-void* g_noalloc_addr[64] = {};
+NoAllocSlot g_noalloc_slots[kNoAllocSlots] = {};
+int g_noalloc_next = 0;
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+int current_context_id(unsigned long long* id) {
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        void* f0 = nullptr;
+        void* f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0 = cudaDriverEntryPointSymbolNotFound, q1 = q0;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0);
+        if (e == cudaSuccess) e = cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1);
+        if (e != cudaSuccess || q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+            return rm_host::fail(RM_ECUDA, "rm_scan_tiles_noalloc: driver context query unavailable (%s)",
+                                 cudaGetErrorString(e));
+        g_ctx_get_current = (CtxGetCurrentFn)f0;
+        g_ctx_get_id = (CtxGetIdFn)f1;
+    }
+    void* ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != 0 || !ctx)
+        return rm_host::fail(RM_ECUDA, "rm_scan_tiles_noalloc: no current CUDA context");
+    if (g_ctx_get_id(ctx, id) != 0) return rm_host::fail(RM_ECUDA, "rm_scan_tiles_noalloc: cuCtxGetId failed");
+    return RM_OK;
+}
+
+// Set-up: the device address of g_noalloc_scan_scratch in the current
+// context.  In host code the array's name is only a host-side handle, so the
+// address is looked up with cudaGetSymbolAddress (a host-side lookup that
+// allocates nothing) and cached per context.
+int noalloc_scratch(void** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_scan_tiles_noalloc: %s", cudaGetErrorString(e));
+    unsigned long long id = 0;
+    int rc = current_context_id(&id);
+    if (rc) {
+        // the runtime creates the device's primary context on its first call
+        // that needs one; the symbol lookup is such a call
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
+        if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_scan_tiles_noalloc: %s", cudaGetErrorString(e));
+        if ((rc = current_context_id(&id))) return rc;
+    }
+    for (const NoAllocSlot& sl : g_noalloc_slots)
+        if (sl.addr && sl.ctx_id == id) {
+            *out = sl.addr;
+            return RM_OK;
+        }
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
+    if (e != cudaSuccess || !p)
+        return rm_host::fail(RM_ECUDA, "rm_scan_tiles_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    g_noalloc_slots[g_noalloc_next] = {id, p};  // oldest context's entry is replaced when the table is full
+    g_noalloc_next = (g_noalloc_next + 1) % kNoAllocSlots;
+    *out = p;
+    return RM_OK;
+}
 
 }  // namespace
 }  // namespace rm
@@ -419,28 +510,20 @@ int rm_scan_tiles_noalloc(const int32_t* tiles_touched, int64_t n_tets, int32_t*
                              "rm_scan_tiles_noalloc: %lld tets exceed the fixed scratch limit of %lld tets; use "
                              "rm_scan_tiles with a caller-provided workspace",
                              (long long)n_tets, (long long)kNoAllocMaxTets);
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_scan_tiles_noalloc: %s", cudaGetErrorString(e));
-    if (dev < 0 || dev >= 64) return rm_host::fail(RM_EINVAL, "rm_scan_tiles_noalloc: device ordinal %d", dev);
     void* scratch = nullptr;
-    {
-        // one-time set-up per device: the array's device address, looked up
-        // with that device current (the host-side symbol is not a device pointer)
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
-            void* p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
-            if (e != cudaSuccess || !p)
-                return rm_host::fail(RM_ECUDA, "rm_scan_tiles_noalloc: cudaGetSymbolAddress: %s",
-                                     cudaGetErrorString(e));
-            g_noalloc_addr[dev] = p;
-        }
-        scratch = g_noalloc_addr[dev];
-    }
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
     // rm_scan_tiles clears the queue counter and the tile states before the
     // kernel runs, so the contents left by an earlier call do not matter
     return rm_scan_tiles(tiles_touched, n_tets, offsets, total_dev, scratch, kNoAllocScratchBytes, stream);
+}
+
+int rm_scan_noalloc_read_status(uint32_t* status_host, void* stream) {
+    if (!status_host) return rm_host::fail(RM_EINVAL, "rm_scan_noalloc_read_status: NULL pointer");
+    void* scratch = nullptr;
+    int rc = rm::noalloc_scratch(&scratch);
+    if (rc) return rc;
+    return rm_read_status((const uint32_t*)scratch, status_host, stream);  // status is the array's first word
 }
 
 }  // extern "C"

@@ -27,7 +27,6 @@ constexpr int kMaxPasses = 8;
 constexpr uint32_t kLbAgg = 1u << 30;
 constexpr uint32_t kLbInc = 2u << 30;
 constexpr uint32_t kLbMask = (1u << 30) - 1;
-constexpr uint32_t kSpinLimit = 1u << 22;
 
 struct SortHeader {
     uint32_t status;
@@ -132,7 +131,7 @@ struct PassSmem {
 __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
     const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint64_t* __restrict__ kout,
     uint32_t* __restrict__ vout, int64_t cap, const int64_t* __restrict__ n_dev, int pass, int shift,
-    uint32_t dmask, SortHeader* hdr, uint32_t* __restrict__ lookback) {
+    uint32_t dmask, SortHeader* hdr, uint32_t* __restrict__ lookback, uint32_t* status, uint32_t spin_limit) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PassSmem& S = *reinterpret_cast<PassSmem*>(smem_raw);
     const int64_t n = n_dev ? min(*n_dev, cap) : cap;
@@ -191,13 +190,13 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
             st_release32(lb, kLbAgg | (vcount & kLbMask));
             excl = 0;
             int64_t t = (int64_t)tile - 1;
-            uint32_t budget = kSpinLimit;
+            uint32_t budget = spin_limit;
             while (t >= 0) {
                 const uint32_t s = ld_acquire32(lookback + (size_t)t * kRadix + d);
                 const uint32_t flag = s & ~kLbMask;
                 if (flag == 0) {
                     if (!spin_budget(budget)) {
-                        atomicOr(&hdr->status, RM_STATUS_SORT_TIMEOUT);
+                        atomicOr(status, RM_STATUS_SORT_TIMEOUT);
                         break;
                     }
                     continue;
@@ -261,7 +260,8 @@ size_t rm_sort_workspace_size(int64_t n) {
 }
 
 int rm_sort_pairs(const int64_t* keys_in, const int32_t* values_in, int64_t n, const int64_t* n_dev, int end_bit,
-                  int64_t* keys_out, int32_t* values_out, void* workspace, size_t workspace_bytes, void* stream) {
+                  int64_t* keys_out, int32_t* values_out, void* workspace, size_t workspace_bytes,
+                  uint32_t* status_dev, void* stream) {
     using namespace rm;
     if (n < 0) return rm_host::fail(RM_EINVAL, "rm_sort_pairs: negative size");
     if (end_bit < 1 || end_bit > 64) return rm_host::fail(RM_EINVAL, "rm_sort_pairs: end_bit %d out of range", end_bit);
@@ -298,7 +298,8 @@ int rm_sort_pairs(const int64_t* keys_in, const int32_t* values_in, int64_t n, c
         const int bits = (end_bit - 8 * p) < 8 ? (end_bit - 8 * p) : 8;
         const uint32_t dmask = (bits >= 8) ? 255u : ((1u << bits) - 1u);
         onesweep_kernel<<<(unsigned)tiles, kSortThreads, sizeof(PassSmem), s>>>(
-            src_k, src_v, dk, dv, n, n_dev, p, 8 * p, dmask, hdr, lookback + (size_t)p * tiles * kRadix);
+            src_k, src_v, dk, dv, n, n_dev, p, 8 * p, dmask, hdr, lookback + (size_t)p * tiles * kRadix,
+            status_dev ? status_dev : &hdr->status, rm_host::wait_limit());
         src_k = dk;
         src_v = dv;
     }

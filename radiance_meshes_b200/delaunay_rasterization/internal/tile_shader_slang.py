@@ -3,9 +3,13 @@ delaunay_rasterization/internal/tile_shader_slang.py (``vertex_and_tile_shader``
 ``VertexShader``), running the sm_100a kernels of librm_b200.so.
 
 Differences from the reference, none of them visible in the results:
-  * the NaN check on vertices (reference line 78) is not a host-side assert,
-    because that would synchronise the stream; non-finite vertices simply
-    produce non-finite depth keys as they would in the reference kernel;
+  * the NaN check on vertices (reference line 78) is not a separate
+    host-side assert, which would synchronise the stream: the projection
+    kernel checks every tet's vertices (and that its indices lie in
+    [0, n_verts)) and reports through the frame's device status word, which
+    is read with the pair count; a NaN or infinite vertex or a bad index
+    raises ``_capi.DeviceStatusError`` (a ``RuntimeError``) here, as the
+    reference's assert raises;
   * the pair count is read back once instead of three times;
   * no cudaMalloc/cudaFree per call: scratch comes from a reusable pool.
 """
@@ -29,7 +33,9 @@ def vertex_and_tile_shader(indices, vertices, cam, render_grid):
     attached to the returned ``sorted_tetra_idx`` (attribute ``rm_fine``);
     ``AlphaBlendTiledRender`` cuts them for its ray jitter and blends over
     them when it is handed that tensor, which gives the same image with fewer
-    ray/tet tests (see ``rasterizer.FineLists``)."""
+    ray/tet tests (see ``rasterizer.FineLists``).  The per-tet tile counts
+    ride along the same way (attribute ``rm_frame``), so that the blend packs
+    the records of visible tets only."""
     camst = tcam_to_struct(cam)
     fs = R.fine_shift_for(camst) if R.fine_lists_enabled() else 0
     pre = None
@@ -41,8 +47,10 @@ def vertex_and_tile_shader(indices, vertices, cam, render_grid):
         indices, vertices, cam, render_grid, "cuda", pre)
     with torch.no_grad():
         lists = R.build_tile_lists(tiles_touched, rect_tile_space, vs_tetra, camst)
+        status = R.frame_status(indices.shape[0], vertices.device)
+        R.attach_frame(lists.sorted_ids, tiles_touched, status)
         if fs:
-            R.attach_fine_lists(lists.sorted_ids, lists.ranges, camst, fs, footprint, lists.sorted_keys)
+            R.attach_fine_lists(lists.sorted_ids, lists.ranges, camst, fs, footprint, lists.sorted_keys, status)
     mask = tiles_touched > 0
     return lists.sorted_ids, lists.ranges, vs_tetra, circumcenter, mask, rect_tile_space
 

@@ -38,7 +38,7 @@ class ActivateOutput(torch.autograd.Function):
         cam = (ctypes_floats := _cam3(camera_center))
         feat = torch.empty((T, 7), dtype=torch.float32, device=dev)
         R._call("rm_activate_features", lambda: C.lib().rm_activate_features(
-            C.ptr(idx), C.ptr(v), C.ptr(cc), C.ptr(d), C.ptr(c), C.ptr(g), C.ptr(shr), shr.shape[1], int(sh_deg),
+            C.ptr(idx), C.ptr(v), v.shape[0], C.ptr(cc), C.ptr(d), C.ptr(c), C.ptr(g), C.ptr(shr), shr.shape[1], int(sh_deg),
             ctypes_floats, T, C.ptr(feat), C.stream_handle()))
         ctx.save_for_backward(idx, v, cc, d, c, g, shr)
         ctx.cam = cam
@@ -58,7 +58,7 @@ class ActivateOutput(torch.autograd.Function):
         gv = torch.zeros_like(v)
         gcc = torch.empty_like(cc)
         R._call("rm_activate_features_bwd", lambda: C.lib().rm_activate_features_bwd(
-            C.ptr(idx), C.ptr(v), C.ptr(cc), C.ptr(d), C.ptr(c), C.ptr(g), C.ptr(shr), shr.shape[1], ctx.sh_deg,
+            C.ptr(idx), C.ptr(v), v.shape[0], C.ptr(cc), C.ptr(d), C.ptr(c), C.ptr(g), C.ptr(shr), shr.shape[1], ctx.sh_deg,
             ctx.cam, T, C.ptr(gf), C.ptr(gd), C.ptr(grgb), C.ptr(ggrd), C.ptr(gsh), C.ptr(gv), C.ptr(gcc),
             C.stream_handle()))
         ds, rs, gs, ss, vs = ctx.shapes

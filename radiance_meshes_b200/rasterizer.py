@@ -62,11 +62,15 @@ class ScratchPool:
     def __init__(self):
         self._bufs = {}
 
-    def get(self, name: str, nbytes: int, device) -> torch.Tensor:
+    def get(self, name: str, nbytes: int, device, zero_head: bool = False) -> torch.Tensor:
+        """A buffer of at least ``nbytes``; zero_head: a newly allocated
+        buffer gets its first 256 bytes zeroed (a status word lives there)."""
         key = (str(device), name)
         buf = self._bufs.get(key)
         if buf is None or buf.numel() < nbytes:
             buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+            if zero_head:
+                buf[:256].zero_()
             self._bufs[key] = buf
         return buf
 
@@ -99,6 +103,54 @@ class TileLists:
 
 def _stream():
     return C.stream_handle()
+
+
+def frame_status(n_tets: int, device, pool: ScratchPool | None = None) -> torch.Tensor:
+    """The device status word (int32 [1]) that the kernels of one frame or
+    their RM_STATUS_* bits into: the first 4 bytes of the frame's scan
+    workspace, whose other bytes every scan resets.  Projection, scan, sort
+    and the fine-list split all report there, and build_tile_lists reads it
+    together with the pair count."""
+    pool = pool or _POOL
+    ws = pool.get("scan", C.lib().rm_scan_workspace_size(n_tets), device, zero_head=True)
+    return ws[:4].view(torch.int32)
+
+
+_HOST_READ: dict = {}  # device -> pinned int32 [4]: pair count (int64) and status word
+
+
+def _read_frame(total: torch.Tensor, status: torch.Tensor | None):
+    """One synchronisation: the pair count and the frame's status word."""
+    key = str(total.device)
+    hb = _HOST_READ.get(key)
+    if hb is None:
+        hb = torch.zeros(4, dtype=torch.int32, pin_memory=True)
+        _HOST_READ[key] = hb
+    hb[0:2].view(torch.int64).copy_(total.reshape(1), non_blocking=True)
+    if status is not None:
+        hb[2:3].copy_(status, non_blocking=True)
+    else:
+        hb[2] = 0
+    torch.cuda.current_stream().synchronize()
+    return int(hb[0:2].view(torch.int64)[0]), int(hb[2]) & 0xffffffff
+
+
+def raise_status(bits: int, status: torch.Tensor | None, where: str) -> None:
+    """Clear the status word and raise if any RM_STATUS_* bit is set."""
+    if bits:
+        if status is not None:
+            status.zero_()
+        raise C.DeviceStatusError(bits, where)
+
+
+def check_status(n_tets: int, device) -> None:
+    """Synchronise the current stream and raise ``_capi.DeviceStatusError``
+    if a kernel of this device's frames reported an error that no readback
+    has seen yet (the fine-list split runs after a frame's readback, so its
+    bits otherwise surface at the next frame)."""
+    status = frame_status(n_tets, device)
+    torch.cuda.current_stream().synchronize()
+    raise_status(int(status.item()) & 0xffffffff, status, "rasterizer")
 
 
 class StageTimer:
@@ -159,8 +211,9 @@ def project_fwd(indices: torch.Tensor, vertices: torch.Tensor, cam: RMCamera):
     rect = torch.empty((T, 4), dtype=torch.int32, device=dev)
     vs = torch.empty((T, 3), dtype=torch.float32, device=dev)
     cc = torch.empty((T, 3), dtype=torch.float32, device=dev)
+    status = frame_status(T, dev)
     _call("rm_project_fwd", lambda: C.lib().rm_project_fwd(C.ptr(indices), C.ptr(vertices), T, vertices.shape[0], ctypes.byref(cam),
-                                   C.ptr(tiles), C.ptr(rect), C.ptr(vs), C.ptr(cc), _stream()))
+                                   C.ptr(tiles), C.ptr(rect), C.ptr(vs), C.ptr(cc), C.ptr(status), _stream()))
     return tiles, rect, vs, cc
 
 
@@ -197,9 +250,10 @@ def project_fwd_fine(indices: torch.Tensor, vertices: torch.Tensor, cam: RMCamer
     vs = torch.empty((T, 3), dtype=torch.float32, device=dev)
     cc = torch.empty((T, 3), dtype=torch.float32, device=dev)
     footprint = torch.empty((T, 12), dtype=torch.float32, device=dev)
+    status = frame_status(T, dev)
     _call("rm_project_fwd", lambda: C.lib().rm_project_fwd_fine(
         C.ptr(indices), C.ptr(vertices), T, vertices.shape[0], ctypes.byref(cam), C.ptr(tiles), C.ptr(rect),
-        C.ptr(vs), C.ptr(cc), C.ptr(footprint), _stream()))
+        C.ptr(vs), C.ptr(cc), C.ptr(footprint), C.ptr(status), _stream()))
     return tiles, rect, vs, cc, footprint
 
 
@@ -241,13 +295,17 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
     """Scan, emit, sort and range the tile/tet pairs.
 
     The pair count P is read back to the host once (the reference reads it
-    three times: tile_shader_slang.py:38-44,68).  After the first frame on a
-    device, the pair buffers are sized from the previous frame's count (plus
-    a quarter) and emission, sort and ranges are queued before P is read, so
-    the GPU keeps working while the host waits for it; the kernels take the
-    pair count from the device.  Should P exceed that capacity, the frame is
-    built again with buffers of exactly P.  The returned tensors are the
-    first P entries of those buffers."""
+    three times: tile_shader_slang.py:38-44,68), together with the frame's
+    status word (frame_status): a bad index, a non-finite vertex, a pair
+    count beyond int32 or a look-back that gave up raises
+    ``_capi.DeviceStatusError`` there, where the reference asserts on the
+    host (tile_shader_slang.py:78).  After the first frame on a device, the
+    pair buffers are sized from the previous frame's count (plus a quarter)
+    and emission, sort and ranges are queued before P is read, so the GPU
+    keeps working while the host waits for it; the kernels take the pair
+    count from the device.  Should P exceed that capacity, the frame is built
+    again with buffers of exactly P (and its status read once more).  The
+    returned tensors are the first P entries of those buffers."""
     pool = pool or _POOL
     dev = tiles.device
     T = tiles.shape[0]
@@ -258,7 +316,8 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
     offsets = torch.empty(T, dtype=torch.int32, device=dev)
     total = torch.zeros(1, dtype=torch.int64, device=dev)
     ws_n = L.rm_scan_workspace_size(T)
-    ws = pool.get("scan", ws_n, dev)
+    ws = pool.get("scan", ws_n, dev, zero_head=True)
+    status = ws[:4].view(torch.int32)  # frame_status(T, dev): the scan keeps it, the stages or into it
     _call("rm_scan_tiles", lambda: L.rm_scan_tiles(C.ptr(tiles), T, C.ptr(offsets), C.ptr(total), C.ptr(ws), ws_n, s))
 
     def pairs(cap, n_dev):
@@ -272,7 +331,7 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
             sws_n = L.rm_sort_workspace_size(cap)
             sws = pool.get("sort", sws_n, dev)
             _call("rm_sort_pairs", lambda: L.rm_sort_pairs(C.ptr(keys), C.ptr(vals), cap, C.ptr(n_dev), end_bit,
-                                                           C.ptr(sk), C.ptr(sv), C.ptr(sws), sws_n, s))
+                                                           C.ptr(sk), C.ptr(sv), C.ptr(sws), sws_n, C.ptr(status), s))
         ranges = torch.empty((G, 2), dtype=torch.int32, device=dev)
         _call("rm_tile_ranges", lambda: L.rm_tile_ranges(C.ptr(sk), cap, C.ptr(n_dev), C.ptr(ranges), G, s))
         return keys, vals, sk, sv, ranges
@@ -283,13 +342,17 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
     if guess is not None:
         cap = guess + guess // 4 + 4096
         out = pairs(cap, total)
-        P = int(total.item())
+        P, bits = _read_frame(total, status)
         if P > cap:
             out = None
     else:
-        P = int(total.item())
+        P, bits = _read_frame(total, status)
+    raise_status(bits, status, "vertex_and_tile_shader")
     if out is None:
         out = pairs(P, None)
+        # the exact-size sort reports now, not at the next frame
+        _, bits = _read_frame(total, status)
+        raise_status(bits, status, "vertex_and_tile_shader")
     _PAIR_GUESS[key] = P
     keys, vals, sk, sv, ranges = out
     if keep_debug:
@@ -329,6 +392,8 @@ class PendingFineLists:
     ranges: torch.Tensor
     footprint: torch.Tensor
     sorted_keys: torch.Tensor
+    status: torch.Tensor | None = None  # the frame's status word (frame_status)
+    tiles_touched: torch.Tensor | None = None  # the projection's counts: the blend packs visible tets only
     jitter: torch.Tensor | None = None  # the jitter of `lists` (kept alive so identity stays meaningful)
     jitter_version: int = -1
     lists: FineLists | None = None
@@ -352,17 +417,38 @@ def _cam_key(cam: RMCamera) -> tuple:
 
 
 def attach_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCamera, fine_shift: int,
-                      footprint: torch.Tensor, sorted_keys: torch.Tensor) -> PendingFineLists:
+                      footprint: torch.Tensor, sorted_keys: torch.Tensor, status: torch.Tensor | None = None,
+                      tiles_touched: torch.Tensor | None = None) -> PendingFineLists:
     """Record on ``sorted_ids`` (attribute ``rm_fine``) what fine_lists_of needs
     to cut the 2^fine_shift times smaller tiles' lists from these lists."""
-    pend = PendingFineLists(fine_shift, cam, _cam_key(cam), ranges, footprint, sorted_keys)
+    pend = PendingFineLists(fine_shift, cam, _cam_key(cam), ranges, footprint, sorted_keys, status, tiles_touched)
     sorted_ids.rm_fine = pend
     return pend
 
 
+@dataclass
+class FrameState:
+    """What the projection of a frame leaves on its sorted ids (attribute
+    ``rm_frame``) for the blend of the same frame: the per-tet tile counts
+    (the blend packs records of visible tets only) and the status word."""
+    tiles_touched: torch.Tensor
+    status: torch.Tensor
+
+
+def attach_frame(sorted_ids: torch.Tensor, tiles_touched: torch.Tensor, status: torch.Tensor) -> None:
+    sorted_ids.rm_frame = FrameState(tiles_touched, status)
+
+
+def frame_of(sorted_ids: torch.Tensor) -> FrameState | None:
+    """The FrameState attached by vertex_and_tile_shader, if ``sorted_ids`` is
+    the tensor it returned (a copy or slice carries none; the blend then packs
+    every tet, with the same results)."""
+    return getattr(sorted_ids, "rm_frame", None)
+
+
 def split_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCamera, fine_shift: int,
                      footprint: torch.Tensor, bounds: torch.Tensor, sorted_keys: torch.Tensor,
-                     pool: ScratchPool | None = None) -> FineLists:
+                     pool: ScratchPool | None = None, status: torch.Tensor | None = None) -> FineLists:
     """Split the sorted coarse lists (ids and keys) into the fine lists for
     the jitter bounds ``bounds`` (rm_fine_lists, no host synchronisation)."""
     pool = pool or _POOL
@@ -380,7 +466,7 @@ def split_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCame
     _call("rm_fine_lists", lambda: L.rm_fine_lists(C.ptr(sorted_keys), C.ptr(sorted_ids), P, None, C.ptr(ranges),
                                                    C.ptr(footprint), C.ptr(bounds), ctypes.byref(cam), fine_shift,
                                                    cap, C.ptr(fine_ids), C.ptr(fine_ranges), C.ptr(total), C.ptr(ws),
-                                                   ws_n, _stream()))
+                                                   ws_n, C.ptr(status), _stream()))
     return FineLists(fine_shift, camf, _cam_key(cam), fine_ids, fine_ranges, total)
 
 
@@ -395,7 +481,7 @@ def fine_lists_of(sorted_ids: torch.Tensor, cam: RMCamera, ray_jitter: torch.Ten
         return pend.lists
     bounds = jitter_bounds(ray_jitter)
     pend.lists = split_fine_lists(sorted_ids, pend.ranges, pend.coarse_cam, pend.shift, pend.footprint, bounds,
-                                  pend.sorted_keys)
+                                  pend.sorted_keys, status=pend.status)
     pend.jitter, pend.jitter_version = ray_jitter, ray_jitter._version
     return pend.lists
 

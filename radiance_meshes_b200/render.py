@@ -1,7 +1,7 @@
 """``render()`` with the reference's signature and outputs (utils/train_util.py:15-77).
 
 ``camera`` is any object with ``image_height``, ``image_width``,
-``gt_alpha_mask`` (optional) and ``to_dict(device)`` returning the reference's
+``gt_alpha_mask`` and ``to_dict(device)`` returning the reference's
 camera keys (data/camera.py:72-91); ``model`` has ``vertices``, ``indices`` and,
 when ``cell_values`` is not given, ``get_cell_values``/``feature_dim``/
 ``mask_values`` as in the reference.  ``rasterize()`` is the same pipeline for
@@ -16,7 +16,15 @@ from .delaunay_rasterization.internal.alphablend_tiled_slang_interp import Alpha
 from .delaunay_rasterization.internal.render_grid import RenderGrid
 from .delaunay_rasterization.internal.tile_shader_slang import vertex_and_tile_shader
 
-__all__ = ["render", "rasterize", "distortion_loss"]
+__all__ = ["render", "rasterize", "distortion_loss", "weigh_degree"]
+
+
+def weigh_degree(sh_coeffs: torch.Tensor, values) -> torch.Tensor:
+    """Per-coefficient weight by SH degree, shape [1, C, 1]: coefficient i has
+    degree floor(sqrt(i)) and gets values[degree] (utils/eval_sh_py.py:28-40)."""
+    C = sh_coeffs.shape[1]
+    degrees = torch.floor(torch.sqrt(torch.arange(C, device=sh_coeffs.device, dtype=torch.float32))).long()
+    return torch.tensor(values, device=sh_coeffs.device, dtype=sh_coeffs.dtype)[degrees].view(1, C, 1)
 
 
 def distortion_loss(distortion_img: torch.Tensor) -> torch.Tensor:
@@ -35,7 +43,7 @@ def rasterize(vertices, indices, cell_values, tcam: dict, ray_jitter=None):
         ray_jitter = torch.full((H, W, 2), 0.5, device=vertices.device)
     sorted_ids, ranges, vs, cc, mask, rect = vertex_and_tile_shader(indices, vertices, tcam, grid)
     img, dist, _ = AlphaBlendTiledRender.apply(sorted_ids, ranges, indices, vertices, cell_values, grid, tcam,
-                                               ray_jitter, "cuda", mask.to(torch.int32))
+                                               ray_jitter)
     return img, dist, dict(sorted_tetra_idx=sorted_ids, tile_ranges=ranges, mask=mask, vs_tetra=vs,
                            circumcenter=cc, rect_tile_space=rect)
 
@@ -65,15 +73,12 @@ def render(camera, model, cell_values=None, tile_size=16, min_t=0.1, scene_scali
             cell_values[mask] = values
         else:
             shs, cell_values = model.get_cell_values(camera, all_circumcenters=circumcenter)
-        sh_reg = (shs ** 2).mean() if shs is not None else 0
+        weighting = weigh_degree(shs, [0, 0.1, 0.5, 1])  # utils/train_util.py:52-53
+        sh_reg = ((weighting * shs) ** 2).mean()
     image_rgb, distortion_img, tet_alive = AlphaBlendTiledRender.apply(
-        sorted_tetra_idx, tile_ranges, model.indices, vertices, cell_values, render_grid, tcam, ray_jitter,
-        "cuda", mask.to(torch.int32))
+        sorted_tetra_idx, tile_ranges, model.indices, vertices, cell_values, render_grid, tcam, ray_jitter)
     alpha = image_rgb.permute(2, 0, 1)[3, ...]
-    gt_mask = getattr(camera, "gt_alpha_mask", None)
-    rgb = image_rgb.permute(2, 0, 1)[:3, ...]
-    if gt_mask is not None:
-        rgb = rgb * gt_mask.to(device)
+    rgb = image_rgb.permute(2, 0, 1)[:3, ...] * camera.gt_alpha_mask.to(device)
     return {
         "render": rgb,
         "alpha": alpha,

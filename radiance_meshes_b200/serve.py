@@ -114,7 +114,7 @@ class _Batch:
     rast: B.BatchedRasterizer
     stream: torch.cuda.Stream
     done: torch.cuda.Event
-    total_host: torch.Tensor
+    total_host: torch.Tensor  # [pair count, status word] of the batch, copied back with the images
     nbytes: int
     retried: bool = False
 
@@ -233,8 +233,9 @@ class Server:
                                        fwd_flags=self.fwd_flags, records=mesh.records, hit_masks=False,
                                        fine_shift=self.fine_shift)
             rast.forward()
-            total_host = torch.empty(1, dtype=torch.int64, pin_memory=True)
-            total_host.copy_(rast.total, non_blocking=True)
+            total_host = torch.empty(2, dtype=torch.int64, pin_memory=True)
+            total_host[0:1].copy_(rast.total, non_blocking=True)
+            total_host[1:2].copy_(rast.status, non_blocking=True)
             done = torch.cuda.Event(enable_timing=True)
             done.record(stream)
         self.reserved += need
@@ -252,7 +253,13 @@ class Server:
             if not b.done.query():
                 still.append(b)
                 continue
-            P = int(b.total_host.item())
+            P = int(b.total_host[0])
+            bits = int(b.total_host[1]) & 0xffffffff & ~C.RM_STATUS_CAPACITY
+            if bits:  # bad mesh data or a wait that gave up: the batch's images are not valid
+                self.reserved -= b.nbytes
+                self.free_streams.append(b.stream_idx)
+                self.inflight = [x for x in self.inflight if x is not b]
+                raise C.DeviceStatusError(bits, f"serving batch {b.bid} on mesh {b.mesh.name}")
             if P > b.rast.capacity:
                 # overflow: re-run this batch with the exact pair count on the same stream
                 self.n_retries += 1

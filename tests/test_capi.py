@@ -38,10 +38,37 @@ def test_struct_layout():
 
 def test_size_queries():
     L = C.lib()
-    assert L.rm_abi_version() == 1
+    assert L.rm_abi_version() == 2
     assert L.rm_blend_workspace_size(1000, 300) >= 1000 * 128 + 300 * 4
     assert L.rm_scan_workspace_size(5000) >= 16 + 8 * 2
     assert L.rm_sort_workspace_size(1_000_000) > 12 * 1_000_000
+
+
+def test_wait_limit_setting():
+    """The bounded-wait limit is a process-wide setting; 0 restores the
+    default (no device work involved)."""
+    default = C.wait_limit()
+    assert default == 1 << 22
+    try:
+        C.set_wait_limit(7)
+        assert C.wait_limit() == 7
+    finally:
+        C.set_wait_limit(0)
+    assert C.wait_limit() == default
+
+
+def test_status_words_in_words():
+    assert C.status_code(C.RM_STATUS_SCAN_TIMEOUT | C.RM_STATUS_BAD_INDEX) == C.RM_ETIMEOUT
+    assert C.status_code(C.RM_STATUS_CAPACITY) == C.RM_ECAPACITY
+    assert C.status_code(C.RM_STATUS_NONFINITE) == C.RM_EINVAL
+    assert C.status_code(0) == C.RM_OK
+    err = C.DeviceStatusError(C.RM_STATUS_BAD_INDEX | C.RM_STATUS_OVERFLOW, "x")
+    assert isinstance(err, RuntimeError) and err.code == C.RM_EINVAL
+    assert "outside [0, n_verts)" in str(err) and "INT32_MAX" in str(err)
+
+
+def test_noalloc_status_rejects_null():
+    assert C.lib().rm_scan_noalloc_read_status(None, None) == C.RM_EINVAL
 
 
 def _cam():
@@ -58,25 +85,25 @@ def test_camera_types_and_distortion():
         cam = _cam()
         cam.camera_type = ctype
         cam.distortion[0] = 0.1
-        rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None)
+        rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None, None)
         assert rc == C.RM_EINVAL and "NULL" in C.last_error()
     cam = _cam()
     cam.camera_type = 2
-    rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None)
+    rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None, None)
     assert rc == C.RM_EINVAL and "camera_type" in C.last_error()
     cam = _cam()
     cam.distortion[1] = float("nan")
-    rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None)
+    rc = L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None, None)
     assert rc == C.RM_EINVAL and "NaN" in C.last_error()
 
 
 def test_rejects_null_and_misaligned():
     L = C.lib()
     cam = _cam()
-    assert L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None) == C.RM_EINVAL
+    assert L.rm_project_fwd(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None, None) == C.RM_EINVAL
     assert "NULL" in C.last_error()
-    assert L.rm_sort_pairs(None, None, 10, None, 0, None, None, None, 0, None) == C.RM_EINVAL
-    assert L.rm_sort_pairs(None, None, 10, None, 65, None, None, None, 0, None) == C.RM_EINVAL
+    assert L.rm_sort_pairs(None, None, 10, None, 0, None, None, None, 0, None, None) == C.RM_EINVAL
+    assert L.rm_sort_pairs(None, None, 10, None, 65, None, None, None, 0, None, None) == C.RM_EINVAL
     # unsupported tile size
     cam.tile_width = 5
     cam.tile_height = 5
@@ -90,8 +117,8 @@ def test_rejects_null_and_misaligned():
 def test_zero_sizes_are_noops():
     L = C.lib()
     cam = _cam()
-    assert L.rm_project_fwd(None, None, 0, 0, ctypes.byref(cam), None, None, None, None, None) == C.RM_OK
-    assert L.rm_sort_pairs(None, None, 0, None, 40, None, None, None, 0, None) == C.RM_OK
+    assert L.rm_project_fwd(None, None, 0, 0, ctypes.byref(cam), None, None, None, None, None, None) == C.RM_OK
+    assert L.rm_sort_pairs(None, None, 0, None, 40, None, None, None, 0, None, None) == C.RM_OK
     assert L.rm_emit_pairs(None, None, None, 0, 1, 0, None, None, None, None, None) == C.RM_OK
 
 
@@ -153,11 +180,11 @@ def test_view_batch_rejects_bad_batches():
     many = (RMCamera * (C.RM_MAX_VIEWS + 1))(*([cams[0]] * (C.RM_MAX_VIEWS + 1)))
     assert L.rm_views_tile_count(many, C.RM_MAX_VIEWS + 1) == -1
     assert L.rm_views_tile_count(arr, 0) == -1
-    rc = L.rm_project_fwd_multi(None, None, 10, 10, arr, 2, None, None, None, None, None, None, None)
+    rc = L.rm_project_fwd_multi(None, None, 10, 10, arr, 2, None, None, None, None, None, None, None, None)
     assert rc == C.RM_EINVAL
     ok = (RMCamera * 2)(*cams)
-    assert L.rm_project_fwd_multi(None, None, 10, 10, ok, 2, None, None, None, None, None, None, None) == C.RM_EINVAL
-    assert L.rm_project_fwd_multi(None, None, 0, 0, ok, 2, None, None, None, None, None, None, None) == C.RM_OK
+    assert L.rm_project_fwd_multi(None, None, 10, 10, ok, 2, None, None, None, None, None, None, None, None) == C.RM_EINVAL
+    assert L.rm_project_fwd_multi(None, None, 0, 0, ok, 2, None, None, None, None, None, None, None, None) == C.RM_OK
     assert L.rm_emit_pairs_multi(None, None, None, 0, ok, 2, 0, None, None, None, None, None, None, None) == C.RM_OK
 
 
@@ -217,9 +244,9 @@ def test_fine_list_entry_points_validate():
     L = C.lib()
     cam = _cam()
     cams = (RMCamera * 1)(cam)
-    rc = L.rm_project_fwd_fine(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None, None)
+    rc = L.rm_project_fwd_fine(None, None, 10, 10, ctypes.byref(cam), None, None, None, None, None, None, None)
     assert rc == C.RM_EINVAL and "NULL" in C.last_error()
-    assert L.rm_project_fwd_fine(None, None, 0, 0, ctypes.byref(cam), None, None, None, None, None, None) == C.RM_OK
+    assert L.rm_project_fwd_fine(None, None, 0, 0, ctypes.byref(cam), None, None, None, None, None, None, None) == C.RM_OK
     assert L.rm_jitter_bounds_workspace_size() >= 16
     assert L.rm_jitter_bounds(None, 10, None, None, 0, None) == C.RM_EINVAL
     assert L.rm_jitter_bounds(8, 10, 16, 16, 0, None) == C.RM_EINVAL and "workspace" in C.last_error()
@@ -228,14 +255,14 @@ def test_fine_list_entry_points_validate():
     assert L.rm_fine_lists_workspace_size(1000, 1_000_000, 1) >= small + 1_000_000 - 256
     assert L.rm_fine_lists_workspace_size(1000, 1_000_000, 3) >= 8 * 1_000_000
     ws = 1 << 30
-    rc = L.rm_fine_lists(16, 16, 10, None, 16, None, 16, ctypes.byref(cam), 1, 10, 16, 16, 16, 256, ws, None)
+    rc = L.rm_fine_lists(16, 16, 10, None, 16, None, 16, ctypes.byref(cam), 1, 10, 16, 16, 16, 256, ws, None, None)
     assert rc == C.RM_EINVAL and "footprint" in C.last_error()
-    rc = L.rm_fine_lists(16, 16, 10, None, 16, 16, None, ctypes.byref(cam), 1, 10, 16, 16, 16, 256, ws, None)
+    rc = L.rm_fine_lists(16, 16, 10, None, 16, 16, None, ctypes.byref(cam), 1, 10, 16, 16, 16, 256, ws, None, None)
     assert rc == C.RM_EINVAL and "jitter_bounds" in C.last_error()
-    rc = L.rm_fine_lists(16, 16, 10, None, 16, 16, 16, ctypes.byref(cam), 4, 10, 16, 16, 16, 256, ws, None)
+    rc = L.rm_fine_lists(16, 16, 10, None, 16, 16, 16, ctypes.byref(cam), 4, 10, 16, 16, 16, 256, ws, None, None)
     assert rc == C.RM_EINVAL and "fine_shift" in C.last_error()
-    rc = L.rm_fine_lists(16, 16, 10, None, 16, 24, 16, ctypes.byref(cam), 1, 10, 16, 16, 16, 256, ws, None)
+    rc = L.rm_fine_lists(16, 16, 10, None, 16, 24, 16, ctypes.byref(cam), 1, 10, 16, 16, 16, 256, ws, None, None)
     assert rc == C.RM_EINVAL and "misaligned" in C.last_error()
     # packed bits (no footprint) only for a 2x split
-    rc = L.rm_fine_lists_multi(16, 16, 10, None, 16, None, None, 10, cams, 1, 2, 10, 16, 16, 16, 256, ws, None)
+    rc = L.rm_fine_lists_multi(16, 16, 10, None, 16, None, None, 10, cams, 1, 2, 10, 16, 16, 16, 256, ws, None, None)
     assert rc == C.RM_EINVAL and "packed" in C.last_error()

@@ -110,8 +110,7 @@ def _dropin_step(mesh, view, jitter, fine, tile=16, cam_shift=None):
         idx = to_dev(mesh.indices)
         sorted_ids, ranges, vs, cc, mask, rect = vertex_and_tile_shader(idx, verts, tcam, grid)
         assert (getattr(sorted_ids, "rm_fine", None) is not None) == fine
-        img, dist, _ = AlphaBlendTiledRender.apply(sorted_ids, ranges, idx, verts, cv, grid, tcam, jitter, "cuda",
-                                                   mask.to(torch.int32))
+        img, dist, _ = AlphaBlendTiledRender.apply(sorted_ids, ranges, idx, verts, cv, grid, tcam, jitter)
         g = torch.Generator(device="cuda").manual_seed(2)
         w = torch.randn(img.shape, device="cuda", generator=g)
         wd = torch.randn(dist.shape, device="cuda", generator=g) * 0.01

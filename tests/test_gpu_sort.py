@@ -26,7 +26,7 @@ def gpu_sort(keys, vals, end_bit, n_dev=None):
     if n_dev is not None:
         nd = torch.tensor([n_dev], dtype=torch.int64, device="cuda")
     C.check(L.rm_sort_pairs(C.ptr(k), C.ptr(v), n, C.ptr(nd), end_bit, C.ptr(ko), C.ptr(vo), C.ptr(ws), ws_n,
-                            C.stream_handle()), "sort")
+                            None, C.stream_handle()), "sort")
     st = ctypes.c_uint32(0)
     C.check(L.rm_read_status(C.ptr(ws), ctypes.byref(st), C.stream_handle()))
     assert st.value == 0

@@ -2,6 +2,8 @@
 FP32 restatement, including colour, uses the host libm, identical across
 machines running this image), and the FP64 integrator within float32
 storage precision."""
+import os
+
 import numpy as np
 import pytest
 
@@ -33,3 +35,19 @@ def test_golden_cover_reference_scenarios():
         assert any(n.startswith(fam) for n in names), fam
     z, _ = G.load("multi_tet_random_point")
     assert len(z["sorted_ids"]) == 0  # empty pair list (camera on the hull looking out)
+
+
+def test_weigh_degree_matches_reference_sh_reg():
+    """render()'s sh_reg = mean((weigh_degree(shs, [0, 0.1, 0.5, 1]) * shs)^2)
+    (utils/train_util.py:52-53) reproduces the value the reference's own
+    render() computed for the fixture (tests/golden/make_ref_golden.py)."""
+    import torch
+
+    from radiance_meshes_b200.render import weigh_degree
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_render.npz"))
+    shs = torch.tensor(g["sh"])[torch.tensor(g["mask"])]
+    sh_reg = ((weigh_degree(shs, [0, 0.1, 0.5, 1]) * shs) ** 2).mean()
+    assert abs(float(sh_reg) - float(g["sh_reg"])) <= 1e-7 * abs(float(g["sh_reg"]))
+    w = weigh_degree(torch.zeros(1, 15, 3), [0, 0.1, 0.5, 1]).reshape(-1)
+    assert w.tolist() == pytest.approx([0] + [0.1] * 3 + [0.5] * 5 + [1] * 6)

@@ -49,6 +49,42 @@ def test_no_alloc_scan_matches_workspace_scan(cuda):
         assert int(tot.item()) == int(ref_tot.item()) == int(tiles.sum().item())
 
 
+def _noalloc_status():
+    st = ctypes.c_uint32(0)
+    C.check(C.lib().rm_scan_noalloc_read_status(ctypes.byref(st), C.stream_handle()), "noalloc status")
+    return st.value
+
+
+def test_no_alloc_scan_reports_through_its_status_word(cuda):
+    """The fixed scratch has its own status word, read (and cleared) with
+    rm_scan_noalloc_read_status: a total beyond int32 and a look-back that
+    gives up (a wait limit of one poll) are reported there, and a clean call
+    leaves it zero."""
+    rng = np.random.default_rng(11)
+    tiles = torch.from_numpy(rng.integers(0, 9, size=3_000_000).astype(np.int32)).cuda()
+    _scan_no_alloc(tiles)
+    assert _noalloc_status() == 0
+    big = torch.full((600_000,), 4096, dtype=torch.int32, device="cuda")
+    _scan_no_alloc(big)
+    assert _noalloc_status() & C.RM_STATUS_OVERFLOW
+    assert _noalloc_status() == 0  # cleared by the read
+    seen = False
+    try:
+        C.set_wait_limit(1)
+        for _ in range(5):
+            _scan_no_alloc(tiles)
+            if _noalloc_status() & C.RM_STATUS_SCAN_TIMEOUT:
+                seen = True
+                break
+    finally:
+        C.set_wait_limit(0)
+    assert seen
+    off, tot = _scan_no_alloc(tiles)
+    ref_off, ref_tot = _scan_with_workspace(tiles)
+    torch.cuda.synchronize()
+    assert _noalloc_status() == 0 and torch.equal(off, ref_off) and int(tot.item()) == int(ref_tot.item())
+
+
 def test_no_alloc_scan_rejects_oversize():
     L = C.lib()
     rc = L.rm_scan_tiles_noalloc(None, (1 << 26) + 1, None, None, None)
