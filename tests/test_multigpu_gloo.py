@@ -53,6 +53,30 @@ def _worker(rank, world, port, out):
         dist.destroy_process_group()
 
 
+def _worker_overlapped(rank, world, port, out):
+    """Each view's gradient reduced while the rank's next view renders
+    (OverlappedGradSum); ranks with fewer views add zeros so the
+    collectives line up."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        mesh, views = _scene()
+        like = [torch.zeros(len(mesh.vertices), 3, dtype=torch.float64),
+                torch.zeros(len(mesh.indices), 7, dtype=torch.float64)]
+        ex = MG.OverlappedGradSum(like, in_flight=1)
+        mine = MG.views_for_rank(N_VIEWS, rank, world)
+        for k in mine:
+            ex.add_view(list(_view_grads(mesh, views[k], seed=k)))
+        for _ in range(MG.views_per_rank(N_VIEWS, world) - len(mine)):
+            ex.add_zero_view()
+        gv, gc = ex.result()
+        assert ex.views == MG.views_per_rank(N_VIEWS, world)
+        torch.save((gv, gc), os.path.join(out, f"rank{rank}.pt"))
+    finally:
+        dist.destroy_process_group()
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -67,8 +91,9 @@ def test_views_for_rank_partition():
         MG.views_for_rank(4, 2, 2)
 
 
-def test_two_rank_gradient_sum_matches_single_process(tmp_path):
-    mp.start_processes(_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+@pytest.mark.parametrize("worker", [_worker, _worker_overlapped], ids=["one_bucket", "overlapped_per_view"])
+def test_two_rank_gradient_sum_matches_single_process(tmp_path, worker):
+    mp.start_processes(worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True, start_method="spawn")
     mesh, views = _scene()
     gv = torch.zeros(len(mesh.vertices), 3, dtype=torch.float64)
     gc = torch.zeros(len(mesh.indices), 7, dtype=torch.float64)
@@ -76,6 +101,7 @@ def test_two_rank_gradient_sum_matches_single_process(tmp_path):
         a, b = _view_grads(mesh, views[k], seed=k)
         gv += a
         gc += b
+    assert MG.views_per_rank(N_VIEWS, 2) == 2  # rank 1 adds one zero view
     for r in range(2):
         rv, rc = torch.load(os.path.join(tmp_path, f"rank{r}.pt"))
         assert torch.allclose(rv, gv, rtol=1e-12, atol=1e-12)
