@@ -238,6 +238,9 @@ RM_API size_t rm_blend_workspace_size(int64_t n_tets, int64_t n_tiles);
 /* Extra workspace bytes for RM_BLEND_HIT_MASKS over n_pairs list entries in
  * n_tiles tiles of tile_pixels pixels (4 bytes per 32 entries per pixel). */
 RM_API size_t rm_blend_hit_mask_bytes(int64_t n_pairs, int64_t n_tiles, int tile_pixels);
+/* Byte offset, inside a workspace of rm_blend_workspace_size(n_tets, n_tiles)
+ * bytes, of the status word a blend pass uses when given no status_dev. */
+RM_API size_t rm_blend_status_offset(int64_t n_tets, int64_t n_tiles);
 
 #define RM_BLEND_REUSE_RECORDS 0x1  /* workspace already holds this frame's records */
 /* Hit masks: with this flag on rm_blend_fwd and rm_blend_bwd (same lists, same
@@ -249,6 +252,10 @@ RM_API size_t rm_blend_hit_mask_bytes(int64_t n_pairs, int64_t n_tiles, int tile
  * flag (or with 16-pixel items) marks the masks invalid, and the backward then
  * tests every entry. */
 #define RM_BLEND_HIT_MASKS 0x2
+/* Records of each shared-memory batch staged by bulk copies (cp.async.bulk
+ * from this GPU's memory, completing on an mbarrier; no multicast), two
+ * batches in flight, instead of per-thread loads.  Backward, 64-pixel items. */
+#define RM_BLEND_STAGE_TMA 0x4
 /* flags bits 8..15: log2 of the pixels per work item strip (16 or 64; 0 = 64) */
 #define RM_BLEND_STRIP_SHIFT 8
 #define RM_BLEND_STRIP(log2_pixels) ((log2_pixels) << RM_BLEND_STRIP_SHIFT)
@@ -270,7 +277,9 @@ RM_API size_t rm_blend_hit_mask_bytes(int64_t n_pairs, int64_t n_tiles, int tile
  * (delaunay_rasterization/internal/alphablend_tiled_slang_interp.py:165-202).
  * tiles_touched may be NULL; when given, records are packed only for visible
  * tets.  Writes every pixel of out_img [H,W,4], out_distortion [H,W,5] and
- * n_contrib [H,W].
+ * n_contrib [H,W].  A staging wait that gives up sets RM_STATUS_QUEUE_TIMEOUT
+ * in *status_dev (NULL: in the workspace word at rm_blend_status_offset,
+ * cleared by the call).
  */
 RM_API int rm_blend_fwd(const int32_t* sorted_ids, const int32_t* ranges,
                  const int32_t* indices, const float* vertices,
@@ -278,14 +287,15 @@ RM_API int rm_blend_fwd(const int32_t* sorted_ids, const int32_t* ranges,
                  const int32_t* tiles_touched, const float* ray_jitter,
                  const rm_camera* cam, float* out_img, float* out_distortion,
                  int32_t* n_contrib, void* workspace, size_t workspace_bytes,
-                 int flags, void* stream);
+                 int flags, uint32_t* status_dev, void* stream);
 
 /*
  * Back-to-front adjoint of the blend.  Replaces splat_tiled.bwd
  * (delaunay_rasterization/internal/alphablend_tiled_slang_interp.py:220-262),
  * i.e. bwd_alpha_blend (delaunay_rasterization/internal/slang/alphablend_shader_interp.slang:273-369).
  * grad_vertices [V,3] and grad_cell_values [T,7] are accumulated into; the
- * caller zeroes them.  grad_distortion may be NULL (zeros).
+ * caller zeroes them.  grad_distortion may be NULL (zeros).  status_dev as
+ * rm_blend_fwd.
  */
 RM_API int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges,
                  const int32_t* indices, const float* vertices,
@@ -295,7 +305,7 @@ RM_API int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges,
                  const float* out_distortion, const int32_t* n_contrib,
                  const float* grad_img, const float* grad_distortion,
                  float* grad_vertices, float* grad_cell_values, void* workspace,
-                 size_t workspace_bytes, int flags, void* stream);
+                 size_t workspace_bytes, int flags, uint32_t* status_dev, void* stream);
 
 /*
  * rm_project_fwd plus each tet's image footprint, footprint [T,12] float:
@@ -481,7 +491,8 @@ RM_API int rm_blend_fwd_multi(const int32_t* sorted_ids, const int32_t* ranges,
                               const rm_camera* cams, int n_views, float* out_img,
                               float* out_distortion, int32_t* n_contrib,
                               const void* records, void* workspace,
-                              size_t workspace_bytes, int flags, void* stream);
+                              size_t workspace_bytes, int flags, uint32_t* status_dev,
+                              void* stream);
 
 /* Adjoint of rm_blend_fwd_multi; gradients of all views are summed into
  * grad_vertices and grad_cell_values. */
@@ -494,7 +505,8 @@ RM_API int rm_blend_bwd_multi(const int32_t* sorted_ids, const int32_t* ranges,
                               const float* grad_img, const float* grad_distortion,
                               float* grad_vertices, float* grad_cell_values,
                               const void* records, void* workspace,
-                              size_t workspace_bytes, int flags, void* stream);
+                              size_t workspace_bytes, int flags, uint32_t* status_dev,
+                              void* stream);
 
 /* ------------------------------------------- densification statistics -- */
 /*

@@ -39,6 +39,7 @@ STATUS_TEXT = {
 
 RM_BLEND_REUSE_RECORDS = 0x1
 RM_BLEND_HIT_MASKS = 0x2
+RM_BLEND_STAGE_TMA = 0x4
 RM_BLEND_STRIP_SHIFT = 8
 RM_BLEND_HEAVY_SHIFT = 16
 RM_BLEND_PAIR_CTAS_SHIFT = 20
@@ -78,10 +79,11 @@ SIGNATURES = {
     "rm_tile_ranges": (ctypes.c_int, [vp, i64, vp, vp, i64, vp]),
     "rm_blend_workspace_size": (sz, [i64, i64]),
     "rm_blend_hit_mask_bytes": (sz, [i64, i64, ctypes.c_int]),
+    "rm_blend_status_offset": (sz, [i64, i64]),
     "rm_blend_fwd": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, vp, vp, vp, vp, sz,
-                                    ctypes.c_int, vp]),
+                                    ctypes.c_int, vp, vp]),
     "rm_blend_bwd": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, vp, vp, vp, vp, vp,
-                                    vp, vp, vp, sz, ctypes.c_int, vp]),
+                                    vp, vp, vp, sz, ctypes.c_int, vp, vp]),
     "rm_project_fwd_fine": (ctypes.c_int, [vp, vp, i64, i64, camp, vp, vp, vp, vp, vp, vp, vp]),
     "rm_jitter_bounds_workspace_size": (sz, []),
     "rm_jitter_bounds": (ctypes.c_int, [vp, i64, vp, vp, sz, vp]),
@@ -103,9 +105,9 @@ SIGNATURES = {
     "rm_blend_records_size": (sz, [i64]),
     "rm_blend_pack_records": (ctypes.c_int, [vp, vp, vp, i64, i64, vp, vp, vp]),
     "rm_blend_fwd_multi": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, ctypes.c_int, vp, vp, vp,
-                                          vp, vp, sz, ctypes.c_int, vp]),
+                                          vp, vp, sz, ctypes.c_int, vp, vp]),
     "rm_blend_bwd_multi": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, ctypes.c_int, vp, vp, vp,
-                                          vp, vp, vp, vp, vp, vp, sz, ctypes.c_int, vp]),
+                                          vp, vp, vp, vp, vp, vp, sz, ctypes.c_int, vp, vp]),
 }
 
 

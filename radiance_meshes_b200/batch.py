@@ -117,7 +117,8 @@ class BatchedRasterizer:
         self.offsets = torch.empty(n * T, dtype=torch.int32, device=dev)
         self.total = torch.zeros(1, dtype=torch.int64, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
-        self.scan_ws = torch.empty(L.rm_scan_workspace_size(n * T), dtype=torch.uint8, device=dev)
+        # zeroed: its first word is the scan's status word, which the scan keeps
+        self.scan_ws = torch.zeros(L.rm_scan_workspace_size(n * T), dtype=torch.uint8, device=dev)
         self.ranges = torch.empty((views.n_tiles, 2), dtype=torch.int32, device=dev)
         # records: per-tet blend records packed once per mesh (rm_blend_pack_records), shared by
         # every batch on it; without them each forward packs its own into the workspace
@@ -256,7 +257,8 @@ class BatchedRasterizer:
                                      C.ptr(self.vertices), C.ptr(self.cell_values), self.T, self.V,
                                      C.ptr(self.tiles_any), C.ptr(self.jitter), v.array, v.n, C.ptr(self.img),
                                      C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.records), C.ptr(self.blend_ws), self.blend_ws.numel(),
-                                     self.fwd_flags | (C.RM_BLEND_HIT_MASKS if self.hit_masks else 0), s))
+                                     self.fwd_flags | (C.RM_BLEND_HIT_MASKS if self.hit_masks else 0),
+                                     C.ptr(self.status), s))
 
     def _blend_bwd(self):
         L, s = C.lib(), C.stream_handle()
@@ -269,7 +271,7 @@ class BatchedRasterizer:
                                      C.ptr(self.dist), C.ptr(self.nc), C.ptr(self.grad_img), C.ptr(self.grad_dist),
                                      C.ptr(self.grad_vertices), C.ptr(self.grad_cell_values), C.ptr(self.records), C.ptr(self.blend_ws),
                                      self.blend_ws.numel(), self.bwd_flags | C.RM_BLEND_REUSE_RECORDS |
-                                     (C.RM_BLEND_HIT_MASKS if self.hit_masks else 0), s),
+                                     (C.RM_BLEND_HIT_MASKS if self.hit_masks else 0), C.ptr(self.status), s),
                 "rm_blend_bwd_multi")
 
     # ---------------------------------------------------------------- API --

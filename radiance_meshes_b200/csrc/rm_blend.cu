@@ -277,6 +277,8 @@ struct Queue {
     int subs;  // strips per tile
     bool heavy;
     HitMasks hm;
+    uint32_t* status;     // RM_STATUS_* bits of the pass (a staging copy whose wait gave up)
+    uint32_t spin_limit;  // polls of a bounded wait
 };
 
 __device__ __forceinline__ int queue_items(const Queue& q) {
@@ -1010,6 +1012,208 @@ __device__ __forceinline__ void bwd_dense_item(
     }
 }
 
+// Dense backward with the records staged by bulk copies (RM_BLEND_STAGE_TMA;
+// 64-pixel items).  The walk and its arithmetic are bwd_dense_item's; what
+// changes is the staging.  Each batch is planned one batch ahead: its hit
+// masks are OR-ed over the item, the entries some pixel hit are listed, their
+// tet ids loaded, and warp 0 starts one 128-byte cp.async.bulk per entry
+// (global -> this CTA's shared memory, completing on the buffer's mbarrier).
+// Two record buffers alternate, so batch k+1's copies are in flight while
+// batch k is walked and flushed; nothing of this GPU's memory is multicast.
+template <int B>
+struct BwdTmaSmem {
+    float4 srec[2][B][kRecFloat4];
+    float sacc[B][kNGrad];
+    int32_t sid[2][B];
+    uint8_t cidx[2][B];
+    int32_t n_keep[2];
+    uint32_t sor[2][2];  // per warp: OR of its pixels' hit bits (two 32-entry blocks)
+    int32_t smax[2];
+    uint64_t bar[2];
+};
+
+// Pipeline position carried across work items: the buffer the next plan
+// fills and the parity of each buffer's next completion.
+struct TmaPipe {
+    uint32_t buf;
+    uint32_t parity;  // bit b: parity to wait for on buffer b
+};
+
+template <int B>
+__device__ __forceinline__ void bwd_tma_plan(BwdTmaSmem<B>& S, int b, int lo, int top, int rgx,
+                                             const int32_t* __restrict__ ids, const float4* __restrict__ recs,
+                                             const HitMasks& hm, int gtile, int sub, int subs, uint32_t& hw0,
+                                             uint32_t& hw1) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n = top - lo;
+    const int kb0 = (lo - rgx) >> 5, kb1 = (top - 1 - rgx) >> 5;
+    hw0 = 0xffffffffu;
+    hw1 = 0xffffffffu;
+    if (hm.words) {
+        const int64_t i0 = mask_word(gtile, rgx, kb0, sub, subs, (int)threadIdx.x);
+        const int64_t i1 = mask_word(gtile, rgx, kb1, sub, subs, (int)threadIdx.x);
+        if (i0 < hm.cap) hw0 = __ldcg(hm.words + i0);
+        if (i1 < hm.cap) hw1 = __ldcg(hm.words + i1);
+    }
+    uint32_t o0 = hw0, o1 = hw1;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        o0 |= __shfl_xor_sync(0xffffffffu, o0, off);
+        o1 |= __shfl_xor_sync(0xffffffffu, o1, off);
+    }
+    if (lane == 0) {
+        S.sor[warp][0] = o0;
+        S.sor[warp][1] = o1;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t c0 = S.sor[0][0] | S.sor[1][0], c1 = S.sor[0][1] | S.sor[1][1];
+        int base_c = 0;
+        for (int k0 = 0; k0 < n; k0 += 32) {
+            const int k = k0 + lane;
+            bool keep = false;
+            if (k < n) {
+                const int off = lo + k - rgx;
+                keep = ((((off >> 5) == kb0 ? c0 : c1) >> (off & 31)) & 1u) != 0u;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (keep) S.cidx[b][base_c + __popc(bal & ((1u << lane) - 1u))] = (uint8_t)k;
+            base_c += __popc(bal);
+        }
+        if (lane == 0) S.n_keep[b] = base_c;
+    }
+    __syncthreads();
+    const int nk = S.n_keep[b];
+    for (int k = threadIdx.x; k < nk; k += 64) S.sid[b][k] = __ldg(ids + lo + S.cidx[b][k]);
+    __syncthreads();
+    if (warp == 0) {
+        // every read of this buffer (the batch two back) is behind the barriers above
+        fence_proxy_async_smem();
+        if (lane == 0) mbar_arrive_expect_tx(&S.bar[b], (uint32_t)nk * (uint32_t)(kRecFloat4 * sizeof(float4)));
+        __syncwarp();
+        for (int k = lane; k < nk; k += 32)
+            bulk_copy_g2s(&S.srec[b][k][0], recs + (int64_t)kRecFloat4 * S.sid[b][k],
+                          (uint32_t)(kRecFloat4 * sizeof(float4)), &S.bar[b]);
+    }
+}
+
+template <int B>
+__device__ __forceinline__ void bwd_dense_item_tma(
+    int tile, int sub, const int32_t* __restrict__ ids, const int2* __restrict__ ranges,
+    const float4* __restrict__ recs, const int4* __restrict__ indices, const float2* __restrict__ jitter,
+    const rm_camera& cam, const float4* __restrict__ img, const float* __restrict__ dist,
+    const int32_t* __restrict__ ncs, const float4* __restrict__ gimg, const float* __restrict__ gdist,
+    float* __restrict__ gverts, float* __restrict__ gcv, BwdTmaSmem<B>& S, const HitMasks& hm, int subs, int gtile,
+    TmaPipe& pipe, const Queue& q) {
+    constexpr int NT = 64;
+    const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
+    int lx, ly;
+    strip_pixel<NT>(cam, sub, (int)threadIdx.x, lx, ly);
+    const int px = tx * cam.tile_width + lx, py = ty * cam.tile_height + ly;
+    const bool inside = px < cam.image_width && py < cam.image_height;
+    const int64_t pix = (int64_t)py * cam.image_width + px;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    f3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
+    float logT = 0.f, D2 = 0.f, D3 = 0.f;
+    float dS_c[3] = {0.f, 0.f, 0.f}, dS_logT = 0.f, dS_D[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    int32_t nc = 0;
+    if (inside) {
+        const float2 j = __ldg(jitter + pix);
+        make_ray(cam, px, py, j.x, j.y, o, d);
+        logT = __ldg(img + pix).w;
+        D2 = __ldg(dist + 5 * pix + 2);
+        D3 = __ldg(dist + 5 * pix + 3);
+        const float4 g = __ldg(gimg + pix);
+        dS_c[0] = g.x; dS_c[1] = g.y; dS_c[2] = g.z; dS_logT = g.w;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) dS_D[k] = gdist ? __ldg(gdist + 5 * pix + k) : 0.f;
+        nc = __ldg(ncs + pix);
+    }
+    int32_t m = nc;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if (lane == 0) S.smax[warp] = m;
+    __syncthreads();
+    const int32_t tile_max = max(S.smax[0], S.smax[1]);
+    const int2 rg = __ldg(ranges + tile);
+    const int end = min(rg.y, rg.x + tile_max);
+    if (end <= rg.x) return;  // uniform over the CTA
+    // batches aligned to multiples of B from the list start (at most two mask blocks each)
+    int ctop = end, clo = rg.x + ((end - 1 - rg.x) / B) * B;
+    uint32_t cw0, cw1;
+    int cb = (int)pipe.buf;
+    bwd_tma_plan<B>(S, cb, clo, ctop, rg.x, ids, recs, hm, gtile, sub, subs, cw0, cw1);
+    pipe.buf ^= 1u;
+    for (;;) {
+        const int ntop = clo;
+        const bool has_next = ntop > rg.x;
+        int nlo = 0, nb = 0;
+        uint32_t nw0 = 0u, nw1 = 0u;
+        if (has_next) {  // the next batch's copies run while this one is walked
+            nlo = rg.x + ((ntop - 1 - rg.x) / B) * B;
+            nb = (int)pipe.buf;
+            bwd_tma_plan<B>(S, nb, nlo, ntop, rg.x, ids, recs, hm, gtile, sub, subs, nw0, nw1);
+            pipe.buf ^= 1u;
+        }
+        const int nk = S.n_keep[cb];
+        for (int k = threadIdx.x; k < nk * kNGrad; k += NT) (&S.sacc[0][0])[k] = 0.f;
+        __syncthreads();
+        if (!mbar_wait(&S.bar[cb], (pipe.parity >> cb) & 1u, q.spin_limit)) {
+            if (threadIdx.x == 0 && q.status) atomicOr(q.status, RM_STATUS_QUEUE_TIMEOUT);
+            mbar_wait(&S.bar[cb], (pipe.parity >> cb) & 1u, q.spin_limit);  // let the copies land before reuse
+        }
+        pipe.parity ^= 1u << cb;
+        const int kb0 = (clo - rg.x) >> 5;
+        for (int jj = nk - 1; jj >= 0; --jj) {
+            const int off = clo + S.cidx[cb][jj] - rg.x;
+            // with the forward's masks, only its hits are revisited
+            const uint32_t hw = (off >> 5) == kb0 ? cw0 : cw1;
+            const bool act = inside && off < nc && ((hw >> (off & 31)) & 1u);
+            if (!__any_sync(0xffffffffu, act)) continue;
+            const float4* qr = S.srec[cb][jj];
+            float gl[kNGrad];
+#pragma unroll
+            for (int k = 0; k < kNGrad; ++k) gl[k] = 0.f;
+            const Isect is = intersect<true>(qr, o, d);
+            const float density = qr[0].w;
+            Segment sg;
+            sg.dt = fmaxf(is.exit - is.enter, 0.f);
+            sg.a = density * sg.dt;
+            const bool hit = act && is.geo && sg.a > 0.f;
+            if (hit) {
+                integrate(qr, o, d, is.enter, is.exit, sg);
+                const float m1 = density * (is.exit + is.enter) / 2.0f;
+                const float logT_old = logT + sg.a;
+                const float T = __expf(logT_old);
+                D2 = D2 - density;
+                D3 = D3 - m1;
+                logT = logT_old;
+                float nD2, nD3;
+                dS_logT = hit_grads(qr, o, d, is, sg, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
+                dS_D[2] = nD2;
+                dS_D[3] = nD3;
+            }
+            if (__any_sync(0xffffffffu, hit)) {
+                using RS = ReduceScatter<kNGrad, 16>;
+                int slot = 0;
+                RS::template run<0xffffffffu>(gl, lane, slot);
+#pragma unroll
+                for (int r = 0; r < RS::R; ++r)
+                    if (slot + r < kNGrad && gl[r] != 0.f) atomicAdd(&S.sacc[jj][slot + r], gl[r]);
+            }
+        }
+        __syncthreads();
+        flush_entries<NT, B>(nk, S.srec[cb], S.sid[cb], S.sacc, indices, gverts, gcv);
+        __syncthreads();
+        if (!has_next) break;
+        cb = nb;
+        clo = nlo;
+        ctop = ntop;
+        cw0 = nw0;
+        cw1 = nw1;
+    }
+}
+
 // Pair backward item: the same strip / thread split as the forward.  Per
 // batch of B entries (walked back to front) the pixels that still have list
 // offsets below their n_contributors are compacted into slots and
@@ -1243,6 +1447,36 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 512 / NT : 16)) blend_bwd_dens
     }
 }
 
+template <int B, class V>
+__global__ void __launch_bounds__(64, 8) blend_bwd_dense_tma_kernel(
+    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
+    const int4* __restrict__ indices, const float2* __restrict__ jitter, const __grid_constant__ V views,
+    const float4* __restrict__ img, const float* __restrict__ dist, const int32_t* __restrict__ ncs,
+    const float4* __restrict__ gimg, const float* __restrict__ gdist, float* __restrict__ gverts,
+    float* __restrict__ gcv, const Queue q) {
+    __shared__ BwdTmaSmem<B> S;
+    __shared__ int s_item;
+    if (threadIdx.x == 0) {
+        mbar_init(&S.bar[0], 1);
+        mbar_init(&S.bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const int n_items = queue_items(q);
+    const HitMasks hm = live_masks(q.hm);
+    TmaPipe pipe = {0u, 0u};
+    for (;;) {
+        const int item = next_item(q, &s_item);
+        if (item >= n_items) return;
+        const int t = queue_tile(q, item), v = views.find(t);
+        const int tb = views.tile_base(v);
+        const int64_t pb = views.pixel_base(v);
+        bwd_dense_item_tma<B>(t - tb, item % q.subs, ids, ranges + tb, recs, indices, jitter + pb,
+                              views.camera(v), img + pb, dist + 5 * pb, ncs + pb, gimg + pb,
+                              gdist ? gdist + 5 * pb : nullptr, gverts, gcv, S, hm, q.subs, t, pipe, q);
+    }
+}
+
 template <int PX, int NT, int B, class V>
 __global__ void __launch_bounds__(NT, 512 / NT) blend_bwd_pair_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
@@ -1412,12 +1646,18 @@ struct BlendWs {
     int32_t* order;
     int32_t* info;
     uint32_t* tickets;
+    uint32_t* status;       // the pass's status word when the caller passes none
+
     uint32_t* mask_header;  // nullptr: the workspace has no room for hit masks
     uint32_t* mask_words;
     int64_t mask_cap;
 };
 
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+// Byte offset of the status word inside the 256-byte header that follows the
+// records and the tile order (info at 0, queue tickets at 64).
+constexpr size_t kBlendStatusOff = 128;
 
 size_t blend_ws_bytes(int64_t n_tets, int64_t n_tiles) {
     const size_t rec = align256((size_t)(n_tets > 0 ? n_tets : 1) * kRecFloat4 * sizeof(float4));
@@ -1432,7 +1672,7 @@ BlendWs blend_ws(void* base, int64_t n_tets, int64_t n_tiles, size_t workspace_b
     const size_t rec = align256((size_t)(n_tets > 0 ? n_tets : 1) * kRecFloat4 * sizeof(float4));
     const size_t ord = align256((size_t)(n_tiles > 0 ? n_tiles : 1) * sizeof(int32_t));
     BlendWs w = {(float4*)p, (int32_t*)(p + rec), (int32_t*)(p + rec + ord), (uint32_t*)(p + rec + ord + 64),
-                 nullptr, nullptr, 0};
+                 (uint32_t*)(p + rec + ord + kBlendStatusOff), nullptr, nullptr, 0};
     const size_t end = rec + ord + 256;
     if (workspace_bytes >= end + 256 + 64 * sizeof(uint32_t)) {
         w.mask_header = (uint32_t*)(p + end);
@@ -1444,19 +1684,39 @@ BlendWs blend_ws(void* base, int64_t n_tets, int64_t n_tiles, size_t workspace_b
 
 // Persistent grid: as many CTAs as fit on the device at once (cached per
 // kernel instantiation and device).
+// Resident CTAs of a persistent kernel on the current device (SMs x CTAs per
+// SM), cached per (kernel, device, block shape): kernels of one signature
+// differ in their resource use, so the kernel's address is part of the key.
+struct GridKey {
+    const void* kernel;
+    int dev, threads, smem, blocks;
+};
+std::mutex g_grid_mu;
+GridKey g_grid_cache[64];
+int g_grid_used = 0;
+
 template <typename K>
 int persistent_grid(K kernel, int threads, int smem, int n_items) {
-    static thread_local int cached_dev = -1, cached_blocks = 0;
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev != cached_dev) {
+    const void* kp = (const void*)kernel;
+    int blocks = -1;
+    {
+        std::lock_guard<std::mutex> lock(g_grid_mu);
+        for (int i = 0; i < g_grid_used; ++i) {
+            const GridKey& k = g_grid_cache[i];
+            if (k.kernel == kp && k.dev == dev && k.threads == threads && k.smem == smem) blocks = k.blocks;
+        }
+    }
+    if (blocks < 0) {
         int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
-        cached_blocks = sms * (per_sm > 0 ? per_sm : 1);
-        cached_dev = dev;
+        blocks = (sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
+        std::lock_guard<std::mutex> lock(g_grid_mu);
+        if (g_grid_used < 64) g_grid_cache[g_grid_used++] = {kp, dev, threads, smem, blocks};
     }
-    return n_items < cached_blocks ? n_items : cached_blocks;
+    return n_items < blocks ? n_items : blocks;
 }
 
 int sm_count() {
@@ -1535,10 +1795,14 @@ struct Tuning {
     int heavy_shift;       // heavy tiles: list-length bucket >= bucket(mean) + heavy_shift; 1: all tiles
     int pair_ctas_per_sm;  // resident CTAs of the pair kernel per SM
     bool hit_masks;        // RM_BLEND_HIT_MASKS
+    bool tma;              // RM_BLEND_STAGE_TMA
+    uint32_t* status;      // where a staging wait that gives up is reported
 };
 
 Tuning tuning_from_flags(int flags, int def_shift, int def_ctas) {
     Tuning t;
+    t.tma = (flags & RM_BLEND_STAGE_TMA) != 0;
+    t.status = nullptr;
     const int hs = (flags >> RM_BLEND_HEAVY_SHIFT) & 0xf;
     const int pc = (flags >> RM_BLEND_PAIR_CTAS_SHIFT) & 0xf;
     t.heavy_shift = hs ? hs : def_shift;
@@ -1569,8 +1833,8 @@ int launch_fwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, cons
     const int subs = sh.tile_px / PX;
     const int subs_pair = sh.tile_px / PX_PAIR;
     const HitMasks hm = {masks ? w.mask_words : nullptr, w.mask_cap, w.mask_header};
-    const Queue qd = {w.order, w.info, w.tickets + 0, G, subs, false, hm};
-    const Queue qp = {w.order, w.info, w.tickets + 1, G, subs_pair, true, hm};
+    const Queue qd = {w.order, w.info, w.tickets + 0, G, subs, false, hm, tn.status, rm_host::wait_limit()};
+    const Queue qp = {w.order, w.info, w.tickets + 1, G, subs_pair, true, hm, tn.status, rm_host::wait_limit()};
     auto pair_kernel = blend_fwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, V>;
     const int smem = (int)sizeof(FwdPairSmem<PX_PAIR, B_PAIR>);
     cudaFuncSetAttribute(pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1607,8 +1871,9 @@ int launch_bwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, cons
     const int subs_pair = sh.tile_px / PX_PAIR;
     const bool masks = tn.hit_masks && PX == 64 && w.mask_header;
     const HitMasks hm = {masks ? w.mask_words : nullptr, w.mask_cap, w.mask_header};
-    const Queue qd = {w.order, w.info, w.tickets + 2, G, subs, false, hm};
-    const Queue qp = {w.order, w.info, w.tickets + 3, G, subs_pair, true, HitMasks{nullptr, 0, nullptr}};
+    const Queue qd = {w.order, w.info, w.tickets + 2, G, subs, false, hm, tn.status, rm_host::wait_limit()};
+    const Queue qp = {w.order, w.info, w.tickets + 3, G, subs_pair, true, HitMasks{nullptr, 0, nullptr},
+                      tn.status, rm_host::wait_limit()};
     auto pair_kernel = blend_bwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, V>;
     const int smem = (int)sizeof(BwdPairSmem<PX_PAIR, B_PAIR>);
     cudaFuncSetAttribute(pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1627,6 +1892,15 @@ int launch_bwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, cons
                                                             (const float2*)jitter, views, (const float4*)img, dist,
                                                             nc, (const float4*)gimg, gdist, gverts, gcv, qp);
     if ((rc = rm_host::check_launch("rm_blend_bwd (pair)"))) return rc;
+    if (PX == 64 && tn.tma) {  // records staged by bulk copies, two batches in flight
+        auto tma_kernel = blend_bwd_dense_tma_kernel<B_DENSE, V>;
+        const int grid = persistent_grid(tma_kernel, 64, 0, G * subs);
+        tma_kernel<<<grid, 64, 0, s>>>(ids, (const int2*)ranges, w.recs, (const int4*)indices,
+                                       (const float2*)jitter, views, (const float4*)img, dist, nc,
+                                       (const float4*)gimg, gdist, gverts, gcv, qd);
+        if ((rc = rm_host::check_launch("rm_blend_bwd (dense, bulk-copy staging)"))) return rc;
+        return join_side(s, side);
+    }
     auto dense_kernel = blend_bwd_dense_kernel<PX, B_DENSE, V>;
     const int grid = persistent_grid(dense_kernel, PX, 0, G * subs);
     dense_kernel<<<grid, PX, 0, s>>>(ids, (const int2*)ranges, w.recs, (const int4*)indices, (const float2*)jitter,
@@ -1685,13 +1959,25 @@ int check_blend_args(const char* who, const int32_t* indices, const float* verti
     return RM_OK;
 }
 
+// The pass's status word: the caller's, else the workspace's own (cleared here).
+int pass_status(const char* who, BlendWs& w, uint32_t* status_dev, cudaStream_t s, uint32_t** out) {
+    if (status_dev) {
+        *out = status_dev;
+        return RM_OK;
+    }
+    cudaError_t e = cudaMemsetAsync(w.status, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "%s: %s", who, cudaGetErrorString(e));
+    *out = w.status;
+    return RM_OK;
+}
+
 template <class V>
 int blend_fwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
                   const float* vertices, const float* cell_values, int64_t n_tets, int64_t n_verts,
                   const int32_t* tiles_touched,
                   const float* ray_jitter, const rm_camera* cam0, const V& views, const Shape& sh, float* out_img,
                   float* out_distortion, int32_t* n_contrib, const void* records, void* workspace,
-                  size_t workspace_bytes, int flags, void* stream) {
+                  size_t workspace_bytes, int flags, uint32_t* status_dev, void* stream) {
     int rc = check_blend_args(who, indices, vertices, cell_values, records ? 0 : n_tets, ray_jitter, cam0, sh.G,
                               workspace, workspace_bytes, flags);
     if (rc) return rc;
@@ -1708,7 +1994,8 @@ int blend_fwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
         if (rc) return rc;
     }
     // measured on the 1.3M-tet workload: every tile through the pair kernel, 4 CTAs/SM
-    const Tuning tn = tuning_from_flags(flags, 1, 4);
+    Tuning tn = tuning_from_flags(flags, 1, 4);
+    if ((rc = pass_status(who, w, status_dev, s, &tn.status))) return rc;
     // tets per shared-memory batch of the pair kernel: 16, 32 (default) or 64
     const int key = strip_pixels(cam0, flags) * 1000 + batch_size(flags, 32);
 #define RM_FWD_CASE(PX, NT, BP)                                                                                  \
@@ -1735,7 +2022,7 @@ int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
                   const float* ray_jitter, const rm_camera* cam0, const V& views, const Shape& sh,
                   const float* out_img, const float* out_distortion, const int32_t* n_contrib, const float* grad_img,
                   const float* grad_distortion, float* grad_vertices, float* grad_cell_values, const void* records,
-                  void* workspace, size_t workspace_bytes, int flags, void* stream) {
+                  void* workspace, size_t workspace_bytes, int flags, uint32_t* status_dev, void* stream) {
     int rc = check_blend_args(who, indices, vertices, cell_values, records ? 0 : n_tets, ray_jitter, cam0, sh.G,
                               workspace, workspace_bytes, flags);
     if (rc) return rc;
@@ -1754,7 +2041,8 @@ int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
         if (rc) return rc;
     }
     // measured: the one-thread-per-pixel backward alone is fastest
-    const Tuning tn = tuning_from_flags(flags, 15, 1);
+    Tuning tn = tuning_from_flags(flags, 15, 1);
+    if ((rc = pass_status(who, w, status_dev, s, &tn.status))) return rc;
     // tets per shared-memory batch of the dense kernel: 16, 32 or 64 (default)
     const int key = strip_pixels(cam0, flags) * 1000 + batch_size(flags, 64);
 #define RM_BWD_CASE(PX, NT, BD)                                                                                  \
@@ -1781,6 +2069,10 @@ int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
 extern "C" {
 
 size_t rm_blend_workspace_size(int64_t n_tets, int64_t n_tiles) { return rm::blend_ws_bytes(n_tets, n_tiles); }
+
+size_t rm_blend_status_offset(int64_t n_tets, int64_t n_tiles) {
+    return rm::blend_ws_bytes(n_tets, n_tiles) - 256 + rm::kBlendStatusOff;
+}
 
 size_t rm_blend_hit_mask_bytes(int64_t n_pairs, int64_t n_tiles, int tile_pixels) {
     const int64_t subs = tile_pixels > 64 ? tile_pixels / 64 : 1;
@@ -1843,21 +2135,23 @@ int rm_blend_pack_records(const int32_t* indices, const float* vertices, const f
 int rm_blend_fwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices, const float* vertices,
                  const float* cell_values, int64_t n_tets, int64_t n_verts, const int32_t* tiles_touched,
                  const float* ray_jitter, const rm_camera* cam, float* out_img, float* out_distortion,
-                 int32_t* n_contrib, void* workspace, size_t workspace_bytes, int flags, void* stream) {
+                 int32_t* n_contrib, void* workspace, size_t workspace_bytes, int flags, uint32_t* status_dev,
+                 void* stream) {
     int rc = rm_host::check_cam(cam);
     if (rc) return rc;
     const rm::OneView one = {*cam};
     const rm::Shape sh = {cam->grid_width * cam->grid_height, cam->tile_width * cam->tile_height};
     return rm::blend_fwd_any("rm_blend_fwd", sorted_ids, ranges, indices, vertices, cell_values, n_tets, n_verts,
                              tiles_touched, ray_jitter, cam, one, sh, out_img, out_distortion, n_contrib, nullptr,
-                             workspace, workspace_bytes, flags, stream);
+                             workspace, workspace_bytes, flags, status_dev, stream);
 }
 
 int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices, const float* vertices,
                  const float* cell_values, int64_t n_tets, int64_t n_verts, const int32_t* tiles_touched,
                  const float* ray_jitter, const rm_camera* cam, const float* out_img, const float* out_distortion,
                  const int32_t* n_contrib, const float* grad_img, const float* grad_distortion, float* grad_vertices,
-                 float* grad_cell_values, void* workspace, size_t workspace_bytes, int flags, void* stream) {
+                 float* grad_cell_values, void* workspace, size_t workspace_bytes, int flags, uint32_t* status_dev,
+                 void* stream) {
     int rc = rm_host::check_cam(cam);
     if (rc) return rc;
     const rm::OneView one = {*cam};
@@ -1865,21 +2159,21 @@ int rm_blend_bwd(const int32_t* sorted_ids, const int32_t* ranges, const int32_t
     return rm::blend_bwd_any("rm_blend_bwd", sorted_ids, ranges, indices, vertices, cell_values, n_tets, n_verts,
                              tiles_touched, ray_jitter, cam, one, sh, out_img, out_distortion, n_contrib, grad_img,
                              grad_distortion, grad_vertices, grad_cell_values, nullptr, workspace, workspace_bytes,
-                             flags, stream);
+                             flags, status_dev, stream);
 }
 
 int rm_blend_fwd_multi(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
                        const float* vertices, const float* cell_values, int64_t n_tets, int64_t n_verts,
                        const int32_t* tiles_touched, const float* ray_jitter, const rm_camera* cams, int n_views,
                        float* out_img, float* out_distortion, int32_t* n_contrib, const void* records,
-                       void* workspace, size_t workspace_bytes, int flags, void* stream) {
+                       void* workspace, size_t workspace_bytes, int flags, uint32_t* status_dev, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_blend_fwd_multi", cams, n_views, &views);
     if (rc) return rc;
     const rm::Shape sh = {views.tiles[n_views], cams[0].tile_width * cams[0].tile_height};
     return rm::blend_fwd_any("rm_blend_fwd_multi", sorted_ids, ranges, indices, vertices, cell_values, n_tets, n_verts,
                              tiles_touched, ray_jitter, cams, views, sh, out_img, out_distortion, n_contrib,
-                             records, workspace, workspace_bytes, flags, stream);
+                             records, workspace, workspace_bytes, flags, status_dev, stream);
 }
 
 int rm_blend_bwd_multi(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices,
@@ -1888,7 +2182,7 @@ int rm_blend_bwd_multi(const int32_t* sorted_ids, const int32_t* ranges, const i
                        const float* out_img, const float* out_distortion, const int32_t* n_contrib,
                        const float* grad_img, const float* grad_distortion, float* grad_vertices,
                        float* grad_cell_values, const void* records, void* workspace, size_t workspace_bytes,
-                       int flags, void* stream) {
+                       int flags, uint32_t* status_dev, void* stream) {
     rm::ViewSet views;
     int rc = rm_host::make_views("rm_blend_bwd_multi", cams, n_views, &views);
     if (rc) return rc;
@@ -1896,7 +2190,7 @@ int rm_blend_bwd_multi(const int32_t* sorted_ids, const int32_t* ranges, const i
     return rm::blend_bwd_any("rm_blend_bwd_multi", sorted_ids, ranges, indices, vertices, cell_values, n_tets, n_verts,
                              tiles_touched, ray_jitter, cams, views, sh, out_img, out_distortion, n_contrib,
                              grad_img, grad_distortion, grad_vertices, grad_cell_values, records, workspace,
-                             workspace_bytes, flags, stream);
+                             workspace_bytes, flags, status_dev, stream);
 }
 
 }  // extern "C"

@@ -265,6 +265,61 @@ __device__ __forceinline__ bool tet_indices_ok(int4 id, int64_t n_verts) {
            (int64_t)id.y < n_verts && (int64_t)id.z < n_verts && (int64_t)id.w < n_verts;
 }
 
+// ------------------------------------------------ bulk copies into shared --
+// One-dimensional bulk copies (cp.async.bulk, the TMA unit's untiled mode)
+// from this GPU's global memory into the issuing CTA's shared memory,
+// completing on an mbarrier that counts the bytes.  No cluster multicast.
+// Source and destination must be 16-byte aligned and the size a multiple of
+// 16 bytes (the per-tet records are 128 B).
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Makes mbarrier initialisation visible to the async proxy (the copy unit).
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Orders this thread's earlier shared-memory accesses (after a barrier: the
+// CTA's) before async-proxy writes that it issues next (write-after-read on
+// a staging buffer).
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Arrive on the barrier (count 1) and expect `bytes` more transaction bytes.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the barrier's phase with the given parity to complete, at most
+// `limit` polls (each try_wait itself suspends for a short, hardware-chosen
+// time).  Returns false when the limit is reached; the caller then reports
+// the timeout and must not read the staged data.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 // Bounded spin helper: returns false once the budget is exhausted.
 __device__ __forceinline__ bool spin_budget(uint32_t& left) {
     if (left == 0) return false;

@@ -38,13 +38,15 @@ class AlphaBlendTiledRender(torch.autograd.Function):
         if fine is not None:
             sorted_tetra_idx, tile_ranges, camst = fine.sorted_ids, fine.ranges, fine.cam
         # hit masks let the backward skip the forward's misses
+        status = frame.status if frame is not None else None
         output_img, distortion_img, n_contributors, records = R.blend_fwd(
             sorted_tetra_idx, tile_ranges, indices, vertices, tet_density, ray_jitter, camst,
-            tiles_touched=tiles_touched, hit_masks=True)
+            tiles_touched=tiles_touched, hit_masks=True, status=status)
         tet_alive = torch.zeros((indices.shape[0]), dtype=torch.bool, device=vertices.device)
         ctx.save_for_backward(sorted_tetra_idx, tile_ranges, indices, vertices, tet_density, output_img,
                               distortion_img, n_contributors, ray_jitter)
         ctx.records = records
+        ctx.status = status
         ctx.camst = camst
         ctx.render_grid = render_grid
         ctx.mark_non_differentiable(tet_alive)
@@ -57,5 +59,5 @@ class AlphaBlendTiledRender(torch.autograd.Function):
         vertices_grad, tet_density_grad = R.blend_bwd(
             sorted_tetra_idx, tile_ranges, indices, vertices, tet_density, ray_jitter, ctx.camst, output_img,
             distortion_img, n_contributors, grad_output_img, grad_distortion_img, ctx.records, reuse_records=True,
-            hit_masks=True)
+            hit_masks=True, status=ctx.status)
         return (None, None, None, vertices_grad, tet_density_grad, None, None, None, None)

@@ -487,6 +487,17 @@ def fine_lists_of(sorted_ids: torch.Tensor, cam: RMCamera, ray_jitter: torch.Ten
 
 
 _BLEND_FLAGS = {"fwd": 0, "bwd": 0}
+_STAGE = {"tma": False}
+
+
+def use_tma_staging(enabled: bool) -> None:
+    """Stage the backward's records with bulk copies (RM_BLEND_STAGE_TMA)
+    instead of per-thread loads.  Single-GPU processes only by policy."""
+    _STAGE["tma"] = bool(enabled)
+
+
+def tma_staging() -> bool:
+    return _STAGE["tma"]
 
 
 def set_blend_tuning(fwd_flags: int = 0, bwd_flags: int = 0) -> None:
@@ -502,11 +513,12 @@ def blend_tuning() -> tuple[int, int]:
 
 def blend_fwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, cam: RMCamera,
               tiles_touched=None, records: torch.Tensor | None = None, reuse_records: bool = False,
-              hit_masks: bool = False):
+              hit_masks: bool = False, status: torch.Tensor | None = None):
     """Forward blend.  Returns (img, dist, n_contrib, workspace); pass the
     workspace to blend_bwd.  hit_masks: also store which pixels hit each list
     entry (RM_BLEND_HIT_MASKS) so that a blend_bwd with hit_masks=True skips
-    the misses."""
+    the misses.  status: a device status word (frame_status) for the pass's
+    RM_STATUS_* bits (None: the workspace's own word)."""
     _require_cuda(sorted_ids=sorted_ids, ranges=ranges, indices=indices, vertices=vertices,
                   cell_values=cell_values, ray_jitter=ray_jitter)
     indices = _i32(indices)
@@ -530,13 +542,15 @@ def blend_fwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, ca
              _BLEND_FLAGS["fwd"])
     _call("rm_blend_fwd", lambda: L.rm_blend_fwd(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(indices), C.ptr(vertices), C.ptr(cell_values),
                            T, vertices.shape[0], C.ptr(tiles_touched), C.ptr(ray_jitter), ctypes.byref(cam),
-                           C.ptr(img), C.ptr(dist), C.ptr(nc), C.ptr(records), records.numel(), flags, _stream()))
+                           C.ptr(img), C.ptr(dist), C.ptr(nc), C.ptr(records), records.numel(), flags, C.ptr(status),
+                           _stream()))
     return img, dist, nc, records
 
 
 def blend_bwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, cam: RMCamera, img, dist, nc,
               grad_img, grad_dist, records, tiles_touched=None, reuse_records=True,
-              grad_vertices=None, grad_cell_values=None, hit_masks: bool = False):
+              grad_vertices=None, grad_cell_values=None, hit_masks: bool = False,
+              status: torch.Tensor | None = None):
     indices = _i32(indices)
     vertices = _f32(vertices)
     cell_values = _f32(cell_values)
@@ -552,11 +566,13 @@ def blend_bwd(sorted_ids, ranges, indices, vertices, cell_values, ray_jitter, ca
     T = indices.shape[0]
     flags = ((C.RM_BLEND_REUSE_RECORDS if reuse_records else 0) | (C.RM_BLEND_HIT_MASKS if hit_masks else 0) |
              _BLEND_FLAGS["bwd"])
+    if hit_masks and _STAGE["tma"]:
+        flags |= C.RM_BLEND_STAGE_TMA
     _call("rm_blend_bwd", lambda: C.lib().rm_blend_bwd(C.ptr(sorted_ids), C.ptr(ranges), C.ptr(indices), C.ptr(vertices),
                                  C.ptr(cell_values), T, vertices.shape[0], C.ptr(tiles_touched), C.ptr(ray_jitter),
                                  ctypes.byref(cam), C.ptr(img), C.ptr(dist), C.ptr(nc), C.ptr(grad_img), C.ptr(gd),
                                  C.ptr(grad_vertices), C.ptr(grad_cell_values), C.ptr(records), records.numel(),
-                                 flags, _stream()))
+                                 flags, C.ptr(status), _stream()))
     return grad_vertices, grad_cell_values
 
 

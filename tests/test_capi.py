@@ -44,6 +44,14 @@ def test_size_queries():
     assert L.rm_sort_workspace_size(1_000_000) > 12 * 1_000_000
 
 
+def test_blend_status_offset_inside_workspace():
+    L = C.lib()
+    for T, G in ((0, 1), (1000, 300), (1_300_000, 4346)):
+        n = L.rm_blend_workspace_size(T, G)
+        off = L.rm_blend_status_offset(T, G)
+        assert off % 4 == 0 and off + 4 <= n and off >= n - 256
+
+
 def test_wait_limit_setting():
     """The bounded-wait limit is a process-wide setting; 0 restores the
     default (no device work involved)."""
@@ -110,7 +118,7 @@ def test_rejects_null_and_misaligned():
     cam.grid_width = 26
     cam.grid_height = 26
     rc = L.rm_blend_fwd(None, 16, 16, 16, 16, 10, 10, None, 16, ctypes.byref(cam), 16, 16, 16, 256, 1 << 20, 0,
-                        None)
+                        None, None)
     assert rc == C.RM_EINVAL and "tile" in C.last_error()
 
 

@@ -224,4 +224,6 @@ def test_blend_without_frame_state_is_identical(cuda):
     (a, ga, ca), (b, gb, cb) = outs
     assert (a[..., 3] == b[..., 3]).all()  # log T: bit for bit over 8x8 or caller's lists
     assert (a - b).abs().max() <= 1e-6
-    assert torch.allclose(ga, gb, rtol=1e-4, atol=1e-6) and torch.allclose(ca, cb, rtol=1e-4, atol=1e-6)
+    # gradients are sums of float atomics in another order: relative L2 error
+    for x, y in ((ga, gb), (ca, cb)):
+        assert float((x - y).norm() / y.norm()) <= 1e-5
