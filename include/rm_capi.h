@@ -563,6 +563,40 @@ RM_API int rm_activate_features_bwd(const int32_t* indices, const float* vertice
                                     float* grad_sh_rest, float* grad_vertices,
                                     float* grad_circumcenters, void* stream);
 
+/* ------------------------------------------------------ Delaunay update -- */
+/*
+ * The steps of a Delaunay update after the tetrahedralisation itself
+ * (update_triangulation, models/ingp_color.py:523-558; the tetrahedralisation,
+ * gDel3D or scipy's Delaunay, is not part of this library).  Each output keeps
+ * the input order.  Workspace: rm_tets_workspace_size(n_tets) bytes, 256-byte
+ * aligned.
+ *
+ * rm_tets_orient: the rows of indices_in [n_tets,4] whose indices all lie in
+ * [0, n_verts) (rows naming gDel3D's point at infinity are dropped, :533), with
+ * vertices 0 and 1 swapped where the signed volume det(v1 - v0, v2 - v0,
+ * v3 - v0) / 6 is negative (:538-542; evaluated in double, so the sign can
+ * differ from the reference's float32 determinant only for tets whose volume
+ * is at float32 rounding level).  indices_out has room for n_tets rows;
+ * *n_out_dev receives the kept count.
+ *
+ * rm_tets_cull: tets with density > density_threshold or alpha >
+ * alpha_threshold, alpha = 1 - exp(-density * shortest edge length)
+ * (:548-554, calc_tet_alpha(mode="min"), models/base_model.py:82-105), go to
+ * kept_out, the others to empty_out (may be NULL); *n_kept_dev receives the
+ * kept count.  A row with an index outside [0, n_verts) is counted as empty,
+ * never dereferenced, and sets RM_STATUS_BAD_INDEX in *status_dev.
+ */
+RM_API size_t rm_tets_workspace_size(int64_t n_tets);
+RM_API int rm_tets_orient(const int32_t* indices_in, int64_t n_tets, const float* vertices,
+                          int64_t n_verts, int32_t* indices_out, int64_t* n_out_dev,
+                          void* workspace, size_t workspace_bytes, uint32_t* status_dev,
+                          void* stream);
+RM_API int rm_tets_cull(const int32_t* indices, int64_t n_tets, const float* vertices,
+                        int64_t n_verts, const float* density, float density_threshold,
+                        float alpha_threshold, int32_t* kept_out, int32_t* empty_out,
+                        int64_t* n_kept_dev, void* workspace, size_t workspace_bytes,
+                        uint32_t* status_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -102,6 +102,10 @@ SIGNATURES = {
                                             vp, vp]),
     "rm_activate_features_bwd": (ctypes.c_int, [vp, vp, i64, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, vp,
                                                 i64, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "rm_tets_workspace_size": (sz, [i64]),
+    "rm_tets_orient": (ctypes.c_int, [vp, i64, vp, i64, vp, vp, vp, sz, vp, vp]),
+    "rm_tets_cull": (ctypes.c_int, [vp, i64, vp, i64, vp, ctypes.c_float, ctypes.c_float, vp, vp, vp, vp, sz, vp,
+                                    vp]),
     "rm_blend_records_size": (sz, [i64]),
     "rm_blend_pack_records": (ctypes.c_int, [vp, vp, vp, i64, i64, vp, vp, vp]),
     "rm_blend_fwd_multi": (ctypes.c_int, [vp, vp, vp, vp, vp, i64, i64, vp, vp, camp, ctypes.c_int, vp, vp, vp,

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIBNAME = "librm_b200.so"
-SOURCES = ["rm_capi.cu", "rm_project.cu", "rm_scan.cu", "rm_sort.cu", "rm_blend.cu", "rm_fine.cu", "rm_features.cu"]
+SOURCES = ["rm_capi.cu", "rm_project.cu", "rm_scan.cu", "rm_sort.cu", "rm_blend.cu", "rm_fine.cu", "rm_features.cu", "rm_tets.cu"]
 HEADERS = ["rm_internal.cuh", os.path.join("..", "..", "include", "rm_capi.h")]
 
 # --fmad=false: every fused multiply-add in the kernels is written explicitly

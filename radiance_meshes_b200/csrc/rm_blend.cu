@@ -142,6 +142,60 @@ __device__ __forceinline__ Isect intersect(const float4* __restrict__ q, f3 o, f
     return r;
 }
 
+// Backward-only geometry.  Rays start at o = cam_pos + min_t * d, so for a
+// plane with normal n through the reference vertex v: n . (v - o) =
+// c - min_t * (n . d) with c = n . (v - cam_pos), which is the same for every
+// pixel of a view.  The backward stages, per list entry, c for the four
+// planes and u0 = v0 - cam_pos, u1 = v1 - cam_pos (entry_ext), and computes
+// the t values with the approximate quotient.  The backward revisits only the
+// forward's hits (hit masks), and its t values feed gradient factors only,
+// whose tolerance is far above the few ulps this changes; the forward keeps
+// the exact, correctly rounded arithmetic of the reference.
+constexpr int kExtFloat4 = 3;  // (c0, c1, c2, c3), (u0, -), (u1, -)
+
+__device__ __forceinline__ void entry_ext(const float4* __restrict__ q, f3 cam_pos, float4* __restrict__ ext) {
+    const f3 u0 = xyz(q[4]) - cam_pos, u1 = xyz(q[5]) - cam_pos;
+    ext[0] = make_float4(dot3(xyz(q[0]), u0), dot3(xyz(q[1]), u0), dot3(xyz(q[2]), u0), dot3(xyz(q[3]), u1));
+    ext[1] = make_float4(u0.x, u0.y, u0.z, 0.f);
+    ext[2] = make_float4(u1.x, u1.y, u1.z, 0.f);
+}
+
+__device__ __forceinline__ Isect intersect_bwd(const float4* __restrict__ q, const float4* __restrict__ ext, f3 d,
+                                               float min_t) {
+    const float4 cq = ext[0];
+    const float c[4] = {cq.x, cq.y, cq.z, cq.w};
+    float te = -1e30f, tx = 1e30f, dene = 1.f, denx = 1.f;
+    int ie = -1, ix = -1;
+    bool miss = false;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float den = dot3(xyz(q[i]), d);
+        const float dist = fmaf(min_t, den, -c[i]);  // -n . (v_ref - o)
+        const bool par = fabsf(den) < 1e-10f;
+        miss |= par && dist > 0.f;
+        const float tp = __fdividef(-dist, den);
+        const bool ue = !par && den < 0.f && tp > te;
+        const bool ux = !par && !(den < 0.f) && tp < tx;
+        te = ue ? tp : te;
+        tx = ux ? tp : tx;
+        ie = ue ? i : ie;
+        dene = ue ? den : dene;
+        ix = ux ? i : ix;
+        denx = ux ? den : denx;
+    }
+    Isect r;
+    r.te = te;
+    r.tx = tx;
+    r.geo = !miss && !(te > tx) && !(tx <= 0.f);
+    r.enter = fmaxf(te, 0.f);
+    r.exit = fmaxf(tx, r.enter);
+    r.dene = dene;
+    r.denx = denx;
+    r.ie = ie;
+    r.ix = ix;
+    return r;
+}
+
 // Weights of the closed-form segment integral (interp_version.slang:21-40)
 // for optical depth x = density * dt >= 0:
 //   alpha = exp(-x), phi = (1 - exp(-x)) / x, w0 = phi - alpha, w1 = 1 - phi.
@@ -189,13 +243,11 @@ struct Segment {
 
 // integrate_tetra_segment + compute_integral (interp_version.slang:30-69):
 // rgb = w0 * c_exit + w1 * c_enter with c = base + dot(grd, p - v0).
-__device__ __forceinline__ void integrate(const float4* __restrict__ q, f3 o, f3 d, float enter, float exit,
-                                          Segment& s) {
+// The colours at the entry and exit points, given those points relative to
+// v0 (s.ve, s.vx).
+__device__ __forceinline__ void integrate_rel(const float4* __restrict__ q, Segment& s) {
     const float density = q[0].w;
-    const f3 v0 = xyz(q[4]);
     const f3 grd = {q[4].w, q[5].w, q[6].w};
-    s.ve = {fmaf(enter, d.x, o.x) - v0.x, fmaf(enter, d.y, o.y) - v0.y, fmaf(enter, d.z, o.z) - v0.z};
-    s.vx = {fmaf(exit, d.x, o.x) - v0.x, fmaf(exit, d.y, o.y) - v0.y, fmaf(exit, d.z, o.z) - v0.z};
     s.ce = dot3(grd, s.ve);
     s.cx = dot3(grd, s.vx);
     s.x = s.dt * density;
@@ -203,6 +255,24 @@ __device__ __forceinline__ void integrate(const float4* __restrict__ q, f3 o, f3
     const float base[3] = {q[1].w, q[2].w, q[3].w};
 #pragma unroll
     for (int k = 0; k < 3; ++k) s.rgb[k] = fmaf(s.w.w1, s.ce + base[k], s.w.w0 * (s.cx + base[k]));
+}
+
+__device__ __forceinline__ void integrate(const float4* __restrict__ q, f3 o, f3 d, float enter, float exit,
+                                          Segment& s) {
+    const f3 v0 = xyz(q[4]);
+    s.ve = {fmaf(enter, d.x, o.x) - v0.x, fmaf(enter, d.y, o.y) - v0.y, fmaf(enter, d.z, o.z) - v0.z};
+    s.vx = {fmaf(exit, d.x, o.x) - v0.x, fmaf(exit, d.y, o.y) - v0.y, fmaf(exit, d.z, o.z) - v0.z};
+    integrate_rel(q, s);
+}
+
+// Backward: p - v0 = (min_t + t) d - u0 (entry_ext).
+__device__ __forceinline__ void integrate_bwd(const float4* __restrict__ q, const float4* __restrict__ ext, f3 d,
+                                              float min_t, float enter, float exit, Segment& s) {
+    const float4 u = ext[1];
+    const float te = min_t + enter, tx = min_t + exit;
+    s.ve = {fmaf(te, d.x, -u.x), fmaf(te, d.y, -u.y), fmaf(te, d.z, -u.z)};
+    s.vx = {fmaf(tx, d.x, -u.x), fmaf(tx, d.y, -u.y), fmaf(tx, d.z, -u.z)};
+    integrate_rel(q, s);
 }
 
 // Pixel (lx, ly) inside the tile of thread t of work item `sub`, for items of
@@ -715,10 +785,11 @@ struct ReduceScatter<M, 0> {
 // dS_D).  Outputs the 25 per-entry partials gl[] (face normals 0..11, direct
 // v0 12..14, v1 15..17, density 18, rgb 19..21, grd 22..24) and returns
 // dL/d(log T before the hit); nD2 / nD3 receive dL/d(D2, D3 before the hit).
-__device__ __forceinline__ float hit_grads(const float4* __restrict__ q, f3 o, f3 d, const Isect& is,
-                                           const Segment& s, float T, float D2_old, float D3_old,
-                                           const float* dS_c, float dS_logT, const float* dS_D, float* gl,
-                                           float& nD2, float& nD3) {
+// a0, a1: v0 - o and v1 - o (the reference vertices of the planes).
+__device__ __forceinline__ float hit_grads_a(const float4* __restrict__ q, f3 a0, f3 a1, f3 d, const Isect& is,
+                                             const Segment& s, float T, float D2_old, float D3_old,
+                                             const float* dS_c, float dS_logT, const float* dS_D, float* gl,
+                                             float& nD2, float& nD3) {
     const float density = q[0].w;
     const float enter = is.enter, exit = is.exit;
     const float m1 = density * (exit + enter) / 2.0f;
@@ -775,8 +846,6 @@ __device__ __forceinline__ float hit_grads(const float4* __restrict__ q, f3 o, f
     if (is.tx > enter) d_tx = d_exit; else d_enter += d_exit;
     const float d_te = is.te > 0.f ? d_enter : 0.f;
     // plane intersections t = dot(n, vref - o) / dot(n, d)
-    const f3 a0 = xyz(q[4]) - o;
-    const f3 a1 = xyz(q[5]) - o;
     // gradient factors only (the hit and its t values are exact above): the
     // approximate quotient (2 ulp) is far inside the gradients' tolerance
     const float ge = __fdividef(d_te, is.dene), gx = __fdividef(d_tx, is.denx);
@@ -803,6 +872,14 @@ __device__ __forceinline__ float hit_grads(const float4* __restrict__ q, f3 o, f
     }
     // safe_exp's clip at log(1e20) never binds: log T <= 0
     return dS_logT + dT * T;
+}
+
+__device__ __forceinline__ float hit_grads(const float4* __restrict__ q, f3 o, f3 d, const Isect& is,
+                                           const Segment& s, float T, float D2_old, float D3_old,
+                                           const float* dS_c, float dS_logT, const float* dS_D, float* gl,
+                                           float& nD2, float& nD3) {
+    return hit_grads_a(q, xyz(q[4]) - o, xyz(q[5]) - o, d, is, s, T, D2_old, D3_old, dS_c, dS_logT, dS_D, gl, nD2,
+                       nD3);
 }
 
 // Converts the per-entry sums of the 25 partials into vertex and cell-value
@@ -857,6 +934,7 @@ __device__ __forceinline__ void flush_entries(int n, const float4 (*srec)[kRecFl
 template <int NT, int B>
 struct BwdDenseSmem {
     float4 srec[B][kRecFloat4];
+    float4 sext[B][kExtFloat4];  // entry_ext of the staged entries (this CTA's view)
     int32_t sid[B];
     float sacc[B][kNGrad];
     int32_t smax[WarpShape<NT>::kWarps];
@@ -881,6 +959,7 @@ __device__ __forceinline__ void bwd_dense_item(
     const bool inside = px < cam.image_width && py < cam.image_height;
     const int64_t pix = (int64_t)py * cam.image_width + px;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const f3 cam_pos = {cam.cam_pos[0], cam.cam_pos[1], cam.cam_pos[2]};
     f3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
     float logT = 0.f, D2 = 0.f, D3 = 0.f;  // state along the reverse walk
     float dS_c[3] = {0.f, 0.f, 0.f}, dS_logT = 0.f, dS_D[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
@@ -967,6 +1046,8 @@ __device__ __forceinline__ void bwd_dense_item(
             S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
         }
         __syncthreads();
+        for (int k = threadIdx.x; k < nk; k += NT) entry_ext(S.srec[k], cam_pos, S.sext[k]);
+        __syncthreads();
         for (int jj = nk - 1; jj >= 0; --jj) {
             const int off = lo + S.cidx[jj] - rg.x;
             // with the forward's masks, only its hits are revisited
@@ -974,17 +1055,18 @@ __device__ __forceinline__ void bwd_dense_item(
             const bool act = inside && off < nc && ((hw >> (off & 31)) & 1u);
             if (!__any_sync(kMask, act)) continue;
             const float4* q = S.srec[jj];
+            const float4* ext = S.sext[jj];
             float gl[kNGrad];
 #pragma unroll
             for (int k = 0; k < kNGrad; ++k) gl[k] = 0.f;
-            const Isect is = intersect<true>(q, o, d);
+            const Isect is = intersect_bwd(q, ext, d, cam.min_t);
             const float density = q[0].w;
             Segment s;
             s.dt = fmaxf(is.exit - is.enter, 0.f);
             s.a = density * s.dt;
             const bool hit = act && is.geo && s.a > 0.f;
             if (hit) {
-                integrate(q, o, d, is.enter, is.exit, s);
+                integrate_bwd(q, ext, d, cam.min_t, is.enter, is.exit, s);
                 // undo_alpha_out (alphablend_shader_interp.slang:128-192): only log T, D2
                 // and D3 of the earlier state enter the adjoint
                 const float m1 = density * (is.exit + is.enter) / 2.0f;
@@ -994,7 +1076,10 @@ __device__ __forceinline__ void bwd_dense_item(
                 D3 = D3 - m1;
                 logT = logT_old;
                 float nD2, nD3;
-                dS_logT = hit_grads(q, o, d, is, s, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
+                const float4 u0 = ext[1], u1 = ext[2];
+                const f3 a0 = {fmaf(-cam.min_t, d.x, u0.x), fmaf(-cam.min_t, d.y, u0.y), fmaf(-cam.min_t, d.z, u0.z)};
+                const f3 a1 = {fmaf(-cam.min_t, d.x, u1.x), fmaf(-cam.min_t, d.y, u1.y), fmaf(-cam.min_t, d.z, u1.z)};
+                dS_logT = hit_grads_a(q, a0, a1, d, is, s, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
                 dS_D[2] = nD2;
                 dS_D[3] = nD3;
             }
@@ -1023,6 +1108,7 @@ __device__ __forceinline__ void bwd_dense_item(
 template <int B>
 struct BwdTmaSmem {
     float4 srec[2][B][kRecFloat4];
+    float4 sext[B][kExtFloat4];  // entry_ext of the batch being walked
     float sacc[B][kNGrad];
     int32_t sid[2][B];
     uint8_t cidx[2][B];
@@ -1113,6 +1199,7 @@ __device__ __forceinline__ void bwd_dense_item_tma(
     const bool inside = px < cam.image_width && py < cam.image_height;
     const int64_t pix = (int64_t)py * cam.image_width + px;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const f3 cam_pos = {cam.cam_pos[0], cam.cam_pos[1], cam.cam_pos[2]};
     f3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
     float logT = 0.f, D2 = 0.f, D3 = 0.f;
     float dS_c[3] = {0.f, 0.f, 0.f}, dS_logT = 0.f, dS_D[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
@@ -1157,12 +1244,13 @@ __device__ __forceinline__ void bwd_dense_item_tma(
         }
         const int nk = S.n_keep[cb];
         for (int k = threadIdx.x; k < nk * kNGrad; k += NT) (&S.sacc[0][0])[k] = 0.f;
-        __syncthreads();
         if (!mbar_wait(&S.bar[cb], (pipe.parity >> cb) & 1u, q.spin_limit)) {
             if (threadIdx.x == 0 && q.status) atomicOr(q.status, RM_STATUS_QUEUE_TIMEOUT);
             mbar_wait(&S.bar[cb], (pipe.parity >> cb) & 1u, q.spin_limit);  // let the copies land before reuse
         }
         pipe.parity ^= 1u << cb;
+        for (int k = threadIdx.x; k < nk; k += NT) entry_ext(S.srec[cb][k], cam_pos, S.sext[k]);
+        __syncthreads();
         const int kb0 = (clo - rg.x) >> 5;
         for (int jj = nk - 1; jj >= 0; --jj) {
             const int off = clo + S.cidx[cb][jj] - rg.x;
@@ -1171,17 +1259,18 @@ __device__ __forceinline__ void bwd_dense_item_tma(
             const bool act = inside && off < nc && ((hw >> (off & 31)) & 1u);
             if (!__any_sync(0xffffffffu, act)) continue;
             const float4* qr = S.srec[cb][jj];
+            const float4* ext = S.sext[jj];
             float gl[kNGrad];
 #pragma unroll
             for (int k = 0; k < kNGrad; ++k) gl[k] = 0.f;
-            const Isect is = intersect<true>(qr, o, d);
+            const Isect is = intersect_bwd(qr, ext, d, cam.min_t);
             const float density = qr[0].w;
             Segment sg;
             sg.dt = fmaxf(is.exit - is.enter, 0.f);
             sg.a = density * sg.dt;
             const bool hit = act && is.geo && sg.a > 0.f;
             if (hit) {
-                integrate(qr, o, d, is.enter, is.exit, sg);
+                integrate_bwd(qr, ext, d, cam.min_t, is.enter, is.exit, sg);
                 const float m1 = density * (is.exit + is.enter) / 2.0f;
                 const float logT_old = logT + sg.a;
                 const float T = __expf(logT_old);
@@ -1189,7 +1278,10 @@ __device__ __forceinline__ void bwd_dense_item_tma(
                 D3 = D3 - m1;
                 logT = logT_old;
                 float nD2, nD3;
-                dS_logT = hit_grads(qr, o, d, is, sg, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
+                const float4 u0 = ext[1], u1 = ext[2];
+                const f3 a0 = {fmaf(-cam.min_t, d.x, u0.x), fmaf(-cam.min_t, d.y, u0.y), fmaf(-cam.min_t, d.z, u0.z)};
+                const f3 a1 = {fmaf(-cam.min_t, d.x, u1.x), fmaf(-cam.min_t, d.y, u1.y), fmaf(-cam.min_t, d.z, u1.z)};
+                dS_logT = hit_grads_a(qr, a0, a1, d, is, sg, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
                 dS_D[2] = nD2;
                 dS_D[3] = nD3;
             }

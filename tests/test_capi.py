@@ -44,6 +44,18 @@ def test_size_queries():
     assert L.rm_sort_workspace_size(1_000_000) > 12 * 1_000_000
 
 
+def test_tets_argument_checks():
+    L = C.lib()
+    assert L.rm_tets_workspace_size(1000) >= 8 * 1000
+    ws = 256
+    assert L.rm_tets_orient(None, 10, 16, 10, 16, 16, ws, 1 << 20, None, None) == C.RM_EINVAL
+    assert L.rm_tets_orient(16, 10, 16, 10, 24, 16, ws, 1 << 20, None, None) == C.RM_EINVAL  # misaligned output
+    assert L.rm_tets_orient(16, 10, 16, 10, 16, 16, ws, 8, None, None) == C.RM_EINVAL  # workspace too small
+    assert "workspace" in C.last_error()
+    assert L.rm_tets_cull(16, 10, 16, 10, None, 0.5, 0.0, 16, None, 16, ws, 1 << 20, None, None) == C.RM_EINVAL
+    assert L.rm_tets_orient(16, -1, 16, 10, 16, 16, ws, 1 << 20, None, None) == C.RM_EINVAL
+
+
 def test_blend_status_offset_inside_workspace():
     L = C.lib()
     for T, G in ((0, 1), (1000, 300), (1_300_000, 4346)):
