@@ -49,9 +49,6 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--bwd", choices=["dense", "hits"], default="dense",
-                    help="backward walk: one pixel per thread (dense) or one thread per hit of the forward's hit "
-                         "masks (hits)")
     ap.add_argument("--stage", choices=["ldg", "tma"], default="ldg",
                     help="how the backward stages tet records in shared memory: per-thread loads, or bulk copies "
                          "(cp.async.bulk, two batches in flight); bulk copies only in single-GPU runs")
@@ -243,8 +240,6 @@ def run_b200(args):
     camst = R.camera(tcam)
     grid = RenderGrid(H, W, tile_width=args.tile, tile_height=args.tile)
     R.use_tma_staging(args.stage == "tma" and world == 1)
-    if args.bwd == "hits":
-        R.set_blend_tuning(R.blend_tuning()[0], R.blend_tuning()[1] | _capi.RM_BLEND_BWD_HITS)
     rng = np.random.default_rng(1000 + rank)
     target_h = torch.from_numpy(rng.uniform(size=(H, W, 3)).astype(np.float32)).pin_memory()
     # The model's raw per-tet outputs (density, base colour, colour gradient),
@@ -477,8 +472,7 @@ def run_b200(args):
                    else "caller's tiles", "parallelism": f"dp{world} (views)" if world > 1
                    else "single view", "l2": "flushed between steps (256 MiB write)",
                    "seed": 2, "jitter": "torch.rand per step (train.py:244)",
-                   "record_staging": "bulk copies (cp.async.bulk)" if R.tma_staging() else "per-thread loads",
-                   "backward": "hit lists" if R.blend_tuning()[1] & _capi.RM_BLEND_BWD_HITS else "dense"},
+                   "record_staging": "bulk copies (cp.async.bulk)" if R.tma_staging() else "per-thread loads"},
         "value_jitter_0_5": {"value": value_const, "ms_per_step": total_ms_const / args.steps,
                              "jitter": "constant 0.5 (render() default)"},
         "e2e": e2e, "roofline": roof, "stages_ms": per_stage, "stages_pass_steps": n_break,

@@ -256,11 +256,7 @@ RM_API size_t rm_blend_status_offset(int64_t n_tets, int64_t n_tiles);
  * from this GPU's memory, completing on an mbarrier; no multicast), two
  * batches in flight, instead of per-thread loads.  Backward, 64-pixel items. */
 #define RM_BLEND_STAGE_TMA 0x4
-/* Backward over hit lists: with hit masks and 64-pixel items, the hits of each
- * batch are listed and every hit gets its own thread (segment, chain walk by
- * the pixel's owner, adjoint), the per-entry sums built with shared-memory
- * atomics; the same gradients up to the order of float additions. */
-#define RM_BLEND_BWD_HITS 0x8
+
 /* flags bits 8..15: log2 of the pixels per work item strip (16 or 64; 0 = 64) */
 #define RM_BLEND_STRIP_SHIFT 8
 #define RM_BLEND_STRIP(log2_pixels) ((log2_pixels) << RM_BLEND_STRIP_SHIFT)

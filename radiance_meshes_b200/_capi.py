@@ -40,7 +40,6 @@ STATUS_TEXT = {
 RM_BLEND_REUSE_RECORDS = 0x1
 RM_BLEND_HIT_MASKS = 0x2
 RM_BLEND_STAGE_TMA = 0x4
-RM_BLEND_BWD_HITS = 0x8
 RM_BLEND_STRIP_SHIFT = 8
 RM_BLEND_HEAVY_SHIFT = 16
 RM_BLEND_PAIR_CTAS_SHIFT = 20

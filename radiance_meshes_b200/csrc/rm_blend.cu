@@ -142,60 +142,6 @@ __device__ __forceinline__ Isect intersect(const float4* __restrict__ q, f3 o, f
     return r;
 }
 
-// Backward-only geometry.  Rays start at o = cam_pos + min_t * d, so for a
-// plane with normal n through the reference vertex v: n . (v - o) =
-// c - min_t * (n . d) with c = n . (v - cam_pos), which is the same for every
-// pixel of a view.  The backward stages, per list entry, c for the four
-// planes and u0 = v0 - cam_pos, u1 = v1 - cam_pos (entry_ext), and computes
-// the t values with the approximate quotient.  The backward revisits only the
-// forward's hits (hit masks), and its t values feed gradient factors only,
-// whose tolerance is far above the few ulps this changes; the forward keeps
-// the exact, correctly rounded arithmetic of the reference.
-constexpr int kExtFloat4 = 3;  // (c0, c1, c2, c3), (u0, -), (u1, -)
-
-__device__ __forceinline__ void entry_ext(const float4* __restrict__ q, f3 cam_pos, float4* __restrict__ ext) {
-    const f3 u0 = xyz(q[4]) - cam_pos, u1 = xyz(q[5]) - cam_pos;
-    ext[0] = make_float4(dot3(xyz(q[0]), u0), dot3(xyz(q[1]), u0), dot3(xyz(q[2]), u0), dot3(xyz(q[3]), u1));
-    ext[1] = make_float4(u0.x, u0.y, u0.z, 0.f);
-    ext[2] = make_float4(u1.x, u1.y, u1.z, 0.f);
-}
-
-__device__ __forceinline__ Isect intersect_bwd(const float4* __restrict__ q, const float4* __restrict__ ext, f3 d,
-                                               float min_t) {
-    const float4 cq = ext[0];
-    const float c[4] = {cq.x, cq.y, cq.z, cq.w};
-    float te = -1e30f, tx = 1e30f, dene = 1.f, denx = 1.f;
-    int ie = -1, ix = -1;
-    bool miss = false;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const float den = dot3(xyz(q[i]), d);
-        const float dist = fmaf(min_t, den, -c[i]);  // -n . (v_ref - o)
-        const bool par = fabsf(den) < 1e-10f;
-        miss |= par && dist > 0.f;
-        const float tp = __fdividef(-dist, den);
-        const bool ue = !par && den < 0.f && tp > te;
-        const bool ux = !par && !(den < 0.f) && tp < tx;
-        te = ue ? tp : te;
-        tx = ux ? tp : tx;
-        ie = ue ? i : ie;
-        dene = ue ? den : dene;
-        ix = ux ? i : ix;
-        denx = ux ? den : denx;
-    }
-    Isect r;
-    r.te = te;
-    r.tx = tx;
-    r.geo = !miss && !(te > tx) && !(tx <= 0.f);
-    r.enter = fmaxf(te, 0.f);
-    r.exit = fmaxf(tx, r.enter);
-    r.dene = dene;
-    r.denx = denx;
-    r.ie = ie;
-    r.ix = ix;
-    return r;
-}
-
 // Weights of the closed-form segment integral (interp_version.slang:21-40)
 // for optical depth x = density * dt >= 0:
 //   alpha = exp(-x), phi = (1 - exp(-x)) / x, w0 = phi - alpha, w1 = 1 - phi.
@@ -265,15 +211,6 @@ __device__ __forceinline__ void integrate(const float4* __restrict__ q, f3 o, f3
     integrate_rel(q, s);
 }
 
-// Backward: p - v0 = (min_t + t) d - u0 (entry_ext).
-__device__ __forceinline__ void integrate_bwd(const float4* __restrict__ q, const float4* __restrict__ ext, f3 d,
-                                              float min_t, float enter, float exit, Segment& s) {
-    const float4 u = ext[1];
-    const float te = min_t + enter, tx = min_t + exit;
-    s.ve = {fmaf(te, d.x, -u.x), fmaf(te, d.y, -u.y), fmaf(te, d.z, -u.z)};
-    s.vx = {fmaf(tx, d.x, -u.x), fmaf(tx, d.y, -u.y), fmaf(tx, d.z, -u.z)};
-    integrate_rel(q, s);
-}
 
 // Pixel (lx, ly) inside the tile of thread t of work item `sub`, for items of
 // NT pixels: square blocks of 8x8 (NT = 64) or 4x4 (NT = 16) pixels, row-major
@@ -934,7 +871,6 @@ __device__ __forceinline__ void flush_entries(int n, const float4 (*srec)[kRecFl
 template <int NT, int B>
 struct BwdDenseSmem {
     float4 srec[B][kRecFloat4];
-    float4 sext[B][kExtFloat4];  // entry_ext of the staged entries (this CTA's view)
     int32_t sid[B];
     float sacc[B][kNGrad];
     int32_t smax[WarpShape<NT>::kWarps];
@@ -959,7 +895,6 @@ __device__ __forceinline__ void bwd_dense_item(
     const bool inside = px < cam.image_width && py < cam.image_height;
     const int64_t pix = (int64_t)py * cam.image_width + px;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const f3 cam_pos = {cam.cam_pos[0], cam.cam_pos[1], cam.cam_pos[2]};
     f3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
     float logT = 0.f, D2 = 0.f, D3 = 0.f;  // state along the reverse walk
     float dS_c[3] = {0.f, 0.f, 0.f}, dS_logT = 0.f, dS_D[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
@@ -1046,8 +981,6 @@ __device__ __forceinline__ void bwd_dense_item(
             S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
         }
         __syncthreads();
-        for (int k = threadIdx.x; k < nk; k += NT) entry_ext(S.srec[k], cam_pos, S.sext[k]);
-        __syncthreads();
         for (int jj = nk - 1; jj >= 0; --jj) {
             const int off = lo + S.cidx[jj] - rg.x;
             // with the forward's masks, only its hits are revisited
@@ -1055,18 +988,17 @@ __device__ __forceinline__ void bwd_dense_item(
             const bool act = inside && off < nc && ((hw >> (off & 31)) & 1u);
             if (!__any_sync(kMask, act)) continue;
             const float4* q = S.srec[jj];
-            const float4* ext = S.sext[jj];
             float gl[kNGrad];
 #pragma unroll
             for (int k = 0; k < kNGrad; ++k) gl[k] = 0.f;
-            const Isect is = intersect_bwd(q, ext, d, cam.min_t);
+            const Isect is = intersect<true>(q, o, d);
             const float density = q[0].w;
             Segment s;
             s.dt = fmaxf(is.exit - is.enter, 0.f);
             s.a = density * s.dt;
             const bool hit = act && is.geo && s.a > 0.f;
             if (hit) {
-                integrate_bwd(q, ext, d, cam.min_t, is.enter, is.exit, s);
+                integrate(q, o, d, is.enter, is.exit, s);
                 // undo_alpha_out (alphablend_shader_interp.slang:128-192): only log T, D2
                 // and D3 of the earlier state enter the adjoint
                 const float m1 = density * (is.exit + is.enter) / 2.0f;
@@ -1076,10 +1008,7 @@ __device__ __forceinline__ void bwd_dense_item(
                 D3 = D3 - m1;
                 logT = logT_old;
                 float nD2, nD3;
-                const float4 u0 = ext[1], u1 = ext[2];
-                const f3 a0 = {fmaf(-cam.min_t, d.x, u0.x), fmaf(-cam.min_t, d.y, u0.y), fmaf(-cam.min_t, d.z, u0.z)};
-                const f3 a1 = {fmaf(-cam.min_t, d.x, u1.x), fmaf(-cam.min_t, d.y, u1.y), fmaf(-cam.min_t, d.z, u1.z)};
-                dS_logT = hit_grads_a(q, a0, a1, d, is, s, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
+                dS_logT = hit_grads(q, o, d, is, s, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
                 dS_D[2] = nD2;
                 dS_D[3] = nD3;
             }
@@ -1108,7 +1037,6 @@ __device__ __forceinline__ void bwd_dense_item(
 template <int B>
 struct BwdTmaSmem {
     float4 srec[2][B][kRecFloat4];
-    float4 sext[B][kExtFloat4];  // entry_ext of the batch being walked
     float sacc[B][kNGrad];
     int32_t sid[2][B];
     uint8_t cidx[2][B];
@@ -1199,7 +1127,6 @@ __device__ __forceinline__ void bwd_dense_item_tma(
     const bool inside = px < cam.image_width && py < cam.image_height;
     const int64_t pix = (int64_t)py * cam.image_width + px;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const f3 cam_pos = {cam.cam_pos[0], cam.cam_pos[1], cam.cam_pos[2]};
     f3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
     float logT = 0.f, D2 = 0.f, D3 = 0.f;
     float dS_c[3] = {0.f, 0.f, 0.f}, dS_logT = 0.f, dS_D[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
@@ -1249,7 +1176,6 @@ __device__ __forceinline__ void bwd_dense_item_tma(
             mbar_wait(&S.bar[cb], (pipe.parity >> cb) & 1u, q.spin_limit);  // let the copies land before reuse
         }
         pipe.parity ^= 1u << cb;
-        for (int k = threadIdx.x; k < nk; k += NT) entry_ext(S.srec[cb][k], cam_pos, S.sext[k]);
         __syncthreads();
         const int kb0 = (clo - rg.x) >> 5;
         for (int jj = nk - 1; jj >= 0; --jj) {
@@ -1259,18 +1185,17 @@ __device__ __forceinline__ void bwd_dense_item_tma(
             const bool act = inside && off < nc && ((hw >> (off & 31)) & 1u);
             if (!__any_sync(0xffffffffu, act)) continue;
             const float4* qr = S.srec[cb][jj];
-            const float4* ext = S.sext[jj];
             float gl[kNGrad];
 #pragma unroll
             for (int k = 0; k < kNGrad; ++k) gl[k] = 0.f;
-            const Isect is = intersect_bwd(qr, ext, d, cam.min_t);
+            const Isect is = intersect<true>(qr, o, d);
             const float density = qr[0].w;
             Segment sg;
             sg.dt = fmaxf(is.exit - is.enter, 0.f);
             sg.a = density * sg.dt;
             const bool hit = act && is.geo && sg.a > 0.f;
             if (hit) {
-                integrate_bwd(qr, ext, d, cam.min_t, is.enter, is.exit, sg);
+                integrate(qr, o, d, is.enter, is.exit, sg);
                 const float m1 = density * (is.exit + is.enter) / 2.0f;
                 const float logT_old = logT + sg.a;
                 const float T = __expf(logT_old);
@@ -1278,10 +1203,7 @@ __device__ __forceinline__ void bwd_dense_item_tma(
                 D3 = D3 - m1;
                 logT = logT_old;
                 float nD2, nD3;
-                const float4 u0 = ext[1], u1 = ext[2];
-                const f3 a0 = {fmaf(-cam.min_t, d.x, u0.x), fmaf(-cam.min_t, d.y, u0.y), fmaf(-cam.min_t, d.z, u0.z)};
-                const f3 a1 = {fmaf(-cam.min_t, d.x, u1.x), fmaf(-cam.min_t, d.y, u1.y), fmaf(-cam.min_t, d.z, u1.z)};
-                dS_logT = hit_grads_a(qr, a0, a1, d, is, sg, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
+                dS_logT = hit_grads(qr, o, d, is, sg, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
                 dS_D[2] = nD2;
                 dS_D[3] = nD3;
             }
@@ -1303,249 +1225,6 @@ __device__ __forceinline__ void bwd_dense_item_tma(
         ctop = ntop;
         cw0 = nw0;
         cw1 = nw1;
-    }
-}
-
-// Hit-list backward (RM_BLEND_BWD_HITS; 64-pixel items, 256 threads).  The
-// forward's hit masks say, per pixel and list entry, which entries were hits
-// before the pixel terminated, so the backward can compact its work to the
-// hits themselves instead of running each entry on the 32 lanes of a pixel
-// warp whatever their number of hits.  Per batch of B list entries (aligned
-// to B from the list start, so one 32-entry mask word covers a batch):
-//   1. each pixel owner takes its mask bits of the batch (and those below its
-//      n_contributors) and counts them; the entries some pixel hit are
-//      staged (records and entry_ext), and the hits are listed pixel-major,
-//      each pixel's hits in descending list order (the reverse walk);
-//   2. A: one thread per hit computes the segment (a, m1) and
-//      dot(dL/dcolour, rgb);
-//   3. B: each owner walks its hits back to front, in exactly the dense
-//      walk's arithmetic, and records T, D2, D3 before the hit and
-//      dL/d(log T, D2, D3) after it;
-//   4. C: one thread per hit computes the 25 partials of its adjoint and adds
-//      them to the entry's shared accumulator (consecutive hits of one pixel
-//      are different entries, so the atomics of a warp rarely collide);
-//   5. the entries' sums become vertex and cell-value gradients (global
-//      atomics), as in the dense kernel.
-template <int B>
-struct BwdHitSmem {
-    static constexpr int kMaxHits = 64 * B;
-    float4 srec[B][kRecFloat4];
-    float4 sext[B][kExtFloat4];
-    float sacc[B][kNGrad];
-    int32_t sid[B];
-    uint8_t cidx[B];  // kept position -> batch offset
-    uint8_t kpos[B];  // batch offset -> kept position
-    float ray[3][64];   // ray directions of the item's pixels
-    float dc[6][64];    // dL/dcolour (3), dL/dD0, dL/dD1, dL/dD4: constant along the walk
-    int32_t cnt[64];
-    int32_t hit_pre[65];
-    uint32_t wor[2];
-    int32_t n_keep;
-    uint8_t hent[kMaxHits];  // per hit: kept position of its entry
-    uint8_t hpix[kMaxHits];  // per hit: pixel
-    float hx[kMaxHits][6];   // A: a, m1, dot(dLdc, rgb); B: T, D2, D3 before, dL/d(logT, D2, D3) after
-};
-
-template <int B>
-__device__ __forceinline__ void bwd_hits_item(
-    int tile, int sub, const int32_t* __restrict__ ids, const int2* __restrict__ ranges,
-    const float4* __restrict__ recs, const int4* __restrict__ indices, const float2* __restrict__ jitter,
-    const rm_camera& cam, const float4* __restrict__ img, const float* __restrict__ dist,
-    const int32_t* __restrict__ ncs, const float4* __restrict__ gimg, const float* __restrict__ gdist,
-    float* __restrict__ gverts, float* __restrict__ gcv, BwdHitSmem<B>& S, const HitMasks& hm, int subs,
-    int gtile) {
-    static_assert(B == 16 || B == 32, "a batch lies inside one 32-entry mask block");
-    constexpr int NT = 256;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool owner = tid < 64;
-    const f3 cam_pos = {cam.cam_pos[0], cam.cam_pos[1], cam.cam_pos[2]};
-    const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
-    int lx = 0, ly = 0;
-    if (owner) strip_pixel<64>(cam, sub, tid, lx, ly);
-    const int px = tx * cam.tile_width + lx, py = ty * cam.tile_height + ly;
-    const bool inside = owner && px < cam.image_width && py < cam.image_height;
-    const int64_t pix = (int64_t)py * cam.image_width + px;
-    float logT = 0.f, D2 = 0.f, D3 = 0.f, dS_logT = 0.f, dS_D2 = 0.f, dS_D3 = 0.f, dS_D0 = 0.f, dS_D1 = 0.f;
-    int32_t nc = 0;
-    if (owner) {
-        f3 o = {0.f, 0.f, 0.f}, d = {0.f, 0.f, 1.f};
-        float g[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (inside) {
-            const float2 j = __ldg(jitter + pix);
-            make_ray(cam, px, py, j.x, j.y, o, d);
-            logT = __ldg(img + pix).w;
-            D2 = __ldg(dist + 5 * pix + 2);
-            D3 = __ldg(dist + 5 * pix + 3);
-            const float4 gi = __ldg(gimg + pix);
-            g[0] = gi.x; g[1] = gi.y; g[2] = gi.z; g[3] = gi.w;
-#pragma unroll
-            for (int k = 0; k < 5; ++k) g[4 + k] = gdist ? __ldg(gdist + 5 * pix + k) : 0.f;
-            nc = __ldg(ncs + pix);
-        }
-        S.ray[0][tid] = d.x; S.ray[1][tid] = d.y; S.ray[2][tid] = d.z;
-        S.dc[0][tid] = g[0]; S.dc[1][tid] = g[1]; S.dc[2][tid] = g[2];
-        S.dc[3][tid] = g[4]; S.dc[4][tid] = g[5]; S.dc[5][tid] = g[8];
-        dS_logT = g[3];
-        dS_D0 = g[4];
-        dS_D1 = g[5];
-        dS_D2 = g[6];
-        dS_D3 = g[7];
-        int32_t m = nc;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
-        if (lane == 0) S.cnt[warp] = m;  // (reused below as counts)
-    }
-    __syncthreads();
-    const int32_t tile_max = max(S.cnt[0], S.cnt[1]);
-    const int2 rg = __ldg(ranges + tile);
-    const int end = min(rg.y, rg.x + tile_max);
-    for (int top = end, lo; top > rg.x; top = lo) {
-        lo = rg.x + ((top - 1 - rg.x) / B) * B;
-        const int n = top - lo;
-        const int off0 = lo - rg.x;
-        __syncthreads();  // the previous batch is flushed; counts may be rewritten
-        // 1. this pixel's hits of the batch: mask bits below its n_contributors
-        uint32_t bits = 0u;
-        if (owner) {
-            uint32_t w = 0xffffffffu;
-            if (hm.words) {
-                const int64_t i = mask_word(gtile, rg.x, off0 >> 5, sub, subs, tid);
-                if (i < hm.cap) w = __ldcg(hm.words + i);
-            }
-            const int valid = min(n, nc - off0);
-            bits = valid <= 0 ? 0u : (w >> (off0 & 31)) & (valid >= 32 ? 0xffffffffu : ((1u << valid) - 1u));
-            S.cnt[tid] = __popc(bits);
-            const uint32_t wo = __reduce_or_sync(0xffffffffu, bits);
-            if (lane == 0) S.wor[warp] = wo;
-        }
-        __syncthreads();
-        if (warp == 0) {
-            const uint32_t kept = S.wor[0] | S.wor[1];
-            const bool keep = lane < n && ((kept >> lane) & 1u);
-            const unsigned bal = __ballot_sync(0xffffffffu, keep);
-            const int pos = __popc(bal & ((1u << lane) - 1u));
-            if (keep) S.cidx[pos] = (uint8_t)lane;
-            if (lane < B) S.kpos[lane] = keep ? (uint8_t)pos : (uint8_t)0xff;
-            if (lane == 0) S.n_keep = __popc(bal);
-            // exclusive prefix of the 64 per-pixel counts (two per lane)
-            const int c0 = S.cnt[2 * lane], c1 = S.cnt[2 * lane + 1];
-            int incl = c0 + c1;
-#pragma unroll
-            for (int o2 = 1; o2 < 32; o2 <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o2);
-                if (lane >= o2) incl += y;
-            }
-            const int excl = incl - c0 - c1;
-            S.hit_pre[2 * lane] = excl;
-            S.hit_pre[2 * lane + 1] = excl + c0;
-            if (lane == 31) S.hit_pre[64] = incl;
-        }
-        __syncthreads();
-        const int nk = S.n_keep;
-        const int n_hits = S.hit_pre[64];
-        if (nk == 0) continue;  // uniform: nothing of this batch was hit
-        for (int k = tid; k < nk; k += NT) S.sid[k] = __ldg(ids + lo + S.cidx[k]);
-        for (int k = tid; k < nk * kNGrad; k += NT) (&S.sacc[0][0])[k] = 0.f;
-        if (owner) {  // list this pixel's hits, descending list order
-            int h = S.hit_pre[tid];
-            uint32_t b = bits;
-            while (b) {
-                const int k = 31 - __clz(b);
-                b &= ~(1u << k);
-                S.hent[h] = S.kpos[k];
-                S.hpix[h] = (uint8_t)tid;
-                ++h;
-            }
-        }
-        __syncthreads();
-        for (int k = tid; k < nk * kRecFloat4; k += NT) {
-            const int j = k >> 3, c = k & 7;
-            S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
-        }
-        __syncthreads();
-        for (int k = tid; k < nk; k += NT) entry_ext(S.srec[k], cam_pos, S.sext[k]);
-        __syncthreads();
-        // 2. A: segment of every hit
-        for (int h = tid; h < n_hits; h += NT) {
-            const int jj = S.hent[h], p = S.hpix[h];
-            const float4* q = S.srec[jj];
-            const float4* ext = S.sext[jj];
-            const f3 d = {S.ray[0][p], S.ray[1][p], S.ray[2][p]};
-            const Isect is = intersect_bwd(q, ext, d, cam.min_t);
-            const float density = q[0].w;
-            Segment sg;
-            sg.dt = fmaxf(is.exit - is.enter, 0.f);
-            sg.a = density * sg.dt;
-            float a = 0.f, m1 = 0.f, rdot = 0.f;
-            if (is.geo && sg.a > 0.f) {
-                integrate_bwd(q, ext, d, cam.min_t, is.enter, is.exit, sg);
-                a = sg.a;
-                m1 = density * (is.exit + is.enter) / 2.0f;
-                rdot = fmaf(S.dc[2][p], sg.rgb[2], fmaf(S.dc[1][p], sg.rgb[1], S.dc[0][p] * sg.rgb[0]));
-            }
-            S.hx[h][0] = a;
-            S.hx[h][1] = m1;
-            S.hx[h][2] = rdot;
-        }
-        __syncthreads();
-        // 3. B: each owner's chain, back to front
-        if (owner) {
-            const int h1 = S.hit_pre[tid + 1];
-            for (int h = S.hit_pre[tid]; h < h1; ++h) {
-                const float a = S.hx[h][0];
-                if (!(a > 0.f)) {
-                    S.hx[h][0] = -1.f;  // no adjoint
-                    continue;
-                }
-                const float m1 = S.hx[h][1], rdot = S.hx[h][2];
-                const float density = S.srec[S.hent[h]][0].w;
-                const float logT_old = logT + a;
-                const float T = __expf(logT_old);
-                D2 = D2 - density;
-                D3 = D3 - m1;
-                logT = logT_old;
-                S.hx[h][0] = T;
-                S.hx[h][1] = D2;
-                S.hx[h][2] = D3;
-                S.hx[h][3] = dS_logT;
-                S.hx[h][4] = dS_D2;
-                S.hx[h][5] = dS_D3;
-                dS_logT = dS_logT + rdot * T;
-                dS_D2 = dS_D2 + dS_D0 * 2.0f * m1;
-                dS_D3 = dS_D3 + dS_D1 * 2.0f * density;
-            }
-        }
-        __syncthreads();
-        // 4. C: the adjoint of every hit into its entry's accumulator
-        for (int h = tid; h < n_hits; h += NT) {
-            const float T = S.hx[h][0];
-            if (T < 0.f) continue;
-            const int jj = S.hent[h], p = S.hpix[h];
-            const float4* q = S.srec[jj];
-            const float4* ext = S.sext[jj];
-            const f3 d = {S.ray[0][p], S.ray[1][p], S.ray[2][p]};
-            const Isect is = intersect_bwd(q, ext, d, cam.min_t);
-            Segment sg;
-            sg.dt = fmaxf(is.exit - is.enter, 0.f);
-            sg.a = q[0].w * sg.dt;
-            integrate_bwd(q, ext, d, cam.min_t, is.enter, is.exit, sg);
-            const float4 u0 = ext[1], u1 = ext[2];
-            const f3 a0 = {fmaf(-cam.min_t, d.x, u0.x), fmaf(-cam.min_t, d.y, u0.y), fmaf(-cam.min_t, d.z, u0.z)};
-            const f3 a1 = {fmaf(-cam.min_t, d.x, u1.x), fmaf(-cam.min_t, d.y, u1.y), fmaf(-cam.min_t, d.z, u1.z)};
-            const float dsc[3] = {S.dc[0][p], S.dc[1][p], S.dc[2][p]};
-            const float dsd[5] = {S.dc[3][p], S.dc[4][p], S.hx[h][4], S.hx[h][5], S.dc[5][p]};
-            float gl[kNGrad];
-#pragma unroll
-            for (int k = 0; k < kNGrad; ++k) gl[k] = 0.f;
-            float nD2, nD3;
-            hit_grads_a(q, a0, a1, d, is, sg, T, S.hx[h][1], S.hx[h][2], dsc, S.hx[h][3], dsd, gl, nD2, nD3);
-#pragma unroll
-            for (int k = 0; k < kNGrad; ++k)
-                if (gl[k] != 0.f) atomicAdd(&S.sacc[jj][k], gl[k]);
-        }
-        __syncthreads();
-        // 5. per entry: vertex and cell-value gradients
-        flush_entries<NT, B>(nk, S.srec, S.sid, S.sacc, indices, gverts, gcv);
     }
 }
 
@@ -1809,30 +1488,6 @@ __global__ void __launch_bounds__(64, 8) blend_bwd_dense_tma_kernel(
         bwd_dense_item_tma<B>(t - tb, item % q.subs, ids, ranges + tb, recs, indices, jitter + pb,
                               views.camera(v), img + pb, dist + 5 * pb, ncs + pb, gimg + pb,
                               gdist ? gdist + 5 * pb : nullptr, gverts, gcv, S, hm, q.subs, t, pipe, q);
-    }
-}
-
-template <int B, class V>
-__global__ void __launch_bounds__(256, 2) blend_bwd_hits_kernel(
-    const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
-    const int4* __restrict__ indices, const float2* __restrict__ jitter, const __grid_constant__ V views,
-    const float4* __restrict__ img, const float* __restrict__ dist, const int32_t* __restrict__ ncs,
-    const float4* __restrict__ gimg, const float* __restrict__ gdist, float* __restrict__ gverts,
-    float* __restrict__ gcv, const Queue q) {
-    extern __shared__ __align__(16) unsigned char hits_smem_raw[];
-    BwdHitSmem<B>& S = *reinterpret_cast<BwdHitSmem<B>*>(hits_smem_raw);
-    __shared__ int s_item;
-    const int n_items = queue_items(q);
-    const HitMasks hm = live_masks(q.hm);
-    for (;;) {
-        const int item = next_item(q, &s_item);
-        if (item >= n_items) return;
-        const int t = queue_tile(q, item), v = views.find(t);
-        const int tb = views.tile_base(v);
-        const int64_t pb = views.pixel_base(v);
-        bwd_hits_item<B>(t - tb, item % q.subs, ids, ranges + tb, recs, indices, jitter + pb, views.camera(v),
-                         img + pb, dist + 5 * pb, ncs + pb, gimg + pb, gdist ? gdist + 5 * pb : nullptr, gverts,
-                         gcv, S, hm, q.subs, t);
     }
 }
 
@@ -2155,14 +1810,12 @@ struct Tuning {
     int pair_ctas_per_sm;  // resident CTAs of the pair kernel per SM
     bool hit_masks;        // RM_BLEND_HIT_MASKS
     bool tma;              // RM_BLEND_STAGE_TMA
-    bool hits;             // RM_BLEND_BWD_HITS
     uint32_t* status;      // where a staging wait that gives up is reported
 };
 
 Tuning tuning_from_flags(int flags, int def_shift, int def_ctas) {
     Tuning t;
     t.tma = (flags & RM_BLEND_STAGE_TMA) != 0;
-    t.hits = (flags & RM_BLEND_BWD_HITS) != 0;
     t.status = nullptr;
     const int hs = (flags >> RM_BLEND_HEAVY_SHIFT) & 0xf;
     const int pc = (flags >> RM_BLEND_PAIR_CTAS_SHIFT) & 0xf;
@@ -2253,19 +1906,6 @@ int launch_bwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, cons
                                                             (const float2*)jitter, views, (const float4*)img, dist,
                                                             nc, (const float4*)gimg, gdist, gverts, gcv, qp);
     if ((rc = rm_host::check_launch("rm_blend_bwd (pair)"))) return rc;
-    if (PX == 64 && tn.hits) {  // one thread per hit of the forward's masks
-        auto run = [&](auto kernel, int smem) {
-            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            const int grid = persistent_grid(kernel, 256, smem, G * subs);
-            kernel<<<grid, 256, smem, s>>>(ids, (const int2*)ranges, w.recs, (const int4*)indices,
-                                           (const float2*)jitter, views, (const float4*)img, dist, nc,
-                                           (const float4*)gimg, gdist, gverts, gcv, qd);
-        };
-        if (B_DENSE == 16) run(blend_bwd_hits_kernel<16, V>, (int)sizeof(BwdHitSmem<16>));
-        else run(blend_bwd_hits_kernel<32, V>, (int)sizeof(BwdHitSmem<32>));
-        if ((rc = rm_host::check_launch("rm_blend_bwd (hit lists)"))) return rc;
-        return join_side(s, side);
-    }
     if (PX == 64 && tn.tma) {  // records staged by bulk copies, two batches in flight
         auto tma_kernel = blend_bwd_dense_tma_kernel<B_DENSE, V>;
         const int grid = persistent_grid(tma_kernel, 64, 0, G * subs);
