@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="single GPU: skip the multi-view and serving results nested in the training line")
     ap.add_argument("--stage", choices=["ldg", "tma"], default="ldg",
                     help="how the backward stages tet records in shared memory: per-thread loads, or bulk copies "
                          "(cp.async.bulk, two batches in flight); bulk copies only in single-GPU runs")
@@ -300,7 +302,7 @@ def run_b200(args):
         torch.cuda.synchronize()
         if world > 1:
             dist.destroy_process_group()
-        return
+        return None
 
     def timed(jitter_mode, timer=None, sampler=None):
         """K steps, per-step events on the launching stream, L2 flushed between steps."""
@@ -420,7 +422,7 @@ def run_b200(args):
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
-        return
+        return None
 
     Npx = H * W
     P = stats["P"]
@@ -480,7 +482,7 @@ def run_b200(args):
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(mesh, view, args.cpu_seconds)
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # ------------------------------------------------------- CPU (reference) --
@@ -606,7 +608,7 @@ def run_reference(args):
 
 
 # ------------------------------------------------------- multi-view batch --
-def run_multiview(args):
+def run_multiview(args, prebuilt=None):
     """16 ring cameras (8 x 1297x840, 4 x 1920x1080, 4 x 640x480) of a 1M-point
     mixture mesh; fwd + L1 loss + bwd of all views per step.  Batched: one
     launch per stage over all views, replayed as a CUDA graph.  Per view: the
@@ -630,7 +632,10 @@ def run_multiview(args):
     from delaunay_rasterization.internal.tile_shader_slang import vertex_and_tile_shader
 
     t0 = time.perf_counter()
-    mesh, views = scenes.workload_multiview(n_points=args.mv_points, seed=3, tile_size=16)
+    if prebuilt is not None:
+        mesh, views = prebuilt, scenes.multiview_cameras(16)
+    else:
+        mesh, views = scenes.workload_multiview(n_points=args.mv_points, seed=3, tile_size=16)
     views = views[:args.mv_views]
     gen_s = time.perf_counter() - t0
     T = len(mesh.indices)
@@ -750,7 +755,7 @@ def run_multiview(args):
         "stages_ms_batched_eager": stages, "mesh_generation_s": gen_s,
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # ----------------------------------------------------------------- serving --
@@ -758,13 +763,18 @@ def _serving_mesh(job):
     n, seed = job
     from radiance_meshes_b200 import scenes
 
-    pts = scenes.mixture_points(n, seed)
-    idx = scenes.delaunay(pts)
-    cv = scenes.make_features(len(idx), seed=seed + 1000, low_density_frac=0.3)
-    return n, pts, idx, cv
+    m = scenes.mixture_mesh(n, seed)
+    return n, m.vertices, m.indices, m.cell_values
 
 
-def run_serving(args):
+def _mesh_job(job):
+    """(points, seed) -> a mixture mesh (runs in a spawned host process)."""
+    from radiance_meshes_b200 import scenes
+
+    return scenes.mixture_mesh(*job)
+
+
+def run_serving(args, prebuilt=None):
     """Three resident meshes (250k / 1M / 3M mixture points, seeds 4-6), a
     Poisson stream of forward render requests (200 req/s, seed 7), each on a
     uniformly chosen mesh with a camera uniform on the radius-4 sphere and a
@@ -776,8 +786,11 @@ def run_serving(args):
     counts = [int(x) for x in args.sv_points.split(",")]
     seeds = [4, 5, 6][:len(counts)]
     t0 = time.perf_counter()
-    with mp.get_context("spawn").Pool(len(counts)) as pool:  # before any CUDA call
-        built = pool.map(_serving_mesh, list(zip(counts, seeds)))
+    if prebuilt is not None:
+        built = [(n, m.vertices, m.indices, m.cell_values) for n, m in zip(counts, prebuilt)]
+    else:
+        with mp.get_context("spawn").Pool(len(counts)) as pool:  # before any CUDA call
+            built = pool.map(_serving_mesh, list(zip(counts, seeds)))
     gen_s = time.perf_counter() - t0
 
     import torch
@@ -857,19 +870,53 @@ def run_serving(args):
         "resident_bytes": sum(m.nbytes for m in resident), "gpu_launches": int(launches),
         "mesh_generation_s": gen_s, "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_default(args):
+    """The training line, with the multi-view and serving results nested in
+    it (single GPU): their meshes are built in spawned host processes while
+    the training step is measured."""
+    import multiprocessing as mp
+
+    world, rank, local = dist_env()
+    extras = world == 1 and not args.no_extras and not args.profile_steps
+    pool = jobs = None
+    if extras:
+        counts = [int(x) for x in args.sv_points.split(",")]
+        spec = [(args.mv_points, 3)] + list(zip(counts, [4, 5, 6][:len(counts)]))
+        pool = mp.get_context("spawn").Pool(len(spec))
+        jobs = pool.map_async(_mesh_job, spec)
+    try:
+        line = run_b200(args)
+        if line is None or not extras:
+            return line
+        t0 = time.perf_counter()
+        meshes = jobs.get()
+        line["extras_mesh_wait_s"] = time.perf_counter() - t0
+        for key, fn, arg in (("multiview", run_multiview, meshes[0]), ("serving", run_serving, meshes[1:])):
+            try:
+                line[key] = fn(args, arg)
+            except Exception as e:  # the training line stands on its own
+                line[key] = {"error": f"{type(e).__name__}: {e}"}
+        return line
+    finally:
+        if pool is not None:
+            pool.terminate()
 
 
 def main():
     args = parse()
     if args.impl == "b200" and args.workload == "serving":
-        return run_serving(args)
-    if args.impl == "reference":
-        run_reference(args)
+        line = run_serving(args)
+    elif args.impl == "reference":
+        return run_reference(args)
     elif args.workload == "multiview":
-        run_multiview(args)
+        line = run_multiview(args)
     else:
-        run_b200(args)
+        line = run_default(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":

@@ -178,15 +178,26 @@ def ring_views(n_views: int, resolutions, radius: float = 4.0, height_offset: fl
     return views
 
 
-def workload_multiview(n_points: int = 1_000_000, seed: int = 3, tile_size: int = 16):
-    """1M mixture points; 16 ring cameras: 8 x 1297x840, 4 x 1920x1080, 4 x 640x480."""
+def multiview_cameras(tile_size: int = 16):
+    """16 cameras evenly spaced on the radius-4 ring: 8 x 1297x840,
+    4 x 1920x1080, 4 x 640x480 (interleaved)."""
+    res = [(840, 1297)] * 8 + [(1080, 1920)] * 4 + [(480, 640)] * 4
+    order = [0, 8, 1, 12, 2, 9, 3, 13, 4, 10, 5, 14, 6, 11, 7, 15]
+    return ring_views(16, [res[i] for i in order], tile_size=tile_size)
+
+
+def mixture_mesh(n_points: int, seed: int) -> "Mesh":
+    """A mixture cloud tetrahedralised, with the workloads' features (30% of
+    densities at 1e-4, feature seed = seed + 1000)."""
     pts = mixture_points(n_points, seed)
     idx = delaunay(pts)
     cv = make_features(len(idx), seed=seed + 1000, low_density_frac=0.3)
-    res = [(840, 1297)] * 8 + [(1080, 1920)] * 4 + [(480, 640)] * 4
-    order = [0, 8, 1, 12, 2, 9, 3, 13, 4, 10, 5, 14, 6, 11, 7, 15]
-    views = ring_views(16, [res[i] for i in order], tile_size=tile_size)
-    return Mesh(pts, idx, cv, f"mixture{n_points}"), views
+    return Mesh(pts, idx, cv, f"mixture{n_points}")
+
+
+def workload_multiview(n_points: int = 1_000_000, seed: int = 3, tile_size: int = 16):
+    """1M mixture points; 16 ring cameras: 8 x 1297x840, 4 x 1920x1080, 4 x 640x480."""
+    return mixture_mesh(n_points, seed), multiview_cameras(tile_size)
 
 
 def sphere_view(rng, height: int, width: int, radius: float = 4.0, tile_size: int = 16) -> View:
