@@ -221,6 +221,45 @@ RM_API int rm_sort_pairs(const int64_t* keys_in, const int32_t* values_in, int64
                   uint32_t* status_dev, void* stream);
 
 /*
+ * rm_sort_pairs on key bits [begin_bit, end_bit) only (cub::DeviceRadixSort::
+ * SortPairs with a begin bit); stable, so equal keys keep their input order.
+ */
+RM_API int rm_sort_pairs_range(const int64_t* keys_in, const int32_t* values_in, int64_t n,
+                               const int64_t* n_dev, int begin_bit, int end_bit, int64_t* keys_out,
+                               int32_t* values_out, void* workspace, size_t workspace_bytes,
+                               uint32_t* status_dev, void* stream);
+
+/*
+ * Depth-first list build, the same sorted lists in fewer sort passes (no
+ * reference counterpart; the reference sorts the pairs once on 32 + msb
+ * bits):
+ *   1. rm_depth_order: the visible tets (tiles_touched > 0), in tet order,
+ *      as (key = sortable depth key of vs[:,2], value = tet id) pairs;
+ *      *n_visible_dev = their count.  Workspace rm_depth_order_workspace_size(T).
+ *   2. rm_sort_pairs_range(..., 0, 32, ...) over them (stable: equal depths
+ *      stay in tet order).
+ *   3. rm_emit_pairs_ordered: the pairs of the tets in that order (keys and
+ *      values as rm_emit_pairs); *total_dev = pair count; the tile counts are
+ *      scanned in that order internally.  Workspace
+ *      rm_emit_ordered_workspace_size(T).
+ *   4. rm_sort_pairs_range(..., 32, 32 + msb, ...): a stable sort on the tile
+ *      bits alone, which leaves each tile's pairs in (depth, tet id) order:
+ *      keys and values equal rm_sort_pairs(..., 32 + msb, ...) of
+ *      rm_emit_pairs' tet-order emission.
+ */
+RM_API size_t rm_depth_order_workspace_size(int64_t n_tets);
+RM_API int rm_depth_order(const int32_t* tiles_touched, const float* vs, int64_t n_tets,
+                          int64_t* keys, int32_t* values, int64_t* n_visible_dev,
+                          void* workspace, size_t workspace_bytes, uint32_t* status_dev,
+                          void* stream);
+RM_API size_t rm_emit_ordered_workspace_size(int64_t n_tets);
+RM_API int rm_emit_pairs_ordered(const float* vs, const int32_t* rect, const int32_t* tiles_touched,
+                                 const int32_t* order, int64_t n_tets, const int64_t* n_items_dev,
+                                 int32_t grid_width, int64_t capacity, int64_t* total_dev,
+                                 int64_t* keys, int32_t* values, void* workspace,
+                                 size_t workspace_bytes, uint32_t* status_dev, void* stream);
+
+/*
  * Per-tile [start, end) ranges of the sorted pair list; empty tiles get [0,0].
  * Replaces compute_tile_ranges (delaunay_rasterization/internal/slang/tile_shader.slang:188-214)
  * launched at delaunay_rasterization/internal/tile_shader_slang.py:61-69 (the

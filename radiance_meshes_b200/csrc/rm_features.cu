@@ -104,6 +104,19 @@ __global__ void __launch_bounds__(128) features_kernel(
         }
         return;
     }
+    if (BWD) {  // a tet that nothing downstream used (e.g. one outside the view): zero gradients, no atomics
+        const float* gf = gfeat + 7 * t;
+        bool zero = true;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) zero &= __ldg(gf + k) == 0.f;
+        if (zero) {
+            g_density[t] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) g_rgb[3 * t + k] = g_grd[3 * t + k] = g_cc[3 * t + k] = 0.f;
+            for (int k = 0; k < 3 * n_rest; ++k) g_sh[(int64_t)3 * n_rest * t + k] = 0.f;
+            return;
+        }
+    }
     const int vid[4] = {id.x, id.y, id.z, id.w};
     f3 v[4];
 #pragma unroll

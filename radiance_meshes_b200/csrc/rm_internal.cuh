@@ -340,6 +340,10 @@ uint32_t wait_limit();
 // of the workspace's own status word (status NULL: the workspace's word).
 int scan_tiles_status(const int32_t* tiles_touched, int64_t n_tets, int32_t* offsets, int64_t* total_dev,
                       void* workspace, size_t workspace_bytes, uint32_t* status, void* stream);
+// mode 1: inclusive scan of (in[i] > 0); mode 2: of in[order[i]] for i < *n_dev
+// (n_dev may be NULL: all n), zero beyond.
+int scan_mode(int mode, const int32_t* in, const int32_t* order, int64_t n, const int64_t* n_dev, int32_t* out,
+              int64_t* total_dev, void* workspace, size_t workspace_bytes, uint32_t* status, void* stream);
 // Checks the launch status of the preceding kernel launches and adds
 // `kernels` to the process-wide launch counter.
 int check_launch(const char* what, int kernels = 1);

@@ -42,9 +42,26 @@ __device__ __forceinline__ uint64_t ld_acquire(const uint64_t* p) {
 // as the reference's cumsum) sets RM_STATUS_OVERFLOW.  The look-back polls a
 // predecessor at most spin_limit times, then sets RM_STATUS_SCAN_TIMEOUT and
 // goes on (the offsets are then invalid; every store stays in bounds).
+// What the scan sums: the input values; 1 for each positive value (counts of
+// the visible tets); or the values gathered through an order, in[order[i]],
+// for i below *n_dev (counts in depth order).
+enum ScanMode { kScanValues = 0, kScanPositive = 1, kScanGather = 2 };
+
+template <int MODE>
+__device__ __forceinline__ int32_t scan_item(const int32_t* __restrict__ in, const int32_t* __restrict__ order,
+                                             int64_t i, int64_t n_eff) {
+    if (i >= n_eff) return 0;
+    if (MODE == kScanGather) return __ldg(in + __ldg(order + i));
+    const int32_t v = __ldg(in + i);
+    return MODE == kScanPositive ? (v > 0 ? 1 : 0) : v;
+}
+
+template <int MODE>
 __global__ void __launch_bounds__(kScanThreads) scan_kernel(const int32_t* __restrict__ in, int64_t n,
                                                             int32_t* __restrict__ out, int64_t* total_dev,
-                                                            ScanWs* ws, uint32_t* status, uint32_t spin_limit) {
+                                                            ScanWs* ws, uint32_t* status, uint32_t spin_limit,
+                                                            const int32_t* __restrict__ order,
+                                                            const int64_t* __restrict__ n_dev) {
     __shared__ uint32_t s_tile;
     __shared__ int64_t s_warp[kScanThreads / 32];
     __shared__ int64_t s_prefix;
@@ -54,7 +71,8 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const int32_t* __res
     const uint32_t tile = s_tile;
     const int64_t base = (int64_t)tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
     int32_t v[kScanItems];
-    if (base + kScanItems <= n && ((((uintptr_t)(in + base)) & 15) == 0)) {
+    const int64_t n_eff = n_dev ? min(*n_dev, n) : n;
+    if (MODE != kScanGather && base + kScanItems <= n_eff && ((((uintptr_t)(in + base)) & 15) == 0)) {
         const int4* p = reinterpret_cast<const int4*>(in + base);
 #pragma unroll
         for (int k = 0; k < kScanItems / 4; ++k) {
@@ -64,9 +82,12 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const int32_t* __res
             v[4 * k + 2] = q.z;
             v[4 * k + 3] = q.w;
         }
+        if (MODE == kScanPositive)
+#pragma unroll
+            for (int k = 0; k < kScanItems; ++k) v[k] = v[k] > 0 ? 1 : 0;
     } else {
 #pragma unroll
-        for (int k = 0; k < kScanItems; ++k) v[k] = (base + k < n) ? __ldg(in + base + k) : 0;
+        for (int k = 0; k < kScanItems; ++k) v[k] = scan_item<MODE>(in, order, base + k, n_eff);
     }
     int64_t sum = 0;
 #pragma unroll
@@ -266,6 +287,65 @@ __global__ void __launch_bounds__(kEmitThreads) emit_multi_kernel(
     }
 }
 
+// Depth-first list build (rm_depth_order, rm_emit_pairs_ordered): the visible
+// tets are compacted in tet order with their sortable depth keys, sorted by
+// depth once (stable, so equal depths stay in tet order), and the pairs are
+// emitted in that order; a stable sort on the tile bits alone then yields
+// the reference's (tile, depth, emission order) sequence.
+__global__ void __launch_bounds__(256) depth_scatter_kernel(const int32_t* __restrict__ tiles,
+                                                            const float* __restrict__ vs, int64_t n_tets,
+                                                            const int32_t* __restrict__ incl,
+                                                            int64_t* __restrict__ keys, int32_t* __restrict__ vals) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_tets || __ldg(tiles + g) <= 0) return;
+    const int64_t pos = (int64_t)__ldg(incl + g) - 1;
+    keys[pos] = (int64_t)sortable_key(__ldg(vs + 3 * g + 2));
+    vals[pos] = (int32_t)g;
+}
+
+// emit_kernel over the tets in the given order (order[0 .. *n_items_dev)),
+// with offsets the inclusive scan of their tile counts in that order.
+__global__ void __launch_bounds__(kEmitThreads) emit_ordered_kernel(
+    const float* __restrict__ vs, const int4* __restrict__ rect, const int32_t* __restrict__ order,
+    const int32_t* __restrict__ offsets, const int64_t* __restrict__ n_items_dev, int64_t n_cap, int32_t grid_w,
+    int64_t capacity, const int64_t* __restrict__ total_dev, int64_t* __restrict__ keys, int32_t* __restrict__ vals,
+    uint32_t* status) {
+    __shared__ int32_t soff[kEmitStage];
+    __shared__ int64_t sg[2];
+    const int64_t n_items = min(*n_items_dev, n_cap);
+    if (n_items <= 0) return;
+    const int64_t n_pairs = min((int64_t)__ldg(offsets + n_items - 1), capacity);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && total_dev && status && *total_dev > capacity)
+        atomicOr(status, RM_STATUS_CAPACITY);
+    const int64_t p0 = (int64_t)blockIdx.x * kEmitPerCta;
+    if (p0 >= n_pairs) return;
+    const int64_t p1 = min(p0 + kEmitPerCta, n_pairs);
+    if (threadIdx.x < 2) sg[threadIdx.x] = upper_bound_i32(offsets, 0, n_items, threadIdx.x ? p1 - 1 : p0);
+    __syncthreads();
+    const int64_t s0 = sg[0], s1 = sg[1];
+    const bool staged = s1 - s0 + 1 <= kEmitStage;
+    if (staged)
+        for (int64_t i = threadIdx.x; i <= s1 - s0; i += kEmitThreads) soff[i] = __ldg(offsets + s0 + i);
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kEmitItems; ++it) {
+        const int64_t p = p0 + it * kEmitThreads + threadIdx.x;
+        if (p >= p1) break;
+        int64_t si;
+        if (staged) si = s0 + upper_bound_i32(soff, 0, s1 - s0 + 1, p);
+        else si = upper_bound_i32(offsets, s0, s1 + 1, p);
+        const int64_t excl = si == 0 ? 0 : (int64_t)__ldg(offsets + si - 1);
+        const int32_t k = (int32_t)(p - excl);
+        const int64_t g = __ldg(order + si);
+        const int4 r = __ldg(rect + g);
+        const int32_t w = r.z - r.x;
+        const int32_t y = r.y + k / w, x = r.x + k % w;
+        const uint64_t fk = sortable_key(__ldg(vs + 3 * g + 2));
+        keys[p] = (int64_t)(((uint64_t)(uint32_t)(y * grid_w + x) << 32) | fk);
+        vals[p] = (int32_t)g;
+    }
+}
+
 __global__ void __launch_bounds__(256) ranges_kernel(const int64_t* __restrict__ keys, int64_t cap,
                                                      const int64_t* __restrict__ n_dev,
                                                      int32_t* __restrict__ ranges, int64_t n_tiles) {
@@ -324,10 +404,39 @@ int rm_host::scan_tiles_status(const int32_t* tiles_touched, int64_t n_tets, int
     if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_scan_tiles: %s", cudaGetErrorString(e));
     const int64_t blocks = (n_tets + rm::kScanTile - 1) / rm::kScanTile;
     rm::ScanWs* ws = (rm::ScanWs*)workspace;
-    rm::scan_kernel<<<(unsigned)blocks, rm::kScanThreads, 0, s>>>(tiles_touched, n_tets, offsets, total_dev, ws,
-                                                                 status ? status : &ws->status,
-                                                                 rm_host::wait_limit());
+    rm::scan_kernel<rm::kScanValues><<<(unsigned)blocks, rm::kScanThreads, 0, s>>>(
+        tiles_touched, n_tets, offsets, total_dev, ws, status ? status : &ws->status, rm_host::wait_limit(), nullptr,
+        nullptr);
     return rm_host::check_launch("rm_scan_tiles");
+}
+
+// The scans of the depth-first list build: counts of positive values, or
+// values gathered through an order for the first *n_dev items.  Same
+// workspace and checks as rm_scan_tiles.
+int rm_host::scan_mode(int mode, const int32_t* in, const int32_t* order, int64_t n, const int64_t* n_dev,
+                       int32_t* out, int64_t* total_dev, void* workspace, size_t workspace_bytes, uint32_t* status,
+                       void* stream) {
+    if (n < 0) return rm_host::fail(RM_EINVAL, "scan: negative size");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n == 0) {
+        cudaError_t e = cudaMemsetAsync(total_dev, 0, sizeof(int64_t), s);
+        return e == cudaSuccess ? RM_OK : rm_host::fail(RM_ECUDA, "scan: %s", cudaGetErrorString(e));
+    }
+    if (n >= (int64_t)INT32_MAX) return rm_host::fail(RM_EINVAL, "scan: too many items");
+    const size_t need = rm_scan_workspace_size(n);
+    if (workspace_bytes < need) return rm_host::fail(RM_EINVAL, "scan: workspace %zu < %zu bytes", workspace_bytes, need);
+    cudaError_t e = cudaMemsetAsync((char*)workspace + 4, 0, need - 4, s);
+    if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "scan: %s", cudaGetErrorString(e));
+    const int64_t blocks = (n + rm::kScanTile - 1) / rm::kScanTile;
+    rm::ScanWs* ws = (rm::ScanWs*)workspace;
+    uint32_t* st = status ? status : &ws->status;
+    if (mode == rm::kScanPositive)
+        rm::scan_kernel<rm::kScanPositive><<<(unsigned)blocks, rm::kScanThreads, 0, s>>>(
+            in, n, out, total_dev, ws, st, rm_host::wait_limit(), nullptr, n_dev);
+    else
+        rm::scan_kernel<rm::kScanGather><<<(unsigned)blocks, rm::kScanThreads, 0, s>>>(
+            in, n, out, total_dev, ws, st, rm_host::wait_limit(), order, n_dev);
+    return rm_host::check_launch("scan");
 }
 
 extern "C" {
@@ -381,6 +490,68 @@ int rm_emit_pairs_multi(const float* depth, const int32_t* rect, const int32_t* 
         depth, (const int4*)rect, offsets, n_tets, views, capacity, total_dev, keys, values, status_dev,
         (const float4*)footprint_2x, (const float4*)jitter_bounds);
     return rm_host::check_launch("rm_emit_pairs_multi");
+}
+
+size_t rm_depth_order_workspace_size(int64_t n_tets) {
+    const size_t a = ((sizeof(int32_t) * (size_t)(n_tets > 0 ? n_tets : 1)) + 255) / 256 * 256;
+    return a + rm_scan_workspace_size(n_tets > 0 ? n_tets : 0);
+}
+
+int rm_depth_order(const int32_t* tiles_touched, const float* vs, int64_t n_tets, int64_t* keys, int32_t* values,
+                   int64_t* n_visible_dev, void* workspace, size_t workspace_bytes, uint32_t* status_dev,
+                   void* stream) {
+    if (n_tets < 0) return rm_host::fail(RM_EINVAL, "rm_depth_order: negative size");
+    if (!n_visible_dev) return rm_host::fail(RM_EINVAL, "rm_depth_order: NULL count");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n_tets == 0) {
+        cudaError_t e = cudaMemsetAsync(n_visible_dev, 0, sizeof(int64_t), s);
+        return e == cudaSuccess ? RM_OK : rm_host::fail(RM_ECUDA, "rm_depth_order: %s", cudaGetErrorString(e));
+    }
+    if (!tiles_touched || !vs || !keys || !values || !workspace)
+        return rm_host::fail(RM_EINVAL, "rm_depth_order: NULL pointer");
+    if (workspace_bytes < rm_depth_order_workspace_size(n_tets) || ((uintptr_t)workspace & 255))
+        return rm_host::fail(RM_EINVAL, "rm_depth_order: workspace of %zu bytes, 256-byte aligned, needed",
+                             rm_depth_order_workspace_size(n_tets));
+    int32_t* incl = (int32_t*)workspace;
+    char* scan_ws = (char*)workspace + (rm_depth_order_workspace_size(n_tets) - rm_scan_workspace_size(n_tets));
+    int rc = rm_host::scan_mode(rm::kScanPositive, tiles_touched, nullptr, n_tets, nullptr, incl, n_visible_dev,
+                                scan_ws, rm_scan_workspace_size(n_tets), status_dev, s);
+    if (rc) return rc;
+    const unsigned blocks = (unsigned)((n_tets + 255) / 256);
+    rm::depth_scatter_kernel<<<blocks, 256, 0, s>>>(tiles_touched, vs, n_tets, incl, keys, values);
+    return rm_host::check_launch("rm_depth_order");
+}
+
+size_t rm_emit_ordered_workspace_size(int64_t n_tets) { return rm_depth_order_workspace_size(n_tets); }
+
+int rm_emit_pairs_ordered(const float* vs, const int32_t* rect, const int32_t* tiles_touched, const int32_t* order,
+                          int64_t n_tets, const int64_t* n_items_dev, int32_t grid_width, int64_t capacity,
+                          int64_t* total_dev, int64_t* keys, int32_t* values, void* workspace,
+                          size_t workspace_bytes, uint32_t* status_dev, void* stream) {
+    if (n_tets < 0 || capacity < 0) return rm_host::fail(RM_EINVAL, "rm_emit_pairs_ordered: negative size");
+    if (!total_dev || !n_items_dev) return rm_host::fail(RM_EINVAL, "rm_emit_pairs_ordered: NULL count");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n_tets == 0) {
+        cudaError_t e = cudaMemsetAsync(total_dev, 0, sizeof(int64_t), s);
+        return e == cudaSuccess ? RM_OK : rm_host::fail(RM_ECUDA, "rm_emit_pairs_ordered: %s", cudaGetErrorString(e));
+    }
+    if (!vs || !rect || !tiles_touched || !order || !workspace || (capacity > 0 && (!keys || !values)))
+        return rm_host::fail(RM_EINVAL, "rm_emit_pairs_ordered: NULL pointer");
+    if ((uintptr_t)rect & 15) return rm_host::fail(RM_EINVAL, "rm_emit_pairs_ordered: rect must be 16-byte aligned");
+    if (workspace_bytes < rm_emit_ordered_workspace_size(n_tets) || ((uintptr_t)workspace & 255))
+        return rm_host::fail(RM_EINVAL, "rm_emit_pairs_ordered: workspace of %zu bytes, 256-byte aligned, needed",
+                             rm_emit_ordered_workspace_size(n_tets));
+    int32_t* offs = (int32_t*)workspace;
+    char* scan_ws = (char*)workspace + (rm_emit_ordered_workspace_size(n_tets) - rm_scan_workspace_size(n_tets));
+    int rc = rm_host::scan_mode(rm::kScanGather, tiles_touched, order, n_tets, n_items_dev, offs, total_dev, scan_ws,
+                                rm_scan_workspace_size(n_tets), status_dev, s);
+    if (rc) return rc;
+    const int64_t blocks = std::max<int64_t>(1, (capacity + rm::kEmitPerCta - 1) / rm::kEmitPerCta);
+    if (blocks > 0x7fffffff) return rm_host::fail(RM_EINVAL, "rm_emit_pairs_ordered: capacity too large");
+    rm::emit_ordered_kernel<<<(unsigned)blocks, rm::kEmitThreads, 0, s>>>(
+        vs, (const int4*)rect, order, offs, n_items_dev, n_tets, grid_width, capacity, total_dev, keys, values,
+        status_dev);
+    return rm_host::check_launch("rm_emit_pairs_ordered");
 }
 
 int64_t rm_views_tile_count(const rm_camera* cams, int n_views) {

@@ -72,7 +72,7 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 
 __global__ void __launch_bounds__(kSortThreads) hist_kernel(const uint64_t* __restrict__ keys, int64_t cap,
                                                             const int64_t* __restrict__ n_dev, int npasses,
-                                                            int end_bit, SortHeader* hdr) {
+                                                            int begin_bit, int end_bit, SortHeader* hdr) {
     __shared__ uint32_t sh[kMaxPasses][kRadix];
     for (int j = threadIdx.x; j < kMaxPasses * kRadix; j += blockDim.x) (&sh[0][0])[j] = 0;
     __syncthreads();
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kSortThreads) hist_kernel(const uint64_t* __re
     for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = i0 + threadIdx.x;
         const bool valid = i < n;
-        const uint64_t k = valid ? (__ldg(keys + i) & mask) : 0;
+        const uint64_t k = valid ? ((__ldg(keys + i) & mask) >> begin_bit) : 0;
         const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
         for (int p = 0; p < npasses; ++p) {
             const uint32_t d = (uint32_t)(k >> (8 * p)) & 255u;
@@ -259,17 +259,18 @@ size_t rm_sort_workspace_size(int64_t n) {
     return rm::sort_layout(n, rm::kMaxPasses).total;
 }
 
-int rm_sort_pairs(const int64_t* keys_in, const int32_t* values_in, int64_t n, const int64_t* n_dev, int end_bit,
-                  int64_t* keys_out, int32_t* values_out, void* workspace, size_t workspace_bytes,
-                  uint32_t* status_dev, void* stream) {
+int rm_sort_pairs_range(const int64_t* keys_in, const int32_t* values_in, int64_t n, const int64_t* n_dev,
+                        int begin_bit, int end_bit, int64_t* keys_out, int32_t* values_out, void* workspace,
+                        size_t workspace_bytes, uint32_t* status_dev, void* stream) {
     using namespace rm;
     if (n < 0) return rm_host::fail(RM_EINVAL, "rm_sort_pairs: negative size");
-    if (end_bit < 1 || end_bit > 64) return rm_host::fail(RM_EINVAL, "rm_sort_pairs: end_bit %d out of range", end_bit);
+    if (end_bit < 1 || end_bit > 64 || begin_bit < 0 || begin_bit >= end_bit)
+        return rm_host::fail(RM_EINVAL, "rm_sort_pairs: key bits [%d, %d) out of range", begin_bit, end_bit);
     if (n >= (int64_t)kLbMask) return rm_host::fail(RM_EINVAL, "rm_sort_pairs: at most 2^30-1 pairs");
     if (n == 0) return RM_OK;
     if (!keys_in || !values_in || !keys_out || !values_out || !workspace)
         return rm_host::fail(RM_EINVAL, "rm_sort_pairs: NULL pointer");
-    const int npasses = (end_bit + 7) / 8;
+    const int npasses = (end_bit - begin_bit + 7) / 8;
     const SortLayout L = sort_layout(n, npasses);
     if (workspace_bytes < L.total)
         return rm_host::fail(RM_EINVAL, "rm_sort_pairs: workspace %zu < %zu bytes", workspace_bytes, L.total);
@@ -286,7 +287,8 @@ int rm_sort_pairs(const int64_t* keys_in, const int32_t* values_in, int64_t n, c
     if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_sort_pairs: %s", cudaGetErrorString(e));
     const int64_t tiles = sort_tiles(n);
     int hist_blocks = (int)(tiles < 148 * 2 ? tiles : 148 * 2);
-    hist_kernel<<<hist_blocks, kSortThreads, 0, s>>>((const uint64_t*)keys_in, n, n_dev, npasses, end_bit, hdr);
+    hist_kernel<<<hist_blocks, kSortThreads, 0, s>>>((const uint64_t*)keys_in, n, n_dev, npasses, begin_bit, end_bit,
+                                                     hdr);
     hist_scan_kernel<<<npasses, kRadix, 0, s>>>(hdr);
     const uint64_t* src_k = (const uint64_t*)keys_in;
     const uint32_t* src_v = (const uint32_t*)values_in;
@@ -295,15 +297,23 @@ int rm_sort_pairs(const int64_t* keys_in, const int32_t* values_in, int64_t n, c
         const bool to_out = ((npasses - 1 - p) % 2) == 0;
         uint64_t* dk = to_out ? (uint64_t*)keys_out : alt_k;
         uint32_t* dv = to_out ? (uint32_t*)values_out : alt_v;
-        const int bits = (end_bit - 8 * p) < 8 ? (end_bit - 8 * p) : 8;
+        const int shift = begin_bit + 8 * p;
+        const int bits = (end_bit - shift) < 8 ? (end_bit - shift) : 8;
         const uint32_t dmask = (bits >= 8) ? 255u : ((1u << bits) - 1u);
         onesweep_kernel<<<(unsigned)tiles, kSortThreads, sizeof(PassSmem), s>>>(
-            src_k, src_v, dk, dv, n, n_dev, p, 8 * p, dmask, hdr, lookback + (size_t)p * tiles * kRadix,
+            src_k, src_v, dk, dv, n, n_dev, p, shift, dmask, hdr, lookback + (size_t)p * tiles * kRadix,
             status_dev ? status_dev : &hdr->status, rm_host::wait_limit());
         src_k = dk;
         src_v = dv;
     }
     return rm_host::check_launch("rm_sort_pairs", 2 + npasses);
+}
+
+int rm_sort_pairs(const int64_t* keys_in, const int32_t* values_in, int64_t n, const int64_t* n_dev, int end_bit,
+                  int64_t* keys_out, int32_t* values_out, void* workspace, size_t workspace_bytes,
+                  uint32_t* status_dev, void* stream) {
+    return rm_sort_pairs_range(keys_in, values_in, n, n_dev, 0, end_bit, keys_out, values_out, workspace,
+                               workspace_bytes, status_dev, stream);
 }
 
 }  // extern "C"
