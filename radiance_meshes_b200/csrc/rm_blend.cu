@@ -286,6 +286,7 @@ struct Queue {
     HitMasks hm;
     uint32_t* status;     // RM_STATUS_* bits of the pass (a staging copy whose wait gave up)
     uint32_t spin_limit;  // polls of a bounded wait
+    int64_t n_recs;       // records (tets) the list ids may name
 };
 
 __device__ __forceinline__ int queue_items(const Queue& q) {
@@ -304,6 +305,21 @@ __device__ __forceinline__ int next_item(const Queue& q, int* s_item) {
     const int item = *s_item;
     __syncthreads();
     return item;
+}
+
+// A list entry's tet id, or -1 when it names no record.  Only lists left
+// invalid by a scan or sort that gave up (or a caller's corrupt lists) hold
+// such ids; the entry is then staged as a zero record, which no ray hits, and
+// RM_STATUS_BAD_INDEX is set.
+__device__ __forceinline__ int32_t list_id(const int32_t* __restrict__ ids, int64_t e, const Queue& lq) {
+    const int32_t g = __ldg(ids + e);
+    if (g >= 0 && (int64_t)g < lq.n_recs) return g;
+    if (lq.status) atomicOr(lq.status, RM_STATUS_BAD_INDEX);
+    return -1;
+}
+
+__device__ __forceinline__ float4 record_part(const float4* __restrict__ recs, int32_t g, int c) {
+    return g >= 0 ? __ldg(recs + (int64_t)kRecFloat4 * g + c) : make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // Stores the hit bits of one batch (B a multiple of 32, starting 32-aligned
@@ -377,7 +393,7 @@ __device__ __forceinline__ void fwd_dense_item(int tile, int sub, const int32_t*
                                                const float2* __restrict__ jitter, const rm_camera& cam,
                                                float4* __restrict__ out_img, float* __restrict__ out_dist,
                                                int32_t* __restrict__ out_nc, FwdDenseSmem<B>& S,
-                                               const HitMasks& hm, int subs, int gtile) {
+                                               const HitMasks& hm, int subs, int gtile, const Queue& lq) {
     constexpr bool kMasks = NT == 64 && B % 32 == 0;
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
     int lx, ly;
@@ -397,11 +413,11 @@ __device__ __forceinline__ void fwd_dense_item(int tile, int sub, const int32_t*
     if (__syncthreads_or(active)) {
         for (int base = rg.x; base < rg.y; base += B) {
             const int n = min(B, rg.y - base);
-            for (int k = threadIdx.x; k < n; k += NT) S.sid[k] = __ldg(ids + base + k);
+            for (int k = threadIdx.x; k < n; k += NT) S.sid[k] = list_id(ids, base + k, lq);
             __syncthreads();
             for (int k = threadIdx.x; k < n * kRecFloat4; k += NT) {
                 const int j = k >> 3, c = k & 7;
-                S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
+                S.srec[j][c] = record_part(recs, S.sid[j], c);
             }
             __syncthreads();
             uint64_t hb = 0;  // bit j: entry j of the batch was a hit
@@ -467,7 +483,7 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
                                          const float2* __restrict__ jitter, const rm_camera& cam,
                                          float4* __restrict__ out_img, float* __restrict__ out_dist,
                                          int32_t* __restrict__ out_nc, FwdPairSmem<PX, B>& S,
-                                         const HitMasks& hm, int subs, int gtile) {
+                                         const HitMasks& hm, int subs, int gtile, const Queue& lq) {
     static_assert(PX <= 64 && NT >= 64, "a lane evaluates at most two slots");
     constexpr bool kMasks = PX == 64 && B % 32 == 0;
     constexpr unsigned kOwnMask = WarpShape<PX>::kMask;
@@ -492,7 +508,7 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
     int n_active = __syncthreads_count(active);
     for (int base = rg.x; base < rg.y && n_active > 0; base += B) {
         const int n = min(B, rg.y - base);
-        for (int k = tid; k < n; k += NT) S.sid[k] = __ldg(ids + base + k);
+        for (int k = tid; k < n; k += NT) S.sid[k] = list_id(ids, base + k, lq);
         int slot = 0;
         if (owner) {
             const unsigned bal = __ballot_sync(kOwnMask, active);
@@ -502,7 +518,7 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
         __syncthreads();
         for (int k = tid; k < n * kRecFloat4; k += NT) {
             const int j = k >> 3, c = k & 7;
-            S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
+            S.srec[j][c] = record_part(recs, S.sid[j], c);
         }
         if (active) {
             for (int w = 0; w < warp; ++w) slot += S.warp_base[w];
@@ -589,7 +605,7 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 1024 / NT : 32)) blend_fwd_den
         const int tb = views.tile_base(v);
         const int64_t pb = views.pixel_base(v);
         fwd_dense_item<NT, B>(t - tb, item % q.subs, ids, ranges + tb, recs, jitter + pb, views.camera(v),
-                              out_img + pb, out_dist + 5 * pb, out_nc + pb, S, hm, q.subs, t);
+                              out_img + pb, out_dist + 5 * pb, out_nc + pb, S, hm, q.subs, t, q);
     }
 }
 
@@ -610,7 +626,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) blend_fwd_pair_kernel(
         const int tb = views.tile_base(v);
         const int64_t pb = views.pixel_base(v);
         fwd_pair_item<PX, NT, B>(t - tb, item % q.subs, ids, ranges + tb, recs, jitter + pb, views.camera(v),
-                                 out_img + pb, out_dist + 5 * pb, out_nc + pb, S, hm, q.subs, t);
+                                 out_img + pb, out_dist + 5 * pb, out_nc + pb, S, hm, q.subs, t, q);
     }
 }
 
@@ -833,9 +849,9 @@ __device__ __forceinline__ void flush_entries(int n, const float4 (*srec)[kRecFl
             v[k] = sacc[jj][k];
             any |= v[k] != 0.f;
         }
-        if (!any) continue;
-        const float4* q = srec[jj];
         const int g = sid[jj];
+        if (!any || g < 0) continue;
+        const float4* q = srec[jj];
         const f3 P[4] = {xyz(q[4]), xyz(q[5]), xyz(q[6]), xyz(q[7])};
         const uint32_t flips = __float_as_uint(q[7].w);
         f3 gv[4] = {{v[12], v[13], v[14]}, {v[15], v[16], v[17]}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
@@ -885,7 +901,8 @@ __device__ __forceinline__ void bwd_dense_item(
     const float4* __restrict__ recs, const int4* __restrict__ indices, const float2* __restrict__ jitter,
     const rm_camera& cam, const float4* __restrict__ img, const float* __restrict__ dist,
     const int32_t* __restrict__ ncs, const float4* __restrict__ gimg, const float* __restrict__ gdist,
-    float* __restrict__ gverts, float* __restrict__ gcv, BwdDenseSmem<NT, B>& S, const HitMasks& hm, int subs, int gtile) {
+    float* __restrict__ gverts, float* __restrict__ gcv, BwdDenseSmem<NT, B>& S, const HitMasks& hm, int subs, int gtile,
+    const Queue& lq) {
     constexpr unsigned kMask = WarpShape<NT>::kMask;
     constexpr bool kMasks = NT == 64;
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
@@ -973,12 +990,12 @@ __device__ __forceinline__ void bwd_dense_item(
         }
         __syncthreads();
         const int nk = S.n_keep;
-        for (int k = threadIdx.x; k < nk; k += NT) S.sid[k] = __ldg(ids + lo + S.cidx[k]);
+        for (int k = threadIdx.x; k < nk; k += NT) S.sid[k] = list_id(ids, lo + S.cidx[k], lq);
         for (int k = threadIdx.x; k < nk * kNGrad; k += NT) (&S.sacc[0][0])[k] = 0.f;
         __syncthreads();
         for (int k = threadIdx.x; k < nk * kRecFloat4; k += NT) {
             const int j = k >> 3, c = k & 7;
-            S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
+            S.srec[j][c] = record_part(recs, S.sid[j], c);
         }
         __syncthreads();
         for (int jj = nk - 1; jj >= 0; --jj) {
@@ -1057,7 +1074,7 @@ template <int B>
 __device__ __forceinline__ void bwd_tma_plan(BwdTmaSmem<B>& S, int b, int lo, int top, int rgx,
                                              const int32_t* __restrict__ ids, const float4* __restrict__ recs,
                                              const HitMasks& hm, int gtile, int sub, int subs, uint32_t& hw0,
-                                             uint32_t& hw1) {
+                                             uint32_t& hw1, const Queue& lq) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n = top - lo;
     const int kb0 = (lo - rgx) >> 5, kb1 = (top - 1 - rgx) >> 5;
@@ -1098,16 +1115,24 @@ __device__ __forceinline__ void bwd_tma_plan(BwdTmaSmem<B>& S, int b, int lo, in
     }
     __syncthreads();
     const int nk = S.n_keep[b];
-    for (int k = threadIdx.x; k < nk; k += 64) S.sid[b][k] = __ldg(ids + lo + S.cidx[b][k]);
+    for (int k = threadIdx.x; k < nk; k += 64) S.sid[b][k] = list_id(ids, lo + S.cidx[b][k], lq);
     __syncthreads();
     if (warp == 0) {
         // every read of this buffer (the batch two back) is behind the barriers above
+        int nv = 0;  // entries with a record to copy (the others are zero-filled)
+        for (int k0 = 0; k0 < nk; k0 += 32)
+            nv += __popc(__ballot_sync(0xffffffffu, k0 + lane < nk && S.sid[b][k0 + lane] >= 0));
         fence_proxy_async_smem();
-        if (lane == 0) mbar_arrive_expect_tx(&S.bar[b], (uint32_t)nk * (uint32_t)(kRecFloat4 * sizeof(float4)));
+        if (lane == 0) mbar_arrive_expect_tx(&S.bar[b], (uint32_t)nv * (uint32_t)(kRecFloat4 * sizeof(float4)));
         __syncwarp();
-        for (int k = lane; k < nk; k += 32)
-            bulk_copy_g2s(&S.srec[b][k][0], recs + (int64_t)kRecFloat4 * S.sid[b][k],
-                          (uint32_t)(kRecFloat4 * sizeof(float4)), &S.bar[b]);
+        for (int k = lane; k < nk; k += 32) {
+            const int32_t g = S.sid[b][k];
+            if (g >= 0)
+                bulk_copy_g2s(&S.srec[b][k][0], recs + (int64_t)kRecFloat4 * g,
+                              (uint32_t)(kRecFloat4 * sizeof(float4)), &S.bar[b]);
+            else
+                for (int c = 0; c < kRecFloat4; ++c) S.srec[b][k][c] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
     }
 }
 
@@ -1156,7 +1181,7 @@ __device__ __forceinline__ void bwd_dense_item_tma(
     int ctop = end, clo = rg.x + ((end - 1 - rg.x) / B) * B;
     uint32_t cw0, cw1;
     int cb = (int)pipe.buf;
-    bwd_tma_plan<B>(S, cb, clo, ctop, rg.x, ids, recs, hm, gtile, sub, subs, cw0, cw1);
+    bwd_tma_plan<B>(S, cb, clo, ctop, rg.x, ids, recs, hm, gtile, sub, subs, cw0, cw1, q);
     pipe.buf ^= 1u;
     for (;;) {
         const int ntop = clo;
@@ -1166,7 +1191,7 @@ __device__ __forceinline__ void bwd_dense_item_tma(
         if (has_next) {  // the next batch's copies run while this one is walked
             nlo = rg.x + ((ntop - 1 - rg.x) / B) * B;
             nb = (int)pipe.buf;
-            bwd_tma_plan<B>(S, nb, nlo, ntop, rg.x, ids, recs, hm, gtile, sub, subs, nw0, nw1);
+            bwd_tma_plan<B>(S, nb, nlo, ntop, rg.x, ids, recs, hm, gtile, sub, subs, nw0, nw1, q);
             pipe.buf ^= 1u;
         }
         const int nk = S.n_keep[cb];
@@ -1262,7 +1287,7 @@ __device__ __forceinline__ void bwd_pair_item(
     const float4* __restrict__ recs, const int4* __restrict__ indices, const float2* __restrict__ jitter,
     const rm_camera& cam, const float4* __restrict__ img, const float* __restrict__ dist,
     const int32_t* __restrict__ ncs, const float4* __restrict__ gimg, const float* __restrict__ gdist,
-    float* __restrict__ gverts, float* __restrict__ gcv, BwdPairSmem<PX, B>& S) {
+    float* __restrict__ gverts, float* __restrict__ gcv, BwdPairSmem<PX, B>& S, const Queue& lq) {
     constexpr unsigned kOwnMask = WarpShape<PX>::kMask;
     constexpr int kWarps = NT / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1307,7 +1332,7 @@ __device__ __forceinline__ void bwd_pair_item(
         // pixels with list offsets below n_contributors in this batch
         const bool walking = inside && (lo - rg.x) < nc;
         __syncthreads();  // the previous batch's flush has read sid / srec / sacc
-        for (int k = tid; k < n; k += NT) S.sid[k] = __ldg(ids + lo + k);
+        for (int k = tid; k < n; k += NT) S.sid[k] = list_id(ids, lo + k, lq);
         for (int k = tid; k < n * kNGrad; k += NT) (&S.sacc[0][0])[k] = 0.f;
         int slot = 0;
         if (owner) {
@@ -1318,7 +1343,7 @@ __device__ __forceinline__ void bwd_pair_item(
         __syncthreads();
         for (int k = tid; k < n * kRecFloat4; k += NT) {
             const int j = k >> 3, c = k & 7;
-            S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
+            S.srec[j][c] = record_part(recs, S.sid[j], c);
         }
         int k_act = 0;
 #pragma unroll
@@ -1457,7 +1482,7 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 512 / NT : 16)) blend_bwd_dens
         const int64_t pb = views.pixel_base(v);
         bwd_dense_item<NT, B>(t - tb, item % q.subs, ids, ranges + tb, recs, indices, jitter + pb, views.camera(v),
                               img + pb, dist + 5 * pb, ncs + pb, gimg + pb, gdist ? gdist + 5 * pb : nullptr,
-                              gverts, gcv, S, hm, q.subs, t);
+                              gverts, gcv, S, hm, q.subs, t, q);
     }
 }
 
@@ -1510,7 +1535,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) blend_bwd_pair_kernel(
         const int64_t pb = views.pixel_base(v);
         bwd_pair_item<PX, NT, B>(t - tb, item % q.subs, ids, ranges + tb, recs, indices, jitter + pb,
                                  views.camera(v), img + pb, dist + 5 * pb, ncs + pb, gimg + pb,
-                                 gdist ? gdist + 5 * pb : nullptr, gverts, gcv, S);
+                                 gdist ? gdist + 5 * pb : nullptr, gverts, gcv, S, q);
     }
 }
 
@@ -1542,7 +1567,7 @@ __device__ __forceinline__ void err_item(int tile, int sub, const int32_t* __res
                                          const int2* __restrict__ ranges, const float4* __restrict__ recs,
                                          const rm_camera& cam, const float* __restrict__ pixel_err,
                                          const float* __restrict__ ssim_err, float* __restrict__ tet_err,
-                                         int32_t* __restrict__ tet_count, ErrSmem<B>& S) {
+                                         int32_t* __restrict__ tet_count, ErrSmem<B>& S, const Queue& lq) {
     constexpr unsigned kMask = WarpShape<NT>::kMask;
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
     int lx, ly;
@@ -1564,7 +1589,7 @@ __device__ __forceinline__ void err_item(int tile, int sub, const int32_t* __res
     for (int base = rg.x; base < rg.y && __syncthreads_or(active); base += B) {
         const int n = min(B, rg.y - base);
         for (int k = threadIdx.x; k < n; k += NT) {
-            S.sid[k] = __ldg(ids + base + k);
+            S.sid[k] = list_id(ids, base + k, lq);
             S.scount[k] = 0;
             S.smax[k] = 0;
         }
@@ -1572,7 +1597,7 @@ __device__ __forceinline__ void err_item(int tile, int sub, const int32_t* __res
         __syncthreads();
         for (int k = threadIdx.x; k < n * kRecFloat4; k += NT) {
             const int j = k >> 3, c = k & 7;
-            S.srec[j][c] = __ldg(recs + (int64_t)kRecFloat4 * S.sid[j] + c);
+            S.srec[j][c] = record_part(recs, S.sid[j], c);
         }
         __syncthreads();
         for (int j = 0; j < n; ++j) {
@@ -1627,8 +1652,8 @@ __device__ __forceinline__ void err_item(int tile, int sub, const int32_t* __res
         __syncthreads();
         for (int jj = threadIdx.x; jj < n; jj += NT) {
             const int cnt = S.scount[jj];
-            if (cnt == 0) continue;
             const int64_t g = S.sid[jj];
+            if (cnt == 0 || g < 0) continue;
             float* te = tet_err + 16 * g;
 #pragma unroll
             for (int k = 0; k < kErrVals; ++k)
@@ -1651,7 +1676,7 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 1024 / NT : 32)) err_kernel(
         const int item = next_item(q, &s_item);
         if (item >= n_items) return;
         err_item<NT, B>(queue_tile(q, item), item % q.subs, ids, ranges, recs, cam, pixel_err, ssim_err, tet_err,
-                        tet_count, S);
+                        tet_count, S, q);
     }
 }
 
@@ -1811,12 +1836,14 @@ struct Tuning {
     bool hit_masks;        // RM_BLEND_HIT_MASKS
     bool tma;              // RM_BLEND_STAGE_TMA
     uint32_t* status;      // where a staging wait that gives up is reported
+    int64_t n_recs;        // records the list ids may name
 };
 
 Tuning tuning_from_flags(int flags, int def_shift, int def_ctas) {
     Tuning t;
     t.tma = (flags & RM_BLEND_STAGE_TMA) != 0;
     t.status = nullptr;
+    t.n_recs = 0;
     const int hs = (flags >> RM_BLEND_HEAVY_SHIFT) & 0xf;
     const int pc = (flags >> RM_BLEND_PAIR_CTAS_SHIFT) & 0xf;
     t.heavy_shift = hs ? hs : def_shift;
@@ -1847,8 +1874,10 @@ int launch_fwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, cons
     const int subs = sh.tile_px / PX;
     const int subs_pair = sh.tile_px / PX_PAIR;
     const HitMasks hm = {masks ? w.mask_words : nullptr, w.mask_cap, w.mask_header};
-    const Queue qd = {w.order, w.info, w.tickets + 0, G, subs, false, hm, tn.status, rm_host::wait_limit()};
-    const Queue qp = {w.order, w.info, w.tickets + 1, G, subs_pair, true, hm, tn.status, rm_host::wait_limit()};
+    const Queue qd = {w.order, w.info, w.tickets + 0, G, subs, false, hm, tn.status, rm_host::wait_limit(),
+                      tn.n_recs};
+    const Queue qp = {w.order, w.info, w.tickets + 1, G, subs_pair, true, hm, tn.status, rm_host::wait_limit(),
+                      tn.n_recs};
     auto pair_kernel = blend_fwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, V>;
     const int smem = (int)sizeof(FwdPairSmem<PX_PAIR, B_PAIR>);
     cudaFuncSetAttribute(pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1885,9 +1914,10 @@ int launch_bwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, cons
     const int subs_pair = sh.tile_px / PX_PAIR;
     const bool masks = tn.hit_masks && PX == 64 && w.mask_header;
     const HitMasks hm = {masks ? w.mask_words : nullptr, w.mask_cap, w.mask_header};
-    const Queue qd = {w.order, w.info, w.tickets + 2, G, subs, false, hm, tn.status, rm_host::wait_limit()};
+    const Queue qd = {w.order, w.info, w.tickets + 2, G, subs, false, hm, tn.status, rm_host::wait_limit(),
+                      tn.n_recs};
     const Queue qp = {w.order, w.info, w.tickets + 3, G, subs_pair, true, HitMasks{nullptr, 0, nullptr},
-                      tn.status, rm_host::wait_limit()};
+                      tn.status, rm_host::wait_limit(), tn.n_recs};
     auto pair_kernel = blend_bwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, V>;
     const int smem = (int)sizeof(BwdPairSmem<PX_PAIR, B_PAIR>);
     cudaFuncSetAttribute(pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -2009,6 +2039,7 @@ int blend_fwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
     }
     // measured on the 1.3M-tet workload: every tile through the pair kernel, 4 CTAs/SM
     Tuning tn = tuning_from_flags(flags, 1, 4);
+    tn.n_recs = n_tets;
     if ((rc = pass_status(who, w, status_dev, s, &tn.status))) return rc;
     // tets per shared-memory batch of the pair kernel: 16, 32 (default) or 64
     const int key = strip_pixels(cam0, flags) * 1000 + batch_size(flags, 32);
@@ -2056,6 +2087,7 @@ int blend_bwd_any(const char* who, const int32_t* sorted_ids, const int32_t* ran
     }
     // measured: the one-thread-per-pixel backward alone is fastest
     Tuning tn = tuning_from_flags(flags, 15, 1);
+    tn.n_recs = n_tets;
     if ((rc = pass_status(who, w, status_dev, s, &tn.status))) return rc;
     // tets per shared-memory batch of the dense kernel: 16, 32 or 64 (default)
     const int key = strip_pixels(cam0, flags) * 1000 + batch_size(flags, 64);
@@ -2117,7 +2149,8 @@ int rm_calc_tet_err(const int32_t* sorted_ids, const int32_t* ranges, const int3
     if ((rc = launch_order(ranges, (int)G, w, 1, s))) return rc;
     const int strip = strip_pixels(cam, flags);
     const int subs = cam->tile_width * cam->tile_height / strip;
-    const Queue qd = {w.order, w.info, w.tickets + 0, (int)G, subs, true, HitMasks{nullptr, 0, nullptr}};
+    const Queue qd = {w.order, w.info, w.tickets + 0, (int)G, subs, true, HitMasks{nullptr, 0, nullptr}, nullptr,
+                      rm_host::wait_limit(), n_tets};
     if (strip == 16) {
         const int grid = persistent_grid(err_kernel<16, 32>, 16, 0, (int)G * subs);
         err_kernel<16, 32><<<grid, 16, 0, s>>>(sorted_ids, (const int2*)ranges, w.recs, *cam, pixel_err, ssim_err,

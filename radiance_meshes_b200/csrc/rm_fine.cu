@@ -123,7 +123,12 @@ __global__ void __launch_bounds__(256) fine_bits_kernel(
         if (in) {
             t = (int)((uint64_t)__ldg((const unsigned long long*)keys + e) >> 32);
             int32_t g = __ldg(ids + e);
-            if (PACKED) {
+            // only lists left invalid by a sort that gave up hold a tile or
+            // tet outside the frame: such an entry reaches no fine tile
+            if (t < 0 || t >= views.tiles[views.n] || (!PACKED && (g < 0 || (int64_t)g >= n_tets))) t = -1;
+            if (t < 0) {
+                if (!PACKED) bits_out[e] = 0;  // the write pass reads it by the coarse ranges
+            } else if (PACKED) {
                 bits = (uint32_t)g >> 28;
             } else {
                 const int v = views.find(t);
@@ -217,7 +222,7 @@ __global__ void __launch_bounds__(kFineThreads, 2) fine_write_kernel(
             const unsigned bal = __ballot_sync(0xffffffffu, hit);
             if (hit) {
                 const int64_t o = (int64_t)start[q] + wpre[warp][q] + __popc(bal & lt);
-                if (o < capacity) fine_ids[o] = g;
+                if (o >= 0 && o < capacity) fine_ids[o] = g;  // o < 0 only after a scan that gave up
                 else if (status) atomicOr(status, RM_STATUS_CAPACITY);
             }
         }
@@ -225,7 +230,10 @@ __global__ void __launch_bounds__(kFineThreads, 2) fine_write_kernel(
     __syncthreads();
     if (threadIdx.x < Q) {
         const int q = threadIdx.x;
-        fine_ranges[fine_tile_id<FS>(views, t, q)] = make_int2(start[q], start[q] + (int)run[q]);
+        // ranges past the capacity (RM_STATUS_CAPACITY) are cut to what was written
+        const int64_t a = max((int64_t)0, min((int64_t)start[q], capacity));
+        const int64_t b = max(a, min((int64_t)start[q] + run[q], capacity));
+        fine_ranges[fine_tile_id<FS>(views, t, q)] = make_int2((int)a, (int)b);
     }
 }
 

@@ -49,9 +49,13 @@ enum ScanMode { kScanValues = 0, kScanPositive = 1, kScanGather = 2 };
 
 template <int MODE>
 __device__ __forceinline__ int32_t scan_item(const int32_t* __restrict__ in, const int32_t* __restrict__ order,
-                                             int64_t i, int64_t n_eff) {
+                                             int64_t i, int64_t n_eff, int64_t n) {
     if (i >= n_eff) return 0;
-    if (MODE == kScanGather) return __ldg(in + __ldg(order + i));
+    if (MODE == kScanGather) {
+        // an order left invalid by a sort that gave up may hold any value
+        const int32_t g = __ldg(order + i);
+        return (g >= 0 && (int64_t)g < n) ? __ldg(in + g) : 0;
+    }
     const int32_t v = __ldg(in + i);
     return MODE == kScanPositive ? (v > 0 ? 1 : 0) : v;
 }
@@ -87,7 +91,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const int32_t* __res
             for (int k = 0; k < kScanItems; ++k) v[k] = v[k] > 0 ? 1 : 0;
     } else {
 #pragma unroll
-        for (int k = 0; k < kScanItems; ++k) v[k] = scan_item<MODE>(in, order, base + k, n_eff);
+        for (int k = 0; k < kScanItems; ++k) v[k] = scan_item<MODE>(in, order, base + k, n_eff, n);
     }
     int64_t sum = 0;
 #pragma unroll
@@ -222,7 +226,7 @@ __global__ void __launch_bounds__(kEmitThreads) emit_kernel(const float* __restr
         const int64_t excl = g == 0 ? 0 : (int64_t)__ldg(offsets + g - 1);
         const int32_t k = (int32_t)(p - excl);
         const int4 r = __ldg(rect + g);
-        const int32_t w = r.z - r.x;
+        const int32_t w = max(r.z - r.x, 1);  // >= 1 for every tet with pairs
         const int32_t y = r.y + k / w, x = r.x + k % w;
         const uint64_t fk = sortable_key(__ldg(vs + 3 * g + 2));
         keys[p] = (int64_t)(((uint64_t)(uint32_t)(y * grid_w + x) << 32) | fk);
@@ -268,7 +272,7 @@ __global__ void __launch_bounds__(kEmitThreads) emit_multi_kernel(
         const int64_t g = i - (int64_t)v * n_tets;
         const rm_camera& c = views.cams[v];
         const int4 r = __ldg(rect + i);
-        const int32_t w = r.z - r.x;
+        const int32_t w = max(r.z - r.x, 1);
         const int32_t y = r.y + k / w, x = r.x + k % w;
         const uint64_t fk = sortable_key(__ldg(depth + i));
         // with footprint: bits 28..31 of the value say which of the tile's 2x2
@@ -299,6 +303,7 @@ __global__ void __launch_bounds__(256) depth_scatter_kernel(const int32_t* __res
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_tets || __ldg(tiles + g) <= 0) return;
     const int64_t pos = (int64_t)__ldg(incl + g) - 1;
+    if (pos < 0 || pos >= n_tets) return;  // only a count scan that gave up leaves such positions
     keys[pos] = (int64_t)sortable_key(__ldg(vs + 3 * g + 2));
     vals[pos] = (int32_t)g;
 }
@@ -337,8 +342,13 @@ __global__ void __launch_bounds__(kEmitThreads) emit_ordered_kernel(
         const int64_t excl = si == 0 ? 0 : (int64_t)__ldg(offsets + si - 1);
         const int32_t k = (int32_t)(p - excl);
         const int64_t g = __ldg(order + si);
+        if (g < 0 || g >= n_cap) {  // an order left invalid by a sort that gave up: a key past every tile
+            keys[p] = -1;
+            vals[p] = 0;
+            continue;
+        }
         const int4 r = __ldg(rect + g);
-        const int32_t w = r.z - r.x;
+        const int32_t w = max(r.z - r.x, 1);  // >= 1 for every tet with pairs
         const int32_t y = r.y + k / w, x = r.x + k % w;
         const uint64_t fk = sortable_key(__ldg(vs + 3 * g + 2));
         keys[p] = (int64_t)(((uint64_t)(uint32_t)(y * grid_w + x) << 32) | fk);

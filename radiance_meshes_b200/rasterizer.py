@@ -394,6 +394,11 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
         if depth_first:  # the ordered scan gives the count; nothing is emitted at capacity 0
             pairs(0, total)
         P, bits = _read_frame(total, status)
+    if out is None and bits & C.RM_STATUS_CAPACITY:
+        # expected: the buffers were sized before P was known; rebuilt at exactly P below
+        bits &= ~C.RM_STATUS_CAPACITY
+        if not bits:
+            status.zero_()
     raise_status(bits, status, "vertex_and_tile_shader")
     if out is None:
         out = pairs(P, None if not depth_first else total)

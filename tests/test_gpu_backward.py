@@ -7,13 +7,13 @@ colour gradient), with the relative L2 error ||g_gpu - g_ref|| / ||g_ref||:
   * the adjoint evaluated in FP32 with the reference's rounding (the
     reference's own backward, restated): <= 1e-4, and every entry within
     1e-3 |g_ref| + 1e-4 max|g_ref|;
-  * the adjoint evaluated in FP64 (the exact reference): <= 1e-3, the stated gradient
-    tolerance, after removing the 0.1% of entries with the largest deviation
-    (<= 5e-3 without trimming).  Rays are jittered randomly; near-tangent
-    hits still occur, where d(segment length)/d(vertex) is unbounded.  At pixel
+  * the adjoint evaluated in FP64 (the exact reference): <= 1e-3, the stated
+    gradient tolerance, over every entry (the FP32 restatement itself is within
+    6.2e-5 of FP64 on these cases).  Rays are jittered randomly.  At pixel
     centres a ray can graze a tet edge, where the segment length is not
     differentiable and FP32 and FP64 resolve the kink differently (for the
-    reference algorithm in FP32 as much as for this kernel).  Distortion
+    reference algorithm in FP32 as much as for this kernel), so that case is
+    compared with the FP32 restatement only.  Distortion
     gradients are compared with the FP32 restatement only: the reference's
     distortion moments add the full density of every hit tet, however short
     the segment (moment_0_int returns the density,
@@ -39,7 +39,7 @@ def _groups(gv, gc):
     return {"vertices": gv.ravel(), "density": gc[:, 0], "rgb": gc[:, 1:4].ravel(), "grd": gc[:, 4:7].ravel()}
 
 
-def _compare(gpu, ref, rel_tol, entry_rtol=None, entry_atol=None, what="", trim=0.0, untrimmed_tol=None):
+def _compare(gpu, ref, rel_tol, entry_rtol=None, entry_atol=None, what=""):
     out = {}
     for k in ref:
         a, b = gpu[k].astype(np.float64), ref[k]
@@ -48,14 +48,6 @@ def _compare(gpu, ref, rel_tol, entry_rtol=None, entry_atol=None, what="", trim=
             assert np.abs(a).max() == 0, k
             continue
         rel = np.linalg.norm(a - b) / nb
-        if trim > 0:
-            d = np.abs(a - b)
-            keep = d <= np.quantile(d, 1.0 - trim)
-            rel_t = np.linalg.norm((a - b)[keep]) / np.linalg.norm(b[keep])
-            out[k] = (rel_t, rel)
-            assert rel_t <= rel_tol, f"{what} {k}: trimmed relative L2 error {rel_t:.3e} (untrimmed {rel:.3e})"
-            assert rel <= untrimmed_tol, f"{what} {k}: relative L2 error {rel:.3e}"
-            continue
         out[k] = rel
         assert rel <= rel_tol, f"{what} {k}: relative L2 error {rel:.3e}"
         if entry_rtol is not None:
@@ -97,7 +89,7 @@ def _run(verts, idx, cv, tcam, jitter, loss, seed=0, check_f64=True, hit_masks=F
         img64, dist64, _, _, _ = O.blend_fwd_f64(lists, idx, v64, c64, jitter, cut=nc)
         rgv, rgc = O.blend_bwd(lists, idx, v64, c64, jitter, img64, dist64, nc, gimg.astype(np.float64),
                                gdist.astype(np.float64), "f64")
-        out["f64"] = _compare(gpu, _groups(rgv, rgc), GRAD_TOL, what="vs fp64", trim=1e-3, untrimmed_tol=5e-3)
+        out["f64"] = _compare(gpu, _groups(rgv, rgc), GRAD_TOL, what="vs fp64")
     return out
 
 

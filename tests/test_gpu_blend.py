@@ -4,9 +4,11 @@ Integer outputs (n_contributors), the log-transmittance channel and the five
 distortion moments involve no transcendental functions and are bit-exact to
 the FP32 restatement of the reference; the colour channels go through
 exp/expm1, whose last bits differ between CUDA and libm, and must agree within
-1e-4 max-abs (the stated image tolerance).  Against the FP64 integrator (same per-pixel list cut) the error
-is that of the reference algorithm in FP32 and is checked at the 99.9th
-percentile (1e-4) and at the maximum (2e-3).
+1e-4 max-abs (the stated image tolerance).  Against the FP64 integrator (same
+per-pixel list cut) every pixel is within 1e-4 unless the FP32 restatement of
+the reference is itself off by more than 1e-4 there (the reference algorithm's
+own FP32 error: on the 4,096-point workload one pixel in 65,536, whose ray runs
+within 0.14 degrees of a face plane), and no pixel is off by more than 5e-4.
 """
 import numpy as np
 import pytest
@@ -29,10 +31,14 @@ def _check(r, img32, dist32, nc, img64=None):
     assert np.abs(img[..., :3] - img32[..., :3]).max() <= IMG_TOL
     assert np.array_equal(bits(dist), bits(dist32)), "distortion moments not bit-exact"
     if img64 is not None:
-        T_gpu, T64 = np.exp(img[..., 3]), np.exp(img64[..., 3])
-        err = np.concatenate([np.abs(img[..., :3] - img64[..., :3]).ravel(), np.abs(T_gpu - T64).ravel()])
-        assert np.quantile(err, 0.999) <= IMG_TOL
-        assert err.max() <= 2e-3
+        def pixel_err(x):
+            ec = np.abs(x[..., :3] - img64[..., :3]).max(-1)
+            return np.maximum(ec, np.abs(np.exp(x[..., 3]) - np.exp(img64[..., 3])))
+
+        err, err32 = pixel_err(img), pixel_err(img32)
+        own = (err > IMG_TOL) & ~(err32 > IMG_TOL)
+        assert not own.any(), f"{own.sum()} pixels beyond {IMG_TOL} of FP64 where the FP32 restatement is within it"
+        assert err.max() <= 5e-4, f"max error against FP64 {err.max():.3e}"
 
 
 @pytest.mark.parametrize("name", G.names())
