@@ -405,7 +405,10 @@ RM_API int rm_jitter_bounds(const float* ray_jitter, int64_t n_pixels, float* bo
  * 256-byte aligned.  The split's own scan look-back and a fine list longer
  * than capacity set RM_STATUS_SCAN_TIMEOUT / RM_STATUS_CAPACITY in
  * *status_dev (status_dev may be NULL: the bits then stay in the workspace).
- * No reference counterpart.
+ * Fine ranges are cut to capacity.  The sorted ids index the footprint
+ * rows, so they must come from a list build whose status word was read
+ * clean (rm_fine_lists_multi, which knows the tet count, skips ids outside
+ * it).  No reference counterpart.
  */
 RM_API size_t rm_fine_lists_workspace_size(int64_t n_fine_tiles, int64_t n_pairs, int fine_shift);
 RM_API int rm_fine_lists(const int64_t* sorted_keys, const int32_t* sorted_ids, int64_t n_pairs,

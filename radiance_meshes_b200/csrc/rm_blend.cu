@@ -731,6 +731,37 @@ struct ReduceScatter<M, 0> {
     static __device__ __forceinline__ void run(float*, int, int&) {}
 };
 
+// Warp sum of the 25 per-lane partials of one entry, through shared memory,
+// added to the entry's accumulator acc[0..25).  Each lane stores its row as
+// seven float4 (row stride 28 floats: the eight lanes of each store phase
+// hit distinct banks); then lane k < 25 adds column k over the 32 rows
+// (consecutive lanes read consecutive words).  Fewer instructions than the
+// 27-shuffle reduce-scatter for full warps.  red: 32 * kRedStride floats,
+// 16-byte aligned, private to the warp.
+constexpr int kRedStride = 28;
+
+__device__ __forceinline__ void warp_sum_rows(float* __restrict__ red, const float* gl, int lane,
+                                              float* __restrict__ acc) {
+    float4* row = reinterpret_cast<float4*>(red + lane * kRedStride);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) row[c] = make_float4(gl[4 * c], gl[4 * c + 1], gl[4 * c + 2], gl[4 * c + 3]);
+    row[6] = make_float4(gl[24], 0.f, 0.f, 0.f);
+    __syncwarp();
+    if (lane < kNGrad) {
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+        for (int r = 0; r < 32; r += 4) {
+            s0 += red[(r + 0) * kRedStride + lane];
+            s1 += red[(r + 1) * kRedStride + lane];
+            s2 += red[(r + 2) * kRedStride + lane];
+            s3 += red[(r + 3) * kRedStride + lane];
+        }
+        const float sum = (s0 + s1) + (s2 + s3);
+        if (sum != 0.f) atomicAdd(acc + lane, sum);
+    }
+    __syncwarp();
+}
+
 // Adjoint of one hit (the Slang autodiff of update_alpha_out,
 // evaluate_tetra_interp and load_tet_alphablend_interp, written out by hand).
 // Inputs: the entry's intersection and segment, T = exp(log T) and D2, D3 of
@@ -887,6 +918,7 @@ __device__ __forceinline__ void flush_entries(int n, const float4 (*srec)[kRecFl
 template <int NT, int B>
 struct BwdDenseSmem {
     float4 srec[B][kRecFloat4];
+    float4 red[NT >= 32 ? NT / 32 : 1][NT >= 32 ? 32 * kRedStride / 4 : 1];  // warp_sum_rows rows, per warp
     int32_t sid[B];
     float sacc[B][kNGrad];
     int32_t smax[WarpShape<NT>::kWarps];
@@ -1030,12 +1062,16 @@ __device__ __forceinline__ void bwd_dense_item(
                 dS_D[3] = nD3;
             }
             if (__any_sync(kMask, hit)) {
-                using RS = ReduceScatter<kNGrad, WarpShape<NT>::kTopOffset>;
-                int slot = 0;
-                RS::template run<kMask>(gl, lane, slot);
+                if constexpr (NT >= 32) {
+                    warp_sum_rows(reinterpret_cast<float*>(S.red[warp]), gl, lane, S.sacc[jj]);
+                } else {
+                    using RS = ReduceScatter<kNGrad, WarpShape<NT>::kTopOffset>;
+                    int slot = 0;
+                    RS::template run<kMask>(gl, lane, slot);
 #pragma unroll
-                for (int r = 0; r < RS::R; ++r)
-                    if (slot + r < kNGrad && gl[r] != 0.f) atomicAdd(&S.sacc[jj][slot + r], gl[r]);
+                    for (int r = 0; r < RS::R; ++r)
+                        if (slot + r < kNGrad && gl[r] != 0.f) atomicAdd(&S.sacc[jj][slot + r], gl[r]);
+                }
             }
         }
         __syncthreads();
@@ -1054,6 +1090,7 @@ __device__ __forceinline__ void bwd_dense_item(
 template <int B>
 struct BwdTmaSmem {
     float4 srec[2][B][kRecFloat4];
+    float4 red[2][32 * kRedStride / 4];  // warp_sum_rows rows, per warp
     float sacc[B][kNGrad];
     int32_t sid[2][B];
     uint8_t cidx[2][B];
@@ -1232,14 +1269,7 @@ __device__ __forceinline__ void bwd_dense_item_tma(
                 dS_D[2] = nD2;
                 dS_D[3] = nD3;
             }
-            if (__any_sync(0xffffffffu, hit)) {
-                using RS = ReduceScatter<kNGrad, 16>;
-                int slot = 0;
-                RS::template run<0xffffffffu>(gl, lane, slot);
-#pragma unroll
-                for (int r = 0; r < RS::R; ++r)
-                    if (slot + r < kNGrad && gl[r] != 0.f) atomicAdd(&S.sacc[jj][slot + r], gl[r]);
-            }
+            if (__any_sync(0xffffffffu, hit)) warp_sum_rows(reinterpret_cast<float*>(S.red[warp]), gl, lane, S.sacc[jj]);
         }
         __syncthreads();
         flush_entries<NT, B>(nk, S.srec[cb], S.sid[cb], S.sacc, indices, gverts, gcv);

@@ -124,8 +124,12 @@ __global__ void __launch_bounds__(256) fine_bits_kernel(
             t = (int)((uint64_t)__ldg((const unsigned long long*)keys + e) >> 32);
             int32_t g = __ldg(ids + e);
             // only lists left invalid by a sort that gave up hold a tile or
-            // tet outside the frame: such an entry reaches no fine tile
-            if (t < 0 || t >= views.tiles[views.n] || (!PACKED && (g < 0 || (int64_t)g >= n_tets))) t = -1;
+            // tet outside the frame: such an entry reaches no fine tile.  The
+            // tet id is checked when the tet count is known (n_tets > 0:
+            // stacked views); the single-view split runs on lists whose
+            // frame status the caller has read.
+            if (t < 0 || t >= views.tiles[views.n] || (!PACKED && (g < 0 || (n_tets > 0 && (int64_t)g >= n_tets))))
+                t = -1;
             if (t < 0) {
                 if (!PACKED) bits_out[e] = 0;  // the write pass reads it by the coarse ranges
             } else if (PACKED) {
