@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--stage", choices=["ldg", "tma"], default="ldg",
                     help="how the backward stages tet records in shared memory: per-thread loads, or bulk copies "
                          "(cp.async.bulk, two batches in flight); bulk copies only in single-GPU runs")
+    ap.add_argument("--pair-ctas", type=int, default=0,
+                    help="resident CTAs per SM of the forward's pair kernel (0: the library default)")
     ap.add_argument("--profile-steps", type=int, default=0, help="(profiling) run N steps after warmup, print nothing")
     ap.add_argument("--workload", choices=["training", "multiview", "serving"], default="training",
                     help="training: the 1.3M-tet fwd+bwd step (default line); multiview: 16 views of a "
@@ -99,19 +101,20 @@ class ClockSampler:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, interval_ms=25):
         vis = os.environ.get("CUDA_VISIBLE_DEVICES")
         if vis:
             ids = [x.strip() for x in vis.split(",") if x.strip()]
             index = ids[index] if index < len(ids) else index
         self.index = index
+        self.interval_ms = int(interval_ms)
         self.proc = None
         self.lines = []
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.index), "-lms", "200"], stdout=subprocess.PIPE,
+                                          "-i", str(self.index), "-lms", str(self.interval_ms)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -122,13 +125,15 @@ class ClockSampler:
         t0 = time.time()
         while self.proc is not None and not self.lines and self.proc.poll() is None and time.time() - t0 < 15:
             time.sleep(0.02)
+        self.t_start = time.time()  # the timed region runs inside the with block
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def __exit__(self, *exc):
+        self.t_end = time.time()
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -139,7 +144,9 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0, t1 = getattr(self, "t_start", 0.0), getattr(self, "t_end", float("inf"))
+        inside = [ln for t, ln in self.lines if t0 <= t <= t1]
+        for ln in inside:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -153,32 +160,48 @@ class ClockSampler:
                     reasons.add(k)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "interval_ms": self.interval_ms}
 
 
 def issue_roofline(kernel, launch_ms, tests, clocks, **extra):
     """The blend kernels are bound by instruction issue, not HBM: the
-    kernel's warp instructions per launch (ray/tet tests of this pass x the
-    instructions per test of the profiled capture, profiles/issue_model.json)
-    over its measured launch time, against the SM's issue peak (148 SMs x 4
-    schedulers x the sampled SM clock)."""
+    kernel's warp instructions per launch over its measured launch time,
+    against the SM's issue peak (148 SMs x 4 schedulers x the sampled SM
+    clock).  The instruction count is smsp__inst_executed.sum of one launch
+    on this workload (profiles/issue_1.3Mtets.json, an ncu capture of the
+    same code; scaled by this pass's ray/tet tests over the capture's), else
+    the tests of this pass x the instructions per test of a smaller capture
+    (profiles/issue_model.json)."""
     out = {"ray_tet_tests_per_pass": tests, **extra}
-    path = os.path.join(ROOT, "profiles", "issue_model.json")
-    if not os.path.exists(path):
-        return out
-    with open(path) as f:
-        model = json.load(f).get(kernel)
-    if not model or not launch_ms:
+    if not launch_ms:
         return out
     import torch
 
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
-    warp_inst = tests * model["thread_instructions_per_test"] / model["active_lanes_per_instruction"]
+    warp_inst, src = None, None
+    path = os.path.join(ROOT, "profiles", "issue_1.3Mtets.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            cap = json.load(f).get(kernel)
+        if cap and cap.get("ray_tet_tests_per_pass"):
+            warp_inst = cap["warp_instructions_per_launch"] * tests / cap["ray_tet_tests_per_pass"]
+            src = "profiles/issue_1.3Mtets.json (smsp__inst_executed.sum of one launch on this workload)"
+    if warp_inst is None:
+        path = os.path.join(ROOT, "profiles", "issue_model.json")
+        if not os.path.exists(path):
+            return out
+        with open(path) as f:
+            model = json.load(f).get(kernel)
+        if not model:
+            return out
+        warp_inst = tests * model["thread_instructions_per_test"] / model["active_lanes_per_instruction"]
+        src = "profiles/issue_model.json (instructions per test of the 50k-point capture)"
     achieved = warp_inst / (launch_ms * 1e-3) / 1e9
     peak = sms * 4 * mhz * 1e6 / 1e9
     out.update({"bound": "issue", "unit": "G warp instructions/s", "achieved": achieved, "peak": peak,
-                "frac": achieved / peak, "instructions_per_test_source": "profiles/issue_model.json"})
+                "frac": achieved / peak, "warp_instructions_per_launch": warp_inst, "instructions_source": src})
     return out
 
 
@@ -242,6 +265,8 @@ def run_b200(args):
     camst = R.camera(tcam)
     grid = RenderGrid(H, W, tile_width=args.tile, tile_height=args.tile)
     R.use_tma_staging(args.stage == "tma" and world == 1)
+    if args.pair_ctas:
+        R.set_blend_tuning(args.pair_ctas << _capi.RM_BLEND_PAIR_CTAS_SHIFT, R.blend_tuning()[1])
     rng = np.random.default_rng(1000 + rank)
     target_h = torch.from_numpy(rng.uniform(size=(H, W, 3)).astype(np.float32)).pin_memory()
     # The model's raw per-tet outputs (density, base colour, colour gradient),
@@ -474,7 +499,8 @@ def run_b200(args):
                    else "caller's tiles", "parallelism": f"dp{world} (views)" if world > 1
                    else "single view", "l2": "flushed between steps (256 MiB write)",
                    "seed": 2, "jitter": "torch.rand per step (train.py:244)",
-                   "record_staging": "bulk copies (cp.async.bulk)" if R.tma_staging() else "per-thread loads"},
+                   "record_staging": "bulk copies (cp.async.bulk)" if R.tma_staging() else "per-thread loads",
+                   "pair_ctas_per_sm": args.pair_ctas or "library default"},
         "value_jitter_0_5": {"value": value_const, "ms_per_step": total_ms_const / args.steps,
                              "jitter": "constant 0.5 (render() default)"},
         "e2e": e2e, "roofline": roof, "stages_ms": per_stage, "stages_pass_steps": n_break,
@@ -673,7 +699,7 @@ def run_multiview(args, prebuilt=None):
     torch.cuda.synchronize()
     launches0 = _capi.launch_count()
     ev = []
-    with ClockSampler(local) as clocks:
+    with ClockSampler(local, interval_ms=50) as clocks:
         for _ in range(args.steps):
             flush.zero_()
             a = torch.cuda.Event(enable_timing=True)
@@ -826,7 +852,7 @@ def run_serving(args, prebuilt=None):
     reqs = [S.RenderRequest(k, name, tcam_to_struct(v.tcam(tile_size=tile)), t)
             for k, (t, name, v) in enumerate(trace)]
     launches0 = _capi.launch_count()
-    with ClockSampler(local) as clocks:
+    with ClockSampler(local, interval_ms=200) as clocks:  # a seconds-long trace: sparse sampling
         results = server.run_trace(reqs, realtime=True)
     launches = _capi.launch_count() - launches0
     low = None

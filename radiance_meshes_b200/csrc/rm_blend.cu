@@ -461,7 +461,7 @@ __device__ __forceinline__ void fwd_dense_item(int tile, int sub, const int32_t*
 template <int PX, int B>
 struct FwdPairSmem {
     float4 srec[B][kRecFloat4];
-    int32_t sid[B];
+    float dens[2][B];      // densities of the batch being folded and of the one being staged
     float ray[6][PX];      // o, d of each slot (structure of arrays)
     float res[6][B][PX];   // a (0: miss), m1, d4, r, g, b per (entry, slot)
     int32_t warp_base[(PX + 31) / 32];
@@ -477,6 +477,21 @@ __device__ __forceinline__ void store_result(FwdPairSmem<PX, B>& S, int j, int s
     S.res[5][j][sl] = r.rgb[2];
 }
 
+// Stages batch [base, base + n) into srec (and its densities into dens[buf])
+// with threads t, t + nt, ...: one float4 of one record each, the thread
+// loading the entry's id itself.
+template <int PX, int B>
+__device__ __forceinline__ void stage_pair_batch(FwdPairSmem<PX, B>& S, int buf, int base, int n,
+                                                 const int32_t* __restrict__ ids, const float4* __restrict__ recs,
+                                                 const Queue& lq, int t, int nt) {
+    for (int k = t; k < n * kRecFloat4; k += nt) {
+        const int j = k >> 3, c = k & 7;
+        const float4 r = record_part(recs, list_id(ids, base + j, lq), c);
+        S.srec[j][c] = r;
+        if (c == 0) S.dens[buf][j] = r.w;
+    }
+}
+
 template <int PX, int NT, int B>
 __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* __restrict__ ids,
                                          const int2* __restrict__ ranges, const float4* __restrict__ recs,
@@ -488,6 +503,8 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
     constexpr bool kMasks = PX == 64 && B % 32 == 0;
     constexpr unsigned kOwnMask = WarpShape<PX>::kMask;
     constexpr int kWarps = NT / 32;
+    constexpr int kOwnThreads = (PX + 31) / 32 * 32;  // the owners' warps; the rest stage during the fold
+    static_assert(NT > kOwnThreads, "staging needs warps besides the owners'");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool owner = tid < PX;
     const int tx = tile % cam.grid_width, ty = tile / cam.grid_width;
@@ -505,21 +522,21 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
     PixelState st = {{0.f, 0.f, 0.f}, 0.f, {0.f, 0.f, 0.f, 0.f, 0.f}};
     int32_t nc = 0;
     bool active = inside;
+    // The first batch is staged by all threads; each later one by the
+    // non-owner warps while the owners fold the batch before it (srec is no
+    // longer read by then: the fold reads the densities kept in dens[cur]).
+    stage_pair_batch(S, 0, rg.x, min(B, rg.y - rg.x), ids, recs, lq, tid, NT);
+    int rank = 0;  // the owner's rank among the active pixels of its warp
+    if (owner) {
+        const unsigned bal = __ballot_sync(kOwnMask, active);
+        if (lane == 0) S.warp_base[warp] = __popc(bal);
+        rank = __popc(bal & ((1u << lane) - 1u));
+    }
     int n_active = __syncthreads_count(active);
+    int cur = 0;
     for (int base = rg.x; base < rg.y && n_active > 0; base += B) {
         const int n = min(B, rg.y - base);
-        for (int k = tid; k < n; k += NT) S.sid[k] = list_id(ids, base + k, lq);
-        int slot = 0;
-        if (owner) {
-            const unsigned bal = __ballot_sync(kOwnMask, active);
-            if (lane == 0) S.warp_base[warp] = __popc(bal);
-            slot = __popc(bal & ((1u << lane) - 1u));
-        }
-        __syncthreads();
-        for (int k = tid; k < n * kRecFloat4; k += NT) {
-            const int j = k >> 3, c = k & 7;
-            S.srec[j][c] = record_part(recs, S.sid[j], c);
-        }
+        int slot = rank;
         if (active) {
             for (int w = 0; w < warp; ++w) slot += S.warp_base[w];
             S.ray[0][slot] = o.x; S.ray[1][slot] = o.y; S.ray[2][slot] = o.z;
@@ -558,26 +575,39 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
                 if (has) store_result(S, j, sl, eval_entry(S.srec[j], o, d));
         }
         __syncthreads();
-        // Fold in list order; the hit tests of four entries are read ahead.
-        uint64_t hb = 0;  // bit j: entry j of the batch was a hit for this owner's pixel
-        for (int j0 = 0; active && j0 < n; j0 += 4) {
-            float a4[4];
+        if (tid >= kOwnThreads) {
+            if (base + B < rg.y)
+                stage_pair_batch(S, cur ^ 1, base + B, min(B, rg.y - base - B), ids, recs, lq, tid - kOwnThreads,
+                                 NT - kOwnThreads);
+        } else {
+            // Fold in list order; the hit tests of four entries are read ahead.
+            uint64_t hb = 0;  // bit j: entry j of the batch was a hit for this owner's pixel
+            for (int j0 = 0; active && j0 < n; j0 += 4) {
+                float a4[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) a4[u] = j0 + u < n ? S.res[0][j0 + u][slot] : 0.f;
+                for (int u = 0; u < 4; ++u) a4[u] = j0 + u < n ? S.res[0][j0 + u][slot] : 0.f;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int j = j0 + u;
-                if (!active || j >= n) break;
-                ++nc;
-                if (a4[u] > 0.f) {
-                    hb |= 1ull << j;
-                    const float rgb[3] = {S.res[3][j][slot], S.res[4][j][slot], S.res[5][j][slot]};
-                    fold_hit(st, a4[u], S.srec[j][0].w, S.res[1][j][slot], S.res[2][j][slot], rgb);
-                    if (st.logT < kTermLogT) active = false;
+                for (int u = 0; u < 4; ++u) {
+                    const int j = j0 + u;
+                    if (!active || j >= n) break;
+                    ++nc;
+                    if (a4[u] > 0.f) {
+                        hb |= 1ull << j;
+                        const float rgb[3] = {S.res[3][j][slot], S.res[4][j][slot], S.res[5][j][slot]};
+                        fold_hit(st, a4[u], S.dens[cur][j], S.res[1][j][slot], S.res[2][j][slot], rgb);
+                        if (st.logT < kTermLogT) active = false;
+                    }
                 }
             }
+            if (kMasks && owner && hm.words) write_masks(hm, hb, gtile, rg.x, base, n, sub, subs, tid);
+            // the next batch's slots: the pixels still active
+            if (owner) {
+                const unsigned bal = __ballot_sync(kOwnMask, active);
+                if (lane == 0) S.warp_base[warp] = __popc(bal);
+                rank = __popc(bal & ((1u << lane) - 1u));
+            }
         }
-        if (kMasks && owner && hm.words) write_masks(hm, hb, gtile, rg.x, base, n, sub, subs, tid);
+        cur ^= 1;
         n_active = __syncthreads_count(active);
     }
     if (inside) {
@@ -609,8 +639,10 @@ __global__ void __launch_bounds__(NT, (NT >= 64 ? 1024 / NT : 32)) blend_fwd_den
     }
 }
 
-template <int PX, int NT, int B, class V>
-__global__ void __launch_bounds__(NT, 1024 / NT) blend_fwd_pair_kernel(
+// MINB resident CTAs per SM: 1024 / NT caps registers at 64 (some spill),
+// 768 / NT at 80 (none spill) for launches asking fewer CTAs per SM.
+template <int PX, int NT, int B, int MINB, class V>
+__global__ void __launch_bounds__(NT, MINB) blend_fwd_pair_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
     const float2* __restrict__ jitter, const __grid_constant__ V views, float4* __restrict__ out_img,
     float* __restrict__ out_dist, int32_t* __restrict__ out_nc, const Queue q) {
@@ -740,12 +772,7 @@ struct ReduceScatter<M, 0> {
 // 16-byte aligned, private to the warp.
 constexpr int kRedStride = 28;
 
-__device__ __forceinline__ void warp_sum_rows(float* __restrict__ red, const float* gl, int lane,
-                                              float* __restrict__ acc) {
-    float4* row = reinterpret_cast<float4*>(red + lane * kRedStride);
-#pragma unroll
-    for (int c = 0; c < 6; ++c) row[c] = make_float4(gl[4 * c], gl[4 * c + 1], gl[4 * c + 2], gl[4 * c + 3]);
-    row[6] = make_float4(gl[24], 0.f, 0.f, 0.f);
+__device__ __forceinline__ void warp_sum_columns(const float* red, int lane, float* __restrict__ acc) {
     __syncwarp();
     if (lane < kNGrad) {
         float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
@@ -762,6 +789,43 @@ __device__ __forceinline__ void warp_sum_rows(float* __restrict__ red, const flo
     __syncwarp();
 }
 
+// Rows of gl[0..25) as computed by hit_grads_a.
+__device__ __forceinline__ void warp_sum_rows(float* __restrict__ red, const float* gl, int lane,
+                                              float* __restrict__ acc) {
+    float4* row = reinterpret_cast<float4*>(red + lane * kRedStride);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) row[c] = make_float4(gl[4 * c], gl[4 * c + 1], gl[4 * c + 2], gl[4 * c + 3]);
+    row[6] = make_float4(gl[24], 0.f, 0.f, 0.f);
+    warp_sum_columns(red, lane, acc);
+}
+
+// Rows of hit_grads_planes' output: gl[12..25) and the two planes' normal
+// gradients, stored at the planes' columns (ie, ix: -1 for none or a lane
+// without a hit, whose gl[12..25) are zero).
+__device__ __forceinline__ void warp_sum_rows_planes(float* __restrict__ red, const float* gl, f3 dne, f3 dnx,
+                                                     int ie, int ix, int lane, float* __restrict__ acc) {
+    float* rowf = red + lane * kRedStride;
+    float4* row = reinterpret_cast<float4*>(rowf);
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    row[0] = z;
+    row[1] = z;
+    row[2] = z;
+#pragma unroll
+    for (int c = 3; c < 6; ++c) row[c] = make_float4(gl[4 * c], gl[4 * c + 1], gl[4 * c + 2], gl[4 * c + 3]);
+    row[6] = make_float4(gl[24], 0.f, 0.f, 0.f);
+    if (ie >= 0) {
+        rowf[3 * ie] = dne.x;
+        rowf[3 * ie + 1] = dne.y;
+        rowf[3 * ie + 2] = dne.z;
+    }
+    if (ix >= 0) {
+        rowf[3 * ix] = dnx.x;
+        rowf[3 * ix + 1] = dnx.y;
+        rowf[3 * ix + 2] = dnx.z;
+    }
+    warp_sum_columns(red, lane, acc);
+}
+
 // Adjoint of one hit (the Slang autodiff of update_alpha_out,
 // evaluate_tetra_interp and load_tet_alphablend_interp, written out by hand).
 // Inputs: the entry's intersection and segment, T = exp(log T) and D2, D3 of
@@ -770,10 +834,15 @@ __device__ __forceinline__ void warp_sum_rows(float* __restrict__ red, const flo
 // v0 12..14, v1 15..17, density 18, rgb 19..21, grd 22..24) and returns
 // dL/d(log T before the hit); nD2 / nD3 receive dL/d(D2, D3 before the hit).
 // a0, a1: v0 - o and v1 - o (the reference vertices of the planes).
-__device__ __forceinline__ float hit_grads_a(const float4* __restrict__ q, f3 a0, f3 a1, f3 d, const Isect& is,
-                                             const Segment& s, float T, float D2_old, float D3_old,
-                                             const float* dS_c, float dS_logT, const float* dS_D, float* gl,
-                                             float& nD2, float& nD3) {
+//
+// hit_grads_planes leaves gl[0..12) alone and returns the gradients of the
+// entering and exiting planes' normals (planes is.ie, is.ix) in dne, dnx
+// (both zero for a plane index of -1); hit_grads_a scatters them into
+// gl[0..12).
+__device__ __forceinline__ float hit_grads_planes(const float4* __restrict__ q, f3 a0, f3 a1, f3 d,
+                                                  const Isect& is, const Segment& s, float T, float D2_old,
+                                                  float D3_old, const float* dS_c, float dS_logT, const float* dS_D,
+                                                  float* gl, f3& dne, f3& dnx, float& nD2, float& nD3) {
     const float density = q[0].w;
     const float enter = is.enter, exit = is.exit;
     const float m1 = density * (exit + enter) / 2.0f;
@@ -833,29 +902,40 @@ __device__ __forceinline__ float hit_grads_a(const float4* __restrict__ q, f3 a0
     // gradient factors only (the hit and its t values are exact above): the
     // approximate quotient (2 ulp) is far inside the gradients' tolerance
     const float ge = __fdividef(d_te, is.dene), gx = __fdividef(d_tx, is.denx);
+    // a plane index of -1 (no entering / exiting plane) contributes nothing
+    const float gek = is.ie >= 0 ? ge : 0.f, gxk = is.ix >= 0 ? gx : 0.f;
     const f3 ae = is.ie == 3 ? a1 : a0, ax = is.ix == 3 ? a1 : a0;
-    const f3 dne = {ge * (ae.x - is.te * d.x), ge * (ae.y - is.te * d.y), ge * (ae.z - is.te * d.z)};
-    const f3 dnx = {gx * (ax.x - is.tx * d.x), gx * (ax.y - is.tx * d.y), gx * (ax.z - is.tx * d.z)};
+    dne = {gek * (ae.x - is.te * d.x), gek * (ae.y - is.te * d.y), gek * (ae.z - is.te * d.z)};
+    dnx = {gxk * (ax.x - is.tx * d.x), gxk * (ax.y - is.tx * d.y), gxk * (ax.z - is.tx * d.z)};
+    // the planes' reference vertices (v1 for plane 3, v0 for the others):
+    // gradient +n * g; the normals are read from the staged record by index
+    const f3 ne = xyz(q[is.ie < 0 ? 0 : is.ie]), nx = xyz(q[is.ix < 0 ? 0 : is.ix]);
+    const float ge0 = is.ie == 3 ? 0.f : gek, ge1 = is.ie == 3 ? gek : 0.f;
+    const float gx0 = is.ix == 3 ? 0.f : gxk, gx1 = is.ix == 3 ? gxk : 0.f;
+    gl[12] += ne.x * ge0 + nx.x * gx0;
+    gl[13] += ne.y * ge0 + nx.y * gx0;
+    gl[14] += ne.z * ge0 + nx.z * gx0;
+    gl[15] += ne.x * ge1 + nx.x * gx1;
+    gl[16] += ne.y * ge1 + nx.y * gx1;
+    gl[17] += ne.z * ge1 + nx.z * gx1;
+    // safe_exp's clip at log(1e20) never binds: log T <= 0
+    return dS_logT + dT * T;
+}
+
+__device__ __forceinline__ float hit_grads_a(const float4* __restrict__ q, f3 a0, f3 a1, f3 d, const Isect& is,
+                                             const Segment& s, float T, float D2_old, float D3_old,
+                                             const float* dS_c, float dS_logT, const float* dS_D, float* gl,
+                                             float& nD2, float& nD3) {
+    f3 dne, dnx;
+    const float r = hit_grads_planes(q, a0, a1, d, is, s, T, D2_old, D3_old, dS_c, dS_logT, dS_D, gl, dne, dnx,
+                                     nD2, nD3);
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
-        const f3 np = xyz(q[p]);
-        const float se = (is.ie == p) ? ge : 0.f, sx = (is.ix == p) ? gx : 0.f;
         gl[3 * p + 0] = (is.ie == p ? dne.x : 0.f) + (is.ix == p ? dnx.x : 0.f);
         gl[3 * p + 1] = (is.ie == p ? dne.y : 0.f) + (is.ix == p ? dnx.y : 0.f);
         gl[3 * p + 2] = (is.ie == p ? dne.z : 0.f) + (is.ix == p ? dnx.z : 0.f);
-        const float sref = se + sx;  // gradient of vref = +n * g
-        if (p == 3) {
-            gl[15] += np.x * sref;
-            gl[16] += np.y * sref;
-            gl[17] += np.z * sref;
-        } else {
-            gl[12] += np.x * sref;
-            gl[13] += np.y * sref;
-            gl[14] += np.z * sref;
-        }
     }
-    // safe_exp's clip at log(1e20) never binds: log T <= 0
-    return dS_logT + dT * T;
+    return r;
 }
 
 __device__ __forceinline__ float hit_grads(const float4* __restrict__ q, f3 o, f3 d, const Isect& is,
@@ -1046,6 +1126,7 @@ __device__ __forceinline__ void bwd_dense_item(
             s.dt = fmaxf(is.exit - is.enter, 0.f);
             s.a = density * s.dt;
             const bool hit = act && is.geo && s.a > 0.f;
+            f3 dne = {0.f, 0.f, 0.f}, dnx = {0.f, 0.f, 0.f};
             if (hit) {
                 integrate(q, o, d, is.enter, is.exit, s);
                 // undo_alpha_out (alphablend_shader_interp.slang:128-192): only log T, D2
@@ -1057,13 +1138,18 @@ __device__ __forceinline__ void bwd_dense_item(
                 D3 = D3 - m1;
                 logT = logT_old;
                 float nD2, nD3;
-                dS_logT = hit_grads(q, o, d, is, s, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
+                if constexpr (NT >= 32)
+                    dS_logT = hit_grads_planes(q, xyz(q[4]) - o, xyz(q[5]) - o, d, is, s, T, D2, D3, dS_c, dS_logT,
+                                               dS_D, gl, dne, dnx, nD2, nD3);
+                else
+                    dS_logT = hit_grads(q, o, d, is, s, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
                 dS_D[2] = nD2;
                 dS_D[3] = nD3;
             }
             if (__any_sync(kMask, hit)) {
                 if constexpr (NT >= 32) {
-                    warp_sum_rows(reinterpret_cast<float*>(S.red[warp]), gl, lane, S.sacc[jj]);
+                    warp_sum_rows_planes(reinterpret_cast<float*>(S.red[warp]), gl, dne, dnx, hit ? is.ie : -1,
+                                         hit ? is.ix : -1, lane, S.sacc[jj]);
                 } else {
                     using RS = ReduceScatter<kNGrad, WarpShape<NT>::kTopOffset>;
                     int slot = 0;
@@ -1256,6 +1342,7 @@ __device__ __forceinline__ void bwd_dense_item_tma(
             sg.dt = fmaxf(is.exit - is.enter, 0.f);
             sg.a = density * sg.dt;
             const bool hit = act && is.geo && sg.a > 0.f;
+            f3 dne = {0.f, 0.f, 0.f}, dnx = {0.f, 0.f, 0.f};
             if (hit) {
                 integrate(qr, o, d, is.enter, is.exit, sg);
                 const float m1 = density * (is.exit + is.enter) / 2.0f;
@@ -1265,11 +1352,14 @@ __device__ __forceinline__ void bwd_dense_item_tma(
                 D3 = D3 - m1;
                 logT = logT_old;
                 float nD2, nD3;
-                dS_logT = hit_grads(qr, o, d, is, sg, T, D2, D3, dS_c, dS_logT, dS_D, gl, nD2, nD3);
+                dS_logT = hit_grads_planes(qr, xyz(qr[4]) - o, xyz(qr[5]) - o, d, is, sg, T, D2, D3, dS_c, dS_logT,
+                                           dS_D, gl, dne, dnx, nD2, nD3);
                 dS_D[2] = nD2;
                 dS_D[3] = nD3;
             }
-            if (__any_sync(0xffffffffu, hit)) warp_sum_rows(reinterpret_cast<float*>(S.red[warp]), gl, lane, S.sacc[jj]);
+            if (__any_sync(0xffffffffu, hit))
+                warp_sum_rows_planes(reinterpret_cast<float*>(S.red[warp]), gl, dne, dnx, hit ? is.ie : -1,
+                                     hit ? is.ix : -1, lane, S.sacc[jj]);
         }
         __syncthreads();
         flush_entries<NT, B>(nk, S.srec[cb], S.sid[cb], S.sacc, indices, gverts, gcv);
@@ -1908,7 +1998,9 @@ int launch_fwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, cons
                       tn.n_recs};
     const Queue qp = {w.order, w.info, w.tickets + 1, G, subs_pair, true, hm, tn.status, rm_host::wait_limit(),
                       tn.n_recs};
-    auto pair_kernel = blend_fwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, V>;
+    auto pair_kernel = tn.pair_ctas_per_sm * NT_PAIR >= 1024
+                           ? blend_fwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, 1024 / NT_PAIR, V>
+                           : blend_fwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, 768 / NT_PAIR, V>;
     const int smem = (int)sizeof(FwdPairSmem<PX_PAIR, B_PAIR>);
     cudaFuncSetAttribute(pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const int pair_cap = tn.pair_ctas_per_sm * sm_count();
