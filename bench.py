@@ -56,6 +56,8 @@ def parse():
                          "(cp.async.bulk, two batches in flight); bulk copies only in single-GPU runs")
     ap.add_argument("--pair-ctas", type=int, default=0,
                     help="resident CTAs per SM of the forward's pair kernel (0: the library default)")
+    ap.add_argument("--bwd-batch", type=int, default=0, choices=[0, 16, 32, 64],
+                    help="tets per shared-memory batch of the backward (0: the library default)")
     ap.add_argument("--profile-steps", type=int, default=0, help="(profiling) run N steps after warmup, print nothing")
     ap.add_argument("--workload", choices=["training", "multiview", "serving"], default="training",
                     help="training: the 1.3M-tet fwd+bwd step (default line); multiview: 16 views of a "
@@ -267,6 +269,8 @@ def run_b200(args):
     R.use_tma_staging(args.stage == "tma" and world == 1)
     if args.pair_ctas:
         R.set_blend_tuning(args.pair_ctas << _capi.RM_BLEND_PAIR_CTAS_SHIFT, R.blend_tuning()[1])
+    if args.bwd_batch:
+        R.set_blend_tuning(R.blend_tuning()[0], (args.bwd_batch.bit_length() - 1) << _capi.RM_BLEND_BATCH_SHIFT)
     rng = np.random.default_rng(1000 + rank)
     target_h = torch.from_numpy(rng.uniform(size=(H, W, 3)).astype(np.float32)).pin_memory()
     # The model's raw per-tet outputs (density, base colour, colour gradient),
@@ -500,7 +504,8 @@ def run_b200(args):
                    else "single view", "l2": "flushed between steps (256 MiB write)",
                    "seed": 2, "jitter": "torch.rand per step (train.py:244)",
                    "record_staging": "bulk copies (cp.async.bulk)" if R.tma_staging() else "per-thread loads",
-                   "pair_ctas_per_sm": args.pair_ctas or "library default"},
+                   "pair_ctas_per_sm": args.pair_ctas or "library default",
+                   "bwd_batch": args.bwd_batch or "library default"},
         "value_jitter_0_5": {"value": value_const, "ms_per_step": total_ms_const / args.steps,
                              "jitter": "constant 0.5 (render() default)"},
         "e2e": e2e, "roofline": roof, "stages_ms": per_stage, "stages_pass_steps": n_break,
@@ -793,6 +798,15 @@ def _serving_mesh(job):
     return n, m.vertices, m.indices, m.cell_values
 
 
+def _mesh_worker_init():
+    """Mesh builders yield the host cores to the measurement running beside
+    them (the e2e step's launches, the CPU baseline's threads)."""
+    try:
+        os.nice(19)
+    except OSError:
+        pass
+
+
 def _mesh_job(job):
     """(points, seed) -> a mixture mesh (runs in a spawned host process)."""
     from radiance_meshes_b200 import scenes
@@ -911,7 +925,18 @@ def run_default(args):
     if extras:
         counts = [int(x) for x in args.sv_points.split(",")]
         spec = [(args.mv_points, 3)] + list(zip(counts, [4, 5, 6][:len(counts)]))
-        pool = mp.get_context("spawn").Pool(len(spec))
+        # one thread per builder (the variables reach the spawned processes
+        # before their numpy loads), at the lowest priority
+        saved = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")}
+        os.environ.update({k: "1" for k in saved})
+        try:
+            pool = mp.get_context("spawn").Pool(len(spec), initializer=_mesh_worker_init)
+        finally:
+            for k, v in saved.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
         jobs = pool.map_async(_mesh_job, spec)
     try:
         line = run_b200(args)

@@ -1583,8 +1583,13 @@ __device__ __forceinline__ void bwd_pair_item(
     }
 }
 
+// Resident CTAs per SM (of 64 threads) the dense backward is compiled for.
+#ifndef RM_BWD_DENSE_MINB
+#define RM_BWD_DENSE_MINB 8
+#endif
+
 template <int NT, int B, class V>
-__global__ void __launch_bounds__(NT, (NT >= 64 ? 512 / NT : 16)) blend_bwd_dense_kernel(
+__global__ void __launch_bounds__(NT, (NT >= 64 ? RM_BWD_DENSE_MINB * 64 / NT : 16)) blend_bwd_dense_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges, const float4* __restrict__ recs,
     const int4* __restrict__ indices, const float2* __restrict__ jitter, const __grid_constant__ V views,
     const float4* __restrict__ img, const float* __restrict__ dist, const int32_t* __restrict__ ncs,
