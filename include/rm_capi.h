@@ -275,8 +275,7 @@ RM_API int rm_tile_ranges(const int64_t* sorted_keys, int64_t n, const int64_t* 
  */
 RM_API size_t rm_blend_workspace_size(int64_t n_tets, int64_t n_tiles);
 /* Extra workspace bytes for RM_BLEND_HIT_MASKS over n_pairs list entries in
- * n_tiles tiles of tile_pixels pixels (per 32 entries per pixel: 4 bytes of
- * hit bits and 16 bytes of 4-bit plane codes). */
+ * n_tiles tiles of tile_pixels pixels (4 bytes per 32 entries per pixel). */
 RM_API size_t rm_blend_hit_mask_bytes(int64_t n_pairs, int64_t n_tiles, int tile_pixels);
 /* Byte offset, inside a workspace of rm_blend_workspace_size(n_tets, n_tiles)
  * bytes, of the status word a blend pass uses when given no status_dev. */
@@ -285,10 +284,8 @@ RM_API size_t rm_blend_status_offset(int64_t n_tets, int64_t n_tiles);
 #define RM_BLEND_REUSE_RECORDS 0x1  /* workspace already holds this frame's records */
 /* Hit masks: with this flag on rm_blend_fwd and rm_blend_bwd (same lists, same
  * workspace, 64-pixel work items) the forward stores, per list entry and work
- * item, which pixels it counted as hits and, for each hit, the two faces
- * through which the ray entered and left the tet; the backward revisits only
- * the hits and recomputes the intersection with those two faces only (the
- * same t values bit for bit).  The workspace must extend
+ * item, which pixels it counted as hits, and the backward revisits only those,
+ * skipping the ray/tet tests of the misses.  The workspace must extend
  * rm_blend_hit_mask_bytes(P, G, tile pixels) beyond rm_blend_workspace_size;
  * entries past that room are tested as without masks.  A forward without the
  * flag (or with 16-pixel items) marks the masks invalid, and the backward then

@@ -142,30 +142,6 @@ __device__ __forceinline__ Isect intersect(const float4* __restrict__ q, f3 o, f
     return r;
 }
 
-// intersect<true> for a hit whose entering and exiting planes are known
-// (code ie | ix << 2 from the forward's plane codes): the same quotients of
-// those two planes, so the same t_enter / t_exit bits, clamps and
-// denominators as testing all four planes.
-__device__ __forceinline__ Isect intersect_known(const float4* __restrict__ q, f3 o, f3 d, uint32_t code) {
-    const int ie = (int)(code & 3u), ix = (int)(code >> 2);
-    const f3 a0 = xyz(q[4]) - o;
-    const f3 a1 = xyz(q[5]) - o;
-    const f3 ne = xyz(q[ie]), nx = xyz(q[ix]);
-    const float diste = -dot3(ne, ie == 3 ? a1 : a0), distx = -dot3(nx, ix == 3 ? a1 : a0);
-    const float dene = dot3(ne, d), denx = dot3(nx, d);
-    Isect r;
-    r.te = -diste / dene;
-    r.tx = -distx / denx;
-    r.geo = true;
-    r.enter = fmaxf(r.te, 0.f);
-    r.exit = fmaxf(r.tx, r.enter);
-    r.dene = dene;
-    r.denx = denx;
-    r.ie = ie;
-    r.ix = ix;
-    return r;
-}
-
 // Weights of the closed-form segment integral (interp_version.slang:21-40)
 // for optical depth x = density * dt >= 0:
 //   alpha = exp(-x), phi = (1 - exp(-x)) / x, w0 = phi - alpha, w1 = 1 - phi.
@@ -282,19 +258,6 @@ struct WarpShape {
 // overlap; a pixel's words of consecutive blocks are 64 words apart, and the
 // 64 pixels of an item are contiguous (coalesced stores and loads).  Words at
 // or beyond cap do not exist: the entries they would describe are tested.
-//
-// Beside each mask word i the forward keeps four plane words (planes[4i ..
-// 4i + 4), one uint4): the 4-bit plane code of each of the block's 32
-// entries, entry e of the block in bits 4 (e % 8) of word e / 8.  For a hit
-// the code is ie | ix << 2, the planes through which the ray entered and
-// left the tet; kNoPlanes when either is missing (the ray starts inside the
-// tet, or no plane bounds it) and for the entries that were no hits.  The
-// backward then needs only those two planes' quotients: the forward's
-// t_enter and t_exit are exactly those quotients (the running maximum and
-// minimum of the quotients are the selected ones), so recomputing them gives
-// the same bits as testing all four planes.
-constexpr uint32_t kNoPlanes = 15u;  // ie = 3, ix = 3 cannot occur: a plane enters or leaves
-
 __device__ __forceinline__ int64_t mask_word(int gtile, int x, int k, int sub, int subs, int p) {
     return (((int64_t)(x >> 5) + k + gtile) * subs + sub) * 64 + p;
 }
@@ -303,7 +266,6 @@ struct HitMasks {
     uint32_t* words;  // nullptr: no masks
     int64_t cap;      // words
     const uint32_t* header;  // kMaskValid: this pass's forward wrote masks with 64-pixel items
-    uint32_t* planes;        // 4 cap words of plane codes (nullptr: none)
 };
 
 constexpr uint32_t kMaskValid = 0x6d61736bu;
@@ -311,7 +273,6 @@ constexpr uint32_t kMaskValid = 0x6d61736bu;
 // The masks a kernel may use: none unless the header says the forward wrote them.
 __device__ __forceinline__ HitMasks live_masks(HitMasks hm) {
     if (hm.words && (!hm.header || __ldcg(hm.header) != kMaskValid)) hm.words = nullptr;
-    if (!hm.words) hm.planes = nullptr;
     return hm;
 }
 
@@ -372,39 +333,6 @@ __device__ __forceinline__ void write_masks(const HitMasks& hm, uint64_t hb, int
     }
 }
 
-// Stores the plane codes of one batch for pixel p: pc[4 w .. 4 w + 4) are
-// the four code words of the batch's block w (as write_masks).
-template <int NW>
-__device__ __forceinline__ void write_planes(const HitMasks& hm, const uint32_t (&pc)[NW], int gtile, int x, int base,
-                                             int n, int sub, int subs, int p) {
-    const int k0 = (base - x) >> 5;
-#pragma unroll
-    for (int w = 0; w < NW / 4; ++w) {
-        if (w * 32 >= n) break;
-        const int64_t i = mask_word(gtile, x, k0 + w, sub, subs, p);
-        if (i < hm.cap)
-            __stcg(reinterpret_cast<uint4*>(hm.planes) + i, make_uint4(pc[4 * w], pc[4 * w + 1], pc[4 * w + 2],
-                                                                       pc[4 * w + 3]));
-    }
-}
-
-// The code words of block (gtile, x, k) for pixel p; all kNoPlanes where
-// there are none (the backward then tests all four planes).
-__device__ __forceinline__ uint4 load_planes(const HitMasks& hm, int gtile, int x, int k, int sub, int subs, int p) {
-    const int64_t i = mask_word(gtile, x, k, sub, subs, p);
-    if (hm.planes && i < hm.cap) return __ldcg(reinterpret_cast<const uint4*>(hm.planes) + i);
-    return make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
-}
-
-// The code of the entry at list offset off (relative to the list start)
-// from the code words c0 / c1 of blocks kb0 / the one after.
-__device__ __forceinline__ uint32_t plane_code(uint4 c0, uint4 c1, int kb0, int off) {
-    const uint4 c = (off >> 5) == kb0 ? c0 : c1;
-    const int w = (off >> 3) & 3;
-    const uint32_t word = w == 0 ? c.x : w == 1 ? c.y : w == 2 ? c.z : c.w;
-    return (word >> (4 * (off & 7))) & 15u;
-}
-
 // One hit folded into the pixel state (update_alpha_out,
 // alphablend_shader_interp.slang:84-183): colour += rgb * T, log T -= a, and
 // the five distortion moments with m0 = density, m1 = density * (a + b) / 2.
@@ -427,12 +355,11 @@ __device__ __forceinline__ void fold_hit(PixelState& st, float a, float m0, floa
 struct EntryResult {
     float a, m1, d4;
     float rgb[3];
-    uint32_t code;  // plane code of a hit (ie | ix << 2, or kNoPlanes)
 };
 
 __device__ __forceinline__ EntryResult eval_entry(const float4* __restrict__ q, f3 o, f3 d) {
     EntryResult r;
-    const Isect is = intersect<true>(q, o, d);
+    const Isect is = intersect<false>(q, o, d);
     Segment s;
     s.dt = fmaxf(is.exit - is.enter, 0.f);
     const float density = q[0].w;
@@ -441,7 +368,6 @@ __device__ __forceinline__ EntryResult eval_entry(const float4* __restrict__ q, 
     r.m1 = 0.f;
     r.d4 = 0.f;
     r.rgb[0] = r.rgb[1] = r.rgb[2] = 0.f;
-    r.code = (is.ie < 0 || is.ix < 0) ? kNoPlanes : (uint32_t)(is.ie | (is.ix << 2));
     if (is.geo && s.a > 0.f) {
         integrate(q, o, d, is.enter, is.exit, s);
         r.a = s.a;
@@ -495,10 +421,6 @@ __device__ __forceinline__ void fwd_dense_item(int tile, int sub, const int32_t*
             }
             __syncthreads();
             uint64_t hb = 0;  // bit j: entry j of the batch was a hit
-            constexpr int kPW = B >= 16 ? B / 16 : 1;
-            uint64_t pcw[kPW];  // plane codes, 16 entries per word (kNoPlanes for the misses)
-#pragma unroll
-            for (int w = 0; w < kPW; ++w) pcw[w] = ~0ull;
             if (__any_sync(WarpShape<NT>::kMask, active)) {
                 for (int j = 0; j < n; ++j) {
                     if (!active) break;
@@ -506,29 +428,12 @@ __device__ __forceinline__ void fwd_dense_item(int tile, int sub, const int32_t*
                     const EntryResult r = eval_entry(S.srec[j], o, d);
                     if (r.a > 0.f) {
                         hb |= 1ull << j;
-                        if (kMasks) {
-                            const int sh = 4 * (j & 15);
-#pragma unroll
-                            for (int w = 0; w < kPW; ++w)
-                                if (w == (j >> 4)) pcw[w] = (pcw[w] & ~(15ull << sh)) | ((uint64_t)r.code << sh);
-                        }
                         fold_hit(st, r.a, S.srec[j][0].w, r.m1, r.d4, r.rgb);
                         if (st.logT < kTermLogT) active = false;
                     }
                 }
             }
-            if (kMasks && hm.words) {
-                write_masks(hm, hb, gtile, rg.x, base, n, sub, subs, (int)threadIdx.x);
-                if (hm.planes) {
-                    uint32_t pc[2 * kPW];
-#pragma unroll
-                    for (int w = 0; w < kPW; ++w) {
-                        pc[2 * w] = (uint32_t)pcw[w];
-                        pc[2 * w + 1] = (uint32_t)(pcw[w] >> 32);
-                    }
-                    write_planes(hm, pc, gtile, rg.x, base, n, sub, subs, (int)threadIdx.x);
-                }
-            }
+            if (kMasks && hm.words) write_masks(hm, hb, gtile, rg.x, base, n, sub, subs, (int)threadIdx.x);
             if (!__syncthreads_or(active)) break;
         }
     }
@@ -559,7 +464,6 @@ struct FwdPairSmem {
     float dens[2][B];      // densities of the batch being folded and of the one being staged
     float ray[6][PX];      // o, d of each slot (structure of arrays)
     float res[6][B][PX];   // a (0: miss), m1, d4, r, g, b per (entry, slot)
-    uint8_t pcode[B][PX];  // plane code per (entry, slot), kept for the hits
     int32_t warp_base[(PX + 31) / 32];
 };
 
@@ -571,7 +475,6 @@ __device__ __forceinline__ void store_result(FwdPairSmem<PX, B>& S, int j, int s
     S.res[3][j][sl] = r.rgb[0];
     S.res[4][j][sl] = r.rgb[1];
     S.res[5][j][sl] = r.rgb[2];
-    S.pcode[j][sl] = (uint8_t)r.code;
 }
 
 // Stages batch [base, base + n) into srec (and its densities into dens[buf])
@@ -696,24 +599,7 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
                     }
                 }
             }
-            if (kMasks && owner && hm.words) {
-                write_masks(hm, hb, gtile, rg.x, base, n, sub, subs, tid);
-                if (hm.planes) {  // the hits' plane codes, kNoPlanes elsewhere
-                    uint32_t pc[B / 8];
-#pragma unroll
-                    for (int w = 0; w < B / 8; ++w) {
-                        uint32_t word = 0u;
-#pragma unroll
-                        for (int e = 0; e < 8; ++e) {
-                            const int j = 8 * w + e;
-                            const uint32_t c = ((hb >> j) & 1u) ? (uint32_t)S.pcode[j][slot] : kNoPlanes;
-                            word |= c << (4 * e);
-                        }
-                        pc[w] = word;
-                    }
-                    write_planes(hm, pc, gtile, rg.x, base, n, sub, subs, tid);
-                }
-            }
+            if (kMasks && owner && hm.words) write_masks(hm, hb, gtile, rg.x, base, n, sub, subs, tid);
             // the next batch's slots: the pixels still active
             if (owner) {
                 const unsigned bal = __ballot_sync(kOwnMask, active);
@@ -1173,14 +1059,11 @@ __device__ __forceinline__ void bwd_dense_item(
         // this pixel's hit bits of the (at most two) 32-entry blocks the batch spans
         const int kb0 = (lo - rg.x) >> 5, kb1 = (top - 1 - rg.x) >> 5;
         uint32_t hw0 = 0xffffffffu, hw1 = 0xffffffffu;
-        uint4 pc0 = make_uint4(~0u, ~0u, ~0u, ~0u), pc1 = pc0;  // plane codes (all kNoPlanes: none)
         if (kMasks && hm.words) {
             const int64_t i0 = mask_word(gtile, rg.x, kb0, sub, subs, (int)threadIdx.x);
             const int64_t i1 = mask_word(gtile, rg.x, kb1, sub, subs, (int)threadIdx.x);
             if (i0 < hm.cap) hw0 = __ldcg(hm.words + i0);
             if (i1 < hm.cap) hw1 = __ldcg(hm.words + i1);
-            pc0 = load_planes(hm, gtile, rg.x, kb0, sub, subs, (int)threadIdx.x);
-            pc1 = kb1 == kb0 ? pc0 : load_planes(hm, gtile, rg.x, kb1, sub, subs, (int)threadIdx.x);
         }
         // entries no pixel of the item hit are dropped from the batch before
         // staging (the masks of pixels past their n_contributors are zero)
@@ -1237,14 +1120,7 @@ __device__ __forceinline__ void bwd_dense_item(
             float gl[kNGrad];
 #pragma unroll
             for (int k = 0; k < kNGrad; ++k) gl[k] = 0.f;
-            // the forward's planes of each hit: two quotients instead of four
-            // (lanes without a hit take any two planes; a hit without codes
-            // makes the warp test all four)
-            Isect is;
-            uint32_t code = kNoPlanes;
-            if constexpr (kMasks) code = act ? plane_code(pc0, pc1, kb0, off) : 4u;
-            if (__any_sync(kMask, act && code == kNoPlanes)) is = intersect<true>(q, o, d);
-            else is = intersect_known(q, o, d, code);
+            const Isect is = intersect<true>(q, o, d);
             const float density = q[0].w;
             Segment s;
             s.dt = fmaxf(is.exit - is.enter, 0.f);
@@ -1939,7 +1815,6 @@ struct BlendWs {
     uint32_t* mask_header;  // nullptr: the workspace has no room for hit masks
     uint32_t* mask_words;
     int64_t mask_cap;
-    uint32_t* plane_words;  // 4 mask_cap words of plane codes
 };
 
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
@@ -1955,21 +1830,18 @@ size_t blend_ws_bytes(int64_t n_tets, int64_t n_tiles) {
 }
 
 // Hit masks, when the caller's workspace is larger than blend_ws_bytes: a
-// 256-byte header, then the mask words (mask_word), then four plane-code
-// words per mask word.
+// 256-byte header, then the mask words (mask_word).
 BlendWs blend_ws(void* base, int64_t n_tets, int64_t n_tiles, size_t workspace_bytes) {
     char* p = (char*)base;
     const size_t rec = align256((size_t)(n_tets > 0 ? n_tets : 1) * kRecFloat4 * sizeof(float4));
     const size_t ord = align256((size_t)(n_tiles > 0 ? n_tiles : 1) * sizeof(int32_t));
     BlendWs w = {(float4*)p, (int32_t*)(p + rec), (int32_t*)(p + rec + ord), (uint32_t*)(p + rec + ord + 64),
-                 (uint32_t*)(p + rec + ord + kBlendStatusOff), nullptr, nullptr, 0, nullptr};
+                 (uint32_t*)(p + rec + ord + kBlendStatusOff), nullptr, nullptr, 0};
     const size_t end = rec + ord + 256;
-    if (workspace_bytes >= end + 256 + 64 * 5 * sizeof(uint32_t)) {
+    if (workspace_bytes >= end + 256 + 64 * sizeof(uint32_t)) {
         w.mask_header = (uint32_t*)(p + end);
         w.mask_words = (uint32_t*)(p + end + 256);
-        // a multiple of 4 words, so the plane words start 16-byte aligned
-        w.mask_cap = (int64_t)((workspace_bytes - end - 256) / (5 * sizeof(uint32_t))) & ~(int64_t)3;
-        w.plane_words = w.mask_words + w.mask_cap;
+        w.mask_cap = (int64_t)((workspace_bytes - end - 256) / sizeof(uint32_t));
     }
     return w;
 }
@@ -2126,8 +1998,7 @@ int launch_fwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, cons
     if (rc) return rc;
     const int subs = sh.tile_px / PX;
     const int subs_pair = sh.tile_px / PX_PAIR;
-    const HitMasks hm = {masks ? w.mask_words : nullptr, w.mask_cap, w.mask_header,
-                         masks ? w.plane_words : nullptr};
+    const HitMasks hm = {masks ? w.mask_words : nullptr, w.mask_cap, w.mask_header};
     const Queue qd = {w.order, w.info, w.tickets + 0, G, subs, false, hm, tn.status, rm_host::wait_limit(),
                       tn.n_recs};
     const Queue qp = {w.order, w.info, w.tickets + 1, G, subs_pair, true, hm, tn.status, rm_host::wait_limit(),
@@ -2169,12 +2040,11 @@ int launch_bwd(const int32_t* ids, const int32_t* ranges, const BlendWs& w, cons
     const int subs = sh.tile_px / PX;
     const int subs_pair = sh.tile_px / PX_PAIR;
     const bool masks = tn.hit_masks && PX == 64 && w.mask_header;
-    const HitMasks hm = {masks ? w.mask_words : nullptr, w.mask_cap, w.mask_header,
-                         masks ? w.plane_words : nullptr};
+    const HitMasks hm = {masks ? w.mask_words : nullptr, w.mask_cap, w.mask_header};
     const Queue qd = {w.order, w.info, w.tickets + 2, G, subs, false, hm, tn.status, rm_host::wait_limit(),
                       tn.n_recs};
-    const Queue qp = {w.order, w.info, w.tickets + 3, G, subs_pair, true,
-                      HitMasks{nullptr, 0, nullptr, nullptr}, tn.status, rm_host::wait_limit(), tn.n_recs};
+    const Queue qp = {w.order, w.info, w.tickets + 3, G, subs_pair, true, HitMasks{nullptr, 0, nullptr},
+                      tn.status, rm_host::wait_limit(), tn.n_recs};
     auto pair_kernel = blend_bwd_pair_kernel<PX_PAIR, NT_PAIR, B_PAIR, V>;
     const int smem = (int)sizeof(BwdPairSmem<PX_PAIR, B_PAIR>);
     cudaFuncSetAttribute(pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -2380,7 +2250,7 @@ size_t rm_blend_status_offset(int64_t n_tets, int64_t n_tiles) {
 size_t rm_blend_hit_mask_bytes(int64_t n_pairs, int64_t n_tiles, int tile_pixels) {
     const int64_t subs = tile_pixels > 64 ? tile_pixels / 64 : 1;
     const int64_t blocks = (n_pairs > 0 ? n_pairs : 0) / 32 + (n_tiles > 0 ? n_tiles : 0) + 2;
-    return 256 + (size_t)blocks * (size_t)subs * 64 * 5 * sizeof(uint32_t);  // hit bits + plane codes
+    return 256 + (size_t)blocks * (size_t)subs * 64 * sizeof(uint32_t);
 }
 
 int rm_calc_tet_err(const int32_t* sorted_ids, const int32_t* ranges, const int32_t* indices, const float* vertices,
@@ -2406,8 +2276,7 @@ int rm_calc_tet_err(const int32_t* sorted_ids, const int32_t* ranges, const int3
     if ((rc = launch_order(ranges, (int)G, w, 1, s))) return rc;
     const int strip = strip_pixels(cam, flags);
     const int subs = cam->tile_width * cam->tile_height / strip;
-    const Queue qd = {w.order, w.info, w.tickets + 0, (int)G, subs, true, HitMasks{nullptr, 0, nullptr, nullptr},
-                      nullptr,
+    const Queue qd = {w.order, w.info, w.tickets + 0, (int)G, subs, true, HitMasks{nullptr, 0, nullptr}, nullptr,
                       rm_host::wait_limit(), n_tets};
     if (strip == 16) {
         const int grid = persistent_grid(err_kernel<16, 32>, 16, 0, (int)G * subs);
