@@ -292,7 +292,7 @@ RM_API size_t rm_blend_status_offset(int64_t n_tets, int64_t n_tiles);
  * tests every entry. */
 #define RM_BLEND_HIT_MASKS 0x2
 /* Records of each shared-memory batch staged by bulk copies (cp.async.bulk
- * from this GPU's memory, completing on an mbarrier; no multicast), two
+ * from this GPU's memory into the issuing CTA, completing on an mbarrier), two
  * batches in flight, instead of per-thread loads.  Backward, 64-pixel items. */
 #define RM_BLEND_STAGE_TMA 0x4
 

@@ -764,57 +764,66 @@ struct ReduceScatter<M, 0> {
 };
 
 // Warp sum of the 25 per-lane partials of one entry, through shared memory,
-// added to the entry's accumulator acc[0..25).  Only the lanes with a hit
-// store a row, packed in lane order into rows 0 .. nh-1 (seven float4 each,
-// row stride 28 floats: the eight lanes of each store phase hit distinct
-// banks); then lane k < 25 adds column k over those nh rows (consecutive
-// lanes read consecutive words).  The row holds gl[12..25) of
-// hit_grads_planes, with the two faces' normal gradients (dne, dnx) stored
-// at their columns 3 ie, 3 ix and zeros at the other faces' columns.  red:
-// 32 * kRedStride floats, 16-byte aligned, private to the warp.
+// added to the entry's accumulator acc[0..25).  Each lane stores its row as
+// seven float4 (row stride 28 floats: the eight lanes of each store phase
+// hit distinct banks); then lane k < 25 adds column k over the 32 rows
+// (consecutive lanes read consecutive words).  Fewer instructions than the
+// 27-shuffle reduce-scatter for full warps.  red: 32 * kRedStride floats,
+// 16-byte aligned, private to the warp.
 constexpr int kRedStride = 28;
 
-__device__ __forceinline__ void warp_sum_rows_planes(float* __restrict__ red, bool hit, const float* gl, f3 dne,
-                                                     f3 dnx, int ie, int ix, int lane, float* __restrict__ acc) {
-    const unsigned bal = __ballot_sync(0xffffffffu, hit);
-    const int nh = __popc(bal);
-    if (hit) {
-        float* rowf = red + __popc(bal & ((1u << lane) - 1u)) * kRedStride;
-        float4* row = reinterpret_cast<float4*>(rowf);
-        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-        row[0] = z;
-        row[1] = z;
-        row[2] = z;
-#pragma unroll
-        for (int c = 3; c < 6; ++c) row[c] = make_float4(gl[4 * c], gl[4 * c + 1], gl[4 * c + 2], gl[4 * c + 3]);
-        row[6] = make_float4(gl[24], 0.f, 0.f, 0.f);
-        if (ie >= 0) {
-            rowf[3 * ie] = dne.x;
-            rowf[3 * ie + 1] = dne.y;
-            rowf[3 * ie + 2] = dne.z;
-        }
-        if (ix >= 0) {
-            rowf[3 * ix] = dnx.x;
-            rowf[3 * ix + 1] = dnx.y;
-            rowf[3 * ix + 2] = dnx.z;
-        }
-    }
+__device__ __forceinline__ void warp_sum_columns(const float* red, int lane, float* __restrict__ acc) {
     __syncwarp();
     if (lane < kNGrad) {
-        const float* col = red + lane;
         float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-        int r = 0;
-        for (; r + 4 <= nh; r += 4) {
-            s0 += col[(r + 0) * kRedStride];
-            s1 += col[(r + 1) * kRedStride];
-            s2 += col[(r + 2) * kRedStride];
-            s3 += col[(r + 3) * kRedStride];
+#pragma unroll
+        for (int r = 0; r < 32; r += 4) {
+            s0 += red[(r + 0) * kRedStride + lane];
+            s1 += red[(r + 1) * kRedStride + lane];
+            s2 += red[(r + 2) * kRedStride + lane];
+            s3 += red[(r + 3) * kRedStride + lane];
         }
-        for (; r < nh; ++r) s0 += col[r * kRedStride];
         const float sum = (s0 + s1) + (s2 + s3);
         if (sum != 0.f) atomicAdd(acc + lane, sum);
     }
     __syncwarp();
+}
+
+// Rows of gl[0..25) as computed by hit_grads_a.
+__device__ __forceinline__ void warp_sum_rows(float* __restrict__ red, const float* gl, int lane,
+                                              float* __restrict__ acc) {
+    float4* row = reinterpret_cast<float4*>(red + lane * kRedStride);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) row[c] = make_float4(gl[4 * c], gl[4 * c + 1], gl[4 * c + 2], gl[4 * c + 3]);
+    row[6] = make_float4(gl[24], 0.f, 0.f, 0.f);
+    warp_sum_columns(red, lane, acc);
+}
+
+// Rows of hit_grads_planes' output: gl[12..25) and the two planes' normal
+// gradients, stored at the planes' columns (ie, ix: -1 for none or a lane
+// without a hit, whose gl[12..25) are zero).
+__device__ __forceinline__ void warp_sum_rows_planes(float* __restrict__ red, const float* gl, f3 dne, f3 dnx,
+                                                     int ie, int ix, int lane, float* __restrict__ acc) {
+    float* rowf = red + lane * kRedStride;
+    float4* row = reinterpret_cast<float4*>(rowf);
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    row[0] = z;
+    row[1] = z;
+    row[2] = z;
+#pragma unroll
+    for (int c = 3; c < 6; ++c) row[c] = make_float4(gl[4 * c], gl[4 * c + 1], gl[4 * c + 2], gl[4 * c + 3]);
+    row[6] = make_float4(gl[24], 0.f, 0.f, 0.f);
+    if (ie >= 0) {
+        rowf[3 * ie] = dne.x;
+        rowf[3 * ie + 1] = dne.y;
+        rowf[3 * ie + 2] = dne.z;
+    }
+    if (ix >= 0) {
+        rowf[3 * ix] = dnx.x;
+        rowf[3 * ix + 1] = dnx.y;
+        rowf[3 * ix + 2] = dnx.z;
+    }
+    warp_sum_columns(red, lane, acc);
 }
 
 // Adjoint of one hit (the Slang autodiff of update_alpha_out,
@@ -989,7 +998,7 @@ __device__ __forceinline__ void flush_entries(int n, const float4 (*srec)[kRecFl
 template <int NT, int B>
 struct BwdDenseSmem {
     float4 srec[B][kRecFloat4];
-    float4 red[NT >= 32 ? NT / 32 : 1][NT >= 32 ? 32 * kRedStride / 4 : 1];  // warp_sum_rows_planes rows, per warp
+    float4 red[NT >= 32 ? NT / 32 : 1][NT >= 32 ? 32 * kRedStride / 4 : 1];  // warp_sum_rows rows, per warp
     int32_t sid[B];
     float sacc[B][kNGrad];
     int32_t smax[WarpShape<NT>::kWarps];
@@ -1139,8 +1148,8 @@ __device__ __forceinline__ void bwd_dense_item(
             }
             if (__any_sync(kMask, hit)) {
                 if constexpr (NT >= 32) {
-                    warp_sum_rows_planes(reinterpret_cast<float*>(S.red[warp]), hit, gl, dne, dnx, is.ie, is.ix, lane,
-                                         S.sacc[jj]);
+                    warp_sum_rows_planes(reinterpret_cast<float*>(S.red[warp]), gl, dne, dnx, hit ? is.ie : -1,
+                                         hit ? is.ix : -1, lane, S.sacc[jj]);
                 } else {
                     using RS = ReduceScatter<kNGrad, WarpShape<NT>::kTopOffset>;
                     int slot = 0;
@@ -1163,11 +1172,11 @@ __device__ __forceinline__ void bwd_dense_item(
 // tet ids loaded, and warp 0 starts one 128-byte cp.async.bulk per entry
 // (global -> this CTA's shared memory, completing on the buffer's mbarrier).
 // Two record buffers alternate, so batch k+1's copies are in flight while
-// batch k is walked and flushed; nothing of this GPU's memory is multicast.
+// batch k is walked and flushed; each copy lands in the issuing CTA only.
 template <int B>
 struct BwdTmaSmem {
     float4 srec[2][B][kRecFloat4];
-    float4 red[2][32 * kRedStride / 4];  // warp_sum_rows_planes rows, per warp
+    float4 red[2][32 * kRedStride / 4];  // warp_sum_rows rows, per warp
     float sacc[B][kNGrad];
     int32_t sid[2][B];
     uint8_t cidx[2][B];
@@ -1349,8 +1358,8 @@ __device__ __forceinline__ void bwd_dense_item_tma(
                 dS_D[3] = nD3;
             }
             if (__any_sync(0xffffffffu, hit))
-                warp_sum_rows_planes(reinterpret_cast<float*>(S.red[warp]), hit, gl, dne, dnx, is.ie, is.ix, lane,
-                                     S.sacc[jj]);
+                warp_sum_rows_planes(reinterpret_cast<float*>(S.red[warp]), gl, dne, dnx, hit ? is.ie : -1,
+                                     hit ? is.ix : -1, lane, S.sacc[jj]);
         }
         __syncthreads();
         flush_entries<NT, B>(nk, S.srec[cb], S.sid[cb], S.sacc, indices, gverts, gcv);

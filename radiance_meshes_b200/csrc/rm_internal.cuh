@@ -268,7 +268,8 @@ __device__ __forceinline__ bool tet_indices_ok(int4 id, int64_t n_verts) {
 // ------------------------------------------------ bulk copies into shared --
 // One-dimensional bulk copies (cp.async.bulk, the TMA unit's untiled mode)
 // from this GPU's global memory into the issuing CTA's shared memory,
-// completing on an mbarrier that counts the bytes.  No cluster multicast.
+// completing on an mbarrier that counts the bytes; each copy lands in the
+// issuing CTA only.
 // Source and destination must be 16-byte aligned and the size a multiple of
 // 16 bytes (the per-tet records are 128 B).
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }

@@ -227,3 +227,43 @@ def test_blend_without_frame_state_is_identical(cuda):
     # gradients are sums of float atomics in another order: relative L2 error
     for x, y in ((ga, gb), (ca, cb)):
         assert float((x - y).norm() / y.norm()) <= 1e-5
+
+
+@pytest.mark.parametrize("bad_id", [-7, 10 ** 6])
+def test_blend_skips_list_ids_outside_the_tets(cuda, bad_id):
+    """A list id that names no tet (only lists left invalid by a wait that
+    gave up, or a caller's corrupt lists, hold one) is never used as an
+    address: the blend stages a zero record for it, which no ray hits, and
+    sets RM_STATUS_BAD_INDEX.  Forward and backward then equal the passes
+    over the intact lists with that tet's density set to zero."""
+    mesh, view, tcam, grid = _scene()
+    cam = tcam_to_struct(view.tcam())
+    i, v = to_dev(mesh.indices), to_dev(mesh.vertices)
+    cv = to_dev(mesh.cell_values)
+    tiles, rect, vs, _ = R.project_fwd(i, v, cam)
+    L = R.build_tile_lists(tiles, rect, vs, cam)
+    ids = L.sorted_ids
+    g = int(ids[ids.shape[0] // 2])
+    bad = ids.clone()
+    bad[ids == g] = bad_id
+    cv0 = cv.clone()
+    cv0[g, 0] = 0.0
+    jitter = torch.rand((view.height, view.width, 2), generator=torch.Generator().manual_seed(5)).cuda()
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    img_b, dist_b, nc_b, ws_b = R.blend_fwd(bad, L.ranges, i, v, cv, jitter, cam, status=status)
+    img_r, dist_r, nc_r, ws_r = R.blend_fwd(ids, L.ranges, i, v, cv0, jitter, cam)
+    torch.cuda.synchronize()
+    assert int(status.item()) & C.RM_STATUS_BAD_INDEX
+    assert torch.equal(img_b, img_r) and torch.equal(dist_b, dist_r) and torch.equal(nc_b, nc_r)
+    gimg = torch.randn(img_b.shape, generator=torch.Generator().manual_seed(6)).cuda()
+    status.zero_()
+    gv_b, gc_b = R.blend_bwd(bad, L.ranges, i, v, cv, jitter, cam, img_b, dist_b, nc_b, gimg, None, ws_b,
+                             status=status)
+    gv_r, gc_r = R.blend_bwd(ids, L.ranges, i, v, cv0, jitter, cam, img_r, dist_r, nc_r, gimg, None, ws_r)
+    torch.cuda.synchronize()
+    assert int(status.item()) & C.RM_STATUS_BAD_INDEX
+    assert float(gc_b[g].abs().max()) == 0.0
+    keep = torch.ones(gc_b.shape[0], dtype=torch.bool, device="cuda")
+    keep[g] = False
+    for x, y in ((gv_b, gv_r), (gc_b[keep], gc_r[keep])):  # float atomics in another order
+        assert float((x - y).norm() / y.norm()) <= 1e-6
