@@ -70,7 +70,16 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
-__global__ void __launch_bounds__(kSortThreads) hist_kernel(const uint64_t* __restrict__ keys, int64_t cap,
+// Digit histograms of every pass in one read of the keys.  Each thread counts
+// a contiguous run of kHistRun keys (16-byte vector loads when the run is
+// whole and aligned; consecutive threads take consecutive runs) and adds to
+// the block's shared histogram only where a pass's digit changes along the
+// run, and once at its end: pairs emitted per tet or per tile repeat their
+// digits, so most keys add nothing, and no warp vote is needed.
+constexpr int kHistThreads = 256;
+constexpr int kHistRun = 16;
+
+__global__ void __launch_bounds__(kHistThreads) hist_kernel(const uint64_t* __restrict__ keys, int64_t cap,
                                                             const int64_t* __restrict__ n_dev, int npasses,
                                                             int begin_bit, int end_bit, SortHeader* hdr) {
     __shared__ uint32_t sh[kMaxPasses][kRadix];
@@ -78,19 +87,40 @@ __global__ void __launch_bounds__(kSortThreads) hist_kernel(const uint64_t* __re
     __syncthreads();
     const int64_t n = n_dev ? min(*n_dev, cap) : cap;
     const uint64_t mask = end_bit >= 64 ? ~0ull : ((1ull << end_bit) - 1);
-    const uint32_t lane = threadIdx.x & 31;
-    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = i0 + threadIdx.x;
-        const bool valid = i < n;
-        const uint64_t k = valid ? ((__ldg(keys + i) & mask) >> begin_bit) : 0;
-        const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
-        for (int p = 0; p < npasses; ++p) {
-            const uint32_t d = (uint32_t)(k >> (8 * p)) & 255u;
-            // warp-aggregated increments: one shared atomic per distinct digit
-            const uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : 0x100u);
-            if (valid && (peers & lanemask_lt()) == 0) atomicAdd(&sh[p][d], (uint32_t)__popc(peers & vmask));
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x * kHistRun;
+    for (int64_t s0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * kHistRun; s0 < n; s0 += stride) {
+        const int m = (int)min((int64_t)kHistRun, n - s0);  // >= 1
+        uint64_t k[kHistRun];
+        if (m == kHistRun && ((reinterpret_cast<uintptr_t>(keys + s0) & 15) == 0)) {
+            const ulonglong2* v = reinterpret_cast<const ulonglong2*>(keys + s0);
+#pragma unroll
+            for (int i = 0; i < kHistRun / 2; ++i) {
+                const ulonglong2 x = __ldg(v + i);
+                k[2 * i] = x.x;
+                k[2 * i + 1] = x.y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < kHistRun; ++i) k[i] = i < m ? __ldg(keys + s0 + i) : 0ull;
         }
-        (void)lane;
+#pragma unroll
+        for (int i = 0; i < kHistRun; ++i) k[i] = (k[i] & mask) >> begin_bit;
+        for (int p = 0; p < npasses; ++p) {
+            const int sh_p = 8 * p;
+            uint32_t last = (uint32_t)(k[0] >> sh_p) & 255u, cnt = 1u;
+#pragma unroll
+            for (int i = 1; i < kHistRun; ++i) {
+                const bool v = i < m;
+                const uint32_t d = v ? ((uint32_t)(k[i] >> sh_p) & 255u) : last;
+                if (d != last) {
+                    atomicAdd(&sh[p][last], cnt);
+                    last = d;
+                    cnt = 0u;
+                }
+                cnt += v ? 1u : 0u;
+            }
+            atomicAdd(&sh[p][last], cnt);
+        }
     }
     __syncthreads();
     for (int j = threadIdx.x; j < npasses * kRadix; j += blockDim.x) {
@@ -286,8 +316,9 @@ int rm_sort_pairs_range(const int64_t* keys_in, const int32_t* values_in, int64_
     e = cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PassSmem));
     if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_sort_pairs: %s", cudaGetErrorString(e));
     const int64_t tiles = sort_tiles(n);
-    int hist_blocks = (int)(tiles < 148 * 2 ? tiles : 148 * 2);
-    hist_kernel<<<hist_blocks, kSortThreads, 0, s>>>((const uint64_t*)keys_in, n, n_dev, npasses, begin_bit, end_bit,
+    const int64_t runs = (n + kHistThreads * kHistRun - 1) / (kHistThreads * kHistRun);
+    const int hist_blocks = (int)(runs < 148 * 4 ? runs : 148 * 4);
+    hist_kernel<<<hist_blocks, kHistThreads, 0, s>>>((const uint64_t*)keys_in, n, n_dev, npasses, begin_bit, end_bit,
                                                      hdr);
     hist_scan_kernel<<<npasses, kRadix, 0, s>>>(hdr);
     const uint64_t* src_k = (const uint64_t*)keys_in;
