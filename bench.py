@@ -59,10 +59,13 @@ def parse():
     ap.add_argument("--bwd-batch", type=int, default=0, choices=[0, 16, 32, 64],
                     help="tets per shared-memory batch of the backward (0: the library default)")
     ap.add_argument("--profile-steps", type=int, default=0, help="(profiling) run N steps after warmup, print nothing")
-    ap.add_argument("--workload", choices=["training", "multiview", "serving"], default="training",
+    ap.add_argument("--workload", choices=["training", "multiview", "serving", "sort"], default="training",
                     help="training: the 1.3M-tet fwd+bwd step (default line); multiview: 16 views of a "
                          "1M-point mesh, batched CUDA-graph step vs 16 plain per-view steps; serving: "
-                         "Poisson requests over three resident meshes, p50/p99 latency")
+                         "Poisson requests over three resident meshes, p50/p99 latency; sort: the pair "
+                         "sort alone on random keys (--sort-pairs, --sort-bits)")
+    ap.add_argument("--sort-pairs", type=int, default=24_000_000)
+    ap.add_argument("--sort-bits", default="0,47", help="key bits [begin,end) of the sort workload")
     ap.add_argument("--sv-points", default="250000,1000000,3000000")
     ap.add_argument("--sv-rate", type=float, default=200.0)
     ap.add_argument("--sv-requests", type=int, default=2000)
@@ -913,6 +916,58 @@ def run_serving(args, prebuilt=None):
     return line
 
 
+def run_sort(args):
+    """rm_sort_pairs_range alone on --sort-pairs random keys of the key bits
+    --sort-bits (seeded), timed with CUDA events per sort (no L2 flush: the
+    keys and the ping-pong buffers exceed L2 from about 5M pairs)."""
+    import torch
+
+    from radiance_meshes_b200 import _capi as C
+
+    torch.cuda.set_device(0)
+    L = C.lib()
+    n = args.sort_pairs
+    begin, end = (int(x) for x in args.sort_bits.split(","))
+    g = torch.Generator(device="cuda").manual_seed(1)
+    hi = torch.randint(0, 1 << max(end - 32, 1), (n,), device="cuda", dtype=torch.int64, generator=g)
+    lo = torch.randint(0, 1 << 31, (n,), device="cuda", dtype=torch.int64, generator=g)
+    keys = ((hi << 32) | lo) & ((1 << end) - 1)
+    vals = torch.arange(n, device="cuda", dtype=torch.int32)
+    ko, vo = torch.empty_like(keys), torch.empty_like(vals)
+    wsn = L.rm_sort_workspace_size(n)
+    ws = torch.empty(wsn, dtype=torch.uint8, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def one():
+        C.check(L.rm_sort_pairs_range(C.ptr(keys), C.ptr(vals), n, None, begin, end, C.ptr(ko), C.ptr(vo),
+                                      C.ptr(ws), wsn, C.ptr(status), C.stream_handle()), "rm_sort_pairs_range")
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        one()
+        b.record()
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    if args.profile_steps:
+        return None
+    passes = (end - begin + 7) // 8
+    ms = float(np.median(times))
+    if begin == 0:
+        assert bool((ko[1:] >= ko[:-1]).all()), "not sorted"
+    assert int(status.item()) == 0
+    return {"metric": "pairs sorted per second", "value": n / (ms * 1e-3) / 1e9, "unit": "G pairs/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64 keys, int32 values",
+            "data": "synthetic", "config": {"workload": f"rm_sort_pairs_range, {n} random keys, bits [{begin},{end}), "
+                                                        f"{passes} passes of 8 bits", "pairs": n},
+            "key_value_gb_s": n * 24 * passes / (ms * 1e-3) / 1e9}
+
+
 def run_default(args):
     """The training line, with the multi-view and serving results nested in
     it (single GPU): their meshes are built in spawned host processes while
@@ -964,6 +1019,8 @@ def main():
         return run_reference(args)
     elif args.workload == "multiview":
         line = run_multiview(args)
+    elif args.workload == "sort":
+        line = run_sort(args)
     else:
         line = run_default(args)
     if line is not None:

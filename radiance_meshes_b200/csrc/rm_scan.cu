@@ -27,12 +27,14 @@ struct ScanWs {
     // followed by uint64_t state[n_tiles]
 };
 
-__device__ __forceinline__ void st_release(uint64_t* p, uint64_t v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+// Look-back states: the flags and the sum share one 64-bit word and nothing
+// else is published through it, so relaxed GPU-scope accesses suffice.
+__device__ __forceinline__ void st_relaxed(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
-__device__ __forceinline__ uint64_t ld_acquire(const uint64_t* p) {
+__device__ __forceinline__ uint64_t ld_relaxed(const uint64_t* p) {
     uint64_t v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
@@ -120,11 +122,11 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const int32_t* __res
             int64_t prefix = 0;
             bool ovf = block_total > (int64_t)INT32_MAX || block_total < 0;
             if (tile != 0) {
-                st_release(&state[tile], kFlagAgg | (ovf ? kFlagOvf : 0ull) | (uint32_t)block_total);
+                st_relaxed(&state[tile], kFlagAgg | (ovf ? kFlagOvf : 0ull) | (uint32_t)block_total);
                 int64_t t = (int64_t)tile - 1;
                 uint32_t budget = spin_limit;
                 while (t >= 0) {
-                    const uint64_t s = ld_acquire(&state[t]);
+                    const uint64_t s = ld_relaxed(&state[t]);
                     const uint64_t flag = s & (3ull << 32);
                     if (flag == 0) {
                         if (!spin_budget(budget)) {
@@ -142,7 +144,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const int32_t* __res
             const int64_t tile_incl = prefix + block_total;
             ovf |= tile_incl > (int64_t)INT32_MAX;
             if (ovf) atomicOr(status, RM_STATUS_OVERFLOW);
-            st_release(&state[tile], kFlagInc | (ovf ? kFlagOvf : 0ull) | (uint32_t)tile_incl);
+            st_relaxed(&state[tile], kFlagInc | (ovf ? kFlagOvf : 0ull) | (uint32_t)tile_incl);
             s_prefix = prefix;
             const int64_t last = (int64_t)tile * kScanTile + kScanTile;
             if (last >= n) *total_dev = tile_incl;

@@ -56,12 +56,15 @@ __host__ SortLayout sort_layout(int64_t n, int npasses) {
     return L;
 }
 
-__device__ __forceinline__ void st_release32(uint32_t* p, uint32_t v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+// Look-back states: the flag and the count share one 32-bit word and nothing
+// else is published through it, so relaxed GPU-scope accesses suffice (no
+// release fence per store, no acquire per poll).
+__device__ __forceinline__ void st_relaxed32(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-__device__ __forceinline__ uint32_t ld_acquire32(const uint32_t* p) {
+__device__ __forceinline__ uint32_t ld_relaxed32(const uint32_t* p) {
     uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -158,7 +161,7 @@ struct PassSmem {
     uint32_t vals[kSortTile];
 };
 
-__global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
+__global__ void __launch_bounds__(kSortThreads, 2) onesweep_kernel(
     const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint64_t* __restrict__ kout,
     uint32_t* __restrict__ vout, int64_t cap, const int64_t* __restrict__ n_dev, int pass, int shift,
     uint32_t dmask, SortHeader* hdr, uint32_t* __restrict__ lookback, uint32_t* status, uint32_t spin_limit) {
@@ -199,8 +202,9 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
         rank[i] = before + __popc(peers & lt);
     }
     __syncthreads();
-    // per digit: exclusive prefix over warps, tile count, look-back
-    uint32_t count = 0;
+    // per digit: exclusive prefix over warps and the tile count, published at
+    // once (the inclusive prefix for tile 0) so that successors can look back
+    uint32_t count = 0, vcount = 0;
     if (threadIdx.x < kRadix) {
         const int d = threadIdx.x;
         uint32_t sum = 0;
@@ -210,34 +214,15 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
             sum += c;
         }
         count = sum;
-        const uint32_t vcount = (d == 255) ? sum - invalid : sum;
+        vcount = (d == 255) ? sum - invalid : sum;
         uint32_t* lb = lookback + (size_t)tile * kRadix + d;
-        uint32_t excl;
         if (tile == 0) {
-            excl = hdr->hist[pass][d];
-            st_release32(lb, kLbInc | ((excl + vcount) & kLbMask));
+            const uint32_t excl = hdr->hist[pass][d];
+            st_relaxed32(lb, kLbInc | ((excl + vcount) & kLbMask));
+            S.global_start[d] = excl;
         } else {
-            st_release32(lb, kLbAgg | (vcount & kLbMask));
-            excl = 0;
-            int64_t t = (int64_t)tile - 1;
-            uint32_t budget = spin_limit;
-            while (t >= 0) {
-                const uint32_t s = ld_acquire32(lookback + (size_t)t * kRadix + d);
-                const uint32_t flag = s & ~kLbMask;
-                if (flag == 0) {
-                    if (!spin_budget(budget)) {
-                        atomicOr(status, RM_STATUS_SORT_TIMEOUT);
-                        break;
-                    }
-                    continue;
-                }
-                excl += s & kLbMask;
-                if (flag == kLbInc) break;
-                --t;
-            }
-            st_release32(lb, kLbInc | ((excl + vcount) & kLbMask));
+            st_relaxed32(lb, kLbAgg | (vcount & kLbMask));
         }
-        S.global_start[d] = excl;
     }
     // exclusive scan of the tile's digit counts -> start of each digit run in smem
     if (threadIdx.x < kRadix) {
@@ -257,11 +242,35 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
         S.tile_off[threadIdx.x] += wpre;
     }
     __syncthreads();
+    // the local scatter needs no global offsets: it runs before the look-back,
+    // so the other warps' scatter overlaps the digit threads' polling
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i) {
         const uint32_t lpos = S.tile_off[dig[i]] + S.warp_hist[warp][dig[i]] + rank[i];
         S.keys[lpos] = key[i];
         S.vals[lpos] = val[i];
+    }
+    if (threadIdx.x < kRadix && tile != 0) {
+        const int d = threadIdx.x;
+        uint32_t excl = 0;
+        int64_t t = (int64_t)tile - 1;
+        uint32_t budget = spin_limit;
+        while (t >= 0) {
+            const uint32_t st = ld_relaxed32(lookback + (size_t)t * kRadix + d);
+            const uint32_t flag = st & ~kLbMask;
+            if (flag == 0) {
+                if (!spin_budget(budget)) {
+                    atomicOr(status, RM_STATUS_SORT_TIMEOUT);
+                    break;
+                }
+                continue;
+            }
+            excl += st & kLbMask;
+            if (flag == kLbInc) break;
+            --t;
+        }
+        st_relaxed32(lookback + (size_t)tile * kRadix + d, kLbInc | ((excl + vcount) & kLbMask));
+        S.global_start[d] = excl;
     }
     __syncthreads();
 #pragma unroll
