@@ -18,9 +18,18 @@
 namespace rm {
 namespace {
 
-constexpr int kSortThreads = 512;
+// Tile shape of a pass (threads x pairs per thread); a build may override it
+// (threads >= 256: one thread per digit).
+#ifndef RM_SORT_THREADS
+#define RM_SORT_THREADS 512
+#endif
+#ifndef RM_SORT_ITEMS
+#define RM_SORT_ITEMS 8
+#endif
+constexpr int kSortThreads = RM_SORT_THREADS;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 8;
+constexpr int kSortItems = RM_SORT_ITEMS;
+static_assert(kSortThreads >= 256, "one thread per 8-bit digit");
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 pairs per CTA
 constexpr int kRadix = 256;
 constexpr int kMaxPasses = 8;
@@ -161,7 +170,7 @@ struct PassSmem {
     uint32_t vals[kSortTile];
 };
 
-__global__ void __launch_bounds__(kSortThreads, 2) onesweep_kernel(
+__global__ void __launch_bounds__(kSortThreads, 1024 / kSortThreads) onesweep_kernel(
     const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint64_t* __restrict__ kout,
     uint32_t* __restrict__ vout, int64_t cap, const int64_t* __restrict__ n_dev, int pass, int shift,
     uint32_t dmask, SortHeader* hdr, uint32_t* __restrict__ lookback, uint32_t* status, uint32_t spin_limit) {
