@@ -789,21 +789,36 @@ __device__ __forceinline__ void warp_sum_columns(const float* red, int lane, flo
     __syncwarp();
 }
 
-// Rows of gl[0..25) as computed by hit_grads_a.
-__device__ __forceinline__ void warp_sum_rows(float* __restrict__ red, const float* gl, int lane,
-                                              float* __restrict__ acc) {
-    float4* row = reinterpret_cast<float4*>(red + lane * kRedStride);
-#pragma unroll
-    for (int c = 0; c < 6; ++c) row[c] = make_float4(gl[4 * c], gl[4 * c + 1], gl[4 * c + 2], gl[4 * c + 3]);
-    row[6] = make_float4(gl[24], 0.f, 0.f, 0.f);
-    warp_sum_columns(red, lane, acc);
-}
-
 // Rows of hit_grads_planes' output: gl[12..25) and the two planes' normal
 // gradients, stored at the planes' columns (ie, ix: -1 for none or a lane
 // without a hit, whose gl[12..25) are zero).
+// As warp_sum_columns for a warp that walked two entries at once: the rows
+// of the lanes in bal_a go to acc_a, the others to acc_b.
+__device__ __forceinline__ void warp_sum_columns_split(const float* red, int lane, uint32_t bal_a,
+                                                       float* __restrict__ acc_a, float* __restrict__ acc_b) {
+    __syncwarp();
+    if (lane < kNGrad) {
+        float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+#pragma unroll
+        for (int r = 0; r < 32; r += 2) {
+            const float v0 = red[r * kRedStride + lane], v1 = red[(r + 1) * kRedStride + lane];
+            const bool in0 = (bal_a >> r) & 1u, in1 = (bal_a >> (r + 1)) & 1u;
+            a0 += in0 ? v0 : 0.f;
+            b0 += in0 ? 0.f : v0;
+            a1 += in1 ? v1 : 0.f;
+            b1 += in1 ? 0.f : v1;
+        }
+        const float sa = a0 + a1, sb = b0 + b1;
+        if (sa != 0.f) atomicAdd(acc_a + lane, sa);
+        if (sb != 0.f) atomicAdd(acc_b + lane, sb);
+    }
+    __syncwarp();
+}
+
+// acc_b != nullptr: the rows of the lanes outside bal_a go to acc_b.
 __device__ __forceinline__ void warp_sum_rows_planes(float* __restrict__ red, const float* gl, f3 dne, f3 dnx,
-                                                     int ie, int ix, int lane, float* __restrict__ acc) {
+                                                     int ie, int ix, int lane, float* __restrict__ acc,
+                                                     uint32_t bal_a = 0u, float* __restrict__ acc_b = nullptr) {
     float* rowf = red + lane * kRedStride;
     float4* row = reinterpret_cast<float4*>(rowf);
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -823,7 +838,10 @@ __device__ __forceinline__ void warp_sum_rows_planes(float* __restrict__ red, co
         rowf[3 * ix + 1] = dnx.y;
         rowf[3 * ix + 2] = dnx.z;
     }
-    warp_sum_columns(red, lane, acc);
+    if (acc_b)
+        warp_sum_columns_split(red, lane, bal_a, acc, acc_b);
+    else
+        warp_sum_columns(red, lane, acc);
 }
 
 // Adjoint of one hit (the Slang autodiff of update_alpha_out,
@@ -998,7 +1016,7 @@ __device__ __forceinline__ void flush_entries(int n, const float4 (*srec)[kRecFl
 template <int NT, int B>
 struct BwdDenseSmem {
     float4 srec[B][kRecFloat4];
-    float4 red[NT >= 32 ? NT / 32 : 1][NT >= 32 ? 32 * kRedStride / 4 : 1];  // warp_sum_rows rows, per warp
+    float4 red[NT >= 32 ? NT / 32 : 1][NT >= 32 ? 32 * kRedStride / 4 : 1];  // warp_sum_rows_planes rows, per warp
     int32_t sid[B];
     float sacc[B][kNGrad];
     int32_t smax[WarpShape<NT>::kWarps];
@@ -1110,13 +1128,37 @@ __device__ __forceinline__ void bwd_dense_item(
             S.srec[j][c] = record_part(recs, S.sid[j], c);
         }
         __syncthreads();
-        for (int jj = nk - 1; jj >= 0; --jj) {
+        for (int jj = nk - 1; jj >= 0;) {
             const int off = lo + S.cidx[jj] - rg.x;
             // with the forward's masks, only its hits are revisited
             const uint32_t hw = (off >> 5) == kb0 ? hw0 : hw1;
-            const bool act = inside && off < nc && ((hw >> (off & 31)) & 1u);
-            if (!__any_sync(kMask, act)) continue;
-            const float4* q = S.srec[jj];
+            const bool act_a = inside && off < nc && ((hw >> (off & 31)) & 1u);
+            const uint32_t bal_a = __ballot_sync(kMask, act_a);
+            if (!bal_a) {
+                --jj;
+                continue;
+            }
+            // When no pixel of the warp walks both this entry and the one
+            // before it, the warp takes both at once: each lane walks the one
+            // it hits (its own order is unchanged), and the partials go to
+            // the two entries' accumulators by lane.
+            bool act_b = false;
+            uint32_t bal_b = 0u;
+            if constexpr (NT >= 32) {
+                if (jj >= 1) {
+                    const int off_b = lo + S.cidx[jj - 1] - rg.x;
+                    const uint32_t hwb = (off_b >> 5) == kb0 ? hw0 : hw1;
+                    act_b = inside && off_b < nc && ((hwb >> (off_b & 31)) & 1u);
+                    bal_b = __ballot_sync(kMask, act_b);
+                    if (bal_a & bal_b) {
+                        act_b = false;
+                        bal_b = 0u;
+                    }
+                }
+            }
+            const bool act = act_a || act_b;
+            const int je = act_b ? jj - 1 : jj;
+            const float4* q = S.srec[je];
             float gl[kNGrad];
 #pragma unroll
             for (int k = 0; k < kNGrad; ++k) gl[k] = 0.f;
@@ -1149,7 +1191,8 @@ __device__ __forceinline__ void bwd_dense_item(
             if (__any_sync(kMask, hit)) {
                 if constexpr (NT >= 32) {
                     warp_sum_rows_planes(reinterpret_cast<float*>(S.red[warp]), gl, dne, dnx, hit ? is.ie : -1,
-                                         hit ? is.ix : -1, lane, S.sacc[jj]);
+                                         hit ? is.ix : -1, lane, S.sacc[jj], bal_a,
+                                         bal_b ? S.sacc[jj - 1] : nullptr);
                 } else {
                     using RS = ReduceScatter<kNGrad, WarpShape<NT>::kTopOffset>;
                     int slot = 0;
@@ -1159,6 +1202,7 @@ __device__ __forceinline__ void bwd_dense_item(
                         if (slot + r < kNGrad && gl[r] != 0.f) atomicAdd(&S.sacc[jj][slot + r], gl[r]);
                 }
             }
+            jj -= bal_b ? 2 : 1;
         }
         __syncthreads();
         flush_entries<NT, B>(nk, S.srec, S.sid, S.sacc, indices, gverts, gcv);
@@ -1176,7 +1220,7 @@ __device__ __forceinline__ void bwd_dense_item(
 template <int B>
 struct BwdTmaSmem {
     float4 srec[2][B][kRecFloat4];
-    float4 red[2][32 * kRedStride / 4];  // warp_sum_rows rows, per warp
+    float4 red[2][32 * kRedStride / 4];  // warp_sum_rows_planes rows, per warp
     float sacc[B][kNGrad];
     int32_t sid[2][B];
     uint8_t cidx[2][B];
