@@ -241,7 +241,7 @@ def stage_bytes(T, V, T_vis, P, G, Pb, Gb, Npx):
     }
 
 
-def run_b200(args):
+def run_b200(args, after_gpu_timing=None):
     import torch
     import torch.distributed as dist
 
@@ -514,6 +514,8 @@ def run_b200(args):
         "e2e": e2e, "roofline": roof, "stages_ms": per_stage, "stages_pass_steps": n_break,
         "gpu_launches": int(launches), "clocks": clocks.summary(),
     }
+    if after_gpu_timing is not None:  # every GPU-timed measurement of this line is done
+        after_gpu_timing()
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(mesh, view, args.cpu_seconds)
     return line
@@ -970,18 +972,24 @@ def run_sort(args):
 
 def run_default(args):
     """The training line, with the multi-view and serving results nested in
-    it (single GPU): their meshes are built in spawned host processes while
-    the training step is measured."""
+    it (single GPU): their meshes are built in spawned host processes, started
+    after the training line's GPU timings, while its CPU baseline runs."""
     import multiprocessing as mp
 
     world, rank, local = dist_env()
     extras = world == 1 and not args.no_extras and not args.profile_steps
     pool = jobs = None
+    spec = None
     if extras:
         counts = [int(x) for x in args.sv_points.split(",")]
         spec = [(args.mv_points, 3)] + list(zip(counts, [4, 5, 6][:len(counts)]))
-        # one thread per builder (the variables reach the spawned processes
-        # before their numpy loads), at the lowest priority
+
+    def start_builders():
+        """Mesh builders for the nested rows, started once the training line's
+        GPU timings are taken (they would compete with its host-side launches):
+        one thread each (the variables reach the spawned processes before their
+        numpy loads), at the lowest priority, beside the CPU baseline."""
+        nonlocal pool, jobs
         saved = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")}
         os.environ.update({k: "1" for k in saved})
         try:
@@ -993,8 +1001,9 @@ def run_default(args):
                 else:
                     os.environ[k] = v
         jobs = pool.map_async(_mesh_job, spec)
+
     try:
-        line = run_b200(args)
+        line = run_b200(args, after_gpu_timing=start_builders if extras else None)
         if line is None or not extras:
             return line
         t0 = time.perf_counter()
