@@ -11,10 +11,14 @@ circumcenters and vertices.
 """
 from __future__ import annotations
 
+import collections
+import ctypes
+
 import torch
 
 from . import _capi as C
 from . import rasterizer as R
+from .camera import _key_of
 
 __all__ = ["activate_output", "ActivateOutput"]
 
@@ -66,11 +70,26 @@ class ActivateOutput(torch.autograd.Function):
                 None, gcc, gv.reshape(vs), None)
 
 
-def _cam3(camera_center):
-    import ctypes
+_CAM3: "collections.OrderedDict" = collections.OrderedDict()
 
+
+def _cam3(camera_center):
+    """The camera centre as three host floats.  Reading a device tensor waits
+    on the stream, so the values are cached per tensor (identity, storage and
+    in-place version, with the tensor held by the cache, as camera.tcam_to_struct
+    does): a training loop that passes the same camera tensor every step reads
+    it once."""
+    key = _key_of(camera_center)
+    hit = _CAM3.get(key)
+    if hit is not None:
+        _CAM3.move_to_end(key)
+        return hit[1]
     vals = [float(x) for x in torch.as_tensor(camera_center).detach().reshape(-1)[:3].cpu()]
-    return (ctypes.c_float * 3)(*vals)
+    out = (ctypes.c_float * 3)(*vals)
+    _CAM3[key] = (camera_center, out)
+    if len(_CAM3) > 64:
+        _CAM3.popitem(last=False)
+    return out
 
 
 def activate_output(camera_center, density, rgb, grd, sh, indices, circumcenters, vertices, current_sh_deg: int,
