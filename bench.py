@@ -70,8 +70,8 @@ def parse():
     ap.add_argument("--sv-rate", type=float, default=200.0)
     ap.add_argument("--sv-requests", type=int, default=2000)
     ap.add_argument("--sv-warmup", type=int, default=200)
-    ap.add_argument("--sv-streams", type=int, default=4)
-    ap.add_argument("--sv-max-views", type=int, default=8)
+    ap.add_argument("--sv-streams", type=int, default=2, help="concurrent batches of the server")
+    ap.add_argument("--sv-max-views", type=int, default=4, help="views per batch of the server")
     ap.add_argument("--sv-tile", type=int, default=0, help="tile size (0: autotuned on the middle mesh)")
     ap.add_argument("--sv-low-rate", type=float, default=120.0,
                     help="a second Poisson run at this rate (0: none): latency below saturation")

@@ -123,12 +123,15 @@ class Server:
     """Continuous-batching render server on one GPU.
 
     meshes: ResidentMesh objects; streams: concurrent batches; max_views:
-    views per batch (<= batch.MAX_VIEWS); hbm_budget: bytes the in-flight
+    views per batch (<= batch.MAX_VIEWS).  The defaults (2 concurrent batches
+    of at most 4 views) gave the steadiest tail near capacity on the
+    three-mesh serving workload: with 4 batches of up to 8 views, a backlog,
+    once formed, grew the batches and drained slowly.  hbm_budget: bytes the in-flight
     batches may hold (default: half the free memory at start); tile:
     tile size of every render; fwd_flags: blend launch flags (autotune.flags).
     """
 
-    def __init__(self, meshes: Sequence[ResidentMesh], streams: int = 4, max_views: int = 8,
+    def __init__(self, meshes: Sequence[ResidentMesh], streams: int = 2, max_views: int = 4,
                  hbm_budget: int | None = None, tile: int = 16, fwd_flags: int = 0, pair_headroom: float = 1.25,
                  keep_outputs: bool = True, device=None, fine_shift: int = 0):
         self.device = torch.device(device or "cuda")
