@@ -28,6 +28,7 @@ render call of that path.
 from __future__ import annotations
 
 import collections
+import gc
 import math
 import time
 from dataclasses import dataclass, field
@@ -302,6 +303,18 @@ class Server:
         the wall clock passes its arrival time (relative to now); otherwise
         all requests are submitted at once in arrival order."""
         reqs = sorted(requests, key=lambda r: r.arrival)
+        # a collector pause in the middle of a trace delays every launch
+        # behind it: collect once, then freeze what exists (the meshes, the
+        # process's modules), so that collections during the trace only walk
+        # the objects the trace itself creates
+        gc.collect()
+        gc.freeze()
+        try:
+            return self._run_trace(reqs, realtime)
+        finally:
+            gc.unfreeze()
+
+    def _run_trace(self, reqs, realtime: bool) -> list[RenderResult]:
         start = self.now()
         for r in reqs:
             r.arrival += start
