@@ -252,6 +252,18 @@ RM_API int rm_depth_order(const int32_t* tiles_touched, const float* vs, int64_t
                           int64_t* keys, int32_t* values, int64_t* n_visible_dev,
                           void* workspace, size_t workspace_bytes, uint32_t* status_dev,
                           void* stream);
+/*
+ * The pair count of a frame before its lists are built: out[0] = the sum of
+ * the positive tiles_touched (int64), the number the reference reads back
+ * as the last inclusive offset (delaunay_rasterization/internal/tile_shader_slang.py:38-44)
+ * and the count that steps 1-4 above emit and sort; out[1] = the status word
+ * *status_dev (NULL: 0) as the work queued before this call left it, so one
+ * read of out gives both.  Reading out while steps 1-2 run lets the caller
+ * size the pair buffers exactly before it queues steps 3-4.  The caller
+ * compares out[0] with INT32_MAX (the lists' offsets are int32).
+ */
+RM_API int rm_count_pairs(const int32_t* tiles_touched, int64_t n_tets, const uint32_t* status_dev,
+                          int64_t* out, void* stream);
 RM_API size_t rm_emit_ordered_workspace_size(int64_t n_tets);
 RM_API int rm_emit_pairs_ordered(const float* vs, const int32_t* rect, const int32_t* tiles_touched,
                                  const int32_t* order, int64_t n_tets, const int64_t* n_items_dev,

@@ -80,6 +80,7 @@ SIGNATURES = {
     "rm_sort_pairs_range": (ctypes.c_int, [vp, vp, i64, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, sz, vp, vp]),
     "rm_depth_order_workspace_size": (sz, [i64]),
     "rm_depth_order": (ctypes.c_int, [vp, vp, i64, vp, vp, vp, vp, sz, vp, vp]),
+    "rm_count_pairs": (ctypes.c_int, [vp, i64, vp, vp, vp]),
     "rm_emit_ordered_workspace_size": (sz, [i64]),
     "rm_emit_pairs_ordered": (ctypes.c_int, [vp, vp, vp, vp, i64, vp, i32, i64, vp, vp, vp, vp, sz, vp, vp]),
     "rm_blend_workspace_size": (sz, [i64, i64]),

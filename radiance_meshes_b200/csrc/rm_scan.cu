@@ -378,6 +378,32 @@ __global__ void __launch_bounds__(256) ranges_kernel(const int64_t* __restrict__
     if (i == n - 1) ranges[2 * (int64_t)cur + 1] = (int32_t)n;
 }
 
+// rm_count_pairs: grid-stride sums of the positive tile counts, one 64-bit
+// atomic per block into out[0] (zeroed by the host call before the launch);
+// block 0 also copies the status word into out[1].
+constexpr int kCountThreads = 256;
+
+__global__ void __launch_bounds__(kCountThreads) count_pairs_kernel(const int32_t* __restrict__ tiles, int64_t n,
+                                                                    const uint32_t* __restrict__ status,
+                                                                    int64_t* __restrict__ out) {
+    __shared__ int64_t part[kCountThreads / 32];
+    int64_t sum = 0;
+    const int64_t stride = (int64_t)gridDim.x * kCountThreads;
+    for (int64_t i = (int64_t)blockIdx.x * kCountThreads + threadIdx.x; i < n; i += stride)
+        sum += max(__ldg(tiles + i), 0);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t b = 0;
+#pragma unroll
+        for (int w = 0; w < kCountThreads / 32; ++w) b += part[w];
+        if (b) atomicAdd((unsigned long long*)out, (unsigned long long)b);
+        if (blockIdx.x == 0) out[1] = status ? (int64_t)*status : 0;
+    }
+}
+
 }  // namespace
 }  // namespace rm
 
@@ -532,6 +558,19 @@ int rm_depth_order(const int32_t* tiles_touched, const float* vs, int64_t n_tets
     const unsigned blocks = (unsigned)((n_tets + 255) / 256);
     rm::depth_scatter_kernel<<<blocks, 256, 0, s>>>(tiles_touched, vs, n_tets, incl, keys, values);
     return rm_host::check_launch("rm_depth_order");
+}
+
+int rm_count_pairs(const int32_t* tiles_touched, int64_t n_tets, const uint32_t* status_dev, int64_t* out,
+                   void* stream) {
+    if (n_tets < 0) return rm_host::fail(RM_EINVAL, "rm_count_pairs: negative size");
+    if (!out || (n_tets > 0 && !tiles_touched)) return rm_host::fail(RM_EINVAL, "rm_count_pairs: NULL pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(int64_t), s);
+    if (e != cudaSuccess) return rm_host::fail(RM_ECUDA, "rm_count_pairs: %s", cudaGetErrorString(e));
+    const int64_t want = (n_tets + rm::kCountThreads * 8 - 1) / (rm::kCountThreads * 8);
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, 148 * 8));
+    rm::count_pairs_kernel<<<blocks, rm::kCountThreads, 0, s>>>(tiles_touched, n_tets, status_dev, out);
+    return rm_host::check_launch("rm_count_pairs");
 }
 
 size_t rm_emit_ordered_workspace_size(int64_t n_tets) { return rm_depth_order_workspace_size(n_tets); }

@@ -287,7 +287,35 @@ def project_bwd(indices, vertices, cam: RMCamera, tiles, grad_vs, grad_cc, grad_
     return grad_vertices
 
 
-_PAIR_GUESS: dict = {}  # device -> pair count of the last frame built there
+_PAIR_GUESS: dict = {}  # device -> pair count of the last frame built there (reference order of work)
+_SIDE: dict = {}  # device -> (side stream, pinned int64 [2], its numpy view) for the pair-count read
+
+
+def _count_read_start(count: torch.Tensor):
+    """Copy ``count`` (int64 [2] on the device: pair count, status word) to
+    pinned host memory on a side stream that waits for the work queued so
+    far only, so the frame's stream goes on with what is queued after this
+    call while the host waits in _count_read_finish."""
+    dev = count.device
+    st = _SIDE.get(dev)
+    if st is None:
+        hb = torch.zeros(2, dtype=torch.int64, pin_memory=True)
+        st = (torch.cuda.Stream(device=dev), hb, hb.numpy())
+        _SIDE[dev] = st
+    side, hb, hn = st
+    side.wait_stream(torch.cuda.current_stream(dev))
+    count.record_stream(side)
+    with torch.cuda.stream(side):
+        hb.copy_(count, non_blocking=True)
+    done = torch.cuda.Event()
+    done.record(side)
+    return done, hn
+
+
+def _count_read_finish(pending) -> tuple[int, int]:
+    done, hn = pending
+    done.synchronize()
+    return int(hn[0]), int(hn[1]) & 0xffffffff
 _LISTS = {"depth_first": True}
 
 
@@ -305,20 +333,24 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
 
     The pair count P is read back to the host once (the reference reads it
     three times: tile_shader_slang.py:38-44,68), together with the frame's
-    status word (frame_status): a bad index, a non-finite vertex, a pair
-    count beyond int32 or a look-back that gave up raises
-    ``_capi.DeviceStatusError`` there, where the reference asserts on the
-    host (tile_shader_slang.py:78).  After the first frame on a device, the
-    pair buffers are sized from the previous frame's count (plus a quarter)
-    and emission, sort and ranges are queued before P is read, so the GPU
-    keeps working while the host waits for it; the kernels take the pair
-    count from the device.  Should P exceed that capacity, the frame is built
-    again with buffers of exactly P (and its status read once more).  The
-    returned tensors are the first P entries of those buffers.
+    status word (frame_status): a bad index, a non-finite vertex or a pair
+    count beyond int32 raises ``_capi.DeviceStatusError`` there, where the
+    reference asserts on the host (tile_shader_slang.py:78).
 
-    By default the lists are built depth first (use_depth_first_lists);
-    keep_debug builds them in the reference's order of work and also returns
-    the tet-order offsets and the emitted keys and values."""
+    By default the lists are built depth first (use_depth_first_lists): P is
+    counted right after the projection (rm_count_pairs) and read on a side
+    stream while the GPU orders the visible tets by depth; the pair buffers
+    then get exactly P entries, emission, sort and ranges are queued, and the
+    call returns while they run, so the host's next work overlaps them.  Bits
+    that those later kernels set (a look-back that gave up) surface at the
+    next readback of the device: the next frame's, or check_status.
+
+    keep_debug builds the lists in the reference's order of work and also
+    returns the tet-order offsets and the emitted keys and values; that path
+    sizes its buffers from the previous frame's count (plus a quarter),
+    queues emission, sort and ranges before P is read, builds the frame again
+    at exactly P should P exceed that, and reads the status word after all of
+    its kernels."""
     pool = pool or _POOL
     dev = tiles.device
     T = tiles.shape[0]
@@ -331,6 +363,11 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
     depth_first = _LISTS["depth_first"] and not keep_debug and T > 0
 
     if depth_first:
+        # the pair count and the status word as the projection left them,
+        # read while the visible tets are ordered by depth
+        count = torch.empty(2, dtype=torch.int64, device=dev)
+        _call("rm_count_pairs", lambda: L.rm_count_pairs(C.ptr(tiles), T, C.ptr(status), C.ptr(count), s))
+        pending = _count_read_start(count)
         # visible tets by depth, once; the pairs then need the tile bits only
         dkeys = torch.empty(T, dtype=torch.int64, device=dev)
         dvals = torch.empty(T, dtype=torch.int32, device=dev)
@@ -381,6 +418,14 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
         _call("rm_tile_ranges", lambda: L.rm_tile_ranges(C.ptr(sk), cap, C.ptr(n_dev), C.ptr(ranges), G, s))
         return keys, vals, sk, sv, ranges
 
+    if depth_first:
+        P, bits = _count_read_finish(pending)
+        raise_status(bits, status, "vertex_and_tile_shader")
+        if P > 0x7FFFFFFF:  # the offsets are int32, as the reference's cumsum
+            raise C.DeviceStatusError(C.RM_STATUS_OVERFLOW, "vertex_and_tile_shader")
+        keys, vals, sk, sv, ranges = pairs(P, total)
+        return TileLists(sv, ranges, P, sorted_keys=sk)
+
     key = str(dev)
     guess = _PAIR_GUESS.get(key)
     out = None
@@ -391,8 +436,6 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
         if P > cap:
             out = None
     else:
-        if depth_first:  # the ordered scan gives the count; nothing is emitted at capacity 0
-            pairs(0, total)
         P, bits = _read_frame(total, status)
     if out is None and bits & C.RM_STATUS_CAPACITY:
         # expected: the buffers were sized before P was known; rebuilt at exactly P below
@@ -401,7 +444,7 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
             status.zero_()
     raise_status(bits, status, "vertex_and_tile_shader")
     if out is None:
-        out = pairs(P, None if not depth_first else total)
+        out = pairs(P, None)
         # the exact-size sort reports now, not at the next frame
         _, bits = _read_frame(total, status)
         raise_status(bits, status, "vertex_and_tile_shader")

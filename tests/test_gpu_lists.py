@@ -19,10 +19,10 @@ pytestmark = pytest.mark.gpu
 
 def _both(tiles, rect, vs, cam):
     ref = R.build_tile_lists(tiles, rect, vs, cam, keep_debug=True)
-    R._PAIR_GUESS.clear()  # the first-frame path of the depth-first build
     a = R.build_tile_lists(tiles, rect, vs, cam)
-    b = R.build_tile_lists(tiles, rect, vs, cam)  # the pipelined path (capacity from the previous frame)
+    b = R.build_tile_lists(tiles, rect, vs, cam)  # a second frame: the scratch pool's buffers reused
     torch.cuda.synchronize()
+    R.check_status(tiles.shape[0], tiles.device)  # what the kernels after the count read reported
     for got in (a, b):
         assert got.n_pairs == ref.n_pairs
         assert torch.equal(got.sorted_ids, ref.sorted_ids)
