@@ -466,7 +466,7 @@ class FineLists:
     counts fine-list entries, which only the backward pass reads."""
     shift: int
     cam: RMCamera  # the fine camera
-    coarse_key: tuple
+    coarse_key: bytes
     sorted_ids: torch.Tensor  # capacity entries; the first n_pairs are used
     ranges: torch.Tensor
     total: torch.Tensor  # [1] int64 on the device
@@ -483,7 +483,7 @@ class PendingFineLists:
     ray jitter of the blend, so it runs in fine_lists_of (once per jitter)."""
     shift: int
     coarse_cam: RMCamera
-    coarse_key: tuple
+    coarse_key: bytes
     ranges: torch.Tensor
     footprint: torch.Tensor
     sorted_keys: torch.Tensor
@@ -506,9 +506,9 @@ def fine_lists_enabled() -> bool:
     return _FINE["enabled"]
 
 
-def _cam_key(cam: RMCamera) -> tuple:
-    return (cam.image_height, cam.image_width, cam.tile_height, cam.tile_width, cam.grid_height, cam.grid_width,
-            tuple(cam.world_view), tuple(cam.K), tuple(cam.cam_pos), cam.min_t)
+def _cam_key(cam: RMCamera) -> bytes:
+    """Every field of the camera record, as its raw bytes."""
+    return bytes(cam)
 
 
 def attach_fine_lists(sorted_ids: torch.Tensor, ranges: torch.Tensor, cam: RMCamera, fine_shift: int,
