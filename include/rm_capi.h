@@ -63,12 +63,13 @@ extern "C" {
 #define RM_STATUS_OVERFLOW 0x40u      /* the pair count exceeds INT32_MAX (int32 offsets)     */
 
 /*
- * Pinhole camera.  Mirrors the reference's TensorCamera/Camera
+ * Camera.  Mirrors the reference's TensorCamera/Camera
  * (delaunay_rasterization/internal/slang/camera.slang:13-76) as filled by
  * utils/train_util.py:31-38 and data/camera.py:72-91.
  * world_view is row-major world->camera (tcam['world_view_transform']),
- * K is row-major 3x3 intrinsics.  Only camera_type 0 (perspective) with zero
- * distortion is supported; anything else is rejected with RM_EINVAL.
+ * K is row-major 3x3 intrinsics.  camera_type 0 (perspective) and 1
+ * (fisheye) are supported, each with the radial/tangential distortion
+ * (k1, k2, p1, p2); any other camera_type is rejected with RM_EINVAL.
  */
 typedef struct rm_camera {
     float world_view[16];
@@ -258,9 +259,12 @@ RM_API int rm_depth_order(const int32_t* tiles_touched, const float* vs, int64_t
  * as the last inclusive offset (delaunay_rasterization/internal/tile_shader_slang.py:38-44)
  * and the count that steps 1-4 above emit and sort; out[1] = the status word
  * *status_dev (NULL: 0) as the work queued before this call left it, so one
- * read of out gives both.  Reading out while steps 1-2 run lets the caller
- * size the pair buffers exactly before it queues steps 3-4.  The caller
- * compares out[0] with INT32_MAX (the lists' offsets are int32).
+ * read of out gives both.  Read on another stream, out tells the caller P
+ * without waiting for the list build: it can size the pair buffers exactly
+ * before it queues steps 3-4, or queue them on buffers sized from an
+ * estimate and check the estimate against out[0] (steps 3-4 set
+ * RM_STATUS_CAPACITY when it was too small).  The caller compares out[0]
+ * with INT32_MAX (the lists' offsets are int32).
  */
 RM_API int rm_count_pairs(const int32_t* tiles_touched, int64_t n_tets, const uint32_t* status_dev,
                           int64_t* out, void* stream);

@@ -24,7 +24,9 @@ __all__ = ["activate_output", "ActivateOutput"]
 
 
 def _prep(t, dtype=torch.float32):
-    return t.detach().to(dtype).contiguous()
+    """t detached, as a contiguous tensor of dtype (no copy when it is one)."""
+    t = t.detach()
+    return t if (t.dtype == dtype and t.is_contiguous()) else t.to(dtype).contiguous()
 
 
 class ActivateOutput(torch.autograd.Function):

@@ -338,11 +338,14 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
     reference asserts on the host (tile_shader_slang.py:78).
 
     By default the lists are built depth first (use_depth_first_lists): P is
-    counted right after the projection (rm_count_pairs) and read on a side
-    stream while the GPU orders the visible tets by depth; the pair buffers
-    then get exactly P entries, emission, sort and ranges are queued, and the
-    call returns while they run, so the host's next work overlaps them.  Bits
-    that those later kernels set (a look-back that gave up) surface at the
+    counted right after the projection (rm_count_pairs) and copied to the
+    host on a side stream.  After the first frame on a device, the pair
+    buffers are sized from the previous frame's count (plus a quarter) and
+    the whole build is queued before P is read, so the host goes on while
+    the GPU builds the lists; a frame with more pairs than that is built
+    again at exactly P.  The first frame waits for the count alone (while the
+    GPU orders the visible tets by depth) and builds at exactly P.  Bits that
+    the kernels after the count set (a look-back that gave up) surface at the
     next readback of the device: the next frame's, or check_status.
 
     keep_debug builds the lists in the reference's order of work and also
@@ -418,16 +421,30 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
         _call("rm_tile_ranges", lambda: L.rm_tile_ranges(C.ptr(sk), cap, C.ptr(n_dev), C.ptr(ranges), G, s))
         return keys, vals, sk, sv, ranges
 
+    key = str(dev)
+    guess = _PAIR_GUESS.get(key)
     if depth_first:
+        out = None
+        if guess is not None:  # queued before the count is read: the host does not wait for the GPU
+            cap = guess + guess // 4 + 4096
+            out = pairs(cap, total)
         P, bits = _count_read_finish(pending)
         raise_status(bits, status, "vertex_and_tile_shader")
         if P > 0x7FFFFFFF:  # the offsets are int32, as the reference's cumsum
             raise C.DeviceStatusError(C.RM_STATUS_OVERFLOW, "vertex_and_tile_shader")
-        keys, vals, sk, sv, ranges = pairs(P, total)
-        return TileLists(sv, ranges, P, sorted_keys=sk)
+        _PAIR_GUESS[key] = P
+        if out is not None and P > cap:
+            # expected: the emission into the smaller buffers set the capacity
+            # bit; it is cleared (other bits stay for the next readback), and
+            # the pairs are built again at exactly P
+            torch.cuda.current_stream(dev).synchronize()
+            status.fill_(int(status.item()) & ~C.RM_STATUS_CAPACITY)
+            out = None
+        if out is None:
+            out = pairs(P, total)
+        keys, vals, sk, sv, ranges = out
+        return TileLists(sv[:P], ranges, P, sorted_keys=sk[:P])
 
-    key = str(dev)
-    guess = _PAIR_GUESS.get(key)
     out = None
     if guess is not None:
         cap = guess + guess // 4 + 4096

@@ -19,8 +19,9 @@ pytestmark = pytest.mark.gpu
 
 def _both(tiles, rect, vs, cam):
     ref = R.build_tile_lists(tiles, rect, vs, cam, keep_debug=True)
+    R._PAIR_GUESS.clear()  # the first-frame path: the count read, then buffers of exactly P
     a = R.build_tile_lists(tiles, rect, vs, cam)
-    b = R.build_tile_lists(tiles, rect, vs, cam)  # a second frame: the scratch pool's buffers reused
+    b = R.build_tile_lists(tiles, rect, vs, cam)  # capacity from the previous frame, all queued before the read
     torch.cuda.synchronize()
     R.check_status(tiles.shape[0], tiles.device)  # what the kernels after the count read reported
     for got in (a, b):

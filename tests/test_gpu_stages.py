@@ -181,11 +181,14 @@ def test_fine_lists_split_matches_restatement(cuda, tile, jit):
     assert n < 0.9 * n_box
 
 
-def test_pair_buffers_sized_from_the_previous_frame(cuda):
+@pytest.mark.parametrize("depth_first", [False, True])
+def test_pair_buffers_sized_from_the_previous_frame(cuda, depth_first):
     """build_tile_lists sizes the pair buffers from the previous frame's count
     and queues emission, sort and ranges before reading P; a frame with many
     more pairs than the last is rebuilt at its exact size.  The lists equal
-    those built with exactly sized buffers, whichever path a frame takes."""
+    those built with exactly sized buffers, whichever path a frame takes, in
+    the reference's order of work and depth first, and the capacity bit of an
+    outgrown frame is not left for the next readback."""
     from radiance_meshes_b200 import rasterizer as R
     from radiance_meshes_b200 import scenes
     from radiance_meshes_b200.camera import tcam_to_struct
@@ -198,7 +201,7 @@ def test_pair_buffers_sized_from_the_previous_frame(cuda):
         i = torch.from_numpy(mesh.indices).cuda()
         v = torch.from_numpy(mesh.vertices).cuda()
         tiles, rect, vs, cc = R.project_fwd(i, v, cam)
-        L = R.build_tile_lists(tiles, rect, vs, cam, keep_debug=True)
+        L = R.build_tile_lists(tiles, rect, vs, cam, keep_debug=not depth_first)
         return L.sorted_ids.clone(), L.ranges.clone(), L.sorted_keys.clone()
 
     def exact(mesh, view):
@@ -212,3 +215,4 @@ def test_pair_buffers_sized_from_the_previous_frame(cuda):
         for a, b in zip(got, ref):
             assert torch.equal(a, b)
     assert ref_big[0].shape[0] > 2 * ref_small[0].shape[0]
+    R.check_status(len(small_mesh.indices), torch.device("cuda"))
