@@ -216,3 +216,24 @@ def test_pair_buffers_sized_from_the_previous_frame(cuda, depth_first):
             assert torch.equal(a, b)
     assert ref_big[0].shape[0] > 2 * ref_small[0].shape[0]
     R.check_status(len(small_mesh.indices), torch.device("cuda"))
+
+
+@pytest.mark.parametrize("n", [0, 1, 1000, 1_000_003])
+def test_count_pairs_sums_positive_counts_and_snapshots_status(cuda, n):
+    """rm_count_pairs: out[0] = the sum of the positive tile counts (int64),
+    out[1] = the status word as the work queued before it left it."""
+    from radiance_meshes_b200 import _capi as C
+
+    rng = np.random.default_rng(n + 7)
+    tiles_h = rng.integers(-3, 40, size=n).astype(np.int32)
+    tiles = torch.from_numpy(tiles_h).cuda()
+    status = torch.tensor([C.RM_STATUS_BAD_INDEX | C.RM_STATUS_NONFINITE], dtype=torch.int32, device="cuda")
+    out = torch.full((2,), -5, dtype=torch.int64, device="cuda")
+    C.check(C.lib().rm_count_pairs(C.ptr(tiles) if n else None, n, C.ptr(status), C.ptr(out), C.stream_handle()),
+            "rm_count_pairs")
+    got = out.cpu().numpy()
+    assert int(got[0]) == int(np.maximum(tiles_h.astype(np.int64), 0).sum())
+    assert int(got[1]) == C.RM_STATUS_BAD_INDEX | C.RM_STATUS_NONFINITE
+    C.check(C.lib().rm_count_pairs(C.ptr(tiles) if n else None, n, None, C.ptr(out), C.stream_handle()),
+            "rm_count_pairs")
+    assert int(out[1].item()) == 0
