@@ -110,7 +110,8 @@ def frame_status(n_tets: int, device, pool: ScratchPool | None = None) -> torch.
     their RM_STATUS_* bits into: the first 4 bytes of the frame's scan
     workspace, whose other bytes every scan resets.  Projection, scan, sort
     and the fine-list split all report there, and build_tile_lists reads it
-    together with the pair count."""
+    together with the pair count (rm_count_pairs takes both right after the
+    projection; the later stages' bits surface at the next readback)."""
     pool = pool or _POOL
     ws = pool.get("scan", C.lib().rm_scan_workspace_size(n_tets), device, zero_head=True)
     return ws[:4].view(torch.int32)
