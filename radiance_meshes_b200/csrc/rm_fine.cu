@@ -23,13 +23,6 @@ namespace {
 
 constexpr int kFineThreads = 1024;
 constexpr int kFineWarps = kFineThreads / 32;
-// The writing pass: one CTA per coarse list, chunks of kWriteThreads entries.
-#ifndef RM_FINE_WRITE_THREADS
-#define RM_FINE_WRITE_THREADS 1024
-#endif
-constexpr int kWriteThreads = RM_FINE_WRITE_THREADS;
-constexpr int kWriteWarps = kWriteThreads / 32;
-static_assert(kWriteThreads >= 64 && kWriteThreads <= 1024 && kWriteThreads % 32 == 0, "whole warps, at most 32");
 
 constexpr int kBoundsThreads = 256;
 constexpr int kBoundsBlocks = 296;
@@ -171,14 +164,14 @@ __global__ void __launch_bounds__(256) fine_bits_kernel(
 // warp ballots and a warp-0 scan of the per-warp counts per chunk of 1024
 // entries), and the fine ranges.
 template <bool PACKED, int FS>
-__global__ void __launch_bounds__(kWriteThreads, 2048 / kWriteThreads) fine_write_kernel(
+__global__ void __launch_bounds__(kFineThreads, 2) fine_write_kernel(
     const int32_t* __restrict__ ids, const int2* __restrict__ ranges,
     const typename FineBits<FS>::type* __restrict__ bits_in, const __grid_constant__ ViewSet views,
     const int32_t* __restrict__ counts, const int32_t* __restrict__ incl, int32_t* __restrict__ fine_ids,
     int64_t capacity, int2* __restrict__ fine_ranges, uint32_t* status) {
     constexpr int Q = (1 << FS) * (1 << FS);
-    __shared__ uint32_t wcnt[kWriteWarps][Q];  // this chunk's count per (warp, fine tile)
-    __shared__ uint32_t wpre[kWriteWarps][Q];  // the warp's first position per fine tile
+    __shared__ uint32_t wcnt[kFineWarps][Q];  // this chunk's count per (warp, fine tile)
+    __shared__ uint32_t wpre[kFineWarps][Q];  // the warp's first position per fine tile
     __shared__ uint32_t run[Q];               // entries per fine tile so far
     __shared__ int32_t start[Q];
     const int t = blockIdx.x;
@@ -191,7 +184,7 @@ __global__ void __launch_bounds__(kWriteThreads, 2048 / kWriteThreads) fine_writ
         start[threadIdx.x] = __ldg(incl + fid) - __ldg(counts + fid);
     }
     __syncthreads();
-    for (int base = r.x; base < r.y; base += kWriteThreads) {
+    for (int base = r.x; base < r.y; base += kFineThreads) {
         const int e = base + (int)threadIdx.x;
         int32_t g = 0;
         uint64_t bits = 0;  // bit q: the entry reaches fine tile q
@@ -212,8 +205,8 @@ __global__ void __launch_bounds__(kWriteThreads, 2048 / kWriteThreads) fine_writ
         __syncthreads();
         // per fine tile (one warp each): exclusive prefix over the warps,
         // offset by the entries of the earlier chunks
-        for (int q = warp; q < Q; q += kWriteWarps) {
-            const uint32_t x = lane < kWriteWarps ? wcnt[lane][q] : 0u;
+        for (int q = warp; q < Q; q += kFineWarps) {
+            const uint32_t x = wcnt[lane][q];
             uint32_t inc = x;
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
@@ -221,7 +214,7 @@ __global__ void __launch_bounds__(kWriteThreads, 2048 / kWriteThreads) fine_writ
                 if (lane >= off) inc += y;
             }
             const uint32_t r0 = run[q];
-            if (lane < kWriteWarps) wpre[lane][q] = r0 + inc - x;
+            wpre[lane][q] = r0 + inc - x;
             __syncwarp();
             if (lane == 31) run[q] = r0 + inc;
             __syncwarp();
@@ -312,7 +305,7 @@ int launch_split(const int64_t* keys, const int32_t* ids, int64_t n_pairs, const
     }
     int rc = rm_host::scan_tiles_status(counts, Gf, incl, total_dev, scan_ws, rm_scan_workspace_size(Gf), status, s);
     if (rc) return rc;
-    rm::fine_write_kernel<PACKED, FS><<<(unsigned)G, rm::kWriteThreads, 0, s>>>(
+    rm::fine_write_kernel<PACKED, FS><<<(unsigned)G, rm::kFineThreads, 0, s>>>(
         ids, (const int2*)ranges, bits, views, counts, incl, fine_ids, capacity, (int2*)fine_ranges, status);
     return rm_host::check_launch("rm_fine_lists (write)");
 }
