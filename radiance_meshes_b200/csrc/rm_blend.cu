@@ -465,6 +465,7 @@ struct FwdPairSmem {
     float ray[6][PX];      // o, d of each slot (structure of arrays)
     float res[6][B][PX];   // a (0: miss), m1, d4, r, g, b per (entry, slot)
     int32_t warp_base[(PX + 31) / 32];
+    float pray[6][PX];     // each owner's own ray, by owner thread (kept out of registers)
 };
 
 template <int PX, int B>
@@ -518,6 +519,10 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
         const float2 j = __ldg(jitter + pix);
         make_ray(cam, px, py, j.x, j.y, o, d);
     }
+    if (owner) {
+        S.pray[0][tid] = o.x; S.pray[1][tid] = o.y; S.pray[2][tid] = o.z;
+        S.pray[3][tid] = d.x; S.pray[4][tid] = d.y; S.pray[5][tid] = d.z;
+    }
     const int2 rg = __ldg(ranges + tile);
     PixelState st = {{0.f, 0.f, 0.f}, 0.f, {0.f, 0.f, 0.f, 0.f, 0.f}};
     int32_t nc = 0;
@@ -539,8 +544,8 @@ __device__ __forceinline__ void fwd_pair_item(int tile, int sub, const int32_t* 
         int slot = rank;
         if (active) {
             for (int w = 0; w < warp; ++w) slot += S.warp_base[w];
-            S.ray[0][slot] = o.x; S.ray[1][slot] = o.y; S.ray[2][slot] = o.z;
-            S.ray[3][slot] = d.x; S.ray[4][slot] = d.y; S.ray[5][slot] = d.z;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) S.ray[k][slot] = S.pray[k][tid];
         }
         __syncthreads();
         // Evaluate.  Rays stay in registers for the whole batch.  With more than
