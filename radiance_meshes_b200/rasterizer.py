@@ -288,7 +288,7 @@ def project_bwd(indices, vertices, cam: RMCamera, tiles, grad_vs, grad_cc, grad_
     return grad_vertices
 
 
-_PAIR_GUESS: dict = {}  # device -> pair count of the last frame built there (reference order of work)
+_PAIR_GUESS: dict = {}  # device -> pair count of the last frame built there
 _SIDE: dict = {}  # device -> (side stream, pinned int64 [2], its numpy view) for the pair-count read
 
 
@@ -368,7 +368,7 @@ def build_tile_lists(tiles: torch.Tensor, rect: torch.Tensor, vs: torch.Tensor, 
 
     if depth_first:
         # the pair count and the status word as the projection left them,
-        # read while the visible tets are ordered by depth
+        # copied to the host on a side stream (read once the build is queued)
         count = torch.empty(2, dtype=torch.int64, device=dev)
         _call("rm_count_pairs", lambda: L.rm_count_pairs(C.ptr(tiles), T, C.ptr(status), C.ptr(count), s))
         pending = _count_read_start(count)
