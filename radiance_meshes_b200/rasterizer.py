@@ -317,6 +317,8 @@ def _count_read_finish(pending) -> tuple[int, int]:
     done, hn = pending
     done.synchronize()
     return int(hn[0]), int(hn[1]) & 0xffffffff
+
+
 _LISTS = {"depth_first": True}
 
 
