@@ -158,3 +158,31 @@ def test_fine_lists_give_the_coarse_frame(cuda, scene, tile, jit):
     assert fine.sorted_ids.shape[0] >= fine.n_pairs
     for a, b in ((gv_f, gv_c), (gc_f, gc_c)):
         assert float((a - b).norm() / b.norm()) < 1e-5
+
+
+def test_dropin_frames_of_changing_size(cuda):
+    """Frames whose pair counts grow and shrink: the lists are built on
+    buffers sized from the previous frame (all queued before the count is
+    read), a frame that outgrows them is built again at its exact size, and
+    every frame's lists, image and distortion equal those of a first frame
+    (buffers of exactly P); no capacity bit is left for the next readback."""
+    from radiance_meshes_b200 import rasterizer as R
+
+    small = scenes.workload_plain_forward()
+    big = scenes.workload_training_step(n_points=20000, seed=2, height=420, width=649)
+    refs = {}
+    for name, (mesh, view) in (("small", small), ("big", big)):
+        R._PAIR_GUESS.clear()  # a first frame: the count read, then exactly P
+        jitter = torch.full((view.height, view.width, 2), 0.5, device="cuda")
+        refs[name] = _dropin_step(mesh, view, jitter, True)[:4]
+    for name in ("small", "big", "big", "small", "big"):
+        mesh, view = small if name == "small" else big
+        jitter = torch.full((view.height, view.width, 2), 0.5, device="cuda")
+        got = _dropin_step(mesh, view, jitter, True)[:4]
+        ids, rg, img, dist = refs[name]
+        assert torch.equal(got[0], ids) and torch.equal(got[1], rg)
+        assert torch.equal(got[2].view(torch.int32), img.view(torch.int32))
+        assert torch.equal(got[3].view(torch.int32), dist.view(torch.int32))
+    n_small = refs["small"][0].shape[0]
+    assert refs["big"][0].shape[0] > n_small + n_small // 4 + 4096  # big after small takes the rebuild
+    R.check_status(len(big[0].indices), torch.device("cuda"))
