@@ -12,6 +12,7 @@ Stage map (reference file:line in delaunay_rasterization/internal/):
 from __future__ import annotations
 
 import ctypes
+import threading
 from dataclasses import dataclass
 
 import torch
@@ -117,12 +118,12 @@ def frame_status(n_tets: int, device, pool: ScratchPool | None = None) -> torch.
     return ws[:4].view(torch.int32)
 
 
-_HOST_READ: dict = {}  # device -> pinned int32 [4]: pair count (int64) and status word
+_HOST_READ: dict = {}  # (device, thread) -> pinned int32 [4]: pair count (int64) and status word
 
 
 def _read_frame(total: torch.Tensor, status: torch.Tensor | None):
     """One synchronisation: the pair count and the frame's status word."""
-    key = str(total.device)
+    key = (str(total.device), threading.get_ident())
     hb = _HOST_READ.get(key)
     if hb is None:
         hb = torch.zeros(4, dtype=torch.int32, pin_memory=True)
@@ -289,7 +290,7 @@ def project_bwd(indices, vertices, cam: RMCamera, tiles, grad_vs, grad_cc, grad_
 
 
 _PAIR_GUESS: dict = {}  # device -> pair count of the last frame built there
-_SIDE: dict = {}  # device -> (side stream, pinned int64 [2], its numpy view) for the pair-count read
+_SIDE: dict = {}  # (device, thread) -> (side stream, pinned int64 [2], its numpy view) for the pair-count read
 
 
 def _count_read_start(count: torch.Tensor):
@@ -298,11 +299,12 @@ def _count_read_start(count: torch.Tensor):
     far only, so the frame's stream goes on with what is queued after this
     call while the host waits in _count_read_finish."""
     dev = count.device
-    st = _SIDE.get(dev)
+    key = (dev, threading.get_ident())  # threads building frames at once each read their own buffer
+    st = _SIDE.get(key)
     if st is None:
         hb = torch.zeros(2, dtype=torch.int64, pin_memory=True)
         st = (torch.cuda.Stream(device=dev), hb, hb.numpy())
-        _SIDE[dev] = st
+        _SIDE[key] = st
     side, hb, hn = st
     side.wait_stream(torch.cuda.current_stream(dev))
     count.record_stream(side)
